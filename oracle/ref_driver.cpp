@@ -1,0 +1,234 @@
+/* Test infrastructure (oracle build only).
+ *
+ * Harness around the reference's own, unmodified host code (compiled from the
+ * reference tree by oracle/Makefile against the shims in oracle/refshim).
+ *
+ *   ref_gen  ACT CON NZONES INNETSEED MZCSEED MZASEED OUT
+ *       builds a new network with the reference's generator
+ *       (CBMState(fstream&, fstream&, nZones, seeds), CBM_STATE_LIB_DEV/src/
+ *       interfaces/cbmstate.cpp:60-64) and writes it with CBMState::writeState
+ *       (cbmstate.cpp:86-103).  Linked against the reference's vendored SFMT.
+ *
+ *   ref_run STATE MFBYTES STEPS TRACE FINALSTATE [SEED...] [-e EVENTS] [-g NGPUP2] [-t]
+ *       loads STATE with CBMState(fstream&) (cbmstate.cpp:12-33), runs STEPS
+ *       calls of updateMFInput + calcActivity (CBM_CORE_LIB_MGPU_DEV/src/
+ *       interface/cbmsimcore.cpp:139-320) and writes one trace record per step
+ *       plus the final state (CBMSimCore::writeToState, cbmsimcore.cpp:75-80).
+ *       -t times the steps and writes no trace.
+ *
+ * After loading, two fields the reference's loader leaves undefined are set
+ * the way the B200 loader sets them:
+ *   - pPCfromPCtoBC: MZoneConnectivityState::stateRW reads pBCfromPCtoBC a
+ *     second time in its place (mzoneconnectivitystate.cpp:150); it is
+ *     rebuilt from connectPCtoBC's formula (mzoneconnectivitystate.cpp:242-257).
+ *   - histPCPopActSum / histPCPopActCurBinN / pcPopAct / errDrive /
+ *     noLTPMFNC / noLTDMFNC: not in the file (mzoneactivitystate.cpp:299-355);
+ *     set to the histogram's sum and zeros.
+ *
+ * Trace record per step (all little-endian, no padding):
+ *   apGR bits  ceil(numGR/8) bytes, GR i at byte i/8 bit i%8
+ *   apGO u8[numGO], vGO f32[numGO], sumGRInputGO u32[numGO]
+ *   apSC u8[numSC], vSC f32[numSC]
+ *   per zone: apBC u8[numBC] vBC f32[numBC] apPC u8[numPC] vPC f32[numPC]
+ *             apIO u8[numIO] vIO f32[numIO] apNC u8[numNC] vNC f32[numNC]
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <fstream>
+#include <iostream>
+#include <chrono>
+
+#include <CBMStateInclude/interfaces/cbmstate.h>
+
+#ifndef CBM_REF_GEN_ONLY
+#include <CBMCoreInclude/interface/cbmsimcore.h>
+uint64_t cbm_refshim_step = 0;
+void cbm_refshim_set_step(uint64_t t) { cbm_refshim_step = t; }
+#endif
+
+static void fixLoadedState(CBMState *st)
+{
+	ConnectivityParams *cp = st->getConParamsInternal();
+	ActivityParams *ap = st->getActParamsInternal();
+	for (unsigned int z = 0; z < st->getNumZones(); z++)
+	{
+		MZoneConnectivityState *cs = st->getMZoneConStateInternal(z);
+		int bcToPCRatio = cp->numBC / cp->numPC;
+		for (int i = 0; i < (int)cp->numPC; i++)
+			for (int j = 0; j < (int)cp->numpPCfromPCtoBC; j++)
+			{
+				int bcInd = i * bcToPCRatio - 6 + j;
+				cs->pPCfromPCtoBC[i][j] = (bcInd % (int)cp->numBC + (int)cp->numBC) % (int)cp->numBC;
+			}
+		MZoneActivityState *as = st->getMZoneActStateInternal(z);
+		ct_uint32_t sum = 0;
+		for (unsigned int k = 0; k < ap->numPopHistBinsPC; k++) sum += as->histPCPopAct[k];
+		as->histPCPopActSum = sum;
+		as->histPCPopActCurBinN = 0;
+		as->pcPopAct = 0;
+		as->errDrive = 0;
+		as->noLTPMFNC = 0;
+		as->noLTDMFNC = 0;
+	}
+}
+
+#ifdef CBM_REF_GEN_ONLY
+int main(int argc, char **argv)
+{
+	if (argc != 8)
+	{
+		fprintf(stderr, "usage: ref_gen ACT CON NZONES INNETSEED MZCSEED MZASEED OUT\n");
+		return 2;
+	}
+	std::fstream act(argv[1], std::ios::in), con(argv[2], std::ios::in);
+	if (!act.good() || !con.good()) { fprintf(stderr, "cannot open params\n"); return 1; }
+	unsigned int nZones = (unsigned int)atoi(argv[3]);
+	int innetSeed = atoi(argv[4]);
+	std::vector<int> cseeds(nZones), aseeds(nZones);
+	for (unsigned int z = 0; z < nZones; z++) { cseeds[z] = atoi(argv[5]) + (int)z; aseeds[z] = atoi(argv[6]) + (int)z; }
+	CBMState st(act, con, nZones, innetSeed, cseeds.data(), aseeds.data());
+	std::fstream out(argv[7], std::ios::out | std::ios::binary | std::ios::trunc);
+	st.writeState(out);
+	out.close();
+	return 0;
+}
+#else
+
+struct Event { unsigned long t; std::string kind; int zone; float a, b; };
+
+static std::vector<Event> readEvents(const char *path)
+{
+	std::vector<Event> ev;
+	std::ifstream f(path);
+	std::string kind;
+	unsigned long t;
+	while (f >> t >> kind)
+	{
+		Event e; e.t = t; e.kind = kind; e.zone = 0; e.a = 0; e.b = 0;
+		if (kind == "errdrive") f >> e.zone >> e.a;
+		else if (kind == "plast") f >> e.zone >> e.a >> e.b;
+		else if (kind == "plastreset") f >> e.zone;
+		else if (kind == "grgoinc") f >> e.a;
+		else if (kind == "grgoincreset") {}
+		else { fprintf(stderr, "bad event %s\n", kind.c_str()); exit(2); }
+		ev.push_back(e);
+	}
+	return ev;
+}
+
+template<typename T> static void put(FILE *f, const T *p, size_t n) { if (n) fwrite(p, sizeof(T), n, f); }
+
+int main(int argc, char **argv)
+{
+	if (argc < 6)
+	{
+		fprintf(stderr, "usage: ref_run STATE MFBYTES STEPS TRACE FINALSTATE [SEED...] [-e EVENTS] [-g NGPUP2] [-t]\n");
+		return 2;
+	}
+	const char *statePath = argv[1], *mfPath = argv[2], *tracePath = argv[4], *finalPath = argv[5];
+	unsigned long steps = strtoul(argv[3], NULL, 10);
+	std::vector<int> seeds;
+	const char *eventsPath = NULL;
+	int numGPUP2 = 0;
+	bool timeOnly = false;
+	for (int i = 6; i < argc; i++)
+	{
+		if (!strcmp(argv[i], "-e") && i + 1 < argc) eventsPath = argv[++i];
+		else if (!strcmp(argv[i], "-g") && i + 1 < argc) numGPUP2 = atoi(argv[++i]);
+		else if (!strcmp(argv[i], "-t")) timeOnly = true;
+		else seeds.push_back(atoi(argv[i]));
+	}
+
+	std::fstream in(statePath, std::ios::in | std::ios::binary);
+	if (!in.good()) { fprintf(stderr, "cannot open state\n"); return 1; }
+	CBMState *st = new CBMState(in);
+	in.close();
+	fixLoadedState(st);
+	ConnectivityParams *cp = st->getConParamsInternal();
+	unsigned int nZones = st->getNumZones();
+	while (seeds.size() < nZones) seeds.push_back(1000 + (int)seeds.size());
+
+	std::vector<ct_uint8_t> mf;
+	{
+		FILE *f = fopen(mfPath, "rb");
+		if (!f) { fprintf(stderr, "cannot open mf\n"); return 1; }
+		mf.resize((size_t)steps * cp->numMF);
+		size_t got = fread(mf.data(), 1, mf.size(), f);
+		fclose(f);
+		if (got != mf.size()) { fprintf(stderr, "mf file too short (%zu of %zu)\n", got, mf.size()); return 1; }
+	}
+	std::vector<Event> events;
+	if (eventsPath) events = readEvents(eventsPath);
+
+	cbm_refshim_set_step(0);
+	CBMSimCore *sim = new CBMSimCore(st, seeds.data(), 0, numGPUP2);
+	InNetInterface *inet = sim->getInputNet();
+	MZoneInterface **zones = sim->getMZoneList();
+
+	FILE *tr = NULL;
+	if (!timeOnly)
+	{
+		tr = fopen(tracePath, "wb");
+		if (!tr) { fprintf(stderr, "cannot open trace\n"); return 1; }
+	}
+	std::vector<ct_uint8_t> bits((cp->numGR + 7) / 8);
+	size_t evi = 0;
+	auto t0 = std::chrono::steady_clock::now();
+	for (unsigned long t = 1; t <= steps; t++)
+	{
+		while (evi < events.size() && events[evi].t == t)
+		{
+			const Event &e = events[evi++];
+			if (e.kind == "errdrive") sim->updateErrDrive((unsigned)e.zone, e.a);
+			else if (e.kind == "plast") zones[e.zone]->setGRPCPlastSteps(e.a, e.b);
+			else if (e.kind == "plastreset") zones[e.zone]->resetGRPCPlastSteps();
+			else if (e.kind == "grgoinc") inet->setGIncGRtoGO(e.a);
+			else if (e.kind == "grgoincreset") inet->resetGIncGRtoGO();
+		}
+		sim->updateMFInput(&mf[(size_t)(t - 1) * cp->numMF]);
+		cbm_refshim_set_step(t);
+		sim->calcActivity();
+		if (timeOnly) continue;
+
+		const ct_uint8_t *apGR = inet->exportAPGR();
+		std::fill(bits.begin(), bits.end(), 0);
+		for (unsigned int i = 0; i < cp->numGR; i++) if (apGR[i]) bits[i >> 3] |= (ct_uint8_t)(1u << (i & 7));
+		put(tr, bits.data(), bits.size());
+		put(tr, inet->exportAPGO(), cp->numGO);
+		put(tr, inet->exportVmGO(), cp->numGO);
+		put(tr, inet->exportSumGRInputGO(), cp->numGO);
+		put(tr, inet->exportAPSC(), cp->numSC);
+		put(tr, inet->exportVmSC(), cp->numSC);
+		for (unsigned int z = 0; z < nZones; z++)
+		{
+			put(tr, zones[z]->exportAPBC(), cp->numBC);
+			put(tr, zones[z]->exportVmBC(), cp->numBC);
+			put(tr, zones[z]->exportAPPC(), cp->numPC);
+			put(tr, zones[z]->exportVmPC(), cp->numPC);
+			put(tr, zones[z]->exportAPIO(), cp->numIO);
+			put(tr, zones[z]->exportVmIO(), cp->numIO);
+			put(tr, zones[z]->exportAPNC(), cp->numNC);
+			put(tr, zones[z]->exportVmNC(), cp->numNC);
+		}
+	}
+	auto t1 = std::chrono::steady_clock::now();
+	double sec = std::chrono::duration<double>(t1 - t0).count();
+	if (tr) fclose(tr);
+	printf("{\"steps\": %lu, \"seconds\": %.6f, \"steps_per_s\": %.3f, \"num_gr\": %u}\n",
+			steps, sec, sec > 0 ? steps / sec : 0.0, cp->numGR);
+	fflush(stdout);
+
+	if (strcmp(finalPath, "-") != 0)
+	{
+		std::fstream out(finalPath, std::ios::out | std::ios::binary | std::ios::trunc);
+		sim->writeToState(out);
+		out.close();
+	}
+	delete sim;
+	delete st;
+	return 0;
+}
+#endif
