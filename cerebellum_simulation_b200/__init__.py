@@ -1,0 +1,322 @@
+"""B200-native cerebellar network step behind the reference's CBM_CORE_LIB API.
+
+Python mirror of the reference's host interface (``CBMState``,
+``CBMSimCore``, ``InNetInterface``, ``MZoneInterface``; see
+``include/cbm_b200.h`` for the C ABI and the reference lines each call
+replaces).  All computation runs in ``libcbm_b200.so`` on the GPU; importing
+this package fails if the library has not been built.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libcbm_b200.so")
+
+CBM_OK = 0
+_DTYPES = {0: np.uint8, 1: np.int32, 2: np.uint32, 3: np.float32, 4: np.uint64}
+
+# enum cbm_field
+FIELDS = [
+    "AP_GR", "VM_GR", "GESUM_GR", "GISUM_GR", "APBUF_GR", "HIST_GR", "THRESH_GR", "GKCA_GR",
+    "AP_GO", "VM_GO", "APBUF_GO", "SUM_GR_INPUT_GO", "SUM_GO_INPUT_GO", "GO_OUT_SCALE_GOGO",
+    "AP_SC", "VM_SC", "APBUF_SC", "HIST_MF", "APBUF_MF",
+    "AP_BC", "VM_BC", "APBUF_BC", "AP_PC", "VM_PC", "APBUF_PC", "AP_IO", "VM_IO", "APBUF_IO",
+    "AP_NC", "VM_NC", "APBUF_NC", "PFPC_WEIGHT", "MFNC_WEIGHT",
+]
+FIELD = {n: i for i, n in enumerate(FIELDS)}
+_FIELD_DTYPE = {
+    "AP": np.uint8, "VM": np.float32, "GESUM": np.float32, "GISUM": np.float32, "APBUF": np.uint32,
+    "HIST": np.uint64, "THRESH": np.float32, "GKCA": np.float32, "SUM": None, "GO": np.float32,
+    "PFPC": np.float32, "MFNC": np.float32,
+}
+
+
+def _field_dtype(name):
+    if name == "SUM_GR_INPUT_GO":
+        return np.uint32
+    if name in ("SUM_GO_INPUT_GO", "GO_OUT_SCALE_GOGO"):
+        return np.float32
+    if name == "HIST_MF":
+        return np.uint8
+    return _FIELD_DTYPE[name.split("_")[0]]
+
+
+class CBMError(RuntimeError):
+    """A failed call of the C ABI; .code holds the CBM_ERR_* status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m cerebellum_simulation_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I, U, F, D, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, ctypes.c_float, ctypes.c_double, ctypes.c_char_p
+    U64, U32 = ctypes.c_uint64, ctypes.c_uint32
+    sig = {
+        "cbm_last_error": (S, []),
+        "cbm_state_load": (I, [S, ctypes.POINTER(P)]),
+        "cbm_state_new": (I, [S, S, U, P, ctypes.POINTER(P)]),
+        "cbm_state_save": (I, [P, S]),
+        "cbm_state_free": (None, [P]),
+        "cbm_state_num_zones": (I, [P, ctypes.POINTER(U)]),
+        "cbm_state_array": (I, [P, S, I, ctypes.POINTER(P), ctypes.POINTER(U64), ctypes.POINTER(I)]),
+        "cbm_state_con_param": (I, [P, S, ctypes.POINTER(U32)]),
+        "cbm_state_act_param": (I, [P, S, ctypes.POINTER(D)]),
+        "cbm_state_set_act_param": (I, [P, S, F]),
+        "cbm_sim_create": (I, [P, P, I, ctypes.POINTER(P)]),
+        "cbm_sim_create_resident": (I, [P, P, I, U64, ctypes.POINTER(P)]),
+        "cbm_sim_update_mf": (I, [P, P]),
+        "cbm_sim_calc_activity": (I, [P]),
+        "cbm_sim_update_err_drive": (I, [P, U, F]),
+        "cbm_sim_set_plast_steps": (I, [P, U, F, F]),
+        "cbm_sim_reset_plast_steps": (I, [P, U]),
+        "cbm_sim_set_ginc_grgo": (I, [P, F]),
+        "cbm_sim_reset_ginc_grgo": (I, [P]),
+        "cbm_sim_export": (I, [P, I, U, P, U64]),
+        "cbm_sim_field_bytes": (U64, [P, I]),
+        "cbm_sim_write_to_state": (I, [P]),
+        "cbm_sim_save": (I, [P, S]),
+        "cbm_sim_steps_done": (I, [P, ctypes.POINTER(U64)]),
+        "cbm_sim_mf_words": (I, [P, ctypes.POINTER(U32)]),
+        "cbm_sim_load_mf_stream": (I, [P, P, U64]),
+        "cbm_sim_run": (I, [P, U64, U32, ctypes.POINTER(F), ctypes.POINTER(F)]),
+        "cbm_sim_algorithmic_bytes_per_step": (D, [P]),
+        "cbm_sim_destroy": (None, [P]),
+        "cbm_device_expf": (I, [I, P, P, U64]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _check(rc):
+    if rc != CBM_OK:
+        raise CBMError(rc, lib.cbm_last_error().decode())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class CBMState:
+    """The reference's CBMState (CBM_STATE_LIB_DEV/CBMStateInclude/interfaces/cbmstate.h:37-62)."""
+
+    def __init__(self, path=None, _handle=None):
+        self._h = ctypes.c_void_p()
+        if _handle is not None:
+            self._h = _handle
+        elif path is not None:
+            _check(lib.cbm_state_load(os.fsencode(path), ctypes.byref(self._h)))
+        else:
+            raise ValueError("CBMState needs a state file path (or use CBMState.new)")
+
+    @classmethod
+    def new(cls, con_text, act_text, n_zones=1, wiring_seeds=None):
+        """CBMState(actPF, conPF, nZones, ...) with input-net wiring left to the caller."""
+        h = ctypes.c_void_p()
+        seeds = None if wiring_seeds is None else np.asarray(wiring_seeds, dtype=np.int32)
+        _check(lib.cbm_state_new(con_text.encode(), act_text.encode(), n_zones, _ptr(seeds), ctypes.byref(h)))
+        return cls(_handle=h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and not getattr(self, "_borrowed", False):
+            lib.cbm_state_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def writeState(self, path):
+        _check(lib.cbm_state_save(self._h, os.fsencode(path)))
+
+    def getNumZones(self):
+        n = ctypes.c_uint()
+        _check(lib.cbm_state_num_zones(self._h, ctypes.byref(n)))
+        return n.value
+
+    def array(self, name, zone=-1):
+        """numpy view of a state array; writes go straight into the state."""
+        data, count, dt = ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_int()
+        _check(lib.cbm_state_array(self._h, name.encode(), zone, ctypes.byref(data), ctypes.byref(count),
+                                   ctypes.byref(dt)))
+        dtype = np.dtype(_DTYPES[dt.value])
+        if count.value == 0:
+            return np.zeros(0, dtype=dtype)
+        buf = (ctypes.c_char * (count.value * dtype.itemsize)).from_address(data.value)
+        return np.frombuffer(buf, dtype=dtype)
+
+    def con(self, name):
+        v = ctypes.c_uint32()
+        _check(lib.cbm_state_con_param(self._h, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    def act(self, name):
+        v = ctypes.c_double()
+        _check(lib.cbm_state_act_param(self._h, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    def setActParam(self, key, value):
+        _check(lib.cbm_state_set_act_param(self._h, key.encode(), value))
+
+
+class _Exporter:
+    def __init__(self, sim, zone):
+        self._sim = sim
+        self._zone = zone
+
+    def _export(self, field):
+        fid = FIELD[field]
+        nbytes = lib.cbm_sim_field_bytes(self._sim._h, fid)
+        out = np.empty(nbytes // np.dtype(_field_dtype(field)).itemsize, dtype=_field_dtype(field))
+        _check(lib.cbm_sim_export(self._sim._h, fid, self._zone, _ptr(out), nbytes))
+        return out
+
+
+class InNet(_Exporter):
+    """InNetInterface (CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/innetinterface.h:18-41)."""
+
+    def setGIncGRtoGO(self, inc):
+        _check(lib.cbm_sim_set_ginc_grgo(self._sim._h, inc))
+
+    def resetGIncGRtoGO(self):
+        _check(lib.cbm_sim_reset_ginc_grgo(self._sim._h))
+
+    def exportAPSC(self): return self._export("AP_SC")
+    def exportAPGO(self): return self._export("AP_GO")
+    def exportAPGR(self): return self._export("AP_GR")
+    def exportHistMF(self): return self._export("HIST_MF")
+    def exportAPBufMF(self): return self._export("APBUF_MF")
+    def exportAPBufGR(self): return self._export("APBUF_GR")
+    def exportAPBufGO(self): return self._export("APBUF_GO")
+    def exportAPBufSC(self): return self._export("APBUF_SC")
+    def exportVmGR(self): return self._export("VM_GR")
+    def exportVmGO(self): return self._export("VM_GO")
+    def exportVmSC(self): return self._export("VM_SC")
+    def exportGESumGR(self): return self._export("GESUM_GR")
+    def exportGISumGR(self): return self._export("GISUM_GR")
+    def exportSumGRInputGO(self): return self._export("SUM_GR_INPUT_GO")
+    def exportSumGOInputGO(self): return self._export("SUM_GO_INPUT_GO")
+    def exportGOOutSynScaleGOGO(self): return self._export("GO_OUT_SCALE_GOGO")
+    def exportHistoryGR(self): return self._export("HIST_GR")
+
+
+class MZone(_Exporter):
+    """MZoneInterface (CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/mzoneinterface.h:18-34)."""
+
+    def setGRPCPlastSteps(self, ltdStep, ltpStep):
+        _check(lib.cbm_sim_set_plast_steps(self._sim._h, self._zone, ltdStep, ltpStep))
+
+    def resetGRPCPlastSteps(self):
+        _check(lib.cbm_sim_reset_plast_steps(self._sim._h, self._zone))
+
+    def exportAPBC(self): return self._export("AP_BC")
+    def exportAPPC(self): return self._export("AP_PC")
+    def exportAPIO(self): return self._export("AP_IO")
+    def exportAPNC(self): return self._export("AP_NC")
+    def exportAPBufBC(self): return self._export("APBUF_BC")
+    def exportAPBufPC(self): return self._export("APBUF_PC")
+    def exportAPBufIO(self): return self._export("APBUF_IO")
+    def exportAPBufNC(self): return self._export("APBUF_NC")
+    def exportVmBC(self): return self._export("VM_BC")
+    def exportVmPC(self): return self._export("VM_PC")
+    def exportVmNC(self): return self._export("VM_NC")
+    def exportVmIO(self): return self._export("VM_IO")
+    def exportPFPCWeights(self): return self._export("PFPC_WEIGHT")
+    def exportMFNCWeights(self): return self._export("MFNC_WEIGHT")
+
+
+class CBMSimCore:
+    """CBMSimCore (CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/cbmsimcore.h:32-75).
+
+    ``mzoneRSeed`` keys each microzone's NC->IO release draws; ``device`` is
+    the GPU that holds the whole network; ``resident_steps`` reserves HBM for
+    that many steps of MF input used by :meth:`run`.
+    """
+
+    def __init__(self, state, mzoneRSeed=None, device=0, resident_steps=0):
+        self.state = state
+        self._h = ctypes.c_void_p()
+        seeds = None if mzoneRSeed is None else np.asarray(mzoneRSeed, dtype=np.int32)
+        if resident_steps:
+            _check(lib.cbm_sim_create_resident(state._h, _ptr(seeds), device, resident_steps, ctypes.byref(self._h)))
+        else:
+            _check(lib.cbm_sim_create(state._h, _ptr(seeds), device, ctypes.byref(self._h)))
+        self._innet = InNet(self, 0)
+        self._zones = [MZone(self, z) for z in range(state.getNumZones())]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.cbm_sim_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def close(self):
+        self.__del__()
+
+    def calcActivity(self):
+        _check(lib.cbm_sim_calc_activity(self._h))
+
+    def updateMFInput(self, mf):
+        mf = np.ascontiguousarray(mf, dtype=np.uint8)
+        _check(lib.cbm_sim_update_mf(self._h, _ptr(mf)))
+
+    def updateErrDrive(self, zoneN, errDriveRelative):
+        _check(lib.cbm_sim_update_err_drive(self._h, zoneN, errDriveRelative))
+
+    def writeToState(self, path=None):
+        if path is None:
+            _check(lib.cbm_sim_write_to_state(self._h))
+        else:
+            _check(lib.cbm_sim_save(self._h, os.fsencode(path)))
+
+    def getInputNet(self):
+        return self._innet
+
+    def getMZoneList(self):
+        return self._zones
+
+    # ---- beyond the reference API: resident input, graph-captured runs
+    def steps_done(self):
+        v = ctypes.c_uint64()
+        _check(lib.cbm_sim_steps_done(self._h, ctypes.byref(v)))
+        return v.value
+
+    def mf_words(self):
+        v = ctypes.c_uint32()
+        _check(lib.cbm_sim_mf_words(self._h, ctypes.byref(v)))
+        return v.value
+
+    def load_mf_stream(self, bits):
+        bits = np.ascontiguousarray(bits, dtype=np.uint32)
+        _check(lib.cbm_sim_load_mf_stream(self._h, _ptr(bits), bits.shape[0]))
+
+    def run(self, nsteps, chunk=50, time_pass=False):
+        ms, pms = ctypes.c_float(), ctypes.c_float()
+        _check(lib.cbm_sim_run(self._h, nsteps, chunk, ctypes.byref(ms), ctypes.byref(pms) if time_pass else None))
+        return ms.value, (pms.value if time_pass else None)
+
+    def algorithmic_bytes_per_step(self):
+        return lib.cbm_sim_algorithmic_bytes_per_step(self._h)
+
+
+def mf_bits(mf_bytes, words):
+    """Pack [steps, numMF] spike bytes into [steps, words] uint32 bit rows."""
+    mf = np.asarray(mf_bytes, dtype=np.uint8) != 0
+    steps, n = mf.shape
+    pad = np.zeros((steps, words * 32), dtype=bool)
+    pad[:, :n] = mf
+    return np.ascontiguousarray(np.packbits(pad, axis=1, bitorder="little").view("<u4")).astype(np.uint32)
+
+
+def device_expf(x, device=0):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    _check(lib.cbm_device_expf(device, _ptr(x), _ptr(out), x.size))
+    return out

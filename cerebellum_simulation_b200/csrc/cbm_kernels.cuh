@@ -1,0 +1,18 @@
+// Kernel entry points of the step (definitions in cbm_kernels.cu).
+#pragma once
+#include <cstdint>
+#include "cbm_device.cuh"
+
+namespace cbm {
+
+constexpr int kPassThreads = 256;
+constexpr int kTailThreads = 1024;
+
+__global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOffset, int numNets,
+		uint32_t stepOffset);
+__global__ void tailKernel(const DevNet *const *nets, uint32_t stepOffset);
+__global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
+__global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);
+__global__ void expfProbeKernel(const float *in, float *out, uint32_t n);
+
+}  // namespace cbm

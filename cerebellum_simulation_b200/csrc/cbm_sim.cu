@@ -1,0 +1,767 @@
+// Host orchestration of the device-resident step; see cbm_sim.hpp.
+#include "cbm_sim.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+
+#include "cbm_kernels.cuh"
+#include "cbm_rng.hpp"
+
+namespace cbm {
+
+std::string cudaErr(cudaError_t e, const char *what)
+{
+	if (e == cudaSuccess) return "";
+	return std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+#define CK(call, what) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return cudaErr(e_, what); } while (0)
+#define CKS(expr) do { std::string s_ = (expr); if (!s_.empty()) return s_; } while (0)
+
+// ------------------------------------------------------------------ Network
+template <typename T> T *Network::alloc(size_t n)
+{
+	void *p = nullptr;
+	size_t bytes = std::max<size_t>(n * sizeof(T), 16);
+	if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+	cudaMemset(p, 0, bytes);
+	allocs_.push_back(p);
+	return (T *)p;
+}
+
+template <typename T> T *Network::upload(const T *src, size_t n)
+{
+	T *d = alloc<T>(n);
+	if (d && n) cudaMemcpy(d, src, n * sizeof(T), cudaMemcpyHostToDevice);
+	return d;
+}
+
+Network::~Network()
+{
+	for (void *p : allocs_) cudaFree(p);
+	if (dNet_.ptr) cudaFree(dNet_.ptr);
+	if (hPinnedBits_) cudaFreeHost(hPinnedBits_);
+	if (hPinnedRaw_) cudaFreeHost(hPinnedRaw_);
+}
+
+// callSumKernel's block size for a row of rowLength elements
+// (CBM_CORE_LIB_MGPU_DEV/src/cuda/kernels.cu:445-469)
+static uint32_t reductionBlockSize(uint32_t rowLength)
+{
+	if (rowLength >= 2048) return 512;
+	if (rowLength >= 512) return 128;
+	if (rowLength >= 128) return 32;
+	if (rowLength >= 32) return 8;
+	return 2;
+}
+
+static bool singleBitOrZero(uint32_t m, uint32_t &bit)
+{
+	if (m == 0) { bit = kNoDelay; return true; }
+	if (m & (m - 1)) return false;
+	bit = (uint32_t)__builtin_ctz(m);
+	return true;
+}
+
+size_t Network::passSmemBytes() const
+{
+	return sizeof(uint32_t) * ((size_t)h_.mfWords + h_.goWords + h_.bcLocal + h_.scLocal) +
+		sizeof(float) * (size_t)h_.numZones * 2 * h_.K * h_.J;
+}
+
+size_t Network::tailSmemBytes() const
+{
+	return sizeof(float) * (size_t)(kTailThreads / 32) * 2 * h_.numpNCfromMFtoNC;
+}
+
+double Network::bytesPerStepAlgorithmic() const
+{
+	return (72.0 + 4.0 * avgMF_ + 4.0 * avgGO_ + 8.0 * avgOut_) * h_.numGR;
+}
+
+std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mfRing, uint32_t mfSeed)
+{
+	(void)mfSeed;
+	st_ = st;
+	const ConParams &c = st->cp;
+	const ActParams &a = st->ap;
+	if (st->numZones < 1 || st->numZones > (uint32_t)kMaxZones) return "zone count must be 1..4";
+	if (c.numMF >= 65535 || c.numGO >= 65535) return "numMF and numGO must be below 65535";
+	const uint32_t N = c.numGR, P = c.numpPCfromGRtoPC;
+	if (P < 4 || (P & (P - 1)) || N % 32) return "GR per PC must be a power of two >= 4 and numGR a multiple of 32";
+	if ((1u << c.numpBCfromGRtoBCP2) != c.numpBCfromGRtoBC || (1u << c.numpSCfromGRtoSCP2) != c.numpSCfromGRtoSC)
+		return "PF->BC/SC block sizes are not powers of two";
+	if (a.tsPerHistBinGR == 0 || a.numTSinMFHist == 0 || a.tsPerPopHistBinPC == 0 || a.numPopHistBinsPC == 0)
+		return "time-bin parameters must be positive";
+
+	DevNet &h = h_;
+	h.numGR = N; h.numMF = c.numMF; h.numGO = c.numGO; h.numSC = c.numSC; h.numBC = c.numBC;
+	h.numPC = c.numPC; h.numNC = c.numNC; h.numIO = c.numIO; h.numZones = st->numZones;
+	h.P = P; h.bs = reductionBlockSize(P); h.K = P / (2 * h.bs); h.J = std::min<uint32_t>(32, h.bs);
+	h.tilesPerPC = h.bs / h.J;
+	h.bcShift = c.numpBCfromGRtoBCP2; h.scShift = c.numpSCfromGRtoSCP2;
+	h.bcLocal = std::max<uint32_t>(1, P >> h.bcShift);
+	h.scLocal = std::max<uint32_t>(1, P >> h.scShift);
+	h.mfWords = c.numMF / 32 + 1; h.goWords = c.numGO / 32 + 1;
+	h.maxnumpMFfromMFtoGO = c.maxnumpMFfromMFtoGO; h.maxnumpGOCoupInGOGO = c.maxnumpGOCoupInGOGO;
+	h.numpPCfromSCtoPC = c.numpPCfromSCtoPC; h.numpNCfromPCtoNC = c.numpNCfromPCtoNC;
+	h.numpNCfromMFtoNC = c.numpNCfromMFtoNC; h.numpIOfromNCtoIO = c.numpIOfromNCtoIO;
+	h.numpIOInIOIO = c.numpIOInIOIO;
+	h.numPopHistBinsPC = a.numPopHistBinsPC; h.tsPerPopHistBinPC = a.tsPerPopHistBinPC;
+	h.tsPerHistBinGR = a.tsPerHistBinGR; h.numTSinMFHist = a.numTSinMFHist;
+	h.mfRing = std::max<uint32_t>(1, mfRing);
+
+	// parameters
+	h.gLeakGR = a.gLeakGR; h.eLeakGR = a.eLeakGR; h.eGOGR = a.eGOGR; h.threshRestGR = a.threshRestGR;
+	h.threshMaxGR = a.threshMaxGR; h.threshDecGR = a.threshDecGR;
+	h.gDecMFtoGR = a.gDecMFtoGR; h.gIncMFtoGR = a.gIncMFtoGR; h.gDecGOtoGR = a.gDecGOtoGR; h.gIncGOtoGR = a.gIncGOtoGR;
+	h.gIncMFtoGO = a.gIncMFtoGO; h.gDecMFtoGO = a.gDecMFtoGO; h.gDecGRtoGO = a.gDecGRtoGO;
+	h.gGABAIncGOtoGO = a.gGABAIncGOtoGO; h.gGABADecGOtoGO = a.gGABADecGOtoGO; h.gluDecayGO = a.gluDecayGO;
+	h.gluScaleGO = a.gluScaleGO; h.mGluRDecayGO = a.mGluRDecayGO; h.mGluRScaleGO = a.mGluRScaleGO;
+	h.gMGluRIncDecayGO = a.gMGluRIncDecayGO; h.gMGluRIncScaleGO = a.gMGluRIncScaleGO;
+	h.gMGluRDecGRtoGO = a.gMGluRDecGRtoGO; h.gMGluRScaleGRtoGO = a.gMGluRScaleGRtoGO;
+	h.threshRestGO = a.threshRestGO; h.threshDecGO = a.threshDecGO; h.gLeakGO = a.gLeakGO;
+	h.eLeakGO = a.eLeakGO; h.eGABAGO = a.eGABAGO; h.threshMaxGO = a.threshMaxGO;
+	h.coupleRiRjRatioGO = a.coupleRiRjRatioGO; h.goGABAGOGOSynRec = a.goGABAGOGOSynRec;
+	h.goGABAGOGOSynDepF = a.goGABAGOGOSynDepF;
+	h.gIncGRtoSC = a.gIncGRtoSC; h.gDecGRtoSC = a.gDecGRtoSC; h.gLeakSC = a.gLeakSC; h.eLeakSC = a.eLeakSC;
+	h.threshDecSC = a.threshDecSC; h.threshRestSC = a.threshRestSC; h.threshMaxSC = a.threshMaxSC;
+	h.gIncGRtoBC = a.gIncGRtoBC; h.gDecGRtoBC = a.gDecGRtoBC; h.gIncPCtoBC = a.gIncPCtoBC;
+	h.gDecPCtoBC = a.gDecPCtoBC; h.gLeakBC = a.gLeakBC; h.eLeakBC = a.eLeakBC; h.ePCtoBC = a.ePCtoBC;
+	h.threshDecBC = a.threshDecBC; h.threshRestBC = a.threshRestBC; h.threshMaxBC = a.threshMaxBC;
+	h.gIncGRtoPC = a.gIncGRtoPC; h.gDecGRtoPC = a.gDecGRtoPC; h.gIncBCtoPC = a.gIncBCtoPC;
+	h.gDecBCtoPC = a.gDecBCtoPC; h.gIncSCtoPC = a.gIncSCtoPC; h.gDecSCtoPC = a.gDecSCtoPC;
+	h.gLeakPC = a.gLeakPC; h.eLeakPC = a.eLeakPC; h.eBCtoPC = a.eBCtoPC; h.eSCtoPC = a.eSCtoPC;
+	h.threshDecPC = a.threshDecPC; h.threshRestPC = a.threshRestPC; h.threshMaxPC = a.threshMaxPC;
+	h.msPerTimeStep = a.msPerTimeStep; h.gDecTSofNCtoIO = a.gDecTSofNCtoIO; h.gDecTTofNCtoIO = a.gDecTTofNCtoIO;
+	h.gDecT0ofNCtoIO = a.gDecT0ofNCtoIO; h.gIncNCtoIO = a.gIncNCtoIO; h.gIncTauNCtoIO = a.gIncTauNCtoIO;
+	h.gLeakIO = a.gLeakIO; h.eLeakIO = a.eLeakIO; h.eNCtoIO = a.eNCtoIO; h.threshMaxIO = a.threshMaxIO;
+	h.threshDecIO = a.threshDecIO; h.threshRestIO = a.threshRestIO; h.coupleRiRjRatioIO = a.coupleRiRjRatioIO;
+	h.tsLTDStartAPIO = a.tsLTDStartAPIO; h.tsLTDEndIO = a.tsLTDStartAPIO + ((int)(a.tsLTDDurationIO));
+	h.tsLTPStartAPIO = a.tsLTPStartAPIO;
+	h.gmaxNMDADecMFtoNC = a.gmaxNMDADecMFtoNC; h.gNMDAIncMFtoNC = a.gNMDAIncMFtoNC;
+	h.gmaxAMPADecMFtoNC = a.gmaxAMPADecMFtoNC; h.gAMPAIncMFtoNC = a.gAMPAIncMFtoNC;
+	h.gDecPCtoNC = a.gDecPCtoNC; h.gLeakNC = a.gLeakNC; h.eLeakNC = a.eLeakNC; h.ePCtoNC = a.ePCtoNC;
+	h.threshDecNC = a.threshDecNC; h.threshRestNC = a.threshRestNC; h.threshMaxNC = a.threshMaxNC;
+	h.relPDecTSofNCtoIO = a.relPDecTSofNCtoIO; h.relPDecTTofNCtoIO = a.relPDecTTofNCtoIO;
+	h.relPDecT0ofNCtoIO = a.relPDecT0ofNCtoIO; h.relPIncNCtoIO = a.relPIncNCtoIO;
+	h.relPIncTauNCtoIO = a.relPIncTauNCtoIO;
+	h.synLTDPCPopActThreshMFtoNC = a.synLTDPCPopActThreshMFtoNC;
+	h.synLTPPCPopActThreshMFtoNC = a.synLTPPCPopActThreshMFtoNC;
+	h.synLTDStepSizeMFtoNC = a.synLTDStepSizeMFtoNC; h.synLTPStepSizeMFtoNC = a.synLTPStepSizeMFtoNC;
+
+	auto A = [&](const char *n, int z = -1) -> NamedArray * { return st->find(n, z); };
+
+	// ---- GR synapse tables: [gr][slot] (reference) -> [slot][gr] with
+	// sentinel padding; counts and indices are checked here once so the
+	// kernels need no bounds checks.
+	const int32_t *numMFin = A("numpGRfromMFtoGR")->as<int32_t>();
+	const uint32_t *pMF = A("pGRfromMFtoGR")->as<uint32_t>();
+	const int32_t *numGOin = A("numpGRfromGOtoGR")->as<int32_t>();
+	const uint32_t *pGO = A("pGRfromGOtoGR")->as<uint32_t>();
+	const int32_t *numOut = A("numpGRfromGRtoGO")->as<int32_t>();
+	const uint32_t *pOut = A("pGRfromGRtoGO")->as<uint32_t>();
+	const uint32_t *pOutMask = A("pGRDelayMaskfromGRtoGO")->as<uint32_t>();
+	const uint32_t *pfMask = A("pGRDelayMaskfromGRtoBSP")->as<uint32_t>();
+	const uint32_t strideGO = c.maxnumpGRfromGOtoGR, strideOut = c.maxnumpGRfromGRtoGO;
+	uint32_t nMF = 0, nGO = 0, nOut = 0;
+	uint64_t sumMF = 0, sumGO = 0, sumOut = 0;
+	for (uint32_t g = 0; g < N; g++) {
+		if (numMFin[g] < 0 || (uint32_t)numMFin[g] > c.maxnumpGRfromMFtoGR) return "MF->GR count out of range";
+		if (numGOin[g] < 0 || (uint32_t)numGOin[g] > c.maxnumpGRfromGOtoGR) return "GO->GR count out of range";
+		if (numOut[g] < 0 || (uint32_t)numOut[g] > c.maxnumpGRfromGRtoGO) return "GR->GO count out of range";
+		nMF = std::max<uint32_t>(nMF, numMFin[g]); nGO = std::max<uint32_t>(nGO, numGOin[g]);
+		nOut = std::max<uint32_t>(nOut, numOut[g]);
+		sumMF += numMFin[g]; sumGO += numGOin[g]; sumOut += numOut[g];
+	}
+	avgMF_ = (double)sumMF / N; avgGO_ = (double)sumGO / N; avgOut_ = (double)sumOut / N;
+	h.nMFSlots = nMF; h.nGOSlots = nGO; h.nOutSlots = nOut;
+	std::vector<uint16_t> mfIdx((size_t)std::max(1u, nMF) * N, (uint16_t)c.numMF);
+	std::vector<uint16_t> goIdx((size_t)std::max(1u, nGO) * N, (uint16_t)c.numGO);
+	std::vector<uint32_t> outCon((size_t)std::max(1u, nOut) * N, kNoDelay);
+	std::vector<uint8_t> pfDelay(N);
+	for (uint32_t g = 0; g < N; g++) {
+		for (int k = 0; k < numMFin[g]; k++) {
+			uint32_t v = pMF[(size_t)g * strideGO + k];
+			if (v >= c.numMF) return "MF->GR index out of range";
+			mfIdx[(size_t)k * N + g] = (uint16_t)v;
+		}
+		for (int k = 0; k < numGOin[g]; k++) {
+			uint32_t v = pGO[(size_t)g * strideGO + k];
+			if (v >= c.numGO) return "GO->GR index out of range";
+			goIdx[(size_t)k * N + g] = (uint16_t)v;
+		}
+		for (int k = 0; k < numOut[g]; k++) {
+			uint32_t v = pOut[(size_t)g * strideOut + k], bit;
+			if (v >= c.numGO) return "GR->GO index out of range";
+			if (!singleBitOrZero(pOutMask[(size_t)g * strideOut + k], bit)) return "GR->GO delay masks must have one bit";
+			outCon[(size_t)k * N + g] = (v << 8) | bit;
+		}
+		uint32_t bit;
+		if (!singleBitOrZero(pfMask[g], bit)) return "PF delay masks must have one bit";
+		pfDelay[g] = (uint8_t)bit;
+	}
+	h.mfIdx = upload(mfIdx.data(), mfIdx.size());
+	h.goIdx = upload(goIdx.data(), goIdx.size());
+	h.outCon = upload(outCon.data(), outCon.size());
+	h.pfDelay = upload(pfDelay.data(), pfDelay.size());
+
+	auto upF = [&](const char *n, int z = -1) { NamedArray *x = A(n, z); return upload(x->as<float>(), x->count); };
+	auto upU = [&](const char *n, int z = -1) { NamedArray *x = A(n, z); return upload(x->as<uint32_t>(), x->count); };
+	auto upB = [&](const char *n, int z = -1) { NamedArray *x = A(n, z); return upload(x->as<uint8_t>(), x->count); };
+	auto upI = [&](const char *n, int z = -1) { NamedArray *x = A(n, z); return upload(x->as<int32_t>(), x->count); };
+
+	h.vGR = upF("vGR"); h.gKCaGR = upF("gKCaGR"); h.threshGR = upF("threshGR");
+	h.gESum = upF("gMFSumGR"); h.gISum = upF("gGOSumGR");
+	h.apBufGR = upU("apBufGR");
+	h.historyGR = upload(A("historyGR")->as<uint64_t>(), N);
+
+	h.histMF = upB("histMF"); h.apBufMF = upU("apBufMF");
+	h.apGO = upB("apGO"); h.apBufGO = upU("apBufGO"); h.vGO = upF("vGO"); h.vCoupleGO = upF("vCoupleGO");
+	h.threshCurGO = upF("threshCurGO"); h.inputMFGO = upU("inputMFGO"); h.inputGOGO = upU("inputGOGO");
+	h.inputGOGABASynDepGO = upF("inputGOGABASynDepGO"); h.goGABAOutSynScaleGOGO = upF("goGABAOutSynScaleGOGO");
+	h.gMFGO = upF("gMFGO"); h.gGRGO = upF("gGRGO"); h.gGOGO = upF("gGOGO"); h.gMGluRGO = upF("gMGluRGO");
+	h.gMGluRIncGO = upF("gMGluRIncGO"); h.mGluRGO = upF("mGluRGO"); h.gluGO = upF("gluGO");
+	h.apSC = upB("apSC"); h.apBufSC = upU("apBufSC"); h.gPFSC = upF("gPFSC"); h.threshSC = upF("threshSC");
+	h.vSC = upF("vSC");
+	h.sumGRInputGO = alloc<uint32_t>(c.numGO); h.sumInputGOGABASynDepGO = alloc<float>(c.numGO);
+	h.threshSnap = alloc<float>(c.numGO);
+
+	// MF->GO out-lists as stored; GO->GO in-lists per destination in the
+	// reference's (source, slot) iteration order (innet.cpp:937-950)
+	const int32_t *numMFGO = A("numpMFfromMFtoGO")->as<int32_t>();
+	const uint32_t *pMFGO = A("pMFfromMFtoGO")->as<uint32_t>();
+	for (uint32_t i = 0; i < c.numMF; i++) {
+		if (numMFGO[i] < 0 || (uint32_t)numMFGO[i] > c.maxnumpMFfromMFtoGO) return "MF->GO count out of range";
+		for (int j = 0; j < numMFGO[i]; j++) if (pMFGO[(size_t)i * c.maxnumpMFfromMFtoGO + j] >= c.numGO) return "MF->GO index out of range";
+	}
+	h.numpMFfromMFtoGO = upI("numpMFfromMFtoGO"); h.pMFfromMFtoGO = upU("pMFfromMFtoGO");
+	{
+		const int32_t *numOutGG = A("numpGOGABAOutGOGO")->as<int32_t>();
+		const uint32_t *pOutGG = A("pGOGABAOutGOGO")->as<uint32_t>();
+		std::vector<std::vector<uint32_t>> in(c.numGO);
+		for (uint32_t i = 0; i < c.numGO; i++) {
+			if (numOutGG[i] < 0 || (uint32_t)numOutGG[i] > c.maxnumpGOGABAOutGOGO) return "GO->GO count out of range";
+			for (int j = 0; j < numOutGG[i]; j++) {
+				uint32_t d = pOutGG[(size_t)i * c.maxnumpGOGABAOutGOGO + j];
+				if (d >= c.numGO) return "GO->GO index out of range";
+				in[d].push_back(i);
+			}
+		}
+		std::vector<uint32_t> start(c.numGO + 1, 0), src;
+		for (uint32_t d = 0; d < c.numGO; d++) { start[d + 1] = start[d] + (uint32_t)in[d].size(); src.insert(src.end(), in[d].begin(), in[d].end()); }
+		h.gogoStart = upload(start.data(), start.size());
+		h.gogoSrc = upload(src.data(), src.size());
+	}
+	{
+		const int32_t *numC = A("numpGOCoupInGOGO")->as<int32_t>();
+		const uint32_t *pC = A("pGOCoupInGOGO")->as<uint32_t>();
+		bool any = false;
+		std::vector<uint32_t> level(c.numGO, 0);
+		uint32_t maxLevel = 0;
+		for (uint32_t i = 0; i < c.numGO; i++) {
+			if (numC[i] < 0 || (uint32_t)numC[i] > c.maxnumpGOCoupInGOGO) return "GO coupling count out of range";
+			for (int j = 0; j < numC[i]; j++) {
+				uint32_t n = pC[(size_t)i * c.maxnumpGOCoupInGOGO + j];
+				if (n >= c.numGO) return "GO coupling index out of range";
+				any = true;
+				if (n < i) level[i] = std::max(level[i], level[n] + 1);
+			}
+			maxLevel = std::max(maxLevel, level[i]);
+		}
+		h.numpGOCoupInGOGO = upI("numpGOCoupInGOGO"); h.pGOCoupInGOGO = upU("pGOCoupInGOGO");
+		std::vector<uint32_t> lstart, lgo;
+		if (any) {
+			h.numCoupLevels = maxLevel + 1;
+			lstart.assign(maxLevel + 2, 0);
+			for (uint32_t i = 0; i < c.numGO; i++) lstart[level[i] + 1]++;
+			for (uint32_t L = 0; L <= maxLevel; L++) lstart[L + 1] += lstart[L];
+			lgo.assign(c.numGO, 0);
+			std::vector<uint32_t> fillPos(lstart.begin(), lstart.end() - 1);
+			for (uint32_t i = 0; i < c.numGO; i++) lgo[fillPos[level[i]]++] = i;
+		} else {
+			h.numCoupLevels = 0;
+			lstart.assign(1, 0);
+			lgo.assign(1, 0);
+		}
+		h.coupLevelStart = upload(lstart.data(), lstart.size());
+		h.coupLevelGO = upload(lgo.data(), lgo.size());
+	}
+
+	// ---- microzones
+	const uint32_t numGRPerIO = N / c.numIO;
+	for (uint32_t z = 0; z < st->numZones; z++) {
+		DevZone &Q = h.zones[z];
+		Q.w = upF("pfSynWeightPC", z);
+		Q.pcPartial = alloc<float>((size_t)3 * c.numPC * h.bs);
+		Q.plastSel = alloc<uint8_t>((size_t)2 * c.numIO);
+		std::vector<uint32_t> ioOfPC(c.numPC);
+		uint32_t cur = 0;
+		for (uint32_t pc = 0; pc < c.numPC; pc++) {
+			// runPFPCPlastCUDA's IO walk (mzone.cpp:682-705)
+			if (pc * P >= (cur + 1) * numGRPerIO) cur++;
+			ioOfPC[pc] = std::min<uint32_t>(cur, c.numIO - 1);
+		}
+		Q.ioOfPC = upload(ioOfPC.data(), ioOfPC.size());
+		auto chk = [&](const char *n, uint32_t lim) -> bool {
+			NamedArray *x = A(n, z);
+			const uint32_t *p = x->as<uint32_t>();
+			for (size_t k = 0; k < x->count; k++) if (p[k] >= lim) return false;
+			return true;
+		};
+		if (!chk("pPCfromSCtoPC", c.numSC) || !chk("pNCfromPCtoNC", c.numPC) || !chk("pNCfromMFtoNC", c.numMF) ||
+				!chk("pIOfromNCtoIO", c.numNC) || !chk("pIOInIOIO", c.numIO) || !chk("pBCfromBCtoPC", c.numPC) ||
+				!chk("pPCfromPCtoBC", c.numBC))
+			return "microzone connectivity index out of range";
+		Q.pPCfromSCtoPC = upU("pPCfromSCtoPC", z); Q.pNCfromPCtoNC = upU("pNCfromPCtoNC", z);
+		Q.pNCfromMFtoNC = upU("pNCfromMFtoNC", z); Q.pIOfromNCtoIO = upU("pIOfromNCtoIO", z);
+		Q.pIOInIOIO = upU("pIOInIOIO", z);
+		{
+			const uint32_t *bcpc = A("pBCfromBCtoPC", z)->as<uint32_t>();
+			std::vector<std::vector<uint32_t>> in(c.numPC);
+			for (uint32_t bc = 0; bc < c.numBC; bc++)
+				for (uint32_t j = 0; j < c.numpBCfromBCtoPC; j++) in[bcpc[(size_t)bc * c.numpBCfromBCtoPC + j]].push_back(bc);
+			std::vector<uint32_t> start(c.numPC + 1, 0), src;
+			for (uint32_t i = 0; i < c.numPC; i++) { start[i + 1] = start[i] + (uint32_t)in[i].size(); src.insert(src.end(), in[i].begin(), in[i].end()); }
+			Q.bcpcStart = upload(start.data(), start.size()); Q.bcpcSrc = upload(src.data(), src.size());
+		}
+		{
+			const uint32_t *pcbc = A("pPCfromPCtoBC", z)->as<uint32_t>();
+			std::vector<std::vector<uint32_t>> in(c.numBC);
+			for (uint32_t pc = 0; pc < c.numPC; pc++)
+				for (uint32_t j = 0; j < c.numpPCfromPCtoBC; j++) in[pcbc[(size_t)pc * c.numpPCfromPCtoBC + j]].push_back(pc);
+			std::vector<uint32_t> start(c.numBC + 1, 0), src;
+			for (uint32_t i = 0; i < c.numBC; i++) { start[i + 1] = start[i] + (uint32_t)in[i].size(); src.insert(src.end(), in[i].begin(), in[i].end()); }
+			Q.pcbcStart = upload(start.data(), start.size()); Q.pcbcSrc = upload(src.data(), src.size());
+		}
+		Q.apBC = upB("apBC", z); Q.apBufBC = upU("apBufBC", z); Q.inputPCBC = upU("inputPCBC", z);
+		Q.gPFBC = upF("gPFBC", z); Q.gPCBC = upF("gPCBC", z); Q.threshBC = upF("threshBC", z); Q.vBC = upF("vBC", z);
+		Q.apPC = upB("apPC", z); Q.apBufPC = upU("apBufPC", z); Q.inputBCPC = upU("inputBCPC", z);
+		Q.inputSCPC = upB("inputSCPC", z); Q.gPFPC = upF("gPFPC", z); Q.gBCPC = upF("gBCPC", z);
+		Q.gSCPC = upF("gSCPC", z); Q.vPC = upF("vPC", z); Q.threshPC = upF("threshPC", z);
+		Q.histPCPopAct = upU("histPCPopAct", z);
+		const ZoneScalars &zs = st->zoneScalars[z];
+		uint32_t sc[5] = {zs.histPCPopActSum, zs.histPCPopActCurBinN, zs.pcPopAct, zs.noLTPMFNC, zs.noLTDMFNC};
+		Q.scal = upload(sc, 5);
+		Q.apIO = upB("apIO", z); Q.apBufIO = upU("apBufIO", z); Q.inputNCIO = upB("inputNCIO", z);
+		Q.gNCIO = upF("gNCIO", z); Q.threshIO = upF("threshIO", z); Q.vIO = upF("vIO", z);
+		Q.vCoupleIO = upF("vCoupleIO", z); Q.pfPCPlastTimerIO = upI("pfPCPlastTimerIO", z);
+		Q.apNC = upB("apNC", z); Q.apBufNC = upU("apBufNC", z); Q.inputPCNC = upB("inputPCNC", z);
+		Q.inputMFNC = upB("inputMFNC", z); Q.gPCNC = upF("gPCNC", z); Q.gPCScaleNC = upF("gPCScaleNC", z);
+		Q.mfSynWeightNC = upF("mfSynWeightNC", z); Q.gmaxNMDAofMFtoNC = upF("gmaxNMDAofMFtoNC", z);
+		Q.gmaxAMPAofMFtoNC = upF("gmaxAMPAofMFtoNC", z); Q.gMFNMDANC = upF("gMFNMDANC", z);
+		Q.gMFAMPANC = upF("gMFAMPANC", z); Q.threshNC = upF("threshNC", z); Q.vNC = upF("vNC", z);
+		Q.synIOPReleaseNC = upF("synIOPReleaseNC", z);
+		int seed = z < seeds.size() ? seeds[z] : 1000 + (int)z;
+		Q.ncioKey = rng::streamKey((uint32_t)seed, rng::kStreamNCIO);
+		// plasticity selector for step 1 (the tail of step t sets it for t+1)
+		std::vector<uint8_t> sel(2 * c.numIO, 0);
+		if (1 % a.tsPerHistBinGR == 0) {
+			const int32_t *tm = A("pfPCPlastTimerIO", z)->as<int32_t>();
+			for (uint32_t i = 0; i < c.numIO; i++)
+				sel[c.numIO + i] = tm[i] < h.tsLTDEndIO ? 1 : (tm[i] > h.tsLTPStartAPIO ? 2 : 0);
+		}
+		cudaMemcpy(Q.plastSel, sel.data(), sel.size(), cudaMemcpyHostToDevice);
+		ctl.ltdStep[z] = a.synLTDStepSizeGRtoPC;
+		ctl.ltpStep[z] = a.synLTPStepSizeGRtoPC;
+		ctl.errDrive[z] = zs.errDrive;
+	}
+	ctl.gIncGRtoGO = a.gIncGRtoGO;
+	ctlDirty = true;
+
+	// ---- pipeline and control
+	h.goCount = alloc<uint32_t>((size_t)2 * c.numGO);
+	h.bcCount = alloc<uint32_t>((size_t)3 * c.numBC);
+	h.scCount = alloc<uint32_t>((size_t)3 * c.numSC);
+	h.goBits = alloc<uint32_t>((size_t)2 * h.goWords);
+	h.mfBits = alloc<uint32_t>((size_t)h.mfRing * h.mfWords);
+	h.mfRaw = alloc<uint8_t>((size_t)h.mfRing * c.numMF);
+	h.hasMFRaw = 0;
+	h.tBase = alloc<uint64_t>(1);
+	h.ctl = alloc<HostCtl>(1);
+	h.errFlag = alloc<uint32_t>(1);
+	for (void *p : allocs_) if (!p) return "device allocation failed";
+	if (cudaMallocHost((void **)&hPinnedBits_, (size_t)h.mfWords * 4) != cudaSuccess ||
+			cudaMallocHost((void **)&hPinnedRaw_, (size_t)c.numMF) != cudaSuccess)
+		return "pinned allocation failed";
+	CK(cudaMalloc(&dNet_.ptr, sizeof(DevNet)), "allocating the network descriptor");
+	dNet_.bytes = sizeof(DevNet);
+	CK(cudaMemcpy(dNet_.ptr, &h, sizeof(DevNet), cudaMemcpyHostToDevice), "uploading the network descriptor");
+	CK(cudaDeviceSynchronize(), "network build");
+	hostT_ = 0;
+	return "";
+}
+
+void Network::setPlastSteps(uint32_t z, float ltd, float ltp) { ctl.ltdStep[z] = ltd; ctl.ltpStep[z] = ltp; ctlDirty = true; }
+void Network::resetPlastSteps(uint32_t z)
+{
+	ctl.ltdStep[z] = st_->ap.synLTDStepSizeGRtoPC;
+	ctl.ltpStep[z] = st_->ap.synLTPStepSizeGRtoPC;
+	ctlDirty = true;
+}
+void Network::setErrDrive(uint32_t z, float rel) { ctl.errDrive[z] = rel * st_->ap.maxExtIncVIO; ctlDirty = true; }
+void Network::setGIncGRtoGO(float v) { ctl.gIncGRtoGO = v; ctlDirty = true; }
+void Network::resetGIncGRtoGO() { ctl.gIncGRtoGO = st_->ap.gIncGRtoGO; ctlDirty = true; }
+
+std::string Network::uploadMFBits(const uint32_t *bits, uint64_t firstSlot, uint64_t n, cudaStream_t s)
+{
+	if (firstSlot + n > h_.mfRing) return "MF ring too small";
+	CK(cudaMemcpyAsync((void *)(h_.mfBits + firstSlot * h_.mfWords), bits, n * h_.mfWords * 4,
+			cudaMemcpyHostToDevice, s), "uploading MF spikes");
+	return "";
+}
+
+size_t Network::fieldBytes(Field f) const
+{
+	const DevNet &h = h_;
+	switch (f) {
+	case F_AP_GR: return h.numGR;
+	case F_VM_GR: case F_GESUM_GR: case F_GISUM_GR: case F_APBUF_GR: case F_THRESH_GR: case F_GKCA_GR: return 4ull * h.numGR;
+	case F_HIST_GR: return 8ull * h.numGR;
+	case F_AP_GO: return h.numGO;
+	case F_VM_GO: case F_APBUF_GO: case F_SUM_GR_INPUT_GO: case F_SUM_GO_INPUT_GO: case F_GO_OUT_SCALE_GOGO: return 4ull * h.numGO;
+	case F_AP_SC: return h.numSC;
+	case F_VM_SC: case F_APBUF_SC: return 4ull * h.numSC;
+	case F_HIST_MF: return h.numMF;
+	case F_APBUF_MF: return 4ull * h.numMF;
+	case F_AP_BC: return h.numBC;
+	case F_VM_BC: case F_APBUF_BC: return 4ull * h.numBC;
+	case F_AP_PC: return h.numPC;
+	case F_VM_PC: case F_APBUF_PC: return 4ull * h.numPC;
+	case F_AP_IO: return h.numIO;
+	case F_VM_IO: case F_APBUF_IO: return 4ull * h.numIO;
+	case F_AP_NC: return h.numNC;
+	case F_VM_NC: case F_APBUF_NC: return 4ull * h.numNC;
+	case F_PFPC_WEIGHT: return 4ull * h.numGR;
+	case F_MFNC_WEIGHT: return 4ull * h.numNC * h.numpNCfromMFtoNC;
+	default: return 0;
+	}
+}
+
+std::string Network::exportField(Field f, uint32_t zone, void *dst, size_t bytes, cudaStream_t s)
+{
+	if (bytes != fieldBytes(f) || bytes == 0) return "export buffer size mismatch";
+	if (zone >= h_.numZones) return "zone out of range";
+	const DevNet &h = h_;
+	const DevZone &Q = h.zones[zone];
+	const void *src = nullptr;
+	switch (f) {
+	case F_AP_GR: {
+		uint8_t *tmp = nullptr;
+		CK(cudaMallocAsync((void **)&tmp, h.numGR, s), "export scratch");
+		extractSpikesKernel<<<(h.numGR + 255) / 256, 256, 0, s>>>(h.apBufGR, tmp, h.numGR);
+		CK(cudaMemcpyAsync(dst, tmp, h.numGR, cudaMemcpyDeviceToHost, s), "export");
+		CK(cudaFreeAsync(tmp, s), "export scratch");
+		CK(cudaStreamSynchronize(s), "export");
+		return "";
+	}
+	case F_VM_GR: src = h.vGR; break;
+	case F_GESUM_GR: src = h.gESum; break;
+	case F_GISUM_GR: src = h.gISum; break;
+	case F_APBUF_GR: src = h.apBufGR; break;
+	case F_HIST_GR: src = h.historyGR; break;
+	case F_THRESH_GR: src = h.threshGR; break;
+	case F_GKCA_GR: src = h.gKCaGR; break;
+	case F_AP_GO: src = h.apGO; break;
+	case F_VM_GO: src = h.vGO; break;
+	case F_APBUF_GO: src = h.apBufGO; break;
+	case F_SUM_GR_INPUT_GO: src = h.sumGRInputGO; break;
+	case F_SUM_GO_INPUT_GO: src = h.sumInputGOGABASynDepGO; break;
+	case F_GO_OUT_SCALE_GOGO: src = h.goGABAOutSynScaleGOGO; break;
+	case F_AP_SC: src = h.apSC; break;
+	case F_VM_SC: src = h.vSC; break;
+	case F_APBUF_SC: src = h.apBufSC; break;
+	case F_HIST_MF: src = h.histMF; break;
+	case F_APBUF_MF: src = h.apBufMF; break;
+	case F_AP_BC: src = Q.apBC; break;
+	case F_VM_BC: src = Q.vBC; break;
+	case F_APBUF_BC: src = Q.apBufBC; break;
+	case F_AP_PC: src = Q.apPC; break;
+	case F_VM_PC: src = Q.vPC; break;
+	case F_APBUF_PC: src = Q.apBufPC; break;
+	case F_AP_IO: src = Q.apIO; break;
+	case F_VM_IO: src = Q.vIO; break;
+	case F_APBUF_IO: src = Q.apBufIO; break;
+	case F_AP_NC: src = Q.apNC; break;
+	case F_VM_NC: src = Q.vNC; break;
+	case F_APBUF_NC: src = Q.apBufNC; break;
+	case F_PFPC_WEIGHT: src = Q.w; break;
+	case F_MFNC_WEIGHT: src = Q.mfSynWeightNC; break;
+	default: return "unknown field";
+	}
+	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "export");
+	CK(cudaStreamSynchronize(s), "export");
+	return "";
+}
+
+// sumInputsNew's halving tree over one PC row's partial sums
+static float hostRowTree(std::vector<float> v)
+{
+	for (size_t h = v.size() / 2; h >= 1; h /= 2)
+		for (size_t t = 0; t < h; t++) v[t] = v[t] + v[t + h];
+	return v[0];
+}
+
+std::string Network::writeToState(cudaStream_t s)
+{
+	CK(cudaStreamSynchronize(s), "sync before writeToState");
+	const DevNet &h = h_;
+	auto D = [&](const char *n, int z, const void *src) -> std::string {
+		NamedArray *x = st_->find(n, z);
+		CK(cudaMemcpy(x->bytes.data(), src, x->bytes.size(), cudaMemcpyDeviceToHost), n);
+		return "";
+	};
+	// InNet::writeToState (innet.cpp:608-667)
+	{
+		std::vector<uint32_t> ab(h.numGR);
+		CK(cudaMemcpy(ab.data(), h.apBufGR, 4ull * h.numGR, cudaMemcpyDeviceToHost), "apBufGR");
+		uint8_t *apGR = st_->find("apGR")->as<uint8_t>();
+		// outputGRGPU holds zeros until the first step (innet.cpp:477)
+		for (uint32_t i = 0; i < h.numGR; i++) apGR[i] = hostT_ ? (uint8_t)(ab[i] & 1u) : 0;
+		memcpy(st_->find("apBufGR")->bytes.data(), ab.data(), 4ull * h.numGR);
+	}
+	CKS(D("gMFSumGR", -1, h.gESum)); CKS(D("gGOSumGR", -1, h.gISum)); CKS(D("threshGR", -1, h.threshGR));
+	CKS(D("vGR", -1, h.vGR)); CKS(D("gKCaGR", -1, h.gKCaGR)); CKS(D("historyGR", -1, h.historyGR));
+	{
+		const uint32_t buf = (uint32_t)((hostT_ + 2) % 3);
+		CKS(D("inputSumPFSC", -1, h.scCount + (size_t)buf * h.numSC));
+	}
+	// state the reference keeps on the host, here on the device
+	CKS(D("histMF", -1, h.histMF)); CKS(D("apBufMF", -1, h.apBufMF));
+	CKS(D("apGO", -1, h.apGO)); CKS(D("apBufGO", -1, h.apBufGO)); CKS(D("vGO", -1, h.vGO));
+	CKS(D("vCoupleGO", -1, h.vCoupleGO)); CKS(D("threshCurGO", -1, h.threshCurGO));
+	CKS(D("inputMFGO", -1, h.inputMFGO)); CKS(D("inputGOGO", -1, h.inputGOGO));
+	CKS(D("inputGOGABASynDepGO", -1, h.inputGOGABASynDepGO)); CKS(D("goGABAOutSynScaleGOGO", -1, h.goGABAOutSynScaleGOGO));
+	CKS(D("gMFGO", -1, h.gMFGO)); CKS(D("gGRGO", -1, h.gGRGO)); CKS(D("gGOGO", -1, h.gGOGO));
+	CKS(D("gMGluRGO", -1, h.gMGluRGO)); CKS(D("gMGluRIncGO", -1, h.gMGluRIncGO)); CKS(D("mGluRGO", -1, h.mGluRGO));
+	CKS(D("gluGO", -1, h.gluGO));
+	CKS(D("apSC", -1, h.apSC)); CKS(D("apBufSC", -1, h.apBufSC)); CKS(D("gPFSC", -1, h.gPFSC));
+	CKS(D("threshSC", -1, h.threshSC)); CKS(D("vSC", -1, h.vSC));
+	for (uint32_t z = 0; z < h.numZones; z++) {
+		const DevZone &Q = h.zones[z];
+		int zi = (int)z;
+		// MZone::writeToState (mzone.cpp:139-147)
+		CKS(D("pfSynWeightPC", zi, Q.w));
+		{
+			const uint32_t buf = (uint32_t)((hostT_ + 2) % 3);
+			std::vector<float> part((size_t)h.numPC * h.bs);
+			CK(cudaMemcpy(part.data(), Q.pcPartial + (size_t)buf * h.numPC * h.bs, part.size() * 4, cudaMemcpyDeviceToHost), "pcPartial");
+			float *dst = st_->find("inputSumPFPC", zi)->as<float>();
+			for (uint32_t pc = 0; pc < h.numPC; pc++)
+				dst[pc] = hostRowTree(std::vector<float>(part.begin() + (size_t)pc * h.bs, part.begin() + (size_t)(pc + 1) * h.bs));
+		}
+		CKS(D("apBC", zi, Q.apBC)); CKS(D("apBufBC", zi, Q.apBufBC)); CKS(D("inputPCBC", zi, Q.inputPCBC));
+		CKS(D("gPFBC", zi, Q.gPFBC)); CKS(D("gPCBC", zi, Q.gPCBC)); CKS(D("threshBC", zi, Q.threshBC));
+		CKS(D("vBC", zi, Q.vBC));
+		CKS(D("apPC", zi, Q.apPC)); CKS(D("apBufPC", zi, Q.apBufPC)); CKS(D("inputBCPC", zi, Q.inputBCPC));
+		CKS(D("inputSCPC", zi, Q.inputSCPC)); CKS(D("gPFPC", zi, Q.gPFPC)); CKS(D("gBCPC", zi, Q.gBCPC));
+		CKS(D("gSCPC", zi, Q.gSCPC)); CKS(D("vPC", zi, Q.vPC)); CKS(D("threshPC", zi, Q.threshPC));
+		CKS(D("histPCPopAct", zi, Q.histPCPopAct));
+		CKS(D("apIO", zi, Q.apIO)); CKS(D("apBufIO", zi, Q.apBufIO)); CKS(D("inputNCIO", zi, Q.inputNCIO));
+		CKS(D("gNCIO", zi, Q.gNCIO)); CKS(D("threshIO", zi, Q.threshIO)); CKS(D("vIO", zi, Q.vIO));
+		CKS(D("vCoupleIO", zi, Q.vCoupleIO)); CKS(D("pfPCPlastTimerIO", zi, Q.pfPCPlastTimerIO));
+		CKS(D("apNC", zi, Q.apNC)); CKS(D("apBufNC", zi, Q.apBufNC)); CKS(D("inputPCNC", zi, Q.inputPCNC));
+		CKS(D("inputMFNC", zi, Q.inputMFNC)); CKS(D("gPCNC", zi, Q.gPCNC)); CKS(D("gPCScaleNC", zi, Q.gPCScaleNC));
+		CKS(D("mfSynWeightNC", zi, Q.mfSynWeightNC)); CKS(D("gmaxNMDAofMFtoNC", zi, Q.gmaxNMDAofMFtoNC));
+		CKS(D("gmaxAMPAofMFtoNC", zi, Q.gmaxAMPAofMFtoNC)); CKS(D("gMFNMDANC", zi, Q.gMFNMDANC));
+		CKS(D("gMFAMPANC", zi, Q.gMFAMPANC)); CKS(D("threshNC", zi, Q.threshNC)); CKS(D("vNC", zi, Q.vNC));
+		CKS(D("synIOPReleaseNC", zi, Q.synIOPReleaseNC));
+		uint32_t sc[5];
+		CK(cudaMemcpy(sc, Q.scal, sizeof(sc), cudaMemcpyDeviceToHost), "zone scalars");
+		ZoneScalars &zs = st_->zoneScalars[z];
+		zs.histPCPopActSum = sc[0]; zs.histPCPopActCurBinN = sc[1]; zs.pcPopAct = sc[2];
+		zs.noLTPMFNC = (uint8_t)sc[3]; zs.noLTDMFNC = (uint8_t)sc[4];
+		zs.errDrive = ctl.errDrive[z];
+	}
+	return "";
+}
+
+std::string Network::resetGOGODepression(cudaStream_t s)
+{
+	std::vector<float> ones(h_.numGO, 1.0f);
+	CK(cudaMemcpyAsync(h_.inputGOGABASynDepGO, ones.data(), 4ull * h_.numGO, cudaMemcpyHostToDevice, s), "reset");
+	CK(cudaMemsetAsync(h_.goGABAOutSynScaleGOGO, 0, 4ull * h_.numGO, s), "reset");
+	CK(cudaStreamSynchronize(s), "reset");
+	float *a = st_->find("inputGOGABASynDepGO")->as<float>();
+	float *b = st_->find("goGABAOutSynScaleGOGO")->as<float>();
+	for (uint32_t i = 0; i < h_.numGO; i++) { a[i] = 1.0f; b[i] = 0.0f; }
+	return "";
+}
+
+// --------------------------------------------------------------- Simulator
+Simulator::~Simulator()
+{
+	if (graphExec_) cudaGraphExecDestroy(graphExec_);
+	for (Network *n : nets_) delete n;
+	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_}) if (b->ptr) cudaFree(b->ptr);
+	if (s0_) cudaStreamDestroy(s0_);
+	if (s1_) cudaStreamDestroy(s1_);
+	for (cudaEvent_t e : {fork_, join_, ev0_, ev1_}) if (e) cudaEventDestroy(e);
+	for (cudaEvent_t e : passEv_) cudaEventDestroy(e);
+}
+
+std::string Simulator::create(const std::vector<State *> &states, const std::vector<std::vector<int>> &seeds,
+		int device, uint32_t mfRing, const std::vector<uint32_t> *mfSeeds)
+{
+	device_ = device;
+	CK(cudaSetDevice(device), "selecting the device");
+	CK(cudaStreamCreateWithFlags(&s0_, cudaStreamNonBlocking), "stream");
+	CK(cudaStreamCreateWithFlags(&s1_, cudaStreamNonBlocking), "stream");
+	CK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "event");
+	CK(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "event");
+	CK(cudaEventCreate(&ev0_), "event");
+	CK(cudaEventCreate(&ev1_), "event");
+	std::vector<DevNet *> ptrs;
+	std::vector<uint64_t *> tb;
+	std::vector<uint32_t> offs;
+	for (size_t i = 0; i < states.size(); i++) {
+		Network *n = new Network();
+		nets_.push_back(n);
+		std::vector<int> sd = i < seeds.size() ? seeds[i] : std::vector<int>();
+		CKS(n->build(states[i], sd, mfRing, mfSeeds && i < mfSeeds->size() ? (*mfSeeds)[i] : 0));
+		offs.push_back(passBlocks_);
+		passBlocks_ += n->passBlocks();
+		ptrs.push_back(n->devPtr());
+		tb.push_back(n->dev().tBase);
+		passSmem_ = std::max(passSmem_, n->passSmemBytes());
+		tailSmem_ = std::max(tailSmem_, n->tailSmemBytes());
+	}
+	auto up = [&](DeviceBuf &b, const void *src, size_t bytes) -> std::string {
+		CK(cudaMalloc(&b.ptr, bytes), "allocating launch tables");
+		b.bytes = bytes;
+		CK(cudaMemcpy(b.ptr, src, bytes, cudaMemcpyHostToDevice), "uploading launch tables");
+		return "";
+	};
+	CKS(up(dNetPtrs_, ptrs.data(), ptrs.size() * sizeof(DevNet *)));
+	CKS(up(dBlockOffset_, offs.data(), offs.size() * sizeof(uint32_t)));
+	CKS(up(dTBasePtrs_, tb.data(), tb.size() * sizeof(uint64_t *)));
+	if (passSmem_ > 48 * 1024)
+		CK(cudaFuncSetAttribute(grPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem_), "pass smem");
+	if (tailSmem_ > 48 * 1024)
+		CK(cudaFuncSetAttribute(tailKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tailSmem_), "tail smem");
+	return "";
+}
+
+std::string Simulator::uploadCtl()
+{
+	for (Network *n : nets_) {
+		if (!n->ctlDirty) continue;
+		CK(cudaMemcpyAsync(n->h_.ctl, &n->ctl, sizeof(HostCtl), cudaMemcpyHostToDevice, s0_), "uploading setters");
+		// the next step consumes the error drive on the device (mzone.cpp:334)
+		for (int z = 0; z < kMaxZones; z++) n->ctl.errDrive[z] = 0;
+		CK(cudaStreamSynchronize(s0_), "uploading setters");
+		n->ctlDirty = false;
+	}
+	return "";
+}
+
+std::string Simulator::enqueueStep(uint32_t k, bool instrument)
+{
+	CK(cudaEventRecord(fork_, s0_), "fork");
+	CK(cudaStreamWaitEvent(s1_, fork_, 0), "fork");
+	if (instrument) CK(cudaEventRecordWithFlags(passEv_[2 * k], s0_, cudaEventRecordExternal), "pass timing");
+	grPassKernel<<<passBlocks_, kPassThreads, passSmem_, s0_>>>((const DevNet *const *)dNetPtrs_.ptr,
+			(const uint32_t *)dBlockOffset_.ptr, (int)nets_.size(), k);
+	CK(cudaGetLastError(), "launching the GR pass");
+	if (instrument) CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
+	tailKernel<<<(unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>((const DevNet *const *)dNetPtrs_.ptr, k);
+	CK(cudaGetLastError(), "launching the small-cell update");
+	CK(cudaEventRecord(join_, s1_), "join");
+	CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
+	return "";
+}
+
+std::string Simulator::launchSteps(uint32_t nsteps)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(uploadCtl());
+	for (uint32_t k = 0; k < nsteps; k++) CKS(enqueueStep(k, false));
+	advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), nsteps);
+	CK(cudaGetLastError(), "advancing the step counter");
+	for (Network *n : nets_) n->hostT_ += nsteps;
+	return "";
+}
+
+std::string Simulator::stageMF(size_t i, const uint8_t *mf)
+{
+	Network &n = *nets_[i];
+	const uint32_t W = n.h_.mfWords, M = n.h_.numMF;
+	memset(n.hPinnedBits_, 0, 4ull * W);
+	bool raw = false;
+	for (uint32_t k = 0; k < M; k++) {
+		if (mf[k]) n.hPinnedBits_[k >> 5] |= 1u << (k & 31);
+		if (mf[k] > 1) raw = true;
+	}
+	const uint64_t slot = n.hostT_ % n.h_.mfRing;
+	CK(cudaMemcpyAsync((void *)(n.h_.mfBits + slot * W), n.hPinnedBits_, 4ull * W, cudaMemcpyHostToDevice, s0_), "MF upload");
+	if (raw || n.h_.hasMFRaw) {
+		memcpy(n.hPinnedRaw_, mf, M);
+		CK(cudaMemcpyAsync((void *)(n.h_.mfRaw + slot * M), n.hPinnedRaw_, M, cudaMemcpyHostToDevice, s0_), "MF upload");
+		if (!n.h_.hasMFRaw) {
+			// from now on NC inputs take the raw bytes (mzone.cpp:521)
+			n.h_.hasMFRaw = 1;
+			CK(cudaMemcpyAsync((char *)n.dNet_.ptr + offsetof(DevNet, hasMFRaw), &n.h_.hasMFRaw, 4,
+					cudaMemcpyHostToDevice, s0_), "MF mode");
+		}
+	}
+	CK(cudaStreamSynchronize(s0_), "MF upload");
+	return "";
+}
+
+std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(uploadCtl());
+	if (chunk == 0) chunk = 1;
+	if (!graphExec_ || graphChunk_ != chunk || graphInstrumented_ != instrument) {
+		if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
+		while (instrument && passEv_.size() < 2 * (size_t)chunk) {
+			cudaEvent_t e;
+			CK(cudaEventCreate(&e), "event");
+			passEv_.push_back(e);
+		}
+		cudaGraph_t g;
+		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
+		for (uint32_t k = 0; k < chunk; k++) {
+			std::string e = enqueueStep(k, instrument);
+			if (!e.empty()) { cudaStreamEndCapture(s0_, &g); return e; }
+		}
+		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), chunk);
+		CK(cudaStreamEndCapture(s0_, &g), "graph capture");
+		CK(cudaGraphInstantiate(&graphExec_, g, 0), "graph instantiate");
+		cudaGraphDestroy(g);
+		graphChunk_ = chunk;
+		graphInstrumented_ = instrument;
+	}
+	const uint64_t reps = nsteps / chunk, rem = nsteps % chunk;
+	CK(cudaEventRecord(ev0_, s0_), "timing");
+	for (uint64_t r = 0; r < reps; r++) CK(cudaGraphLaunch(graphExec_, s0_), "graph launch");
+	for (Network *n : nets_) n->hostT_ += reps * chunk;
+	if (rem) CKS(launchSteps((uint32_t)rem));
+	CK(cudaEventRecord(ev1_, s0_), "timing");
+	CK(cudaEventSynchronize(ev1_), "graph run");
+	CK(cudaEventElapsedTime(&lastGraphMs_, ev0_, ev1_), "timing");
+	lastPassMs_ = 0;
+	if (instrument && reps) {
+		// pass durations of the last chunk replayed
+		float total = 0;
+		for (uint32_t k = 0; k < chunk; k++) {
+			float ms = 0;
+			CK(cudaEventElapsedTime(&ms, passEv_[2 * k], passEv_[2 * k + 1]), "pass timing");
+			total += ms;
+		}
+		lastPassMs_ = total / chunk;
+	}
+	return "";
+}
+
+std::string Simulator::sync()
+{
+	CK(cudaStreamSynchronize(s0_), "sync");
+	CK(cudaStreamSynchronize(s1_), "sync");
+	CK(cudaGetLastError(), "sync");
+	return "";
+}
+
+}  // namespace cbm

@@ -1,0 +1,129 @@
+// Host object driving one or more device-resident networks: the B200
+// counterpart of the reference's CBMSimCore + InNet + MZone objects
+// (CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/cbmsimcore.h:32-75,
+// innetmodules/innet.h, mzonemodules/mzone.h).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "cbm_device.cuh"
+#include "cbm_state.hpp"
+
+namespace cbm {
+
+// Fields a caller can read back (the reference's export* calls and the
+// state arrays behind them).
+enum Field : int {
+	F_AP_GR = 0, F_VM_GR, F_GESUM_GR, F_GISUM_GR, F_APBUF_GR, F_HIST_GR, F_THRESH_GR, F_GKCA_GR,
+	F_AP_GO, F_VM_GO, F_APBUF_GO, F_SUM_GR_INPUT_GO, F_SUM_GO_INPUT_GO, F_GO_OUT_SCALE_GOGO,
+	F_AP_SC, F_VM_SC, F_APBUF_SC, F_HIST_MF, F_APBUF_MF,
+	F_AP_BC, F_VM_BC, F_APBUF_BC, F_AP_PC, F_VM_PC, F_APBUF_PC, F_AP_IO, F_VM_IO, F_APBUF_IO,
+	F_AP_NC, F_VM_NC, F_APBUF_NC, F_PFPC_WEIGHT, F_MFNC_WEIGHT,
+	F_COUNT
+};
+
+struct DeviceBuf {
+	void *ptr = nullptr;
+	size_t bytes = 0;
+};
+
+class Network;
+
+// A set of networks that advance together: one network for the drop-in
+// CBMSimCore path, many for the batched sweep.
+class Simulator {
+public:
+	~Simulator();
+	std::string create(const std::vector<State *> &states, const std::vector<std::vector<int>> &seeds,
+			int device, uint32_t mfRing, const std::vector<uint32_t> *mfSeeds = nullptr);
+	size_t numNets() const { return nets_.size(); }
+	Network &net(size_t i) { return *nets_[i]; }
+
+	// One step of every network with MF input already in each network's ring.
+	std::string launchSteps(uint32_t nsteps);
+	// Host MF input for the next step of network i (updateMFInput).
+	std::string stageMF(size_t i, const uint8_t *mf);
+	// Run nsteps as CUDA-graph chunks of chunk steps (inputs resident in HBM).
+	// With instrument, external events around every GR pass of the chunk
+	// give lastPassMs(): the pass's mean duration over the last replay.
+	std::string runGraph(uint64_t nsteps, uint32_t chunk, bool instrument = false);
+	std::string sync();
+	cudaStream_t stream() const { return s0_; }
+	int device() const { return device_; }
+	// Time of the last runGraph call measured with events on the launch stream.
+	float lastGraphMs() const { return lastGraphMs_; }
+	float lastPassMs() const { return lastPassMs_; }
+
+private:
+	friend class Network;
+	std::string uploadCtl();
+	std::string enqueueStep(uint32_t stepOffset, bool instrument);
+	std::vector<Network *> nets_;
+	int device_ = 0;
+	cudaStream_t s0_ = nullptr, s1_ = nullptr;
+	cudaEvent_t fork_ = nullptr, join_ = nullptr, ev0_ = nullptr, ev1_ = nullptr;
+	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_;
+	uint32_t passBlocks_ = 0;
+	size_t passSmem_ = 0, tailSmem_ = 0;
+	cudaGraphExec_t graphExec_ = nullptr;
+	uint32_t graphChunk_ = 0;
+	bool graphInstrumented_ = false;
+	std::vector<cudaEvent_t> passEv_;
+	float lastGraphMs_ = 0, lastPassMs_ = 0;
+};
+
+class Network {
+public:
+	~Network();
+	std::string build(State *st, const std::vector<int> &seeds, uint32_t mfRing, uint32_t mfSeed);
+	// host setters of the reference's API
+	void setPlastSteps(uint32_t zone, float ltd, float ltp);
+	void resetPlastSteps(uint32_t zone);
+	void setErrDrive(uint32_t zone, float rel);
+	void setGIncGRtoGO(float v);
+	void resetGIncGRtoGO();
+	// Copy one field to host memory (bytes must equal fieldBytes).
+	std::string exportField(Field f, uint32_t zone, void *dst, size_t bytes, cudaStream_t s);
+	size_t fieldBytes(Field f) const;
+	// CBMSimCore::writeToState(): device values back into the state.
+	std::string writeToState(cudaStream_t s);
+	// The reference's writeState resets the GO->GO depression arrays of the
+	// live state (innetactivitystate.cpp:247-248); mirrored on the device.
+	std::string resetGOGODepression(cudaStream_t s);
+	// MF spikes for steps [t0, t0+n) as bit rows, into the ring.
+	std::string uploadMFBits(const uint32_t *bits, uint64_t firstSlot, uint64_t n, cudaStream_t s);
+	uint64_t stepsDone() const { return hostT_; }
+	const DevNet &dev() const { return h_; }
+	DevNet *devPtr() const { return (DevNet *)dNet_.ptr; }
+	State *state() { return st_; }
+	uint32_t passBlocks() const { return h_.numPC * h_.tilesPerPC; }
+	size_t passSmemBytes() const;
+	size_t tailSmemBytes() const;
+	uint32_t mfWords() const { return h_.mfWords; }
+	uint32_t mfRing() const { return h_.mfRing; }
+	double bytesPerStepAlgorithmic() const;  // 72 + 4 n_mf + 4 n_go + 8 n_out per GR
+
+	HostCtl ctl{};
+	bool ctlDirty = true;
+	uint64_t hostT_ = 0;
+	std::vector<uint32_t> stagedBits;
+	std::vector<uint8_t> stagedRaw;
+
+private:
+	friend class Simulator;
+	template <typename T> T *alloc(size_t n);
+	template <typename T> T *upload(const T *src, size_t n);
+	State *st_ = nullptr;
+	DevNet h_{};
+	DeviceBuf dNet_;
+	std::vector<void *> allocs_;
+	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;
+	uint32_t *hPinnedBits_ = nullptr;
+	uint8_t *hPinnedRaw_ = nullptr;
+};
+
+std::string cudaErr(cudaError_t e, const char *what);
+
+}  // namespace cbm

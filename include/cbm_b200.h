@@ -1,0 +1,198 @@
+/* C ABI of the B200 cerebellar network step.
+ *
+ * This is the boundary a host program binds to in place of the reference's
+ * CBM_CORE_LIB (CBMSimCore / InNetInterface / MZoneInterface) and
+ * CBM_STATE_LIB (CBMState).  Every call returns a status code (CBM_OK on
+ * success); cbm_last_error() describes the last failure of the calling
+ * thread.  Objects are not thread-safe: one thread per simulator, like the
+ * reference (its GUI serialises access through a mutex,
+ * Eyelid_Sim_CBM_Dev/src/gui/simthread.cpp:196).
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   CBMState         CBM_STATE_LIB_DEV/CBMStateInclude/interfaces/cbmstate.h:37-62
+ *   CBMSimCore       CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/cbmsimcore.h:35-49
+ *   InNetInterface   CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/innetinterface.h:18-41
+ *   MZoneInterface   CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/mzoneinterface.h:18-34
+ */
+#ifndef CBM_B200_H
+#define CBM_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CBM_OK 0
+#define CBM_ERR_ARG 1          /* bad argument (null pointer, zone or size out of range) */
+#define CBM_ERR_CUDA 2         /* CUDA runtime error */
+#define CBM_ERR_IO 3           /* file could not be read or written */
+#define CBM_ERR_FORMAT 4       /* malformed or truncated state file / parameter text */
+#define CBM_ERR_RANGE 5        /* connectivity index or count out of range */
+#define CBM_ERR_UNSUPPORTED 6  /* network shape outside what the kernels implement */
+
+/* array element types reported by cbm_state_array */
+#define CBM_U8 0
+#define CBM_I32 1
+#define CBM_U32 2
+#define CBM_F32 3
+#define CBM_U64 4
+
+/* fields readable with cbm_sim_export; the *_GR, *_GO, *_SC and *_MF fields
+ * are the input net's, the rest are per microzone */
+enum cbm_field {
+	CBM_AP_GR = 0,            /* u8[numGR]   InNetInterface::exportAPGR   (innet.cpp:687) */
+	CBM_VM_GR,                /* f32[numGR]  exportVmGR                   (innet.cpp:715) */
+	CBM_GESUM_GR,             /* f32[numGR]  exportGESumGR                (innet.cpp:730) */
+	CBM_GISUM_GR,             /* f32[numGR]  exportGISumGR                (innet.cpp:735) */
+	CBM_APBUF_GR,             /* u32[numGR]  exportAPBufGR                (innet.cpp:768) */
+	CBM_HIST_GR,              /* u64[numGR]  GR spike history (innetactivitystate.h:79) */
+	CBM_THRESH_GR,            /* f32[numGR] */
+	CBM_GKCA_GR,              /* f32[numGR] */
+	CBM_AP_GO,                /* u8[numGO]   exportAPGO                   (innet.cpp:683) */
+	CBM_VM_GO,                /* f32[numGO]  exportVmGO                   (innet.cpp:721) */
+	CBM_APBUF_GO,             /* u32[numGO]  exportAPBufGO                (innet.cpp:764) */
+	CBM_SUM_GR_INPUT_GO,      /* u32[numGO]  exportSumGRInputGO           (innet.cpp:741) */
+	CBM_SUM_GO_INPUT_GO,      /* f32[numGO]  exportSumGOInputGO           (innet.cpp:746) */
+	CBM_GO_OUT_SCALE_GOGO,    /* f32[numGO]  exportGOOutSynScaleGOGO      (innet.cpp:751) */
+	CBM_AP_SC,                /* u8[numSC]   exportAPSC                   (innet.cpp:679) */
+	CBM_VM_SC,                /* f32[numSC]  exportVmSC                   (innet.cpp:725) */
+	CBM_APBUF_SC,             /* u32[numSC]  exportAPBufSC                (innet.cpp:773) */
+	CBM_HIST_MF,              /* u8[numMF]   exportHistMF                 (innet.cpp:756) */
+	CBM_APBUF_MF,             /* u32[numMF]  exportAPBufMF                (innet.cpp:760) */
+	CBM_AP_BC,                /* u8[numBC]   MZoneInterface::exportAPBC   (mzone.cpp:743) */
+	CBM_VM_BC,                /* f32[numBC]  exportVmBC                   (mzone.cpp:756) */
+	CBM_APBUF_BC,             /* u32[numBC]  exportAPBufBC                (mzone.cpp:773) */
+	CBM_AP_PC,                /* u8[numPC]   exportAPPC                   (mzone.cpp:747) */
+	CBM_VM_PC,                /* f32[numPC]  exportVmPC                   (mzone.cpp:760) */
+	CBM_APBUF_PC,             /* u32[numPC]  exportAPBufPC                (mzone.cpp:777) */
+	CBM_AP_IO,                /* u8[numIO]   exportAPIO                   (mzone.cpp:751) */
+	CBM_VM_IO,                /* f32[numIO]  exportVmIO                   (mzone.cpp:768) */
+	CBM_APBUF_IO,             /* u32[numIO]  exportAPBufIO                (mzone.cpp:781) */
+	CBM_AP_NC,                /* u8[numNC]   exportAPNC                   (mzone.cpp:739) */
+	CBM_VM_NC,                /* f32[numNC]  exportVmNC                   (mzone.cpp:764) */
+	CBM_APBUF_NC,             /* u32[numNC]  exportAPBufNC                (mzone.cpp:785) */
+	CBM_PFPC_WEIGHT,          /* f32[numGR]  PF->PC weights, PC-major (mzone.cpp:97-103) */
+	CBM_MFNC_WEIGHT,          /* f32[numNC*numMF/numNC] MF->NC weights (mzoneactivitystate.h:93) */
+	CBM_FIELD_COUNT
+};
+
+typedef struct cbm_state cbm_state;
+typedef struct cbm_sim cbm_sim;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *cbm_last_error(void);
+
+/* ------------------------------------------------------------- CBMState */
+/* CBMState(fstream&): read a state file in the reference's format
+ * (cbmstate.cpp:12-33).  Fields the reference's loader leaves undefined are
+ * defined here: pPCfromPCtoBC is rebuilt with connectPCtoBC's formula
+ * (mzoneconnectivitystate.cpp:242-257, the file holds pBCfromPCtoBC twice,
+ * :150) and the unsaved microzone scalars start from the stored histogram
+ * (histPCPopActSum) and zero. */
+int cbm_state_load(const char *path, cbm_state **out);
+
+/* A new network from the texts of a connectivity-parameter file and an
+ * activity-parameter file (the two fstreams of CBMState(actPF, conPF,
+ * nZones, ...), cbmstate.cpp:60-64 / 176-204).  Activity state takes the
+ * reference's initial values and the microzone wiring its formulas
+ * (mzoneconnectivitystate.cpp:213-417); wiringSeeds (one per zone, may be
+ * NULL) seed the random part of the PC->NC wiring.  Input-net connectivity is
+ * left "unconnected" for the caller to fill through cbm_state_array. */
+int cbm_state_new(const char *conParamsText, const char *actParamsText, unsigned nZones,
+		const int *wiringSeeds, cbm_state **out);
+
+/* CBMState::writeState (cbmstate.cpp:86-103), byte-compatible with the
+ * reference.  Like the reference it resets the two GO->GO depression arrays
+ * of the state it writes (innetactivitystate.cpp:247-248). */
+int cbm_state_save(cbm_state *s, const char *path);
+void cbm_state_free(cbm_state *s);
+int cbm_state_num_zones(const cbm_state *s, unsigned *out);
+
+/* Named array of the state (the reference's member names, e.g. "vGR",
+ * "pGRfromMFtoGR", "pfSynWeightPC"); zone -1 for input-net arrays.  The
+ * pointer stays valid until the state is freed. */
+int cbm_state_array(cbm_state *s, const char *name, int zone, void **data, uint64_t *count, int *dtype);
+
+/* Connectivity / activity parameter by the reference's member name
+ * (e.g. "numGR", "numpPCfromGRtoPC", "gDecMFtoGR", "tsPerHistBinGR"). */
+int cbm_state_con_param(const cbm_state *s, const char *name, uint32_t *value);
+int cbm_state_act_param(const cbm_state *s, const char *name, double *value);
+/* ActivityParams::setParam (activityparams.cpp:423-434): raw key, re-derive. */
+int cbm_state_set_act_param(cbm_state *s, const char *rawKey, float value);
+
+/* ----------------------------------------------------------- CBMSimCore */
+/* CBMSimCore(CBMState*, int *mzoneRSeed, gpuIndStart, numGPUP2)
+ * (cbmsimcore.cpp:14-17, 337-392).  The whole network lives on `device`.
+ * mzoneSeeds (one per zone, may be NULL) key each microzone's NC->IO release
+ * draws.  The state is borrowed and must outlive the simulator, as in the
+ * reference (ecmanagementbase.cpp destroys the core first). */
+int cbm_sim_create(cbm_state *s, const int *mzoneSeeds, int device, cbm_sim **out);
+
+/* As cbm_sim_create with room for mfSteps steps of resident MF input
+ * (cbm_sim_load_mf_stream / cbm_sim_run). */
+int cbm_sim_create_resident(cbm_state *s, const int *mzoneSeeds, int device, uint64_t mfSteps, cbm_sim **out);
+
+/* CBMSimCore::updateMFInput (cbmsimcore.cpp:312-320): numMF bytes, nonzero
+ * = spike; the raw byte value feeds the NC inputs as in mzone.cpp:521.
+ * Takes effect for the next cbm_sim_calc_activity. */
+int cbm_sim_update_mf(cbm_sim *sim, const uint8_t *mf);
+
+/* CBMSimCore::calcActivity (cbmsimcore.cpp:139-310): one 1 ms step. */
+int cbm_sim_calc_activity(cbm_sim *sim);
+
+/* CBMSimCore::updateErrDrive (cbmsimcore.cpp:322-325). */
+int cbm_sim_update_err_drive(cbm_sim *sim, unsigned zone, float errDriveRelative);
+
+/* MZoneInterface::setGRPCPlastSteps / resetGRPCPlastSteps (mzone.cpp:726-736) */
+int cbm_sim_set_plast_steps(cbm_sim *sim, unsigned zone, float ltdStep, float ltpStep);
+int cbm_sim_reset_plast_steps(cbm_sim *sim, unsigned zone);
+
+/* InNetInterface::setGIncGRtoGO / resetGIncGRtoGO (innet.cpp:669-677) */
+int cbm_sim_set_ginc_grgo(cbm_sim *sim, float inc);
+int cbm_sim_reset_ginc_grgo(cbm_sim *sim);
+
+/* Copy one field (enum cbm_field) into dst; bytes must equal
+ * cbm_sim_field_bytes(sim, field).  zone selects the microzone for
+ * per-zone fields and is ignored otherwise (pass 0). */
+int cbm_sim_export(cbm_sim *sim, int field, unsigned zone, void *dst, uint64_t bytes);
+uint64_t cbm_sim_field_bytes(cbm_sim *sim, int field);
+
+/* CBMSimCore::writeToState() (cbmsimcore.cpp:65-73): device state back
+ * into the borrowed CBMState. */
+int cbm_sim_write_to_state(cbm_sim *sim);
+
+/* CBMSimCore::writeToState(fstream&) (cbmsimcore.cpp:75-80): write back and
+ * save; like the reference, the save also resets the live GO->GO depression
+ * arrays. */
+int cbm_sim_save(cbm_sim *sim, const char *path);
+
+int cbm_sim_steps_done(cbm_sim *sim, uint64_t *steps);
+/* Words per MF bit row: bit k of word k/32 is MF k (numMF/32 + 1 words). */
+int cbm_sim_mf_words(cbm_sim *sim, uint32_t *words);
+
+/* Resident input path: nsteps bit rows, step s's row at bits + s*words,
+ * copied into HBM as the input of the next nsteps steps. */
+int cbm_sim_load_mf_stream(cbm_sim *sim, const uint32_t *bits, uint64_t nsteps);
+
+/* Run nsteps steps from the resident input as CUDA-graph chunks of
+ * graphChunk steps.  On return *gpuMs (if not NULL) holds the device time of
+ * the run and *passMs (if not NULL) the mean duration of the GR pass kernel
+ * over the last chunk. */
+int cbm_sim_run(cbm_sim *sim, uint64_t nsteps, uint32_t graphChunk, float *gpuMs, float *passMs);
+
+/* Algorithmic HBM bytes of one step: (72 + 4 n_mf + 4 n_go + 8 n_out) per GR
+ * with the network's mean synapse counts. */
+double cbm_sim_algorithmic_bytes_per_step(cbm_sim *sim);
+
+void cbm_sim_destroy(cbm_sim *sim);
+
+/* Device evaluation of the float exponential the small-cell updates use
+ * (the published expf algorithm glibc ships), for checking it against the
+ * host's expf: out[i] = exp(in[i]) for n values in host memory. */
+int cbm_device_expf(int device, const float *in, float *out, uint64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1126,6 +1126,12 @@ void cbm_oracle_run(cbm_oracle *o, const uint8_t *mf, uint64_t nsteps, uint8_t *
 	}
 }
 
+void cbm_oracle_expf_array(const float *in, float *out, uint64_t n)
+{
+	/* the host C library's expf, which the reference's exp(float) calls use */
+	for (uint64_t i = 0; i < n; i++) out[i] = expf(in[i]);
+}
+
 uint32_t cbm_oracle_num(const cbm_oracle *o, const char *w)
 {
 	if (!strcmp(w, "GR")) return o->numGR;

@@ -48,6 +48,9 @@ size_t cbm_oracle_trace_record_bytes(const cbm_oracle *o);
 /* writeToState(fstream&) of the reference: returns 0 on success. */
 int cbm_oracle_save(cbm_oracle *o, const char *path);
 
+/* out[i] = the host C library's expf(in[i]) (the reference's exp(float)). */
+void cbm_oracle_expf_array(const float *in, float *out, uint64_t n);
+
 /* Sizes, for callers sizing buffers. */
 uint32_t cbm_oracle_num(const cbm_oracle *o, const char *what);
 

@@ -1,0 +1,248 @@
+"""Test helpers: the CPU oracle (oracle/libcbm_oracle.so), the reference
+harness (oracle/_ref/ref_run) and trace records of the B200 simulator in the
+oracle's record layout."""
+import ctypes
+import hashlib
+import json
+import lzma
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "libcbm_oracle.so")
+REF_RUN = os.path.join(ORACLE_DIR, "_ref", "ref_run")
+REF_GEN = os.path.join(ORACLE_DIR, "_ref", "ref_gen")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def ensure_oracle():
+    if not os.path.exists(ORACLE_LIB):
+        subprocess.run(["make", "-C", ORACLE_DIR, "oracle"], check=True, capture_output=True)
+    return ORACLE_LIB
+
+
+class Oracle:
+    """ctypes view of the C oracle (oracle/cbm_oracle.h)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = ctypes.CDLL(ensure_oracle())
+            P, S, I, U, F = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint, ctypes.c_float
+            lib.cbm_oracle_load.restype = P
+            lib.cbm_oracle_load.argtypes = [S, S, ctypes.c_size_t]
+            lib.cbm_oracle_free.argtypes = [P]
+            lib.cbm_oracle_set_seeds.argtypes = [P, P]
+            lib.cbm_oracle_update_err_drive.argtypes = [P, U, F]
+            lib.cbm_oracle_set_plast_steps.argtypes = [P, U, F, F]
+            lib.cbm_oracle_reset_plast_steps.argtypes = [P, U]
+            lib.cbm_oracle_set_ginc_grgo.argtypes = [P, F]
+            lib.cbm_oracle_reset_ginc_grgo.argtypes = [P]
+            lib.cbm_oracle_run.argtypes = [P, P, ctypes.c_uint64, P]
+            lib.cbm_oracle_trace_record_bytes.restype = ctypes.c_size_t
+            lib.cbm_oracle_trace_record_bytes.argtypes = [P]
+            lib.cbm_oracle_save.restype = I
+            lib.cbm_oracle_save.argtypes = [P, S]
+            lib.cbm_oracle_num.restype = ctypes.c_uint32
+            lib.cbm_oracle_num.argtypes = [P, S]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, state_path, seeds=None):
+        lib = self.lib()
+        err = ctypes.create_string_buffer(256)
+        self.h = lib.cbm_oracle_load(os.fsencode(state_path), err, 256)
+        if not self.h:
+            raise RuntimeError(err.value.decode())
+        if seeds is not None:
+            s = np.asarray(seeds, dtype=np.int32)
+            lib.cbm_oracle_set_seeds(self.h, s.ctypes.data)
+        self.rb = lib.cbm_oracle_trace_record_bytes(self.h)
+        self.num = {k: lib.cbm_oracle_num(self.h, k.encode()) for k in ("GR", "GO", "MF", "SC", "BC", "PC", "NC", "IO", "zones")}
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib().cbm_oracle_free(self.h)
+            self.h = None
+
+    def apply(self, ev):
+        lib = self.lib()
+        k = ev[0]
+        if k == "errdrive":
+            lib.cbm_oracle_update_err_drive(self.h, ev[1], ev[2])
+        elif k == "plast":
+            lib.cbm_oracle_set_plast_steps(self.h, ev[1], ev[2], ev[3])
+        elif k == "plastreset":
+            lib.cbm_oracle_reset_plast_steps(self.h, ev[1])
+        elif k == "grgoinc":
+            lib.cbm_oracle_set_ginc_grgo(self.h, ev[1])
+        elif k == "grgoincreset":
+            lib.cbm_oracle_reset_ginc_grgo(self.h)
+
+    def run(self, mf, events=None, t0=0):
+        """Steps t0+1 .. t0+len(mf); events maps 1-based step -> list of events."""
+        mf = np.ascontiguousarray(mf, dtype=np.uint8)
+        steps = mf.shape[0]
+        tr = np.zeros((steps, self.rb), dtype=np.uint8)
+        lib = self.lib()
+        for s in range(steps):
+            for ev in (events or {}).get(t0 + s + 1, []):
+                self.apply(ev)
+            row = np.ascontiguousarray(mf[s])
+            lib.cbm_oracle_run(self.h, row.ctypes.data, 1, tr[s].ctypes.data)
+        return tr
+
+    def save(self, path):
+        if self.lib().cbm_oracle_save(self.h, os.fsencode(path)) != 0:
+            raise RuntimeError("oracle save failed")
+
+
+def events_file(events, path):
+    with open(path, "w") as f:
+        for t in sorted(events):
+            for ev in events[t]:
+                f.write(f"{t} {ev[0]} " + " ".join(str(x) for x in ev[1:]) + "\n")
+
+
+def ref_available():
+    return os.path.exists(REF_RUN)
+
+
+def ref_run(state_path, mf, seeds, events=None, num_gpus=1, final_path=None):
+    """The reference's own host code (oracle/_ref/ref_run) on the same input."""
+    mf = np.ascontiguousarray(mf, dtype=np.uint8)
+    with tempfile.TemporaryDirectory() as d:
+        mfp = os.path.join(d, "mf.u8")
+        mf.tofile(mfp)
+        trp = os.path.join(d, "trace.bin")
+        cmd = [REF_RUN, state_path, mfp, str(mf.shape[0]), trp, final_path or "-"] + [str(s) for s in seeds]
+        if events:
+            evp = os.path.join(d, "ev.txt")
+            events_file(events, evp)
+            cmd += ["-e", evp]
+        env = dict(os.environ)
+        if num_gpus > 1:
+            env["CBM_FAKE_NUM_GPUS"] = str(num_gpus)
+            cmd += ["-g", str(int(np.log2(num_gpus)))]
+        subprocess.run(cmd, check=True, capture_output=True, env=env)
+        return np.fromfile(trp, dtype=np.uint8)
+
+
+def product_record(sim, num):
+    """One trace record of a CBMSimCore in the oracle's layout."""
+    inet = sim.getInputNet()
+    parts = [np.packbits(inet.exportAPGR().astype(bool), bitorder="little"), inet.exportAPGO(),
+             inet.exportVmGO().view(np.uint8), inet.exportSumGRInputGO().view(np.uint8),
+             inet.exportAPSC(), inet.exportVmSC().view(np.uint8)]
+    for z in sim.getMZoneList():
+        parts += [z.exportAPBC(), z.exportVmBC().view(np.uint8), z.exportAPPC(), z.exportVmPC().view(np.uint8),
+                  z.exportAPIO(), z.exportVmIO().view(np.uint8), z.exportAPNC(), z.exportVmNC().view(np.uint8)]
+    return np.concatenate([np.asarray(p, dtype=np.uint8).ravel() for p in parts])
+
+
+def product_run(sim, mf, events=None, t0=0, record=True):
+    recs = []
+    zones = sim.getMZoneList()
+    inet = sim.getInputNet()
+    for s in range(mf.shape[0]):
+        for ev in (events or {}).get(t0 + s + 1, []):
+            k = ev[0]
+            if k == "errdrive":
+                sim.updateErrDrive(ev[1], ev[2])
+            elif k == "plast":
+                zones[ev[1]].setGRPCPlastSteps(ev[2], ev[3])
+            elif k == "plastreset":
+                zones[ev[1]].resetGRPCPlastSteps()
+            elif k == "grgoinc":
+                inet.setGIncGRtoGO(ev[1])
+            elif k == "grgoincreset":
+                inet.resetGIncGRtoGO()
+        sim.updateMFInput(mf[s])
+        sim.calcActivity()
+        if record:
+            recs.append(product_record(sim, None))
+    return np.stack(recs) if record else None
+
+
+def record_layout(num):
+    """(name, dtype, count) of the fields of one trace record."""
+    lay = [("apGR", np.uint8, (num["GR"] + 7) // 8), ("apGO", np.uint8, num["GO"]), ("vGO", np.float32, num["GO"]),
+           ("sumGRInputGO", np.uint32, num["GO"]), ("apSC", np.uint8, num["SC"]), ("vSC", np.float32, num["SC"])]
+    for z in range(num["zones"]):
+        lay += [(f"apBC{z}", np.uint8, num["BC"]), (f"vBC{z}", np.float32, num["BC"]),
+                (f"apPC{z}", np.uint8, num["PC"]), (f"vPC{z}", np.float32, num["PC"]),
+                (f"apIO{z}", np.uint8, num["IO"]), (f"vIO{z}", np.float32, num["IO"]),
+                (f"apNC{z}", np.uint8, num["NC"]), (f"vNC{z}", np.float32, num["NC"])]
+    return lay
+
+
+def same_values(x, y):
+    """Bitwise equality, except that any two NaNs are equal: the host CPU and
+    the GPU encode the NaN of an invalid operation with different sign and
+    payload bits, which carry no meaning."""
+    x, y = np.asarray(x), np.asarray(y)
+    if x.dtype.kind == "f":
+        return (x.view(np.uint8).reshape(x.size, -1) == y.view(np.uint8).reshape(y.size, -1)).all(axis=1) | \
+            (np.isnan(x) & np.isnan(y))
+    return x == y
+
+
+def first_difference(a, b, num):
+    """Human-readable location of the first differing value of two traces."""
+    rb = a.shape[-1]
+    a = a.reshape(-1, rb)
+    b = b.reshape(a.shape)
+    cand = np.nonzero((a != b).any(axis=1))[0]
+    for step in cand:
+        off = 0
+        for name, dt, cnt in record_layout(num):
+            nb = np.dtype(dt).itemsize * cnt
+            x = a[step, off:off + nb].view(dt)
+            y = b[step, off:off + nb].view(dt)
+            if not same_values(x, y).all():
+                return f"step {int(step) + 1}: field {name}"
+            off += nb
+    return None
+
+
+def counter_mf(num_mf, steps, seed, rate_lo=0.001, rate_hi=0.06):
+    """Deterministic MF spikes from the counter-based stream: fibre i fires at
+    step s with a fixed per-fibre probability in [rate_lo, rate_hi)."""
+    from cerebellum_simulation_b200.networks import uniform24
+    rates = rate_lo + (rate_hi - rate_lo) * uniform24(seed, 0x52415445, np.arange(num_mf, dtype=np.uint64))
+    out = np.empty((steps, num_mf), dtype=np.uint8)
+    for s in range(steps):
+        u = uniform24(seed, 0x4D46494E, (np.uint64(s + 1) << np.uint64(20)) | np.arange(num_mf, dtype=np.uint64))
+        out[s] = u < rates
+    return out
+
+
+def sha(b):
+    return hashlib.sha256(np.ascontiguousarray(b).tobytes()).hexdigest()
+
+
+def golden_state(name, dest_dir):
+    """Decompress tests/golden/<name>.state.xz into dest_dir; returns the path."""
+    out = os.path.join(dest_dir, name + ".state")
+    with lzma.open(os.path.join(GOLDEN, name + ".state.xz")) as f, open(out, "wb") as g:
+        g.write(f.read())
+    return out
+
+
+def load_json(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+# The GO glutamate/mGluR state uses the double-precision exp of the host C
+# library in the reference and CUDA's double exp on the device; the two can
+# differ in the last double bit, which reaches these float arrays as at most a
+# few float ulps.  No spike depends on them (innet.cpp:850-858).
+FP_TOLERANT_ARRAYS = {"gluGO", "mGluRGO", "gMGluRIncGO", "gMGluRGO"}
+FP_RTOL = 1e-5

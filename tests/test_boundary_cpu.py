@@ -1,0 +1,94 @@
+"""CPU checks of the boundary: the C-ABI library loads and exports every
+function include/cbm_b200.h declares, state files round-trip byte for byte
+through the reference format, and malformed input fails with an error code."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import cbmtest
+
+ROOT = cbmtest.ROOT
+
+
+def declared_functions():
+    with open(os.path.join(ROOT, "include", "cbm_b200.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cbm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import cerebellum_simulation_b200 as cbm
+    names = declared_functions()
+    assert len(names) >= 30
+    lib = ctypes.CDLL(cbm.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_state_roundtrip_reference_file(tmp_path):
+    import cerebellum_simulation_b200 as cbm
+    p = cbmtest.golden_state("ref16k", str(tmp_path))
+    s = cbm.CBMState(p)
+    assert s.getNumZones() == 1
+    assert s.con("numGR") == 16384 and s.con("numGO") == 1024 and s.con("numpPCfromGRtoPC") == 512
+    out = str(tmp_path / "rt.state")
+    s.writeState(out)
+    assert open(p, "rb").read() == open(out, "rb").read()
+
+
+def test_loader_rebuilds_pc_to_bc_wiring(tmp_path):
+    """The reference's file holds pBCfromPCtoBC where pPCfromPCtoBC belongs;
+    the loader rebuilds pPCfromPCtoBC with connectPCtoBC's formula."""
+    import cerebellum_simulation_b200 as cbm
+    s = cbm.CBMState(cbmtest.golden_state("ref16k", str(tmp_path)))
+    npc, nbc = s.con("numPC"), s.con("numBC")
+    got = s.array("pPCfromPCtoBC", 0).reshape(npc, 16)
+    want = np.array([[((i * (nbc // npc) - 6 + j) % nbc + nbc) % nbc for j in range(16)] for i in range(npc)])
+    assert np.array_equal(got, want)
+
+
+def test_derived_parameters():
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    s = networks.config1_network(seed=0)
+    assert s.con("numGR") == 16384 and s.con("numGO") == 256 and s.con("numBC") == 128 and s.con("numSC") == 512
+    # gLeak = raw/(6-dt), decays exp(-dt/tau) in float (activityparams.cpp:499-519)
+    raw = s.act("rawGLeakGR")
+    assert s.act("gLeakGR") == pytest.approx(raw / 5.0, rel=1e-7)
+    assert s.act("gDecMFtoGR") == float(np.float32(np.exp(np.float32(-1) / np.float32(s.act("gMFDecayTGR")))))
+    assert s.act("tsPerHistBinGR") == 5
+
+
+@pytest.mark.parametrize("damage", ["truncate", "header"])
+def test_malformed_state_file_is_rejected(tmp_path, damage):
+    import cerebellum_simulation_b200 as cbm
+    p = cbmtest.golden_state("ref16k", str(tmp_path))
+    data = open(p, "rb").read()
+    bad = str(tmp_path / "bad.state")
+    with open(bad, "wb") as f:
+        f.write(data[: len(data) // 2] if damage == "truncate" else b"1\nfoo 3\n")
+    with pytest.raises(cbm.CBMError) as e:
+        cbm.CBMState(bad)
+    assert e.value.code == 4
+
+
+def test_missing_state_file_is_an_io_error(tmp_path):
+    import cerebellum_simulation_b200 as cbm
+    with pytest.raises(cbm.CBMError) as e:
+        cbm.CBMState(str(tmp_path / "nope.state"))
+    assert e.value.code == 3
+
+
+def test_mf_bits_packing():
+    import cerebellum_simulation_b200 as cbm
+    x = np.zeros((2, 1024), np.uint8)
+    x[0, 0] = 1
+    x[0, 33] = 1
+    x[1, 1023] = 1
+    b = cbm.mf_bits(x, 33)
+    assert b.shape == (2, 33)
+    assert b[0, 0] == 1 and b[0, 1] == 2 and b[1, 31] == 1 << 31 and b[1, 32] == 0

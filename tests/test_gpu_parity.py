@@ -1,0 +1,164 @@
+"""Parity of the B200 step with the CPU oracle (which is pinned to the
+reference by tests/test_oracle_pin.py).
+
+Spike rasters and every float state that spikes depend on must match bit for
+bit; the GO glutamate/mGluR arrays, which no spike depends on, are compared
+within FP_RTOL (they use the double-precision exp of two different math
+libraries).  All calls go through the C ABI (libcbm_b200.so).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cbmtest
+from cbmtest import Oracle
+
+pytestmark = pytest.mark.gpu
+
+INNET_CON = ["haspGLfromMFtoGL", "pGLfromMFtoGL", "numpGLfromGLtoGO", "pGLfromGLtoGO", "numpGRfromMFtoGR",
+             "pGRfromMFtoGR", "numpGRfromGOtoGR", "pGRfromGOtoGR", "numpGRfromGRtoGO", "pGRfromGRtoGO",
+             "pGRDelayMaskfromGRtoGO", "pGRDelayMaskfromGRtoBSP", "numpMFfromMFtoGO", "pMFfromMFtoGO",
+             "numpGOGABAOutGOGO", "pGOGABAOutGOGO"]
+INNET_ACT = ["histMF", "apBufMF", "apGO", "apBufGO", "vGO", "vCoupleGO", "threshCurGO", "inputMFGO", "inputGOGO",
+             "gMFGO", "gGRGO", "gGOGO", "gMGluRGO", "gMGluRIncGO", "mGluRGO", "gluGO", "apGR", "apBufGR",
+             "gMFGR", "gMFSumGR", "gGOGR", "gGOSumGR", "threshGR", "vGR", "gKCaGR", "historyGR", "apSC",
+             "apBufSC", "gPFSC", "threshSC", "vSC", "inputSumPFSC"]
+ZONE_ACT = ["apBC", "apBufBC", "inputPCBC", "gPFBC", "gPCBC", "threshBC", "vBC", "apPC", "apBufPC", "inputBCPC",
+            "inputSCPC", "pfSynWeightPC", "inputSumPFPC", "gPFPC", "gBCPC", "gSCPC", "vPC", "threshPC",
+            "histPCPopAct", "apIO", "apBufIO", "inputNCIO", "gNCIO", "threshIO", "vIO", "vCoupleIO",
+            "pfPCPlastTimerIO", "apNC", "apBufNC", "inputPCNC", "inputMFNC", "gPCNC", "gPCScaleNC",
+            "mfSynWeightNC", "gmaxNMDAofMFtoNC", "gmaxAMPAofMFtoNC", "gMFNMDANC", "gMFAMPANC", "threshNC",
+            "vNC", "synIOPReleaseNC"]
+
+
+def compare_states(path_a, path_b):
+    import cerebellum_simulation_b200 as cbm
+    a, b = cbm.CBMState(path_a), cbm.CBMState(path_b)
+    problems = []
+    names = [(n, -1) for n in INNET_CON + INNET_ACT] + [(n, z) for z in range(a.getNumZones()) for n in ZONE_ACT]
+    for n, z in names:
+        x, y = a.array(n, z), b.array(n, z)
+        if n in cbmtest.FP_TOLERANT_ARRAYS:
+            if not np.allclose(x, y, rtol=cbmtest.FP_RTOL, atol=1e-30, equal_nan=True):
+                problems.append(f"{n}: beyond rtol {cbmtest.FP_RTOL}")
+        elif not cbmtest.same_values(x, y).all():
+            problems.append(f"{n}[{z}]: {int(np.sum(~cbmtest.same_values(x, y)))} elements differ")
+    return problems
+
+
+def run_both(tmp_path, st_path, mf, seeds, events=None):
+    import cerebellum_simulation_b200 as cbm
+    o = Oracle(st_path, seeds=seeds)
+    tr_o = o.run(mf, events)
+    st = cbm.CBMState(st_path)
+    sim = cbm.CBMSimCore(st, seeds, device=0)
+    tr_p = cbmtest.product_run(sim, mf, events)
+    fin_o, fin_p = str(tmp_path / "oracle.state"), str(tmp_path / "b200.state")
+    o.save(fin_o)
+    sim.writeToState(fin_p)
+    return o, tr_o, tr_p, fin_o, fin_p
+
+
+EVENTS = {
+    5: [("plast", 0, -0.01, 0.005)],
+    700: [("errdrive", 0, 1.0)],
+    1000: [("errdrive", 0, 0.6)],
+    1200: [("plastreset", 0)],
+    1300: [("grgoinc", 0.01)],
+    1400: [("grgoincreset",)],
+}
+
+
+def test_reference_network_16k_bit_exact(tmp_path):
+    """The reference's own 16K network (its generator), 1500 steps with
+    plasticity, error-drive and GR->GO gain events."""
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    mf = cbmtest.counter_mf(1024, 1500, 11)
+    o, tr_o, tr_p, fo, fp = run_both(tmp_path, st, mf, [7], EVENTS)
+    gold = cbmtest.load_json("ref16k_digests.json")
+    assert [cbmtest.sha(r) for r in tr_o] == gold["records"]
+    assert cbmtest.first_difference(tr_o, tr_p, o.num) is None
+    assert compare_states(fo, fp) == []
+
+
+def test_config1_bit_exact(tmp_path):
+    """Config 1: 16,384 GR with random wiring, 2000 steps of regenerating
+    Poisson MF input at 1-30 Hz, PF->PC plasticity forced on."""
+    from cerebellum_simulation_b200 import networks
+    net = networks.config1_network(seed=0)
+    p = str(tmp_path / "c1.state")
+    net.writeState(p)
+    mf = networks.uniform_mf_stream(1024, 2000, seed=0)
+    ev = {1: [("plast", 0, -0.002, 0.001)], 1500: [("errdrive", 0, 1.0)]}
+    o, tr_o, tr_p, fo, fp = run_both(tmp_path, p, mf, [3], ev)
+    assert cbmtest.first_difference(tr_o, tr_p, o.num) is None
+    assert compare_states(fo, fp) == []
+
+
+def test_two_zones_bit_exact(tmp_path):
+    from cerebellum_simulation_b200 import networks
+    net = networks.build_random_network(8, 6, 4, 4, 10, networks.act_params("16k"), seed=5, gr_per_go=128,
+                                       mf_per_go=3, vel=40, gogo=((1, 1, 0.0),), n_zones=2)
+    p = str(tmp_path / "z2.state")
+    net.writeState(p)
+    mf = cbmtest.counter_mf(1024, 600, 8, rate_hi=0.08)
+    ev = {2: [("plast", 1, -0.003, 0.002)], 300: [("errdrive", 1, 1.0), ("errdrive", 0, 0.5)]}
+    o, tr_o, tr_p, fo, fp = run_both(tmp_path, p, mf, [3, 4], ev)
+    assert cbmtest.first_difference(tr_o, tr_p, o.num) is None
+    assert compare_states(fo, fp) == []
+
+
+def test_config2_1m_bit_exact_short(tmp_path):
+    """Config 2 size (1,048,576 GR, 1024 GO, 32 PC x 32,768 PF): 150 steps."""
+    from cerebellum_simulation_b200 import networks
+    net = networks.config2_network(seed=0)
+    p = str(tmp_path / "c2.state")
+    net.writeState(p)
+    mf = networks.eyelid_mf_stream(1024, 150, seed=0, cs_on=50, cs_off=120)
+    ev = {1: [("plast", 0, -0.0005, 0.0005)], 119: [("errdrive", 0, 1.0)]}
+    o, tr_o, tr_p, fo, fp = run_both(tmp_path, p, mf, [9], ev)
+    assert cbmtest.first_difference(tr_o, tr_p, o.num) is None
+    assert compare_states(fo, fp) == []
+
+
+def test_graph_run_equals_step_calls(tmp_path):
+    """Resident-input CUDA-graph runs give the step-by-step API's result."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    net = networks.config1_network(seed=1)
+    p = str(tmp_path / "c1.state")
+    net.writeState(p)
+    mf = networks.uniform_mf_stream(1024, 700, seed=4)
+    a = cbm.CBMSimCore(cbm.CBMState(p), [5], device=0)
+    cbmtest.product_run(a, mf, record=False)
+    fa = str(tmp_path / "a.state")
+    a.writeToState(fa)
+    b = cbm.CBMSimCore(cbm.CBMState(p), [5], device=0, resident_steps=700)
+    b.load_mf_stream(cbm.mf_bits(mf, b.mf_words()))
+    b.run(700, chunk=64)
+    assert b.steps_done() == 700
+    fb = str(tmp_path / "b.state")
+    b.writeToState(fb)
+    assert open(fa, "rb").read() == open(fb, "rb").read()
+
+
+def test_device_expf_matches_host_expf():
+    """The small-cell updates' float exponential equals the host C library's
+    expf (the reference's exp(float)) on every probed input."""
+    import ctypes
+    import cerebellum_simulation_b200 as cbm
+    rng = np.random.default_rng(0)
+    x = np.concatenate([
+        rng.uniform(-110, 95, 4_000_000).astype(np.float32),
+        rng.uniform(-2, 2, 4_000_000).astype(np.float32),
+        (rng.integers(0, 2**32, 4_000_000, dtype=np.uint64).astype(np.uint32)).view(np.float32),
+        np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 88.0, 88.7228, 88.72284, -103.97, -103.9721, -104.0,
+                  1e-30, -1e-30, float.fromhex('0x1.04845ep+5'), float.fromhex('-0x1.f8cbb2p+5')], dtype=np.float32)])
+    dev = cbm.device_expf(x)
+    lib = Oracle.lib()
+    lib.cbm_oracle_expf_array.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
+    host = np.empty_like(x)
+    lib.cbm_oracle_expf_array(x.ctypes.data, host.ctypes.data, x.size)
+    same = (dev.view(np.uint32) == host.view(np.uint32)) | (np.isnan(dev) & np.isnan(host))
+    assert same.all(), f"{int((~same).sum())} mismatches, first at x={x[~same][0]!r}"

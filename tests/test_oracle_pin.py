@@ -1,0 +1,88 @@
+"""Pins the CPU oracle to the reference.
+
+The oracle (oracle/cbm_oracle.c) restates the reference's calcActivity; here
+it must reproduce, bit for bit, the trace records and final state of the
+reference's own host code:
+  - against golden digests recorded from oracle/_ref/ref_run (always run);
+  - against oracle/_ref/ref_run live, where the harness is built;
+  - with the reference's GR-sharded multi-GPU host path (2 and 4 fake GPUs),
+    which must equal its single-GPU result.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cbmtest
+from cbmtest import Oracle
+
+EVENTS16K = {
+    5: [("plast", 0, -0.01, 0.005)],
+    700: [("errdrive", 0, 1.0)],
+    1000: [("errdrive", 0, 0.6)],
+    1200: [("plastreset", 0)],
+    1300: [("grgoinc", 0.01)],
+    1400: [("grgoincreset",)],
+}
+
+
+def test_oracle_matches_reference_golden_16k(tmp_path):
+    gold = cbmtest.load_json("ref16k_digests.json")
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    o = Oracle(st, seeds=[7])
+    mf = cbmtest.counter_mf(1024, gold["steps"], 11)
+    tr = o.run(mf, EVENTS16K)
+    assert tr.shape[1] == gold["record_bytes"]
+    got = [cbmtest.sha(r) for r in tr]
+    bad = [i for i, (a, b) in enumerate(zip(got, gold["records"])) if a != b]
+    assert not bad, f"first differing step {bad[0] + 1}"
+    fin = str(tmp_path / "final.state")
+    o.save(fin)
+    with open(fin, "rb") as f:
+        assert cbmtest.sha(np.frombuffer(f.read(), np.uint8)) == gold["final_state"]
+
+
+def test_oracle_matches_reference_golden_config1(tmp_path):
+    from cerebellum_simulation_b200 import networks
+    gold = cbmtest.load_json("config1_digests.json")
+    net = networks.config1_network(seed=0)
+    p = str(tmp_path / "c1.state")
+    net.writeState(p)
+    with open(p, "rb") as f:
+        assert cbmtest.sha(np.frombuffer(f.read(), np.uint8)) == gold["initial_state"], \
+            "config-1 generator is not deterministic"
+    o = Oracle(p, seeds=[7])
+    mf = networks.uniform_mf_stream(1024, gold["steps"], seed=0)
+    tr = o.run(mf)
+    got = [cbmtest.sha(r) for r in tr]
+    bad = [i for i, (a, b) in enumerate(zip(got, gold["records"])) if a != b]
+    assert not bad, f"first differing step {bad[0] + 1}"
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+@pytest.mark.parametrize("mf_seed,zone_seed", [(3, 99), (4, 12345)])
+def test_oracle_matches_reference_live(tmp_path, mf_seed, zone_seed):
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    mf = cbmtest.counter_mf(1024, 800, mf_seed, rate_hi=0.1)
+    ev = {3: [("plast", 0, -0.02, 0.01)], 400: [("errdrive", 0, 1.0)], 401: [("errdrive", 0, 0.2)]}
+    fin_ref = str(tmp_path / "ref_final.state")
+    ref = cbmtest.ref_run(st, mf, [zone_seed], ev, final_path=fin_ref).reshape(800, -1)
+    o = Oracle(st, seeds=[zone_seed])
+    tr = o.run(mf, ev)
+    assert cbmtest.first_difference(ref, tr, o.num) is None
+    fin = str(tmp_path / "oracle_final.state")
+    o.save(fin)
+    assert open(fin, "rb").read() == open(fin_ref, "rb").read()
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+@pytest.mark.parametrize("gpus", [2, 4])
+def test_reference_sharded_path_equals_single(tmp_path, gpus):
+    """The reference splits GR across GPUs and sums GR->GO counts on the
+    host (innet.cpp:177, 835-838); with the fake runtime reporting several
+    devices it must give the single-device result, which the oracle pins."""
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    mf = cbmtest.counter_mf(1024, 300, 5)
+    single = cbmtest.ref_run(st, mf, [7], None)
+    sharded = cbmtest.ref_run(st, mf, [7], None, num_gpus=gpus)
+    assert np.array_equal(single, sharded)
