@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the 1 ms cerebellar network step on B200.
+
+Workload: the 1M-GR eyelid-conditioning network (1,048,576 GR with 4 MF + 3
+GO dendrites and 4 GO targets each, 1024 GO, 1024 MF, 32 PC x 32,768 PF,
+128 BC, 512 SC, 8 NC, 4 IO), random wiring and random-init state, MF input
+from the regenerating-Poisson rule with the eyelid protocol's rates (10%
+tonic 50-80 Hz, the rest 1-10 Hz, 80 CS fibres at 100 Hz from 2000 to 2500 ms
+of each 5000-step trial), the US (error drive 1.0) at CS offset, PF->PC LTD/LTP
+on with the reference driver's plasticity window (csOn+200 .. csOff+200).
+
+A step is one calcActivity of the whole network.  `value` is whole-job
+network steps per second with the MF input resident in HBM and the steps
+replayed as CUDA graphs; `e2e` is the same metric through the per-step C-ABI
+calls a drop-in user makes (updateMFInput from pinned host memory,
+calcActivity, exportAPNC read back every step).
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TRIAL = 5000
+CS_ON, CS_OFF = 2000, 2500
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--chunk", type=int, default=50)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def protocol_events(t0, t1):
+    """Eyelid-driver host calls (ecmanagementdelay.cpp:201-235) that fall
+    before steps t0+1..t1 (1-based global step t = trial*5000 + currentTime + 1)."""
+    ev = {}
+    for t in range(t0 + 1, t1 + 1):
+        ct = (t - 1) % TRIAL
+        if ct == CS_ON + 200:
+            ev[t] = ("plast", -0.0005, 0.0005)
+        elif ct == CS_OFF - 1:
+            ev[t] = ("errdrive", 1.0)
+        elif ct == CS_OFF + 200:
+            ev[t] = ("plastreset",)
+    return ev
+
+
+def apply_event(sim, e):
+    z = sim.getMZoneList()[0]
+    if e[0] == "plast":
+        z.setGRPCPlastSteps(e[1], e[2])
+    elif e[0] == "plastreset":
+        z.resetGRPCPlastSteps()
+    elif e[0] == "errdrive":
+        sim.updateErrDrive(0, e[1])
+
+
+def run_protocol(sim, t0, nsteps, chunk):
+    """Advance nsteps graph-replayed steps, stopping at protocol events."""
+    ev = protocol_events(t0, t0 + nsteps)
+    t = t0
+    for te in sorted(ev):
+        if te - 1 > t:
+            sim.run(te - 1 - t, chunk)
+            t = te - 1
+        apply_event(sim, ev[te])
+    if t0 + nsteps > t:
+        sim.run(t0 + nsteps - t, chunk)
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                     stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9 and p[1].replace(".", "").isdigit():
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()) if rows else None,
+                "reasons": sorted(reasons)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the GR pass from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "gr_pass_1M_eyelid.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def cpu_reference(state_path, mf, steps, threads):
+    """The reference's own calcActivity (oracle/_ref, OpenMP build) on host cores."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_run_omp")
+    if not os.path.exists(exe):
+        exe = os.path.join(ROOT, "oracle", "_ref", "ref_run")
+        threads = 1
+    if not os.path.exists(exe):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        mfp = os.path.join(d, "mf.u8")
+        np.ascontiguousarray(mf[:steps], dtype=np.uint8).tofile(mfp)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        out = subprocess.run([exe, state_path, mfp, str(steps), "-", "-", "7", "-t"], capture_output=True,
+                             text=True, env=env, check=True).stdout
+    line = [l for l in out.splitlines() if l.startswith("{")][-1]
+    r = json.loads(line)
+    return {"value": r["steps_per_s"], "unit": "steps/s", "cores": threads, "kind": "reference",
+            "sample": f"{steps} steps of the same 1M-GR network and MF input (first {steps} ms of trial 1), "
+                      f"reference host code + CPU kernel restatement, OpenMP {threads} threads"}
+
+
+WORKLOAD = ("1M-GR eyelid network: 1,048,576 GR (4 MF + 3 GO inputs, 4 GO targets each), 1024 GO, 1024 MF, "
+            "32 PC x 32,768 PF, 128 BC, 512 SC, 8 NC, 4 IO; CS 2000-2500 of 5000-step trials, US at CS offset, "
+            "PF->PC LTD/LTP on")
+
+
+def main():
+    args = parse()
+    assert args.warmup >= 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    total_steps = args.warmup + args.steps
+
+    from cerebellum_simulation_b200 import networks
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        st = networks.config2_network(seed=args.seed)
+        n_ref = min(args.steps, 200)
+        mf = networks.eyelid_mf_stream(1024, n_ref + 3, seed=args.seed)
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "c2.state")
+            st.writeState(p)
+            res = cpu_reference(p, mf, n_ref, threads)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
+            return
+        v = res["value"]
+        print(json.dumps({"metric": "1 ms steps/s at 1M GR", "value": v, "unit": "steps/s", "impl": "reference",
+                          "n_gpus": args.gpus, "steps": n_ref, "warmup": 0, "ms_per_step": 1000.0 / v,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+                          "cpu_baseline": res,
+                          "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    device = local
+    torch.cuda.set_device(device)
+
+    import cerebellum_simulation_b200 as cbm
+    st = networks.config2_network(seed=args.seed + rank)
+    mf = networks.eyelid_mf_stream(1024, total_steps, seed=args.seed + rank)
+    sim = cbm.CBMSimCore(st, [7 + rank], device=device, resident_steps=total_steps)
+    bits = cbm.mf_bits(mf, sim.mf_words())
+    sim.load_mf_stream(bits)
+
+    # warm-up, then flush L2 before the timed region
+    run_protocol(sim, 0, args.warmup, args.chunk)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
+    flush.fill_(1.0)
+    torch.cuda.synchronize(device)
+    del flush
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+
+    clocks = ClockSampler(device)
+    clocks.start()
+    sim.timer_start()
+    run_protocol(sim, args.warmup, args.steps, args.chunk)
+    ms = sim.timer_stop()
+    clock_info = clocks.stop()
+    torch.cuda.synchronize(device)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_per_s = world * args.steps / (ms / 1000.0)
+
+    # roofline: GR-pass durations from events around each pass in the graph
+    n_roof = min(args.steps, 1000)
+    sim2 = cbm.CBMSimCore(st, [7 + rank], device=device, resident_steps=n_roof + 3 * args.chunk)
+    sim2.load_mf_stream(cbm.mf_bits(mf[: n_roof + 3 * args.chunk], sim2.mf_words()))
+    sim2.run(2 * args.chunk, args.chunk, time_pass=True)
+    _, pass_ms = sim2.run(n_roof - (n_roof % args.chunk) or args.chunk, args.chunk, time_pass=True)
+    tail_ms = sim2.last_tail_ms()
+    alg_bytes = sim.algorithmic_bytes_per_step()
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (pass_ms / 1000.0) / 1e9
+    sim2.close()
+
+    # end to end through the per-step C ABI
+    n_e2e = min(args.steps, 2000)
+    sim3 = cbm.CBMSimCore(st, [7 + rank], device=device)
+    zone = sim3.getMZoneList()[0]
+    for s in range(20):
+        sim3.updateMFInput(mf[s])
+        sim3.calcActivity()
+        zone.exportAPNC()
+    if dist:
+        dist.barrier()
+    sim3.timer_start()
+    for s in range(20, 20 + n_e2e):
+        sim3.updateMFInput(mf[s % total_steps])
+        sim3.calcActivity()
+        zone.exportAPNC()
+    e2e_ms = sim3.timer_stop()
+    if dist:
+        t = torch.tensor([e2e_ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * n_e2e / (e2e_ms / 1000.0)
+    h2d = sim3.mf_words() * 4
+    d2h = st.con("numNC")
+    sim3.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "c2.state")
+            st.writeState(p)
+            cpu = cpu_reference(p, mf, 200, os.cpu_count() or 1)
+
+    launches = 2 * args.steps + (args.steps // args.chunk + 8)
+    if rank == 0:
+        out = {
+            "metric": "1 ms steps/s at 1M GR", "value": steps_per_s, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (random wiring, random-init state, regenerating-Poisson MF input)",
+            "config": {"workload": WORKLOAD, "global_batch": world, "parallelism": f"replicas x{world}",
+                       "graph_chunk": args.chunk,
+                       "l2": "flushed (2x L2 written) before the timed region; the K steps inside it are one "
+                             "continuous simulation whose 67 MB per-step working set stays partly L2-resident"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic(),
+                         "kernel": "grPassKernel", "pass_ms": pass_ms, "tail_ms": tail_ms,
+                         "algorithmic_bytes": alg_bytes,
+                         "peak_source": peak_kind},
+            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+        }
+        if cpu:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

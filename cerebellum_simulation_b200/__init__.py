@@ -54,7 +54,7 @@ class CBMError(RuntimeError):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m cerebellum_simulation_b200.build`")
+            f"{LIB_PATH} is missing: build it with `python cerebellum_simulation_b200/build.py`")
     lib = ctypes.CDLL(LIB_PATH)
     P, I, U, F, D, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, ctypes.c_float, ctypes.c_double, ctypes.c_char_p
     U64, U32 = ctypes.c_uint64, ctypes.c_uint32
@@ -87,6 +87,9 @@ def _load():
         "cbm_sim_load_mf_stream": (I, [P, P, U64]),
         "cbm_sim_run": (I, [P, U64, U32, ctypes.POINTER(F), ctypes.POINTER(F)]),
         "cbm_sim_algorithmic_bytes_per_step": (D, [P]),
+        "cbm_sim_timer_start": (I, [P]),
+        "cbm_sim_last_tail_ms": (I, [P, ctypes.POINTER(F)]),
+        "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_destroy": (None, [P]),
         "cbm_device_expf": (I, [I, P, P, U64]),
     }
@@ -301,6 +304,19 @@ class CBMSimCore:
         ms, pms = ctypes.c_float(), ctypes.c_float()
         _check(lib.cbm_sim_run(self._h, nsteps, chunk, ctypes.byref(ms), ctypes.byref(pms) if time_pass else None))
         return ms.value, (pms.value if time_pass else None)
+
+    def last_tail_ms(self):
+        ms = ctypes.c_float()
+        _check(lib.cbm_sim_last_tail_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def timer_start(self):
+        _check(lib.cbm_sim_timer_start(self._h))
+
+    def timer_stop(self):
+        ms = ctypes.c_float()
+        _check(lib.cbm_sim_timer_stop(self._h, ctypes.byref(ms)))
+        return ms.value
 
     def algorithmic_bytes_per_step(self):
         return lib.cbm_sim_algorithmic_bytes_per_step(self._h)

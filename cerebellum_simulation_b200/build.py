@@ -2,8 +2,8 @@
 
 The library holds the CUDA kernels, the host orchestration and the C ABI
 declared in ``include/cbm_b200.h``.  It is built in the package directory so
-that it travels with the source tree; ``python -m cerebellum_simulation_b200.build``
-rebuilds it.
+that it travels with the source tree; ``python cerebellum_simulation_b200/build.py``
+rebuilds it (run as a file: importing the package needs the library).
 """
 import os
 import shutil

@@ -314,6 +314,27 @@ int cbm_sim_run(cbm_sim *sim, uint64_t nsteps, uint32_t chunk, float *gpuMs, flo
 	return CBM_OK;
 }
 
+int cbm_sim_last_tail_ms(cbm_sim *sim, float *ms)
+{
+	NEED(sim); NEED(ms);
+	*ms = sim->sim.lastTailMs();
+	return CBM_OK;
+}
+
+int cbm_sim_timer_start(cbm_sim *sim)
+{
+	NEED(sim);
+	TRY(sim->sim.timerStart());
+	return CBM_OK;
+}
+
+int cbm_sim_timer_stop(cbm_sim *sim, float *ms)
+{
+	NEED(sim); NEED(ms);
+	TRY(sim->sim.timerStop(ms));
+	return CBM_OK;
+}
+
 double cbm_sim_algorithmic_bytes_per_step(cbm_sim *sim)
 {
 	return sim ? NET(sim).bytesPerStepAlgorithmic() : 0.0;

@@ -104,11 +104,11 @@ struct DevNet {
 	float *gMFGO, *gGRGO, *gGOGO, *gMGluRGO, *gMGluRIncGO, *mGluRGO, *gluGO;
 	uint8_t *apSC; uint32_t *apBufSC; float *gPFSC, *threshSC, *vSC;
 	uint32_t *sumGRInputGO; float *sumInputGOGABASynDepGO;
-	float *threshSnap;        // GO thresholds before the coupling sweep
 
 	// ---- input-net connectivity used by the small-cell updates
 	const int32_t *numpMFfromMFtoGO; const uint32_t *pMFfromMFtoGO;
 	const uint32_t *gogoStart, *gogoSrc;  // per GO: sources of GO->GO synapses in (source, slot) order
+	const uint32_t *mfgoStart, *mfgoSrc;  // per GO: MF sources (with repeats) of updateMFtoGOOut
 	const int32_t *numpGOCoupInGOGO; const uint32_t *pGOCoupInGOGO;
 	const uint32_t *coupLevelStart, *coupLevelGO;  // coupling sweep schedule
 

@@ -274,46 +274,172 @@ __device__ float pcRowTree(const float *part, uint32_t bs, uint32_t lane)
 	return x;
 }
 
-__global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, uint32_t stepOffset)
+// Sequential left-to-right float sum of one value per lane (lanes 0..n-1),
+// the order of the reference's `sum = sum + x[j]` loops; every lane gets it.
+__device__ __forceinline__ float orderedLaneSum(float v, uint32_t n)
 {
-	const DevNet *__restrict__ N = nets[blockIdx.x];
-	const uint64_t t = *N->tBase + 1 + stepOffset;
+	float s = 0;
+	for (uint32_t j = 0; j < n; j++) s = s + __shfl_sync(0xffffffffu, v, j);
+	return s;
+}
+
+// Golgi role (one CTA per network): calcGOActivities, updateMFtoGOOut and
+// updateGOtoGOOut (innet.cpp:816-980).  Reads GR->GO counts of pass(t-1),
+// writes GO spikes of step t for pass(t+1).
+__device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
+{
+	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u;
+	const uint32_t numGO = N->numGO;
+	const uint32_t G = (uint32_t)((t - 1) & 1);
+	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	uint32_t *sMF = sm;
+	float *sScale = reinterpret_cast<float *>(sMF + N->mfWords);
+	float *sV = sScale + numGO;
+	float *sTh = sV + numGO;
+	uint8_t *sAp = reinterpret_cast<uint8_t *>(sTh + numGO);
+	for (uint32_t i = tid; i < N->mfWords; i += nThr) sMF[i] = mfW[i];
+	__syncthreads();
+
+	uint32_t *goIn = N->goCount + (size_t)G * numGO;
+	uint32_t *goBitsOut = N->goBits + (size_t)(t & 1) * N->goWords;
+	const float gIncGRtoGO = N->ctl->gIncGRtoGO;
+	for (uint32_t base = 0; base < numGO; base += nThr) {
+		const uint32_t i = base + tid;
+		uint8_t ap = 0;
+		if (i < numGO) {
+			const unsigned int totalGRIn = goIn[i];
+			goIn[i] = 0;
+			const uint32_t inMF = N->inputMFGO[i];
+			const float inDep = N->inputGOGABASynDepGO[i];
+			N->sumGRInputGO[i] = totalGRIn;
+			N->sumInputGOGABASynDepGO[i] = inDep;
+			const float gMF = inMF * N->gIncMFtoGO + N->gMFGO[i] * N->gDecMFtoGO;
+			const float gGR = totalGRIn * gIncGRtoGO + N->gGRGO[i] * N->gDecGRtoGO;
+			const float gGO = inDep * N->gGABAIncGOtoGO + N->gGOGO[i] * N->gGABADecGOtoGO;
+			N->gMFGO[i] = gMF; N->gGRGO[i] = gGR; N->gGOGO[i] = gGO;
+			float glu = N->gluGO[i];
+			glu = glu * N->gluDecayGO + totalGRIn * N->gluScaleGO * exp(-1.5 * glu);
+			float mg = N->mGluRGO[i];
+			mg = mg * N->mGluRDecayGO + glu * N->mGluRScaleGO * cbmExpf(-mg);
+			float mgi = N->gMGluRIncGO[i];
+			mgi = mgi * N->gMGluRIncDecayGO + mg * N->gMGluRIncScaleGO * cbmExpf(-mgi);
+			N->gluGO[i] = glu; N->mGluRGO[i] = mg; N->gMGluRIncGO[i] = mgi;
+			N->gMGluRGO[i] = N->gMGluRGO[i] * N->gMGluRDecGRtoGO + mgi * N->gMGluRScaleGRtoGO;
+			float th = N->threshCurGO[i] + (N->threshRestGO - N->threshCurGO[i]) * N->threshDecGO;
+			float v = N->vGO[i];
+			v = v + (N->gLeakGO * (N->eLeakGO - v)) + (gGO * (N->eGABAGO - v)) - (gMF + gGR) * v + N->vCoupleGO[i];
+			N->vGO[i] = v;
+			ap = v > th;
+			N->apGO[i] = ap;
+			N->apBufGO[i] = (N->apBufGO[i] << 1) | (ap * 0x00000001u);
+			th = ap * N->threshMaxGO + (!ap) * th;
+			N->threshCurGO[i] = th;
+			sScale[i] = N->goGABAOutSynScaleGOGO[i];
+			sV[i] = v; sTh[i] = th; sAp[i] = ap;
+			// updateMFtoGOOut for this step's MF spikes, gathered per GO
+			uint32_t cnt = 0;
+			for (uint32_t e = N->mfgoStart[i]; e < N->mfgoStart[i + 1]; e++) cnt += spikeBit(sMF, N->mfgoSrc[e]);
+			N->inputMFGO[i] = cnt;
+		}
+		const uint32_t word = __ballot_sync(0xffffffffu, ap != 0);
+		if (lane == 0 && i < numGO) goBitsOut[i >> 5] = word;
+	}
+	__syncthreads();
+	// updateGOtoGOOut: GABA inputs in (source, slot) order, depression scale,
+	// electrical coupling (innet.cpp:937-978)
+	for (uint32_t d = tid; d < numGO; d += nThr) {
+		uint32_t cnt = 0;
+		float acc = 0;
+		for (uint32_t e = N->gogoStart[d]; e < N->gogoStart[d + 1]; e++) {
+			const uint32_t src = N->gogoSrc[e];
+			if (sAp[src]) { cnt++; acc += sScale[src]; }
+		}
+		N->inputGOGO[d] = cnt;
+		N->inputGOGABASynDepGO[d] = acc;
+		const float s = sScale[d];
+		const uint8_t ap = sAp[d];
+		N->goGABAOutSynScaleGOGO[d] = s + (!ap) * (1 - s) * N->goGABAGOGOSynRec - ap * (s * (1 - N->goGABAGOGOSynDepF));
+		float vc = 0;
+		const int nc = N->numpGOCoupInGOGO[d];
+		for (int j = 0; j < nc; j++) {
+			const uint32_t n = N->pGOCoupInGOGO[(size_t)d * N->maxnumpGOCoupInGOGO + j];
+			vc = vc + N->coupleRiRjRatioGO * (sV[n] - sV[d]);
+		}
+		N->vCoupleGO[d] = vc;
+	}
+	// threshold coupling: the reference's serial sweep reads already-updated
+	// thresholds of lower-indexed neighbours; the level schedule preserves it
+	for (uint32_t L = 0; L < N->numCoupLevels; L++) {
+		__syncthreads();
+		for (uint32_t e = N->coupLevelStart[L] + tid; e < N->coupLevelStart[L + 1]; e += nThr) {
+			const uint32_t i = N->coupLevelGO[e];
+			const float own = sTh[i];
+			float tc = 0;
+			const int nc = N->numpGOCoupInGOGO[i];
+			for (int j = 0; j < nc; j++) {
+				const uint32_t n = N->pGOCoupInGOGO[(size_t)i * N->maxnumpGOCoupInGOGO + j];
+				const float other = n < i ? N->threshCurGO[n] : sTh[n];
+				tc = tc + N->coupleRiRjRatioGO * (other - own);
+			}
+			N->threshCurGO[i] = own + tc;
+		}
+	}
+}
+
+// Microzone role (one CTA per network): calcSCActivities (innet.cpp:892-911),
+// the MF bookkeeping of updateMFInput (innet.cpp:800-815) and resetMFHist
+// (:982-995), and every microzone update and fan-out (mzone.cpp:167-605).
+// Reads the PF sums of pass(t-2).
+__device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
+{
 	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u, warp = tid >> 5, nWarps = nThr >> 5;
 	const uint32_t Z = N->numZones;
-	const uint32_t numGO = N->numGO, numMF = N->numMF, numPC = N->numPC, numBC = N->numBC,
-		numSC = N->numSC, numNC = N->numNC, numIO = N->numIO;
-	const uint32_t R = (uint32_t)((t + 1) % 3);     // buffers of pass(t-2)
-	const uint32_t G = (uint32_t)((t - 1) & 1);     // GR->GO counts of pass(t-1)
+	const uint32_t numMF = N->numMF, numPC = N->numPC, numBC = N->numBC, numSC = N->numSC, numNC = N->numNC,
+		numIO = N->numIO;
+	const uint32_t R = (uint32_t)((t + 1) % 3);
 	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
 	const uint8_t *mfRaw = N->hasMFRaw ? N->mfRaw + (size_t)((t - 1) % N->mfRing) * numMF : nullptr;
 	HostCtl *ctl = N->ctl;
+	const uint32_t nMFNC = N->numpNCfromMFtoNC, nIONC = N->numpIOfromNCtoIO;
+	uint32_t *sMF = sm;
+	uint8_t *sApSC = reinterpret_cast<uint8_t *>(sMF + N->mfWords);
+	float *ncScratch = reinterpret_cast<float *>(sApSC + ((numSC + 15) & ~15u));
+	float *ioScratch = ncScratch + (size_t)Z * numNC * 2 * nMFNC;
+	int *sFlags = reinterpret_cast<int *>(ioScratch + (size_t)Z * numIO * nIONC);
+	for (uint32_t i = tid; i < N->mfWords; i += nThr) sMF[i] = mfW[i];
+	__syncthreads();
 
-	extern __shared__ float tsm[];
-	float *ncScratch = tsm;                          // [nWarps][2][numpNCfromMFtoNC]
-	__shared__ int sDoLTD[kMaxZones], sDoLTP[kMaxZones];
-
-	// ---- phase 1 cells: PC, BC (per zone), SC (cbmsimcore.cpp:192-200)
+	// ---- phase 1 (cbmsimcore.cpp:192-200): PC and BC per zone, SC
 	for (uint32_t task = warp; task < Z * numPC; task += nWarps) {
 		const uint32_t z = task / numPC, i = task % numPC;
 		const DevZone &Q = N->zones[z];
 		const float inputSum = pcRowTree(Q.pcPartial + ((size_t)R * numPC + i) * N->bs, N->bs, lane);
-		if (lane == 0) {
-			// calcPCActivities (mzone.cpp:187-226)
-			float gSCPCSum;
-			Q.gPFPC[i] = Q.gPFPC[i] + inputSum * N->gIncGRtoPC;
-			Q.gPFPC[i] = Q.gPFPC[i] * N->gDecGRtoPC;
-			Q.gBCPC[i] = Q.gBCPC[i] + Q.inputBCPC[i] * N->gIncBCtoPC;
-			Q.gBCPC[i] = Q.gBCPC[i] * N->gDecBCtoPC;
-			gSCPCSum = 0;
-			for (uint32_t j = 0; j < N->numpPCfromSCtoPC; j++) {
+		// calcPCActivities (mzone.cpp:187-226); the SC conductances update
+		// elementwise, their sum runs in the reference's order
+		float gSCPCSum = 0;
+		for (uint32_t j0 = 0; j0 < N->numpPCfromSCtoPC; j0 += 32) {
+			const uint32_t j = j0 + lane;
+			float g = 0;
+			if (j < N->numpPCfromSCtoPC) {
 				const size_t k = (size_t)i * N->numpPCfromSCtoPC + j;
-				Q.gSCPC[k] = Q.gSCPC[k] + N->gIncSCtoPC * (1 - Q.gSCPC[k]) * Q.inputSCPC[k];
-				Q.gSCPC[k] = Q.gSCPC[k] * N->gDecSCtoPC;
-				gSCPCSum += Q.gSCPC[k];
+				g = Q.gSCPC[k];
+				g = g + N->gIncSCtoPC * (1 - g) * Q.inputSCPC[k];
+				g = g * N->gDecSCtoPC;
+				Q.gSCPC[k] = g;
 			}
+			const uint32_t n = min(32u, N->numpPCfromSCtoPC - j0);
+			for (uint32_t q = 0; q < n; q++) gSCPCSum += __shfl_sync(0xffffffffu, g, q);
+		}
+		if (lane == 0) {
+			float gPF = Q.gPFPC[i] + inputSum * N->gIncGRtoPC;
+			gPF = gPF * N->gDecGRtoPC;
+			Q.gPFPC[i] = gPF;
+			float gBC = Q.gBCPC[i] + Q.inputBCPC[i] * N->gIncBCtoPC;
+			gBC = gBC * N->gDecBCtoPC;
+			Q.gBCPC[i] = gBC;
 			float vPC = Q.vPC[i];
-			vPC = vPC + (N->gLeakPC * (N->eLeakPC - vPC)) - (Q.gPFPC[i] * vPC) +
-				(Q.gBCPC[i] * (N->eBCtoPC - vPC)) + (gSCPCSum * (N->eSCtoPC - vPC));
+			vPC = vPC + (N->gLeakPC * (N->eLeakPC - vPC)) - (gPF * vPC) +
+				(gBC * (N->eBCtoPC - vPC)) + (gSCPCSum * (N->eSCtoPC - vPC));
 			Q.vPC[i] = vPC;
 			float th = Q.threshPC[i] + (N->threshDecPC * (N->threshRestPC - Q.threshPC[i]));
 			const uint8_t ap = vPC > th;
@@ -329,12 +455,14 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 		const uint32_t z = task / numBC, i = task % numBC;
 		const DevZone &Q = N->zones[z];
 		// calcBCActivities (mzone.cpp:228-256)
-		Q.gPFBC[i] = Q.gPFBC[i] + (bcSum[i] * N->gIncGRtoBC);
-		Q.gPFBC[i] = Q.gPFBC[i] * N->gDecGRtoBC;
-		Q.gPCBC[i] = Q.gPCBC[i] + (Q.inputPCBC[i] * N->gIncPCtoBC);
-		Q.gPCBC[i] = Q.gPCBC[i] * N->gDecPCtoBC;
+		float gPF = Q.gPFBC[i] + (bcSum[i] * N->gIncGRtoBC);
+		gPF = gPF * N->gDecGRtoBC;
+		Q.gPFBC[i] = gPF;
+		float gPC = Q.gPCBC[i] + (Q.inputPCBC[i] * N->gIncPCtoBC);
+		gPC = gPC * N->gDecPCtoBC;
+		Q.gPCBC[i] = gPC;
 		float v = Q.vBC[i];
-		v = v + (N->gLeakBC * (N->eLeakBC - v)) - (Q.gPFBC[i] * v) + (Q.gPCBC[i] * (N->ePCtoBC - v));
+		v = v + (N->gLeakBC * (N->eLeakBC - v)) - (gPF * v) + (gPC * (N->ePCtoBC - v));
 		Q.vBC[i] = v;
 		float th = Q.threshBC[i] + N->threshDecBC * (N->threshRestBC - Q.threshBC[i]);
 		const uint8_t ap = v > th;
@@ -343,58 +471,22 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 		Q.threshBC[i] = ap * N->threshMaxBC + (!ap) * (th);
 	}
 	for (uint32_t i = tid; i < numSC; i += nThr) {
-		// calcSCActivities (innet.cpp:892-911)
 		float g = N->gPFSC[i] + (scSum[i] * N->gIncGRtoSC);
 		g = g * N->gDecGRtoSC;
 		N->gPFSC[i] = g;
 		float v = N->vSC[i];
 		v = v + (N->gLeakSC * (N->eLeakSC - v)) - g * v;
 		N->vSC[i] = v;
-		const uint8_t ap = v > N->threshSC[i];
+		const float thOld = N->threshSC[i];
+		const uint8_t ap = v > thOld;
 		N->apSC[i] = ap;
+		sApSC[i] = ap;
 		N->apBufSC[i] = (N->apBufSC[i] << 1) | (ap * 0x00000001u);
-		float th = N->threshSC[i] + N->threshDecSC * (N->threshRestSC - N->threshSC[i]);
+		float th = thOld + N->threshDecSC * (N->threshRestSC - thOld);
 		N->threshSC[i] = ap * N->threshMaxSC + (!ap) * (th);
 	}
-	__syncthreads();
-
-	// ---- phase 2: GO update (innet.cpp:816-891), MF bookkeeping (innet.cpp:800-815)
-	uint32_t *goIn = N->goCount + (size_t)G * numGO;
-	uint32_t *goBitsOut = N->goBits + (size_t)(t & 1) * N->goWords;
-	const float gIncGRtoGO = ctl->gIncGRtoGO;
-	for (uint32_t base = 0; base < numGO; base += nThr) {
-		const uint32_t i = base + tid;
-		uint8_t ap = 0;
-		if (i < numGO) {
-			const unsigned int totalGRIn = goIn[i];
-			goIn[i] = 0;
-			N->sumGRInputGO[i] = totalGRIn;
-			N->sumInputGOGABASynDepGO[i] = N->inputGOGABASynDepGO[i];
-			N->gMFGO[i] = N->inputMFGO[i] * N->gIncMFtoGO + N->gMFGO[i] * N->gDecMFtoGO;
-			N->gGRGO[i] = totalGRIn * gIncGRtoGO + N->gGRGO[i] * N->gDecGRtoGO;
-			N->gGOGO[i] = N->inputGOGABASynDepGO[i] * N->gGABAIncGOtoGO + N->gGOGO[i] * N->gGABADecGOtoGO;
-			N->gluGO[i] = N->gluGO[i] * N->gluDecayGO + totalGRIn * N->gluScaleGO * exp(-1.5 * N->gluGO[i]);
-			N->mGluRGO[i] = N->mGluRGO[i] * N->mGluRDecayGO + N->gluGO[i] * N->mGluRScaleGO * cbmExpf(-N->mGluRGO[i]);
-			N->gMGluRIncGO[i] = N->gMGluRIncGO[i] * N->gMGluRIncDecayGO + N->mGluRGO[i] * N->gMGluRIncScaleGO * cbmExpf(-N->gMGluRIncGO[i]);
-			N->gMGluRGO[i] = N->gMGluRGO[i] * N->gMGluRDecGRtoGO + N->gMGluRIncGO[i] * N->gMGluRScaleGRtoGO;
-			float th = N->threshCurGO[i] + (N->threshRestGO - N->threshCurGO[i]) * N->threshDecGO;
-			float v = N->vGO[i];
-			v = v + (N->gLeakGO * (N->eLeakGO - v)) + (N->gGOGO[i] * (N->eGABAGO - v))
-				- (N->gMFGO[i] + N->gGRGO[i]) * v + N->vCoupleGO[i];
-			N->vGO[i] = v;
-			ap = v > th;
-			N->apGO[i] = ap;
-			N->apBufGO[i] = (N->apBufGO[i] << 1) | (ap * 0x00000001u);
-			N->threshCurGO[i] = ap * N->threshMaxGO + (!ap) * th;
-			N->inputMFGO[i] = 0;
-			N->inputGOGO[i] = 0;
-			N->inputGOGABASynDepGO[i] = 0;
-		}
-		const uint32_t word = __ballot_sync(0xffffffffu, ap != 0);
-		if (lane == 0 && i < numGO) goBitsOut[i >> 5] = word;
-	}
 	for (uint32_t i = tid; i < numMF; i += nThr) {
-		const uint32_t m = spikeBit(mfW, i);
+		const uint32_t m = spikeBit(sMF, i);
 		N->histMF[i] = N->histMF[i] || (m > 0);
 		N->apBufMF[i] = (N->apBufMF[i] << 1) | (m * 0x00000001u);
 	}
@@ -402,134 +494,89 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 	for (uint32_t i = tid; i < numBC; i += nThr) N->bcCount[(size_t)R * numBC + i] = 0;
 	for (uint32_t i = tid; i < numSC; i += nThr) N->scCount[(size_t)R * numSC + i] = 0;
 
-	// ---- GO fan-outs (innet.cpp:912-980)
-	for (uint32_t i = tid; i < numMF; i += nThr) {
-		if (!spikeBit(mfW, i)) continue;
-		const int n = N->numpMFfromMFtoGO[i];
-		for (int j = 0; j < n; j++) atomicAdd(&N->inputMFGO[N->pMFfromMFtoGO[(size_t)i * N->maxnumpMFfromMFtoGO + j]], 1u);
+	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
+	// calcNCActivities (mzone.cpp:341-407) one warp per NC
+	for (uint32_t task = tid; task < Z * numIO * nIONC; task += nThr) {
+		const uint32_t z = task / (numIO * nIONC), k = task % (numIO * nIONC);
+		const DevZone &Q = N->zones[z];
+		float g = Q.gNCIO[k];
+		g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO) + N->gDecT0ofNCtoIO));
+		g = g + Q.inputNCIO[k] * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO);
+		Q.gNCIO[k] = g;
+		Q.inputNCIO[k] = 0;
+		ioScratch[task] = g;
 	}
-	for (uint32_t d = tid; d < numGO; d += nThr) {
-		uint32_t cnt = 0;
-		float acc = 0;
-		for (uint32_t e = N->gogoStart[d]; e < N->gogoStart[d + 1]; e++) {
-			const uint32_t src = N->gogoSrc[e];
-			if (N->apGO[src]) { cnt++; acc += N->goGABAOutSynScaleGOGO[src]; }
+	for (uint32_t task = warp; task < Z * numNC; task += nWarps) {
+		const uint32_t z = task / numNC, i = task % numNC;
+		const DevZone &Q = N->zones[z];
+		float *sN = ncScratch + (size_t)task * 2 * nMFNC;
+		for (uint32_t j = lane; j < nMFNC; j += 32) {
+			const size_t k = (size_t)i * nMFNC + j;
+			const float in = Q.inputMFNC[k], wt = Q.mfSynWeightNC[k];
+			float gmN = Q.gmaxNMDAofMFtoNC[k];
+			gmN = gmN * N->gmaxNMDADecMFtoNC + in * wt * (1 - gmN);
+			Q.gmaxNMDAofMFtoNC[k] = gmN;
+			float gN = Q.gMFNMDANC[k];
+			gN = gN + N->gNMDAIncMFtoNC * (gmN - gN);
+			Q.gMFNMDANC[k] = gN;
+			float gmA = Q.gmaxAMPAofMFtoNC[k];
+			gmA = gmA * N->gmaxAMPADecMFtoNC + in * wt * (1 - gmA);
+			Q.gmaxAMPAofMFtoNC[k] = gmA;
+			float gA = Q.gMFAMPANC[k];
+			gA = gA + N->gAMPAIncMFtoNC * (gmA - gA);
+			Q.gMFAMPANC[k] = gA;
+			sN[j] = gN;
+			sN[nMFNC + j] = gA;
 		}
-		N->inputGOGO[d] = cnt;
-		N->inputGOGABASynDepGO[d] = acc;
-		float vc = 0;
-		const int nc = N->numpGOCoupInGOGO[d];
-		for (int j = 0; j < nc; j++) {
-			const uint32_t n = N->pGOCoupInGOGO[(size_t)d * N->maxnumpGOCoupInGOGO + j];
-			vc = vc + N->coupleRiRjRatioGO * (N->vGO[n] - N->vGO[d]);
+		float gPCNCSum = 0;
+		for (uint32_t j0 = 0; j0 < N->numpNCfromPCtoNC; j0 += 32) {
+			const uint32_t j = j0 + lane;
+			float g = 0;
+			if (j < N->numpNCfromPCtoNC) {
+				const size_t k = (size_t)i * N->numpNCfromPCtoNC + j;
+				g = Q.gPCNC[k] * N->gDecPCtoNC + Q.inputPCNC[k] * Q.gPCScaleNC[k] * (1 - Q.gPCNC[k]);
+				Q.gPCNC[k] = g;
+			}
+			const uint32_t n = min(32u, N->numpNCfromPCtoNC - j0);
+			for (uint32_t q = 0; q < n; q++) gPCNCSum = gPCNCSum + __shfl_sync(0xffffffffu, g, q);
 		}
-		N->vCoupleGO[d] = vc;
-		N->threshSnap[d] = N->threshCurGO[d];
+		__syncwarp();
+		float partial = 0;
+		if (lane < 2) {
+			const float *src = sN + lane * nMFNC;
+			for (uint32_t j = 0; j < nMFNC; j++) partial = partial + src[j];
+		}
+		const float ampaSum = __shfl_sync(0xffffffffu, partial, 1);
+		if (lane == 0) {
+			float gMFNMDASum = partial, gMFAMPASum = ampaSum;
+			gMFNMDASum = gMFNMDASum * N->msPerTimeStep / ((float)nMFNC);
+			gMFAMPASum = gMFAMPASum * N->msPerTimeStep / ((float)nMFNC);
+			float vNC = Q.vNC[i];
+			gMFNMDASum = gMFNMDASum * vNC / (-80.0f);
+			gPCNCSum = gPCNCSum * N->msPerTimeStep / ((float)N->numpNCfromPCtoNC);
+			vNC = vNC + N->gLeakNC * (N->eLeakNC - vNC) - (gMFNMDASum + gMFAMPASum) * vNC + gPCNCSum * (N->ePCtoNC - vNC);
+			Q.vNC[i] = vNC;
+			float th = Q.threshNC[i] + N->threshDecNC * (N->threshRestNC - Q.threshNC[i]);
+			const uint8_t ap = vNC > th;
+			Q.apNC[i] = ap;
+			Q.apBufNC[i] = (Q.apBufNC[i] << 1) | (ap * 0x00000001u);
+			Q.threshNC[i] = ap * N->threshMaxNC + (!ap) * th;
+		}
 	}
 	__syncthreads();
-	for (uint32_t i = tid; i < numGO; i += nThr) {
-		const float s = N->goGABAOutSynScaleGOGO[i];
-		const uint8_t ap = N->apGO[i];
-		N->goGABAOutSynScaleGOGO[i] = s + (!ap) * (1 - s) * N->goGABAGOGOSynRec - ap * (s * (1 - N->goGABAGOGOSynDepF));
-	}
-	// threshold coupling: the reference's serial sweep reads already-updated
-	// thresholds of lower-indexed neighbours; the level schedule preserves it
-	for (uint32_t L = 0; L < N->numCoupLevels; L++) {
-		for (uint32_t e = N->coupLevelStart[L] + tid; e < N->coupLevelStart[L + 1]; e += nThr) {
-			const uint32_t i = N->coupLevelGO[e];
-			const float own = N->threshSnap[i];
-			float tc = 0;
-			const int nc = N->numpGOCoupInGOGO[i];
-			for (int j = 0; j < nc; j++) {
-				const uint32_t n = N->pGOCoupInGOGO[(size_t)i * N->maxnumpGOCoupInGOGO + j];
-				const float other = n < i ? N->threshCurGO[n] : N->threshSnap[n];
-				tc = tc + N->coupleRiRjRatioGO * (other - own);
-			}
-			N->threshCurGO[i] = own + tc;
-		}
-		__syncthreads();
-	}
-
-	// ---- microzone phase 2 (cbmsimcore.cpp:263-304)
-	// calcIOActivities (mzone.cpp:258-339) on the last warp, calcNCActivities
-	// (mzone.cpp:341-407) one warp per NC
-	const uint32_t nMFNC = N->numpNCfromMFtoNC;
-	if (warp == nWarps - 1) {
-		for (uint32_t task = lane; task < Z * numIO; task += 32) {
-			const uint32_t z = task / numIO, i = task % numIO;
-			const DevZone &Q = N->zones[z];
-			float gNCSum = 0;
-			for (uint32_t j = 0; j < N->numpIOfromNCtoIO; j++) {
-				const size_t k = (size_t)i * N->numpIOfromNCtoIO + j;
-				float g = Q.gNCIO[k];
-				g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO) + N->gDecT0ofNCtoIO));
-				g = g + Q.inputNCIO[k] * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO);
-				Q.gNCIO[k] = g;
-				gNCSum = gNCSum + g;
-				Q.inputNCIO[k] = 0;
-			}
-			gNCSum = gNCSum / 3.1;
-			float v = Q.vIO[i];
-			v = v + N->gLeakIO * (N->eLeakIO - v) + gNCSum * 1.5 * (N->eNCtoIO - v) + Q.vCoupleIO[i] + ctl->errDrive[z];
-			Q.vIO[i] = v;
-			const uint8_t ap = v > Q.threshIO[i];
-			Q.apIO[i] = ap;
-			Q.apBufIO[i] = (Q.apBufIO[i] << 1) | (ap * 0x00000001u);
-			Q.threshIO[i] = N->threshMaxIO * ap + (!ap) * (Q.threshIO[i] + N->threshDecIO * (N->threshRestIO - Q.threshIO[i]));
-		}
-	} else {
-		for (uint32_t task = warp; task < Z * numNC; task += nWarps - 1) {
-			const uint32_t z = task / numNC, i = task % numNC;
-			const DevZone &Q = N->zones[z];
-			float *sN = ncScratch + (size_t)warp * 2 * nMFNC;
-			for (uint32_t j = lane; j < nMFNC; j += 32) {
-				const size_t k = (size_t)i * nMFNC + j;
-				const float in = Q.inputMFNC[k], wt = Q.mfSynWeightNC[k];
-				float gmN = Q.gmaxNMDAofMFtoNC[k];
-				gmN = gmN * N->gmaxNMDADecMFtoNC + in * wt * (1 - gmN);
-				Q.gmaxNMDAofMFtoNC[k] = gmN;
-				float gN = Q.gMFNMDANC[k];
-				gN = gN + N->gNMDAIncMFtoNC * (gmN - gN);
-				Q.gMFNMDANC[k] = gN;
-				float gmA = Q.gmaxAMPAofMFtoNC[k];
-				gmA = gmA * N->gmaxAMPADecMFtoNC + in * wt * (1 - gmA);
-				Q.gmaxAMPAofMFtoNC[k] = gmA;
-				float gA = Q.gMFAMPANC[k];
-				gA = gA + N->gAMPAIncMFtoNC * (gmA - gA);
-				Q.gMFAMPANC[k] = gA;
-				sN[j] = gN;
-				sN[nMFNC + j] = gA;
-			}
-			__syncwarp();
-			float partial = 0;
-			if (lane < 2) {
-				const float *src = sN + lane * nMFNC;
-				for (uint32_t j = 0; j < nMFNC; j++) partial = partial + src[j];
-			}
-			const float ampaSum = __shfl_sync(0xffffffffu, partial, 1);
-			if (lane == 0) {
-				float gMFNMDASum = partial, gMFAMPASum = ampaSum;
-				gMFNMDASum = gMFNMDASum * N->msPerTimeStep / ((float)nMFNC);
-				gMFAMPASum = gMFAMPASum * N->msPerTimeStep / ((float)nMFNC);
-				float vNC = Q.vNC[i];
-				gMFNMDASum = gMFNMDASum * vNC / (-80.0f);
-				float gPCNCSum = 0;
-				for (uint32_t j = 0; j < N->numpNCfromPCtoNC; j++) {
-					const size_t k = (size_t)i * N->numpNCfromPCtoNC + j;
-					Q.gPCNC[k] = Q.gPCNC[k] * N->gDecPCtoNC + Q.inputPCNC[k] * Q.gPCScaleNC[k] * (1 - Q.gPCNC[k]);
-					gPCNCSum = gPCNCSum + Q.gPCNC[k];
-				}
-				gPCNCSum = gPCNCSum * N->msPerTimeStep / ((float)N->numpNCfromPCtoNC);
-				vNC = vNC + N->gLeakNC * (N->eLeakNC - vNC) - (gMFNMDASum + gMFAMPASum) * vNC + gPCNCSum * (N->ePCtoNC - vNC);
-				Q.vNC[i] = vNC;
-				float th = Q.threshNC[i] + N->threshDecNC * (N->threshRestNC - Q.threshNC[i]);
-				const uint8_t ap = vNC > th;
-				Q.apNC[i] = ap;
-				Q.apBufNC[i] = (Q.apBufNC[i] << 1) | (ap * 0x00000001u);
-				Q.threshNC[i] = ap * N->threshMaxNC + (!ap) * th;
-			}
-			__syncwarp();
-		}
+	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
+		const uint32_t z = task / numIO, i = task % numIO;
+		const DevZone &Q = N->zones[z];
+		float gNCSum = 0;
+		for (uint32_t j = 0; j < nIONC; j++) gNCSum = gNCSum + ioScratch[(size_t)task * nIONC + j];
+		gNCSum = gNCSum / 3.1;
+		float v = Q.vIO[i];
+		v = v + N->gLeakIO * (N->eLeakIO - v) + gNCSum * 1.5 * (N->eNCtoIO - v) + Q.vCoupleIO[i] + ctl->errDrive[z];
+		Q.vIO[i] = v;
+		const uint8_t ap = v > Q.threshIO[i];
+		Q.apIO[i] = ap;
+		Q.apBufIO[i] = (Q.apBufIO[i] << 1) | (ap * 0x00000001u);
+		Q.threshIO[i] = N->threshMaxIO * ap + (!ap) * (Q.threshIO[i] + N->threshDecIO * (N->threshRestIO - Q.threshIO[i]));
 	}
 	__syncthreads();
 
@@ -537,7 +584,7 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 	for (uint32_t task = tid; task < Z * numNC * nMFNC; task += nThr) {
 		const uint32_t z = task / (numNC * nMFNC), k = task % (numNC * nMFNC);
 		const uint32_t src = N->zones[z].pNCfromMFtoNC[k];
-		N->zones[z].inputMFNC[k] = mfRaw ? mfRaw[src] : (uint8_t)spikeBit(mfW, src);
+		N->zones[z].inputMFNC[k] = mfRaw ? mfRaw[src] : (uint8_t)spikeBit(sMF, src);
 	}
 	for (uint32_t task = tid; task < Z * numPC; task += nThr) {
 		const uint32_t z = task / numPC, i = task % numPC;
@@ -545,10 +592,11 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 		uint32_t c = 0;
 		for (uint32_t e = Q.bcpcStart[i]; e < Q.bcpcStart[i + 1]; e++) c += Q.apBC[Q.bcpcSrc[e]];
 		Q.inputBCPC[i] = c;
-		for (uint32_t j = 0; j < N->numpPCfromSCtoPC; j++) {
-			const size_t k = (size_t)i * N->numpPCfromSCtoPC + j;
-			Q.inputSCPC[k] = N->apSC[Q.pPCfromSCtoPC[k]];
-		}
+	}
+	for (uint32_t task = tid; task < Z * numPC * N->numpPCfromSCtoPC; task += nThr) {
+		const uint32_t per = numPC * N->numpPCfromSCtoPC;
+		const uint32_t z = task / per, k = task % per;
+		N->zones[z].inputSCPC[k] = sApSC[N->zones[z].pPCfromSCtoPC[k]];
 	}
 	for (uint32_t task = tid; task < Z * numBC; task += nThr) {
 		const uint32_t z = task / numBC, i = task % numBC;
@@ -597,26 +645,26 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 			if (avgAllAPPC <= N->synLTPPCPopActThreshMFtoNC && !s[3]) { doLTP = 1; s[3] = 1; }
 			else if (avgAllAPPC > N->synLTPPCPopActThreshMFtoNC) s[3] = 0;
 		}
-		sDoLTD[tid] = doLTD;
-		sDoLTP[tid] = doLTP;
+		sFlags[2 * tid] = doLTD;
+		sFlags[2 * tid + 1] = doLTP;
 	}
 	__syncthreads();
 
 	// NC->IO release draws (mzone.cpp:505-511), MF->NC plasticity
-	// (mzone.cpp:586-600), plasticity selector for the next step
-	for (uint32_t task = tid; task < Z * numIO * N->numpIOfromNCtoIO; task += nThr) {
-		const uint32_t per = numIO * N->numpIOfromNCtoIO;
+	// (mzone.cpp:586-600), plasticity selector of the next step
+	for (uint32_t task = tid; task < Z * numIO * nIONC; task += nThr) {
+		const uint32_t per = numIO * nIONC;
 		const uint32_t z = task / per, k = task % per;
-		const uint32_t i = k / N->numpIOfromNCtoIO, j = k % N->numpIOfromNCtoIO;
+		const uint32_t i = k / nIONC, j = k % nIONC;
 		const DevZone &Q = N->zones[z];
-		const double u = (double)rng::uniform24Keyed(Q.ncioKey, rng::ncioCounter(t, i, j, N->numpIOfromNCtoIO));
+		const double u = (double)rng::uniform24Keyed(Q.ncioKey, rng::ncioCounter(t, i, j, nIONC));
 		Q.inputNCIO[k] = (u < Q.synIOPReleaseNC[Q.pIOfromNCtoIO[k]]);
 	}
 	if (popStep) {
 		for (uint32_t task = tid; task < Z * numNC * nMFNC; task += nThr) {
 			const uint32_t z = task / (numNC * nMFNC), k = task % (numNC * nMFNC);
 			const DevZone &Q = N->zones[z];
-			const int doLTD = sDoLTD[z], doLTP = sDoLTP[z];
+			const int doLTD = sFlags[2 * z], doLTP = sFlags[2 * z + 1];
 			const float synWDelta = N->histMF[Q.pNCfromMFtoNC[k]] *
 				(doLTD * N->synLTDStepSizeMFtoNC + doLTP * N->synLTPStepSizeMFtoNC);
 			float w = Q.mfSynWeightNC[k];
@@ -638,10 +686,20 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 		Q.plastSel[((t + 1) & 1) * numIO + i] = sel;
 	}
 	__syncthreads();
-	// resetMFHist (innet.cpp:982-995) and the consumed error drive
 	if ((t % N->numTSinMFHist) == 0)
 		for (uint32_t i = tid; i < numMF; i += nThr) N->histMF[i] = 0;
 	if (tid < Z) ctl->errDrive[tid] = 0;
+}
+
+// Small-cell update of step t: block 2n is network n's Golgi role, block
+// 2n+1 its microzone role.  The two roles share no state.
+__global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, uint32_t stepOffset)
+{
+	const DevNet *__restrict__ N = nets[blockIdx.x >> 1];
+	const uint64_t t = *N->tBase + 1 + stepOffset;
+	extern __shared__ uint32_t tailSmem[];
+	if (blockIdx.x & 1) zoneRole(N, t, tailSmem);
+	else golgiRole(N, t, tailSmem);
 }
 
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps)

@@ -72,7 +72,13 @@ size_t Network::passSmemBytes() const
 
 size_t Network::tailSmemBytes() const
 {
-	return sizeof(float) * (size_t)(kTailThreads / 32) * 2 * h_.numpNCfromMFtoNC;
+	// Golgi role: MF bits, GO scales, potentials, thresholds, spikes
+	const size_t golgi = 4ull * h_.mfWords + 12ull * h_.numGO + h_.numGO;
+	// microzone role: MF bits, SC spikes, NC and IO scratch, plasticity flags
+	const size_t zone = 4ull * h_.mfWords + ((h_.numSC + 15) & ~15u) +
+		4ull * h_.numZones * h_.numNC * 2 * h_.numpNCfromMFtoNC + 4ull * h_.numZones * h_.numIO * h_.numpIOfromNCtoIO +
+		8ull * kMaxZones;
+	return std::max(golgi, zone);
 }
 
 double Network::bytesPerStepAlgorithmic() const
@@ -226,7 +232,6 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	h.apSC = upB("apSC"); h.apBufSC = upU("apBufSC"); h.gPFSC = upF("gPFSC"); h.threshSC = upF("threshSC");
 	h.vSC = upF("vSC");
 	h.sumGRInputGO = alloc<uint32_t>(c.numGO); h.sumInputGOGABASynDepGO = alloc<float>(c.numGO);
-	h.threshSnap = alloc<float>(c.numGO);
 
 	// MF->GO out-lists as stored; GO->GO in-lists per destination in the
 	// reference's (source, slot) iteration order (innet.cpp:937-950)
@@ -237,6 +242,17 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 		for (int j = 0; j < numMFGO[i]; j++) if (pMFGO[(size_t)i * c.maxnumpMFfromMFtoGO + j] >= c.numGO) return "MF->GO index out of range";
 	}
 	h.numpMFfromMFtoGO = upI("numpMFfromMFtoGO"); h.pMFfromMFtoGO = upU("pMFfromMFtoGO");
+	{
+		// destination-side MF lists: each (fibre, slot) synapse of
+		// pMFfromMFtoGO once under its GO
+		std::vector<std::vector<uint32_t>> in(c.numGO);
+		for (uint32_t i = 0; i < c.numMF; i++)
+			for (int j = 0; j < numMFGO[i]; j++) in[pMFGO[(size_t)i * c.maxnumpMFfromMFtoGO + j]].push_back(i);
+		std::vector<uint32_t> start(c.numGO + 1, 0), src;
+		for (uint32_t d = 0; d < c.numGO; d++) { start[d + 1] = start[d] + (uint32_t)in[d].size(); src.insert(src.end(), in[d].begin(), in[d].end()); }
+		h.mfgoStart = upload(start.data(), start.size());
+		h.mfgoSrc = upload(src.data(), src.size());
+	}
 	{
 		const int32_t *numOutGG = A("numpGOGABAOutGOGO")->as<int32_t>();
 		const uint32_t *pOutGG = A("pGOGABAOutGOGO")->as<uint32_t>();
@@ -597,8 +613,9 @@ Simulator::~Simulator()
 	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_}) if (b->ptr) cudaFree(b->ptr);
 	if (s0_) cudaStreamDestroy(s0_);
 	if (s1_) cudaStreamDestroy(s1_);
-	for (cudaEvent_t e : {fork_, join_, ev0_, ev1_}) if (e) cudaEventDestroy(e);
+	for (cudaEvent_t e : {fork_, join_, ev0_, ev1_, tev0_, tev1_}) if (e) cudaEventDestroy(e);
 	for (cudaEvent_t e : passEv_) cudaEventDestroy(e);
+	for (cudaEvent_t e : tailEv_) cudaEventDestroy(e);
 }
 
 std::string Simulator::create(const std::vector<State *> &states, const std::vector<std::vector<int>> &seeds,
@@ -612,6 +629,8 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 	CK(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "event");
 	CK(cudaEventCreate(&ev0_), "event");
 	CK(cudaEventCreate(&ev1_), "event");
+	CK(cudaEventCreate(&tev0_), "event");
+	CK(cudaEventCreate(&tev1_), "event");
 	std::vector<DevNet *> ptrs;
 	std::vector<uint64_t *> tb;
 	std::vector<uint32_t> offs;
@@ -665,8 +684,10 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 			(const uint32_t *)dBlockOffset_.ptr, (int)nets_.size(), k);
 	CK(cudaGetLastError(), "launching the GR pass");
 	if (instrument) CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
-	tailKernel<<<(unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>((const DevNet *const *)dNetPtrs_.ptr, k);
+	if (instrument) CK(cudaEventRecordWithFlags(tailEv_[2 * k], s1_, cudaEventRecordExternal), "tail timing");
+	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>((const DevNet *const *)dNetPtrs_.ptr, k);
 	CK(cudaGetLastError(), "launching the small-cell update");
+	if (instrument) CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
 	CK(cudaEventRecord(join_, s1_), "join");
 	CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
 	return "";
@@ -717,9 +738,11 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 	if (!graphExec_ || graphChunk_ != chunk || graphInstrumented_ != instrument) {
 		if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
 		while (instrument && passEv_.size() < 2 * (size_t)chunk) {
-			cudaEvent_t e;
+			cudaEvent_t e, f;
 			CK(cudaEventCreate(&e), "event");
+			CK(cudaEventCreate(&f), "event");
 			passEv_.push_back(e);
+			tailEv_.push_back(f);
 		}
 		cudaGraph_t g;
 		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
@@ -752,7 +775,28 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 			total += ms;
 		}
 		lastPassMs_ = total / chunk;
+		total = 0;
+		for (uint32_t k = 0; k < chunk; k++) {
+			float ms = 0;
+			CK(cudaEventElapsedTime(&ms, tailEv_[2 * k], tailEv_[2 * k + 1]), "tail timing");
+			total += ms;
+		}
+		lastTailMs_ = total / chunk;
 	}
+	return "";
+}
+
+std::string Simulator::timerStart()
+{
+	CK(cudaEventRecord(tev0_, s0_), "timer");
+	return "";
+}
+
+std::string Simulator::timerStop(float *ms)
+{
+	CK(cudaEventRecord(tev1_, s0_), "timer");
+	CK(cudaEventSynchronize(tev1_), "timer");
+	CK(cudaEventElapsedTime(ms, tev0_, tev1_), "timer");
 	return "";
 }
 

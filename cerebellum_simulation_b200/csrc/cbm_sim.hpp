@@ -55,6 +55,9 @@ public:
 	// Time of the last runGraph call measured with events on the launch stream.
 	float lastGraphMs() const { return lastGraphMs_; }
 	float lastPassMs() const { return lastPassMs_; }
+	float lastTailMs() const { return lastTailMs_; }
+	std::string timerStart();
+	std::string timerStop(float *ms);
 
 private:
 	friend class Network;
@@ -63,15 +66,15 @@ private:
 	std::vector<Network *> nets_;
 	int device_ = 0;
 	cudaStream_t s0_ = nullptr, s1_ = nullptr;
-	cudaEvent_t fork_ = nullptr, join_ = nullptr, ev0_ = nullptr, ev1_ = nullptr;
+	cudaEvent_t fork_ = nullptr, join_ = nullptr, ev0_ = nullptr, ev1_ = nullptr, tev0_ = nullptr, tev1_ = nullptr;
 	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_;
 	uint32_t passBlocks_ = 0;
 	size_t passSmem_ = 0, tailSmem_ = 0;
 	cudaGraphExec_t graphExec_ = nullptr;
 	uint32_t graphChunk_ = 0;
 	bool graphInstrumented_ = false;
-	std::vector<cudaEvent_t> passEv_;
-	float lastGraphMs_ = 0, lastPassMs_ = 0;
+	std::vector<cudaEvent_t> passEv_, tailEv_;
+	float lastGraphMs_ = 0, lastPassMs_ = 0, lastTailMs_ = 0;
 };
 
 class Network {

@@ -181,6 +181,16 @@ int cbm_sim_load_mf_stream(cbm_sim *sim, const uint32_t *bits, uint64_t nsteps);
  * over the last chunk. */
 int cbm_sim_run(cbm_sim *sim, uint64_t nsteps, uint32_t graphChunk, float *gpuMs, float *passMs);
 
+/* Device-timeline timer on the simulator's launch stream: events recorded
+ * at start and stop; *ms receives the time between them (host gaps
+ * included). */
+int cbm_sim_timer_start(cbm_sim *sim);
+int cbm_sim_timer_stop(cbm_sim *sim, float *ms);
+
+/* Mean duration of the small-cell update kernel over the last chunk of the
+ * last cbm_sim_run that timed the GR pass (0 before). */
+int cbm_sim_last_tail_ms(cbm_sim *sim, float *ms);
+
 /* Algorithmic HBM bytes of one step: (72 + 4 n_mf + 4 n_go + 8 n_out) per GR
  * with the network's mean synapse counts. */
 double cbm_sim_algorithmic_bytes_per_step(cbm_sim *sim);

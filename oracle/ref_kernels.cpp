@@ -12,7 +12,10 @@
  * i = tid, tid+2bs, ..., then reduces the bs partial sums with a halving tree
  * (strides bs/2 ... 1).  The last-warp part of that tree is written
  * warp-synchronously without __syncwarp; the intended lockstep semantics
- * (all loads of a statement before its stores) are what is restated here. */
+ * (all loads of a statement before its stores) are what is restated here.
+ *
+ * The OpenMP pragmas only take effect in the all-core timing build
+ * (oracle/_ref/ref_run_omp); every loop they split writes disjoint cells. */
 #include <cstring>
 #include <vector>
 #include <CBMCoreInclude/cuda/kernels.h>
@@ -32,8 +35,9 @@ void callGRActKernel(cudaStream_t &st, unsigned int numBlocks, unsigned int numG
 		float threshBase, float threshMax, float threshDecay)
 {
 	(void)st;
-	unsigned long n = (unsigned long)numBlocks * numGRPerBlock;
-	for (unsigned long i = 0; i < n; i++)
+	long n = (long)numBlocks * numGRPerBlock;
+#pragma omp parallel for schedule(static)
+	for (long i = 0; i < n; i++)
 	{
 		float tempV = vm[i];
 		float tempGKCa = gKCa[i];
@@ -92,7 +96,8 @@ void callSumKernel(cudaStream_t &st, Type *inGPU, size_t inGPUP, Type *outSumGPU
 	else if (numElementsPerBlock >= 128) bs = 32;
 	else if (numElementsPerBlock >= 32) bs = 8;
 	else bs = 2;
-	for (unsigned int by = 0; by < nOutCells; by++)
+#pragma omp parallel for schedule(static)
+	for (int by = 0; by < (int)nOutCells; by++)
 		for (unsigned int bx = 0; bx < nOutCols; bx++)
 			sumBlock<Type, inMultiP, outMultiP>(bs, bx, by, nOutCols, inGPU, inGPUP, outSumGPU, outSumGPUP, rowLength);
 }
@@ -113,11 +118,11 @@ void callUpdateGROutGOKernel(cudaStream_t &st, unsigned int numBlocks, unsigned 
 		ct_int32_t *numGOPerGRGPU)
 {
 	(void)st;
-	std::vector<ct_uint32_t> hist(numGO);
 	unsigned int nWrites = numGO / numGRPerBlock;
-	for (unsigned int b = 0; b < numBlocks; b++)
+#pragma omp parallel for schedule(static)
+	for (int b = 0; b < (int)numBlocks; b++)
 	{
-		std::fill(hist.begin(), hist.end(), 0u);
+		std::vector<ct_uint32_t> hist(numGO, 0u);
 		for (unsigned int tid = 0; tid < numGRPerBlock; tid++)
 		{
 			unsigned long index = (unsigned long)b * numGRPerBlock + tid;
@@ -159,8 +164,9 @@ void callUpdateInGROPKernel(cudaStream_t &st, unsigned int numBlocks, unsigned i
 	unsigned int inNLoads = numInCells / numGRPerBlock;
 	std::vector<ct_uint32_t> staged(inNLoads * numGRPerBlock);
 	for (unsigned int k = 0; k < staged.size(); k++) staged[k] = apInGPU[k];
-	unsigned long n = (unsigned long)numBlocks * numGRPerBlock;
-	for (unsigned long index = 0; index < n; index++)
+	long n = (long)numBlocks * numGRPerBlock;
+#pragma omp parallel for schedule(static)
+	for (long index = 0; index < n; index++)
 	{
 		int tempNSyn = numInPerGRGPU[index];
 		int tempApInSum = 0;
@@ -182,8 +188,9 @@ void callUpdatePFBCSCOutKernel(cudaStream_t &st, unsigned int numBlocks, unsigne
 	(void)st;
 	unsigned int numPFInPerBC = 1u << numPFInPerBCP2;
 	unsigned int numPFInPerSC = 1u << numPFInPerSCP2;
-	unsigned long n = (unsigned long)numBlocks * numGRPerBlock;
-	for (unsigned long index = 0; index < n; index++)
+	long n = (long)numBlocks * numGRPerBlock;
+#pragma omp parallel for schedule(static)
+	for (long index = 0; index < n; index++)
 	{
 		ct_uint32_t *pfBCRow = (ct_uint32_t *)((char *)inPFBCGPU + (index >> numPFInPerBCP2) * inPFBCGPUPitch);
 		ct_uint32_t *pfSCRow = (ct_uint32_t *)((char *)inPFSCGPU + (index >> numPFInPerSCP2) * inPFSCGPUPitch);
@@ -200,8 +207,9 @@ void callUpdatePFPCOutKernel(cudaStream_t &st, unsigned int numBlocks, unsigned 
 {
 	(void)st;
 	unsigned int numPFInPerPC = 1u << numPFInPerPCP2;
-	unsigned long n = (unsigned long)numBlocks * numGRPerBlock;
-	for (unsigned long index = 0; index < n; index++)
+	long n = (long)numBlocks * numGRPerBlock;
+#pragma omp parallel for schedule(static)
+	for (long index = 0; index < n; index++)
 	{
 		float *pfPCRow = (float *)((char *)inPFPCGPU + (index >> numPFInPerPCP2) * inPFPCGPUPitch);
 		unsigned int tempOut = (apBufGPU[index] & delayMaskGPU[index]) > 0;
@@ -214,8 +222,9 @@ void callUpdateGRHistKernel(cudaStream_t &st, unsigned int numBlocks, unsigned i
 		ct_uint32_t *apBufGPU, ct_uint64_t *historyGPU, ct_uint32_t apBufGRHistMask)
 {
 	(void)st; (void)apBufGRHistMask;
-	unsigned long n = (unsigned long)numBlocks * numGRPerBlock;
-	for (unsigned long i = 0; i < n; i++)
+	long n = (long)numBlocks * numGRPerBlock;
+#pragma omp parallel for schedule(static)
+	for (long i = 0; i < n; i++)
 	{
 		ct_uint64_t tempHist = historyGPU[i] << 1;
 		historyGPU[i] = tempHist | ((apBufGPU[i] & 0x0000001F) > 0) * 0x00000001;
@@ -228,10 +237,11 @@ void callUpdatePFPCPlasticityIOKernel(cudaStream_t &st, unsigned int numBlocks, 
 		int offSet, float pfPCPlastStep)
 {
 	(void)st; (void)pastBinNToCheck;
-	unsigned long n = (unsigned long)numBlocks * numGRPerBlock;
-	for (unsigned long k = 0; k < n; k++)
+	long n = (long)numBlocks * numGRPerBlock;
+#pragma omp parallel for schedule(static)
+	for (long k = 0; k < n; k++)
 	{
-		unsigned long i = k + (unsigned long)offSet;
+		unsigned long i = (unsigned long)k + (unsigned long)offSet;
 		synWeightGPU[i] = synWeightGPU[i] + ((historyGPU[i] & 0x0000008000000000ull) > 0) * pfPCPlastStep;
 		synWeightGPU[i] = (synWeightGPU[i] > 0) * synWeightGPU[i];
 		synWeightGPU[i] = (synWeightGPU[i] > 1) + (synWeightGPU[i] <= 1) * synWeightGPU[i];
