@@ -246,3 +246,17 @@ def load_json(name):
 # few float ulps.  No spike depends on them (innet.cpp:850-858).
 FP_TOLERANT_ARRAYS = {"gluGO", "mGluRGO", "gMGluRIncGO", "gMGluRGO"}
 FP_RTOL = 1e-5
+
+
+def build_facade_check(dest_dir):
+    """Compile tests/cpp/facade_check.cpp against include/cbm_core.hpp and
+    libcbm_b200.so; returns the executable's path."""
+    import subprocess
+    import cerebellum_simulation_b200 as cbm
+    libdir = os.path.dirname(cbm.LIB_PATH)
+    exe = os.path.join(dest_dir, "facade_check")
+    cmd = ["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "facade_check.cpp"), "-L", libdir, "-lcbm_b200",
+           f"-Wl,-rpath,{libdir}", "-o", exe]
+    subprocess.run(cmd, check=True, capture_output=True)
+    return exe

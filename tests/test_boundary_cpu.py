@@ -92,3 +92,13 @@ def test_mf_bits_packing():
     b = cbm.mf_bits(x, 33)
     assert b.shape == (2, 33)
     assert b[0, 0] == 1 and b[0, 1] == 2 and b[1, 31] == 1 << 31 and b[1, 32] == 0
+
+
+def test_cpp_facade_compiles_and_loads_a_reference_state(tmp_path):
+    """include/cbm_core.hpp keeps the reference's class names; a driver
+    written against them builds and loads a reference state file."""
+    import subprocess
+    exe = cbmtest.build_facade_check(str(tmp_path))
+    p = cbmtest.golden_state("ref16k", str(tmp_path))
+    out = subprocess.run([exe, p], check=True, capture_output=True, text=True).stdout
+    assert "zones 1" in out
