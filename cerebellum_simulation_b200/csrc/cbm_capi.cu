@@ -15,11 +15,12 @@ using namespace cbm;
 struct cbm_state { State st; };
 struct cbm_sim { Simulator sim; cbm_state *owner = nullptr; };
 
-static thread_local std::string g_lastError;
+// last error message of the calling thread (cbm_last_error)
+thread_local std::string g_cbmLastError;
 
 static int fail(int code, const std::string &msg)
 {
-	g_lastError = msg;
+	g_cbmLastError = msg;
 	return code;
 }
 
@@ -41,7 +42,7 @@ static int classify(const std::string &msg)
 
 extern "C" {
 
-const char *cbm_last_error(void) { return g_lastError.c_str(); }
+const char *cbm_last_error(void) { return g_cbmLastError.c_str(); }
 
 int cbm_state_load(const char *path, cbm_state **out)
 {

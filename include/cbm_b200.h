@@ -197,6 +197,27 @@ double cbm_sim_algorithmic_bytes_per_step(cbm_sim *sim);
 
 void cbm_sim_destroy(cbm_sim *sim);
 
+/* PF->PC input sums without device allocation.  No counterpart in the
+ * reference; it is for callers that cannot let a library allocate device
+ * memory while they call it (a framework that owns every allocation through
+ * its own pool, code running while a stream is captured into a CUDA graph in
+ * the global capture mode, a real-time loop that cannot absorb allocation
+ * latency).  From buffers on the current device it computes, for each of
+ * numPC rows of numGR/numPC parallel fibres, the sum of
+ * weights[i] * ((apBuf[i] & pfDelayMask[i]) != 0) in the reference's
+ * order (updatePFPCOutGPU then sumInputsNew) into sums[numPC], on `stream`
+ * (a cudaStream_t, NULL for the default stream).
+ * Scratch is one file-scope device array of CBM_NOALLOC_MAX_PARTIALS floats
+ * that every device loading the library keeps until exit: numPC times the
+ * reduction width (512 for rows of 2048 fibres or more) must fit in it, or
+ * the call fails with CBM_ERR_ARG.  All calls on a device share the array;
+ * each call rewrites the part it reads, so no clearing is needed, but calls
+ * that overlap on the GPU race.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
+#define CBM_NOALLOC_MAX_PARTIALS 65536
+int cbm_pfpc_sums_noalloc(const uint32_t *apBuf, const uint32_t *pfDelayMask, const float *weights,
+		uint32_t numGR, uint32_t numPC, float *sums, void *stream);
+
 /* Device evaluation of the float exponential the small-cell updates use
  * (the published expf algorithm glibc ships), for checking it against the
  * host's expf: out[i] = exp(in[i]) for n values in host memory. */
