@@ -11,11 +11,69 @@
 // mzoneactivitystate.h).
 #pragma once
 #include <cstdint>
+#include <cuda.h>
+
+#if defined(__CUDACC__)
+#define CBM_LAYOUT_FN __host__ __device__ inline
+#else
+#define CBM_LAYOUT_FN inline
+#endif
 
 namespace cbm {
 
 constexpr int kMaxZones = 4;
 constexpr uint32_t kNoDelay = 0xFFu;
+
+// Bits of DevNet::errFlag.
+constexpr uint32_t kErrPassWait = 1u;  // a GR-pass pipeline wait timed out
+
+// TMA descriptors of the GR arrays the GR pass streams, each viewed as rows
+// of bs cells ([numGR/bs][bs], slot tables as [slot][numGR/bs][bs]) and
+// copied in boxes of 32 cells x R rows (x all slots).
+enum PassMap : int {
+	PM_V = 0, PM_GKCA, PM_THRESH, PM_GESUM, PM_GISUM, PM_APBUF,  // 4-byte state, read and rewritten
+	PM_MFIDX, PM_GOIDX, PM_OUTCON, PM_PFDELAY, PM_HIST, PM_W0,
+	PM_COUNT = PM_W0 + kMaxZones
+};
+
+// A device array that a small-cell CTA copies into shared memory for the
+// step (and back when it changes): the CTA then runs on a shared-memory copy
+// of the network descriptor whose pointer at fieldOff points into the copy.
+struct StageSeg {
+	uint32_t fieldOff;   // byte offset of the array's pointer within DevNet
+	uint32_t bytes;      // array size, a multiple of 16
+	uint32_t smemOff;    // offset in the staging arena (16-byte aligned)
+	uint32_t writeBack;  // copied back to global memory after the step
+};
+
+// Shared-memory layout of one pipeline stage of the GR pass (R rows of 32
+// cells); every region starts on a 128-byte boundary.
+struct PassLayout {
+	uint32_t mfIdx, goIdx, outCon, pfDelay, w, hist;  // region offsets (the six state arrays start at 0)
+	uint32_t bytes;    // stage size
+	uint32_t txBase;   // bytes the stage's copies deliver, history excluded
+	uint32_t txHist;   // bytes of the history box (plasticity steps only)
+};
+
+CBM_LAYOUT_FN uint32_t align128(uint32_t x) { return (x + 127u) & ~127u; }
+
+CBM_LAYOUT_FN PassLayout passLayout(uint32_t R, uint32_t nMF, uint32_t nGO, uint32_t nOut, uint32_t Z)
+{
+	const uint32_t mfS = nMF ? nMF : 1, goS = nGO ? nGO : 1, outS = nOut ? nOut : 1;
+	const uint32_t row4 = 128u * R;  // one 4-byte array: R rows x 32 cells
+	PassLayout L;
+	uint32_t o = 6 * row4;
+	L.mfIdx = o; o = align128(o + 64u * R * mfS);
+	L.goIdx = o; o = align128(o + 64u * R * goS);
+	L.outCon = o; o = align128(o + row4 * outS);
+	L.pfDelay = o; o = align128(o + 32u * R);
+	L.w = o; o = align128(o + row4 * Z);
+	L.hist = o; o = align128(o + 256u * R);
+	L.bytes = o;
+	L.txBase = 6 * row4 + 64u * R * mfS + 64u * R * goS + row4 * outS + 32u * R + row4 * Z;
+	L.txHist = 256u * R;
+	return L;
+}
 
 // Values the host may change between steps (setter calls of the reference's
 // API): read by the kernels of the next step.
@@ -108,7 +166,6 @@ struct DevNet {
 	// ---- input-net connectivity used by the small-cell updates
 	const int32_t *numpMFfromMFtoGO; const uint32_t *pMFfromMFtoGO;
 	const uint32_t *gogoStart, *gogoSrc;  // per GO: sources of GO->GO synapses in (source, slot) order
-	const uint32_t *mfgoStart, *mfgoSrc;  // per GO: MF sources (with repeats) of updateMFtoGOOut
 	const int32_t *numpGOCoupInGOGO; const uint32_t *pGOCoupInGOGO;
 	const uint32_t *coupLevelStart, *coupLevelGO;  // coupling sweep schedule
 
@@ -121,7 +178,11 @@ struct DevNet {
 	const uint8_t *mfRaw;    // [mfRing][numMF] raw MF input bytes (NC inputs), or null
 	uint64_t *tBase;     // steps completed
 	HostCtl *ctl;
-	uint32_t *errFlag;   // device error word (bounds violations found by checks)
+	uint32_t *errFlag;   // device error word (kErr* bits)
+	const CUtensorMap *passMaps;  // [PM_COUNT] descriptors of the TMA GR pass, or null
+	const StageSeg *zoneSegs;     // arrays the microzone CTA stages in shared memory
+	uint32_t numZoneSegs;         // 0: the microzone CTA works on global memory
+	uint32_t zoneArenaBytes;
 
 	DevZone zones[kMaxZones];
 };

@@ -35,6 +35,7 @@
 #include "cbm_device.cuh"
 #include "cbm_kernels.cuh"
 #include "cbm_rng.hpp"
+#include "cbm_tma.cuh"
 
 namespace cbm {
 
@@ -239,6 +240,277 @@ __global__ void __launch_bounds__(kPassThreads) grPassKernel(const DevNet *const
 	}
 }
 
+// ------------------------------------------------------------ GR pass, TMA
+// The same tile and per-cell work as grPassKernel for networks whose
+// reduction width bs is at least 32 (tiles of 32-cell rows), with the tile's
+// input rows streamed by TMA: one producer warp copies R = W*RW rows x 32
+// cells of every GR array per stage into an S-deep ring of shared-memory
+// stages; each of the W consumer warps updates RW rows of a stage, reading
+// its inputs from shared memory and writing the new state straight to global
+// memory.  Waits are bounded (kPassWaitLimitNs); a time-out sets
+// kErrPassWait in the network's error word, which the host reports.
+constexpr uint64_t kPassWaitLimitNs = 2000000000ull;
+
+// Slot loops: MS > 0 compiles them for at most MS synapse slots per cell
+// (predicated, fully unrolled); MS == 0 keeps runtime trip counts.
+template <int MS>
+__device__ __forceinline__ int countSpikes(const uint8_t *spikes, const uint16_t *idx, uint32_t n, uint32_t stride)
+{
+	int c = 0;
+	if constexpr (MS > 0) {
+#pragma unroll
+		for (uint32_t s = 0; s < (uint32_t)MS; s++)
+			if (s < n) c += spikes[idx[s * stride]];
+	} else {
+#pragma unroll 4
+		for (uint32_t s = 0; s < n; s++) c += spikes[idx[s * stride]];
+	}
+	return c;
+}
+
+template <int W, int RW, int S, int MINB, int MS>
+__global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevNet *const *nets,
+		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
+{
+	constexpr uint32_t R = W * RW;
+	uint32_t local;
+	const DevNet *__restrict__ N = locateNet(nets, blockOffset, numNets, blockIdx.x, local);
+	const uint64_t t = *N->tBase + 1 + stepOffset;
+
+	const uint32_t P = N->P, bs = N->bs, K = N->K, Z = N->numZones;
+	const uint32_t pc = local / N->tilesPerPC;
+	const uint32_t j0 = (local % N->tilesPerPC) * 32u;
+	const uint32_t rows = 2 * K, nStages = rows / R;
+	const uint32_t nMFSlots = N->nMFSlots, nGOSlots = N->nGOSlots, nOutSlots = N->nOutSlots;
+	const PassLayout L = passLayout(R, nMFSlots, nGOSlots, nOutSlots, Z);
+
+	extern __shared__ uint8_t passSmemRaw[];
+	uint8_t *stages = passSmemRaw + ((128u - (tma::smemAddr(passSmemRaw) & 127u)) & 127u);
+	uint64_t *full = reinterpret_cast<uint64_t *>(stages + (size_t)S * L.bytes);
+	uint64_t *empty = full + S;
+	// spikes of this step's MF and last step's GO as one byte per cell (the
+	// sentinel index numMF / numGO reads 0)
+	uint32_t *sBC = reinterpret_cast<uint32_t *>(empty + S);
+	uint32_t *sSC = sBC + N->bcLocal;
+	float *sX = reinterpret_cast<float *>(sSC + N->scLocal);
+	uint8_t *sMF = reinterpret_cast<uint8_t *>(sX + (size_t)Z * rows * 32u);
+	uint8_t *sGO = sMF + 32u * N->mfWords;
+
+	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < S; s++) {
+			tma::mbarInit(&full[s], 1);
+			tma::mbarInit(&empty[s], W);
+		}
+		tma::fenceBarrierInit();
+	}
+	const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
+	for (uint32_t i = threadIdx.x; i < 32u * N->mfWords; i += blockDim.x) sMF[i] = (uint8_t)spikeBit(mfSrc, i);
+	for (uint32_t i = threadIdx.x; i < 32u * N->goWords; i += blockDim.x) sGO[i] = (uint8_t)spikeBit(goSrc, i);
+	for (uint32_t i = threadIdx.x; i < N->bcLocal + N->scLocal; i += blockDim.x) sBC[i] = 0;
+	__syncthreads();
+
+	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
+	const uint32_t rowBase = pc * rows;  // first row of the tile in the [numGR/bs][bs] view
+	const uint32_t bcBase = (pc * P) >> N->bcShift, scBase = (pc * P) >> N->scShift;
+
+	if (warp == W) {
+		// ---- producer
+		if (lane == 0) {
+			const CUtensorMap *maps = N->passMaps;
+			for (int m = 0; m < PM_W0 + (int)Z; m++) tma::prefetchMap(&maps[m]);
+			const uint32_t tx = L.txBase + (plastStep ? L.txHist : 0u);
+			uint32_t issued = 0, slot = 0, phase = 0;
+			bool ok = true;
+			for (uint32_t st = 0; st < nStages; st++) {
+				// refill number st/S of this slot waits until its previous contents are consumed
+				if (st >= (uint32_t)S && !tma::waitBounded(&empty[slot], phase ^ 1u, kPassWaitLimitNs)) { ok = false; break; }
+				uint8_t *b = stages + (size_t)slot * L.bytes;
+				uint64_t *bar = &full[slot];
+				tma::arriveExpectTx(bar, tx);
+				const int32_t x = (int32_t)j0, y = (int32_t)(rowBase + st * R);
+#pragma unroll
+				for (int m = PM_V; m <= PM_APBUF; m++) tma::load2d(b + (uint32_t)m * 128u * R, &maps[m], x, y, bar);
+				tma::load3d(b + L.mfIdx, &maps[PM_MFIDX], x, y, 0, bar);
+				tma::load3d(b + L.goIdx, &maps[PM_GOIDX], x, y, 0, bar);
+				tma::load3d(b + L.outCon, &maps[PM_OUTCON], x, y, 0, bar);
+				tma::load2d(b + L.pfDelay, &maps[PM_PFDELAY], x, y, bar);
+				for (uint32_t z = 0; z < Z; z++) tma::load2d(b + L.w + z * 128u * R, &maps[PM_W0 + z], x, y, bar);
+				if (plastStep) tma::load2d(b + L.hist, &maps[PM_HIST], x, y, bar);
+				issued = st + 1;
+				if (++slot == (uint32_t)S) { slot = 0; phase ^= 1u; }
+			}
+			if (!ok) {
+				atomicOr(N->errFlag, kErrPassWait);
+				// let the copies in flight land before the CTA's shared memory is released
+				for (uint32_t st = issued > (uint32_t)S ? issued - S : 0; st < issued; st++)
+					tma::waitBounded(&full[st % S], (st / S) & 1u, kPassWaitLimitNs);
+			}
+		}
+	} else {
+		// ---- consumers: warp w updates rows w, w+W, ..., w+(RW-1)W of every stage
+		float stepW[kMaxZones];
+#pragma unroll
+		for (uint32_t z = 0; z < kMaxZones; z++) {
+			stepW[z] = 0.0f;
+			if (z < Z && plastStep) {
+				const uint8_t sel = N->zones[z].plastSel[(t & 1) * N->numIO + N->zones[z].ioOfPC[pc]];
+				stepW[z] = sel == 1 ? N->ctl->ltdStep[z] : (sel == 2 ? N->ctl->ltpStep[z] : 0.0f);
+			}
+		}
+		const float gLeak = N->gLeakGR, eLeak = N->eLeakGR, eGOIn = N->eGOGR;
+		const float threshBase = N->threshRestGR, threshMax = N->threshMaxGR, threshDecay = N->threshDecGR;
+		const float gDecMF = N->gDecMFtoGR, gIncMF = N->gIncMFtoGR, gDecGO = N->gDecGOtoGR, gIncGO = N->gIncGOtoGR;
+		uint32_t *goCount = N->goCount + (size_t)(t & 1) * N->numGO;
+		const bool bcWarpUniform = (1u << N->bcShift) >= 32u, scWarpUniform = (1u << N->scShift) >= 32u;
+		float *const vGR = N->vGR, *const gKCaGR = N->gKCaGR, *const threshGR = N->threshGR;
+		float *const gESum = N->gESum, *const gISum = N->gISum;
+		uint32_t *const apBufGR = N->apBufGR;
+		uint64_t *const historyGR = N->historyGR;
+		const uint32_t bcShift = N->bcShift, scShift = N->scShift;
+		const uint32_t gTile = pc * P + j0 + lane;  // this lane's cell in row 0 of the tile
+		uint32_t slot = 0, phase = 0;
+
+		for (uint32_t st = 0; st < nStages; st++) {
+			const bool ready = tma::waitBounded(&full[slot], phase, kPassWaitLimitNs);
+			if (!__all_sync(0xffffffffu, ready)) {
+				if (lane == 0) atomicOr(N->errFlag, kErrPassWait);
+				break;
+			}
+			const uint8_t *b = stages + (size_t)slot * L.bytes;
+			uint32_t pfs[RW];
+#pragma unroll
+			for (int q = 0; q < RW; q++) {
+				const uint32_t rr = warp + q * W;          // row within the stage
+				const uint32_t e = rr * 32u + lane;        // element within a region of R x 32
+				const uint32_t r = st * R + rr;            // row within the tile
+				const uint32_t g = gTile + r * bs;
+				const float *sF = reinterpret_cast<const float *>(b);
+				const float v = sF[0 * 32 * R + e];
+				const float gk = sF[1 * 32 * R + e];
+				const float th = sF[2 * 32 * R + e];
+				const float gE = sF[3 * 32 * R + e];
+				const float gI = sF[4 * 32 * R + e];
+				const uint32_t ab = reinterpret_cast<const uint32_t *>(b)[5 * 32 * R + e];
+				const uint16_t *mfI = reinterpret_cast<const uint16_t *>(b + L.mfIdx) + e;
+				const uint16_t *goI = reinterpret_cast<const uint16_t *>(b + L.goIdx) + e;
+				const uint32_t *outC = reinterpret_cast<const uint32_t *>(b + L.outCon) + e;
+				const uint32_t d = (b + L.pfDelay)[e];
+				const uint64_t h = plastStep ? reinterpret_cast<const uint64_t *>(b + L.hist)[e] : 0ull;
+				const int cntMF = countSpikes<MS>(sMF, mfI, nMFSlots, 32 * R);
+				const int cntGO = countSpikes<MS>(sGO, goI, nGOSlots, 32 * R);
+
+				// calcActivityGRGPU (kernels.cu:79-110)
+				const float tempV = v + (gLeak + gk * gk * gk * gk) * (eLeak - v) - (gE) * v + (gI) * (eGOIn - v);
+				const float tempThresh = th + (threshBase - th) * threshDecay;
+				const unsigned int tempAP = tempV > tempThresh;
+				const float thN = tempAP * threshMax + (!tempAP) * tempThresh;
+				const float gkd = gk * 0.9999f;
+				const float gkN = tempAP * (gkd + 0.003f) + (!tempAP) * gkd;
+				const uint32_t abN = (ab << 1) | tempAP;
+				// updateGRInOPGPU for MF (this step's spikes) and GO (last step's)
+				const float gEN = gE * gDecMF + gIncMF * (cntMF);
+				const float gIN = gI * gDecGO + gIncGO * (cntGO);
+				vGR[g] = tempV;
+				gKCaGR[g] = gkN;
+				threshGR[g] = thN;
+				gESum[g] = gEN;
+				gISum[g] = gIN;
+				apBufGR[g] = abN;
+				// plasticity (phase 1) before this step's PF->PC output (phase 2)
+				const uint32_t pf = d < 32u ? (abN >> d) & 1u : 0u;
+#pragma unroll
+				for (uint32_t z = 0; z < kMaxZones; z++) {
+					if (z >= Z) break;
+					float w = reinterpret_cast<const float *>(b + L.w)[z * 32 * R + e];
+					if (plastStep) {
+						w = w + ((h & 0x0000008000000000ull) > 0) * stepW[z];
+						w = (w > 0) * w;
+						w = (w > 1) + (w <= 1) * w;
+						N->zones[z].w[g] = w;
+					}
+					sX[((size_t)z * rows + r) * 32u + lane] = w * pf;
+				}
+				if (plastStep) historyGR[g] = (h << 1) | ((abN & 0x0000001Fu) > 0);
+				// GR->GO synapses whose delayed spike arrives now
+				if (abN) {
+					if constexpr (MS > 0) {
+#pragma unroll
+						for (uint32_t s = 0; s < (uint32_t)MS; s++) {
+							if (s >= nOutSlots) break;
+							const uint32_t c = outC[s * 32 * R];
+							const uint32_t dl = c & 0xFFu;
+							if (dl < 32u && ((abN >> dl) & 1u)) atomicAdd(&goCount[c >> 8], 1u);
+						}
+					} else {
+#pragma unroll 4
+						for (uint32_t s = 0; s < nOutSlots; s++) {
+							const uint32_t c = outC[s * 32 * R];
+							const uint32_t dl = c & 0xFFu;
+							if (dl < 32u && ((abN >> dl) & 1u)) atomicAdd(&goCount[c >> 8], 1u);
+						}
+					}
+				}
+				pfs[q] = pf;
+			}
+			__syncwarp();
+			if (lane == 0) tma::arrive(&empty[slot]);
+			if (++slot == (uint32_t)S) { slot = 0; phase ^= 1u; }
+#pragma unroll
+			for (int q = 0; q < RW; q++) {
+				const uint32_t pf = pfs[q];
+				const uint32_t g = gTile + (st * R + warp + q * W) * bs;
+				if (!bcWarpUniform) atomicAdd(&sBC[(g >> bcShift) - bcBase], pf);
+				if (!scWarpUniform) atomicAdd(&sSC[(g >> scShift) - scBase], pf);
+				const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, pf != 0));
+				if (lane == 0 && cnt) {
+					const uint32_t base = g - lane;
+					if (bcWarpUniform) atomicAdd(&sBC[(base >> bcShift) - bcBase], cnt);
+					if (scWarpUniform) atomicAdd(&sSC[(base >> scShift) - scBase], cnt);
+				}
+			}
+		}
+	}
+	__syncthreads();
+
+	// sumInputsNew's per-thread running sums: tempSum += x[i] + x[i+bs]
+	const uint32_t buf = (uint32_t)(t % 3);
+	for (uint32_t task = threadIdx.x; task < Z * 32u; task += blockDim.x) {
+		const uint32_t z = task / 32u, jj = task % 32u;
+		const float *xs = sX + (size_t)z * rows * 32u + jj;
+		float s = 0;
+		for (uint32_t kk = 0; kk < K; kk++) s += xs[(2 * kk) * 32u] + xs[(2 * kk + 1) * 32u];
+		N->zones[z].pcPartial[((size_t)buf * N->numPC + pc) * bs + j0 + jj] = s;
+	}
+	uint32_t *bcOut = N->bcCount + (size_t)buf * N->numBC;
+	uint32_t *scOut = N->scCount + (size_t)buf * N->numSC;
+	for (uint32_t i = threadIdx.x; i < N->bcLocal + N->scLocal; i += blockDim.x) {
+		const uint32_t c = sBC[i];
+		if (!c) continue;
+		if (i < N->bcLocal) atomicAdd(&bcOut[bcBase + i], c);
+		else atomicAdd(&scOut[scBase + i - N->bcLocal], c);
+	}
+}
+
+// Geometries the host can pick: (consumer warps, rows per warp, stages,
+// minimum resident CTAs per SM, slot bound MS).
+#define CBM_PASS_TMA_CONFIGS(X) \
+	X(8, 1, 3, 2, 4) X(8, 1, 3, 3, 4) X(8, 1, 4, 2, 4) X(8, 1, 2, 3, 4) X(4, 1, 4, 4, 4) X(4, 2, 3, 3, 4) X(4, 2, 4, 2, 4) \
+	X(8, 1, 3, 2, 0) X(4, 1, 4, 1, 0) X(2, 1, 4, 1, 0) X(1, 1, 4, 1, 0)
+#define CBM_PASS_TMA_INST(W, RW, S, B, M) \
+	template __global__ void grPassTmaKernel<W, RW, S, B, M>(const DevNet *const *, const uint32_t *, int, uint32_t);
+CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_INST)
+
+const void *passTmaKernelFor(int W, int RW, int S, int B, int M)
+{
+#define CBM_PASS_TMA_PICK(w, rw, s, b, m) \
+	if (W == w && RW == rw && S == s && B == b && M == m) return (const void *)&grPassTmaKernel<w, rw, s, b, m>;
+	CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_PICK)
+#undef CBM_PASS_TMA_PICK
+	return nullptr;
+}
+
 // ------------------------------------------------------------------- tail
 // Every small-cell update of step t for one network (one CTA per network).
 // Statement forms follow the reference line by line so that each float and
@@ -256,20 +528,29 @@ __device__ __forceinline__ float sumTree32(float v)
 
 // Reduction of one PC's bs partial sums with the halving tree of
 // sumInputsNew (kernels.cu:326-362): strides bs/2, bs/4, ..., 1.
+template <int PER> __device__ __forceinline__ float pcRowTreeWide(const float *part, uint32_t lane)
+{
+	// lane l holds partials l, l+32, ..., l+32(PER-1); strides >= 32 combine
+	// registers of the same lane
+	float v[PER];
+#pragma unroll
+	for (int m = 0; m < PER; m++) v[m] = part[lane + 32 * m];
+#pragma unroll
+	for (int h = PER / 2; h >= 1; h /= 2)
+#pragma unroll
+		for (int m = 0; m < h; m++) v[m] = v[m] + v[m + h];
+	return sumTree32(v[0]);
+}
+
 __device__ float pcRowTree(const float *part, uint32_t bs, uint32_t lane)
 {
-	float v[16];
-	const uint32_t per = bs >= 32 ? bs / 32 : 1;
-	for (uint32_t m = 0; m < 16; m++) v[m] = 0.0f;
-	for (uint32_t m = 0; m < per; m++) {
-		const uint32_t idx = lane + 32 * m;
-		v[m] = idx < bs ? part[idx] : 0.0f;
+	switch (bs) {
+	case 512: return pcRowTreeWide<16>(part, lane);
+	case 128: return pcRowTreeWide<4>(part, lane);
+	case 32: return pcRowTreeWide<1>(part, lane);
+	default: break;
 	}
-	// strides >= 32 combine registers of the same lane
-	for (uint32_t h = per / 2; h >= 1; h /= 2)
-		for (uint32_t m = 0; m < h; m++) v[m] = v[m] + v[m + h];
-	float x = v[0];
-	if (bs >= 32) return sumTree32(x);
+	float x = lane < bs ? part[lane] : 0.0f;
 	for (uint32_t h = bs / 2; h >= 1; h /= 2) x = x + __shfl_down_sync(0xffffffffu, x, h);
 	return x;
 }
@@ -293,11 +574,13 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 	const uint32_t G = (uint32_t)((t - 1) & 1);
 	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
 	uint32_t *sMF = sm;
-	float *sScale = reinterpret_cast<float *>(sMF + N->mfWords);
+	uint32_t *sMFGO = sMF + N->mfWords;  // MF->GO input counts of this step
+	float *sScale = reinterpret_cast<float *>(sMFGO + numGO);
 	float *sV = sScale + numGO;
 	float *sTh = sV + numGO;
 	uint8_t *sAp = reinterpret_cast<uint8_t *>(sTh + numGO);
 	for (uint32_t i = tid; i < N->mfWords; i += nThr) sMF[i] = mfW[i];
+	for (uint32_t i = tid; i < numGO; i += nThr) sMFGO[i] = 0;
 	__syncthreads();
 
 	uint32_t *goIn = N->goCount + (size_t)G * numGO;
@@ -307,50 +590,66 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 		const uint32_t i = base + tid;
 		uint8_t ap = 0;
 		if (i < numGO) {
+			// every load of the update first, so that they are in flight
+			// together (the compiler cannot reorder them past the stores)
 			const unsigned int totalGRIn = goIn[i];
-			goIn[i] = 0;
 			const uint32_t inMF = N->inputMFGO[i];
 			const float inDep = N->inputGOGABASynDepGO[i];
+			const float gMF0 = N->gMFGO[i], gGR0 = N->gGRGO[i], gGO0 = N->gGOGO[i];
+			const float glu0 = N->gluGO[i], mg0 = N->mGluRGO[i], mgi0 = N->gMGluRIncGO[i], gMGluR0 = N->gMGluRGO[i];
+			const float thCur = N->threshCurGO[i], v0 = N->vGO[i], vCouple = N->vCoupleGO[i];
+			const uint32_t apBuf = N->apBufGO[i];
+			const float scale = N->goGABAOutSynScaleGOGO[i];
+
+			goIn[i] = 0;
 			N->sumGRInputGO[i] = totalGRIn;
 			N->sumInputGOGABASynDepGO[i] = inDep;
-			const float gMF = inMF * N->gIncMFtoGO + N->gMFGO[i] * N->gDecMFtoGO;
-			const float gGR = totalGRIn * gIncGRtoGO + N->gGRGO[i] * N->gDecGRtoGO;
-			const float gGO = inDep * N->gGABAIncGOtoGO + N->gGOGO[i] * N->gGABADecGOtoGO;
+			const float gMF = inMF * N->gIncMFtoGO + gMF0 * N->gDecMFtoGO;
+			const float gGR = totalGRIn * gIncGRtoGO + gGR0 * N->gDecGRtoGO;
+			const float gGO = inDep * N->gGABAIncGOtoGO + gGO0 * N->gGABADecGOtoGO;
 			N->gMFGO[i] = gMF; N->gGRGO[i] = gGR; N->gGOGO[i] = gGO;
-			float glu = N->gluGO[i];
+			float glu = glu0;
 			glu = glu * N->gluDecayGO + totalGRIn * N->gluScaleGO * exp(-1.5 * glu);
-			float mg = N->mGluRGO[i];
+			float mg = mg0;
 			mg = mg * N->mGluRDecayGO + glu * N->mGluRScaleGO * cbmExpf(-mg);
-			float mgi = N->gMGluRIncGO[i];
+			float mgi = mgi0;
 			mgi = mgi * N->gMGluRIncDecayGO + mg * N->gMGluRIncScaleGO * cbmExpf(-mgi);
 			N->gluGO[i] = glu; N->mGluRGO[i] = mg; N->gMGluRIncGO[i] = mgi;
-			N->gMGluRGO[i] = N->gMGluRGO[i] * N->gMGluRDecGRtoGO + mgi * N->gMGluRScaleGRtoGO;
-			float th = N->threshCurGO[i] + (N->threshRestGO - N->threshCurGO[i]) * N->threshDecGO;
-			float v = N->vGO[i];
-			v = v + (N->gLeakGO * (N->eLeakGO - v)) + (gGO * (N->eGABAGO - v)) - (gMF + gGR) * v + N->vCoupleGO[i];
+			N->gMGluRGO[i] = gMGluR0 * N->gMGluRDecGRtoGO + mgi * N->gMGluRScaleGRtoGO;
+			float th = thCur + (N->threshRestGO - thCur) * N->threshDecGO;
+			float v = v0;
+			v = v + (N->gLeakGO * (N->eLeakGO - v)) + (gGO * (N->eGABAGO - v)) - (gMF + gGR) * v + vCouple;
 			N->vGO[i] = v;
 			ap = v > th;
 			N->apGO[i] = ap;
-			N->apBufGO[i] = (N->apBufGO[i] << 1) | (ap * 0x00000001u);
+			N->apBufGO[i] = (apBuf << 1) | (ap * 0x00000001u);
 			th = ap * N->threshMaxGO + (!ap) * th;
 			N->threshCurGO[i] = th;
-			sScale[i] = N->goGABAOutSynScaleGOGO[i];
+			sScale[i] = scale;
 			sV[i] = v; sTh[i] = th; sAp[i] = ap;
-			// updateMFtoGOOut for this step's MF spikes, gathered per GO
-			uint32_t cnt = 0;
-			for (uint32_t e = N->mfgoStart[i]; e < N->mfgoStart[i + 1]; e++) cnt += spikeBit(sMF, N->mfgoSrc[e]);
-			N->inputMFGO[i] = cnt;
 		}
 		const uint32_t word = __ballot_sync(0xffffffffu, ap != 0);
 		if (lane == 0 && i < numGO) goBitsOut[i >> 5] = word;
 	}
 	__syncthreads();
+	// updateMFtoGOOut (innet.cpp:912-931): every spiking MF adds one to each
+	// GO it targets (integer counts: the order of the additions is immaterial)
+	for (uint32_t i = tid; i < N->numMF; i += nThr) {
+		if (!spikeBit(sMF, i)) continue;
+		const int n = N->numpMFfromMFtoGO[i];
+		const uint32_t *dst = N->pMFfromMFtoGO + (size_t)i * N->maxnumpMFfromMFtoGO;
+#pragma unroll 4
+		for (int j = 0; j < n; j++) atomicAdd(&sMFGO[dst[j]], 1u);
+	}
 	// updateGOtoGOOut: GABA inputs in (source, slot) order, depression scale,
 	// electrical coupling (innet.cpp:937-978)
 	for (uint32_t d = tid; d < numGO; d += nThr) {
 		uint32_t cnt = 0;
 		float acc = 0;
-		for (uint32_t e = N->gogoStart[d]; e < N->gogoStart[d + 1]; e++) {
+		const uint32_t e0 = N->gogoStart[d], e1 = N->gogoStart[d + 1];
+		const int nc = N->numpGOCoupInGOGO[d];
+#pragma unroll 4
+		for (uint32_t e = e0; e < e1; e++) {
 			const uint32_t src = N->gogoSrc[e];
 			if (sAp[src]) { cnt++; acc += sScale[src]; }
 		}
@@ -360,13 +659,14 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 		const uint8_t ap = sAp[d];
 		N->goGABAOutSynScaleGOGO[d] = s + (!ap) * (1 - s) * N->goGABAGOGOSynRec - ap * (s * (1 - N->goGABAGOGOSynDepF));
 		float vc = 0;
-		const int nc = N->numpGOCoupInGOGO[d];
 		for (int j = 0; j < nc; j++) {
 			const uint32_t n = N->pGOCoupInGOGO[(size_t)d * N->maxnumpGOCoupInGOGO + j];
 			vc = vc + N->coupleRiRjRatioGO * (sV[n] - sV[d]);
 		}
 		N->vCoupleGO[d] = vc;
 	}
+	__syncthreads();
+	for (uint32_t i = tid; i < numGO; i += nThr) N->inputMFGO[i] = sMFGO[i];
 	// threshold coupling: the reference's serial sweep reads already-updated
 	// thresholds of lower-indexed neighbours; the level schedule preserves it
 	for (uint32_t L = 0; L < N->numCoupLevels; L++) {
@@ -409,86 +709,124 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	for (uint32_t i = tid; i < N->mfWords; i += nThr) sMF[i] = mfW[i];
 	__syncthreads();
 
-	// ---- phase 1 (cbmsimcore.cpp:192-200): PC and BC per zone, SC
-	for (uint32_t task = warp; task < Z * numPC; task += nWarps) {
-		const uint32_t z = task / numPC, i = task % numPC;
-		const DevZone &Q = N->zones[z];
-		const float inputSum = pcRowTree(Q.pcPartial + ((size_t)R * numPC + i) * N->bs, N->bs, lane);
-		// calcPCActivities (mzone.cpp:187-226); the SC conductances update
-		// elementwise, their sum runs in the reference's order
-		float gSCPCSum = 0;
-		for (uint32_t j0 = 0; j0 < N->numpPCfromSCtoPC; j0 += 32) {
-			const uint32_t j = j0 + lane;
-			float g = 0;
-			if (j < N->numpPCfromSCtoPC) {
-				const size_t k = (size_t)i * N->numpPCfromSCtoPC + j;
-				g = Q.gSCPC[k];
-				g = g + N->gIncSCtoPC * (1 - g) * Q.inputSCPC[k];
-				g = g * N->gDecSCtoPC;
-				Q.gSCPC[k] = g;
-			}
-			const uint32_t n = min(32u, N->numpPCfromSCtoPC - j0);
-			for (uint32_t q = 0; q < n; q++) gSCPCSum += __shfl_sync(0xffffffffu, g, q);
-		}
-		if (lane == 0) {
-			float gPF = Q.gPFPC[i] + inputSum * N->gIncGRtoPC;
-			gPF = gPF * N->gDecGRtoPC;
-			Q.gPFPC[i] = gPF;
-			float gBC = Q.gBCPC[i] + Q.inputBCPC[i] * N->gIncBCtoPC;
-			gBC = gBC * N->gDecBCtoPC;
-			Q.gBCPC[i] = gBC;
-			float vPC = Q.vPC[i];
-			vPC = vPC + (N->gLeakPC * (N->eLeakPC - vPC)) - (gPF * vPC) +
-				(gBC * (N->eBCtoPC - vPC)) + (gSCPCSum * (N->eSCtoPC - vPC));
-			Q.vPC[i] = vPC;
-			float th = Q.threshPC[i] + (N->threshDecPC * (N->threshRestPC - Q.threshPC[i]));
-			const uint8_t ap = vPC > th;
-			Q.apPC[i] = ap;
-			Q.apBufPC[i] = (Q.apBufPC[i] << 1) | (ap * 0x00000001u);
-			Q.threshPC[i] = ap * N->threshMaxPC + (!ap) * th;
-			if (ap) atomicAdd(&Q.scal[2], 1u);
-		}
-	}
+	// ---- phase 1 (cbmsimcore.cpp:192-200): PC and BC per zone, SC, and the
+	// MF bookkeeping.  The updates are independent; they run in rounds in
+	// which every thread first loads the inputs of its BC, SC and MF cells,
+	// then takes part in its warp's PC, then finishes its cells, so that the
+	// loads of a round are in flight together.
 	const uint32_t *bcSum = N->bcCount + (size_t)R * numBC;
 	const uint32_t *scSum = N->scCount + (size_t)R * numSC;
-	for (uint32_t task = tid; task < Z * numBC; task += nThr) {
-		const uint32_t z = task / numBC, i = task % numBC;
-		const DevZone &Q = N->zones[z];
-		// calcBCActivities (mzone.cpp:228-256)
-		float gPF = Q.gPFBC[i] + (bcSum[i] * N->gIncGRtoBC);
-		gPF = gPF * N->gDecGRtoBC;
-		Q.gPFBC[i] = gPF;
-		float gPC = Q.gPCBC[i] + (Q.inputPCBC[i] * N->gIncPCtoBC);
-		gPC = gPC * N->gDecPCtoBC;
-		Q.gPCBC[i] = gPC;
-		float v = Q.vBC[i];
-		v = v + (N->gLeakBC * (N->eLeakBC - v)) - (gPF * v) + (gPC * (N->ePCtoBC - v));
-		Q.vBC[i] = v;
-		float th = Q.threshBC[i] + N->threshDecBC * (N->threshRestBC - Q.threshBC[i]);
-		const uint8_t ap = v > th;
-		Q.apBC[i] = ap;
-		Q.apBufBC[i] = (Q.apBufBC[i] << 1) | (ap * 0x00000001u);
-		Q.threshBC[i] = ap * N->threshMaxBC + (!ap) * (th);
-	}
-	for (uint32_t i = tid; i < numSC; i += nThr) {
-		float g = N->gPFSC[i] + (scSum[i] * N->gIncGRtoSC);
-		g = g * N->gDecGRtoSC;
-		N->gPFSC[i] = g;
-		float v = N->vSC[i];
-		v = v + (N->gLeakSC * (N->eLeakSC - v)) - g * v;
-		N->vSC[i] = v;
-		const float thOld = N->threshSC[i];
-		const uint8_t ap = v > thOld;
-		N->apSC[i] = ap;
-		sApSC[i] = ap;
-		N->apBufSC[i] = (N->apBufSC[i] << 1) | (ap * 0x00000001u);
-		float th = thOld + N->threshDecSC * (N->threshRestSC - thOld);
-		N->threshSC[i] = ap * N->threshMaxSC + (!ap) * (th);
-	}
-	for (uint32_t i = tid; i < numMF; i += nThr) {
-		const uint32_t m = spikeBit(sMF, i);
-		N->histMF[i] = N->histMF[i] || (m > 0);
-		N->apBufMF[i] = (N->apBufMF[i] << 1) | (m * 0x00000001u);
+	const uint32_t nBCTasks = Z * numBC, nPCTasks = Z * numPC;
+	uint32_t rounds = (nPCTasks + nWarps - 1) / nWarps;
+	rounds = max(rounds, (nBCTasks + nThr - 1) / nThr);
+	rounds = max(rounds, (numSC + nThr - 1) / nThr);
+	rounds = max(rounds, (numMF + nThr - 1) / nThr);
+	for (uint32_t rd = 0; rd < rounds; rd++) {
+		const uint32_t c = rd * nThr + tid;
+		const bool hasBC = c < nBCTasks, hasSC = c < numSC, hasMF = c < numMF;
+		// calcBCActivities inputs (mzone.cpp:228-256)
+		const uint32_t bz = hasBC ? c / numBC : 0, bi = hasBC ? c % numBC : 0;
+		uint32_t bInPF = 0, bInPC = 0, bApBuf = 0;
+		float bgPF0 = 0, bgPC0 = 0, bv0 = 0, bth0 = 0;
+		if (hasBC) {
+			const DevZone &Q = N->zones[bz];
+			bInPF = bcSum[bi]; bInPC = Q.inputPCBC[bi]; bApBuf = Q.apBufBC[bi];
+			bgPF0 = Q.gPFBC[bi]; bgPC0 = Q.gPCBC[bi]; bv0 = Q.vBC[bi]; bth0 = Q.threshBC[bi];
+		}
+		// calcSCActivities inputs (innet.cpp:892-911)
+		uint32_t sInPF = 0, sApBuf = 0;
+		float sg0 = 0, sv0 = 0, sthOld = 0;
+		if (hasSC) {
+			sInPF = scSum[c]; sApBuf = N->apBufSC[c];
+			sg0 = N->gPFSC[c]; sv0 = N->vSC[c]; sthOld = N->threshSC[c];
+		}
+		// updateMFInput's bookkeeping inputs (innet.cpp:800-815)
+		uint8_t mHist = 0;
+		uint32_t mApBuf = 0;
+		if (hasMF) { mHist = N->histMF[c]; mApBuf = N->apBufMF[c]; }
+
+		const uint32_t task = rd * nWarps + warp;
+		if (task < nPCTasks) {
+			const uint32_t z = task / numPC, i = task % numPC;
+			const DevZone &Q = N->zones[z];
+			// the PC's own state, loaded before any store of this task
+			const float gPF0 = Q.gPFPC[i], gBC0 = Q.gBCPC[i], vPC0 = Q.vPC[i], th0 = Q.threshPC[i];
+			const uint32_t inBC = Q.inputBCPC[i], apBuf = Q.apBufPC[i];
+			const float inputSum = pcRowTree(Q.pcPartial + ((size_t)R * numPC + i) * N->bs, N->bs, lane);
+			// calcPCActivities (mzone.cpp:187-226); the SC conductances update
+			// elementwise, their sum runs in the reference's order
+			float gSCPCSum = 0;
+			for (uint32_t j0 = 0; j0 < N->numpPCfromSCtoPC; j0 += 32) {
+				const uint32_t j = j0 + lane;
+				float g = 0;
+				if (j < N->numpPCfromSCtoPC) {
+					const size_t k = (size_t)i * N->numpPCfromSCtoPC + j;
+					const float g0 = Q.gSCPC[k];
+					const uint8_t in = Q.inputSCPC[k];
+					g = g0;
+					g = g + N->gIncSCtoPC * (1 - g) * in;
+					g = g * N->gDecSCtoPC;
+					Q.gSCPC[k] = g;
+				}
+				const uint32_t n = min(32u, N->numpPCfromSCtoPC - j0);
+				for (uint32_t q = 0; q < n; q++) gSCPCSum += __shfl_sync(0xffffffffu, g, q);
+			}
+			if (lane == 0) {
+				float gPF = gPF0 + inputSum * N->gIncGRtoPC;
+				gPF = gPF * N->gDecGRtoPC;
+				Q.gPFPC[i] = gPF;
+				float gBC = gBC0 + inBC * N->gIncBCtoPC;
+				gBC = gBC * N->gDecBCtoPC;
+				Q.gBCPC[i] = gBC;
+				float vPC = vPC0;
+				vPC = vPC + (N->gLeakPC * (N->eLeakPC - vPC)) - (gPF * vPC) +
+					(gBC * (N->eBCtoPC - vPC)) + (gSCPCSum * (N->eSCtoPC - vPC));
+				Q.vPC[i] = vPC;
+				float th = th0 + (N->threshDecPC * (N->threshRestPC - th0));
+				const uint8_t ap = vPC > th;
+				Q.apPC[i] = ap;
+				Q.apBufPC[i] = (apBuf << 1) | (ap * 0x00000001u);
+				Q.threshPC[i] = ap * N->threshMaxPC + (!ap) * th;
+				if (ap) atomicAdd(&Q.scal[2], 1u);
+			}
+		}
+
+		if (hasBC) {
+			const DevZone &Q = N->zones[bz];
+			float gPF = bgPF0 + (bInPF * N->gIncGRtoBC);
+			gPF = gPF * N->gDecGRtoBC;
+			Q.gPFBC[bi] = gPF;
+			float gPC = bgPC0 + (bInPC * N->gIncPCtoBC);
+			gPC = gPC * N->gDecPCtoBC;
+			Q.gPCBC[bi] = gPC;
+			float v = bv0;
+			v = v + (N->gLeakBC * (N->eLeakBC - v)) - (gPF * v) + (gPC * (N->ePCtoBC - v));
+			Q.vBC[bi] = v;
+			float th = bth0 + N->threshDecBC * (N->threshRestBC - bth0);
+			const uint8_t ap = v > th;
+			Q.apBC[bi] = ap;
+			Q.apBufBC[bi] = (bApBuf << 1) | (ap * 0x00000001u);
+			Q.threshBC[bi] = ap * N->threshMaxBC + (!ap) * (th);
+		}
+		if (hasSC) {
+			float g = sg0 + (sInPF * N->gIncGRtoSC);
+			g = g * N->gDecGRtoSC;
+			N->gPFSC[c] = g;
+			float v = sv0;
+			v = v + (N->gLeakSC * (N->eLeakSC - v)) - g * v;
+			N->vSC[c] = v;
+			const uint8_t ap = v > sthOld;
+			N->apSC[c] = ap;
+			sApSC[c] = ap;
+			N->apBufSC[c] = (sApBuf << 1) | (ap * 0x00000001u);
+			float th = sthOld + N->threshDecSC * (N->threshRestSC - sthOld);
+			N->threshSC[c] = ap * N->threshMaxSC + (!ap) * (th);
+		}
+		if (hasMF) {
+			const uint32_t m = spikeBit(sMF, c);
+			N->histMF[c] = mHist || (m > 0);
+			N->apBufMF[c] = (mApBuf << 1) | (m * 0x00000001u);
+		}
 	}
 	__syncthreads();
 	for (uint32_t i = tid; i < numBC; i += nThr) N->bcCount[(size_t)R * numBC + i] = 0;
@@ -496,51 +834,77 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 
 	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
 	// calcNCActivities (mzone.cpp:341-407) one warp per NC
-	for (uint32_t task = tid; task < Z * numIO * nIONC; task += nThr) {
-		const uint32_t z = task / (numIO * nIONC), k = task % (numIO * nIONC);
-		const DevZone &Q = N->zones[z];
-		float g = Q.gNCIO[k];
-		g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO) + N->gDecT0ofNCtoIO));
-		g = g + Q.inputNCIO[k] * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO);
-		Q.gNCIO[k] = g;
-		Q.inputNCIO[k] = 0;
-		ioScratch[task] = g;
+	// NC->IO conductances (one thread per synapse) and MF->NC synaptic
+	// conductances (one thread per synapse), in rounds with the loads first
+	{
+		const uint32_t nIOSyn = Z * numIO * nIONC, nNCSyn = Z * numNC * nMFNC;
+		const uint32_t rounds2 = max((nIOSyn + nThr - 1) / nThr, (nNCSyn + nThr - 1) / nThr);
+		for (uint32_t rd = 0; rd < rounds2; rd++) {
+			const uint32_t c = rd * nThr + tid;
+			const bool hasIO = c < nIOSyn, hasNC = c < nNCSyn;
+			const uint32_t iz = hasIO ? c / (numIO * nIONC) : 0, ik = hasIO ? c % (numIO * nIONC) : 0;
+			float ig0 = 0;
+			uint8_t iIn = 0;
+			if (hasIO) { ig0 = N->zones[iz].gNCIO[ik]; iIn = N->zones[iz].inputNCIO[ik]; }
+			const uint32_t nz = hasNC ? c / (numNC * nMFNC) : 0, nk = hasNC ? c % (numNC * nMFNC) : 0;
+			float nIn = 0, nWt = 0, gmN0 = 0, gN0 = 0, gmA0 = 0, gA0 = 0;
+			if (hasNC) {
+				const DevZone &Q = N->zones[nz];
+				nIn = Q.inputMFNC[nk]; nWt = Q.mfSynWeightNC[nk];
+				gmN0 = Q.gmaxNMDAofMFtoNC[nk]; gN0 = Q.gMFNMDANC[nk];
+				gmA0 = Q.gmaxAMPAofMFtoNC[nk]; gA0 = Q.gMFAMPANC[nk];
+			}
+			if (hasIO) {
+				const DevZone &Q = N->zones[iz];
+				float g = ig0;
+				g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO) + N->gDecT0ofNCtoIO));
+				g = g + iIn * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO);
+				Q.gNCIO[ik] = g;
+				Q.inputNCIO[ik] = 0;
+				ioScratch[c] = g;
+			}
+			if (hasNC) {
+				const DevZone &Q = N->zones[nz];
+				const uint32_t i = nk / nMFNC, j = nk % nMFNC;
+				float gmN = gmN0;
+				gmN = gmN * N->gmaxNMDADecMFtoNC + nIn * nWt * (1 - gmN);
+				Q.gmaxNMDAofMFtoNC[nk] = gmN;
+				float gN = gN0;
+				gN = gN + N->gNMDAIncMFtoNC * (gmN - gN);
+				Q.gMFNMDANC[nk] = gN;
+				float gmA = gmA0;
+				gmA = gmA * N->gmaxAMPADecMFtoNC + nIn * nWt * (1 - gmA);
+				Q.gmaxAMPAofMFtoNC[nk] = gmA;
+				float gA = gA0;
+				gA = gA + N->gAMPAIncMFtoNC * (gmA - gA);
+				Q.gMFAMPANC[nk] = gA;
+				float *sN = ncScratch + ((size_t)nz * numNC + i) * 2 * nMFNC;
+				sN[j] = gN;
+				sN[nMFNC + j] = gA;
+			}
+		}
 	}
+	__syncthreads();
 	for (uint32_t task = warp; task < Z * numNC; task += nWarps) {
 		const uint32_t z = task / numNC, i = task % numNC;
 		const DevZone &Q = N->zones[z];
-		float *sN = ncScratch + (size_t)task * 2 * nMFNC;
-		for (uint32_t j = lane; j < nMFNC; j += 32) {
-			const size_t k = (size_t)i * nMFNC + j;
-			const float in = Q.inputMFNC[k], wt = Q.mfSynWeightNC[k];
-			float gmN = Q.gmaxNMDAofMFtoNC[k];
-			gmN = gmN * N->gmaxNMDADecMFtoNC + in * wt * (1 - gmN);
-			Q.gmaxNMDAofMFtoNC[k] = gmN;
-			float gN = Q.gMFNMDANC[k];
-			gN = gN + N->gNMDAIncMFtoNC * (gmN - gN);
-			Q.gMFNMDANC[k] = gN;
-			float gmA = Q.gmaxAMPAofMFtoNC[k];
-			gmA = gmA * N->gmaxAMPADecMFtoNC + in * wt * (1 - gmA);
-			Q.gmaxAMPAofMFtoNC[k] = gmA;
-			float gA = Q.gMFAMPANC[k];
-			gA = gA + N->gAMPAIncMFtoNC * (gmA - gA);
-			Q.gMFAMPANC[k] = gA;
-			sN[j] = gN;
-			sN[nMFNC + j] = gA;
-		}
+		const float *sN = ncScratch + (size_t)task * 2 * nMFNC;
+		const float vNC0 = Q.vNC[i], thNC0 = Q.threshNC[i];
+		const uint32_t apBufNC = Q.apBufNC[i];
 		float gPCNCSum = 0;
 		for (uint32_t j0 = 0; j0 < N->numpNCfromPCtoNC; j0 += 32) {
 			const uint32_t j = j0 + lane;
 			float g = 0;
 			if (j < N->numpNCfromPCtoNC) {
 				const size_t k = (size_t)i * N->numpNCfromPCtoNC + j;
-				g = Q.gPCNC[k] * N->gDecPCtoNC + Q.inputPCNC[k] * Q.gPCScaleNC[k] * (1 - Q.gPCNC[k]);
+				const float g0 = Q.gPCNC[k], scale = Q.gPCScaleNC[k];
+				const uint8_t in = Q.inputPCNC[k];
+				g = g0 * N->gDecPCtoNC + in * scale * (1 - g0);
 				Q.gPCNC[k] = g;
 			}
 			const uint32_t n = min(32u, N->numpNCfromPCtoNC - j0);
 			for (uint32_t q = 0; q < n; q++) gPCNCSum = gPCNCSum + __shfl_sync(0xffffffffu, g, q);
 		}
-		__syncwarp();
 		float partial = 0;
 		if (lane < 2) {
 			const float *src = sN + lane * nMFNC;
@@ -551,15 +915,15 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 			float gMFNMDASum = partial, gMFAMPASum = ampaSum;
 			gMFNMDASum = gMFNMDASum * N->msPerTimeStep / ((float)nMFNC);
 			gMFAMPASum = gMFAMPASum * N->msPerTimeStep / ((float)nMFNC);
-			float vNC = Q.vNC[i];
+			float vNC = vNC0;
 			gMFNMDASum = gMFNMDASum * vNC / (-80.0f);
 			gPCNCSum = gPCNCSum * N->msPerTimeStep / ((float)N->numpNCfromPCtoNC);
 			vNC = vNC + N->gLeakNC * (N->eLeakNC - vNC) - (gMFNMDASum + gMFAMPASum) * vNC + gPCNCSum * (N->ePCtoNC - vNC);
 			Q.vNC[i] = vNC;
-			float th = Q.threshNC[i] + N->threshDecNC * (N->threshRestNC - Q.threshNC[i]);
+			float th = thNC0 + N->threshDecNC * (N->threshRestNC - thNC0);
 			const uint8_t ap = vNC > th;
 			Q.apNC[i] = ap;
-			Q.apBufNC[i] = (Q.apBufNC[i] << 1) | (ap * 0x00000001u);
+			Q.apBufNC[i] = (apBufNC << 1) | (ap * 0x00000001u);
 			Q.threshNC[i] = ap * N->threshMaxNC + (!ap) * th;
 		}
 	}
@@ -567,123 +931,168 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
 		const uint32_t z = task / numIO, i = task % numIO;
 		const DevZone &Q = N->zones[z];
+		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], errDrive = ctl->errDrive[z], th0 = Q.threshIO[i];
+		const uint32_t apBuf = Q.apBufIO[i];
 		float gNCSum = 0;
 		for (uint32_t j = 0; j < nIONC; j++) gNCSum = gNCSum + ioScratch[(size_t)task * nIONC + j];
 		gNCSum = gNCSum / 3.1;
-		float v = Q.vIO[i];
-		v = v + N->gLeakIO * (N->eLeakIO - v) + gNCSum * 1.5 * (N->eNCtoIO - v) + Q.vCoupleIO[i] + ctl->errDrive[z];
+		float v = v0;
+		v = v + N->gLeakIO * (N->eLeakIO - v) + gNCSum * 1.5 * (N->eNCtoIO - v) + vCouple + errDrive;
 		Q.vIO[i] = v;
-		const uint8_t ap = v > Q.threshIO[i];
+		const uint8_t ap = v > th0;
 		Q.apIO[i] = ap;
-		Q.apBufIO[i] = (Q.apBufIO[i] << 1) | (ap * 0x00000001u);
-		Q.threshIO[i] = N->threshMaxIO * ap + (!ap) * (Q.threshIO[i] + N->threshDecIO * (N->threshRestIO - Q.threshIO[i]));
+		Q.apBufIO[i] = (apBuf << 1) | (ap * 0x00000001u);
+		Q.threshIO[i] = N->threshMaxIO * ap + (!ap) * (th0 + N->threshDecIO * (N->threshRestIO - th0));
 	}
 	__syncthreads();
 
-	// ---- microzone outputs (mzone.cpp:409-524)
-	for (uint32_t task = tid; task < Z * numNC * nMFNC; task += nThr) {
-		const uint32_t z = task / (numNC * nMFNC), k = task % (numNC * nMFNC);
-		const uint32_t src = N->zones[z].pNCfromMFtoNC[k];
-		N->zones[z].inputMFNC[k] = mfRaw ? mfRaw[src] : (uint8_t)spikeBit(sMF, src);
-	}
-	for (uint32_t task = tid; task < Z * numPC; task += nThr) {
-		const uint32_t z = task / numPC, i = task % numPC;
-		const DevZone &Q = N->zones[z];
-		uint32_t c = 0;
-		for (uint32_t e = Q.bcpcStart[i]; e < Q.bcpcStart[i + 1]; e++) c += Q.apBC[Q.bcpcSrc[e]];
-		Q.inputBCPC[i] = c;
-	}
-	for (uint32_t task = tid; task < Z * numPC * N->numpPCfromSCtoPC; task += nThr) {
-		const uint32_t per = numPC * N->numpPCfromSCtoPC;
-		const uint32_t z = task / per, k = task % per;
-		N->zones[z].inputSCPC[k] = sApSC[N->zones[z].pPCfromSCtoPC[k]];
-	}
-	for (uint32_t task = tid; task < Z * numBC; task += nThr) {
-		const uint32_t z = task / numBC, i = task % numBC;
-		const DevZone &Q = N->zones[z];
-		uint32_t c = 0;
-		for (uint32_t e = Q.pcbcStart[i]; e < Q.pcbcStart[i + 1]; e++) c += Q.apPC[Q.pcbcSrc[e]];
-		Q.inputPCBC[i] = c;
-	}
-	for (uint32_t task = tid; task < Z * numNC * N->numpNCfromPCtoNC; task += nThr) {
-		const uint32_t per = numNC * N->numpNCfromPCtoNC;
-		const uint32_t z = task / per, k = task % per;
-		N->zones[z].inputPCNC[k] = N->zones[z].apPC[N->zones[z].pNCfromPCtoNC[k]];
-	}
-	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
-		const uint32_t z = task / numIO, i = task % numIO;
-		const DevZone &Q = N->zones[z];
-		const uint8_t ap = Q.apIO[i];
-		Q.pfPCPlastTimerIO[i] = (!ap) * (Q.pfPCPlastTimerIO[i] + 1) + ap * N->tsLTDStartAPIO;
-		float vc = 0;
-		for (uint32_t j = 0; j < N->numpIOInIOIO; j++)
-			vc = vc + N->coupleRiRjRatioIO * (Q.vIO[Q.pIOInIOIO[(size_t)i * N->numpIOInIOIO + j]] - Q.vIO[i]);
-		Q.vCoupleIO[i] = vc;
-	}
-	for (uint32_t task = tid; task < Z * numNC; task += nThr) {
-		const uint32_t z = task / numNC, i = task % numNC;
-		const DevZone &Q = N->zones[z];
-		float p = Q.synIOPReleaseNC[i];
-		p = p * cbmExpf(-N->msPerTimeStep / (N->relPDecTSofNCtoIO * cbmExpf(-p / N->relPDecTTofNCtoIO) + N->relPDecT0ofNCtoIO));
-		p = p + Q.apNC[i] * N->relPIncNCtoIO * cbmExpf(-p / N->relPIncTauNCtoIO);
-		Q.synIOPReleaseNC[i] = p;
-	}
+	// ---- microzone outputs (mzone.cpp:409-524) and the MF->NC population
+	// bookkeeping (mzone.cpp:536-580): independent gathers, run as one flat
+	// task space so that their loads are in flight together
 	const bool popStep = (t % N->tsPerPopHistBinPC) == 0;
-	if (tid < Z) {
-		const DevZone &Q = N->zones[tid];
-		int doLTD = 0, doLTP = 0;
-		if (popStep) {
-			// updateMFNCSyn bookkeeping (mzone.cpp:536-580)
-			uint32_t *s = Q.scal;
-			s[0] = s[0] - Q.histPCPopAct[s[1]] + s[2];
-			Q.histPCPopAct[s[1]] = s[2];
-			s[2] = 0;
-			s[1] = (s[1] + 1) % N->numPopHistBinsPC;
-			const float avgAllAPPC = ((float)s[0]) / N->numPopHistBinsPC;
-			if (avgAllAPPC >= N->synLTDPCPopActThreshMFtoNC && !s[4]) { doLTD = 1; s[4] = 1; }
-			else if (avgAllAPPC < N->synLTDPCPopActThreshMFtoNC) s[4] = 0;
-			if (avgAllAPPC <= N->synLTPPCPopActThreshMFtoNC && !s[3]) { doLTP = 1; s[3] = 1; }
-			else if (avgAllAPPC > N->synLTPPCPopActThreshMFtoNC) s[3] = 0;
+	{
+		const uint32_t nMFIn = Z * numNC * nMFNC, nBCPC = Z * numPC, nSCPC = Z * numPC * N->numpPCfromSCtoPC,
+			nPCBC = Z * numBC, nPCNC = Z * numNC * N->numpNCfromPCtoNC, nIO = Z * numIO, nNC = Z * numNC;
+		const uint32_t total = nMFIn + nBCPC + nSCPC + nPCBC + nPCNC + nIO + nNC + Z;
+		for (uint32_t task = tid; task < total; task += nThr) {
+			uint32_t r = task;
+			if (r < nMFIn) {
+				const uint32_t z = r / (numNC * nMFNC), k = r % (numNC * nMFNC);
+				const uint32_t src = N->zones[z].pNCfromMFtoNC[k];
+				N->zones[z].inputMFNC[k] = mfRaw ? mfRaw[src] : (uint8_t)spikeBit(sMF, src);
+				continue;
+			}
+			r -= nMFIn;
+			if (r < nBCPC) {
+				const uint32_t z = r / numPC, i = r % numPC;
+				const DevZone &Q = N->zones[z];
+				uint32_t c = 0;
+				const uint32_t e0 = Q.bcpcStart[i], e1 = Q.bcpcStart[i + 1];
+#pragma unroll 4
+				for (uint32_t e = e0; e < e1; e++) c += Q.apBC[Q.bcpcSrc[e]];
+				Q.inputBCPC[i] = c;
+				continue;
+			}
+			r -= nBCPC;
+			if (r < nSCPC) {
+				const uint32_t per = numPC * N->numpPCfromSCtoPC;
+				const uint32_t z = r / per, k = r % per;
+				N->zones[z].inputSCPC[k] = sApSC[N->zones[z].pPCfromSCtoPC[k]];
+				continue;
+			}
+			r -= nSCPC;
+			if (r < nPCBC) {
+				const uint32_t z = r / numBC, i = r % numBC;
+				const DevZone &Q = N->zones[z];
+				uint32_t c = 0;
+				const uint32_t e0 = Q.pcbcStart[i], e1 = Q.pcbcStart[i + 1];
+#pragma unroll 4
+				for (uint32_t e = e0; e < e1; e++) c += Q.apPC[Q.pcbcSrc[e]];
+				Q.inputPCBC[i] = c;
+				continue;
+			}
+			r -= nPCBC;
+			if (r < nPCNC) {
+				const uint32_t per = numNC * N->numpNCfromPCtoNC;
+				const uint32_t z = r / per, k = r % per;
+				N->zones[z].inputPCNC[k] = N->zones[z].apPC[N->zones[z].pNCfromPCtoNC[k]];
+				continue;
+			}
+			r -= nPCNC;
+			if (r < nIO) {
+				const uint32_t z = r / numIO, i = r % numIO;
+				const DevZone &Q = N->zones[z];
+				const uint8_t ap = Q.apIO[i];
+				const int32_t timer = Q.pfPCPlastTimerIO[i];
+				const float vOwn = Q.vIO[i];
+				float vc = 0;
+				for (uint32_t j = 0; j < N->numpIOInIOIO; j++)
+					vc = vc + N->coupleRiRjRatioIO * (Q.vIO[Q.pIOInIOIO[(size_t)i * N->numpIOInIOIO + j]] - vOwn);
+				Q.pfPCPlastTimerIO[i] = (!ap) * (timer + 1) + ap * N->tsLTDStartAPIO;
+				Q.vCoupleIO[i] = vc;
+				continue;
+			}
+			r -= nIO;
+			if (r < nNC) {
+				const uint32_t z = r / numNC, i = r % numNC;
+				const DevZone &Q = N->zones[z];
+				const uint8_t apNC = Q.apNC[i];
+				float p = Q.synIOPReleaseNC[i];
+				p = p * cbmExpf(-N->msPerTimeStep / (N->relPDecTSofNCtoIO * cbmExpf(-p / N->relPDecTTofNCtoIO) + N->relPDecT0ofNCtoIO));
+				p = p + apNC * N->relPIncNCtoIO * cbmExpf(-p / N->relPIncTauNCtoIO);
+				Q.synIOPReleaseNC[i] = p;
+				continue;
+			}
+			r -= nNC;
+			{
+				// updateMFNCSyn's population-activity bookkeeping for zone r
+				const DevZone &Q = N->zones[r];
+				int doLTD = 0, doLTP = 0;
+				if (popStep) {
+					uint32_t *s = Q.scal;
+					const uint32_t sum = s[0], bin = s[1], popAct = s[2], noLTP = s[3], noLTD = s[4];
+					const uint32_t old = Q.histPCPopAct[bin];
+					const uint32_t newSum = sum - old + popAct;
+					Q.histPCPopAct[bin] = popAct;
+					s[0] = newSum;
+					s[2] = 0;
+					s[1] = (bin + 1) % N->numPopHistBinsPC;
+					const float avgAllAPPC = ((float)newSum) / N->numPopHistBinsPC;
+					if (avgAllAPPC >= N->synLTDPCPopActThreshMFtoNC && !noLTD) { doLTD = 1; s[4] = 1; }
+					else if (avgAllAPPC < N->synLTDPCPopActThreshMFtoNC) s[4] = 0;
+					if (avgAllAPPC <= N->synLTPPCPopActThreshMFtoNC && !noLTP) { doLTP = 1; s[3] = 1; }
+					else if (avgAllAPPC > N->synLTPPCPopActThreshMFtoNC) s[3] = 0;
+				}
+				sFlags[2 * r] = doLTD;
+				sFlags[2 * r + 1] = doLTP;
+			}
 		}
-		sFlags[2 * tid] = doLTD;
-		sFlags[2 * tid + 1] = doLTP;
 	}
 	__syncthreads();
 
 	// NC->IO release draws (mzone.cpp:505-511), MF->NC plasticity
 	// (mzone.cpp:586-600), plasticity selector of the next step
-	for (uint32_t task = tid; task < Z * numIO * nIONC; task += nThr) {
-		const uint32_t per = numIO * nIONC;
-		const uint32_t z = task / per, k = task % per;
-		const uint32_t i = k / nIONC, j = k % nIONC;
-		const DevZone &Q = N->zones[z];
-		const double u = (double)rng::uniform24Keyed(Q.ncioKey, rng::ncioCounter(t, i, j, nIONC));
-		Q.inputNCIO[k] = (u < Q.synIOPReleaseNC[Q.pIOfromNCtoIO[k]]);
-	}
-	if (popStep) {
-		for (uint32_t task = tid; task < Z * numNC * nMFNC; task += nThr) {
-			const uint32_t z = task / (numNC * nMFNC), k = task % (numNC * nMFNC);
-			const DevZone &Q = N->zones[z];
-			const int doLTD = sFlags[2 * z], doLTP = sFlags[2 * z + 1];
-			const float synWDelta = N->histMF[Q.pNCfromMFtoNC[k]] *
-				(doLTD * N->synLTDStepSizeMFtoNC + doLTP * N->synLTPStepSizeMFtoNC);
-			float w = Q.mfSynWeightNC[k];
-			w = w + synWDelta;
-			w = (w > 0) * w;
-			w = (w <= 1) * w + (w > 1);
-			Q.mfSynWeightNC[k] = w;
+	{
+		const uint32_t nDraw = Z * numIO * nIONC, nW = popStep ? Z * numNC * nMFNC : 0, nSel = Z * numIO;
+		const bool nextPlast = ((t + 1) % N->tsPerHistBinGR) == 0;
+		for (uint32_t task = tid; task < nDraw + nW + nSel; task += nThr) {
+			uint32_t r = task;
+			if (r < nDraw) {
+				const uint32_t per = numIO * nIONC;
+				const uint32_t z = r / per, k = r % per;
+				const uint32_t i = k / nIONC, j = k % nIONC;
+				const DevZone &Q = N->zones[z];
+				const double u = (double)rng::uniform24Keyed(Q.ncioKey, rng::ncioCounter(t, i, j, nIONC));
+				Q.inputNCIO[k] = (u < Q.synIOPReleaseNC[Q.pIOfromNCtoIO[k]]);
+				continue;
+			}
+			r -= nDraw;
+			if (r < nW) {
+				const uint32_t z = r / (numNC * nMFNC), k = r % (numNC * nMFNC);
+				const DevZone &Q = N->zones[z];
+				const int doLTD = sFlags[2 * z], doLTP = sFlags[2 * z + 1];
+				const float wOld = Q.mfSynWeightNC[k];
+				const float synWDelta = N->histMF[Q.pNCfromMFtoNC[k]] *
+					(doLTD * N->synLTDStepSizeMFtoNC + doLTP * N->synLTPStepSizeMFtoNC);
+				float w = wOld;
+				w = w + synWDelta;
+				w = (w > 0) * w;
+				w = (w <= 1) * w + (w > 1);
+				Q.mfSynWeightNC[k] = w;
+				continue;
+			}
+			r -= nW;
+			{
+				const uint32_t z = r / numIO, i = r % numIO;
+				const DevZone &Q = N->zones[z];
+				uint8_t sel = 0;
+				if (nextPlast) {
+					const int32_t tm = Q.pfPCPlastTimerIO[i];
+					sel = tm < N->tsLTDEndIO ? 1 : (tm > N->tsLTPStartAPIO ? 2 : 0);
+				}
+				Q.plastSel[((t + 1) & 1) * numIO + i] = sel;
+			}
 		}
-	}
-	const bool nextPlast = ((t + 1) % N->tsPerHistBinGR) == 0;
-	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
-		const uint32_t z = task / numIO, i = task % numIO;
-		const DevZone &Q = N->zones[z];
-		uint8_t sel = 0;
-		if (nextPlast) {
-			const int32_t tm = Q.pfPCPlastTimerIO[i];
-			sel = tm < N->tsLTDEndIO ? 1 : (tm > N->tsLTPStartAPIO ? 2 : 0);
-		}
-		Q.plastSel[((t + 1) & 1) * numIO + i] = sel;
 	}
 	__syncthreads();
 	if ((t % N->numTSinMFHist) == 0)
@@ -691,15 +1100,66 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	if (tid < Z) ctl->errDrive[tid] = 0;
 }
 
+// Copy the descriptor and every staged array into shared memory and point
+// the copy's array pointers there.
+__device__ void stageIn(const DevNet *N, DevNet *sNet, uint8_t *arena, const StageSeg *segs, uint32_t nSegs)
+{
+	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u, warp = tid >> 5, nWarps = nThr >> 5;
+	for (uint32_t i = tid; i < sizeof(DevNet) / 4; i += nThr)
+		reinterpret_cast<uint32_t *>(sNet)[i] = reinterpret_cast<const uint32_t *>(N)[i];
+	for (uint32_t k = warp; k < nSegs; k += nWarps) {
+		const StageSeg sg = segs[k];
+		const uint4 *src = *reinterpret_cast<const uint4 *const *>(reinterpret_cast<const char *>(N) + sg.fieldOff);
+		uint4 *dst = reinterpret_cast<uint4 *>(arena + sg.smemOff);
+#pragma unroll 4
+		for (uint32_t i = lane; i < sg.bytes / 16u; i += 32u) dst[i] = src[i];
+	}
+	__syncthreads();
+	for (uint32_t k = tid; k < nSegs; k += nThr)
+		*reinterpret_cast<uint8_t **>(reinterpret_cast<char *>(sNet) + segs[k].fieldOff) = arena + segs[k].smemOff;
+	__syncthreads();
+}
+
+// Write the staged arrays that the step changes back to global memory.
+__device__ void stageOut(const DevNet *N, const uint8_t *arena, const StageSeg *segs, uint32_t nSegs)
+{
+	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+	for (uint32_t k = warp; k < nSegs; k += nWarps) {
+		const StageSeg sg = segs[k];
+		if (!sg.writeBack) continue;
+		uint4 *dst = *reinterpret_cast<uint4 *const *>(reinterpret_cast<const char *>(N) + sg.fieldOff);
+		const uint4 *src = reinterpret_cast<const uint4 *>(arena + sg.smemOff);
+#pragma unroll 4
+		for (uint32_t i = lane; i < sg.bytes / 16u; i += 32u) dst[i] = src[i];
+	}
+}
+
 // Small-cell update of step t: block 2n is network n's Golgi role, block
-// 2n+1 its microzone role.  The two roles share no state.
+// 2n+1 its microzone role.  The two roles share no state.  The microzone
+// role runs on shared-memory copies of its arrays when they fit (one bulk
+// copy in and out per step instead of a global round trip per phase).
 __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, uint32_t stepOffset)
 {
 	const DevNet *__restrict__ N = nets[blockIdx.x >> 1];
 	const uint64_t t = *N->tBase + 1 + stepOffset;
-	extern __shared__ uint32_t tailSmem[];
-	if (blockIdx.x & 1) zoneRole(N, t, tailSmem);
-	else golgiRole(N, t, tailSmem);
+	extern __shared__ __align__(16) uint32_t tailSmem[];
+	if (blockIdx.x & 1) {
+		const uint32_t nSegs = N->numZoneSegs;
+		if (nSegs) {
+			uint8_t *base = reinterpret_cast<uint8_t *>(tailSmem);
+			DevNet *sNet = reinterpret_cast<DevNet *>(base);
+			uint8_t *arena = base + ((sizeof(DevNet) + 15) & ~(size_t)15);
+			const StageSeg *segs = N->zoneSegs;
+			stageIn(N, sNet, arena, segs, nSegs);
+			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(arena + N->zoneArenaBytes));
+			__syncthreads();
+			stageOut(N, arena, segs, nSegs);
+		} else {
+			zoneRole(N, t, tailSmem);
+		}
+	} else {
+		golgiRole(N, t, tailSmem);
+	}
 }
 
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps)

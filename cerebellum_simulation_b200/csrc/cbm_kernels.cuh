@@ -10,6 +10,11 @@ constexpr int kTailThreads = 1024;
 
 __global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOffset, int numNets,
 		uint32_t stepOffset);
+// TMA GR pass with W consumer warps of RW rows each per stage, S stages
+// deep, at least B resident CTAs per SM, synapse-slot loops bounded by M
+// (0: any count); launched with 32 * (W + 1) threads and the grPassKernel
+// arguments.  Returns null for a geometry that is not compiled in.
+const void *passTmaKernelFor(int W, int RW, int S, int B, int M);
 __global__ void tailKernel(const DevNet *const *nets, uint32_t stepOffset);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);

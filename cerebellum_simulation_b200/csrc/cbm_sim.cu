@@ -2,6 +2,9 @@
 #include "cbm_sim.hpp"
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstddef>
+#include <cstdio>
 #include <cstring>
 #include <map>
 
@@ -23,10 +26,12 @@ std::string cudaErr(cudaError_t e, const char *what)
 template <typename T> T *Network::alloc(size_t n)
 {
 	void *p = nullptr;
-	size_t bytes = std::max<size_t>(n * sizeof(T), 16);
+	// whole 16-byte units, so that arrays can be copied with 16-byte accesses
+	size_t bytes = (std::max<size_t>(n * sizeof(T), 16) + 15) & ~(size_t)15;
 	if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
 	cudaMemset(p, 0, bytes);
 	allocs_.push_back(p);
+	allocBytes_[p] = bytes;
 	return (T *)p;
 }
 
@@ -70,14 +75,153 @@ size_t Network::passSmemBytes() const
 		sizeof(float) * (size_t)h_.numZones * 2 * h_.K * h_.J;
 }
 
-size_t Network::tailSmemBytes() const
+size_t Network::passTmaSmemBytes(uint32_t R, uint32_t S) const
 {
-	// Golgi role: MF bits, GO scales, potentials, thresholds, spikes
-	const size_t golgi = 4ull * h_.mfWords + 12ull * h_.numGO + h_.numGO;
-	// microzone role: MF bits, SC spikes, NC and IO scratch, plasticity flags
-	const size_t zone = 4ull * h_.mfWords + ((h_.numSC + 15) & ~15u) +
+	const PassLayout L = passLayout(R, h_.nMFSlots, h_.nGOSlots, h_.nOutSlots, h_.numZones);
+	return 128 + (size_t)S * L.bytes + 16ull * S + sizeof(uint32_t) * ((size_t)h_.bcLocal + h_.scLocal) +
+		sizeof(float) * (size_t)h_.numZones * 2 * h_.K * 32 + 32ull * (h_.mfWords + h_.goWords);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+		const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+		CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encodeTiledFn()
+{
+	static EncodeTiledFn fn = nullptr;
+	if (!fn) {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+				q == cudaDriverEntryPointSuccess)
+			fn = (EncodeTiledFn)p;
+	}
+	return fn;
+}
+
+std::string Network::buildPassMaps(uint32_t R)
+{
+	EncodeTiledFn enc = encodeTiledFn();
+	if (!enc) return "cuTensorMapEncodeTiled is unavailable";
+	const uint32_t N = h_.numGR, bs = h_.bs;
+	if ((uint64_t)h_.numPC * h_.P != N || bs < 32 || N % bs || 2 * h_.K % R) return "GR pass tiling does not cover the cells";
+	std::vector<CUtensorMap> maps(PM_COUNT);
+	memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+	auto enc2 = [&](int m, const void *ptr, CUtensorMapDataType dt, uint32_t es) -> std::string {
+		const cuuint64_t dims[2] = {bs, N / bs};
+		const cuuint64_t strides[1] = {(cuuint64_t)bs * es};
+		const cuuint32_t box[2] = {32, R};
+		const cuuint32_t estr[2] = {1, 1};
+		if (enc(&maps[m], dt, 2, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+				CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+			return "encoding a TMA descriptor failed";
+		return "";
+	};
+	auto enc3 = [&](int m, const void *ptr, CUtensorMapDataType dt, uint32_t es, uint32_t slots) -> std::string {
+		const cuuint64_t dims[3] = {bs, N / bs, slots};
+		const cuuint64_t strides[2] = {(cuuint64_t)bs * es, (cuuint64_t)N * es};
+		const cuuint32_t box[3] = {32, R, slots};
+		const cuuint32_t estr[3] = {1, 1, 1};
+		if (enc(&maps[m], dt, 3, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+				CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+			return "encoding a TMA descriptor failed";
+		return "";
+	};
+	if (std::max({h_.nMFSlots, h_.nGOSlots, h_.nOutSlots}) > 256) return "more than 256 synapse slots per GR";
+	CKS(enc2(PM_V, h_.vGR, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
+	CKS(enc2(PM_GKCA, h_.gKCaGR, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
+	CKS(enc2(PM_THRESH, h_.threshGR, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
+	CKS(enc2(PM_GESUM, h_.gESum, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
+	CKS(enc2(PM_GISUM, h_.gISum, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
+	CKS(enc2(PM_APBUF, h_.apBufGR, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4));
+	CKS(enc3(PM_MFIDX, h_.mfIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nMFSlots)));
+	CKS(enc3(PM_GOIDX, h_.goIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nGOSlots)));
+	CKS(enc3(PM_OUTCON, h_.outCon, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, std::max(1u, h_.nOutSlots)));
+	CKS(enc2(PM_PFDELAY, h_.pfDelay, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1));
+	CKS(enc2(PM_HIST, h_.historyGR, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8));
+	for (uint32_t z = 0; z < h_.numZones; z++) CKS(enc2(PM_W0 + z, h_.zones[z].w, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
+	CUtensorMap *d = alloc<CUtensorMap>(PM_COUNT);
+	if (!d) return "device allocation failed";
+	CK(cudaMemcpy(d, maps.data(), PM_COUNT * sizeof(CUtensorMap), cudaMemcpyHostToDevice), "uploading TMA descriptors");
+	h_.passMaps = d;
+	CK(cudaMemcpy(dNet_.ptr, &h_, sizeof(DevNet), cudaMemcpyHostToDevice), "uploading the network descriptor");
+	return "";
+}
+
+// Arrays the microzone CTA stages in shared memory for each step: its
+// state (written back) and its connectivity (read only).  Arrays that the GR
+// pass reads during the same step (weights, plasticity selectors, partial
+// sums, counters) stay in global memory.
+std::string Network::buildZoneStaging()
+{
+	std::vector<StageSeg> segs;
+	uint32_t arena = 0;
+	auto add = [&](size_t fieldOff, bool writeBack) -> std::string {
+		void *ptr = *(void **)((char *)&h_ + fieldOff);
+		auto it = allocBytes_.find(ptr);
+		if (it == allocBytes_.end()) return "staging: unknown array";
+		StageSeg sg;
+		sg.fieldOff = (uint32_t)fieldOff;
+		sg.bytes = (uint32_t)it->second;
+		sg.smemOff = arena;
+		sg.writeBack = writeBack ? 1u : 0u;
+		arena += sg.bytes;
+		segs.push_back(sg);
+		return "";
+	};
+#define CBM_NET(f, wb) CKS(add(offsetof(DevNet, f), wb))
+	CBM_NET(apSC, true); CBM_NET(apBufSC, true); CBM_NET(gPFSC, true); CBM_NET(threshSC, true); CBM_NET(vSC, true);
+	CBM_NET(histMF, true); CBM_NET(apBufMF, true);
+#undef CBM_NET
+	for (uint32_t z = 0; z < h_.numZones; z++) {
+		const size_t zb = offsetof(DevNet, zones) + z * sizeof(DevZone);
+#define CBM_ZONE(f, wb) CKS(add(zb + offsetof(DevZone, f), wb))
+		CBM_ZONE(pPCfromSCtoPC, false); CBM_ZONE(pNCfromPCtoNC, false); CBM_ZONE(pNCfromMFtoNC, false);
+		CBM_ZONE(pIOfromNCtoIO, false); CBM_ZONE(pIOInIOIO, false); CBM_ZONE(bcpcStart, false);
+		CBM_ZONE(bcpcSrc, false); CBM_ZONE(pcbcStart, false); CBM_ZONE(pcbcSrc, false); CBM_ZONE(gPCScaleNC, false);
+		CBM_ZONE(apBC, true); CBM_ZONE(apBufBC, true); CBM_ZONE(inputPCBC, true); CBM_ZONE(gPFBC, true);
+		CBM_ZONE(gPCBC, true); CBM_ZONE(threshBC, true); CBM_ZONE(vBC, true);
+		CBM_ZONE(apPC, true); CBM_ZONE(apBufPC, true); CBM_ZONE(inputBCPC, true); CBM_ZONE(inputSCPC, true);
+		CBM_ZONE(gPFPC, true); CBM_ZONE(gBCPC, true); CBM_ZONE(gSCPC, true); CBM_ZONE(vPC, true);
+		CBM_ZONE(threshPC, true); CBM_ZONE(histPCPopAct, true); CBM_ZONE(scal, true);
+		CBM_ZONE(apIO, true); CBM_ZONE(apBufIO, true); CBM_ZONE(inputNCIO, true); CBM_ZONE(gNCIO, true);
+		CBM_ZONE(threshIO, true); CBM_ZONE(vIO, true); CBM_ZONE(vCoupleIO, true); CBM_ZONE(pfPCPlastTimerIO, true);
+		CBM_ZONE(apNC, true); CBM_ZONE(apBufNC, true); CBM_ZONE(inputPCNC, true); CBM_ZONE(inputMFNC, true);
+		CBM_ZONE(gPCNC, true); CBM_ZONE(mfSynWeightNC, true); CBM_ZONE(gmaxNMDAofMFtoNC, true);
+		CBM_ZONE(gmaxAMPAofMFtoNC, true); CBM_ZONE(gMFNMDANC, true); CBM_ZONE(gMFAMPANC, true);
+		CBM_ZONE(threshNC, true); CBM_ZONE(vNC, true); CBM_ZONE(synIOPReleaseNC, true);
+#undef CBM_ZONE
+	}
+	h_.numZoneSegs = 0;
+	h_.zoneArenaBytes = 0;
+	h_.zoneSegs = nullptr;
+	const size_t total = ((sizeof(DevNet) + 15) & ~(size_t)15) + arena + zoneScratchBytes();
+	if (total > kTailSmemBudget) return "";  // too large: the microzone CTA works on global memory
+	StageSeg *d = upload(segs.data(), segs.size());
+	if (!d) return "device allocation failed";
+	h_.zoneSegs = d;
+	h_.numZoneSegs = (uint32_t)segs.size();
+	h_.zoneArenaBytes = arena;
+	return "";
+}
+
+size_t Network::zoneScratchBytes() const
+{
+	// MF bits, SC spikes, NC and IO scratch, plasticity flags
+	return 4ull * h_.mfWords + ((h_.numSC + 15) & ~15u) +
 		4ull * h_.numZones * h_.numNC * 2 * h_.numpNCfromMFtoNC + 4ull * h_.numZones * h_.numIO * h_.numpIOfromNCtoIO +
 		8ull * kMaxZones;
+}
+
+size_t Network::tailSmemBytes() const
+{
+	// Golgi role: MF bits, MF->GO counts, GO scales, potentials, thresholds, spikes
+	const size_t golgi = 4ull * h_.mfWords + 16ull * h_.numGO + h_.numGO;
+	// microzone role: its scratch, after the staged descriptor and arrays
+	size_t zone = zoneScratchBytes();
+	if (h_.numZoneSegs) zone += ((sizeof(DevNet) + 15) & ~(size_t)15) + h_.zoneArenaBytes;
 	return std::max(golgi, zone);
 }
 
@@ -243,17 +387,6 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	}
 	h.numpMFfromMFtoGO = upI("numpMFfromMFtoGO"); h.pMFfromMFtoGO = upU("pMFfromMFtoGO");
 	{
-		// destination-side MF lists: each (fibre, slot) synapse of
-		// pMFfromMFtoGO once under its GO
-		std::vector<std::vector<uint32_t>> in(c.numGO);
-		for (uint32_t i = 0; i < c.numMF; i++)
-			for (int j = 0; j < numMFGO[i]; j++) in[pMFGO[(size_t)i * c.maxnumpMFfromMFtoGO + j]].push_back(i);
-		std::vector<uint32_t> start(c.numGO + 1, 0), src;
-		for (uint32_t d = 0; d < c.numGO; d++) { start[d + 1] = start[d] + (uint32_t)in[d].size(); src.insert(src.end(), in[d].begin(), in[d].end()); }
-		h.mfgoStart = upload(start.data(), start.size());
-		h.mfgoSrc = upload(src.data(), src.size());
-	}
-	{
 		const int32_t *numOutGG = A("numpGOGABAOutGOGO")->as<int32_t>();
 		const uint32_t *pOutGG = A("pGOGABAOutGOGO")->as<uint32_t>();
 		std::vector<std::vector<uint32_t>> in(c.numGO);
@@ -398,6 +531,7 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	h.ctl = alloc<HostCtl>(1);
 	h.errFlag = alloc<uint32_t>(1);
 	for (void *p : allocs_) if (!p) return "device allocation failed";
+	CKS(buildZoneStaging());
 	if (cudaMallocHost((void **)&hPinnedBits_, (size_t)h.mfWords * 4) != cudaSuccess ||
 			cudaMallocHost((void **)&hPinnedRaw_, (size_t)c.numMF) != cudaSuccess)
 		return "pinned allocation failed";
@@ -623,8 +757,13 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 {
 	device_ = device;
 	CK(cudaSetDevice(device), "selecting the device");
-	CK(cudaStreamCreateWithFlags(&s0_, cudaStreamNonBlocking), "stream");
-	CK(cudaStreamCreateWithFlags(&s1_, cudaStreamNonBlocking), "stream");
+	// The small-cell CTAs (one SM's register file each) go on the
+	// high-priority stream so that they are dispatched before the GR pass
+	// fills every SM; graphs keep the per-node priority.
+	int leastPrio = 0, greatestPrio = 0;
+	CK(cudaDeviceGetStreamPriorityRange(&leastPrio, &greatestPrio), "stream priorities");
+	CK(cudaStreamCreateWithPriority(&s0_, cudaStreamNonBlocking, leastPrio), "stream");
+	CK(cudaStreamCreateWithPriority(&s1_, cudaStreamNonBlocking, greatestPrio), "stream");
 	CK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "event");
 	CK(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "event");
 	CK(cudaEventCreate(&ev0_), "event");
@@ -659,6 +798,47 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 		CK(cudaFuncSetAttribute(grPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem_), "pass smem");
 	if (tailSmem_ > 48 * 1024)
 		CK(cudaFuncSetAttribute(tailKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tailSmem_), "tail smem");
+
+	// TMA GR pass: W consumer warps of RW rows each per stage, S stages deep;
+	// every network of the set must have 32-cell tile rows and at least
+	// W*RW rows per tile.  CBM_PASS_TMA="W,RW,S" picks another compiled
+	// geometry (tuning), CBM_PASS_TMA=0 the plain pass kernel.
+	bool tma = !nets_.empty();
+	uint32_t minRows = UINT32_MAX, maxSlots = 0;
+	for (Network *n : nets_) {
+		tma = tma && n->passTmaCapable();
+		minRows = std::min(minRows, n->passRows());
+		maxSlots = std::max({maxSlots, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutSlots});
+	}
+	int W = 4, RW = 1, S = 4, B = 4, M = 4;
+	if (maxSlots > 4) { W = 8; S = 3; B = 2; M = 0; }
+	if (const char *env = getenv("CBM_PASS_TMA")) {
+		if (!strcmp(env, "0")) tma = false;
+		else if (sscanf(env, "%d,%d,%d,%d,%d", &W, &RW, &S, &B, &M) != 5 || !passTmaKernelFor(W, RW, S, B, M) ||
+				(M > 0 && maxSlots > (uint32_t)M))
+			return "CBM_PASS_TMA names a geometry that is not compiled in or does not fit the network";
+	}
+	if (tma && (uint32_t)(W * RW) > minRows) {
+		// small tiles: fewer rows per stage
+		const int cand[][5] = {{4, 1, 4, 1, 0}, {2, 1, 4, 1, 0}, {1, 1, 4, 1, 0}};
+		tma = false;
+		for (const int *c : cand)
+			if ((uint32_t)(c[0] * c[1]) <= minRows) { W = c[0]; RW = c[1]; S = c[2]; B = c[3]; M = c[4]; tma = true; break; }
+	}
+	if (tma) {
+		const uint32_t R = (uint32_t)(W * RW);
+		size_t smem = 0;
+		for (Network *n : nets_) smem = std::max(smem, n->passTmaSmemBytes(R, (uint32_t)S));
+		if (smem <= 227 * 1024) {
+			for (Network *n : nets_) CKS(n->buildPassMaps(R));
+			passTmaFn_ = passTmaKernelFor(W, RW, S, B, M);
+			passTmaW_ = (uint32_t)W;
+			passTmaR_ = R;
+			passTmaS_ = (uint32_t)S;
+			passTmaSmem_ = smem;
+			CK(cudaFuncSetAttribute(passTmaFn_, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "pass smem");
+		}
+	}
 	return "";
 }
 
@@ -680,8 +860,17 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	CK(cudaEventRecord(fork_, s0_), "fork");
 	CK(cudaStreamWaitEvent(s1_, fork_, 0), "fork");
 	if (instrument) CK(cudaEventRecordWithFlags(passEv_[2 * k], s0_, cudaEventRecordExternal), "pass timing");
-	grPassKernel<<<passBlocks_, kPassThreads, passSmem_, s0_>>>((const DevNet *const *)dNetPtrs_.ptr,
-			(const uint32_t *)dBlockOffset_.ptr, (int)nets_.size(), k);
+	const DevNet *const *netsArg = (const DevNet *const *)dNetPtrs_.ptr;
+	const uint32_t *offsArg = (const uint32_t *)dBlockOffset_.ptr;
+	int numNetsArg = (int)nets_.size();
+	uint32_t stepArg = k;
+	if (passTmaFn_) {
+		void *args[] = {&netsArg, &offsArg, &numNetsArg, &stepArg};
+		CK(cudaLaunchKernel(passTmaFn_, dim3(passBlocks_), dim3(32 * (passTmaW_ + 1)), args, passTmaSmem_, s0_),
+				"launching the GR pass");
+	} else {
+		grPassKernel<<<passBlocks_, kPassThreads, passSmem_, s0_>>>(netsArg, offsArg, numNetsArg, stepArg);
+	}
 	CK(cudaGetLastError(), "launching the GR pass");
 	if (instrument) CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
 	if (instrument) CK(cudaEventRecordWithFlags(tailEv_[2 * k], s1_, cudaEventRecordExternal), "tail timing");
@@ -752,7 +941,7 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 		}
 		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), chunk);
 		CK(cudaStreamEndCapture(s0_, &g), "graph capture");
-		CK(cudaGraphInstantiate(&graphExec_, g, 0), "graph instantiate");
+		CK(cudaGraphInstantiate(&graphExec_, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
 		cudaGraphDestroy(g);
 		graphChunk_ = chunk;
 		graphInstrumented_ = instrument;
@@ -764,6 +953,7 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 	if (rem) CKS(launchSteps((uint32_t)rem));
 	CK(cudaEventRecord(ev1_, s0_), "timing");
 	CK(cudaEventSynchronize(ev1_), "graph run");
+	CKS(checkDeviceErrors());
 	CK(cudaEventElapsedTime(&lastGraphMs_, ev0_, ev1_), "timing");
 	lastPassMs_ = 0;
 	if (instrument && reps) {
@@ -805,6 +995,17 @@ std::string Simulator::sync()
 	CK(cudaStreamSynchronize(s0_), "sync");
 	CK(cudaStreamSynchronize(s1_), "sync");
 	CK(cudaGetLastError(), "sync");
+	return checkDeviceErrors();
+}
+
+std::string Simulator::checkDeviceErrors()
+{
+	for (Network *n : nets_) {
+		uint32_t flag = 0;
+		CK(cudaMemcpy(&flag, n->h_.errFlag, sizeof(flag), cudaMemcpyDeviceToHost), "reading the device error word");
+		if (flag & kErrPassWait) return "GR pass: a pipeline wait timed out on the device";
+		if (flag) return "device error word set";
+	}
 	return "";
 }
 

@@ -4,6 +4,7 @@
 // innetmodules/innet.h, mzonemodules/mzone.h).
 #pragma once
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -56,6 +57,11 @@ public:
 	float lastGraphMs() const { return lastGraphMs_; }
 	float lastPassMs() const { return lastPassMs_; }
 	float lastTailMs() const { return lastTailMs_; }
+	// rows per stage and stages of the TMA GR pass (0, 0 when the plain pass runs)
+	uint32_t passStageRows() const { return passTmaR_; }
+	uint32_t passStages() const { return passTmaS_; }
+	// Device error word of every network (kErr* bits): non-empty on error.
+	std::string checkDeviceErrors();
 	std::string timerStart();
 	std::string timerStop(float *ms);
 
@@ -70,6 +76,10 @@ private:
 	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_;
 	uint32_t passBlocks_ = 0;
 	size_t passSmem_ = 0, tailSmem_ = 0;
+	// TMA GR pass geometry (passTmaFn_ null: the plain pass kernel runs)
+	const void *passTmaFn_ = nullptr;
+	uint32_t passTmaW_ = 0, passTmaR_ = 0, passTmaS_ = 0;
+	size_t passTmaSmem_ = 0;
 	cudaGraphExec_t graphExec_ = nullptr;
 	uint32_t graphChunk_ = 0;
 	bool graphInstrumented_ = false;
@@ -104,6 +114,15 @@ public:
 	uint32_t passBlocks() const { return h_.numPC * h_.tilesPerPC; }
 	size_t passSmemBytes() const;
 	size_t tailSmemBytes() const;
+	// TMA GR pass: possible when every row of the reduction tile is 32 cells
+	bool passTmaCapable() const { return h_.J == 32; }
+	uint32_t passRows() const { return 2 * h_.K; }
+	// Encode the TMA descriptors for boxes of R rows and upload them.
+	std::string buildPassMaps(uint32_t R);
+	size_t passTmaSmemBytes(uint32_t R, uint32_t S) const;
+	size_t zoneScratchBytes() const;
+	// shared memory a small-cell CTA may use (the staged arrays included)
+	static constexpr size_t kTailSmemBudget = 200 * 1024;
 	uint32_t mfWords() const { return h_.mfWords; }
 	uint32_t mfRing() const { return h_.mfRing; }
 	double bytesPerStepAlgorithmic() const;  // 72 + 4 n_mf + 4 n_go + 8 n_out per GR
@@ -121,7 +140,9 @@ private:
 	State *st_ = nullptr;
 	DevNet h_{};
 	DeviceBuf dNet_;
+	std::string buildZoneStaging();
 	std::vector<void *> allocs_;
+	std::map<const void *, size_t> allocBytes_;
 	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;
 	uint32_t *hPinnedBits_ = nullptr;
 	uint8_t *hPinnedRaw_ = nullptr;

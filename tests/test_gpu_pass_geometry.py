@@ -1,0 +1,49 @@
+"""Every compiled geometry of the TMA GR pass (consumer warps x rows per warp
+x stages x resident CTAs x slot bound) gives the same network state, bit for
+bit, as the plain GR pass kernel; the plain kernel is pinned to the oracle by
+test_gpu_parity.py."""
+import os
+
+import numpy as np
+import pytest
+
+import cbmtest
+
+pytestmark = pytest.mark.gpu
+
+GEOMETRIES = ["8,1,3,2,4", "8,1,3,3,4", "8,1,4,2,4", "8,1,2,3,4", "4,1,4,4,4", "4,2,3,3,4", "4,2,4,2,4",
+              "8,1,3,2,0", "4,1,4,1,0", "2,1,4,1,0", "1,1,4,1,0"]
+EVENTS = {1: [("plast", 0, -0.002, 0.002)], 60: [("errdrive", 0, 1.0)], 90: [("grgoinc", 0.01)]}
+
+
+def run_with(geometry, state_path, mf, out_path):
+    import cerebellum_simulation_b200 as cbm
+    old = os.environ.get("CBM_PASS_TMA")
+    os.environ["CBM_PASS_TMA"] = geometry
+    try:
+        sim = cbm.CBMSimCore(cbm.CBMState(state_path), [3], device=0)
+    finally:
+        if old is None:
+            del os.environ["CBM_PASS_TMA"]
+        else:
+            os.environ["CBM_PASS_TMA"] = old
+    cbmtest.product_run(sim, mf, EVENTS, record=False)
+    sim.writeToState(out_path)
+    sim.close()
+    with open(out_path, "rb") as f:
+        return f.read()
+
+
+def test_tma_pass_geometries_match_plain_pass(tmp_path):
+    from cerebellum_simulation_b200 import networks
+    # 131,072 GR, 32 PCs of 4096 fibres: tiles of 8 rows x 32 cells; 4 MF,
+    # 3 GO and 4 GR->GO slots per cell
+    st = networks.build_random_network(9, 8, 5, 5, 10, networks.act_params("dense"), seed=5,
+                                       go_out_per_gr=4, mf_per_go=16, vel=147)
+    path = str(tmp_path / "net.state")
+    st.writeState(path)
+    mf = networks.uniform_mf_stream(1024, 120, seed=5, lo=5.0, hi=60.0)
+    want = run_with("0", path, mf, str(tmp_path / "plain.state"))
+    for g in GEOMETRIES:
+        got = run_with(g, path, mf, str(tmp_path / f"tma_{g}.state"))
+        assert got == want, f"geometry {g} differs from the plain pass"
