@@ -88,6 +88,7 @@ struct HostCtl {
 struct DevZone {
 	float *w;           // pfSynWeightPC, PC-major (mzone.cpp:97-103)
 	float *pcPartial;   // [3][numPC][bs] per-thread partial sums of the PF->PC reduction
+	float *pairSum;     // [2][numPC][K][bs] x[i] + x[i+bs] of the reduction per step parity (persistent GR pass)
 	uint8_t *plastSel;  // [2][numIO]: 0 none, 1 LTD, 2 LTP for the next plasticity step
 	const uint32_t *ioOfPC;  // IO whose timer drives each PC block's plasticity (mzone.cpp:682-705)
 

@@ -304,11 +304,6 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 		}
 		tma::fenceBarrierInit();
 	}
-	const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
-	const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
-	for (uint32_t i = threadIdx.x; i < 32u * N->mfWords; i += blockDim.x) sMF[i] = (uint8_t)spikeBit(mfSrc, i);
-	for (uint32_t i = threadIdx.x; i < 32u * N->goWords; i += blockDim.x) sGO[i] = (uint8_t)spikeBit(goSrc, i);
-	for (uint32_t i = threadIdx.x; i < N->bcLocal + N->scLocal; i += blockDim.x) sBC[i] = 0;
 	__syncthreads();
 
 	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
@@ -349,7 +344,14 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 			}
 		}
 	} else {
-		// ---- consumers: warp w updates rows w, w+W, ..., w+(RW-1)W of every stage
+		// ---- consumers: warp w updates rows w, w+W, ..., w+(RW-1)W of every
+		// stage.  They stage the spike tables while the first copies fly.
+		const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+		const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
+		for (uint32_t i = threadIdx.x; i < 32u * N->mfWords; i += 32u * W) sMF[i] = (uint8_t)spikeBit(mfSrc, i);
+		for (uint32_t i = threadIdx.x; i < 32u * N->goWords; i += 32u * W) sGO[i] = (uint8_t)spikeBit(goSrc, i);
+		for (uint32_t i = threadIdx.x; i < N->bcLocal + N->scLocal; i += 32u * W) sBC[i] = 0;
+		asm volatile("bar.sync 1, %0;" ::"r"(32u * W) : "memory");
 		float stepW[kMaxZones];
 #pragma unroll
 		for (uint32_t z = 0; z < kMaxZones; z++) {
@@ -508,6 +510,266 @@ const void *passTmaKernelFor(int W, int RW, int S, int B, int M)
 	if (W == w && RW == rw && S == s && B == b && M == m) return (const void *)&grPassTmaKernel<w, rw, s, b, m>;
 	CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_PICK)
 #undef CBM_PASS_TMA_PICK
+	return nullptr;
+}
+
+// ----------------------------------------------------- GR pass, persistent
+// Single-network GR pass in persistent CTAs.  The work is cut into units of
+// R = 2W rows x 32 cells of one tile, numbered tile-major; CTA c takes units
+// c, c + gridDim, ... so that every SM gets the same number of units to
+// within one.  A producer warp streams each unit's rows by TMA into an
+// S-deep ring; consumer warp w updates rows 2w and 2w+1 of the unit, which
+// are the two terms x[i], x[i+bs] of one step kk of sumInputsNew's per-thread
+// running sum, and stores their sum (pairSum, one buffer per step parity).
+// The running sums over kk (tempSum += x[i] + x[i+bs], kernels.cu:326-362)
+// of step t-1 are taken in order at the start of step t's pass, when all of
+// step t-1's pair sums are in memory, so the float order is the reference's
+// and no CTA waits for another.  Spike counts go to global memory with
+// integer reductions.
+template <int MS>
+__device__ __forceinline__ uint32_t outSpikes(const uint32_t *outC, uint32_t n, uint32_t stride, uint32_t abN,
+		uint32_t *goCount)
+{
+	if (!abN) return 0;
+	if constexpr (MS > 0) {
+#pragma unroll
+		for (uint32_t s = 0; s < (uint32_t)MS; s++) {
+			if (s >= n) break;
+			const uint32_t c = outC[s * stride];
+			const uint32_t dl = c & 0xFFu;
+			if (dl < 32u && ((abN >> dl) & 1u)) atomicAdd(&goCount[c >> 8], 1u);
+		}
+	} else {
+#pragma unroll 4
+		for (uint32_t s = 0; s < n; s++) {
+			const uint32_t c = outC[s * stride];
+			const uint32_t dl = c & 0xFFu;
+			if (dl < 32u && ((abN >> dl) & 1u)) atomicAdd(&goCount[c >> 8], 1u);
+		}
+	}
+	return 0;
+}
+
+template <int W, int S, int MINB, int MS>
+__global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(const DevNet *const *nets,
+		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
+{
+	(void)blockOffset; (void)numNets;
+	constexpr uint32_t R = 2 * W;
+	const DevNet *__restrict__ N = nets[0];
+	const uint64_t t = *N->tBase + 1 + stepOffset;
+
+	const uint32_t P = N->P, bs = N->bs, K = N->K, Z = N->numZones, numPC = N->numPC;
+	const uint32_t rows = 2 * K, unitsPerTile = rows / R, tilesPerPC = N->tilesPerPC;
+	const uint32_t numUnits = numPC * tilesPerPC * unitsPerTile;
+	const uint32_t nMFSlots = N->nMFSlots, nGOSlots = N->nGOSlots, nOutSlots = N->nOutSlots;
+	const PassLayout L = passLayout(R, nMFSlots, nGOSlots, nOutSlots, Z);
+
+	extern __shared__ uint8_t passSmemRaw[];
+	uint8_t *stages = passSmemRaw + ((128u - (tma::smemAddr(passSmemRaw) & 127u)) & 127u);
+	uint64_t *full = reinterpret_cast<uint64_t *>(stages + (size_t)S * L.bytes);
+	uint64_t *empty = full + S;
+	float *sStepW = reinterpret_cast<float *>(empty + S);        // [numPC][Z] plasticity steps
+	uint8_t *sMF = reinterpret_cast<uint8_t *>(sStepW + (size_t)numPC * Z);
+	uint8_t *sGO = sMF + 32u * N->mfWords;
+
+	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < S; s++) {
+			tma::mbarInit(&full[s], 1);
+			tma::mbarInit(&empty[s], W);
+		}
+		tma::fenceBarrierInit();
+	}
+	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
+	const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
+	for (uint32_t i = threadIdx.x; i < 32u * N->mfWords; i += blockDim.x) sMF[i] = (uint8_t)spikeBit(mfSrc, i);
+	for (uint32_t i = threadIdx.x; i < 32u * N->goWords; i += blockDim.x) sGO[i] = (uint8_t)spikeBit(goSrc, i);
+	if (plastStep) {
+		for (uint32_t i = threadIdx.x; i < numPC * Z; i += blockDim.x) {
+			const uint32_t pc = i / Z, z = i % Z;
+			const uint8_t sel = N->zones[z].plastSel[(t & 1) * N->numIO + N->zones[z].ioOfPC[pc]];
+			sStepW[i] = sel == 1 ? N->ctl->ltdStep[z] : (sel == 2 ? N->ctl->ltpStep[z] : 0.0f);
+		}
+	}
+	__syncthreads();
+
+	if (warp == W) {
+		// ---- producer
+		if (lane == 0) {
+			const CUtensorMap *maps = N->passMaps;
+			for (int m = 0; m < PM_W0 + (int)Z; m++) tma::prefetchMap(&maps[m]);
+			const uint32_t tx = L.txBase + (plastStep ? L.txHist : 0u);
+			uint32_t issued = 0, slot = 0, phase = 0;
+			bool ok = true;
+			for (uint32_t u = blockIdx.x; u < numUnits; u += gridDim.x) {
+				if (issued >= (uint32_t)S && !tma::waitBounded(&empty[slot], phase ^ 1u, kPassWaitLimitNs)) { ok = false; break; }
+				const uint32_t tile = u / unitsPerTile, chunk = u % unitsPerTile;
+				const uint32_t pc = tile / tilesPerPC, jt = tile % tilesPerPC;
+				uint8_t *b = stages + (size_t)slot * L.bytes;
+				uint64_t *bar = &full[slot];
+				tma::arriveExpectTx(bar, tx);
+				const int32_t x = (int32_t)(jt * 32u), y = (int32_t)(pc * rows + chunk * R);
+#pragma unroll
+				for (int m = PM_V; m <= PM_APBUF; m++) tma::load2d(b + (uint32_t)m * 128u * R, &maps[m], x, y, bar);
+				tma::load3d(b + L.mfIdx, &maps[PM_MFIDX], x, y, 0, bar);
+				tma::load3d(b + L.goIdx, &maps[PM_GOIDX], x, y, 0, bar);
+				tma::load3d(b + L.outCon, &maps[PM_OUTCON], x, y, 0, bar);
+				tma::load2d(b + L.pfDelay, &maps[PM_PFDELAY], x, y, bar);
+				for (uint32_t z = 0; z < Z; z++) tma::load2d(b + L.w + z * 128u * R, &maps[PM_W0 + z], x, y, bar);
+				if (plastStep) tma::load2d(b + L.hist, &maps[PM_HIST], x, y, bar);
+				issued++;
+				if (++slot == (uint32_t)S) { slot = 0; phase ^= 1u; }
+			}
+			if (!ok) {
+				atomicOr(N->errFlag, kErrPassWait);
+				for (uint32_t k = issued > (uint32_t)S ? issued - S : 0; k < issued; k++)
+					tma::waitBounded(&full[k % S], (k / S) & 1u, kPassWaitLimitNs);
+			}
+		}
+		return;
+	}
+
+	// ---- consumers
+	const float gLeak = N->gLeakGR, eLeak = N->eLeakGR, eGOIn = N->eGOGR;
+	const float threshBase = N->threshRestGR, threshMax = N->threshMaxGR, threshDecay = N->threshDecGR;
+	const float gDecMF = N->gDecMFtoGR, gIncMF = N->gIncMFtoGR, gDecGO = N->gDecGOtoGR, gIncGO = N->gIncGOtoGR;
+	uint32_t *goCount = N->goCount + (size_t)(t & 1) * N->numGO;
+	const uint32_t buf = (uint32_t)(t % 3);
+	uint32_t *bcOut = N->bcCount + (size_t)buf * N->numBC;
+	uint32_t *scOut = N->scCount + (size_t)buf * N->numSC;
+	const uint32_t bcShift = N->bcShift, scShift = N->scShift;
+	const bool bcWarpUniform = (1u << bcShift) >= 32u, scWarpUniform = (1u << scShift) >= 32u;
+	float *const vGR = N->vGR, *const gKCaGR = N->gKCaGR, *const threshGR = N->threshGR;
+	float *const gESum = N->gESum, *const gISum = N->gISum;
+	uint32_t *const apBufGR = N->apBufGR;
+	uint64_t *const historyGR = N->historyGR;
+	const uint32_t pairParity = (uint32_t)(t & 1), pairStride = numPC * K * bs;
+
+	// running sums of step t-1 from its pair sums, in the reference's order
+	{
+		const uint32_t prevBuf = (uint32_t)((t - 1) % 3);
+		const float *prevPairs = nullptr;
+		for (uint32_t c = blockIdx.x * (W * 32u) + threadIdx.x; c < Z * numPC * bs; c += gridDim.x * (W * 32u)) {
+			const uint32_t z = c / (numPC * bs), r = c % (numPC * bs), pc = r / bs, j = r % bs;
+			prevPairs = N->zones[z].pairSum + (size_t)(pairParity ^ 1u) * pairStride + (size_t)pc * K * bs + j;
+			float sum = 0;
+#pragma unroll 8
+			for (uint32_t k2 = 0; k2 < K; k2++) sum += prevPairs[(size_t)k2 * bs];
+			N->zones[z].pcPartial[((size_t)prevBuf * numPC + pc) * bs + j] = sum;
+		}
+	}
+	uint32_t slot = 0, phase = 0;
+
+	for (uint32_t u = blockIdx.x; u < numUnits; u += gridDim.x) {
+		const bool ready = tma::waitBounded(&full[slot], phase, kPassWaitLimitNs);
+		if (!__all_sync(0xffffffffu, ready)) {
+			if (lane == 0) atomicOr(N->errFlag, kErrPassWait);
+			break;
+		}
+		const uint32_t tile = u / unitsPerTile, chunk = u % unitsPerTile;
+		const uint32_t pc = tile / tilesPerPC, jt = tile % tilesPerPC;
+		const uint32_t kk = (chunk * R) / 2 + warp;            // reduction step of this warp's row pair
+		const uint32_t col = jt * 32u + lane;                  // reduction thread index j
+		const uint8_t *b = stages + (size_t)slot * L.bytes;
+		float x[2][kMaxZones];
+		uint32_t pfs[2];
+#pragma unroll
+		for (int q = 0; q < 2; q++) {
+			const uint32_t rr = 2 * warp + q;                  // row within the unit
+			const uint32_t e = rr * 32u + lane;
+			const uint32_t g = pc * P + (chunk * R + rr) * bs + col;
+			const float *sF = reinterpret_cast<const float *>(b);
+			const float v = sF[0 * 32 * R + e];
+			const float gk = sF[1 * 32 * R + e];
+			const float th = sF[2 * 32 * R + e];
+			const float gE = sF[3 * 32 * R + e];
+			const float gI = sF[4 * 32 * R + e];
+			const uint32_t ab = reinterpret_cast<const uint32_t *>(b)[5 * 32 * R + e];
+			const uint16_t *mfI = reinterpret_cast<const uint16_t *>(b + L.mfIdx) + e;
+			const uint16_t *goI = reinterpret_cast<const uint16_t *>(b + L.goIdx) + e;
+			const uint32_t *outC = reinterpret_cast<const uint32_t *>(b + L.outCon) + e;
+			const uint32_t d = (b + L.pfDelay)[e];
+			const uint64_t h = plastStep ? reinterpret_cast<const uint64_t *>(b + L.hist)[e] : 0ull;
+			const int cntMF = countSpikes<MS>(sMF, mfI, nMFSlots, 32 * R);
+			const int cntGO = countSpikes<MS>(sGO, goI, nGOSlots, 32 * R);
+
+			// calcActivityGRGPU (kernels.cu:79-110)
+			const float tempV = v + (gLeak + gk * gk * gk * gk) * (eLeak - v) - (gE) * v + (gI) * (eGOIn - v);
+			const float tempThresh = th + (threshBase - th) * threshDecay;
+			const unsigned int tempAP = tempV > tempThresh;
+			const float thN = tempAP * threshMax + (!tempAP) * tempThresh;
+			const float gkd = gk * 0.9999f;
+			const float gkN = tempAP * (gkd + 0.003f) + (!tempAP) * gkd;
+			const uint32_t abN = (ab << 1) | tempAP;
+			// updateGRInOPGPU for MF (this step's spikes) and GO (last step's)
+			const float gEN = gE * gDecMF + gIncMF * (cntMF);
+			const float gIN = gI * gDecGO + gIncGO * (cntGO);
+			vGR[g] = tempV;
+			gKCaGR[g] = gkN;
+			threshGR[g] = thN;
+			gESum[g] = gEN;
+			gISum[g] = gIN;
+			apBufGR[g] = abN;
+			// plasticity (phase 1) before this step's PF->PC output (phase 2)
+			const uint32_t pf = d < 32u ? (abN >> d) & 1u : 0u;
+#pragma unroll
+			for (uint32_t z = 0; z < kMaxZones; z++) {
+				x[q][z] = 0.0f;
+				if (z >= Z) continue;
+				float w = reinterpret_cast<const float *>(b + L.w)[z * 32 * R + e];
+				if (plastStep) {
+					w = w + ((h & 0x0000008000000000ull) > 0) * sStepW[pc * Z + z];
+					w = (w > 0) * w;
+					w = (w > 1) + (w <= 1) * w;
+					N->zones[z].w[g] = w;
+				}
+				x[q][z] = w * pf;
+			}
+			if (plastStep) historyGR[g] = (h << 1) | ((abN & 0x0000001Fu) > 0);
+			// GR->GO synapses whose delayed spike arrives now
+			outSpikes<MS>(outC, nOutSlots, 32 * R, abN, goCount);
+			pfs[q] = pf;
+		}
+		__syncwarp();
+		if (lane == 0) tma::arrive(&empty[slot]);
+		if (++slot == (uint32_t)S) { slot = 0; phase ^= 1u; }
+
+		// x[i] + x[i+bs] of reduction step kk, per zone
+#pragma unroll
+		for (uint32_t z = 0; z < kMaxZones; z++) {
+			if (z >= Z) break;
+			N->zones[z].pairSum[(size_t)pairParity * pairStride + ((size_t)pc * K + kk) * bs + col] = x[0][z] + x[1][z];
+		}
+		// PF->BC and PF->SC counts
+#pragma unroll
+		for (int q = 0; q < 2; q++) {
+			const uint32_t g = pc * P + (chunk * R + 2 * warp + q) * bs + col;
+			const uint32_t pf = pfs[q];
+			if (!bcWarpUniform && pf) atomicAdd(&bcOut[g >> bcShift], 1u);
+			if (!scWarpUniform && pf) atomicAdd(&scOut[g >> scShift], 1u);
+			const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, pf != 0));
+			if (lane == 0 && cnt) {
+				if (bcWarpUniform) atomicAdd(&bcOut[g >> bcShift], cnt);
+				if (scWarpUniform) atomicAdd(&scOut[g >> scShift], cnt);
+			}
+		}
+	}
+}
+
+#define CBM_PASS_PERSIST_CONFIGS(X) \
+	X(4, 4, 2, 4) X(4, 3, 3, 4) X(2, 4, 4, 4) X(2, 6, 3, 4) X(8, 2, 2, 4) X(4, 4, 2, 0) X(2, 4, 2, 0) X(1, 4, 2, 0)
+#define CBM_PASS_PERSIST_INST(W, S, B, M) \
+	template __global__ void grPassPersistentKernel<W, S, B, M>(const DevNet *const *, const uint32_t *, int, uint32_t);
+CBM_PASS_PERSIST_CONFIGS(CBM_PASS_PERSIST_INST)
+
+const void *passPersistentKernelFor(int W, int S, int B, int M)
+{
+#define CBM_PASS_PERSIST_PICK(w, s, b, m) \
+	if (W == w && S == s && B == b && M == m) return (const void *)&grPassPersistentKernel<w, s, b, m>;
+	CBM_PASS_PERSIST_CONFIGS(CBM_PASS_PERSIST_PICK)
+#undef CBM_PASS_PERSIST_PICK
 	return nullptr;
 }
 

@@ -444,6 +444,7 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 		DevZone &Q = h.zones[z];
 		Q.w = upF("pfSynWeightPC", z);
 		Q.pcPartial = alloc<float>((size_t)3 * c.numPC * h.bs);
+		Q.pairSum = alloc<float>((size_t)2 * c.numPC * h.K * h.bs);
 		Q.plastSel = alloc<uint8_t>((size_t)2 * c.numIO);
 		std::vector<uint32_t> ioOfPC(c.numPC);
 		uint32_t cur = 0;
@@ -825,11 +826,53 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 		for (const int *c : cand)
 			if ((uint32_t)(c[0] * c[1]) <= minRows) { W = c[0]; RW = c[1]; S = c[2]; B = c[3]; M = c[4]; tma = true; break; }
 	}
+	// A single network may run the persistent TMA pass instead: W consumer
+	// warps (2W rows per unit), S stages, B resident CTAs per SM, slot bound
+	// M, chosen with CBM_PASS_PERSIST="W,S,B,M".
+	if (tma && nets_.size() == 1) {
+		int pW = 2, pS = 4, pB = 4, pM = maxSlots <= 4 ? 4 : 0;
+		if (pM == 0) pB = 2;
+		bool persist = false;  // measured slower than the per-tile pass on the 1M network
+		if (const char *env = getenv("CBM_PASS_PERSIST")) {
+			if (!strcmp(env, "0")) persist = false;
+			else if (sscanf(env, "%d,%d,%d,%d", &pW, &pS, &pB, &pM) != 4 || !passPersistentKernelFor(pW, pS, pB, pM) ||
+					(pM > 0 && maxSlots > (uint32_t)pM))
+				return "CBM_PASS_PERSIST names a geometry that is not compiled in or does not fit the network";
+			else persist = true;
+		}
+		while (persist && (uint32_t)(2 * pW) > minRows) pW /= 2;
+		if (persist && pW >= 1 && !passPersistentKernelFor(pW, pS, pB, pM)) { pS = 4; pB = 2; pM = 0; }
+		const void *fn = persist && pW >= 1 ? passPersistentKernelFor(pW, pS, pB, pM) : nullptr;
+		if (fn) {
+			Network &n = *nets_[0];
+			const uint32_t R = (uint32_t)(2 * pW);
+			const PassLayout L = passLayout(R, n.dev().nMFSlots, n.dev().nGOSlots, n.dev().nOutSlots, n.dev().numZones);
+			const size_t smem = 128 + (size_t)pS * L.bytes + 16ull * pS + 4ull * n.dev().numPC * n.dev().numZones +
+				32ull * (n.dev().mfWords + n.dev().goWords);
+			if (smem <= 227 * 1024) {
+				CKS(n.buildPassMaps(R));
+				CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "pass smem");
+				int perSM = 0, numSMs = 0;
+				CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, 32 * (pW + 1), smem), "pass occupancy");
+				CK(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device), "SM count");
+				const uint32_t units = n.dev().numPC * n.dev().tilesPerPC * (n.passRows() / R);
+				passTmaFn_ = fn;
+				passTmaW_ = (uint32_t)pW;
+				passTmaR_ = R;
+				passTmaS_ = (uint32_t)pS;
+				passTmaSmem_ = smem;
+				passGrid_ = std::min<uint32_t>(units, (uint32_t)std::max(1, perSM) * (uint32_t)numSMs);
+				passPersistent_ = true;
+				return "";
+			}
+		}
+	}
 	if (tma) {
 		const uint32_t R = (uint32_t)(W * RW);
 		size_t smem = 0;
 		for (Network *n : nets_) smem = std::max(smem, n->passTmaSmemBytes(R, (uint32_t)S));
 		if (smem <= 227 * 1024) {
+			passGrid_ = passBlocks_;
 			for (Network *n : nets_) CKS(n->buildPassMaps(R));
 			passTmaFn_ = passTmaKernelFor(W, RW, S, B, M);
 			passTmaW_ = (uint32_t)W;
@@ -866,7 +909,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	uint32_t stepArg = k;
 	if (passTmaFn_) {
 		void *args[] = {&netsArg, &offsArg, &numNetsArg, &stepArg};
-		CK(cudaLaunchKernel(passTmaFn_, dim3(passBlocks_), dim3(32 * (passTmaW_ + 1)), args, passTmaSmem_, s0_),
+		CK(cudaLaunchKernel(passTmaFn_, dim3(passGrid_), dim3(32 * (passTmaW_ + 1)), args, passTmaSmem_, s0_),
 				"launching the GR pass");
 	} else {
 		grPassKernel<<<passBlocks_, kPassThreads, passSmem_, s0_>>>(netsArg, offsArg, numNetsArg, stepArg);

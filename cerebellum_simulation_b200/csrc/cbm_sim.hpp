@@ -78,7 +78,8 @@ private:
 	size_t passSmem_ = 0, tailSmem_ = 0;
 	// TMA GR pass geometry (passTmaFn_ null: the plain pass kernel runs)
 	const void *passTmaFn_ = nullptr;
-	uint32_t passTmaW_ = 0, passTmaR_ = 0, passTmaS_ = 0;
+	uint32_t passTmaW_ = 0, passTmaR_ = 0, passTmaS_ = 0, passGrid_ = 0;
+	bool passPersistent_ = false;
 	size_t passTmaSmem_ = 0;
 	cudaGraphExec_t graphExec_ = nullptr;
 	uint32_t graphChunk_ = 0;

@@ -1,7 +1,8 @@
-"""Every compiled geometry of the TMA GR pass (consumer warps x rows per warp
-x stages x resident CTAs x slot bound) gives the same network state, bit for
-bit, as the plain GR pass kernel; the plain kernel is pinned to the oracle by
-test_gpu_parity.py."""
+"""Every compiled geometry of the two TMA GR passes gives the same network
+state, bit for bit, as the plain GR pass kernel (the plain kernel is pinned
+to the oracle by test_gpu_parity.py): the per-tile pass (consumer warps x
+rows per warp x stages x resident CTAs x slot bound) and the persistent pass
+(consumer warps x stages x resident CTAs x slot bound)."""
 import os
 
 import numpy as np
@@ -11,22 +12,24 @@ import cbmtest
 
 pytestmark = pytest.mark.gpu
 
-GEOMETRIES = ["8,1,3,2,4", "8,1,3,3,4", "8,1,4,2,4", "8,1,2,3,4", "4,1,4,4,4", "4,2,3,3,4", "4,2,4,2,4",
-              "8,1,3,2,0", "4,1,4,1,0", "2,1,4,1,0", "1,1,4,1,0"]
+TILE_GEOMETRIES = ["8,1,3,2,4", "8,1,3,3,4", "8,1,4,2,4", "8,1,2,3,4", "4,1,4,4,4", "4,2,3,3,4", "4,2,4,2,4",
+                   "8,1,3,2,0", "4,1,4,1,0", "2,1,4,1,0", "1,1,4,1,0"]
+PERSISTENT_GEOMETRIES = ["4,4,2,4", "4,3,3,4", "2,4,4,4", "2,6,3,4", "8,2,2,4", "4,4,2,0", "2,4,2,0", "1,4,2,0"]
 EVENTS = {1: [("plast", 0, -0.002, 0.002)], 60: [("errdrive", 0, 1.0)], 90: [("grgoinc", 0.01)]}
 
 
-def run_with(geometry, state_path, mf, out_path):
+def run_with(env, state_path, mf, out_path):
     import cerebellum_simulation_b200 as cbm
-    old = os.environ.get("CBM_PASS_TMA")
-    os.environ["CBM_PASS_TMA"] = geometry
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         sim = cbm.CBMSimCore(cbm.CBMState(state_path), [3], device=0)
     finally:
-        if old is None:
-            del os.environ["CBM_PASS_TMA"]
-        else:
-            os.environ["CBM_PASS_TMA"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
     cbmtest.product_run(sim, mf, EVENTS, record=False)
     sim.writeToState(out_path)
     sim.close()
@@ -43,7 +46,10 @@ def test_tma_pass_geometries_match_plain_pass(tmp_path):
     path = str(tmp_path / "net.state")
     st.writeState(path)
     mf = networks.uniform_mf_stream(1024, 120, seed=5, lo=5.0, hi=60.0)
-    want = run_with("0", path, mf, str(tmp_path / "plain.state"))
-    for g in GEOMETRIES:
-        got = run_with(g, path, mf, str(tmp_path / f"tma_{g}.state"))
-        assert got == want, f"geometry {g} differs from the plain pass"
+    want = run_with({"CBM_PASS_TMA": "0"}, path, mf, str(tmp_path / "plain.state"))
+    for g in TILE_GEOMETRIES:
+        got = run_with({"CBM_PASS_TMA": g, "CBM_PASS_PERSIST": "0"}, path, mf, str(tmp_path / f"tma_{g}.state"))
+        assert got == want, f"per-tile geometry {g} differs from the plain pass"
+    for g in PERSISTENT_GEOMETRIES:
+        got = run_with({"CBM_PASS_PERSIST": g}, path, mf, str(tmp_path / f"persist_{g}.state"))
+        assert got == want, f"persistent geometry {g} differs from the plain pass"
