@@ -87,8 +87,12 @@ def _load():
         "cbm_sim_load_mf_stream": (I, [P, P, U64]),
         "cbm_sim_run": (I, [P, U64, U32, ctypes.POINTER(F), ctypes.POINTER(F)]),
         "cbm_sim_algorithmic_bytes_per_step": (D, [P]),
+        "cbm_sim_layout_bytes_per_step": (D, [P]),
+        "cbm_sim_pass_geometry": (I, [P, ctypes.POINTER(U32), ctypes.POINTER(U32), ctypes.POINTER(U32),
+                                      ctypes.POINTER(U32)]),
         "cbm_sim_timer_start": (I, [P]),
         "cbm_sim_last_tail_ms": (I, [P, ctypes.POINTER(F)]),
+        "cbm_sim_run_flushed": (I, [P, U64, U64, ctypes.POINTER(F)]),
         "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_destroy": (None, [P]),
         "cbm_device_expf": (I, [I, P, P, U64]),
@@ -320,6 +324,23 @@ class CBMSimCore:
 
     def algorithmic_bytes_per_step(self):
         return lib.cbm_sim_algorithmic_bytes_per_step(self._h)
+
+    def run_flushed(self, nsteps, flush_bytes):
+        """nsteps steps, each after an L2 flush (a write of flush_bytes); the
+        summed device time of the steps alone, in ms."""
+        ms = ctypes.c_float()
+        _check(lib.cbm_sim_run_flushed(self._h, nsteps, flush_bytes, ctypes.byref(ms)))
+        return ms.value
+
+    def layout_bytes_per_step(self):
+        return lib.cbm_sim_layout_bytes_per_step(self._h)
+
+    def pass_geometry(self):
+        """(kernel name, consumer warps, rows per stage, stages) of the GR pass."""
+        v = [ctypes.c_uint32() for _ in range(4)]
+        _check(lib.cbm_sim_pass_geometry(self._h, *[ctypes.byref(x) for x in v]))
+        kind = ("grPassKernel", "grPassTmaKernel", "grPassPersistentKernel")[v[0].value]
+        return kind, v[1].value, v[2].value, v[3].value
 
 
 def mf_bits(mf_bytes, words):

@@ -315,6 +315,13 @@ int cbm_sim_run(cbm_sim *sim, uint64_t nsteps, uint32_t chunk, float *gpuMs, flo
 	return CBM_OK;
 }
 
+int cbm_sim_run_flushed(cbm_sim *sim, uint64_t nsteps, uint64_t flushBytes, float *stepMs)
+{
+	NEED(sim); NEED(stepMs);
+	TRY(sim->sim.runFlushed(nsteps, (size_t)flushBytes, stepMs));
+	return CBM_OK;
+}
+
 int cbm_sim_last_tail_ms(cbm_sim *sim, float *ms)
 {
 	NEED(sim); NEED(ms);
@@ -339,6 +346,19 @@ int cbm_sim_timer_stop(cbm_sim *sim, float *ms)
 double cbm_sim_algorithmic_bytes_per_step(cbm_sim *sim)
 {
 	return sim ? NET(sim).bytesPerStepAlgorithmic() : 0.0;
+}
+
+double cbm_sim_layout_bytes_per_step(cbm_sim *sim)
+{
+	return sim ? NET(sim).bytesPerStepLayout() : 0.0;
+}
+
+int cbm_sim_pass_geometry(cbm_sim *sim, unsigned *kind, unsigned *consumerWarps, unsigned *rowsPerStage,
+		unsigned *stages)
+{
+	NEED(sim); NEED(kind); NEED(consumerWarps); NEED(rowsPerStage); NEED(stages);
+	sim->sim.passGeometry(kind, consumerWarps, rowsPerStage, stages);
+	return CBM_OK;
 }
 
 void cbm_sim_destroy(cbm_sim *sim) { delete sim; }

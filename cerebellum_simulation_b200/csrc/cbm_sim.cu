@@ -230,6 +230,16 @@ double Network::bytesPerStepAlgorithmic() const
 	return (72.0 + 4.0 * avgMF_ + 4.0 * avgGO_ + 8.0 * avgOut_) * h_.numGR;
 }
 
+double Network::bytesPerStepLayout() const
+{
+	// GR state read and written (6 x 4 B each way), synapse slots (u16 MF and
+	// GO indices, u32 GR->GO targets), the PF delay byte, the PF->PC weight
+	// of every zone; history read + write and weight writes on plasticity steps
+	const double perGR = 48.0 + 2.0 * h_.nMFSlots + 2.0 * h_.nGOSlots + 4.0 * h_.nOutSlots + 1.0 + 4.0 * h_.numZones +
+		(16.0 + 4.0 * h_.numZones) / h_.tsPerHistBinGR;
+	return perGR * h_.numGR;
+}
+
 std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mfRing, uint32_t mfSeed)
 {
 	(void)mfSeed;
@@ -744,6 +754,9 @@ std::string Network::resetGOGODepression(cudaStream_t s)
 Simulator::~Simulator()
 {
 	if (graphExec_) cudaGraphExecDestroy(graphExec_);
+	if (flushGraph_) cudaGraphExecDestroy(flushGraph_);
+	if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
+	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
 	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_}) if (b->ptr) cudaFree(b->ptr);
 	if (s0_) cudaStreamDestroy(s0_);
@@ -1016,6 +1029,47 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 		}
 		lastTailMs_ = total / chunk;
 	}
+	return "";
+}
+
+std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(uploadCtl());
+	if (flushBytes && flushBytes != flushBuf_.bytes) {
+		if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
+		flushBuf_.ptr = nullptr;
+		CK(cudaMalloc(&flushBuf_.ptr, flushBytes), "allocating the L2 flush buffer");
+		flushBuf_.bytes = flushBytes;
+	}
+	if (!flushGraph_) {
+		// one step bracketed by events, after a write of the flush buffer
+		if (!stepEv0_) CK(cudaEventCreate(&stepEv0_), "event");
+		if (!stepEv1_) CK(cudaEventCreate(&stepEv1_), "event");
+		cudaGraph_t g;
+		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
+		if (flushBuf_.ptr) cudaMemsetAsync(flushBuf_.ptr, 0x5a, flushBuf_.bytes, s0_);
+		cudaEventRecordWithFlags(stepEv0_, s0_, cudaEventRecordExternal);
+		std::string e = enqueueStep(0, false);
+		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
+		cudaEventRecordWithFlags(stepEv1_, s0_, cudaEventRecordExternal);
+		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
+		if (!e.empty()) return e;
+		CK(ce, "graph capture");
+		CK(cudaGraphInstantiate(&flushGraph_, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
+		cudaGraphDestroy(g);
+	}
+	double total = 0;
+	for (uint64_t k = 0; k < nsteps; k++) {
+		CK(cudaGraphLaunch(flushGraph_, s0_), "graph launch");
+		CK(cudaEventSynchronize(stepEv1_), "step");
+		float ms = 0;
+		CK(cudaEventElapsedTime(&ms, stepEv0_, stepEv1_), "step timing");
+		total += ms;
+		for (Network *n : nets_) n->hostT_ += 1;
+	}
+	CKS(checkDeviceErrors());
+	*stepMs = (float)total;
 	return "";
 }
 

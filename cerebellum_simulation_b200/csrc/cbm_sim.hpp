@@ -50,6 +50,11 @@ public:
 	// With instrument, external events around every GR pass of the chunk
 	// give lastPassMs(): the pass's mean duration over the last replay.
 	std::string runGraph(uint64_t nsteps, uint32_t chunk, bool instrument = false);
+	// Measurement helper: nsteps single-step graph launches, each after a
+	// write of a flushBytes device buffer (an L2 flush when larger than L2),
+	// with events on the launch stream around every step only; *stepMs is
+	// the summed step time.
+	std::string runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs);
 	std::string sync();
 	cudaStream_t stream() const { return s0_; }
 	int device() const { return device_; }
@@ -62,6 +67,13 @@ public:
 	uint32_t passStages() const { return passTmaS_; }
 	// Device error word of every network (kErr* bits): non-empty on error.
 	std::string checkDeviceErrors();
+	void passGeometry(unsigned *kind, unsigned *warps, unsigned *rows, unsigned *stages) const
+	{
+		*kind = passTmaFn_ ? (passPersistent_ ? 2u : 1u) : 0u;
+		*warps = passTmaW_;
+		*rows = passTmaR_;
+		*stages = passTmaS_;
+	}
 	std::string timerStart();
 	std::string timerStop(float *ms);
 
@@ -85,6 +97,9 @@ private:
 	uint32_t graphChunk_ = 0;
 	bool graphInstrumented_ = false;
 	std::vector<cudaEvent_t> passEv_, tailEv_;
+	cudaGraphExec_t flushGraph_ = nullptr;
+	DeviceBuf flushBuf_;
+	cudaEvent_t stepEv0_ = nullptr, stepEv1_ = nullptr;
 	float lastGraphMs_ = 0, lastPassMs_ = 0, lastTailMs_ = 0;
 };
 
@@ -127,6 +142,7 @@ public:
 	uint32_t mfWords() const { return h_.mfWords; }
 	uint32_t mfRing() const { return h_.mfRing; }
 	double bytesPerStepAlgorithmic() const;  // 72 + 4 n_mf + 4 n_go + 8 n_out per GR
+	double bytesPerStepLayout() const;       // what this layout moves (see cbm_sim_layout_bytes_per_step)
 
 	HostCtl ctl{};
 	bool ctlDirty = true;

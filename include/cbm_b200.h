@@ -187,6 +187,13 @@ int cbm_sim_run(cbm_sim *sim, uint64_t nsteps, uint32_t graphChunk, float *gpuMs
 int cbm_sim_timer_start(cbm_sim *sim);
 int cbm_sim_timer_stop(cbm_sim *sim, float *ms);
 
+/* Measurement helper, no counterpart in the reference: nsteps steps with
+ * resident MF input, each launched alone after a write of a flushBytes
+ * device buffer (an L2 flush when larger than the L2 cache); *stepMs is the
+ * summed device time of the steps alone (events on the launch stream around
+ * each step). */
+int cbm_sim_run_flushed(cbm_sim *sim, uint64_t nsteps, uint64_t flushBytes, float *stepMs);
+
 /* Mean duration of the small-cell update kernel over the last chunk of the
  * last cbm_sim_run that timed the GR pass (0 before). */
 int cbm_sim_last_tail_ms(cbm_sim *sim, float *ms);
@@ -194,6 +201,19 @@ int cbm_sim_last_tail_ms(cbm_sim *sim, float *ms);
 /* Algorithmic HBM bytes of one step: (72 + 4 n_mf + 4 n_go + 8 n_out) per GR
  * with the network's mean synapse counts. */
 double cbm_sim_algorithmic_bytes_per_step(cbm_sim *sim);
+
+/* Bytes the GR pass moves per step with this library's layout (16-bit
+ * synapse indices, 8-bit delays, packed GR->GO targets): reads and writes of
+ * the GR state, indices, delays and weights, history and weight writes every
+ * tsPerHistBinGR steps averaged.  No counterpart in the reference. */
+double cbm_sim_layout_bytes_per_step(cbm_sim *sim);
+
+/* Which GR-pass kernel runs: *kind 0 = plain (one warp-row per load), 1 =
+ * TMA-pipelined per tile, 2 = TMA-pipelined persistent; *consumerWarps,
+ * *rowsPerStage, *stages describe the TMA pipeline (0 for the plain kernel).
+ * No counterpart in the reference. */
+int cbm_sim_pass_geometry(cbm_sim *sim, unsigned *kind, unsigned *consumerWarps, unsigned *rowsPerStage,
+		unsigned *stages);
 
 void cbm_sim_destroy(cbm_sim *sim);
 
