@@ -1402,6 +1402,8 @@ __device__ void stageOut(const DevNet *N, const uint8_t *arena, const StageSeg *
 // copy in and out per step instead of a global round trip per phase).
 __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, uint32_t stepOffset)
 {
+	// the GR pass of the same step may launch once these CTAs are resident
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 	const DevNet *__restrict__ N = nets[blockIdx.x >> 1];
 	const uint64_t t = *N->tBase + 1 + stepOffset;
 	extern __shared__ __align__(16) uint32_t tailSmem[];

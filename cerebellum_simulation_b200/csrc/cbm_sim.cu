@@ -913,27 +913,62 @@ std::string Simulator::uploadCtl()
 
 std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 {
-	CK(cudaEventRecord(fork_, s0_), "fork");
-	CK(cudaStreamWaitEvent(s1_, fork_, 0), "fork");
-	if (instrument) CK(cudaEventRecordWithFlags(passEv_[2 * k], s0_, cudaEventRecordExternal), "pass timing");
 	const DevNet *const *netsArg = (const DevNet *const *)dNetPtrs_.ptr;
 	const uint32_t *offsArg = (const uint32_t *)dBlockOffset_.ptr;
 	int numNetsArg = (int)nets_.size();
 	uint32_t stepArg = k;
-	if (passTmaFn_) {
-		void *args[] = {&netsArg, &offsArg, &numNetsArg, &stepArg};
-		CK(cudaLaunchKernel(passTmaFn_, dim3(passGrid_), dim3(32 * (passTmaW_ + 1)), args, passTmaSmem_, s0_),
-				"launching the GR pass");
-	} else {
-		grPassKernel<<<passBlocks_, kPassThreads, passSmem_, s0_>>>(netsArg, offsArg, numNetsArg, stepArg);
+	auto launchPass = [&](cudaStream_t st, bool dependent) -> std::string {
+		if (passTmaFn_) {
+			void *args[] = {&netsArg, &offsArg, &numNetsArg, &stepArg};
+			cudaLaunchConfig_t cfg = {};
+			cfg.gridDim = dim3(passGrid_);
+			cfg.blockDim = dim3(32 * (passTmaW_ + 1));
+			cfg.dynamicSmemBytes = passTmaSmem_;
+			cfg.stream = st;
+			cudaLaunchAttribute attr;
+			attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+			attr.val.programmaticStreamSerializationAllowed = 1;
+			cfg.attrs = &attr;
+			cfg.numAttrs = dependent ? 1 : 0;
+			CK(cudaLaunchKernelExC(&cfg, passTmaFn_, args), "launching the GR pass");
+		} else {
+			cudaLaunchConfig_t cfg = {};
+			cfg.gridDim = dim3(passBlocks_);
+			cfg.blockDim = dim3(kPassThreads);
+			cfg.dynamicSmemBytes = passSmem_;
+			cfg.stream = st;
+			cudaLaunchAttribute attr;
+			attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+			attr.val.programmaticStreamSerializationAllowed = 1;
+			cfg.attrs = &attr;
+			cfg.numAttrs = dependent ? 1 : 0;
+			CK(cudaLaunchKernelEx(&cfg, grPassKernel, netsArg, offsArg, numNetsArg, stepArg), "launching the GR pass");
+		}
+		return "";
+	};
+	if (instrument) {
+		// fork/join on two streams with external events around each kernel
+		CK(cudaEventRecord(fork_, s0_), "fork");
+		CK(cudaStreamWaitEvent(s1_, fork_, 0), "fork");
+		CK(cudaEventRecordWithFlags(passEv_[2 * k], s0_, cudaEventRecordExternal), "pass timing");
+		CKS(launchPass(s0_, false));
+		CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
+		CK(cudaEventRecordWithFlags(tailEv_[2 * k], s1_, cudaEventRecordExternal), "tail timing");
+		tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>(netsArg, k);
+		CK(cudaGetLastError(), "launching the small-cell update");
+		CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
+		CK(cudaEventRecord(join_, s1_), "join");
+		CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
+		return "";
 	}
-	CK(cudaGetLastError(), "launching the GR pass");
-	if (instrument) CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
-	if (instrument) CK(cudaEventRecordWithFlags(tailEv_[2 * k], s1_, cudaEventRecordExternal), "tail timing");
-	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>((const DevNet *const *)dNetPtrs_.ptr, k);
+	// One stream: the small-cell CTAs launch first and let the GR pass start
+	// as soon as they are resident (programmatic dependent launch; the two
+	// kernels of a step share no buffer), so the pass cannot take the SMs the
+	// small-cell CTAs need.  The next step waits for both.
+	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s0_>>>(netsArg, k);
 	CK(cudaGetLastError(), "launching the small-cell update");
-	if (instrument) CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
-	CK(cudaEventRecord(join_, s1_), "join");
+	CK(cudaEventRecord(join_, s0_), "join");
+	CKS(launchPass(s0_, true));
 	CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
 	return "";
 }
