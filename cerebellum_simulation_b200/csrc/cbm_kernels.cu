@@ -952,6 +952,12 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 // the MF bookkeeping of updateMFInput (innet.cpp:800-815) and resetMFHist
 // (:982-995), and every microzone update and fan-out (mzone.cpp:167-605).
 // Reads the PF sums of pass(t-2).
+// Barrier among the `count` threads of a warp group (barrier id >= 1).
+__device__ __forceinline__ void barSync(uint32_t id, uint32_t count)
+{
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 {
 	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u, warp = tid >> 5, nWarps = nThr >> 5;
@@ -971,6 +977,15 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	for (uint32_t i = tid; i < N->mfWords; i += nThr) sMF[i] = mfW[i];
 	__syncthreads();
 
+	// The PC/BC/SC/MF updates (warps [0, half)) and the NC/IO updates (warps
+	// [half, all)) of a step do not read each other's results; the two warp
+	// groups run them side by side and meet before the outputs.
+	const uint32_t half = nWarps / 2, gThr = half * 32u;
+	const bool groupA = warp < half;
+	const uint32_t gTid = groupA ? tid : tid - gThr, gWarp = groupA ? warp : warp - half;
+	if (groupA) {
+	// (tid, nThr, warp, nWarps) of the PC/BC/SC/MF warp group
+	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
 	// ---- phase 1 (cbmsimcore.cpp:192-200): PC and BC per zone, SC, and the
 	// MF bookkeeping.  The updates are independent; they run in rounds in
 	// which every thread first loads the inputs of its BC, SC and MF cells,
@@ -1090,10 +1105,14 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 			N->apBufMF[c] = (mApBuf << 1) | (m * 0x00000001u);
 		}
 	}
-	__syncthreads();
+	barSync(1, gThr);
 	for (uint32_t i = tid; i < numBC; i += nThr) N->bcCount[(size_t)R * numBC + i] = 0;
 	for (uint32_t i = tid; i < numSC; i += nThr) N->scCount[(size_t)R * numSC + i] = 0;
+	}
 
+	if (!groupA) {
+	// (tid, nThr, warp, nWarps) of the NC/IO warp group
+	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
 	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
 	// calcNCActivities (mzone.cpp:341-407) one warp per NC
 	// NC->IO conductances (one thread per synapse) and MF->NC synaptic
@@ -1146,7 +1165,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 			}
 		}
 	}
-	__syncthreads();
+	barSync(2, gThr);
 	for (uint32_t task = warp; task < Z * numNC; task += nWarps) {
 		const uint32_t z = task / numNC, i = task % numNC;
 		const DevZone &Q = N->zones[z];
@@ -1189,7 +1208,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 			Q.threshNC[i] = ap * N->threshMaxNC + (!ap) * th;
 		}
 	}
-	__syncthreads();
+	barSync(2, gThr);
 	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
 		const uint32_t z = task / numIO, i = task % numIO;
 		const DevZone &Q = N->zones[z];
@@ -1205,6 +1224,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 		Q.apIO[i] = ap;
 		Q.apBufIO[i] = (apBuf << 1) | (ap * 0x00000001u);
 		Q.threshIO[i] = N->threshMaxIO * ap + (!ap) * (th0 + N->threshDecIO * (N->threshRestIO - th0));
+	}
 	}
 	__syncthreads();
 
