@@ -93,6 +93,9 @@ def _load():
         "cbm_sim_timer_start": (I, [P]),
         "cbm_sim_last_tail_ms": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_run_flushed": (I, [P, U64, U64, ctypes.POINTER(F)]),
+        "cbm_sim_set_eyelid_protocol": (I, [P, P]),
+        "cbm_sim_trial_record_bytes": (U64, [P, I]),
+        "cbm_sim_trial_record": (I, [P, I, P, U64]),
         "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_destroy": (None, [P]),
         "cbm_device_expf": (I, [I, P, P, U64]),
@@ -325,6 +328,30 @@ class CBMSimCore:
     def algorithmic_bytes_per_step(self):
         return lib.cbm_sim_algorithmic_bytes_per_step(self._h)
 
+    def set_eyelid_protocol(self, rates, **protocol):
+        """Drive the next steps with the device eyelid protocol
+        (cbm_sim_set_eyelid_protocol); rates is [3, numMF] Hz (background, CS
+        tonic, CS phasic); keyword fields as cbm_eyelid_protocol."""
+        rates = np.ascontiguousarray(rates, dtype=np.float32)
+        p = EyelidProtocol.from_fields(rates, protocol)
+        _check(lib.cbm_sim_set_eyelid_protocol(self._h, ctypes.byref(p)))
+        self._protocol = protocol
+
+    def trial_record(self, kind):
+        """Records of the running protocol: 'nc' / 'pc' spike counts
+        [trials, bins, cells] (u32) or 'eyelid' [trials, window steps] (f32)."""
+        k = {"nc": 0, "pc": 1, "eyelid": 2}[kind]
+        n = lib.cbm_sim_trial_record_bytes(self._h, k)
+        if not n:
+            raise CBMError(1, "no protocol is running")
+        out = np.empty(n // 4, dtype=np.float32 if kind == "eyelid" else np.uint32)
+        _check(lib.cbm_sim_trial_record(self._h, k, out.ctypes.data, n))
+        p = self._protocol
+        trials = max(1, p["numDataTrials"])
+        if kind == "eyelid":
+            return out.reshape(trials, -1)
+        return out.reshape(trials, -1, self.state.con("numNC" if kind == "nc" else "numPC"))
+
     def run_flushed(self, nsteps, flush_bytes):
         """nsteps steps, each after an L2 flush (a write of flush_bytes); the
         summed device time of the steps alone, in ms."""
@@ -341,6 +368,49 @@ class CBMSimCore:
         _check(lib.cbm_sim_pass_geometry(self._h, *[ctypes.byref(x) for x in v]))
         kind = ("grPassKernel", "grPassTmaKernel", "grPassPersistentKernel")[v[0].value]
         return kind, v[1].value, v[2].value, v[3].value
+
+
+_PROTOCOL_FIELDS = [("trialSteps", ctypes.c_uint32), ("csOn", ctypes.c_int32), ("csOff", ctypes.c_int32),
+                    ("csPhasicOff", ctypes.c_int32), ("csStartTrial", ctypes.c_uint32),
+                    ("plastOnDelay", ctypes.c_int32), ("plastOffDelay", ctypes.c_int32),
+                    ("plastLTD", ctypes.c_float), ("plastLTP", ctypes.c_float), ("usErrDrive", ctypes.c_float),
+                    ("mfSeed", ctypes.c_int32), ("mfThreshDecayTau", ctypes.c_float),
+                    ("mfFreqBG", ctypes.c_void_p), ("mfFreqCSTonic", ctypes.c_void_p),
+                    ("mfFreqCSPhasic", ctypes.c_void_p), ("dataStartTrial", ctypes.c_uint32),
+                    ("numDataTrials", ctypes.c_uint32), ("preCS", ctypes.c_int32), ("postCS", ctypes.c_int32),
+                    ("binSteps", ctypes.c_uint32), ("eyeGDecayTau", ctypes.c_float), ("eyeGInc", ctypes.c_float),
+                    ("eyeGShift", ctypes.c_float), ("eyeGLeakRaw", ctypes.c_float), ("eyeMaxAmp", ctypes.c_float)]
+
+
+class EyelidProtocol(ctypes.Structure):
+    """cbm_eyelid_protocol (include/cbm_b200.h)."""
+    _fields_ = _PROTOCOL_FIELDS
+
+    @classmethod
+    def from_fields(cls, rates, fields):
+        p = cls(**{n: fields[n] for n, _ in _PROTOCOL_FIELDS if not n.startswith("mfFreq")})
+        p.mfFreqBG = rates[0].ctypes.data
+        p.mfFreqCSTonic = rates[1].ctypes.data
+        p.mfFreqCSPhasic = rates[2].ctypes.data
+        p._rates = rates  # keeps the tables alive during the call
+        return p
+
+
+def eyelid_protocol_defaults(state, **kw):
+    """The reference eyelid driver's settings (ecmanagementdelay.cpp:90-170,
+    201-235) for 5000-step trials with the CS at 2000-2500 ms: LTD step
+    -0.0005 x the LTD/LTP ratio ((csOff - csOn + msLTDStartAPIO) /
+    msLTDDurationIO, at least 0.5), LTP step 0.0005, eyelid integrator
+    (10.5, 0.012, -0.13, 0.13, 100), recording window 500 ms either side."""
+    p = dict(trialSteps=5000, csOn=2000, csOff=2500, csPhasicOff=2000, csStartTrial=0, plastOnDelay=200,
+             plastOffDelay=200, usErrDrive=1.0, mfSeed=0, mfThreshDecayTau=4.0, dataStartTrial=0,
+             numDataTrials=1, preCS=500, postCS=500, binSteps=10, eyeGDecayTau=10.5, eyeGInc=0.012,
+             eyeGShift=-0.13, eyeGLeakRaw=0.13, eyeMaxAmp=100.0, plastLTP=0.0005)
+    p.update(kw)
+    if "plastLTD" not in p:
+        ratio = ((p["csOff"] - p["csOn"]) + state.act("msLTDStartAPIO")) / state.act("msLTDDurationIO")
+        p["plastLTD"] = -0.0005 * max(ratio, 0.5)
+    return p
 
 
 def mf_bits(mf_bytes, words):

@@ -295,6 +295,7 @@ int cbm_sim_load_mf_stream(cbm_sim *sim, const uint32_t *bits, uint64_t nsteps)
 {
 	NEED(sim); NEED(bits);
 	Network &n = NET(sim);
+	if (n.hasProtocol()) return fail(CBM_ERR_ARG, "a device protocol drives the MF input of this network");
 	if (nsteps > n.mfRing()) return fail(CBM_ERR_ARG, "more MF steps than the resident ring holds");
 	// rows land in the slots of the next nsteps steps
 	const uint64_t first = n.stepsDone() % n.mfRing();
@@ -319,6 +320,25 @@ int cbm_sim_run_flushed(cbm_sim *sim, uint64_t nsteps, uint64_t flushBytes, floa
 {
 	NEED(sim); NEED(stepMs);
 	TRY(sim->sim.runFlushed(nsteps, (size_t)flushBytes, stepMs));
+	return CBM_OK;
+}
+
+int cbm_sim_set_eyelid_protocol(cbm_sim *sim, const cbm_eyelid_protocol *protocol)
+{
+	NEED(sim); NEED(protocol);
+	TRY(sim->sim.setProtocol(0, *protocol));
+	return CBM_OK;
+}
+
+uint64_t cbm_sim_trial_record_bytes(cbm_sim *sim, int kind)
+{
+	return sim ? NET(sim).recordBytes(kind) : 0;
+}
+
+int cbm_sim_trial_record(cbm_sim *sim, int kind, void *dst, uint64_t bytes)
+{
+	NEED(sim); NEED(dst);
+	TRY(NET(sim).readRecord(kind, dst, (size_t)bytes, sim->sim.stream()));
 	return CBM_OK;
 }
 

@@ -85,6 +85,40 @@ struct HostCtl {
 	uint32_t pad[3];
 };
 
+// The eyelid-conditioning trial driven on the device (the reference's
+// ECManagementDelay, Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp):
+// MF input from a Poisson regenerating population (PoissonRegenCells,
+// CBM_TOOLS_LIB_DEV/src/poissonregencells.cpp:49-66) with background / CS
+// tonic / CS phasic rates, the US error drive and the PF->PC plasticity
+// window, and the recording of the trials it keeps (NC and PC spike counts
+// per bin, the eyelid integrator's output, eyelidintegrator.cpp:50-68).
+// Steps of the protocol are numbered from startT: step t has in-trial time
+// (t - 1 - startT) % trialSteps and trial (t - 1 - startT) / trialSteps.
+struct DevProtocol {
+	uint64_t startT;
+	uint32_t trialSteps, csStartTrial;
+	int32_t csOn, csOff, csPOff, plastOn, plastOff;  // plastOn/Off: steps after csOn / csOff
+	float plastLTD, plastLTP, usErrDrive;           // usErrDrive already times maxExtIncVIO
+	float defaultLTD, defaultLTP;                   // resetGRPCPlastSteps values
+	// MF generator
+	const float *freqBG, *freqCSTonic, *freqCSPhasic;  // Hz, numMF each
+	float *mfThresh;       // regeneration state per MF
+	uint64_t mfKey;        // stream key of the MF draws
+	float sPerTS, mfThreshDecay;
+	int32_t *plastState;   // [2]: the driver's grPCPlastSet, grPCPlastReset
+	float *curSteps;       // [2]: zone 0's LTD and LTP steps in force
+	float *ctlSlots;       // [2][3]: zone 0's LTD step, LTP step and error drive per step parity
+	// recording
+	uint32_t dataStartTrial, numDataTrials, binSteps, nBins;
+	int32_t recFrom, recLen;   // in-trial window [recFrom, recFrom + recLen)
+	uint32_t *ncPSH;       // [numDataTrials][nBins][numNC]
+	uint32_t *pcPSH;       // [numDataTrials][nBins][numPC]
+	float *eyelid;         // [numDataTrials][recLen] integrator output per step
+	float *eyeG;           // [numNC] integrator conductances
+	float *eyeVm;          // [1]
+	float eyeGDecay, eyeGInc, eyeGShift, eyeGLeak, eyeMaxAmp;
+};
+
 struct DevZone {
 	float *w;           // pfSynWeightPC, PC-major (mzone.cpp:97-103)
 	float *pcPartial;   // [3][numPC][bs] per-thread partial sums of the PF->PC reduction
@@ -181,6 +215,7 @@ struct DevNet {
 	HostCtl *ctl;
 	uint32_t *errFlag;   // device error word (kErr* bits)
 	const CUtensorMap *passMaps;  // [PM_COUNT] descriptors of the TMA GR pass, or null
+	DevProtocol *proto;           // device-driven trial protocol, or null
 	const StageSeg *zoneSegs;     // arrays the microzone CTA stages in shared memory
 	uint32_t numZoneSegs;         // 0: the microzone CTA works on global memory
 	uint32_t zoneArenaBytes;

@@ -95,6 +95,23 @@ __device__ __forceinline__ uint32_t spikeBit(const uint32_t *bits, uint32_t idx)
 	return (bits[idx >> 5] >> (idx & 31u)) & 1u;
 }
 
+// Zone z's PF->PC step for plasticity selector sel (1 LTD, 2 LTP) at step t:
+// the host setters' value, or for zone 0 under a device protocol the value
+// the protocol set for step t.
+__device__ __forceinline__ float plasticityStep(const DevNet *N, uint64_t t, uint32_t z, uint8_t sel)
+{
+	if (sel == 0) return 0.0f;
+	if (z == 0 && N->proto) return N->proto->ctlSlots[(t & 1) * 3 + (sel == 1 ? 0 : 1)];
+	return sel == 1 ? N->ctl->ltdStep[z] : N->ctl->ltpStep[z];
+}
+
+// Zone z's error drive at step t (setters, or the protocol for zone 0).
+__device__ __forceinline__ float errDriveOf(const DevNet *N, uint64_t t, uint32_t z)
+{
+	if (z == 0 && N->proto) return N->proto->ctlSlots[(t & 1) * 3 + 2];
+	return N->ctl->errDrive[z];
+}
+
 __device__ __forceinline__ const DevNet *locateNet(const DevNet *const *nets, const uint32_t *blockOffset,
 		int numNets, uint32_t b, uint32_t &local)
 {
@@ -144,7 +161,7 @@ __global__ void __launch_bounds__(kPassThreads) grPassKernel(const DevNet *const
 		stepW[z] = 0.0f;
 		if (plastStep) {
 			const uint8_t sel = N->zones[z].plastSel[(t & 1) * N->numIO + N->zones[z].ioOfPC[pc]];
-			stepW[z] = sel == 1 ? N->ctl->ltdStep[z] : (sel == 2 ? N->ctl->ltpStep[z] : 0.0f);
+			stepW[z] = plasticityStep(N, t, z, sel);
 		}
 	}
 	const float gLeak = N->gLeakGR, eLeak = N->eLeakGR, eGOIn = N->eGOGR;
@@ -358,7 +375,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 			stepW[z] = 0.0f;
 			if (z < Z && plastStep) {
 				const uint8_t sel = N->zones[z].plastSel[(t & 1) * N->numIO + N->zones[z].ioOfPC[pc]];
-				stepW[z] = sel == 1 ? N->ctl->ltdStep[z] : (sel == 2 ? N->ctl->ltpStep[z] : 0.0f);
+				stepW[z] = plasticityStep(N, t, z, sel);
 			}
 		}
 		const float gLeak = N->gLeakGR, eLeak = N->eLeakGR, eGOIn = N->eGOGR;
@@ -590,7 +607,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(con
 		for (uint32_t i = threadIdx.x; i < numPC * Z; i += blockDim.x) {
 			const uint32_t pc = i / Z, z = i % Z;
 			const uint8_t sel = N->zones[z].plastSel[(t & 1) * N->numIO + N->zones[z].ioOfPC[pc]];
-			sStepW[i] = sel == 1 ? N->ctl->ltdStep[z] : (sel == 2 ? N->ctl->ltpStep[z] : 0.0f);
+			sStepW[i] = plasticityStep(N, t, z, sel);
 		}
 	}
 	__syncthreads();
@@ -1212,7 +1229,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
 		const uint32_t z = task / numIO, i = task % numIO;
 		const DevZone &Q = N->zones[z];
-		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], errDrive = ctl->errDrive[z], th0 = Q.threshIO[i];
+		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], errDrive = errDriveOf(N, t, z), th0 = Q.threshIO[i];
 		const uint32_t apBuf = Q.apBufIO[i];
 		float gNCSum = 0;
 		for (uint32_t j = 0; j < nIONC; j++) gNCSum = gNCSum + ioScratch[(size_t)task * nIONC + j];
@@ -1379,6 +1396,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	__syncthreads();
 	if ((t % N->numTSinMFHist) == 0)
 		for (uint32_t i = tid; i < numMF; i += nThr) N->histMF[i] = 0;
+	// the error drive is consumed once (mzone.cpp:334)
 	if (tid < Z) ctl->errDrive[tid] = 0;
 }
 
@@ -1416,6 +1434,110 @@ __device__ void stageOut(const DevNet *N, const uint8_t *arena, const StageSeg *
 	}
 }
 
+// ---------------------------------------------------------- trial protocol
+// Prepare step t+1 of a device protocol (in the Golgi CTA of step t, after
+// its own work): the MF spikes of step t+1 into ring slot t % mfRing
+// (PoissonRegenCells::calcActivity, poissonregencells.cpp:49-66, with the
+// rate table ECManagementDelay::calcMFActivity picks, ecmanagementdelay.cpp:
+// 175-194), and zone 0's error drive and PF->PC plasticity steps for step
+// t+1 (ECManagementDelay::calcSimActivity, ecmanagementdelay.cpp:201-235).
+// The draw of MF i for step t+1 is keyed by ((t+1) << 20) | i.
+__device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
+{
+	DevProtocol *P = N->proto;
+	const uint64_t k = t - P->startT;  // index of step t+1 within the protocol
+	const int32_t time = (int32_t)(k % P->trialSteps);
+	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const bool csTrial = trial >= P->csStartTrial;
+	const float *freq = P->freqBG;
+	if (csTrial && time >= P->csOn && time < P->csOff) freq = time < P->csPOff ? P->freqCSPhasic : P->freqCSTonic;
+	uint32_t *bits = const_cast<uint32_t *>(N->mfBits) + (size_t)(t % N->mfRing) * N->mfWords;
+	const uint64_t ctr = (t + 1) << 20;
+	const uint32_t numMF = N->numMF, words = N->mfWords;
+	for (uint32_t base = 0; base < 32u * words; base += blockDim.x) {
+		const uint32_t i = base + threadIdx.x;
+		uint32_t ap = 0;
+		if (i < numMF) {
+			float th = P->mfThresh[i];
+			const float f = freq[i];
+			th = th + (1 - th) * P->mfThreshDecay;
+			const double u = (double)rng::uniform24Keyed(P->mfKey, ctr | i);
+			ap = u < ((f * P->sPerTS) * th);
+			th = (!ap) * th;
+			P->mfThresh[i] = th;
+		}
+		const uint32_t word = __ballot_sync(0xffffffffu, ap != 0);
+		if ((threadIdx.x & 31u) == 0 && i < 32u * words) bits[i >> 5] = word;
+	}
+	if (threadIdx.x == 0) {
+		int32_t *ps = P->plastState;  // the driver's grPCPlastSet, grPCPlastReset
+		float *cur = P->curSteps;     // zone 0's LTD and LTP steps in force
+		if (time >= P->csOn + P->plastOn && !ps[0] && csTrial && time < P->csOff + P->plastOff) {
+			ps[0] = 1; ps[1] = 0;
+			cur[0] = P->plastLTD; cur[1] = P->plastLTP;
+		}
+		if (!ps[1] && time >= P->csOff + P->plastOff && csTrial) {
+			ps[0] = 0; ps[1] = 1;
+			cur[0] = P->defaultLTD; cur[1] = P->defaultLTP;
+		}
+		// step t reads the other parity's slot while this one is written
+		float *slot = P->ctlSlots + ((t + 1) & 1) * 3;
+		slot[0] = cur[0];
+		slot[1] = cur[1];
+		slot[2] = (time == P->csOff - 1 && csTrial) ? P->usErrDrive : 0.0f;
+	}
+}
+
+// Record step t of a device protocol (in the microzone CTA of step t, after
+// its own work; N may be its shared-memory copy): the eyelid integrator on
+// zone 0's NC spikes every step (EyelidIntegrator::calcStep,
+// eyelidintegrator.cpp:50-68) and, inside the recording window of a kept
+// trial, NC and PC spike counts per bin and the integrator's output
+// (ECTrialsData's PSH and eyelid trace, ecmanagementdelay.cpp:239-273).
+__device__ void protocolRecord(const DevNet *__restrict__ N, uint64_t t)
+{
+	DevProtocol *P = N->proto;
+	if (t < P->startT + 1) return;
+	const uint64_t k = t - 1 - P->startT;
+	const int32_t time = (int32_t)(k % P->trialSteps);
+	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const DevZone &Q = N->zones[0];
+	const int32_t ct = time - P->recFrom;
+	const bool rec = trial >= P->dataStartTrial && trial < P->dataStartTrial + P->numDataTrials && ct >= 0 &&
+		ct < P->recLen;
+	const uint32_t dt = trial - P->dataStartTrial;
+	if (threadIdx.x == 0) {
+		float gSum = 0;
+		for (uint32_t i = 0; i < N->numNC; i++) {
+			float g = P->eyeG[i];
+			g = g * P->eyeGDecay;
+			g = g + Q.apNC[i] * P->eyeGInc;
+			P->eyeG[i] = g;
+			gSum += g;
+		}
+		gSum = gSum + P->eyeGShift;
+		gSum = (gSum > 0) * gSum;
+		float vm = *P->eyeVm;
+		vm = vm + (P->eyeGLeak * (0 - vm)) + (gSum * (P->eyeMaxAmp - vm));
+		*P->eyeVm = vm;
+		if (rec) P->eyelid[(size_t)dt * P->recLen + ct] = vm;
+	}
+	if (rec) {
+		const uint32_t bin = (uint32_t)ct / P->binSteps;
+		const uint32_t numNC = N->numNC, numPC = N->numPC;
+		for (uint32_t i = threadIdx.x; i < numNC + numPC; i += blockDim.x) {
+			if (i < numNC) P->ncPSH[((size_t)dt * P->nBins + bin) * numNC + i] += Q.apNC[i];
+			else P->pcPSH[((size_t)dt * P->nBins + bin) * numPC + (i - numNC)] += Q.apPC[i - numNC];
+		}
+	}
+}
+
+// Prepare the first step of a newly set protocol (the network's step tBase + 1).
+__global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet *N)
+{
+	protocolPrepare(N, *N->tBase);
+}
+
 // Small-cell update of step t: block 2n is network n's Golgi role, block
 // 2n+1 its microzone role.  The two roles share no state.  The microzone
 // role runs on shared-memory copies of its arrays when they fit (one bulk
@@ -1437,12 +1559,24 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 			stageIn(N, sNet, arena, segs, nSegs);
 			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(arena + N->zoneArenaBytes));
 			__syncthreads();
+			if (N->proto) {
+				protocolRecord(sNet, t);
+				__syncthreads();
+			}
 			stageOut(N, arena, segs, nSegs);
 		} else {
 			zoneRole(N, t, tailSmem);
+			if (N->proto) {
+				__syncthreads();
+				protocolRecord(N, t);
+			}
 		}
 	} else {
 		golgiRole(N, t, tailSmem);
+		if (N->proto) {
+			__syncthreads();
+			protocolPrepare(N, t);
+		}
 	}
 }
 

@@ -20,6 +20,7 @@ const void *passTmaKernelFor(int W, int RW, int S, int B, int M);
 // 32 * (W + 1) threads, the grPassKernel arguments with one network.
 const void *passPersistentKernelFor(int W, int S, int B, int M);
 __global__ void tailKernel(const DevNet *const *nets, uint32_t stepOffset);
+__global__ void protocolPrimeKernel(const DevNet *N);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);
 __global__ void expfProbeKernel(const float *in, float *out, uint32_t n);

@@ -565,6 +565,115 @@ void Network::setErrDrive(uint32_t z, float rel) { ctl.errDrive[z] = rel * st_->
 void Network::setGIncGRtoGO(float v) { ctl.gIncGRtoGO = v; ctlDirty = true; }
 void Network::resetGIncGRtoGO() { ctl.gIncGRtoGO = st_->ap.gIncGRtoGO; ctlDirty = true; }
 
+std::string Network::setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s)
+{
+	const ConParams &c = st_->cp;
+	const ActParams &a = st_->ap;
+	if (!p.mfFreqBG || !p.mfFreqCSTonic || !p.mfFreqCSPhasic) return "protocol: MF rate tables missing";
+	if (p.trialSteps == 0 || p.binSteps == 0) return "protocol: trialSteps and binSteps must be positive";
+	if (p.csOn < 0 || p.csOff < p.csOn || p.csOff > (int32_t)p.trialSteps || p.csPhasicOff < p.csOn ||
+			p.csPhasicOff > p.csOff)
+		return "protocol: need 0 <= csOn <= csPhasicOff <= csOff <= trialSteps";
+	if (p.preCS < 0 || p.postCS < 0 || p.mfThreshDecayTau <= 0 || p.eyeGDecayTau <= 0)
+		return "protocol: negative window or time constant";
+	const int32_t recFrom = p.csOn - p.preCS, recLen = p.csOff + p.postCS - recFrom;
+	if (recLen <= 0) return "protocol: empty recording window";
+	// the MF spikes of step t+1 are written while step t reads its own slot
+	if (h_.mfRing < 2) {
+		uint32_t *bits = alloc<uint32_t>(2ull * h_.mfWords);
+		uint8_t *raw = alloc<uint8_t>(2ull * c.numMF);
+		if (!bits || !raw) return "device allocation failed";
+		h_.mfBits = bits;
+		h_.mfRaw = raw;
+		h_.mfRing = 2;
+	}
+	h_.hasMFRaw = 0;
+	DevProtocol d{};
+	d.startT = hostT_;
+	d.trialSteps = p.trialSteps;
+	d.csStartTrial = p.csStartTrial;
+	d.csOn = p.csOn; d.csOff = p.csOff; d.csPOff = p.csPhasicOff;
+	d.plastOn = p.plastOnDelay; d.plastOff = p.plastOffDelay;
+	d.plastLTD = p.plastLTD; d.plastLTP = p.plastLTP;
+	d.usErrDrive = p.usErrDrive * a.maxExtIncVIO;  // MZone::setErrDrive (mzone.cpp:167-173)
+	d.defaultLTD = a.synLTDStepSizeGRtoPC; d.defaultLTP = a.synLTPStepSizeGRtoPC;
+	d.freqBG = upload(p.mfFreqBG, c.numMF);
+	d.freqCSTonic = upload(p.mfFreqCSTonic, c.numMF);
+	d.freqCSPhasic = upload(p.mfFreqCSPhasic, c.numMF);
+	std::vector<float> ones(c.numMF, 1.0f);  // PoissonRegenCells starts every threshold at 1
+	d.mfThresh = upload(ones.data(), ones.size());
+	// The driver builds its generator with 1 ms steps (ecmanagementdelay.cpp:96),
+	// and seeds it with a draw of a generator seeded by mfSeed
+	// (poissonregencells.cpp:12-19): the first draw of the seed's stream.
+	const float msPerTS = 1.0f;
+	d.sPerTS = msPerTS / 1000;
+	d.mfThreshDecay = 1 - expf(-msPerTS / p.mfThreshDecayTau);
+	const double u0 = (double)rng::uniform24((uint32_t)p.mfSeed, rng::kStreamNCIO, 0);
+	const int derived = (int)(u0 * 2147483648.0);
+	d.mfKey = rng::streamKey((uint32_t)derived, rng::kStreamNCIO);
+	int32_t ps[2] = {0, 1};  // grPCPlastSet = false, grPCPlastReset = true (ecmanagementdelay.cpp:168-169)
+	d.plastState = upload(ps, 2);
+	// the steps in force when the protocol starts: the setters' current values
+	float cur[2] = {ctl.ltdStep[0], ctl.ltpStep[0]};
+	d.curSteps = upload(cur, 2);
+	d.ctlSlots = alloc<float>(6);
+	d.dataStartTrial = p.dataStartTrial; d.numDataTrials = p.numDataTrials;
+	d.binSteps = p.binSteps;
+	d.recFrom = recFrom; d.recLen = recLen;
+	d.nBins = ((uint32_t)recLen + p.binSteps - 1) / p.binSteps;
+	const size_t nd = std::max<uint32_t>(1, p.numDataTrials);
+	d.ncPSH = alloc<uint32_t>(nd * d.nBins * c.numNC);
+	d.pcPSH = alloc<uint32_t>(nd * d.nBins * c.numPC);
+	d.eyelid = alloc<float>(nd * (size_t)recLen);
+	d.eyeG = alloc<float>(c.numNC);
+	d.eyeVm = alloc<float>(1);
+	// EyelidIntegrator(numNC, msPerTimeStep, 10.5, 0.012, -0.13, 0.13, 100)
+	// (ecmanagementdelay.cpp:108, eyelidintegrator.cpp:13-28)
+	const int eyeMS = (int)(unsigned)a.msPerTimeStep;
+	d.eyeGDecay = expf(-eyeMS / p.eyeGDecayTau);
+	d.eyeGInc = p.eyeGInc;
+	d.eyeGShift = p.eyeGShift;
+	d.eyeGLeak = p.eyeGLeakRaw / (6 - eyeMS);
+	d.eyeMaxAmp = p.eyeMaxAmp;
+	for (void *q : {(void *)d.freqBG, (void *)d.freqCSTonic, (void *)d.freqCSPhasic, (void *)d.mfThresh,
+			(void *)d.plastState, (void *)d.curSteps, (void *)d.ctlSlots, (void *)d.ncPSH, (void *)d.pcPSH, (void *)d.eyelid, (void *)d.eyeG, (void *)d.eyeVm})
+		if (!q) return "device allocation failed";
+	DevProtocol *dp = upload(&d, 1);
+	if (!dp) return "device allocation failed";
+	hProto_ = d;
+	h_.proto = dp;
+	CK(cudaMemcpyAsync(dNet_.ptr, &h_, sizeof(DevNet), cudaMemcpyHostToDevice, s), "uploading the network descriptor");
+	protocolPrimeKernel<<<1, kTailThreads, 0, s>>>(devPtr());
+	CK(cudaGetLastError(), "starting the protocol");
+	CK(cudaStreamSynchronize(s), "starting the protocol");
+	return "";
+}
+
+size_t Network::recordBytes(int kind) const
+{
+	if (!h_.proto) return 0;
+	const size_t nd = std::max<uint32_t>(1, hProto_.numDataTrials);
+	switch (kind) {
+	case CBM_REC_NC_PSH: return 4 * nd * hProto_.nBins * h_.numNC;
+	case CBM_REC_PC_PSH: return 4 * nd * hProto_.nBins * h_.numPC;
+	case CBM_REC_EYELID: return 4 * nd * (size_t)hProto_.recLen;
+	default: return 0;
+	}
+}
+
+std::string Network::readRecord(int kind, void *dst, size_t bytes, cudaStream_t s)
+{
+	if (!h_.proto) return "no protocol is running";
+	const size_t need = recordBytes(kind);
+	if (!need) return "unknown record kind";
+	if (bytes != need) return "record size mismatch";
+	const void *src = kind == CBM_REC_NC_PSH ? (const void *)hProto_.ncPSH
+		: kind == CBM_REC_PC_PSH ? (const void *)hProto_.pcPSH : (const void *)hProto_.eyelid;
+	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "reading a record");
+	CK(cudaStreamSynchronize(s), "reading a record");
+	return "";
+}
+
 std::string Network::uploadMFBits(const uint32_t *bits, uint64_t firstSlot, uint64_t n, cudaStream_t s)
 {
 	if (firstSlot + n > h_.mfRing) return "MF ring too small";
@@ -984,9 +1093,18 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 	return "";
 }
 
+std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(uploadCtl());
+	CK(cudaStreamSynchronize(s0_), "sync");
+	return nets_[i]->setProtocol(p, s0_);
+}
+
 std::string Simulator::stageMF(size_t i, const uint8_t *mf)
 {
 	Network &n = *nets_[i];
+	if (n.hasProtocol()) return "a device protocol drives the MF input of this network";
 	const uint32_t W = n.h_.mfWords, M = n.h_.numMF;
 	memset(n.hPinnedBits_, 0, 4ull * W);
 	bool raw = false;

@@ -9,6 +9,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 
+#include "../../include/cbm_b200.h"
 #include "cbm_device.cuh"
 #include "cbm_state.hpp"
 
@@ -46,6 +47,8 @@ public:
 	std::string launchSteps(uint32_t nsteps);
 	// Host MF input for the next step of network i (updateMFInput).
 	std::string stageMF(size_t i, const uint8_t *mf);
+	// Start a device-driven trial protocol on network i from the next step.
+	std::string setProtocol(size_t i, const cbm_eyelid_protocol &p);
 	// Run nsteps as CUDA-graph chunks of chunk steps (inputs resident in HBM).
 	// With instrument, external events around every GR pass of the chunk
 	// give lastPassMs(): the pass's mean duration over the last replay.
@@ -121,6 +124,11 @@ public:
 	// The reference's writeState resets the GO->GO depression arrays of the
 	// live state (innetactivitystate.cpp:247-248); mirrored on the device.
 	std::string resetGOGODepression(cudaStream_t s);
+	// Device-driven trial protocol (cbm_eyelid_protocol) from the next step on.
+	std::string setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s);
+	bool hasProtocol() const { return h_.proto != nullptr; }
+	size_t recordBytes(int kind) const;
+	std::string readRecord(int kind, void *dst, size_t bytes, cudaStream_t s);
 	// MF spikes for steps [t0, t0+n) as bit rows, into the ring.
 	std::string uploadMFBits(const uint32_t *bits, uint64_t firstSlot, uint64_t n, cudaStream_t s);
 	uint64_t stepsDone() const { return hostT_; }
@@ -158,6 +166,7 @@ private:
 	DevNet h_{};
 	DeviceBuf dNet_;
 	std::string buildZoneStaging();
+	DevProtocol hProto_{};  // host copy of the protocol descriptor
 	std::vector<void *> allocs_;
 	std::map<const void *, size_t> allocBytes_;
 	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;

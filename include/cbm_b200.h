@@ -187,6 +187,61 @@ int cbm_sim_run(cbm_sim *sim, uint64_t nsteps, uint32_t graphChunk, float *gpuMs
 int cbm_sim_timer_start(cbm_sim *sim);
 int cbm_sim_timer_stop(cbm_sim *sim, float *ms);
 
+/* ---- Trials driven on the device.
+ *
+ * The eyelid-conditioning driver of the reference (ECManagementDelay,
+ * Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:175-273) as a device
+ * protocol, so that whole trials run without a host call per step:
+ *   - MF input from the reference's Poisson regenerating population
+ *     (PoissonRegenCells, CBM_TOOLS_LIB_DEV/src/poissonregencells.cpp:49-66)
+ *     with background rates, and in CS trials phasic rates in
+ *     [csOn, csPhasicOff) and tonic rates in [csPhasicOff, csOff);
+ *   - the US as updateErrDrive(0, usErrDrive) at step csOff - 1 of CS trials;
+ *   - PF->PC steps (plastLTD, plastLTP) set on zone 0 from csOn + plastOnDelay
+ *     and reset at csOff + plastOffDelay of CS trials;
+ *   - recording of trials [dataStartTrial, dataStartTrial + numDataTrials):
+ *     NC and PC spike counts of zone 0 per bin of binSteps steps over the
+ *     window [csOn - preCS, csOff + postCS), and the eyelid integrator
+ *     (EyelidIntegrator, CBM_TOOLS_LIB_DEV/src/eyelidintegrator.cpp:50-68)
+ *     on zone 0's NC spikes, one value per step of the window.
+ * Trial steps are counted from the call: the next step is step 0 of trial 0.
+ * The MF draw of fibre i at simulator step t is the counter-based stream of
+ * the NC->IO draws keyed by a seed derived from mfSeed, counter (t << 20) | i.
+ * While a protocol runs, cbm_sim_update_mf and cbm_sim_load_mf_stream fail. */
+typedef struct cbm_eyelid_protocol {
+	uint32_t trialSteps;          /* steps per trial (5000) */
+	int32_t csOn, csOff;          /* in-trial steps of CS onset and offset (2000, 2500) */
+	int32_t csPhasicOff;          /* end of the phasic CS rates (csOn: tonic rates only) */
+	uint32_t csStartTrial;        /* first trial with CS and US */
+	int32_t plastOnDelay, plastOffDelay;  /* 200, 200 */
+	float plastLTD, plastLTP;     /* -0.0005 x LTD/LTP ratio, 0.0005 */
+	float usErrDrive;             /* relative error drive of the US (1.0) */
+	int32_t mfSeed;               /* seed of the MF generator */
+	float mfThreshDecayTau;       /* ms (4) */
+	const float *mfFreqBG;        /* Hz, numMF values each, host memory */
+	const float *mfFreqCSTonic;
+	const float *mfFreqCSPhasic;
+	uint32_t dataStartTrial, numDataTrials;
+	int32_t preCS, postCS;        /* 500, 500 */
+	uint32_t binSteps;            /* 10 */
+	float eyeGDecayTau, eyeGInc, eyeGShift, eyeGLeakRaw, eyeMaxAmp;  /* 10.5, 0.012, -0.13, 0.13, 100 */
+} cbm_eyelid_protocol;
+
+/* Record kinds of cbm_sim_trial_record. */
+enum {
+	CBM_REC_NC_PSH = 0,  /* u32 [numDataTrials][bins][numNC] */
+	CBM_REC_PC_PSH = 1,  /* u32 [numDataTrials][bins][numPC] */
+	CBM_REC_EYELID = 2   /* f32 [numDataTrials][window steps] */
+};
+
+/* Start a device protocol on network 0 of the simulator (no counterpart in
+ * the reference's core library: it replaces the driver's per-step calls). */
+int cbm_sim_set_eyelid_protocol(cbm_sim *sim, const cbm_eyelid_protocol *protocol);
+/* Size in bytes of a record of the running protocol (0 without one). */
+uint64_t cbm_sim_trial_record_bytes(cbm_sim *sim, int kind);
+/* Copy a record of the running protocol to host memory. */
+int cbm_sim_trial_record(cbm_sim *sim, int kind, void *dst, uint64_t bytes);
+
 /* Measurement helper, no counterpart in the reference: nsteps steps with
  * resident MF input, each launched alone after a write of a flushBytes
  * device buffer (an L2 flush when larger than the L2 cache); *stepMs is the

@@ -1126,6 +1126,105 @@ void cbm_oracle_run(cbm_oracle *o, const uint8_t *mf, uint64_t nsteps, uint8_t *
 	}
 }
 
+static void protocol_window(const cbm_oracle_protocol *p, int32_t *from, int32_t *len, uint32_t *bins)
+{
+	*from = p->csOn - p->preCS;
+	*len = p->csOff + p->postCS - *from;
+	*bins = ((uint32_t)*len + p->binSteps - 1) / p->binSteps;
+}
+
+void cbm_oracle_protocol_sizes(const cbm_oracle *o, const cbm_oracle_protocol *p, uint64_t *ncPSH,
+		uint64_t *pcPSH, uint64_t *eyelid)
+{
+	int32_t from, len; uint32_t bins;
+	protocol_window(p, &from, &len, &bins);
+	uint64_t nd = p->numDataTrials ? p->numDataTrials : 1;
+	*ncPSH = nd * bins * o->numNC;
+	*pcPSH = nd * bins * o->numPC;
+	*eyelid = nd * (uint64_t)len;
+}
+
+void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, uint64_t nsteps,
+		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid)
+{
+	const uint32_t numMF = o->numMF, numNC = o->numNC, numPC = o->numPC;
+	const float *freqBG = rates, *freqCST = rates + numMF, *freqCSP = rates + 2 * (size_t)numMF;
+	int32_t recFrom, recLen; uint32_t nBins;
+	protocol_window(p, &recFrom, &recLen, &nBins);
+	uint64_t nNC, nPC, nEye;
+	cbm_oracle_protocol_sizes(o, p, &nNC, &nPC, &nEye);
+	memset(ncPSH, 0, nNC * 4); memset(pcPSH, 0, nPC * 4); memset(eyelid, 0, nEye * 4);
+	/* PoissonRegenCells(numMF, mfSeed, tau, 1) (ecmanagementdelay.cpp:96,
+	 * poissonregencells.cpp:10-35): its generator's seed is the first draw of
+	 * a generator seeded with mfSeed, scaled to [0, 2^31) */
+	const float msPerTS = 1.0f, sPerTS = msPerTS / 1000;
+	const float threshDecay = 1 - expf(-msPerTS / p->mfThreshDecayTau);
+	const double u0 = (double)cbm_oracle_uniform24((uint32_t)p->mfSeed, CBM_STREAM_NCIO, 0);
+	const uint32_t mfGenSeed = (uint32_t)(int)(u0 * 2147483648.0);
+	float *thresh = malloc(numMF * sizeof(float));
+	uint8_t *apMF = malloc(numMF);
+	for (uint32_t i = 0; i < numMF; i++) thresh[i] = 1;
+	/* EyelidIntegrator(numNC, msPerTimeStep, ...) (eyelidintegrator.cpp:13-28) */
+	const int eyeMS = (int)(unsigned)o->msPerTimeStep;
+	const float eyeGDecay = expf(-eyeMS / p->eyeGDecayTau), eyeGLeak = p->eyeGLeakRaw / (6 - eyeMS);
+	float *gIn = calloc(numNC, sizeof(float));
+	float vm = 0;
+	int plastSet = 0, plastReset = 1;
+	size_t rb = cbm_oracle_trace_record_bytes(o);
+	zone_t *z0 = &o->zones[0];
+	for (uint64_t s = 0; s < nsteps; s++)
+	{
+		const uint64_t t = o->curTime + 1;
+		const int32_t time = (int32_t)(s % p->trialSteps);
+		const uint32_t trial = (uint32_t)(s / p->trialSteps);
+		const int csTrial = trial >= p->csStartTrial;
+		/* calcMFActivity (ecmanagementdelay.cpp:175-194) */
+		const float *freq = freqBG;
+		if (csTrial && time >= p->csOn && time < p->csOff) freq = time < p->csPhasicOff ? freqCSP : freqCST;
+		for (uint32_t i = 0; i < numMF; i++)
+		{
+			thresh[i] = thresh[i] + (1 - thresh[i]) * threshDecay;
+			apMF[i] = (double)cbm_oracle_uniform24(mfGenSeed, CBM_STREAM_NCIO, (t << 20) | i) <
+				((freq[i] * sPerTS) * thresh[i]);
+			thresh[i] = (!apMF[i]) * thresh[i];
+		}
+		/* calcSimActivity (ecmanagementdelay.cpp:196-235) */
+		if (time == p->csOff - 1 && csTrial) cbm_oracle_update_err_drive(o, 0, p->usErrDrive);
+		if (time >= p->csOn + p->plastOnDelay && !plastSet && csTrial && time < p->csOff + p->plastOffDelay)
+		{
+			plastSet = 1; plastReset = 0;
+			cbm_oracle_set_plast_steps(o, 0, p->plastLTD, p->plastLTP);
+		}
+		if (!plastReset && time >= p->csOff + p->plastOffDelay && csTrial)
+		{
+			plastSet = 0; plastReset = 1;
+			cbm_oracle_reset_plast_steps(o, 0);
+		}
+		cbm_oracle_step(o, apMF);
+		if (trace) trace_record(o, trace + s * rb);
+		/* EyelidIntegrator::calcStep (eyelidintegrator.cpp:50-68) */
+		float gSum = 0;
+		for (uint32_t i = 0; i < numNC; i++)
+		{
+			gIn[i] = gIn[i] * eyeGDecay;
+			gIn[i] = gIn[i] + z0->apNC[i] * p->eyeGInc;
+			gSum += gIn[i];
+		}
+		gSum = gSum + p->eyeGShift;
+		gSum = (gSum > 0) * gSum;
+		vm = vm + (eyeGLeak * (0 - vm)) + (gSum * (p->eyeMaxAmp - vm));
+		const int32_t ct = time - recFrom;
+		if (trial >= p->dataStartTrial && trial < p->dataStartTrial + p->numDataTrials && ct >= 0 && ct < recLen)
+		{
+			const size_t dt = trial - p->dataStartTrial, bin = (size_t)ct / p->binSteps;
+			for (uint32_t i = 0; i < numNC; i++) ncPSH[(dt * nBins + bin) * numNC + i] += z0->apNC[i];
+			for (uint32_t i = 0; i < numPC; i++) pcPSH[(dt * nBins + bin) * numPC + i] += z0->apPC[i];
+			eyelid[dt * recLen + ct] = vm;
+		}
+	}
+	free(thresh); free(apMF); free(gIn);
+}
+
 void cbm_oracle_expf_array(const float *in, float *out, uint64_t n)
 {
 	/* the host C library's expf, which the reference's exp(float) calls use */

@@ -51,6 +51,30 @@ int cbm_oracle_save(cbm_oracle *o, const char *path);
 /* out[i] = the host C library's expf(in[i]) (the reference's exp(float)). */
 void cbm_oracle_expf_array(const float *in, float *out, uint64_t n);
 
+/* The eyelid-conditioning driver (ECManagementDelay::calcMFActivity and
+ * calcSimActivity, Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:
+ * 175-273) around nsteps steps, starting at trial 0, step 0: MF input from a
+ * Poisson regenerating population (PoissonRegenCells, CBM_TOOLS_LIB_DEV/src/
+ * poissonregencells.cpp:49-66) whose draw of fibre i at step t is keyed by
+ * ((t << 20) | i) under a seed derived from mfSeed, the US error drive, the
+ * PF->PC step window, the eyelid integrator (eyelidintegrator.cpp:13-68) and
+ * the records of the kept trials (NC / PC counts per bin, integrator output
+ * per step of the window).  rates: 3 x numMF floats (background, CS tonic,
+ * CS phasic).  Field meanings as cbm_eyelid_protocol in include/cbm_b200.h. */
+typedef struct {
+	uint32_t trialSteps; int32_t csOn, csOff, csPhasicOff; uint32_t csStartTrial;
+	int32_t plastOnDelay, plastOffDelay; float plastLTD, plastLTP, usErrDrive;
+	int32_t mfSeed; float mfThreshDecayTau;
+	uint32_t dataStartTrial, numDataTrials; int32_t preCS, postCS; uint32_t binSteps;
+	float eyeGDecayTau, eyeGInc, eyeGShift, eyeGLeakRaw, eyeMaxAmp;
+} cbm_oracle_protocol;
+
+/* Record sizes in elements: *ncPSH, *pcPSH (u32) and *eyelid (f32). */
+void cbm_oracle_protocol_sizes(const cbm_oracle *o, const cbm_oracle_protocol *p, uint64_t *ncPSH,
+		uint64_t *pcPSH, uint64_t *eyelid);
+void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, uint64_t nsteps,
+		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid);
+
 /* Sizes, for callers sizing buffers. */
 uint32_t cbm_oracle_num(const cbm_oracle *o, const char *what);
 

@@ -15,6 +15,21 @@
  *       interface/cbmsimcore.cpp:139-320) and writes one trace record per step
  *       plus the final state (CBMSimCore::writeToState, cbmsimcore.cpp:75-80).
  *       -t times the steps and writes no trace.
+ *       -p PROTOCOL -r RECORDS: the MF input comes from the reference's
+ *       PoissonRegenCells (CBM_TOOLS_LIB_DEV/src/poissonregencells.cpp) and the
+ *       eyelid-conditioning driver's per-step calls are made in the order of
+ *       ECManagementDelay::calcMFActivity / calcSimActivity
+ *       (Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:175-273,
+ *       restated below); the reference's EyelidIntegrator
+ *       (CBM_TOOLS_LIB_DEV/src/eyelidintegrator.cpp) runs on zone 0's NC
+ *       spikes; RECORDS receives NC and PC spike counts per bin and the
+ *       integrator's output over the recording window of the kept trials
+ *       (MFBYTES is then ignored).  PROTOCOL is "key value" text: trialSteps,
+ *       csOn, csOff, csPhasicOff, csStartTrial, plastOnDelay, plastOffDelay,
+ *       plastLTD, plastLTP, usErrDrive, mfSeed, mfThreshDecayTau, rates (a file
+ *       of 3 x numMF f32: background, CS tonic, CS phasic), dataStartTrial,
+ *       numDataTrials, preCS, postCS, binSteps, eyeGDecayTau, eyeGInc,
+ *       eyeGShift, eyeGLeakRaw, eyeMaxAmp.
  *
  * After loading, two fields the reference's loader leaves undefined are set
  * the way the B200 loader sets them:
@@ -44,7 +59,10 @@
 #include <CBMStateInclude/interfaces/cbmstate.h>
 
 #ifndef CBM_REF_GEN_ONLY
+#include <map>
 #include <CBMCoreInclude/interface/cbmsimcore.h>
+#include <CBMToolsInclude/poissonregencells.h>
+#include <CBMToolsInclude/eyelidintegrator.h>
 uint64_t cbm_refshim_step = 0;
 void cbm_refshim_set_step(uint64_t t) { cbm_refshim_step = t; }
 #endif
@@ -121,6 +139,22 @@ static std::vector<Event> readEvents(const char *path)
 
 template<typename T> static void put(FILE *f, const T *p, size_t n) { if (n) fwrite(p, sizeof(T), n, f); }
 
+// Trial protocol of the eyelid driver (see the file comment).
+struct Protocol
+{
+	std::map<std::string, std::string> kv;
+	bool load(const char *path)
+	{
+		std::ifstream f(path);
+		if (!f.good()) return false;
+		std::string k, v;
+		while (f >> k >> v) kv[k] = v;
+		return true;
+	}
+	double num(const char *k) const { auto it = kv.find(k); return it == kv.end() ? 0.0 : atof(it->second.c_str()); }
+	std::string str(const char *k) const { auto it = kv.find(k); return it == kv.end() ? "" : it->second; }
+};
+
 int main(int argc, char **argv)
 {
 	if (argc < 6)
@@ -131,12 +165,14 @@ int main(int argc, char **argv)
 	const char *statePath = argv[1], *mfPath = argv[2], *tracePath = argv[4], *finalPath = argv[5];
 	unsigned long steps = strtoul(argv[3], NULL, 10);
 	std::vector<int> seeds;
-	const char *eventsPath = NULL;
+	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL;
 	int numGPUP2 = 0;
 	bool timeOnly = false;
 	for (int i = 6; i < argc; i++)
 	{
 		if (!strcmp(argv[i], "-e") && i + 1 < argc) eventsPath = argv[++i];
+		else if (!strcmp(argv[i], "-p") && i + 1 < argc) protocolPath = argv[++i];
+		else if (!strcmp(argv[i], "-r") && i + 1 < argc) recordsPath = argv[++i];
 		else if (!strcmp(argv[i], "-g") && i + 1 < argc) numGPUP2 = atoi(argv[++i]);
 		else if (!strcmp(argv[i], "-t")) timeOnly = true;
 		else seeds.push_back(atoi(argv[i]));
@@ -152,6 +188,10 @@ int main(int argc, char **argv)
 	while (seeds.size() < nZones) seeds.push_back(1000 + (int)seeds.size());
 
 	std::vector<ct_uint8_t> mf;
+	Protocol proto;
+	const bool useProtocol = protocolPath != NULL;
+	if (useProtocol && (!proto.load(protocolPath) || !recordsPath)) { fprintf(stderr, "bad protocol\n"); return 1; }
+	if (!useProtocol)
 	{
 		FILE *f = fopen(mfPath, "rb");
 		if (!f) { fprintf(stderr, "cannot open mf\n"); return 1; }
@@ -176,10 +216,86 @@ int main(int argc, char **argv)
 	}
 	std::vector<ct_uint8_t> bits((cp->numGR + 7) / 8);
 	size_t evi = 0;
+
+	// eyelid driver state (ecmanagementdelay.cpp:90-170)
+	const unsigned int trialSteps = (unsigned int)proto.num("trialSteps");
+	const int csOn = (int)proto.num("csOn"), csOff = (int)proto.num("csOff"), csPOff = (int)proto.num("csPhasicOff");
+	const unsigned int csStartTN = (unsigned int)proto.num("csStartTrial");
+	const int plastOn = (int)proto.num("plastOnDelay"), plastOff = (int)proto.num("plastOffDelay");
+	const float plastLTD = (float)proto.num("plastLTD"), plastLTP = (float)proto.num("plastLTP");
+	const float usErr = (float)proto.num("usErrDrive");
+	const unsigned int dataStartTN = (unsigned int)proto.num("dataStartTrial"), numDataT = (unsigned int)proto.num("numDataTrials");
+	const int recFrom = csOn - (int)proto.num("preCS"), recLen = csOff + (int)proto.num("postCS") - recFrom;
+	const unsigned int binSteps = useProtocol ? (unsigned int)proto.num("binSteps") : 1;
+	const unsigned int nBins = useProtocol ? ((unsigned int)recLen + binSteps - 1) / binSteps : 0;
+	std::vector<float> freqBG, freqCST, freqCSP;
+	PoissonRegenCells *mfs = NULL;
+	EyelidIntegrator *eyelid = NULL;
+	std::vector<ct_uint32_t> ncPSH, pcPSH;
+	std::vector<float> eyeTrace;
+	bool grPCPlastSet = false, grPCPlastReset = true;
+	if (useProtocol)
+	{
+		freqBG.resize(cp->numMF); freqCST.resize(cp->numMF); freqCSP.resize(cp->numMF);
+		FILE *f = fopen(proto.str("rates").c_str(), "rb");
+		if (!f) { fprintf(stderr, "cannot open rates\n"); return 1; }
+		size_t got = fread(freqBG.data(), 4, cp->numMF, f) + fread(freqCST.data(), 4, cp->numMF, f) +
+			fread(freqCSP.data(), 4, cp->numMF, f);
+		fclose(f);
+		if (got != 3 * (size_t)cp->numMF) { fprintf(stderr, "rates file too short\n"); return 1; }
+		cbm_refshim_set_step(0);
+		mfs = new PoissonRegenCells(cp->numMF, (int)proto.num("mfSeed"), (float)proto.num("mfThreshDecayTau"), 1);
+		eyelid = new EyelidIntegrator(cp->numNC, (unsigned int)st->getActParamsInternal()->msPerTimeStep,
+				(float)proto.num("eyeGDecayTau"), (float)proto.num("eyeGInc"), (float)proto.num("eyeGShift"),
+				(float)proto.num("eyeGLeakRaw"), (float)proto.num("eyeMaxAmp"));
+		const size_t nd = numDataT ? numDataT : 1;
+		ncPSH.assign(nd * nBins * cp->numNC, 0);
+		pcPSH.assign(nd * nBins * cp->numPC, 0);
+		eyeTrace.assign(nd * (size_t)recLen, 0.0f);
+	}
+
 	auto t0 = std::chrono::steady_clock::now();
 	for (unsigned long t = 1; t <= steps; t++)
 	{
-		while (evi < events.size() && events[evi].t == t)
+		if (useProtocol)
+		{
+			const int time = (int)((t - 1) % trialSteps);
+			const unsigned int trial = (unsigned int)((t - 1) / trialSteps);
+			const bool csTrial = trial >= csStartTN;
+			// calcMFActivity (ecmanagementdelay.cpp:175-194); the MF draws of step t
+			cbm_refshim_set_step(t);
+			const float *freq = freqBG.data();
+			if (csTrial && time >= csOn && time < csOff) freq = time < csPOff ? freqCSP.data() : freqCST.data();
+			const ct_uint8_t *apMF = mfs->calcActivity(freq);
+			// calcSimActivity (ecmanagementdelay.cpp:196-235)
+			if (time == csOff - 1 && csTrial) sim->updateErrDrive(0, usErr);
+			if (time >= csOn + plastOn && !grPCPlastSet && csTrial && time < csOff + plastOff)
+			{
+				grPCPlastSet = true;
+				grPCPlastReset = false;
+				zones[0]->setGRPCPlastSteps(plastLTD, plastLTP);
+			}
+			if (!grPCPlastReset && time >= csOff + plastOff && csTrial)
+			{
+				grPCPlastSet = false;
+				grPCPlastReset = true;
+				zones[0]->resetGRPCPlastSteps();
+			}
+			sim->updateMFInput(apMF);
+			sim->calcActivity();
+			const ct_uint8_t *apNC = zones[0]->exportAPNC();
+			const float vm = eyelid->calcStep(apNC);
+			const int ct = time - recFrom;
+			if (trial >= dataStartTN && trial < dataStartTN + numDataT && ct >= 0 && ct < recLen)
+			{
+				const size_t dt = trial - dataStartTN, bin = (size_t)ct / binSteps;
+				const ct_uint8_t *apPC = zones[0]->exportAPPC();
+				for (unsigned int i = 0; i < cp->numNC; i++) ncPSH[(dt * nBins + bin) * cp->numNC + i] += apNC[i];
+				for (unsigned int i = 0; i < cp->numPC; i++) pcPSH[(dt * nBins + bin) * cp->numPC + i] += apPC[i];
+				eyeTrace[dt * recLen + ct] = vm;
+			}
+		}
+		while (!useProtocol && evi < events.size() && events[evi].t == t)
 		{
 			const Event &e = events[evi++];
 			if (e.kind == "errdrive") sim->updateErrDrive((unsigned)e.zone, e.a);
@@ -188,9 +304,12 @@ int main(int argc, char **argv)
 			else if (e.kind == "grgoinc") inet->setGIncGRtoGO(e.a);
 			else if (e.kind == "grgoincreset") inet->resetGIncGRtoGO();
 		}
-		sim->updateMFInput(&mf[(size_t)(t - 1) * cp->numMF]);
-		cbm_refshim_set_step(t);
-		sim->calcActivity();
+		if (!useProtocol)
+		{
+			sim->updateMFInput(&mf[(size_t)(t - 1) * cp->numMF]);
+			cbm_refshim_set_step(t);
+			sim->calcActivity();
+		}
 		if (timeOnly) continue;
 
 		const ct_uint8_t *apGR = inet->exportAPGR();
@@ -221,6 +340,17 @@ int main(int argc, char **argv)
 			steps, sec, sec > 0 ? steps / sec : 0.0, cp->numGR);
 	fflush(stdout);
 
+	if (useProtocol)
+	{
+		FILE *f = fopen(recordsPath, "wb");
+		if (!f) { fprintf(stderr, "cannot open records\n"); return 1; }
+		put(f, ncPSH.data(), ncPSH.size());
+		put(f, pcPSH.data(), pcPSH.size());
+		put(f, eyeTrace.data(), eyeTrace.size());
+		fclose(f);
+		delete mfs;
+		delete eyelid;
+	}
 	if (strcmp(finalPath, "-") != 0)
 	{
 		std::fstream out(finalPath, std::ios::out | std::ios::binary | std::ios::trunc);

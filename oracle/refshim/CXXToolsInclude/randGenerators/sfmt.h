@@ -28,7 +28,8 @@ public:
 		return (double)cbm_oracle_uniform24(seed_, CBM_STREAM_NCIO, c);
 	}
 	uint32_t BRandom() { return (uint32_t)(Random() * 4294967296.0); }
-	int IRandom(int min, int max) { return min + (int)(Random() * (double)(max - min + 1)); }
+	// interval max - min + 1 in 64 bits (SFMT's IRandom takes it as an unsigned 32-bit count)
+	int IRandom(int min, int max) { return min + (int)(Random() * (double)((int64_t)max - min + 1)); }
 	int IRandomX(int min, int max) { return IRandom(min, max); }
 private:
 	uint32_t seed_;

@@ -51,6 +51,8 @@ class Oracle:
             lib.cbm_oracle_save.argtypes = [P, S]
             lib.cbm_oracle_num.restype = ctypes.c_uint32
             lib.cbm_oracle_num.argtypes = [P, S]
+            lib.cbm_oracle_protocol_sizes.argtypes = [P, P, P, P, P]
+            lib.cbm_oracle_run_protocol.argtypes = [P, P, P, ctypes.c_uint64, P, P, P, P]
             cls._lib = lib
         return cls._lib
 
@@ -98,9 +100,80 @@ class Oracle:
             lib.cbm_oracle_run(self.h, row.ctypes.data, 1, tr[s].ctypes.data)
         return tr
 
+    def run_protocol(self, proto, rates, nsteps, record=True):
+        """The eyelid driver around nsteps steps (cbm_oracle_run_protocol):
+        (trace, ncPSH, pcPSH, eyelid)."""
+        lib = self.lib()
+        p = ProtocolStruct.from_dict(proto)
+        sizes = [ctypes.c_uint64() for _ in range(3)]
+        lib.cbm_oracle_protocol_sizes(self.h, ctypes.byref(p), *[ctypes.byref(x) for x in sizes])
+        nc = np.zeros(sizes[0].value, dtype=np.uint32)
+        pc = np.zeros(sizes[1].value, dtype=np.uint32)
+        eye = np.zeros(sizes[2].value, dtype=np.float32)
+        rates = np.ascontiguousarray(rates, dtype=np.float32)
+        tr = np.zeros((nsteps, self.rb), dtype=np.uint8) if record else None
+        lib.cbm_oracle_run_protocol(self.h, ctypes.byref(p), rates.ctypes.data, nsteps,
+                                    tr.ctypes.data if record else None, nc.ctypes.data, pc.ctypes.data,
+                                    eye.ctypes.data)
+        return tr, nc, pc, eye
+
     def save(self, path):
         if self.lib().cbm_oracle_save(self.h, os.fsencode(path)) != 0:
             raise RuntimeError("oracle save failed")
+
+
+PROTOCOL_FIELDS = [("trialSteps", "u"), ("csOn", "i"), ("csOff", "i"), ("csPhasicOff", "i"), ("csStartTrial", "u"),
+                   ("plastOnDelay", "i"), ("plastOffDelay", "i"), ("plastLTD", "f"), ("plastLTP", "f"),
+                   ("usErrDrive", "f"), ("mfSeed", "i"), ("mfThreshDecayTau", "f"), ("dataStartTrial", "u"),
+                   ("numDataTrials", "u"), ("preCS", "i"), ("postCS", "i"), ("binSteps", "u"),
+                   ("eyeGDecayTau", "f"), ("eyeGInc", "f"), ("eyeGShift", "f"), ("eyeGLeakRaw", "f"),
+                   ("eyeMaxAmp", "f")]
+
+
+class ProtocolStruct(ctypes.Structure):
+    """cbm_oracle_protocol (oracle/cbm_oracle.h)."""
+    _fields_ = [(n, {"u": ctypes.c_uint32, "i": ctypes.c_int32, "f": ctypes.c_float}[k]) for n, k in PROTOCOL_FIELDS]
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(**{n: d[n] for n, _ in PROTOCOL_FIELDS})
+
+
+def short_protocol(**kw):
+    """A small eyelid protocol for tests: 400-step trials, CS 120-260."""
+    p = dict(trialSteps=400, csOn=120, csOff=260, csPhasicOff=150, csStartTrial=1, plastOnDelay=40,
+             plastOffDelay=30, plastLTD=-0.004, plastLTP=0.002, usErrDrive=1.0, mfSeed=11, mfThreshDecayTau=4.0,
+             dataStartTrial=0, numDataTrials=3, preCS=60, postCS=80, binSteps=10, eyeGDecayTau=10.5,
+             eyeGInc=0.012, eyeGShift=-0.13, eyeGLeakRaw=0.13, eyeMaxAmp=100.0)
+    p.update(kw)
+    return p
+
+
+def protocol_rates(num_mf, seed=0):
+    """[3, num_mf] Hz: background 1-30, CS tonic and phasic raised on a random 10%."""
+    rng = np.random.Generator(np.random.PCG64(seed + 500))
+    bg = rng.uniform(1.0, 30.0, num_mf).astype(np.float32)
+    tonic, phasic = bg.copy(), bg.copy()
+    cs = rng.permutation(num_mf)[: max(1, num_mf // 10)]
+    tonic[cs] = 80.0
+    phasic[cs] = 150.0
+    return np.stack([bg, tonic, phasic])
+
+
+def ref_run_protocol(state_path, proto, rates, nsteps, seeds):
+    """oracle/_ref/ref_run in protocol mode: (trace, ncPSH, pcPSH, eyelid)."""
+    with tempfile.TemporaryDirectory() as d:
+        rp = os.path.join(d, "rates.f32")
+        np.ascontiguousarray(rates, dtype=np.float32).tofile(rp)
+        pp = os.path.join(d, "protocol.txt")
+        with open(pp, "w") as f:
+            for n, _ in PROTOCOL_FIELDS:
+                f.write(f"{n} {proto[n]!r}\n")
+            f.write(f"rates {rp}\n")
+        trp, rec = os.path.join(d, "trace.bin"), os.path.join(d, "records.bin")
+        cmd = [REF_RUN, state_path, "-", str(nsteps), trp, "-"] + [str(s) for s in seeds] + ["-p", pp, "-r", rec]
+        subprocess.run(cmd, check=True, capture_output=True)
+        return np.fromfile(trp, dtype=np.uint8), np.fromfile(rec, dtype=np.uint8)
 
 
 def events_file(events, path):

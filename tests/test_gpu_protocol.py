@@ -1,0 +1,80 @@
+"""Trials driven on the device (cbm_sim_set_eyelid_protocol): MF generation,
+US, PF->PC plasticity window, eyelid integrator and trial records against
+the oracle's restatement of the reference's eyelid driver (pinned to the
+reference's PoissonRegenCells / EyelidIntegrator in test_oracle_pin.py)."""
+import numpy as np
+import pytest
+
+import cbmtest
+from cbmtest import Oracle
+from test_gpu_parity import compare_states
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle(state_path, proto, rates, steps, tmp_path):
+    o = Oracle(state_path, seeds=[7])
+    tr, nc, pc, eye = o.run_protocol(proto, rates, steps)
+    fin = str(tmp_path / "oracle.state")
+    o.save(fin)
+    return o, tr, nc, pc, eye, fin
+
+
+def _compare_records(sim, o_nc, o_pc, o_eye):
+    nc, pc, eye = sim.trial_record("nc"), sim.trial_record("pc"), sim.trial_record("eyelid")
+    assert np.array_equal(nc.ravel(), o_nc)
+    assert np.array_equal(pc.ravel(), o_pc)
+    assert cbmtest.same_values(eye.ravel(), o_eye).all()
+    return nc, eye
+
+
+def test_protocol_step_by_step_bit_exact(tmp_path):
+    import cerebellum_simulation_b200 as cbm
+    st_path = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol()
+    st = cbm.CBMState(st_path)
+    rates = cbmtest.protocol_rates(st.con("numMF"), seed=1)
+    steps = 3 * proto["trialSteps"]
+    o, tr_o, o_nc, o_pc, o_eye, fin_o = _oracle(st_path, proto, rates, steps, tmp_path)
+    sim = cbm.CBMSimCore(st, [7], device=0)
+    sim.set_eyelid_protocol(rates, **proto)
+    for s in range(steps):
+        sim.calcActivity()
+        rec = cbmtest.product_record(sim, None)
+        if not cbmtest.same_values(rec, tr_o[s]).all():
+            pytest.fail(f"step {s + 1}: " + cbmtest.first_difference(rec, tr_o[s], o.num))
+    nc, eye = _compare_records(sim, o_nc, o_pc, o_eye)
+    assert nc.sum() > 0 and eye.max() > 0
+    fin_p = str(tmp_path / "b200.state")
+    sim.writeToState(fin_p)
+    assert compare_states(fin_o, fin_p) == []
+
+
+def test_protocol_graph_replay_bit_exact(tmp_path):
+    """Whole trials replayed as CUDA graphs, the protocol started after some
+    host-driven steps."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    st = networks.config1_network(seed=4)
+    st_path = str(tmp_path / "c1.state")
+    st.writeState(st_path)
+    proto = cbmtest.short_protocol(trialSteps=300, csOn=80, csOff=200, csPhasicOff=80, csStartTrial=0,
+                                   numDataTrials=2, dataStartTrial=1, mfSeed=23)
+    rates = cbmtest.protocol_rates(st.con("numMF"), seed=2)
+    lead = cbmtest.counter_mf(st.con("numMF"), 37, 5)
+    steps = 3 * proto["trialSteps"]
+    o = Oracle(st_path, seeds=[7])
+    o.run(lead)
+    _, o_nc, o_pc, o_eye = o.run_protocol(proto, rates, steps, record=False)
+    fin_o = str(tmp_path / "oracle.state")
+    o.save(fin_o)
+    sim = cbm.CBMSimCore(cbm.CBMState(st_path), [7], device=0)
+    cbmtest.product_run(sim, lead, record=False)
+    sim.set_eyelid_protocol(rates, **proto)
+    sim.run(steps, 50)
+    _compare_records(sim, o_nc, o_pc, o_eye)
+    fin_p = str(tmp_path / "b200.state")
+    sim.writeToState(fin_p)
+    assert compare_states(fin_o, fin_p) == []
+    with pytest.raises(cbm.CBMError):
+        sim.updateMFInput(np.zeros(st.con("numMF"), dtype=np.uint8))

@@ -86,3 +86,26 @@ def test_reference_sharded_path_equals_single(tmp_path, gpus):
     single = cbmtest.ref_run(st, mf, [7], None)
     sharded = cbmtest.ref_run(st, mf, [7], None, num_gpus=gpus)
     assert np.array_equal(single, sharded)
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+def test_oracle_protocol_matches_reference_driver(tmp_path):
+    """The oracle's eyelid driver (MF generation, US, plasticity window,
+    eyelid integrator, records) against the reference's PoissonRegenCells and
+    EyelidIntegrator driven in the order of ECManagementDelay, over 3 short
+    trials of the reference's 16K network."""
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol()
+    o = Oracle(st, seeds=[7])
+    rates = cbmtest.protocol_rates(o.num["MF"], seed=1)
+    steps = 3 * proto["trialSteps"]
+    tr_o, nc, pc, eye = o.run_protocol(proto, rates, steps)
+    tr_r, rec_r = cbmtest.ref_run_protocol(st, proto, rates, steps, [7])
+    assert tr_r.size == tr_o.size
+    assert cbmtest.same_values(tr_r, tr_o.ravel()).all()
+    rec_o = np.concatenate([nc.view(np.uint8), pc.view(np.uint8), eye.view(np.uint8)])
+    assert rec_r.size == rec_o.size
+    assert cbmtest.same_values(rec_r.view(np.float32)[-eye.size:], eye).all()
+    assert np.array_equal(rec_r[: nc.nbytes + pc.nbytes], rec_o[: nc.nbytes + pc.nbytes])
+    # the protocol did something: CS trials spike NCs and move the eyelid
+    assert nc.sum() > 0 and eye.max() > 0
