@@ -94,6 +94,15 @@ def _load():
         "cbm_sim_last_tail_ms": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_run_flushed": (I, [P, U64, U64, ctypes.POINTER(F)]),
         "cbm_sim_set_eyelid_protocol": (I, [P, P]),
+        "cbm_batch_create": (I, [P, U32, P, I, P]),
+        "cbm_batch_destroy": (None, [P]),
+        "cbm_batch_set_eyelid_protocol": (I, [P, U32, P]),
+        "cbm_batch_run": (I, [P, U64, U32, ctypes.POINTER(F)]),
+        "cbm_batch_autotune": (I, [P, U32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(F)]),
+        "cbm_batch_trial_record_bytes": (U64, [P, U32, I]),
+        "cbm_batch_trial_record": (I, [P, U32, I, P, U64]),
+        "cbm_batch_write_to_state": (I, [P, U32]),
+        "cbm_batch_num_gr": (U64, [P]),
         "cbm_sim_trial_record_bytes": (U64, [P, I]),
         "cbm_sim_trial_record": (I, [P, I, P, U64]),
         "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
@@ -368,6 +377,69 @@ class CBMSimCore:
         _check(lib.cbm_sim_pass_geometry(self._h, *[ctypes.byref(x) for x in v]))
         kind = ("grPassKernel", "grPassTmaKernel", "grPassPersistentKernel")[v[0].value]
         return kind, v[1].value, v[2].value, v[3].value
+
+
+class CBMBatch:
+    """Independent networks advanced together (cbm_batch_*): one GR-pass
+    launch over all of them per step, each driven by its own device protocol."""
+
+    def __init__(self, states, mzoneRSeeds=None, device=0):
+        self.states = list(states)
+        arr = (ctypes.c_void_p * len(self.states))(*[st._h for st in self.states])
+        seeds = None
+        if mzoneRSeeds is not None:
+            seeds = np.ascontiguousarray(np.concatenate([np.atleast_1d(np.asarray(x, dtype=np.int32))
+                                                          for x in mzoneRSeeds]), dtype=np.int32)
+        self._h = ctypes.c_void_p()
+        self._protocols = [None] * len(self.states)
+        _check(lib.cbm_batch_create(arr, len(self.states), _ptr(seeds), device, ctypes.byref(self._h)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.cbm_batch_destroy(self._h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    def set_eyelid_protocol(self, i, rates, **protocol):
+        rates = np.ascontiguousarray(rates, dtype=np.float32)
+        p = EyelidProtocol.from_fields(rates, protocol)
+        _check(lib.cbm_batch_set_eyelid_protocol(self._h, i, ctypes.byref(p)))
+        self._protocols[i] = protocol
+
+    def run(self, nsteps, chunk=50):
+        ms = ctypes.c_float()
+        _check(lib.cbm_batch_run(self._h, nsteps, chunk, ctypes.byref(ms)))
+        return ms.value
+
+    def autotune(self, nsteps=100):
+        """Time every GR-pass geometry on a scratch copy; keep the fastest.
+        Returns (\"kind,W,RW,S,B,M\", ms)."""
+        buf = ctypes.create_string_buffer(64)
+        ms = ctypes.c_float()
+        _check(lib.cbm_batch_autotune(self._h, nsteps, buf, 64, ctypes.byref(ms)))
+        return buf.value.decode(), ms.value
+
+    def trial_record(self, i, kind):
+        k = {"nc": 0, "pc": 1, "eyelid": 2}[kind]
+        n = lib.cbm_batch_trial_record_bytes(self._h, i, k)
+        if not n:
+            raise CBMError(1, "no protocol is running on that instance")
+        out = np.empty(n // 4, dtype=np.float32 if kind == "eyelid" else np.uint32)
+        _check(lib.cbm_batch_trial_record(self._h, i, k, out.ctypes.data, n))
+        trials = max(1, self._protocols[i]["numDataTrials"])
+        if kind == "eyelid":
+            return out.reshape(trials, -1)
+        return out.reshape(trials, -1, self.states[i].con("numNC" if kind == "nc" else "numPC"))
+
+    def writeToState(self, i, path=None):
+        _check(lib.cbm_batch_write_to_state(self._h, i))
+        if path is not None:
+            self.states[i].writeState(path)
+
+    def num_gr(self):
+        return lib.cbm_batch_num_gr(self._h)
 
 
 _PROTOCOL_FIELDS = [("trialSteps", ctypes.c_uint32), ("csOn", ctypes.c_int32), ("csOff", ctypes.c_int32),

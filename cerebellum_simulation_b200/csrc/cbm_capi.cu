@@ -1,6 +1,8 @@
 // C ABI (include/cbm_b200.h) over the state and simulator classes.
 #include "../../include/cbm_b200.h"
 
+#include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -340,6 +342,145 @@ int cbm_sim_trial_record(cbm_sim *sim, int kind, void *dst, uint64_t bytes)
 	NEED(sim); NEED(dst);
 	TRY(NET(sim).readRecord(kind, dst, (size_t)bytes, sim->sim.stream()));
 	return CBM_OK;
+}
+
+// ---------------------------------------------------------------- batches
+struct cbm_batch {
+	Simulator sim;
+	std::vector<cbm_state *> states;
+	std::vector<std::vector<int>> seeds;
+	int device = 0;
+	// protocols as set, with copies of their rate tables (for the autotuner's scratch copy)
+	std::vector<int> hasProto;
+	std::vector<cbm_eyelid_protocol> protos;
+	std::vector<std::vector<float>> rates;
+};
+
+static int batchBuild(Simulator &sim, const std::vector<cbm_state *> &states, const std::vector<std::vector<int>> &seeds,
+		int device)
+{
+	std::vector<State *> st;
+	for (cbm_state *s : states) st.push_back(&s->st);
+	std::string e = sim.create(st, seeds, device, 2);
+	if (!e.empty()) return fail(classify(e), e);
+	return CBM_OK;
+}
+
+int cbm_batch_create(cbm_state *const *states, unsigned n, const int *mzoneSeeds, int device, cbm_batch **out)
+{
+	NEED(states); NEED(out);
+	if (n == 0) return fail(CBM_ERR_ARG, "empty batch");
+	cbm_batch *b = new (std::nothrow) cbm_batch();
+	if (!b) return fail(CBM_ERR_ARG, "out of host memory");
+	size_t k = 0;
+	for (unsigned i = 0; i < n; i++) {
+		if (!states[i]) { delete b; return fail(CBM_ERR_ARG, "null state"); }
+		b->states.push_back(states[i]);
+		std::vector<int> sd;
+		if (mzoneSeeds) sd.assign(mzoneSeeds + k, mzoneSeeds + k + states[i]->st.numZones);
+		k += states[i]->st.numZones;
+		b->seeds.push_back(sd);
+	}
+	b->device = device;
+	b->hasProto.assign(n, 0);
+	b->protos.resize(n);
+	b->rates.resize(n);
+	int rc = batchBuild(b->sim, b->states, b->seeds, device);
+	if (rc != CBM_OK) { delete b; return rc; }
+	*out = b;
+	return CBM_OK;
+}
+
+void cbm_batch_destroy(cbm_batch *b) { delete b; }
+
+#define BATCH_OK(b, i) do { NEED(b); if ((i) >= (b)->states.size()) return fail(CBM_ERR_ARG, "instance out of range"); } while (0)
+
+int cbm_batch_set_eyelid_protocol(cbm_batch *b, unsigned i, const cbm_eyelid_protocol *p)
+{
+	BATCH_OK(b, i); NEED(p);
+	TRY(b->sim.setProtocol(i, *p));
+	const uint32_t M = b->states[i]->st.cp.numMF;
+	std::vector<float> &r = b->rates[i];
+	r.resize(3ull * M);
+	memcpy(r.data(), p->mfFreqBG, 4ull * M);
+	memcpy(r.data() + M, p->mfFreqCSTonic, 4ull * M);
+	memcpy(r.data() + 2 * M, p->mfFreqCSPhasic, 4ull * M);
+	b->protos[i] = *p;
+	b->hasProto[i] = 1;
+	return CBM_OK;
+}
+
+int cbm_batch_run(cbm_batch *b, uint64_t nsteps, uint32_t chunk, float *gpuMs)
+{
+	NEED(b);
+	TRY(b->sim.runGraph(nsteps, chunk, false));
+	if (gpuMs) *gpuMs = b->sim.lastGraphMs();
+	return CBM_OK;
+}
+
+int cbm_batch_autotune(cbm_batch *b, uint32_t nsteps, char *choice, size_t choiceLen, float *ms)
+{
+	NEED(b);
+	if (nsteps == 0) return fail(CBM_ERR_ARG, "nsteps must be positive");
+	const uint32_t chunk = std::min<uint32_t>(nsteps, 25);
+	PassGeometry best;
+	float bestMs = -1;
+	{
+		Simulator scratch;
+		int rc = batchBuild(scratch, b->states, b->seeds, b->device);
+		if (rc != CBM_OK) return rc;
+		for (size_t i = 0; i < b->states.size(); i++) {
+			if (!b->hasProto[i]) continue;
+			cbm_eyelid_protocol p = b->protos[i];
+			const uint32_t M = b->states[i]->st.cp.numMF;
+			p.mfFreqBG = b->rates[i].data();
+			p.mfFreqCSTonic = b->rates[i].data() + M;
+			p.mfFreqCSPhasic = b->rates[i].data() + 2 * M;
+			TRY(scratch.setProtocol(i, p));
+		}
+		for (const PassGeometry &g : scratch.passCandidates()) {
+			if (!scratch.usePassGeometry(g).empty()) continue;
+			TRY(scratch.runGraph(2 * chunk, chunk, false));  // warm-up and capture
+			TRY(scratch.runGraph(nsteps - nsteps % chunk ? nsteps - nsteps % chunk : chunk, chunk, false));
+			const float t = scratch.lastGraphMs();
+			if (bestMs < 0 || t < bestMs) { bestMs = t; best = g; }
+		}
+	}
+	if (bestMs < 0) return fail(CBM_ERR_UNSUPPORTED, "no GR-pass geometry runs this batch");
+	TRY(b->sim.usePassGeometry(best));
+	if (choice && choiceLen) snprintf(choice, choiceLen, "%d,%d,%d,%d,%d,%d", best.kind, best.W, best.RW, best.S, best.B, best.M);
+	if (ms) *ms = bestMs;
+	return CBM_OK;
+}
+
+uint64_t cbm_batch_trial_record_bytes(cbm_batch *b, unsigned i, int kind)
+{
+	if (!b || i >= b->states.size()) return 0;
+	return b->sim.net(i).recordBytes(kind);
+}
+
+int cbm_batch_trial_record(cbm_batch *b, unsigned i, int kind, void *dst, uint64_t bytes)
+{
+	BATCH_OK(b, i); NEED(dst);
+	TRY(b->sim.sync());
+	TRY(b->sim.net(i).readRecord(kind, dst, (size_t)bytes, b->sim.stream()));
+	return CBM_OK;
+}
+
+int cbm_batch_write_to_state(cbm_batch *b, unsigned i)
+{
+	BATCH_OK(b, i);
+	TRY(b->sim.sync());
+	TRY(b->sim.net(i).writeToState(b->sim.stream()));
+	return CBM_OK;
+}
+
+uint64_t cbm_batch_num_gr(cbm_batch *b)
+{
+	if (!b) return 0;
+	uint64_t n = 0;
+	for (cbm_state *s : b->states) n += s->st.cp.numGR;
+	return n;
 }
 
 int cbm_sim_last_tail_ms(cbm_sim *sim, float *ms)

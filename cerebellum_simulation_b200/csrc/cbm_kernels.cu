@@ -521,6 +521,23 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	template __global__ void grPassTmaKernel<W, RW, S, B, M>(const DevNet *const *, const uint32_t *, int, uint32_t);
 CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_INST)
 
+int passTmaConfigCount()
+{
+	int n = 0;
+#define CBM_PASS_TMA_COUNT(w, rw, s, b, m) n++;
+	CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_COUNT)
+#undef CBM_PASS_TMA_COUNT
+	return n;
+}
+
+void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M)
+{
+	int k = 0;
+#define CBM_PASS_TMA_NTH(w, rw, s, b, m) if (k++ == i) { *W = w; *RW = rw; *S = s; *B = b; *M = m; return; }
+	CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_NTH)
+#undef CBM_PASS_TMA_NTH
+}
+
 const void *passTmaKernelFor(int W, int RW, int S, int B, int M)
 {
 #define CBM_PASS_TMA_PICK(w, rw, s, b, m) \

@@ -15,6 +15,9 @@ __global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOff
 // (0: any count); launched with 32 * (W + 1) threads and the grPassKernel
 // arguments.  Returns null for a geometry that is not compiled in.
 const void *passTmaKernelFor(int W, int RW, int S, int B, int M);
+// The compiled per-tile geometries, in table order.
+int passTmaConfigCount();
+void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M);
 // Persistent single-network TMA GR pass: W consumer warps (2W rows per
 // unit), S stages, B resident CTAs per SM, slot bound M; grid of any size,
 // 32 * (W + 1) threads, the grPassKernel arguments with one network.

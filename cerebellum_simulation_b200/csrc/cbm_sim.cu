@@ -922,10 +922,33 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 	if (tailSmem_ > 48 * 1024)
 		CK(cudaFuncSetAttribute(tailKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tailSmem_), "tail smem");
 
-	// TMA GR pass: W consumer warps of RW rows each per stage, S stages deep;
-	// every network of the set must have 32-cell tile rows and at least
-	// W*RW rows per tile.  CBM_PASS_TMA="W,RW,S" picks another compiled
-	// geometry (tuning), CBM_PASS_TMA=0 the plain pass kernel.
+	// GR-pass kernel: the per-tile TMA pass with a default geometry where
+	// every network has 32-cell tile rows, else the plain pass.
+	// CBM_PASS_TMA="W,RW,S,B,M" / CBM_PASS_PERSIST="W,S,B,M" pick another
+	// compiled geometry (tuning), CBM_PASS_TMA=0 the plain pass kernel.
+	PassGeometry g;
+	if (const char *env = getenv("CBM_PASS_PERSIST")) {
+		if (strcmp(env, "0") != 0) {
+			g.kind = 2;
+			if (sscanf(env, "%d,%d,%d,%d", &g.W, &g.S, &g.B, &g.M) != 4) return "CBM_PASS_PERSIST must be W,S,B,M";
+			return usePassGeometry(g);
+		}
+	}
+	if (const char *env = getenv("CBM_PASS_TMA")) {
+		if (!strcmp(env, "0")) { g.kind = 0; return usePassGeometry(g); }
+		g.kind = 1;
+		if (sscanf(env, "%d,%d,%d,%d,%d", &g.W, &g.RW, &g.S, &g.B, &g.M) != 5) return "CBM_PASS_TMA must be W,RW,S,B,M";
+		return usePassGeometry(g);
+	}
+	const std::vector<PassGeometry> cands = passCandidates();
+	return usePassGeometry(cands.front());
+}
+
+std::vector<PassGeometry> Simulator::passCandidates() const
+{
+	// the default first: 4 consumer warps of 1 row, 4 stages, 4 CTAs/SM,
+	// slot loops for at most 4 slots (8,1,3,2 with open slot loops past 4)
+	std::vector<PassGeometry> out;
 	bool tma = !nets_.empty();
 	uint32_t minRows = UINT32_MAX, maxSlots = 0;
 	for (Network *n : nets_) {
@@ -933,77 +956,92 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 		minRows = std::min(minRows, n->passRows());
 		maxSlots = std::max({maxSlots, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutSlots});
 	}
-	int W = 4, RW = 1, S = 4, B = 4, M = 4;
-	if (maxSlots > 4) { W = 8; S = 3; B = 2; M = 0; }
-	if (const char *env = getenv("CBM_PASS_TMA")) {
-		if (!strcmp(env, "0")) tma = false;
-		else if (sscanf(env, "%d,%d,%d,%d,%d", &W, &RW, &S, &B, &M) != 5 || !passTmaKernelFor(W, RW, S, B, M) ||
-				(M > 0 && maxSlots > (uint32_t)M))
-			return "CBM_PASS_TMA names a geometry that is not compiled in or does not fit the network";
-	}
-	if (tma && (uint32_t)(W * RW) > minRows) {
-		// small tiles: fewer rows per stage
-		const int cand[][5] = {{4, 1, 4, 1, 0}, {2, 1, 4, 1, 0}, {1, 1, 4, 1, 0}};
-		tma = false;
-		for (const int *c : cand)
-			if ((uint32_t)(c[0] * c[1]) <= minRows) { W = c[0]; RW = c[1]; S = c[2]; B = c[3]; M = c[4]; tma = true; break; }
-	}
-	// A single network may run the persistent TMA pass instead: W consumer
-	// warps (2W rows per unit), S stages, B resident CTAs per SM, slot bound
-	// M, chosen with CBM_PASS_PERSIST="W,S,B,M".
-	if (tma && nets_.size() == 1) {
-		int pW = 2, pS = 4, pB = 4, pM = maxSlots <= 4 ? 4 : 0;
-		if (pM == 0) pB = 2;
-		bool persist = false;  // measured slower than the per-tile pass on the 1M network
-		if (const char *env = getenv("CBM_PASS_PERSIST")) {
-			if (!strcmp(env, "0")) persist = false;
-			else if (sscanf(env, "%d,%d,%d,%d", &pW, &pS, &pB, &pM) != 4 || !passPersistentKernelFor(pW, pS, pB, pM) ||
-					(pM > 0 && maxSlots > (uint32_t)pM))
-				return "CBM_PASS_PERSIST names a geometry that is not compiled in or does not fit the network";
-			else persist = true;
-		}
-		while (persist && (uint32_t)(2 * pW) > minRows) pW /= 2;
-		if (persist && pW >= 1 && !passPersistentKernelFor(pW, pS, pB, pM)) { pS = 4; pB = 2; pM = 0; }
-		const void *fn = persist && pW >= 1 ? passPersistentKernelFor(pW, pS, pB, pM) : nullptr;
-		if (fn) {
-			Network &n = *nets_[0];
-			const uint32_t R = (uint32_t)(2 * pW);
-			const PassLayout L = passLayout(R, n.dev().nMFSlots, n.dev().nGOSlots, n.dev().nOutSlots, n.dev().numZones);
-			const size_t smem = 128 + (size_t)pS * L.bytes + 16ull * pS + 4ull * n.dev().numPC * n.dev().numZones +
-				32ull * (n.dev().mfWords + n.dev().goWords);
-			if (smem <= 227 * 1024) {
-				CKS(n.buildPassMaps(R));
-				CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "pass smem");
-				int perSM = 0, numSMs = 0;
-				CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, 32 * (pW + 1), smem), "pass occupancy");
-				CK(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device), "SM count");
-				const uint32_t units = n.dev().numPC * n.dev().tilesPerPC * (n.passRows() / R);
-				passTmaFn_ = fn;
-				passTmaW_ = (uint32_t)pW;
-				passTmaR_ = R;
-				passTmaS_ = (uint32_t)pS;
-				passTmaSmem_ = smem;
-				passGrid_ = std::min<uint32_t>(units, (uint32_t)std::max(1, perSM) * (uint32_t)numSMs);
-				passPersistent_ = true;
-				return "";
-			}
-		}
-	}
 	if (tma) {
-		const uint32_t R = (uint32_t)(W * RW);
-		size_t smem = 0;
-		for (Network *n : nets_) smem = std::max(smem, n->passTmaSmemBytes(R, (uint32_t)S));
-		if (smem <= 227 * 1024) {
-			passGrid_ = passBlocks_;
-			for (Network *n : nets_) CKS(n->buildPassMaps(R));
-			passTmaFn_ = passTmaKernelFor(W, RW, S, B, M);
-			passTmaW_ = (uint32_t)W;
-			passTmaR_ = R;
-			passTmaS_ = (uint32_t)S;
-			passTmaSmem_ = smem;
-			CK(cudaFuncSetAttribute(passTmaFn_, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "pass smem");
+		PassGeometry d;
+		d.kind = 1;
+		if (maxSlots <= 4) { d.W = 4; d.RW = 1; d.S = 4; d.B = 4; d.M = 4; }
+		else { d.W = 8; d.RW = 1; d.S = 3; d.B = 2; d.M = 0; }
+		if ((uint32_t)(d.W * d.RW) <= minRows) out.push_back(d);
+		for (int i = 0; i < passTmaConfigCount(); i++) {
+			PassGeometry c;
+			c.kind = 1;
+			passTmaConfig(i, &c.W, &c.RW, &c.S, &c.B, &c.M);
+			if ((uint32_t)(c.W * c.RW) > minRows || (c.M > 0 && maxSlots > (uint32_t)c.M)) continue;
+			if (c.W == d.W && c.RW == d.RW && c.S == d.S && c.B == d.B && c.M == d.M) continue;
+			out.push_back(c);
 		}
 	}
+	PassGeometry plain;
+	plain.kind = 0;
+	out.push_back(plain);
+	return out;
+}
+
+std::string Simulator::usePassGeometry(const PassGeometry &g)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	uint32_t minRows = UINT32_MAX, maxSlots = 0;
+	bool capable = !nets_.empty();
+	for (Network *n : nets_) {
+		capable = capable && n->passTmaCapable();
+		minRows = std::min(minRows, n->passRows());
+		maxSlots = std::max({maxSlots, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutSlots});
+	}
+	if (g.kind == 0) {
+		passTmaFn_ = nullptr;
+		passPersistent_ = false;
+		passTmaW_ = passTmaR_ = passTmaS_ = 0;
+		passGeom_ = g;
+		if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
+		if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+		return "";
+	}
+	if (!capable) return "the TMA GR pass needs tiles of 32-cell rows in every network";
+	if (g.M > 0 && maxSlots > (uint32_t)g.M) return "a network has more synapse slots than the geometry's slot bound";
+	const void *fn = nullptr;
+	uint32_t R = 0, threads = 0, grid = passBlocks_;
+	size_t smem = 0;
+	if (g.kind == 1) {
+		fn = passTmaKernelFor(g.W, g.RW, g.S, g.B, g.M);
+		if (!fn) return "per-tile GR-pass geometry not compiled in";
+		R = (uint32_t)(g.W * g.RW);
+		if (R > minRows) return "more rows per stage than a tile has";
+		for (Network *n : nets_) smem = std::max(smem, n->passTmaSmemBytes(R, (uint32_t)g.S));
+		threads = 32u * (g.W + 1);
+	} else {
+		if (nets_.size() != 1) return "the persistent GR pass runs one network";
+		fn = passPersistentKernelFor(g.W, g.S, g.B, g.M);
+		if (!fn) return "persistent GR-pass geometry not compiled in";
+		R = (uint32_t)(2 * g.W);
+		if (R > minRows) return "more rows per unit than a tile has";
+		Network &n = *nets_[0];
+		const PassLayout L = passLayout(R, n.dev().nMFSlots, n.dev().nGOSlots, n.dev().nOutSlots, n.dev().numZones);
+		smem = 128 + (size_t)g.S * L.bytes + 16ull * g.S + 4ull * n.dev().numPC * n.dev().numZones +
+			32ull * (n.dev().mfWords + n.dev().goWords);
+		threads = 32u * (g.W + 1);
+	}
+	if (smem > 227 * 1024) return "GR-pass geometry needs more shared memory than a CTA has";
+	for (Network *n : nets_) CKS(n->buildPassMaps(R));
+	CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "pass smem");
+	if (g.kind == 2) {
+		int perSM = 0, numSMs = 0;
+		CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, (int)threads, smem), "pass occupancy");
+		CK(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device_), "SM count");
+		Network &n = *nets_[0];
+		const uint32_t units = n.dev().numPC * n.dev().tilesPerPC * (n.passRows() / R);
+		grid = std::min<uint32_t>(units, (uint32_t)std::max(1, perSM) * (uint32_t)numSMs);
+	}
+	passTmaFn_ = fn;
+	passPersistent_ = g.kind == 2;
+	passTmaW_ = (uint32_t)g.W;
+	passTmaR_ = R;
+	passTmaS_ = (uint32_t)g.S;
+	passTmaSmem_ = smem;
+	passGrid_ = grid;
+	passGeom_ = g;
+	// captured graphs hold the old kernel
+	if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
+	if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
 	return "";
 }
 

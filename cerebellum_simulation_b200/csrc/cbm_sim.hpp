@@ -33,6 +33,12 @@ struct DeviceBuf {
 
 class Network;
 
+// A GR-pass kernel choice: kind 0 plain, 1 per-tile TMA (W consumer warps of
+// RW rows, S stages, B CTAs/SM, slot bound M), 2 persistent TMA (W, S, B, M).
+struct PassGeometry {
+	int kind = 0, W = 0, RW = 1, S = 0, B = 0, M = 0;
+};
+
 // A set of networks that advance together: one network for the drop-in
 // CBMSimCore path, many for the batched sweep.
 class Simulator {
@@ -68,6 +74,11 @@ public:
 	// rows per stage and stages of the TMA GR pass (0, 0 when the plain pass runs)
 	uint32_t passStageRows() const { return passTmaR_; }
 	uint32_t passStages() const { return passTmaS_; }
+	// GR-pass kernels that fit every network (the default first), the one in
+	// use, and switching to another (graphs are re-captured).
+	std::vector<PassGeometry> passCandidates() const;
+	const PassGeometry &passGeometryInUse() const { return passGeom_; }
+	std::string usePassGeometry(const PassGeometry &g);
 	// Device error word of every network (kErr* bits): non-empty on error.
 	std::string checkDeviceErrors();
 	void passGeometry(unsigned *kind, unsigned *warps, unsigned *rows, unsigned *stages) const
@@ -95,6 +106,7 @@ private:
 	const void *passTmaFn_ = nullptr;
 	uint32_t passTmaW_ = 0, passTmaR_ = 0, passTmaS_ = 0, passGrid_ = 0;
 	bool passPersistent_ = false;
+	PassGeometry passGeom_;
 	size_t passTmaSmem_ = 0;
 	cudaGraphExec_t graphExec_ = nullptr;
 	uint32_t graphChunk_ = 0;

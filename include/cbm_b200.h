@@ -242,6 +242,33 @@ uint64_t cbm_sim_trial_record_bytes(cbm_sim *sim, int kind);
 /* Copy a record of the running protocol to host memory. */
 int cbm_sim_trial_record(cbm_sim *sim, int kind, void *dst, uint64_t bytes);
 
+/* ---- Batched instances (no counterpart in the reference, which runs one
+ * network per CBMSimCore).  n independent networks of any sizes, seeds and
+ * parameters advance together: every step is one GR-pass launch over all of
+ * them and one small-cell launch with two CTAs per network, replayed as CUDA
+ * graphs.  Each instance is driven by a device protocol
+ * (cbm_batch_set_eyelid_protocol); the states must outlive the batch. */
+typedef struct cbm_batch cbm_batch;
+
+/* mzoneSeeds: n x (that state's zone count) seeds, or NULL (1000 + zone). */
+int cbm_batch_create(cbm_state *const *states, unsigned n, const int *mzoneSeeds, int device, cbm_batch **out);
+void cbm_batch_destroy(cbm_batch *b);
+int cbm_batch_set_eyelid_protocol(cbm_batch *b, unsigned instance, const cbm_eyelid_protocol *protocol);
+/* Advance every instance nsteps steps (graphs of graphChunk steps); *gpuMs
+ * receives the device time (events on the launch stream), may be NULL. */
+int cbm_batch_run(cbm_batch *b, uint64_t nsteps, uint32_t graphChunk, float *gpuMs);
+/* Time every compiled GR-pass geometry that fits all instances on a scratch
+ * copy of the batch (the same states and protocols; the batch itself does not
+ * advance) over nsteps steps each, and keep the fastest.  *choice receives
+ * "kind,W,RW,S,B,M" and *ms its time; either may be NULL. */
+int cbm_batch_autotune(cbm_batch *b, uint32_t nsteps, char *choice, size_t choiceLen, float *ms);
+uint64_t cbm_batch_trial_record_bytes(cbm_batch *b, unsigned instance, int kind);
+int cbm_batch_trial_record(cbm_batch *b, unsigned instance, int kind, void *dst, uint64_t bytes);
+/* Write instance i's device state into its cbm_state (writeToState). */
+int cbm_batch_write_to_state(cbm_batch *b, unsigned instance);
+/* Total GR of the instances (GR updates per batch step). */
+uint64_t cbm_batch_num_gr(cbm_batch *b);
+
 /* Measurement helper, no counterpart in the reference: nsteps steps with
  * resident MF input, each launched alone after a write of a flushBytes
  * device buffer (an L2 flush when larger than the L2 cache); *stepMs is the
