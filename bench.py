@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--chunk", type=int, default=50)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="1m", choices=["1m", "batch"],
+                    help="1m: the 1M-GR eyelid network (default); batch: 64 uneven instances in one launch")
+    ap.add_argument("--instances", type=int, default=64)
     return ap.parse_args()
 
 
@@ -196,9 +199,110 @@ WORKLOAD = ("1M-GR eyelid network: 1,048,576 GR (4 MF + 3 GO inputs, 4 GO target
             "PF->PC LTD/LTP on")
 
 
+BATCH_SIZES = {18: (10, 8), 19: (10, 9), 20: (11, 9), 21: (11, 10)}  # log2 GR -> GR grid exponents
+
+
+def batch_workload(n, seed):
+    """Instances of the batched sweep: GR counts log-uniform in 256K..2M
+    (powers of two), 1024 GO, 1024 MF, 32 PC, own wiring seed, GO threshold
+    x0.8-1.2, PF->PC LTD step x0.5-2, eyelid protocol with own MF seed."""
+    from cerebellum_simulation_b200 import networks
+    rng = np.random.Generator(np.random.PCG64(seed + 4242))
+    out = []
+    for i in range(n):
+        p2 = int(np.clip(np.round(rng.uniform(18, 21)), 18, 21))
+        gx, gy = BATCH_SIZES[p2]
+        st = networks.build_random_network(gx, gy, 6, 4, 10, networks.act_params("dense"), seed=seed + 1000 + i,
+                                           go_out_per_gr=4, mf_per_go=16, vel=147)
+        go_scale = float(rng.uniform(0.8, 1.2))
+        ltd_scale = float(np.exp(rng.uniform(np.log(0.5), np.log(2.0))))
+        st.setActParam("threshBaseGO", st.act("threshBaseGO") * go_scale)
+        out.append((st, go_scale, ltd_scale))
+    return out
+
+
+def main_batch(args):
+    import torch
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(device)
+    t_build = time.time()
+    inst = batch_workload(args.instances, args.seed)
+    states = [x[0] for x in inst]
+    b = cbm.CBMBatch(states, [[7 + i] for i in range(len(states))], device=device)
+    for i, (st, go_scale, ltd_scale) in enumerate(inst):
+        bg, cs = networks.eyelid_mf_rates(st.con("numMF"), seed=args.seed + i)
+        rates = np.stack([bg, cs, cs])
+        proto = cbm.eyelid_protocol_defaults(st, mfSeed=args.seed + 17 * i + 1, numDataTrials=1)
+        proto["plastLTD"] *= ltd_scale
+        b.set_eyelid_protocol(i, rates, **proto)
+    build_s = time.time() - t_build
+    b.run(args.warmup, args.chunk)
+    choice, tune_ms = b.autotune(50)
+    b.run(args.chunk, args.chunk)
+    clocks = ClockSampler(device)
+    clocks.start()
+    ms = b.run(args.steps - args.steps % args.chunk or args.chunk, args.chunk)
+    clock_info = clocks.stop()
+    steps = args.steps - args.steps % args.chunk or args.chunk
+    gr = b.num_gr()
+    value = gr * steps / (ms / 1000.0)
+    # end to end through the public API: run, then read every instance's records
+    t0 = time.perf_counter()
+    b.run(steps, args.chunk)
+    d2h = 0
+    for i in range(len(states)):
+        for kind in ("nc", "pc", "eyelid"):
+            d2h += b.trial_record(i, kind).nbytes
+    e2e_s = time.perf_counter() - t0
+    sizes = [st.con("numGR") for st in states]
+    step_s = ms / 1000.0 / steps
+    # the plain alternative: the same instances one at a time through the
+    # single-network simulator (continuous graph replay), timed per GR size
+    plain_step_s = {}
+    for i, (st, _, _) in enumerate(inst):
+        n = st.con("numGR")
+        if n in plain_step_s:
+            continue
+        one = cbm.CBMSimCore(st, [7 + i], device=device)
+        bg, cs = networks.eyelid_mf_rates(st.con("numMF"), seed=args.seed + i)
+        one.set_eyelid_protocol(np.stack([bg, cs, cs]), **cbm.eyelid_protocol_defaults(st, mfSeed=i + 1))
+        one.run(2 * args.chunk, args.chunk)
+        t_ms, _ = one.run(10 * args.chunk, args.chunk)
+        plain_step_s[n] = t_ms / 1000.0 / (10 * args.chunk)
+        one.close()
+    plain_set_s = sum(20 * 5000 * plain_step_s[n] for n in sizes)
+    out = {
+        "metric": "batched GR-updates/s", "value": value, "unit": "GR-updates/s", "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (random wiring, MF from the on-device Poisson regenerating generator)",
+        "config": {"workload": f"batched sweep: {len(states)} independent eyelid-protocol instances in one "
+                               "launch, GR counts log-uniform 256K-2M (powers of two), 1024 GO, 1024 MF, 32 PC, "
+                               "GO threshold x0.8-1.2, PF->PC LTD step x0.5-2, own seeds",
+                   "instances": len(states), "total_gr": gr,
+                   "gr_sizes": {str(k): sizes.count(k) for k in sorted(set(sizes))},
+                   "graph_chunk": args.chunk, "autotuned_pass": choice,
+                   "l2": f"inputs larger than L2 (~{gr * 90 / 1e9:.1f} GB of per-step GR state)",
+                   "build_s": build_s},
+        "sweep": {"steps_per_set": 20 * 5000,
+                  "sets_per_hour": len(states) * 3600.0 / (20 * 5000 * step_s),
+                  "plain_sets_per_hour": len(states) * 3600.0 / plain_set_s,
+                  "plain_step_ms_by_gr": {str(k): v * 1000 for k, v in sorted(plain_step_s.items())}},
+        "e2e": {"value": gr * steps / e2e_s, "unit": "GR-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": d2h / steps},
+        "gpu_launches": 2 * steps + steps // args.chunk,
+        "clocks": clock_info,
+    }
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     assert args.warmup >= 3
+    if args.workload == "batch" and args.impl == "b200":
+        return main_batch(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
