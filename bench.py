@@ -46,8 +46,13 @@ def parse():
     ap.add_argument("--chunk", type=int, default=50)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="1m", choices=["1m", "batch"],
-                    help="1m: the 1M-GR eyelid network (default); batch: 64 uneven instances in one launch")
+    ap.add_argument("--workload", default="1m", choices=["1m", "batch", "surrogate"],
+                    help="1m: the 1M-GR eyelid network (default); batch: 64 uneven instances in one launch; "
+                         "surrogate: the surrogate-proposed sweep")
+    ap.add_argument("--train-instances", type=int, default=2000)
+    ap.add_argument("--trials", type=int, default=10)
+    ap.add_argument("--candidates", type=int, default=4096)
+    ap.add_argument("--simulate-top", type=int, default=256)
     ap.add_argument("--instances", type=int, default=64)
     return ap.parse_args()
 
@@ -298,11 +303,95 @@ def main_batch(args):
     print(json.dumps(out))
 
 
+def main_surrogate(args):
+    """Surrogate-proposed sweep: training trials from the batched simulator,
+    the tensor-core MLP ranks the candidates, the top ones are simulated in
+    full; compared with simulating every candidate one at a time."""
+    import torch
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import sweep
+    from cerebellum_simulation_b200.surrogate import MLP
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(device)
+    T = args.trials
+    with tempfile.TemporaryDirectory() as d:
+        base = os.path.join(d, "base.state")
+        import lzma
+        with lzma.open(os.path.join(ROOT, "tests", "golden", "ref16k.state.xz")) as f, open(base, "wb") as g:
+            g.write(f.read())
+        st = cbm.CBMState(base)
+        conn = sweep.nc_inputs_of(st)
+        num_mf = st.con("numMF")
+        # training trials
+        t0 = time.time()
+        p_tr, s_tr = sweep.draw_params(args.train_instances, seed=args.seed + 1)
+        tr, gpu_train = sweep.simulate(base, p_tr, s_tr, T, device=device)
+        wall_data = time.time() - t0
+        x = np.concatenate([sweep.features(p_tr, s_tr, [k] * len(p_tr), T, conn, num_mf) for k in range(1, T)])
+        y = np.concatenate([tr[:, k] for k in range(1, T)])
+        net = MLP(sweep.N_FEATURES, 256, 256, sweep.N_TRACE, max_batch=256, seed=args.seed + 3, device=device)
+        t0 = time.time()
+        loss = sweep.fit_surrogate(net, x, y, epochs=100, lr=1e-3, seed=args.seed + 4)
+        train_s = time.time() - t0
+        # screening of the candidates
+        p_c, s_c = sweep.draw_params(args.candidates, seed=args.seed + 7)
+        t0 = time.time()
+        xc = sweep.features(p_c, s_c, [T - 1] * len(p_c), T, conn, num_mf)
+        t1 = time.time()
+        pred = sweep.predict(net, xc)
+        infer_s = time.time() - t1
+        feat_s = t1 - t0
+        K = args.simulate_top
+        top = np.argsort(-sweep.objective(pred))[:K]
+        rnd = np.random.Generator(np.random.PCG64(args.seed + 9)).permutation(len(p_c))[:K]
+        t0 = time.time()
+        sim_top, gpu_top = sweep.simulate(base, p_c[top], s_c[top], T, device=device)
+        wall_top = time.time() - t0
+        sim_rnd, _ = sweep.simulate(base, p_c[rnd], s_c[rnd], T, device=device)
+        # the plain alternative: one candidate at a time through the single-network simulator
+        one = cbm.CBMSimCore(cbm.CBMState(base), [11], device=device)
+        proto = cbm.eyelid_protocol_defaults(st, mfSeed=1, numDataTrials=1, dataStartTrial=0, **sweep.TRIAL)
+        one.set_eyelid_protocol(sweep.mf_rates(num_mf, p_c[0], s_c[0]), **proto)
+        one.run(250, 250)
+        plain_ms, _ = one.run(T * sweep.TRIAL["trialSteps"], 250)
+        one.close()
+    plain_set_s = plain_ms / 1000.0
+    last_top = sim_top[:, T - 1]
+    err = pred[top] - last_top
+    rmse = float(np.sqrt(np.mean(err ** 2)))
+    surrogate_sweep_s = feat_s + infer_s + gpu_top
+    out = {
+        "metric": "sweep sets/hr vs plain", "value": len(p_c) * 3600.0 / surrogate_sweep_s, "unit": "sets/hr",
+        "n_gpus": 1, "steps": T * sweep.TRIAL["trialSteps"], "warmup": 250, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 simulation, bf16 MLP (fp32 accumulate)",
+        "data": "synthetic (the reference generator's 16K network, random parameter sets, device MF generator)",
+        "config": {"workload": f"surrogate-proposed sweep: {len(p_c)} candidate sets ranked by a 64-256-256-50 MLP "
+                               f"trained on {len(p_tr) * (T - 1)} trials of the batched simulator, top {K} simulated "
+                               f"in full ({T} trials of {sweep.TRIAL['trialSteps']} steps)",
+                   "l2": "inputs larger than L2 (batches of 256 networks)"},
+        "plain_sets_per_hour": 3600.0 / plain_set_s,
+        "speedup_vs_plain": (len(p_c) * plain_set_s) / surrogate_sweep_s,
+        "speedup_vs_plain_incl_training": (len(p_c) * plain_set_s) / (surrogate_sweep_s + gpu_train + train_s),
+        "surrogate": {"train_trials": int(len(y)), "train_loss_log": loss, "train_s": train_s,
+                      "training_data_gpu_s": gpu_train, "training_data_wall_s": wall_data,
+                      "inference_s": infer_s, "features_s": feat_s,
+                      "nc_trace_rmse_hz": rmse, "nc_trace_mean_hz": float(last_top.mean()),
+                      "nc_trace_rel_rmse": rmse / max(float(last_top.mean()), 1e-9),
+                      "nc_trace_median_abs_err_hz": float(np.median(np.abs(err))),
+                      "objective_top_mean": float(sweep.objective(last_top).mean()),
+                      "objective_random_mean": float(sweep.objective(sim_rnd[:, T - 1]).mean())},
+        "batched_top_gpu_s": gpu_top, "batched_top_wall_s": wall_top,
+    }
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     assert args.warmup >= 3
     if args.workload == "batch" and args.impl == "b200":
         return main_batch(args)
+    if args.workload == "surrogate" and args.impl == "b200":
+        return main_surrogate(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
