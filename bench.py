@@ -423,18 +423,17 @@ def main():
         return
 
     import torch
-    dist = None
+    from cerebellum_simulation_b200 import replicas
     if world > 1:
-        import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    dist, rank, world, local = replicas.init("nccl")
     device = local
     torch.cuda.set_device(device)
 
     import cerebellum_simulation_b200 as cbm
-    st = networks.config2_network(seed=args.seed + rank)
-    mf = networks.eyelid_mf_stream(1024, total_steps, seed=args.seed + rank)
-    sim = cbm.CBMSimCore(st, [7 + rank], device=device, resident_steps=total_steps)
+    st = networks.config2_network(seed=replicas.replica_seed(args.seed, rank))
+    mf = networks.eyelid_mf_stream(1024, total_steps, seed=replicas.replica_seed(args.seed, rank))
+    sim = cbm.CBMSimCore(st, [replicas.replica_seed(7, rank)], device=device, resident_steps=total_steps)
     bits = cbm.mf_bits(mf, sim.mf_words())
     sim.load_mf_stream(bits)
 
@@ -460,16 +459,13 @@ def main():
     sim.timer_start()
     run_protocol(sim, args.warmup + args.steps, args.steps, args.chunk)
     ms_cont = sim.timer_stop()
-    if dist:
-        t = torch.tensor([ms, ms_cont], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_cont = float(t[0].item()), float(t[1].item())
-    steps_per_s = world * args.steps / (ms / 1000.0)
-    cont_steps_per_s = world * args.steps / (ms_cont / 1000.0)
+    ms, ms_cont = replicas.max_over_ranks(dist, [ms, ms_cont], device=f"cuda:{device}")
+    steps_per_s = replicas.throughput(world, args.steps, ms)
+    cont_steps_per_s = replicas.throughput(world, args.steps, ms_cont)
 
     # roofline: GR-pass durations from events around each pass in the graph
     n_roof = min(args.steps, 1000)
-    sim2 = cbm.CBMSimCore(st, [7 + rank], device=device, resident_steps=n_roof + 3 * args.chunk)
+    sim2 = cbm.CBMSimCore(st, [replicas.replica_seed(7, rank)], device=device, resident_steps=n_roof + 3 * args.chunk)
     sim2.load_mf_stream(cbm.mf_bits(mf[: n_roof + 3 * args.chunk], sim2.mf_words()))
     sim2.run(2 * args.chunk, args.chunk, time_pass=True)
     _, pass_ms = sim2.run(n_roof - (n_roof % args.chunk) or args.chunk, args.chunk, time_pass=True)
@@ -484,7 +480,7 @@ def main():
 
     # end to end through the per-step C ABI
     n_e2e = min(args.steps, 2000)
-    sim3 = cbm.CBMSimCore(st, [7 + rank], device=device)
+    sim3 = cbm.CBMSimCore(st, [replicas.replica_seed(7, rank)], device=device)
     zone = sim3.getMZoneList()[0]
     for s in range(20):
         sim3.updateMFInput(mf[s])
@@ -498,11 +494,8 @@ def main():
         sim3.calcActivity()
         zone.exportAPNC()
     e2e_ms = sim3.timer_stop()
-    if dist:
-        t = torch.tensor([e2e_ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * n_e2e / (e2e_ms / 1000.0)
+    e2e_ms, = replicas.max_over_ranks(dist, [e2e_ms], device=f"cuda:{device}")
+    e2e = replicas.throughput(world, n_e2e, e2e_ms)
     h2d = sim3.mf_words() * 4
     d2h = st.con("numNC")
     sim3.close()
@@ -545,9 +538,7 @@ def main():
         if cpu:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
 
 
 if __name__ == "__main__":

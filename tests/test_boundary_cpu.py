@@ -1,5 +1,5 @@
 """CPU checks of the boundary: the C-ABI library loads and exports every
-function include/cbm_b200.h declares, state files round-trip byte for byte
+function the headers in include/ declare, state files round-trip byte for byte
 through the reference format, and malformed input fails with an error code."""
 import ctypes
 import os
@@ -14,10 +14,13 @@ ROOT = cbmtest.ROOT
 
 
 def declared_functions():
-    with open(os.path.join(ROOT, "include", "cbm_b200.h")) as f:
-        text = f.read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(cbm_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    for h in ("cbm_b200.h", "cbm_surrogate.h"):
+        with open(os.path.join(ROOT, "include", h)) as f:
+            text = f.read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(cbm_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_symbol():
