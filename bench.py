@@ -178,8 +178,9 @@ def profiled_traffic():
     return None
 
 
-def cpu_reference(state_path, mf, steps, threads):
-    """The reference's own calcActivity (oracle/_ref, OpenMP build) on host cores."""
+def cpu_reference(state_path, mf, steps, threads, warmup=0):
+    """The reference's own calcActivity (oracle/_ref, OpenMP build) on host cores:
+    warmup untimed steps, then steps timed ones (mf holds rows for both)."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_run_omp")
     if not os.path.exists(exe):
         exe = os.path.join(ROOT, "oracle", "_ref", "ref_run")
@@ -188,15 +189,16 @@ def cpu_reference(state_path, mf, steps, threads):
         return None
     with tempfile.TemporaryDirectory() as d:
         mfp = os.path.join(d, "mf.u8")
-        np.ascontiguousarray(mf[:steps], dtype=np.uint8).tofile(mfp)
+        np.ascontiguousarray(mf[:warmup + steps], dtype=np.uint8).tofile(mfp)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        out = subprocess.run([exe, state_path, mfp, str(steps), "-", "-", "7", "-t"], capture_output=True,
-                             text=True, env=env, check=True).stdout
+        out = subprocess.run([exe, state_path, mfp, str(warmup + steps), "-", "-", "7", "-t", "-w", str(warmup)],
+                             capture_output=True, text=True, env=env, check=True).stdout
     line = [l for l in out.splitlines() if l.startswith("{")][-1]
     r = json.loads(line)
     return {"value": r["steps_per_s"], "unit": "steps/s", "cores": threads, "kind": "reference",
-            "sample": f"{steps} steps of the same 1M-GR network and MF input (first {steps} ms of trial 1), "
-                      f"reference host code + CPU kernel restatement, OpenMP {threads} threads"}
+            "sample": f"{steps} steps of the same 1M-GR network and MF input (ms {warmup}-{warmup + steps} of "
+                      f"trial 1, after {warmup} untimed steps), reference host code + CPU kernel restatement, "
+                      f"OpenMP {threads} threads"}
 
 
 WORKLOAD = ("1M-GR eyelid network: 1,048,576 GR (4 MF + 3 GO inputs, 4 GO targets each), 1024 GO, 1024 MF, "
@@ -404,18 +406,18 @@ def main():
             return
         threads = os.cpu_count() or 1
         st = networks.config2_network(seed=args.seed)
-        n_ref = min(args.steps, 200)
-        mf = networks.eyelid_mf_stream(1024, n_ref + 3, seed=args.seed)
+        n_ref, w_ref = min(args.steps, 200), min(args.warmup, 200)
+        mf = networks.eyelid_mf_stream(1024, w_ref + n_ref + 3, seed=args.seed)
         with tempfile.TemporaryDirectory() as d:
             p = os.path.join(d, "c2.state")
             st.writeState(p)
-            res = cpu_reference(p, mf, n_ref, threads)
+            res = cpu_reference(p, mf, n_ref, threads, warmup=w_ref)
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
             return
         v = res["value"]
         print(json.dumps({"metric": "1 ms steps/s at 1M GR", "value": v, "unit": "steps/s", "impl": "reference",
-                          "n_gpus": args.gpus, "steps": n_ref, "warmup": 0, "ms_per_step": 1000.0 / v,
+                          "n_gpus": args.gpus, "steps": n_ref, "warmup": w_ref, "ms_per_step": 1000.0 / v,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                           "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host threads"},
                           "cpu_baseline": res,
@@ -505,7 +507,7 @@ def main():
         with tempfile.TemporaryDirectory() as d:
             p = os.path.join(d, "c2.state")
             st.writeState(p)
-            cpu = cpu_reference(p, mf, 200, os.cpu_count() or 1)
+            cpu = cpu_reference(p, mf, 200, os.cpu_count() or 1, warmup=20)
 
     launches = 2 * args.steps + (args.steps // args.chunk + 8)
     if rank == 0:

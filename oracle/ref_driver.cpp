@@ -159,7 +159,7 @@ int main(int argc, char **argv)
 {
 	if (argc < 6)
 	{
-		fprintf(stderr, "usage: ref_run STATE MFBYTES STEPS TRACE FINALSTATE [SEED...] [-e EVENTS] [-g NGPUP2] [-t]\n");
+		fprintf(stderr, "usage: ref_run STATE MFBYTES STEPS TRACE FINALSTATE [SEED...] [-e EVENTS] [-g NGPUP2] [-t] [-w WARMUP]\n");
 		return 2;
 	}
 	const char *statePath = argv[1], *mfPath = argv[2], *tracePath = argv[4], *finalPath = argv[5];
@@ -168,6 +168,7 @@ int main(int argc, char **argv)
 	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL;
 	int numGPUP2 = 0;
 	bool timeOnly = false;
+	unsigned long warm = 0;  // leading steps run before the clock starts
 	for (int i = 6; i < argc; i++)
 	{
 		if (!strcmp(argv[i], "-e") && i + 1 < argc) eventsPath = argv[++i];
@@ -175,6 +176,7 @@ int main(int argc, char **argv)
 		else if (!strcmp(argv[i], "-r") && i + 1 < argc) recordsPath = argv[++i];
 		else if (!strcmp(argv[i], "-g") && i + 1 < argc) numGPUP2 = atoi(argv[++i]);
 		else if (!strcmp(argv[i], "-t")) timeOnly = true;
+		else if (!strcmp(argv[i], "-w") && i + 1 < argc) warm = strtoul(argv[++i], NULL, 10);
 		else seeds.push_back(atoi(argv[i]));
 	}
 
@@ -257,6 +259,7 @@ int main(int argc, char **argv)
 	auto t0 = std::chrono::steady_clock::now();
 	for (unsigned long t = 1; t <= steps; t++)
 	{
+		if (t == warm + 1) t0 = std::chrono::steady_clock::now();
 		if (useProtocol)
 		{
 			const int time = (int)((t - 1) % trialSteps);
@@ -337,7 +340,7 @@ int main(int argc, char **argv)
 	double sec = std::chrono::duration<double>(t1 - t0).count();
 	if (tr) fclose(tr);
 	printf("{\"steps\": %lu, \"seconds\": %.6f, \"steps_per_s\": %.3f, \"num_gr\": %u}\n",
-			steps, sec, sec > 0 ? steps / sec : 0.0, cp->numGR);
+			steps - (warm < steps ? warm : steps), sec, sec > 0 ? (steps - (warm < steps ? warm : steps)) / sec : 0.0, cp->numGR);
 	fflush(stdout);
 
 	if (useProtocol)
