@@ -218,9 +218,43 @@ struct DevNet {
 	DevProtocol *proto;           // device-driven trial protocol, or null
 	const StageSeg *zoneSegs;     // arrays the microzone CTA stages in shared memory
 	uint32_t numZoneSegs;         // 0: the microzone CTA works on global memory
-	uint32_t zoneArenaBytes;
+	uint32_t zoneArenaBytes;      // staged arrays: read-only ones, then from zoneWbOff on the written ones
+	uint32_t zoneWbOff;
+	uint32_t zoneStageBytes;      // the whole staging block (stageBlockBytes)
 
 	DevZone zones[kMaxZones];
 };
+
+// Staging block of a network whose microzone arrays fit in shared memory: one
+// allocation that the microzone CTA copies as it is, laid out as its shared
+// memory copy: the descriptor, the step counter (tBase points here), the
+// staged arrays, then the StageSeg table.
+constexpr uint32_t kStageNetBytes = (uint32_t)((sizeof(DevNet) + 15) & ~(size_t)15);
+constexpr uint32_t kStageArenaOff = kStageNetBytes + 16;
+CBM_LAYOUT_FN uint32_t stageBlockBytes(uint32_t arenaBytes, uint32_t numSegs)
+{
+	return kStageArenaOff + arenaBytes + ((numSegs * (uint32_t)sizeof(StageSeg) + 15u) & ~15u);
+}
+
+// Inputs of a microzone step that other kernels write, copied into shared
+// memory after the staging block: the cbmExpf table, the MF spike bits of
+// step t, the PF->BC and PF->SC counts and the PF->PC partial sums of
+// pass(t-2) for every zone (byte offsets, 16-byte aligned).
+struct ZoneInputLayout {
+	uint32_t exp2, mf, bc, sc, pc, bytes;
+};
+CBM_LAYOUT_FN ZoneInputLayout zoneInputLayout(uint32_t mfWords, uint32_t numBC, uint32_t numSC, uint32_t Z,
+		uint32_t numPC, uint32_t bs)
+{
+	ZoneInputLayout L;
+	uint32_t o = 0;
+	L.exp2 = o; o += 256;
+	L.mf = o; o += (4 * mfWords + 15) & ~15u;
+	L.bc = o; o += (4 * numBC + 15) & ~15u;
+	L.sc = o; o += (4 * numSC + 15) & ~15u;
+	L.pc = o; o += (4 * Z * numPC * bs + 15) & ~15u;
+	L.bytes = o;
+	return L;
+}
 
 }  // namespace cbm

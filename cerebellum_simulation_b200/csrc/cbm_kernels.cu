@@ -40,8 +40,9 @@
 namespace cbm {
 
 // 2^(i/32) as doubles with i/32 folded out of the exponent field:
-// asuint64(2^(i/32)) - (i << 47).
-__constant__ uint64_t kExp2Tab[32] = {
+// asuint64(2^(i/32)) - (i << 47).  Kernels copy it into shared memory:
+// lanes index it with different i, which the constant cache would serialise.
+__device__ uint64_t kExp2Tab[32] = {
 	0x3ff0000000000000ull, 0x3fefd9b0d3158574ull, 0x3fefb5586cf9890full, 0x3fef9301d0125b51ull,
 	0x3fef72b83c7d517bull, 0x3fef54873168b9aaull, 0x3fef387a6e756238ull, 0x3fef1e9df51fdee1ull,
 	0x3fef06fe0a31b715ull, 0x3feef1a7373aa9cbull, 0x3feedea64c123422ull, 0x3feece086061892dull,
@@ -52,9 +53,10 @@ __constant__ uint64_t kExp2Tab[32] = {
 	0x3fef5818dcfba487ull, 0x3fef7c97337b9b5full, 0x3fefa4afa2a490daull, 0x3fefd0765b6e4540ull,
 };
 
-// exp of a float: x = (k + r) ln2/32, 2^(k/32) from the table, 2^(r/32) from
-// a cubic in r (coefficients of the published algorithm).
-__device__ float cbmExpf(float x)
+// exp of a float: x = (k + r) ln2/32, 2^(k/32) from the table (kExp2Tab or
+// a shared-memory copy), 2^(r/32) from a cubic in r (coefficients of the
+// published algorithm).
+__device__ float cbmExpf(float x, const uint64_t *__restrict__ tab)
 {
 	const uint32_t ux = __float_as_uint(x);
 	const uint32_t abstop = (ux >> 20) & 0x7ffu;
@@ -74,7 +76,7 @@ __device__ float cbmExpf(float x)
 	const uint64_t ki = (uint64_t)__double_as_longlong(kd);
 	kd = kd - shift;
 	const double r = fma(invLn2N, xd, -kd);
-	const uint64_t tb = kExp2Tab[ki & 31u] + (ki << 47);
+	const uint64_t tb = tab[ki & 31u] + (ki << 47);
 	const double s = __longlong_as_double((long long)tb);
 	const double z = fma(c0, r, c1);
 	const double r2 = r * r;
@@ -87,7 +89,7 @@ __device__ float cbmExpf(float x)
 __global__ void expfProbeKernel(const float *in, float *out, uint32_t n)
 {
 	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < n) out[i] = cbmExpf(in[i]);
+	if (i < n) out[i] = cbmExpf(in[i], kExp2Tab);
 }
 
 __device__ __forceinline__ uint32_t spikeBit(const uint32_t *bits, uint32_t idx)
@@ -869,7 +871,8 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 	const uint32_t numGO = N->numGO;
 	const uint32_t G = (uint32_t)((t - 1) & 1);
 	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
-	uint32_t *sMF = sm;
+	uint64_t *sExp2 = reinterpret_cast<uint64_t *>(sm);
+	uint32_t *sMF = sm + 64;
 	uint32_t *sMFGO = sMF + N->mfWords;  // MF->GO input counts of this step
 	float *sScale = reinterpret_cast<float *>(sMFGO + numGO);
 	float *sV = sScale + numGO;
@@ -877,6 +880,7 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 	uint8_t *sAp = reinterpret_cast<uint8_t *>(sTh + numGO);
 	for (uint32_t i = tid; i < N->mfWords; i += nThr) sMF[i] = mfW[i];
 	for (uint32_t i = tid; i < numGO; i += nThr) sMFGO[i] = 0;
+	if (tid < 32) sExp2[tid] = kExp2Tab[tid];
 	__syncthreads();
 
 	uint32_t *goIn = N->goCount + (size_t)G * numGO;
@@ -907,9 +911,9 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 			float glu = glu0;
 			glu = glu * N->gluDecayGO + totalGRIn * N->gluScaleGO * exp(-1.5 * glu);
 			float mg = mg0;
-			mg = mg * N->mGluRDecayGO + glu * N->mGluRScaleGO * cbmExpf(-mg);
+			mg = mg * N->mGluRDecayGO + glu * N->mGluRScaleGO * cbmExpf(-mg, sExp2);
 			float mgi = mgi0;
-			mgi = mgi * N->gMGluRIncDecayGO + mg * N->gMGluRIncScaleGO * cbmExpf(-mgi);
+			mgi = mgi * N->gMGluRIncDecayGO + mg * N->gMGluRIncScaleGO * cbmExpf(-mgi, sExp2);
 			N->gluGO[i] = glu; N->mGluRGO[i] = mg; N->gMGluRIncGO[i] = mgi;
 			N->gMGluRGO[i] = gMGluR0 * N->gMGluRDecGRtoGO + mgi * N->gMGluRScaleGRtoGO;
 			float th = thCur + (N->threshRestGO - thCur) * N->threshDecGO;
@@ -992,24 +996,32 @@ __device__ __forceinline__ void barSync(uint32_t id, uint32_t count)
 	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-__device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
+// Where the microzone role of step t finds the inputs that other kernels
+// wrote: shared-memory copies when the network is staged, else global memory
+// (mf, exp2 always in shared memory).  One copy per CTA, in shared memory.
+struct ZoneIn {
+	const uint32_t *mf;                 // MF spike bits of step t
+	const uint32_t *bcSum, *scSum;      // PF->BC / PF->SC counts of pass(t-2)
+	const float *pcPart[kMaxZones];     // [numPC][bs] PF->PC partial sums of pass(t-2) per zone
+	const uint64_t *exp2;               // cbmExpf table
+};
+
+__device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm, const ZoneIn &in)
 {
 	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u, warp = tid >> 5, nWarps = nThr >> 5;
 	const uint32_t Z = N->numZones;
 	const uint32_t numMF = N->numMF, numPC = N->numPC, numBC = N->numBC, numSC = N->numSC, numNC = N->numNC,
 		numIO = N->numIO;
 	const uint32_t R = (uint32_t)((t + 1) % 3);
-	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
 	const uint8_t *mfRaw = N->hasMFRaw ? N->mfRaw + (size_t)((t - 1) % N->mfRing) * numMF : nullptr;
 	HostCtl *ctl = N->ctl;
 	const uint32_t nMFNC = N->numpNCfromMFtoNC, nIONC = N->numpIOfromNCtoIO;
-	uint32_t *sMF = sm;
-	uint8_t *sApSC = reinterpret_cast<uint8_t *>(sMF + N->mfWords);
+	const uint32_t *sMF = in.mf;
+	const uint64_t *exp2 = in.exp2;
+	uint8_t *sApSC = reinterpret_cast<uint8_t *>(sm);
 	float *ncScratch = reinterpret_cast<float *>(sApSC + ((numSC + 15) & ~15u));
 	float *ioScratch = ncScratch + (size_t)Z * numNC * 2 * nMFNC;
 	int *sFlags = reinterpret_cast<int *>(ioScratch + (size_t)Z * numIO * nIONC);
-	for (uint32_t i = tid; i < N->mfWords; i += nThr) sMF[i] = mfW[i];
-	__syncthreads();
 
 	// The PC/BC/SC/MF updates (warps [0, half)) and the NC/IO updates (warps
 	// [half, all)) of a step do not read each other's results; the two warp
@@ -1021,123 +1033,93 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	// (tid, nThr, warp, nWarps) of the PC/BC/SC/MF warp group
 	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
 	// ---- phase 1 (cbmsimcore.cpp:192-200): PC and BC per zone, SC, and the
-	// MF bookkeeping.  The updates are independent; they run in rounds in
-	// which every thread first loads the inputs of its BC, SC and MF cells,
-	// then takes part in its warp's PC, then finishes its cells, so that the
-	// loads of a round are in flight together.
-	const uint32_t *bcSum = N->bcCount + (size_t)R * numBC;
-	const uint32_t *scSum = N->scCount + (size_t)R * numSC;
-	const uint32_t nBCTasks = Z * numBC, nPCTasks = Z * numPC;
-	uint32_t rounds = (nPCTasks + nWarps - 1) / nWarps;
-	rounds = max(rounds, (nBCTasks + nThr - 1) / nThr);
-	rounds = max(rounds, (numSC + nThr - 1) / nThr);
-	rounds = max(rounds, (numMF + nThr - 1) / nThr);
-	for (uint32_t rd = 0; rd < rounds; rd++) {
-		const uint32_t c = rd * nThr + tid;
-		const bool hasBC = c < nBCTasks, hasSC = c < numSC, hasMF = c < numMF;
-		// calcBCActivities inputs (mzone.cpp:228-256)
-		const uint32_t bz = hasBC ? c / numBC : 0, bi = hasBC ? c % numBC : 0;
-		uint32_t bInPF = 0, bInPC = 0, bApBuf = 0;
-		float bgPF0 = 0, bgPC0 = 0, bv0 = 0, bth0 = 0;
-		if (hasBC) {
-			const DevZone &Q = N->zones[bz];
-			bInPF = bcSum[bi]; bInPC = Q.inputPCBC[bi]; bApBuf = Q.apBufBC[bi];
-			bgPF0 = Q.gPFBC[bi]; bgPC0 = Q.gPCBC[bi]; bv0 = Q.vBC[bi]; bth0 = Q.threshBC[bi];
+	// MF bookkeeping; the updates are independent.
+	// calcPCActivities (mzone.cpp:187-226), one warp per PC; the SC
+	// conductances update elementwise, their sum runs in the reference's order
+	for (uint32_t task = warp; task < Z * numPC; task += nWarps) {
+		const uint32_t z = task / numPC, i = task % numPC;
+		const DevZone &Q = N->zones[z];
+		const float inputSum = pcRowTree(in.pcPart[z] + (size_t)i * N->bs, N->bs, lane);
+		float gSCPCSum = 0;
+		for (uint32_t j0 = 0; j0 < N->numpPCfromSCtoPC; j0 += 32) {
+			const uint32_t j = j0 + lane;
+			float g = 0;
+			if (j < N->numpPCfromSCtoPC) {
+				const size_t k = (size_t)i * N->numpPCfromSCtoPC + j;
+				const float g0 = Q.gSCPC[k];
+				const uint8_t inp = Q.inputSCPC[k];
+				g = g0;
+				g = g + N->gIncSCtoPC * (1 - g) * inp;
+				g = g * N->gDecSCtoPC;
+				Q.gSCPC[k] = g;
+			}
+			const uint32_t n = min(32u, N->numpPCfromSCtoPC - j0);
+			for (uint32_t q = 0; q < n; q++) gSCPCSum += __shfl_sync(0xffffffffu, g, q);
 		}
-		// calcSCActivities inputs (innet.cpp:892-911)
-		uint32_t sInPF = 0, sApBuf = 0;
-		float sg0 = 0, sv0 = 0, sthOld = 0;
-		if (hasSC) {
-			sInPF = scSum[c]; sApBuf = N->apBufSC[c];
-			sg0 = N->gPFSC[c]; sv0 = N->vSC[c]; sthOld = N->threshSC[c];
-		}
-		// updateMFInput's bookkeeping inputs (innet.cpp:800-815)
-		uint8_t mHist = 0;
-		uint32_t mApBuf = 0;
-		if (hasMF) { mHist = N->histMF[c]; mApBuf = N->apBufMF[c]; }
-
-		const uint32_t task = rd * nWarps + warp;
-		if (task < nPCTasks) {
-			const uint32_t z = task / numPC, i = task % numPC;
-			const DevZone &Q = N->zones[z];
-			// the PC's own state, loaded before any store of this task
+		if (lane == 0) {
 			const float gPF0 = Q.gPFPC[i], gBC0 = Q.gBCPC[i], vPC0 = Q.vPC[i], th0 = Q.threshPC[i];
 			const uint32_t inBC = Q.inputBCPC[i], apBuf = Q.apBufPC[i];
-			const float inputSum = pcRowTree(Q.pcPartial + ((size_t)R * numPC + i) * N->bs, N->bs, lane);
-			// calcPCActivities (mzone.cpp:187-226); the SC conductances update
-			// elementwise, their sum runs in the reference's order
-			float gSCPCSum = 0;
-			for (uint32_t j0 = 0; j0 < N->numpPCfromSCtoPC; j0 += 32) {
-				const uint32_t j = j0 + lane;
-				float g = 0;
-				if (j < N->numpPCfromSCtoPC) {
-					const size_t k = (size_t)i * N->numpPCfromSCtoPC + j;
-					const float g0 = Q.gSCPC[k];
-					const uint8_t in = Q.inputSCPC[k];
-					g = g0;
-					g = g + N->gIncSCtoPC * (1 - g) * in;
-					g = g * N->gDecSCtoPC;
-					Q.gSCPC[k] = g;
-				}
-				const uint32_t n = min(32u, N->numpPCfromSCtoPC - j0);
-				for (uint32_t q = 0; q < n; q++) gSCPCSum += __shfl_sync(0xffffffffu, g, q);
-			}
-			if (lane == 0) {
-				float gPF = gPF0 + inputSum * N->gIncGRtoPC;
-				gPF = gPF * N->gDecGRtoPC;
-				Q.gPFPC[i] = gPF;
-				float gBC = gBC0 + inBC * N->gIncBCtoPC;
-				gBC = gBC * N->gDecBCtoPC;
-				Q.gBCPC[i] = gBC;
-				float vPC = vPC0;
-				vPC = vPC + (N->gLeakPC * (N->eLeakPC - vPC)) - (gPF * vPC) +
-					(gBC * (N->eBCtoPC - vPC)) + (gSCPCSum * (N->eSCtoPC - vPC));
-				Q.vPC[i] = vPC;
-				float th = th0 + (N->threshDecPC * (N->threshRestPC - th0));
-				const uint8_t ap = vPC > th;
-				Q.apPC[i] = ap;
-				Q.apBufPC[i] = (apBuf << 1) | (ap * 0x00000001u);
-				Q.threshPC[i] = ap * N->threshMaxPC + (!ap) * th;
-				if (ap) atomicAdd(&Q.scal[2], 1u);
-			}
+			float gPF = gPF0 + inputSum * N->gIncGRtoPC;
+			gPF = gPF * N->gDecGRtoPC;
+			Q.gPFPC[i] = gPF;
+			float gBC = gBC0 + inBC * N->gIncBCtoPC;
+			gBC = gBC * N->gDecBCtoPC;
+			Q.gBCPC[i] = gBC;
+			float vPC = vPC0;
+			vPC = vPC + (N->gLeakPC * (N->eLeakPC - vPC)) - (gPF * vPC) +
+				(gBC * (N->eBCtoPC - vPC)) + (gSCPCSum * (N->eSCtoPC - vPC));
+			Q.vPC[i] = vPC;
+			float th = th0 + (N->threshDecPC * (N->threshRestPC - th0));
+			const uint8_t ap = vPC > th;
+			Q.apPC[i] = ap;
+			Q.apBufPC[i] = (apBuf << 1) | (ap * 0x00000001u);
+			Q.threshPC[i] = ap * N->threshMaxPC + (!ap) * th;
+			if (ap) atomicAdd(&Q.scal[2], 1u);
 		}
-
-		if (hasBC) {
-			const DevZone &Q = N->zones[bz];
-			float gPF = bgPF0 + (bInPF * N->gIncGRtoBC);
-			gPF = gPF * N->gDecGRtoBC;
-			Q.gPFBC[bi] = gPF;
-			float gPC = bgPC0 + (bInPC * N->gIncPCtoBC);
-			gPC = gPC * N->gDecPCtoBC;
-			Q.gPCBC[bi] = gPC;
-			float v = bv0;
-			v = v + (N->gLeakBC * (N->eLeakBC - v)) - (gPF * v) + (gPC * (N->ePCtoBC - v));
-			Q.vBC[bi] = v;
-			float th = bth0 + N->threshDecBC * (N->threshRestBC - bth0);
-			const uint8_t ap = v > th;
-			Q.apBC[bi] = ap;
-			Q.apBufBC[bi] = (bApBuf << 1) | (ap * 0x00000001u);
-			Q.threshBC[bi] = ap * N->threshMaxBC + (!ap) * (th);
-		}
-		if (hasSC) {
-			float g = sg0 + (sInPF * N->gIncGRtoSC);
-			g = g * N->gDecGRtoSC;
-			N->gPFSC[c] = g;
-			float v = sv0;
-			v = v + (N->gLeakSC * (N->eLeakSC - v)) - g * v;
-			N->vSC[c] = v;
-			const uint8_t ap = v > sthOld;
-			N->apSC[c] = ap;
-			sApSC[c] = ap;
-			N->apBufSC[c] = (sApBuf << 1) | (ap * 0x00000001u);
-			float th = sthOld + N->threshDecSC * (N->threshRestSC - sthOld);
-			N->threshSC[c] = ap * N->threshMaxSC + (!ap) * (th);
-		}
-		if (hasMF) {
-			const uint32_t m = spikeBit(sMF, c);
-			N->histMF[c] = mHist || (m > 0);
-			N->apBufMF[c] = (mApBuf << 1) | (m * 0x00000001u);
-		}
+	}
+	// calcBCActivities (mzone.cpp:228-256)
+	for (uint32_t c = tid; c < Z * numBC; c += nThr) {
+		const uint32_t bz = c / numBC, bi = c % numBC;
+		const DevZone &Q = N->zones[bz];
+		const uint32_t bInPF = in.bcSum[bi], bInPC = Q.inputPCBC[bi], bApBuf = Q.apBufBC[bi];
+		const float bth0 = Q.threshBC[bi];
+		float gPF = Q.gPFBC[bi] + (bInPF * N->gIncGRtoBC);
+		gPF = gPF * N->gDecGRtoBC;
+		Q.gPFBC[bi] = gPF;
+		float gPC = Q.gPCBC[bi] + (bInPC * N->gIncPCtoBC);
+		gPC = gPC * N->gDecPCtoBC;
+		Q.gPCBC[bi] = gPC;
+		float v = Q.vBC[bi];
+		v = v + (N->gLeakBC * (N->eLeakBC - v)) - (gPF * v) + (gPC * (N->ePCtoBC - v));
+		Q.vBC[bi] = v;
+		float th = bth0 + N->threshDecBC * (N->threshRestBC - bth0);
+		const uint8_t ap = v > th;
+		Q.apBC[bi] = ap;
+		Q.apBufBC[bi] = (bApBuf << 1) | (ap * 0x00000001u);
+		Q.threshBC[bi] = ap * N->threshMaxBC + (!ap) * (th);
+	}
+	// calcSCActivities (innet.cpp:892-911)
+	for (uint32_t c = tid; c < numSC; c += nThr) {
+		const uint32_t sApBuf = N->apBufSC[c];
+		const float sthOld = N->threshSC[c];
+		float g = N->gPFSC[c] + (in.scSum[c] * N->gIncGRtoSC);
+		g = g * N->gDecGRtoSC;
+		N->gPFSC[c] = g;
+		float v = N->vSC[c];
+		v = v + (N->gLeakSC * (N->eLeakSC - v)) - g * v;
+		N->vSC[c] = v;
+		const uint8_t ap = v > sthOld;
+		N->apSC[c] = ap;
+		sApSC[c] = ap;
+		N->apBufSC[c] = (sApBuf << 1) | (ap * 0x00000001u);
+		float th = sthOld + N->threshDecSC * (N->threshRestSC - sthOld);
+		N->threshSC[c] = ap * N->threshMaxSC + (!ap) * (th);
+	}
+	// updateMFInput's bookkeeping (innet.cpp:800-815)
+	for (uint32_t c = tid; c < numMF; c += nThr) {
+		const uint32_t m = spikeBit(sMF, c);
+		N->histMF[c] = N->histMF[c] || (m > 0);
+		N->apBufMF[c] = (N->apBufMF[c] << 1) | (m * 0x00000001u);
 	}
 	barSync(1, gThr);
 	for (uint32_t i = tid; i < numBC; i += nThr) N->bcCount[(size_t)R * numBC + i] = 0;
@@ -1147,6 +1129,9 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	if (!groupA) {
 	// (tid, nThr, warp, nWarps) of the NC/IO warp group
 	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
+	// this step's error drive of the IO a thread updates at the end, loaded
+	// now so that the load overlaps the synapse and NC updates
+	const float errOwn = tid < Z * numIO ? errDriveOf(N, t, tid / numIO) : 0.0f;
 	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
 	// calcNCActivities (mzone.cpp:341-407) one warp per NC
 	// NC->IO conductances (one thread per synapse) and MF->NC synaptic
@@ -1172,8 +1157,8 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 			if (hasIO) {
 				const DevZone &Q = N->zones[iz];
 				float g = ig0;
-				g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO) + N->gDecT0ofNCtoIO));
-				g = g + iIn * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO);
+				g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO, exp2) + N->gDecT0ofNCtoIO), exp2);
+				g = g + iIn * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO, exp2);
 				Q.gNCIO[ik] = g;
 				Q.inputNCIO[ik] = 0;
 				ioScratch[c] = g;
@@ -1246,7 +1231,8 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
 		const uint32_t z = task / numIO, i = task % numIO;
 		const DevZone &Q = N->zones[z];
-		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], errDrive = errDriveOf(N, t, z), th0 = Q.threshIO[i];
+		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], th0 = Q.threshIO[i];
+		const float errDrive = task == tid ? errOwn : errDriveOf(N, t, z);
 		const uint32_t apBuf = Q.apBufIO[i];
 		float gNCSum = 0;
 		for (uint32_t j = 0; j < nIONC; j++) gNCSum = gNCSum + ioScratch[(size_t)task * nIONC + j];
@@ -1334,8 +1320,8 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 				const DevZone &Q = N->zones[z];
 				const uint8_t apNC = Q.apNC[i];
 				float p = Q.synIOPReleaseNC[i];
-				p = p * cbmExpf(-N->msPerTimeStep / (N->relPDecTSofNCtoIO * cbmExpf(-p / N->relPDecTTofNCtoIO) + N->relPDecT0ofNCtoIO));
-				p = p + apNC * N->relPIncNCtoIO * cbmExpf(-p / N->relPIncTauNCtoIO);
+				p = p * cbmExpf(-N->msPerTimeStep / (N->relPDecTSofNCtoIO * cbmExpf(-p / N->relPDecTTofNCtoIO, exp2) + N->relPDecT0ofNCtoIO), exp2);
+				p = p + apNC * N->relPIncNCtoIO * cbmExpf(-p / N->relPIncTauNCtoIO, exp2);
 				Q.synIOPReleaseNC[i] = p;
 				continue;
 			}
@@ -1417,38 +1403,89 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
 	if (tid < Z) ctl->errDrive[tid] = 0;
 }
 
-// Copy the descriptor and every staged array into shared memory and point
-// the copy's array pointers there.
-__device__ void stageIn(const DevNet *N, DevNet *sNet, uint8_t *arena, const StageSeg *segs, uint32_t nSegs)
+// Asynchronous global -> shared copies (no registers held while in flight).
+__device__ __forceinline__ void cpAsync16(void *dst, const void *src)
 {
-	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u, warp = tid >> 5, nWarps = nThr >> 5;
-	for (uint32_t i = tid; i < sizeof(DevNet) / 4; i += nThr)
-		reinterpret_cast<uint32_t *>(sNet)[i] = reinterpret_cast<const uint32_t *>(N)[i];
-	for (uint32_t k = warp; k < nSegs; k += nWarps) {
-		const StageSeg sg = segs[k];
-		const uint4 *src = *reinterpret_cast<const uint4 *const *>(reinterpret_cast<const char *>(N) + sg.fieldOff);
-		uint4 *dst = reinterpret_cast<uint4 *>(arena + sg.smemOff);
-#pragma unroll 4
-		for (uint32_t i = lane; i < sg.bytes / 16u; i += 32u) dst[i] = src[i];
-	}
-	__syncthreads();
-	for (uint32_t k = tid; k < nSegs; k += nThr)
-		*reinterpret_cast<uint8_t **>(reinterpret_cast<char *>(sNet) + segs[k].fieldOff) = arena + segs[k].smemOff;
-	__syncthreads();
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tma::smemAddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsync4(void *dst, const void *src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(tma::smemAddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncWaitAll()
+{
+	asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-// Write the staged arrays that the step changes back to global memory.
-__device__ void stageOut(const DevNet *N, const uint8_t *arena, const StageSeg *segs, uint32_t nSegs)
+// Copy a network's staging block (descriptor, step counter, staged arrays,
+// segment table: one allocation laid out as its shared-memory copy) in one
+// pass, every thread's copies in flight together; then point the copy's
+// array pointers at shared memory.
+__device__ void stageIn(const DevNet *N, uint8_t *base, uint32_t bytes)
 {
-	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
-	for (uint32_t k = warp; k < nSegs; k += nWarps) {
-		const StageSeg sg = segs[k];
-		if (!sg.writeBack) continue;
-		uint4 *dst = *reinterpret_cast<uint4 *const *>(reinterpret_cast<const char *>(N) + sg.fieldOff);
-		const uint4 *src = reinterpret_cast<const uint4 *>(arena + sg.smemOff);
-#pragma unroll 4
-		for (uint32_t i = lane; i < sg.bytes / 16u; i += 32u) dst[i] = src[i];
+	const uint32_t tid = threadIdx.x, nThr = blockDim.x;
+	const uint8_t *src = reinterpret_cast<const uint8_t *>(N);
+	for (uint32_t o = 16u * tid; o < bytes; o += 16u * nThr) cpAsync16(base + o, src + o);
+	cpAsyncWaitAll();
+	__syncthreads();
+	DevNet *sNet = reinterpret_cast<DevNet *>(base);
+	const StageSeg *segs = reinterpret_cast<const StageSeg *>(base + kStageArenaOff + sNet->zoneArenaBytes);
+	for (uint32_t k = tid; k < sNet->numZoneSegs; k += nThr)
+		*reinterpret_cast<uint8_t **>(reinterpret_cast<char *>(sNet) + segs[k].fieldOff) =
+			base + kStageArenaOff + segs[k].smemOff;
+}
+
+// Copy the inputs of microzone step t that other kernels wrote
+// (ZoneInputLayout) after the staging block and point `in` at them; the
+// caller synchronises the CTA before use.  N is the staged descriptor, whose
+// pointers to these inputs are global.
+__device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &in)
+{
+	const uint32_t tid = threadIdx.x, nThr = blockDim.x;
+	const uint32_t Z = N->numZones, numPC = N->numPC, bs = N->bs, R = (uint32_t)((t + 1) % 3);
+	const ZoneInputLayout L = zoneInputLayout(N->mfWords, N->numBC, N->numSC, Z, numPC, N->bs);
+	const uint32_t nPC = numPC * bs;
+	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	// small pieces as 4-byte words: table, MF bits, BC counts, SC counts
+	const uint32_t e0 = 64, e1 = e0 + N->mfWords, e2 = e1 + N->numBC, e3 = e2 + N->numSC;
+	for (uint32_t w = tid; w < e3; w += nThr) {
+		const void *src;
+		uint8_t *dst;
+		if (w < e0) { src = reinterpret_cast<const uint32_t *>(kExp2Tab) + w; dst = dyn + L.exp2 + 4 * w; }
+		else if (w < e1) { src = mfW + (w - e0); dst = dyn + L.mf + 4 * (w - e0); }
+		else if (w < e2) { src = N->bcCount + (size_t)R * N->numBC + (w - e1); dst = dyn + L.bc + 4 * (w - e1); }
+		else { src = N->scCount + (size_t)R * N->numSC + (w - e2); dst = dyn + L.sc + 4 * (w - e2); }
+		cpAsync4(dst, src);
 	}
+	// the PF->PC partial sums of every zone: 16-byte pieces when the slot
+	// is 16-byte aligned (numPC * bs a multiple of 4), else words
+	for (uint32_t z = 0; z < Z; z++) {
+		const float *src = N->zones[z].pcPartial + (size_t)R * nPC;
+		uint8_t *dst = dyn + L.pc + 4ull * z * nPC;
+		if ((nPC & 3u) == 0)
+			for (uint32_t w = 4 * tid; w < nPC; w += 4 * nThr) cpAsync16(dst + 4 * w, src + w);
+		else
+			for (uint32_t w = tid; w < nPC; w += nThr) cpAsync4(dst + 4 * w, src + w);
+	}
+	cpAsyncWaitAll();
+	if (tid == 0) {
+		in.mf = reinterpret_cast<const uint32_t *>(dyn + L.mf);
+		in.bcSum = reinterpret_cast<const uint32_t *>(dyn + L.bc);
+		in.scSum = reinterpret_cast<const uint32_t *>(dyn + L.sc);
+		for (uint32_t z = 0; z < kMaxZones; z++)
+			in.pcPart[z] = reinterpret_cast<const float *>(dyn + L.pc) + (size_t)(z < Z ? z : 0) * nPC;
+		in.exp2 = reinterpret_cast<const uint64_t *>(dyn + L.exp2);
+	}
+}
+
+// Write the staged arrays that the step changes (the block's range from
+// zoneWbOff to the end of the arena) back to global memory.
+__device__ void stageOut(const DevNet *N, const uint8_t *base, const DevNet *sNet)
+{
+	const uint32_t from = kStageArenaOff + sNet->zoneWbOff, to = kStageArenaOff + sNet->zoneArenaBytes;
+	uint4 *dst = reinterpret_cast<uint4 *>(const_cast<DevNet *>(N));
+	const uint4 *src = reinterpret_cast<const uint4 *>(base);
+	for (uint32_t i = from / 16u + threadIdx.x; i < to / 16u; i += blockDim.x) dst[i] = src[i];
 }
 
 // ---------------------------------------------------------- trial protocol
@@ -1557,38 +1594,64 @@ __global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet
 
 // Small-cell update of step t: block 2n is network n's Golgi role, block
 // 2n+1 its microzone role.  The two roles share no state.  The microzone
-// role runs on shared-memory copies of its arrays when they fit (one bulk
-// copy in and out per step instead of a global round trip per phase).
-__global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, uint32_t stepOffset)
+// role runs on shared-memory copies of its arrays and inputs when they fit
+// (one bulk copy in and one out per step instead of a global round trip per
+// phase).
+__global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, const uint32_t *stageBytes,
+		uint32_t stepOffset)
 {
 	// the GR pass of the same step may launch once these CTAs are resident
 	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-	const DevNet *__restrict__ N = nets[blockIdx.x >> 1];
-	const uint64_t t = *N->tBase + 1 + stepOffset;
+	const uint32_t net = blockIdx.x >> 1;
+	const DevNet *__restrict__ N = nets[net];
 	extern __shared__ __align__(16) uint32_t tailSmem[];
+	__shared__ ZoneIn in;
 	if (blockIdx.x & 1) {
-		const uint32_t nSegs = N->numZoneSegs;
-		if (nSegs) {
+		const uint32_t bytes = stageBytes[net];
+		if (bytes) {
 			uint8_t *base = reinterpret_cast<uint8_t *>(tailSmem);
-			DevNet *sNet = reinterpret_cast<DevNet *>(base);
-			uint8_t *arena = base + ((sizeof(DevNet) + 15) & ~(size_t)15);
-			const StageSeg *segs = N->zoneSegs;
-			stageIn(N, sNet, arena, segs, nSegs);
-			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(arena + N->zoneArenaBytes));
+			stageIn(N, base, bytes);
+			const DevNet *sNet = reinterpret_cast<const DevNet *>(base);
+			const uint64_t t = *reinterpret_cast<const uint64_t *>(base + kStageNetBytes) + 1 + stepOffset;
+			uint8_t *dyn = base + bytes;
+			stageInputs(sNet, t, dyn, in);
 			__syncthreads();
-			if (N->proto) {
+			const ZoneInputLayout L = zoneInputLayout(sNet->mfWords, sNet->numBC, sNet->numSC, sNet->numZones,
+					sNet->numPC, sNet->bs);
+			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(dyn + L.bytes), in);
+			__syncthreads();
+			if (sNet->proto) {
 				protocolRecord(sNet, t);
 				__syncthreads();
 			}
-			stageOut(N, arena, segs, nSegs);
+			stageOut(N, base, sNet);
 		} else {
-			zoneRole(N, t, tailSmem);
+			// global-memory mode: the table and the MF bits in shared
+			// memory, then the role's scratch
+			const uint64_t t = *N->tBase + 1 + stepOffset;
+			uint64_t *sExp2 = reinterpret_cast<uint64_t *>(tailSmem);
+			uint32_t *sMF = tailSmem + 64;
+			const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+			for (uint32_t i = threadIdx.x; i < N->mfWords; i += blockDim.x) sMF[i] = mfW[i];
+			if (threadIdx.x < 32) sExp2[threadIdx.x] = kExp2Tab[threadIdx.x];
+			const uint32_t R = (uint32_t)((t + 1) % 3);
+			if (threadIdx.x == 0) {
+				in.mf = sMF;
+				in.bcSum = N->bcCount + (size_t)R * N->numBC;
+				in.scSum = N->scCount + (size_t)R * N->numSC;
+				for (uint32_t z = 0; z < kMaxZones; z++)
+					in.pcPart[z] = N->zones[z < N->numZones ? z : 0].pcPartial + (size_t)R * N->numPC * N->bs;
+				in.exp2 = sExp2;
+			}
+			__syncthreads();
+			zoneRole(N, t, sMF + ((N->mfWords + 3) & ~3u), in);
 			if (N->proto) {
 				__syncthreads();
 				protocolRecord(N, t);
 			}
 		}
 	} else {
+		const uint64_t t = *N->tBase + 1 + stepOffset;
 		golgiRole(N, t, tailSmem);
 		if (N->proto) {
 			__syncthreads();

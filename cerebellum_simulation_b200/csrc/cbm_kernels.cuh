@@ -22,7 +22,9 @@ void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M);
 // unit), S stages, B resident CTAs per SM, slot bound M; grid of any size,
 // 32 * (W + 1) threads, the grPassKernel arguments with one network.
 const void *passPersistentKernelFor(int W, int S, int B, int M);
-__global__ void tailKernel(const DevNet *const *nets, uint32_t stepOffset);
+// Small-cell update; stageBytes[n] is network n's staging block size (0:
+// its microzone CTA works on global memory).
+__global__ void tailKernel(const DevNet *const *nets, const uint32_t *stageBytes, uint32_t stepOffset);
 __global__ void protocolPrimeKernel(const DevNet *N);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);

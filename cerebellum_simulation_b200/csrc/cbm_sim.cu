@@ -153,11 +153,13 @@ std::string Network::buildPassMaps(uint32_t R)
 // Arrays the microzone CTA stages in shared memory for each step: its
 // state (written back) and its connectivity (read only).  Arrays that the GR
 // pass reads during the same step (weights, plasticity selectors, partial
-// sums, counters) stay in global memory.
+// sums, counters) stay where they are.  When everything fits, the staged
+// arrays move into one staging block behind the network descriptor and the
+// step counter (stageBlockBytes), read-only arrays first, so that the CTA
+// copies the block in one pass and writes back one contiguous range.
 std::string Network::buildZoneStaging()
 {
-	std::vector<StageSeg> segs;
-	uint32_t arena = 0;
+	std::vector<StageSeg> ro, wb;
 	auto add = [&](size_t fieldOff, bool writeBack) -> std::string {
 		void *ptr = *(void **)((char *)&h_ + fieldOff);
 		auto it = allocBytes_.find(ptr);
@@ -165,10 +167,9 @@ std::string Network::buildZoneStaging()
 		StageSeg sg;
 		sg.fieldOff = (uint32_t)fieldOff;
 		sg.bytes = (uint32_t)it->second;
-		sg.smemOff = arena;
+		sg.smemOff = 0;
 		sg.writeBack = writeBack ? 1u : 0u;
-		arena += sg.bytes;
-		segs.push_back(sg);
+		(writeBack ? wb : ro).push_back(sg);
 		return "";
 	};
 #define CBM_NET(f, wb) CKS(add(offsetof(DevNet, f), wb))
@@ -194,34 +195,80 @@ std::string Network::buildZoneStaging()
 		CBM_ZONE(threshNC, true); CBM_ZONE(vNC, true); CBM_ZONE(synIOPReleaseNC, true);
 #undef CBM_ZONE
 	}
+	std::vector<StageSeg> segs(ro);
+	segs.insert(segs.end(), wb.begin(), wb.end());
+	uint32_t arena = 0, wbOff = 0;
+	for (size_t k = 0; k < segs.size(); k++) {
+		if (k == ro.size()) wbOff = arena;
+		segs[k].smemOff = arena;
+		arena += segs[k].bytes;
+	}
+	if (wb.empty()) wbOff = arena;
 	h_.numZoneSegs = 0;
 	h_.zoneArenaBytes = 0;
+	h_.zoneWbOff = 0;
+	h_.zoneStageBytes = 0;
 	h_.zoneSegs = nullptr;
-	const size_t total = ((sizeof(DevNet) + 15) & ~(size_t)15) + arena + zoneScratchBytes();
-	if (total > kTailSmemBudget) return "";  // too large: the microzone CTA works on global memory
-	StageSeg *d = upload(segs.data(), segs.size());
-	if (!d) return "device allocation failed";
-	h_.zoneSegs = d;
+	const uint32_t block = stageBlockBytes(arena, (uint32_t)segs.size());
+	const ZoneInputLayout L = zoneInputLayout(h_.mfWords, h_.numBC, h_.numSC, h_.numZones, h_.numPC, h_.bs);
+	if ((size_t)block + L.bytes + zoneScratchBytes() > kTailSmemBudget) return "";  // the CTA works on global memory
+	if (const char *env = getenv("CBM_ZONE_STAGE"))  // "0": global-memory mode regardless of size (testing)
+		if (!strcmp(env, "0")) return "";
+
+	uint8_t *blk = nullptr;
+	CK(cudaMalloc((void **)&blk, block), "allocating the staging block");
+	zoneBlock_ = blk;
+	dNet_.ptr = blk;  // the descriptor heads the block (freed with it)
+	CK(cudaMemset(blk, 0, block), "clearing the staging block");
+	for (const StageSeg &sg : segs) {
+		void **field = (void **)((char *)&h_ + sg.fieldOff);
+		uint8_t *dst = blk + kStageArenaOff + sg.smemOff;
+		CK(cudaMemcpy(dst, *field, sg.bytes, cudaMemcpyDeviceToDevice), "filling the staging block");
+		release(*field);
+		*field = dst;
+	}
+	// the step counter lives in the block, so that the copy brings it along
+	uint64_t *tb = (uint64_t *)(blk + kStageNetBytes);
+	CK(cudaMemcpy(tb, h_.tBase, sizeof(uint64_t), cudaMemcpyDeviceToDevice), "moving the step counter");
+	release(h_.tBase);
+	h_.tBase = tb;
+	StageSeg *dSegs = (StageSeg *)(blk + kStageArenaOff + arena);
+	CK(cudaMemcpy(dSegs, segs.data(), segs.size() * sizeof(StageSeg), cudaMemcpyHostToDevice), "staging table");
+	h_.zoneSegs = dSegs;
 	h_.numZoneSegs = (uint32_t)segs.size();
 	h_.zoneArenaBytes = arena;
+	h_.zoneWbOff = wbOff;
+	h_.zoneStageBytes = block;
 	return "";
+}
+
+void Network::release(void *p)
+{
+	auto it = std::find(allocs_.begin(), allocs_.end(), p);
+	if (it != allocs_.end()) allocs_.erase(it);
+	allocBytes_.erase(p);
+	cudaFree(p);
 }
 
 size_t Network::zoneScratchBytes() const
 {
-	// MF bits, SC spikes, NC and IO scratch, plasticity flags
-	return 4ull * h_.mfWords + ((h_.numSC + 15) & ~15u) +
-		4ull * h_.numZones * h_.numNC * 2 * h_.numpNCfromMFtoNC + 4ull * h_.numZones * h_.numIO * h_.numpIOfromNCtoIO +
-		8ull * kMaxZones;
+	// SC spikes, NC and IO scratch, plasticity flags
+	return ((h_.numSC + 15) & ~15u) + 4ull * h_.numZones * h_.numNC * 2 * h_.numpNCfromMFtoNC +
+		4ull * h_.numZones * h_.numIO * h_.numpIOfromNCtoIO + 8ull * kMaxZones;
 }
 
 size_t Network::tailSmemBytes() const
 {
-	// Golgi role: MF bits, MF->GO counts, GO scales, potentials, thresholds, spikes
-	const size_t golgi = 4ull * h_.mfWords + 16ull * h_.numGO + h_.numGO;
-	// microzone role: its scratch, after the staged descriptor and arrays
+	// Golgi role: cbmExpf table, MF bits, MF->GO counts, GO scales,
+	// potentials, thresholds, spikes
+	const size_t golgi = 256 + 4ull * h_.mfWords + 16ull * h_.numGO + h_.numGO;
+	// microzone role: staging block and inputs, or table and MF bits; then its scratch
 	size_t zone = zoneScratchBytes();
-	if (h_.numZoneSegs) zone += ((sizeof(DevNet) + 15) & ~(size_t)15) + h_.zoneArenaBytes;
+	if (h_.numZoneSegs)
+		zone += h_.zoneStageBytes +
+			zoneInputLayout(h_.mfWords, h_.numBC, h_.numSC, h_.numZones, h_.numPC, h_.bs).bytes;
+	else
+		zone += 256 + 16ull * ((h_.mfWords + 3) / 4);
 	return std::max(golgi, zone);
 }
 
@@ -546,7 +593,9 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	if (cudaMallocHost((void **)&hPinnedBits_, (size_t)h.mfWords * 4) != cudaSuccess ||
 			cudaMallocHost((void **)&hPinnedRaw_, (size_t)c.numMF) != cudaSuccess)
 		return "pinned allocation failed";
-	CK(cudaMalloc(&dNet_.ptr, sizeof(DevNet)), "allocating the network descriptor");
+	// a staged network's descriptor heads its staging block
+	if (zoneBlock_) dNet_.ptr = zoneBlock_;
+	else CK(cudaMalloc(&dNet_.ptr, sizeof(DevNet)), "allocating the network descriptor");
 	dNet_.bytes = sizeof(DevNet);
 	CK(cudaMemcpy(dNet_.ptr, &h, sizeof(DevNet), cudaMemcpyHostToDevice), "uploading the network descriptor");
 	CK(cudaDeviceSynchronize(), "network build");
@@ -867,7 +916,7 @@ Simulator::~Simulator()
 	if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
 	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
-	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_}) if (b->ptr) cudaFree(b->ptr);
+	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_}) if (b->ptr) cudaFree(b->ptr);
 	if (s0_) cudaStreamDestroy(s0_);
 	if (s1_) cudaStreamDestroy(s1_);
 	for (cudaEvent_t e : {fork_, join_, ev0_, ev1_, tev0_, tev1_}) if (e) cudaEventDestroy(e);
@@ -895,7 +944,7 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 	CK(cudaEventCreate(&tev1_), "event");
 	std::vector<DevNet *> ptrs;
 	std::vector<uint64_t *> tb;
-	std::vector<uint32_t> offs;
+	std::vector<uint32_t> offs, stage;
 	for (size_t i = 0; i < states.size(); i++) {
 		Network *n = new Network();
 		nets_.push_back(n);
@@ -905,6 +954,7 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 		passBlocks_ += n->passBlocks();
 		ptrs.push_back(n->devPtr());
 		tb.push_back(n->dev().tBase);
+		stage.push_back(n->stageBytes());
 		passSmem_ = std::max(passSmem_, n->passSmemBytes());
 		tailSmem_ = std::max(tailSmem_, n->tailSmemBytes());
 	}
@@ -917,6 +967,7 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 	CKS(up(dNetPtrs_, ptrs.data(), ptrs.size() * sizeof(DevNet *)));
 	CKS(up(dBlockOffset_, offs.data(), offs.size() * sizeof(uint32_t)));
 	CKS(up(dTBasePtrs_, tb.data(), tb.size() * sizeof(uint64_t *)));
+	CKS(up(dStageBytes_, stage.data(), stage.size() * sizeof(uint32_t)));
 	if (passSmem_ > 48 * 1024)
 		CK(cudaFuncSetAttribute(grPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem_), "pass smem");
 	if (tailSmem_ > 48 * 1024)
@@ -1061,6 +1112,7 @@ std::string Simulator::uploadCtl()
 std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 {
 	const DevNet *const *netsArg = (const DevNet *const *)dNetPtrs_.ptr;
+	const uint32_t *stageArg = (const uint32_t *)dStageBytes_.ptr;
 	const uint32_t *offsArg = (const uint32_t *)dBlockOffset_.ptr;
 	int numNetsArg = (int)nets_.size();
 	uint32_t stepArg = k;
@@ -1101,7 +1153,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 		CKS(launchPass(s0_, false));
 		CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k], s1_, cudaEventRecordExternal), "tail timing");
-		tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>(netsArg, k);
+		tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>(netsArg, stageArg, k);
 		CK(cudaGetLastError(), "launching the small-cell update");
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
 		CK(cudaEventRecord(join_, s1_), "join");
@@ -1112,7 +1164,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	// as soon as they are resident (programmatic dependent launch; the two
 	// kernels of a step share no buffer), so the pass cannot take the SMs the
 	// small-cell CTAs need.  The next step waits for both.
-	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s0_>>>(netsArg, k);
+	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s0_>>>(netsArg, stageArg, k);
 	CK(cudaGetLastError(), "launching the small-cell update");
 	CK(cudaEventRecord(join_, s0_), "join");
 	CKS(launchPass(s0_, true));

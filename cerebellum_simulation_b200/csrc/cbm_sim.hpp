@@ -99,7 +99,7 @@ private:
 	int device_ = 0;
 	cudaStream_t s0_ = nullptr, s1_ = nullptr;
 	cudaEvent_t fork_ = nullptr, join_ = nullptr, ev0_ = nullptr, ev1_ = nullptr, tev0_ = nullptr, tev1_ = nullptr;
-	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_;
+	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_, dStageBytes_;
 	uint32_t passBlocks_ = 0;
 	size_t passSmem_ = 0, tailSmem_ = 0;
 	// TMA GR pass geometry (passTmaFn_ null: the plain pass kernel runs)
@@ -150,6 +150,8 @@ public:
 	uint32_t passBlocks() const { return h_.numPC * h_.tilesPerPC; }
 	size_t passSmemBytes() const;
 	size_t tailSmemBytes() const;
+	// bytes of the staging block the microzone CTA copies, 0 when not staged
+	uint32_t stageBytes() const { return h_.numZoneSegs ? h_.zoneStageBytes : 0; }
 	// TMA GR pass: possible when every row of the reduction tile is 32 cells
 	bool passTmaCapable() const { return h_.J == 32; }
 	uint32_t passRows() const { return 2 * h_.K; }
@@ -178,6 +180,8 @@ private:
 	DevNet h_{};
 	DeviceBuf dNet_;
 	std::string buildZoneStaging();
+	void release(void *p);   // free one of allocs_
+	void *zoneBlock_ = nullptr;  // staging block (owned through dNet_), or null
 	DevProtocol hProto_{};  // host copy of the protocol descriptor
 	std::vector<void *> allocs_;
 	std::map<const void *, size_t> allocBytes_;

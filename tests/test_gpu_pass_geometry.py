@@ -2,7 +2,9 @@
 state, bit for bit, as the plain GR pass kernel (the plain kernel is pinned
 to the oracle by test_gpu_parity.py): the per-tile pass (consumer warps x
 rows per warp x stages x resident CTAs x slot bound) and the persistent pass
-(consumer warps x stages x resident CTAs x slot bound)."""
+(consumer warps x stages x resident CTAs x slot bound).  The microzone CTA's
+global-memory mode (networks whose arrays do not fit in shared memory) gives
+the same state as its staged mode."""
 import os
 
 import numpy as np
@@ -54,3 +56,15 @@ def test_tma_pass_geometries_match_plain_pass(tmp_path):
     for g in PERSISTENT_GEOMETRIES:
         got = run_with({"CBM_PASS_PERSIST": g}, path, mf, str(tmp_path / f"persist_{g}.state"))
         assert got == want, f"persistent geometry {g} differs from the plain pass"
+
+
+def test_zone_global_memory_mode_matches_staged(tmp_path):
+    from cerebellum_simulation_b200 import networks
+    st = networks.build_random_network(9, 8, 5, 5, 10, networks.act_params("dense"), seed=6,
+                                       go_out_per_gr=4, mf_per_go=16, vel=147)
+    path = str(tmp_path / "net.state")
+    st.writeState(path)
+    mf = networks.uniform_mf_stream(1024, 120, seed=6, lo=5.0, hi=60.0)
+    want = run_with({}, path, mf, str(tmp_path / "staged.state"))
+    got = run_with({"CBM_ZONE_STAGE": "0"}, path, mf, str(tmp_path / "global.state"))
+    assert got == want, "the microzone CTA's global-memory mode differs from its staged mode"
