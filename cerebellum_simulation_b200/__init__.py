@@ -190,12 +190,18 @@ class _Exporter:
     def __init__(self, sim, zone):
         self._sim = sim
         self._zone = zone
+        self._shapes = {}  # field -> (id, bytes, dtype, count); sizes are fixed per network
 
     def _export(self, field):
-        fid = FIELD[field]
-        nbytes = lib.cbm_sim_field_bytes(self._sim._h, fid)
-        out = np.empty(nbytes // np.dtype(_field_dtype(field)).itemsize, dtype=_field_dtype(field))
-        _check(lib.cbm_sim_export(self._sim._h, fid, self._zone, _ptr(out), nbytes))
+        sh = self._shapes.get(field)
+        if sh is None:
+            fid = FIELD[field]
+            nbytes = lib.cbm_sim_field_bytes(self._sim._h, fid)
+            dt = np.dtype(_field_dtype(field))
+            sh = self._shapes[field] = (fid, nbytes, dt, nbytes // dt.itemsize)
+        fid, nbytes, dt, count = sh
+        out = np.empty(count, dtype=dt)
+        _check(lib.cbm_sim_export(self._sim._h, fid, self._zone, out.ctypes.data, nbytes))
         return out
 
 

@@ -250,8 +250,7 @@ int cbm_sim_export(cbm_sim *sim, int field, unsigned zone, void *dst, uint64_t b
 {
 	NEED(sim); NEED(dst);
 	if (field < 0 || field >= CBM_FIELD_COUNT) return fail(CBM_ERR_ARG, "unknown field");
-	TRY(sim->sim.sync());
-	TRY(NET(sim).exportField((Field)field, zone, dst, bytes, sim->sim.stream()));
+	TRY(sim->sim.exportField(0, (Field)field, zone, dst, bytes));
 	return CBM_OK;
 }
 

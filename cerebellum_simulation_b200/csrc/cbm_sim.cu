@@ -48,6 +48,7 @@ Network::~Network()
 	if (dNet_.ptr) cudaFree(dNet_.ptr);
 	if (hPinnedBits_) cudaFreeHost(hPinnedBits_);
 	if (hPinnedRaw_) cudaFreeHost(hPinnedRaw_);
+	for (cudaEvent_t e : mfStageEv_) if (e) cudaEventDestroy(e);
 }
 
 // callSumKernel's block size for a row of rowLength elements
@@ -590,9 +591,10 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	h.errFlag = alloc<uint32_t>(1);
 	for (void *p : allocs_) if (!p) return "device allocation failed";
 	CKS(buildZoneStaging());
-	if (cudaMallocHost((void **)&hPinnedBits_, (size_t)h.mfWords * 4) != cudaSuccess ||
-			cudaMallocHost((void **)&hPinnedRaw_, (size_t)c.numMF) != cudaSuccess)
+	if (cudaMallocHost((void **)&hPinnedBits_, (size_t)kMFStage * h.mfWords * 4) != cudaSuccess ||
+			cudaMallocHost((void **)&hPinnedRaw_, (size_t)kMFStage * c.numMF) != cudaSuccess)
 		return "pinned allocation failed";
+	for (cudaEvent_t &e : mfStageEv_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
 	// a staged network's descriptor heads its staging block
 	if (zoneBlock_) dNet_.ptr = zoneBlock_;
 	else CK(cudaMalloc(&dNet_.ptr, sizeof(DevNet)), "allocating the network descriptor");
@@ -772,7 +774,6 @@ std::string Network::exportField(Field f, uint32_t zone, void *dst, size_t bytes
 		extractSpikesKernel<<<(h.numGR + 255) / 256, 256, 0, s>>>(h.apBufGR, tmp, h.numGR);
 		CK(cudaMemcpyAsync(dst, tmp, h.numGR, cudaMemcpyDeviceToHost, s), "export");
 		CK(cudaFreeAsync(tmp, s), "export scratch");
-		CK(cudaStreamSynchronize(s), "export");
 		return "";
 	}
 	case F_VM_GR: src = h.vGR; break;
@@ -810,7 +811,6 @@ std::string Network::exportField(Field f, uint32_t zone, void *dst, size_t bytes
 	default: return "unknown field";
 	}
 	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "export");
-	CK(cudaStreamSynchronize(s), "export");
 	return "";
 }
 
@@ -911,9 +911,10 @@ std::string Network::resetGOGODepression(cudaStream_t s)
 // --------------------------------------------------------------- Simulator
 Simulator::~Simulator()
 {
-	if (graphExec_) cudaGraphExecDestroy(graphExec_);
-	if (flushGraph_) cudaGraphExecDestroy(flushGraph_);
+	dropGraphs();
 	if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
+	if (hErr_) cudaFreeHost(hErr_);
+	if (hExport_) cudaFreeHost(hExport_);
 	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
 	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_}) if (b->ptr) cudaFree(b->ptr);
@@ -1043,8 +1044,7 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 		passPersistent_ = false;
 		passTmaW_ = passTmaR_ = passTmaS_ = 0;
 		passGeom_ = g;
-		if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
-		if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+		dropGraphs();
 		return "";
 	}
 	if (!capable) return "the TMA GR pass needs tiles of 32-cell rows in every network";
@@ -1091,8 +1091,7 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 	passGrid_ = grid;
 	passGeom_ = g;
 	// captured graphs hold the old kernel
-	if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
-	if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+	dropGraphs();
 	return "";
 }
 
@@ -1176,11 +1175,28 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
 	CKS(uploadCtl());
-	for (uint32_t k = 0; k < nsteps; k++) CKS(enqueueStep(k, false));
-	advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), nsteps);
-	CK(cudaGetLastError(), "advancing the step counter");
+	if (!stepGraph_) {
+		// one step and its counter update as one graph launch
+		cudaGraph_t g;
+		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
+		std::string e = enqueueStep(0, false);
+		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
+		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
+		if (!e.empty()) return e;
+		CK(ce, "graph capture");
+		CK(cudaGraphInstantiate(&stepGraph_, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
+		cudaGraphDestroy(g);
+	}
+	for (uint32_t k = 0; k < nsteps; k++) CK(cudaGraphLaunch(stepGraph_, s0_), "graph launch");
 	for (Network *n : nets_) n->hostT_ += nsteps;
 	return "";
+}
+
+void Simulator::dropGraphs()
+{
+	if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
+	if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+	if (stepGraph_) { cudaGraphExecDestroy(stepGraph_); stepGraph_ = nullptr; }
 }
 
 std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
@@ -1196,25 +1212,54 @@ std::string Simulator::stageMF(size_t i, const uint8_t *mf)
 	Network &n = *nets_[i];
 	if (n.hasProtocol()) return "a device protocol drives the MF input of this network";
 	const uint32_t W = n.h_.mfWords, M = n.h_.numMF;
-	memset(n.hPinnedBits_, 0, 4ull * W);
+	const uint32_t k = n.mfStageNext_++ % Network::kMFStage;
+	if (n.mfStageUsed_[k]) CK(cudaEventSynchronize(n.mfStageEv_[k]), "MF staging");
+	uint32_t *bits = n.hPinnedBits_ + (size_t)k * W;
+	memset(bits, 0, 4ull * W);
 	bool raw = false;
-	for (uint32_t k = 0; k < M; k++) {
-		if (mf[k]) n.hPinnedBits_[k >> 5] |= 1u << (k & 31);
-		if (mf[k] > 1) raw = true;
+	for (uint32_t c = 0; c < M; c++) {
+		if (mf[c]) bits[c >> 5] |= 1u << (c & 31);
+		if (mf[c] > 1) raw = true;
 	}
 	const uint64_t slot = n.hostT_ % n.h_.mfRing;
-	CK(cudaMemcpyAsync((void *)(n.h_.mfBits + slot * W), n.hPinnedBits_, 4ull * W, cudaMemcpyHostToDevice, s0_), "MF upload");
+	CK(cudaMemcpyAsync((void *)(n.h_.mfBits + slot * W), bits, 4ull * W, cudaMemcpyHostToDevice, s0_), "MF upload");
 	if (raw || n.h_.hasMFRaw) {
-		memcpy(n.hPinnedRaw_, mf, M);
-		CK(cudaMemcpyAsync((void *)(n.h_.mfRaw + slot * M), n.hPinnedRaw_, M, cudaMemcpyHostToDevice, s0_), "MF upload");
+		uint8_t *rb = n.hPinnedRaw_ + (size_t)k * M;
+		memcpy(rb, mf, M);
+		CK(cudaMemcpyAsync((void *)(n.h_.mfRaw + slot * M), rb, M, cudaMemcpyHostToDevice, s0_), "MF upload");
 		if (!n.h_.hasMFRaw) {
 			// from now on NC inputs take the raw bytes (mzone.cpp:521)
 			n.h_.hasMFRaw = 1;
 			CK(cudaMemcpyAsync((char *)n.dNet_.ptr + offsetof(DevNet, hasMFRaw), &n.h_.hasMFRaw, 4,
 					cudaMemcpyHostToDevice, s0_), "MF mode");
+			CK(cudaStreamSynchronize(s0_), "MF mode");
 		}
 	}
-	CK(cudaStreamSynchronize(s0_), "MF upload");
+	CK(cudaEventRecord(n.mfStageEv_[k], s0_), "MF staging");
+	n.mfStageUsed_[k] = true;
+	return "";
+}
+
+std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, size_t bytes)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	if (!hErr_) CK(cudaMallocHost((void **)&hErr_, 4 * nets_.size()), "pinned allocation");
+	if (bytes > hExportBytes_) {
+		if (hExport_) cudaFreeHost(hExport_);
+		hExport_ = nullptr;
+		hExportBytes_ = 0;
+		CK(cudaMallocHost((void **)&hExport_, bytes), "pinned allocation");
+		hExportBytes_ = bytes;
+	}
+	CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s0_));
+	for (size_t k = 0; k < nets_.size(); k++)
+		CK(cudaMemcpyAsync(hErr_ + k, nets_[k]->h_.errFlag, 4, cudaMemcpyDeviceToHost, s0_), "reading the device error word");
+	CK(cudaStreamSynchronize(s0_), "export");
+	for (size_t k = 0; k < nets_.size(); k++) {
+		if (hErr_[k] & kErrPassWait) return "GR pass: a pipeline wait timed out on the device";
+		if (hErr_[k]) return "device error word set";
+	}
+	memcpy(dst, hExport_, bytes);
 	return "";
 }
 

@@ -65,6 +65,9 @@ public:
 	// the summed step time.
 	std::string runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs);
 	std::string sync();
+	// A field of network i into host memory: the copy and a read of every
+	// network's device error word share one synchronisation.
+	std::string exportField(size_t i, Field f, uint32_t zone, void *dst, size_t bytes);
 	cudaStream_t stream() const { return s0_; }
 	int device() const { return device_; }
 	// Time of the last runGraph call measured with events on the launch stream.
@@ -95,6 +98,11 @@ private:
 	friend class Network;
 	std::string uploadCtl();
 	std::string enqueueStep(uint32_t stepOffset, bool instrument);
+	void dropGraphs();
+	cudaGraphExec_t stepGraph_ = nullptr;  // one step and its counter update (launchSteps)
+	uint32_t *hErr_ = nullptr;             // pinned copies of the networks' error words
+	uint8_t *hExport_ = nullptr;           // pinned export staging
+	size_t hExportBytes_ = 0;
 	std::vector<Network *> nets_;
 	int device_ = 0;
 	cudaStream_t s0_ = nullptr, s1_ = nullptr;
@@ -128,7 +136,8 @@ public:
 	void setErrDrive(uint32_t zone, float rel);
 	void setGIncGRtoGO(float v);
 	void resetGIncGRtoGO();
-	// Copy one field to host memory (bytes must equal fieldBytes).
+	// Enqueue a copy of one field into host memory on stream s (bytes must
+	// equal fieldBytes); the caller synchronises before reading dst.
 	std::string exportField(Field f, uint32_t zone, void *dst, size_t bytes, cudaStream_t s);
 	size_t fieldBytes(Field f) const;
 	// CBMSimCore::writeToState(): device values back into the state.
@@ -186,8 +195,14 @@ private:
 	std::vector<void *> allocs_;
 	std::map<const void *, size_t> allocBytes_;
 	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;
+	// pinned staging of host MF input: kMFStage slots, each reused once the
+	// copy that last read it has run (mfStageEv_)
+	static constexpr uint32_t kMFStage = 8;
 	uint32_t *hPinnedBits_ = nullptr;
 	uint8_t *hPinnedRaw_ = nullptr;
+	cudaEvent_t mfStageEv_[kMFStage] = {};
+	bool mfStageUsed_[kMFStage] = {};
+	uint32_t mfStageNext_ = 0;
 };
 
 std::string cudaErr(cudaError_t e, const char *what);
