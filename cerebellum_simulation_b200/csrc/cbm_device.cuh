@@ -228,9 +228,20 @@ struct DevNet {
 // Staging block of a network whose microzone arrays fit in shared memory: one
 // allocation that the microzone CTA copies as it is, laid out as its shared
 // memory copy: the descriptor, the step counter (tBase points here), the
-// staged arrays, then the StageSeg table.
+// staged arrays, then the StageSeg table.  Networks that are not staged
+// allocate the descriptor and the step counter alone (kStageArenaOff bytes).
 constexpr uint32_t kStageNetBytes = (uint32_t)((sizeof(DevNet) + 15) & ~(size_t)15);
 constexpr uint32_t kStageArenaOff = kStageNetBytes + 16;
+#if defined(__CUDACC__)
+// Steps the network has completed: every descriptor allocation holds the
+// step counter at kStageNetBytes (DevNet::tBase points there), so kernels
+// read it together with the descriptor instead of after it.
+__device__ __forceinline__ uint64_t stepsDone(const DevNet *N)
+{
+	return *reinterpret_cast<const uint64_t *>(reinterpret_cast<const char *>(N) + kStageNetBytes);
+}
+#endif
+
 CBM_LAYOUT_FN uint32_t stageBlockBytes(uint32_t arenaBytes, uint32_t numSegs)
 {
 	return kStageArenaOff + arenaBytes + ((numSegs * (uint32_t)sizeof(StageSeg) + 15u) & ~15u);

@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kPassThreads) grPassKernel(const DevNet *const
 {
 	uint32_t local;
 	const DevNet *__restrict__ N = locateNet(nets, blockOffset, numNets, blockIdx.x, local);
-	const uint64_t t = *N->tBase + 1 + stepOffset;
+	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 
 	const uint32_t P = N->P, bs = N->bs, K = N->K, J = N->J, Z = N->numZones, numGR = N->numGR;
 	const uint32_t pc = local / N->tilesPerPC;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	constexpr uint32_t R = W * RW;
 	uint32_t local;
 	const DevNet *__restrict__ N = locateNet(nets, blockOffset, numNets, blockIdx.x, local);
-	const uint64_t t = *N->tBase + 1 + stepOffset;
+	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 
 	const uint32_t P = N->P, bs = N->bs, K = N->K, Z = N->numZones;
 	const uint32_t pc = local / N->tilesPerPC;
@@ -311,7 +311,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	// sentinel index numMF / numGO reads 0)
 	uint32_t *sBC = reinterpret_cast<uint32_t *>(empty + S);
 	uint32_t *sSC = sBC + N->bcLocal;
-	float *sX = reinterpret_cast<float *>(sSC + N->scLocal);
+	// 16-byte aligned: the spike tables after it take 16-byte stores
+	float *sX = reinterpret_cast<float *>(sSC + ((N->bcLocal + N->scLocal + 3u) & ~3u) - N->bcLocal);
 	uint8_t *sMF = reinterpret_cast<uint8_t *>(sX + (size_t)Z * rows * 32u);
 	uint8_t *sGO = sMF + 32u * N->mfWords;
 
@@ -367,8 +368,30 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 		// stage.  They stage the spike tables while the first copies fly.
 		const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
 		const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
-		for (uint32_t i = threadIdx.x; i < 32u * N->mfWords; i += 32u * W) sMF[i] = (uint8_t)spikeBit(mfSrc, i);
-		for (uint32_t i = threadIdx.x; i < 32u * N->goWords; i += 32u * W) sGO[i] = (uint8_t)spikeBit(goSrc, i);
+		// one spike word per thread and round (the loads of a round in flight
+		// together), spread to a byte per cell: (nibble * 0x204081) & 0x01010101
+		// moves bit k of a nibble to bit 8k
+		const uint32_t mfWords = N->mfWords, nWords = mfWords + N->goWords;
+		for (uint32_t w0 = 0; w0 < nWords; w0 += 2u * 32u * W) {
+			uint32_t v[2];
+#pragma unroll
+			for (int u = 0; u < 2; u++) {
+				const uint32_t w = w0 + u * 32u * W + threadIdx.x;
+				v[u] = w < nWords ? __ldg(w < mfWords ? mfSrc + w : goSrc + (w - mfWords)) : 0u;
+			}
+#pragma unroll
+			for (int u = 0; u < 2; u++) {
+				const uint32_t w = w0 + u * 32u * W + threadIdx.x;
+				if (w < nWords) {
+					uint4 *dst = reinterpret_cast<uint4 *>(w < mfWords ? sMF + 32u * w : sGO + 32u * (w - mfWords));
+					uint32_t q[8];
+#pragma unroll
+					for (int k = 0; k < 8; k++) q[k] = (((v[u] >> (4 * k)) & 0xFu) * 0x00204081u) & 0x01010101u;
+					dst[0] = make_uint4(q[0], q[1], q[2], q[3]);
+					dst[1] = make_uint4(q[4], q[5], q[6], q[7]);
+				}
+			}
+		}
 		for (uint32_t i = threadIdx.x; i < N->bcLocal + N->scLocal; i += 32u * W) sBC[i] = 0;
 		asm volatile("bar.sync 1, %0;" ::"r"(32u * W) : "memory");
 		float stepW[kMaxZones];
@@ -593,7 +616,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(con
 	(void)blockOffset; (void)numNets;
 	constexpr uint32_t R = 2 * W;
 	const DevNet *__restrict__ N = nets[0];
-	const uint64_t t = *N->tBase + 1 + stepOffset;
+	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 
 	const uint32_t P = N->P, bs = N->bs, K = N->K, Z = N->numZones, numPC = N->numPC;
 	const uint32_t rows = 2 * K, unitsPerTile = rows / R, tilesPerPC = N->tilesPerPC;
@@ -1589,7 +1612,7 @@ __device__ void protocolRecord(const DevNet *__restrict__ N, uint64_t t)
 // Prepare the first step of a newly set protocol (the network's step tBase + 1).
 __global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet *N)
 {
-	protocolPrepare(N, *N->tBase);
+	protocolPrepare(N, stepsDone(N));
 }
 
 // Small-cell update of step t: block 2n is network n's Golgi role, block
@@ -1628,7 +1651,7 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 		} else {
 			// global-memory mode: the table and the MF bits in shared
 			// memory, then the role's scratch
-			const uint64_t t = *N->tBase + 1 + stepOffset;
+			const uint64_t t = stepsDone(N) + 1 + stepOffset;
 			uint64_t *sExp2 = reinterpret_cast<uint64_t *>(tailSmem);
 			uint32_t *sMF = tailSmem + 64;
 			const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
@@ -1651,7 +1674,7 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 			}
 		}
 	} else {
-		const uint64_t t = *N->tBase + 1 + stepOffset;
+		const uint64_t t = stepsDone(N) + 1 + stepOffset;
 		golgiRole(N, t, tailSmem);
 		if (N->proto) {
 			__syncthreads();

@@ -79,7 +79,7 @@ size_t Network::passSmemBytes() const
 size_t Network::passTmaSmemBytes(uint32_t R, uint32_t S) const
 {
 	const PassLayout L = passLayout(R, h_.nMFSlots, h_.nGOSlots, h_.nOutSlots, h_.numZones);
-	return 128 + (size_t)S * L.bytes + 16ull * S + sizeof(uint32_t) * ((size_t)h_.bcLocal + h_.scLocal) +
+	return 128 + (size_t)S * L.bytes + 16ull * S + sizeof(uint32_t) * (((size_t)h_.bcLocal + h_.scLocal + 3) & ~(size_t)3) +
 		sizeof(float) * (size_t)h_.numZones * 2 * h_.K * 32 + 32ull * (h_.mfWords + h_.goWords);
 }
 
@@ -595,9 +595,18 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 			cudaMallocHost((void **)&hPinnedRaw_, (size_t)kMFStage * c.numMF) != cudaSuccess)
 		return "pinned allocation failed";
 	for (cudaEvent_t &e : mfStageEv_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-	// a staged network's descriptor heads its staging block
-	if (zoneBlock_) dNet_.ptr = zoneBlock_;
-	else CK(cudaMalloc(&dNet_.ptr, sizeof(DevNet)), "allocating the network descriptor");
+	// a staged network's descriptor heads its staging block; otherwise the
+	// descriptor and the step counter get an allocation of their own
+	if (zoneBlock_) {
+		dNet_.ptr = zoneBlock_;
+	} else {
+		CK(cudaMalloc(&dNet_.ptr, kStageArenaOff), "allocating the network descriptor");
+		CK(cudaMemset(dNet_.ptr, 0, kStageArenaOff), "clearing the network descriptor");
+		uint64_t *tb = (uint64_t *)((char *)dNet_.ptr + kStageNetBytes);
+		CK(cudaMemcpy(tb, h.tBase, sizeof(uint64_t), cudaMemcpyDeviceToDevice), "moving the step counter");
+		release(h.tBase);
+		h.tBase = tb;
+	}
 	dNet_.bytes = sizeof(DevNet);
 	CK(cudaMemcpy(dNet_.ptr, &h, sizeof(DevNet), cudaMemcpyHostToDevice), "uploading the network descriptor");
 	CK(cudaDeviceSynchronize(), "network build");
