@@ -46,8 +46,9 @@ def parse():
     ap.add_argument("--chunk", type=int, default=50)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="1m", choices=["1m", "batch", "surrogate"],
-                    help="1m: the 1M-GR eyelid network (default); batch: 64 uneven instances in one launch; "
+    ap.add_argument("--workload", default="1m", choices=["1m", "dense4m", "batch", "surrogate"],
+                    help="1m: the 1M-GR eyelid network (default); dense4m: the 4M-GR network with "
+                         "state-variable MF coding; batch: 64 uneven instances in one launch; "
                          "surrogate: the surrogate-proposed sweep")
     ap.add_argument("--train-instances", type=int, default=2000)
     ap.add_argument("--trials", type=int, default=10)
@@ -387,9 +388,98 @@ def main_surrogate(args):
     print(json.dumps(out))
 
 
+WORKLOAD_4M = ("dense 4M-GR network: 4,194,304 GR (4 MF + 3 GO inputs), 4096 GO x 1024 random GR (1 GO target "
+               "per GR on average), 1024 MF, 128 PC x 32,768 PF, 128 BC, 512 SC, 8 NC, 4 IO; MF rates a Gaussian "
+               "tuning of 4 state variables (sigma 0.2 of range) on regenerating-Poisson fibres")
+
+
+def main_dense4m(args):
+    """The dense 4M-GR network: its per-step working set (~360 MB) exceeds L2,
+    so graph chunks replay back to back with every step's inputs from HBM."""
+    import torch
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(device)
+    st = networks.config3_network(seed=args.seed)
+    steps = args.steps - args.steps % args.chunk or args.chunk
+    n_roof = min(steps, 1000)
+    n_roof -= n_roof % args.chunk
+    n_roof = n_roof or args.chunk
+    total = args.warmup + steps + n_roof
+    mf = networks.config3_mf_stream(1024, total, seed=args.seed)
+    sim = cbm.CBMSimCore(st, [7], device=device, resident_steps=total)
+    sim.load_mf_stream(cbm.mf_bits(mf, sim.mf_words()))
+    sim.run(args.warmup, args.chunk)
+    clocks = ClockSampler(device)
+    clocks.start()
+    ms, _ = sim.run(steps, args.chunk)
+    clock_info = clocks.stop()
+    _, pass_ms = sim.run(n_roof, args.chunk, time_pass=True)
+    tail_ms = sim.last_tail_ms()
+    alg_bytes = sim.algorithmic_bytes_per_step()
+    layout_bytes = sim.layout_bytes_per_step()
+    kernel, warps, rows, stages = sim.pass_geometry()
+    sim.close()
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (pass_ms / 1000.0) / 1e9
+
+    # end to end through the per-step C ABI
+    n_e2e = min(steps, 500)
+    sim3 = cbm.CBMSimCore(st, [7], device=device)
+    zone = sim3.getMZoneList()[0]
+    for s in range(10):
+        sim3.updateMFInput(mf[s])
+        sim3.calcActivity()
+        zone.exportAPNC()
+    sim3.timer_start()
+    for s in range(10, 10 + n_e2e):
+        sim3.updateMFInput(mf[s % total])
+        sim3.calcActivity()
+        zone.exportAPNC()
+    e2e_ms = sim3.timer_stop()
+    h2d, d2h = sim3.mf_words() * 4, st.con("numNC")
+    sim3.close()
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "c3.state")
+            st.writeState(p)
+            cpu = cpu_reference(p, mf, 40, os.cpu_count() or 1, warmup=5)
+            if cpu:
+                cpu["sample"] = cpu["sample"].replace("1M-GR network", "4M-GR network").replace(
+                    "(ms", "(state-variable input, ms")
+    out = {
+        "metric": "1 ms steps/s at 4M GR (dense)", "value": 1000.0 * steps / ms, "unit": "steps/s", "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (random wiring, random-init state, state-variable-coded regenerating-Poisson MF input)",
+        "config": {"workload": WORKLOAD_4M, "global_batch": 1, "parallelism": "replicas x1",
+                   "graph_chunk": args.chunk,
+                   "l2": "not flushed: the per-step working set (layout %.0f MB) is larger than L2"
+                         % (layout_bytes / 1e6)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": kernel,
+                     "pipeline": {"consumer_warps": warps, "rows_per_stage": rows, "stages": stages},
+                     "pass_ms": pass_ms, "tail_ms": tail_ms, "algorithmic_bytes": alg_bytes,
+                     "layout_bytes": layout_bytes, "layout_achieved": layout_bytes / (pass_ms / 1000.0) / 1e9,
+                     "layout_frac": layout_bytes / (pass_ms / 1000.0) / 1e9 / peak, "peak_source": peak_kind},
+        "e2e": {"value": 1000.0 * n_e2e / e2e_ms, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": 2 * steps + steps // args.chunk,
+        "clocks": clock_info,
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     assert args.warmup >= 3
+    if args.workload == "dense4m" and args.impl == "b200":
+        return main_dense4m(args)
     if args.workload == "batch" and args.impl == "b200":
         return main_batch(args)
     if args.workload == "surrogate" and args.impl == "b200":

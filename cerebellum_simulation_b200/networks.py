@@ -255,6 +255,72 @@ def config3_network(seed=0):
                                 mf_per_go=16, vel=294, pc_p2=7)
 
 
+class StateVariableMF:
+    """Cart-pole-style MF rate coding: each of n_vars state variables owns an
+    equal, ordered share of the fibres (StateVariable::assignOrderedMFInds,
+    Matthew_Sim_CBM/includes/statevariable.hpp:35-43, with the unassigned
+    list built from the last fibre down, environment.cpp:47-51), and fibre k
+    of a variable fires at a Gaussian blend of its relaxed and excited rates
+    around preferred value min + (k + 1/2) * range / n (gaussMFAct,
+    statevariable.hpp:108-129): with a = exp(-(x - mean)^2 / (2 var^2)), the
+    rate is a * excited + (1 - a) * relaxed, in float32.  Relaxed rates are
+    U(1, 10) Hz and excited rates 40 Hz (Environment::setupMossyFibers,
+    environment.cpp:19-39, whose excited range expression reduces to its
+    minimum).  var is sigma_frac of the variable's range.
+
+    The environment that moves the variables (the cart-pole dynamics) lies
+    outside the simulator; values() supplies a fixed synthetic trajectory:
+    variable v follows 0.5 + 0.45 sin(2 pi t / period_v + phase_v) of its
+    range.
+    """
+
+    PERIODS = (1000.0, 1700.0, 2300.0, 3100.0)
+
+    def __init__(self, num_mf, seed=0, n_vars=4, sigma_frac=0.2, lo=-1.0, hi=1.0):
+        rng = np.random.Generator(np.random.PCG64(seed + 303))
+        self.num_mf = num_mf
+        self.n_vars = n_vars
+        self.lo, self.hi = np.float32(lo), np.float32(hi)
+        self.relaxed = rng.uniform(1.0, 10.0, num_mf).astype(np.float32)
+        self.excited = np.full(num_mf, 40.0, dtype=np.float32)
+        self.phase = rng.uniform(0, 2 * np.pi, n_vars)
+        per = num_mf // n_vars
+        rng_f = np.float32(hi - lo)
+        interval = np.float32(rng_f / np.float32(per))
+        self.var_of = np.full(num_mf, -1, dtype=np.int64)
+        self.mean = np.zeros(num_mf, dtype=np.float32)
+        for v in range(n_vars):
+            idx = np.arange(v * per, (v + 1) * per)
+            self.var_of[idx] = v
+            self.mean[idx] = (self.lo + interval / np.float32(2) + interval * np.arange(per, dtype=np.float32)).astype(
+                np.float32)
+        self.variance = np.float32(np.float32(sigma_frac) * rng_f)
+
+    def values(self, t):
+        """The n_vars state-variable values at step t (synthetic trajectory)."""
+        ph = 2 * np.pi * t / np.array(self.PERIODS[: self.n_vars]) + self.phase
+        return (self.lo + (self.hi - self.lo) * (0.5 + 0.45 * np.sin(ph))).astype(np.float32)
+
+    def rates(self, t):
+        """[num_mf] Hz at step t; fibres beyond the variables' shares stay relaxed."""
+        x = self.values(t)
+        out = self.relaxed.copy()
+        m = self.var_of >= 0
+        xv = np.clip(x[self.var_of[m]], self.lo, self.hi).astype(np.float32)
+        d = (xv - self.mean[m]).astype(np.float32)
+        a = np.exp(-(d * d) / (np.float32(2) * (self.variance * self.variance)), dtype=np.float32)
+        out[m] = (a * self.excited[m] + (np.float32(1) - a) * self.relaxed[m]).astype(np.float32)
+        return out
+
+
+def config3_mf_stream(num_mf, steps, seed=0):
+    """MF spikes of the dense 4M configuration: regenerating Poisson fibres
+    driven by the state-variable rate coding."""
+    coding = StateVariableMF(num_mf, seed=seed)
+    gen = RegenPoissonMF(num_mf, seed)
+    return gen.run(coding.rates, steps)
+
+
 def eyelid_mf_rates(num_mf, seed=0, cs_count=80):
     """Config-2 MF rates: 10% tonic at U(50,80) Hz, the rest U(1,10) Hz; the
     first cs_count fibres of a random permutation carry the CS (100 Hz)."""

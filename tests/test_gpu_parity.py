@@ -122,6 +122,21 @@ def test_config2_1m_bit_exact_short(tmp_path):
     assert compare_states(fo, fp) == []
 
 
+def test_config3_4m_bit_exact_short(tmp_path):
+    """Config 3 size (4,194,304 GR, 4096 GO x 1024 GR, 128 PC x 32,768 PF;
+    its microzone arrays exceed shared memory, so the microzone CTA runs on
+    global memory): 80 steps of state-variable-coded MF input."""
+    from cerebellum_simulation_b200 import networks
+    net = networks.config3_network(seed=0)
+    p = str(tmp_path / "c3.state")
+    net.writeState(p)
+    mf = networks.config3_mf_stream(1024, 80, seed=0)
+    ev = {1: [("plast", 0, -0.0005, 0.0005)], 60: [("errdrive", 0, 1.0)]}
+    o, tr_o, tr_p, fo, fp = run_both(tmp_path, p, mf, [9], ev)
+    assert cbmtest.first_difference(tr_o, tr_p, o.num) is None
+    assert compare_states(fo, fp) == []
+
+
 def test_graph_run_equals_step_calls(tmp_path):
     """Resident-input CUDA-graph runs give the step-by-step API's result."""
     import cerebellum_simulation_b200 as cbm
