@@ -93,6 +93,7 @@ def _load():
         "cbm_sim_timer_start": (I, [P]),
         "cbm_sim_last_tail_ms": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_run_flushed": (I, [P, U64, U64, ctypes.POINTER(F)]),
+        "cbm_sim_run_flushed_kernels": (I, [P, U64, U64, ctypes.POINTER(F), ctypes.POINTER(F)]),
         "cbm_sim_set_eyelid_protocol": (I, [P, P]),
         "cbm_batch_create": (I, [P, U32, P, I, P]),
         "cbm_batch_destroy": (None, [P]),
@@ -373,6 +374,13 @@ class CBMSimCore:
         ms = ctypes.c_float()
         _check(lib.cbm_sim_run_flushed(self._h, nsteps, flush_bytes, ctypes.byref(ms)))
         return ms.value
+
+    def run_flushed_kernels(self, nsteps, flush_bytes):
+        """nsteps steps after an L2 flush each, the two step kernels timed
+        separately: (mean GR-pass ms, mean small-cell kernel ms)."""
+        p, t = ctypes.c_float(), ctypes.c_float()
+        _check(lib.cbm_sim_run_flushed_kernels(self._h, nsteps, flush_bytes, ctypes.byref(p), ctypes.byref(t)))
+        return p.value, t.value
 
     def layout_bytes_per_step(self):
         return lib.cbm_sim_layout_bytes_per_step(self._h)

@@ -324,6 +324,13 @@ int cbm_sim_run_flushed(cbm_sim *sim, uint64_t nsteps, uint64_t flushBytes, floa
 	return CBM_OK;
 }
 
+int cbm_sim_run_flushed_kernels(cbm_sim *sim, uint64_t nsteps, uint64_t flushBytes, float *passMs, float *tailMs)
+{
+	NEED(sim); NEED(passMs); NEED(tailMs);
+	TRY(sim->sim.runFlushedKernels(nsteps, (size_t)flushBytes, passMs, tailMs));
+	return CBM_OK;
+}
+
 int cbm_sim_set_eyelid_protocol(cbm_sim *sim, const cbm_eyelid_protocol *protocol)
 {
 	NEED(sim); NEED(protocol);

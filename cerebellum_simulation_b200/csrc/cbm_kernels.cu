@@ -287,20 +287,37 @@ __device__ __forceinline__ int countSpikes(const uint8_t *spikes, const uint16_t
 	return c;
 }
 
-template <int W, int RW, int S, int MINB, int MS>
+// Network shapes the TMA pass can be compiled for: slot counts, zones and
+// whether every 32-cell row feeds a single BC and a single SC become
+// compile-time constants (shared-memory offsets fold into immediates, slot
+// loops lose their predicates).  Shape 0 reads them at run time.
+template <int SH> struct PassShape {
+	static constexpr uint32_t mf = 0, go = 0, out = 0, z = 0;
+	static constexpr bool uniform = false;
+};
+// 4 MF and 3 GO dendrites, 4 GR->GO slots, one zone, BC and SC blocks of at
+// least 32 cells (the eyelid networks)
+template <> struct PassShape<1> {
+	static constexpr uint32_t mf = 4, go = 3, out = 4, z = 1;
+	static constexpr bool uniform = true;
+};
+
+template <int W, int RW, int S, int MINB, int MS, int SH>
 __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevNet *const *nets,
 		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
 {
+	using Sh = PassShape<SH>;
 	constexpr uint32_t R = W * RW;
 	uint32_t local;
 	const DevNet *__restrict__ N = locateNet(nets, blockOffset, numNets, blockIdx.x, local);
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 
-	const uint32_t P = N->P, bs = N->bs, K = N->K, Z = N->numZones;
+	const uint32_t P = N->P, bs = N->bs, K = N->K, Z = Sh::z ? Sh::z : N->numZones;
 	const uint32_t pc = local / N->tilesPerPC;
 	const uint32_t j0 = (local % N->tilesPerPC) * 32u;
 	const uint32_t rows = 2 * K, nStages = rows / R;
-	const uint32_t nMFSlots = N->nMFSlots, nGOSlots = N->nGOSlots, nOutSlots = N->nOutSlots;
+	const uint32_t nMFSlots = Sh::mf ? Sh::mf : N->nMFSlots, nGOSlots = Sh::go ? Sh::go : N->nGOSlots,
+		nOutSlots = Sh::out ? Sh::out : N->nOutSlots;
 	const PassLayout L = passLayout(R, nMFSlots, nGOSlots, nOutSlots, Z);
 
 	extern __shared__ uint8_t passSmemRaw[];
@@ -407,7 +424,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 		const float threshBase = N->threshRestGR, threshMax = N->threshMaxGR, threshDecay = N->threshDecGR;
 		const float gDecMF = N->gDecMFtoGR, gIncMF = N->gIncMFtoGR, gDecGO = N->gDecGOtoGR, gIncGO = N->gIncGOtoGR;
 		uint32_t *goCount = N->goCount + (size_t)(t & 1) * N->numGO;
-		const bool bcWarpUniform = (1u << N->bcShift) >= 32u, scWarpUniform = (1u << N->scShift) >= 32u;
+		const bool bcWarpUniform = Sh::uniform || (1u << N->bcShift) >= 32u;
+		const bool scWarpUniform = Sh::uniform || (1u << N->scShift) >= 32u;
 		float *const vGR = N->vGR, *const gKCaGR = N->gKCaGR, *const threshGR = N->threshGR;
 		float *const gESum = N->gESum, *const gISum = N->gISum;
 		uint32_t *const apBufGR = N->apBufGR;
@@ -538,12 +556,13 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 }
 
 // Geometries the host can pick: (consumer warps, rows per warp, stages,
-// minimum resident CTAs per SM, slot bound MS).
+// minimum resident CTAs per SM, slot bound MS); those with MS = 4 are also
+// compiled for shape 1 (instantiated where passTmaKernelFor takes them).
 #define CBM_PASS_TMA_CONFIGS(X) \
 	X(8, 1, 3, 2, 4) X(8, 1, 3, 3, 4) X(8, 1, 4, 2, 4) X(8, 1, 2, 3, 4) X(4, 1, 4, 4, 4) X(4, 2, 3, 3, 4) X(4, 2, 4, 2, 4) \
 	X(8, 1, 3, 2, 0) X(4, 1, 4, 1, 0) X(2, 1, 4, 1, 0) X(1, 1, 4, 1, 0)
 #define CBM_PASS_TMA_INST(W, RW, S, B, M) \
-	template __global__ void grPassTmaKernel<W, RW, S, B, M>(const DevNet *const *, const uint32_t *, int, uint32_t);
+	template __global__ void grPassTmaKernel<W, RW, S, B, M, 0>(const DevNet *const *, const uint32_t *, int, uint32_t);
 CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_INST)
 
 int passTmaConfigCount()
@@ -563,13 +582,26 @@ void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M)
 #undef CBM_PASS_TMA_NTH
 }
 
-const void *passTmaKernelFor(int W, int RW, int S, int B, int M)
+const void *passTmaKernelFor(int W, int RW, int S, int B, int M, int shape)
 {
 #define CBM_PASS_TMA_PICK(w, rw, s, b, m) \
-	if (W == w && RW == rw && S == s && B == b && M == m) return (const void *)&grPassTmaKernel<w, rw, s, b, m>;
+	if (W == w && RW == rw && S == s && B == b && M == m) { \
+		if (shape == 0) return (const void *)&grPassTmaKernel<w, rw, s, b, m, 0>; \
+		if (shape == 1 && m == 4) return (const void *)&grPassTmaKernel<w, rw, s, b, m, (m == 4 ? 1 : 0)>; \
+		return nullptr; \
+	}
 	CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_PICK)
 #undef CBM_PASS_TMA_PICK
 	return nullptr;
+}
+
+int passShapeOf(const DevNet &h)
+{
+	using E = PassShape<1>;
+	if (h.numZones == E::z && h.nMFSlots == E::mf && h.nGOSlots == E::go && h.nOutSlots == E::out &&
+			(1u << h.bcShift) >= 32u && (1u << h.scShift) >= 32u)
+		return 1;
+	return 0;
 }
 
 // ----------------------------------------------------- GR pass, persistent

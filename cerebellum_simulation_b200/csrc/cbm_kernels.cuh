@@ -12,9 +12,12 @@ __global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOff
 		uint32_t stepOffset);
 // TMA GR pass with W consumer warps of RW rows each per stage, S stages
 // deep, at least B resident CTAs per SM, synapse-slot loops bounded by M
-// (0: any count); launched with 32 * (W + 1) threads and the grPassKernel
+// (0: any count), compiled for network shape `shape` (0: any network; see
+// passShapeOf); launched with 32 * (W + 1) threads and the grPassKernel
 // arguments.  Returns null for a geometry that is not compiled in.
-const void *passTmaKernelFor(int W, int RW, int S, int B, int M);
+const void *passTmaKernelFor(int W, int RW, int S, int B, int M, int shape);
+// The most specific pass shape a network matches (0 when none).
+int passShapeOf(const DevNet &h);
 // The compiled per-tile geometries, in table order.
 int passTmaConfigCount();
 void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M);

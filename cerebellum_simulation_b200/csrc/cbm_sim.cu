@@ -1062,7 +1062,13 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 	uint32_t R = 0, threads = 0, grid = passBlocks_;
 	size_t smem = 0;
 	if (g.kind == 1) {
-		fn = passTmaKernelFor(g.W, g.RW, g.S, g.B, g.M);
+		// the shape-specialised instance when every network has that shape
+		// (CBM_PASS_SHAPE=0 keeps the run-time-shape kernel: testing)
+		int shape = g.M == 4 ? 1 : 0;
+		for (Network *n : nets_) if (passShapeOf(n->dev()) != 1) shape = 0;
+		if (const char *env = getenv("CBM_PASS_SHAPE"))
+			if (!strcmp(env, "0")) shape = 0;
+		fn = passTmaKernelFor(g.W, g.RW, g.S, g.B, g.M, shape);
 		if (!fn) return "per-tile GR-pass geometry not compiled in";
 		R = (uint32_t)(g.W * g.RW);
 		if (R > minRows) return "more rows per stage than a tile has";
@@ -1205,6 +1211,7 @@ void Simulator::dropGraphs()
 {
 	if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
 	if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+	if (flushKernGraph_) { cudaGraphExecDestroy(flushKernGraph_); flushKernGraph_ = nullptr; }
 	if (stepGraph_) { cudaGraphExecDestroy(stepGraph_); stepGraph_ = nullptr; }
 }
 
@@ -1334,6 +1341,9 @@ std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *ste
 	CK(cudaSetDevice(device_), "selecting the device");
 	CKS(uploadCtl());
 	if (flushBytes && flushBytes != flushBuf_.bytes) {
+		// the flush graphs write the old buffer
+		if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+		if (flushKernGraph_) { cudaGraphExecDestroy(flushKernGraph_); flushKernGraph_ = nullptr; }
 		if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
 		flushBuf_.ptr = nullptr;
 		CK(cudaMalloc(&flushBuf_.ptr, flushBytes), "allocating the L2 flush buffer");
@@ -1368,6 +1378,56 @@ std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *ste
 	}
 	CKS(checkDeviceErrors());
 	*stepMs = (float)total;
+	return "";
+}
+
+std::string Simulator::runFlushedKernels(uint64_t nsteps, size_t flushBytes, float *passMs, float *tailMs)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(uploadCtl());
+	if (flushBytes && flushBytes != flushBuf_.bytes) {
+		if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
+		flushBuf_.ptr = nullptr;
+		if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+		if (flushKernGraph_) { cudaGraphExecDestroy(flushKernGraph_); flushKernGraph_ = nullptr; }
+		CK(cudaMalloc(&flushBuf_.ptr, flushBytes), "allocating the L2 flush buffer");
+		flushBuf_.bytes = flushBytes;
+	}
+	while (passEv_.size() < 2) {
+		cudaEvent_t e, f;
+		CK(cudaEventCreate(&e), "event");
+		CK(cudaEventCreate(&f), "event");
+		passEv_.push_back(e);
+		tailEv_.push_back(f);
+	}
+	if (!flushKernGraph_) {
+		// one step in the two-stream form, events around each kernel, after
+		// a write of the flush buffer
+		cudaGraph_t g;
+		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
+		if (flushBuf_.ptr) cudaMemsetAsync(flushBuf_.ptr, 0x5a, flushBuf_.bytes, s0_);
+		std::string e = enqueueStep(0, true);
+		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
+		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
+		if (!e.empty()) return e;
+		CK(ce, "graph capture");
+		CK(cudaGraphInstantiate(&flushKernGraph_, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
+		cudaGraphDestroy(g);
+	}
+	double pass = 0, tail = 0;
+	for (uint64_t k = 0; k < nsteps; k++) {
+		CK(cudaGraphLaunch(flushKernGraph_, s0_), "graph launch");
+		CK(cudaStreamSynchronize(s0_), "step");
+		float a = 0, b = 0;
+		CK(cudaEventElapsedTime(&a, passEv_[0], passEv_[1]), "pass timing");
+		CK(cudaEventElapsedTime(&b, tailEv_[0], tailEv_[1]), "tail timing");
+		pass += a;
+		tail += b;
+		for (Network *n : nets_) n->hostT_ += 1;
+	}
+	CKS(checkDeviceErrors());
+	*passMs = nsteps ? (float)(pass / nsteps) : 0.0f;
+	*tailMs = nsteps ? (float)(tail / nsteps) : 0.0f;
 	return "";
 }
 

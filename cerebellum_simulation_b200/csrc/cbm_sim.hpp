@@ -64,6 +64,9 @@ public:
 	// with events on the launch stream around every step only; *stepMs is
 	// the summed step time.
 	std::string runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs);
+	// The same steps in the two-stream form with events around each kernel:
+	// mean GR-pass and small-cell kernel durations of a step after a flush.
+	std::string runFlushedKernels(uint64_t nsteps, size_t flushBytes, float *passMs, float *tailMs);
 	std::string sync();
 	// A field of network i into host memory: the copy and a read of every
 	// network's device error word share one synchronisation.
@@ -120,7 +123,7 @@ private:
 	uint32_t graphChunk_ = 0;
 	bool graphInstrumented_ = false;
 	std::vector<cudaEvent_t> passEv_, tailEv_;
-	cudaGraphExec_t flushGraph_ = nullptr;
+	cudaGraphExec_t flushGraph_ = nullptr, flushKernGraph_ = nullptr;
 	DeviceBuf flushBuf_;
 	cudaEvent_t stepEv0_ = nullptr, stepEv1_ = nullptr;
 	float lastGraphMs_ = 0, lastPassMs_ = 0, lastTailMs_ = 0;

@@ -275,6 +275,10 @@ uint64_t cbm_batch_num_gr(cbm_batch *b);
  * summed device time of the steps alone (events on the launch stream around
  * each step). */
 int cbm_sim_run_flushed(cbm_sim *sim, uint64_t nsteps, uint64_t flushBytes, float *stepMs);
+/* Measurement helper: nsteps flushed steps as cbm_sim_run_flushed, with the
+ * two step kernels on separate streams and events around each; *passMs and
+ * *tailMs are the mean GR-pass and small-cell kernel durations. */
+int cbm_sim_run_flushed_kernels(cbm_sim *sim, uint64_t nsteps, uint64_t flushBytes, float *passMs, float *tailMs);
 
 /* Mean duration of the small-cell update kernel over the last chunk of the
  * last cbm_sim_run that timed the GR pass (0 before). */

@@ -1,4 +1,5 @@
-"""Every compiled geometry of the two TMA GR passes gives the same network
+"""Every compiled geometry of the two TMA GR passes, the per-tile pass both
+specialised for the network's shape and not, gives the same network
 state, bit for bit, as the plain GR pass kernel (the plain kernel is pinned
 to the oracle by test_gpu_parity.py): the per-tile pass (consumer warps x
 rows per warp x stages x resident CTAs x slot bound) and the persistent pass
@@ -51,8 +52,12 @@ def test_tma_pass_geometries_match_plain_pass(tmp_path):
     mf = networks.uniform_mf_stream(1024, 120, seed=5, lo=5.0, hi=60.0)
     want = run_with({"CBM_PASS_TMA": "0"}, path, mf, str(tmp_path / "plain.state"))
     for g in TILE_GEOMETRIES:
-        got = run_with({"CBM_PASS_TMA": g, "CBM_PASS_PERSIST": "0"}, path, mf, str(tmp_path / f"tma_{g}.state"))
-        assert got == want, f"per-tile geometry {g} differs from the plain pass"
+        # this network has the eyelid shape: slot bound 4 runs the
+        # shape-specialised kernel, CBM_PASS_SHAPE=0 the run-time-shape one
+        for shape_env in ({}, {"CBM_PASS_SHAPE": "0"}) if g.endswith(",4") else ({},):
+            env = {"CBM_PASS_TMA": g, "CBM_PASS_PERSIST": "0", **shape_env}
+            got = run_with(env, path, mf, str(tmp_path / f"tma_{g}.state"))
+            assert got == want, f"per-tile geometry {g} {shape_env} differs from the plain pass"
     for g in PERSISTENT_GEOMETRIES:
         got = run_with({"CBM_PASS_PERSIST": g}, path, mf, str(tmp_path / f"persist_{g}.state"))
         assert got == want, f"persistent geometry {g} differs from the plain pass"
