@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 // compiled for shape 1 (instantiated where passTmaKernelFor takes them).
 #define CBM_PASS_TMA_CONFIGS(X) \
 	X(8, 1, 3, 2, 4) X(8, 1, 3, 3, 4) X(8, 1, 4, 2, 4) X(8, 1, 2, 3, 4) X(4, 1, 4, 4, 4) X(4, 2, 3, 3, 4) X(4, 2, 4, 2, 4) \
-	X(8, 1, 3, 2, 0) X(4, 1, 4, 1, 0) X(2, 1, 4, 1, 0) X(1, 1, 4, 1, 0)
+	X(4, 2, 2, 4, 4) X(8, 1, 3, 2, 0) X(4, 1, 4, 1, 0) X(2, 1, 4, 1, 0) X(1, 1, 4, 1, 0)
 #define CBM_PASS_TMA_INST(W, RW, S, B, M) \
 	template __global__ void grPassTmaKernel<W, RW, S, B, M, 0>(const DevNet *const *, const uint32_t *, int, uint32_t);
 CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_INST)

@@ -16,7 +16,7 @@ import cbmtest
 pytestmark = pytest.mark.gpu
 
 TILE_GEOMETRIES = ["8,1,3,2,4", "8,1,3,3,4", "8,1,4,2,4", "8,1,2,3,4", "4,1,4,4,4", "4,2,3,3,4", "4,2,4,2,4",
-                   "8,1,3,2,0", "4,1,4,1,0", "2,1,4,1,0", "1,1,4,1,0"]
+                   "4,2,2,4,4", "8,1,3,2,0", "4,1,4,1,0", "2,1,4,1,0", "1,1,4,1,0"]
 PERSISTENT_GEOMETRIES = ["4,4,2,4", "4,3,3,4", "2,4,4,4", "2,6,3,4", "4,4,2,0", "2,4,2,0", "1,4,2,0"]
 # 8,2,2,4 (16-row units) does not fit tiles of 8 rows
 EVENTS = {1: [("plast", 0, -0.002, 0.002)], 60: [("errdrive", 0, 1.0)], 90: [("grgoinc", 0.01)]}
