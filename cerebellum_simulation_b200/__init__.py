@@ -291,7 +291,7 @@ class CBMSimCore:
 
     def updateMFInput(self, mf):
         mf = np.ascontiguousarray(mf, dtype=np.uint8)
-        _check(lib.cbm_sim_update_mf(self._h, _ptr(mf)))
+        _check(lib.cbm_sim_update_mf(self._h, mf.ctypes.data))
 
     def updateErrDrive(self, zoneN, errDriveRelative):
         _check(lib.cbm_sim_update_err_drive(self._h, zoneN, errDriveRelative))

@@ -1190,20 +1190,50 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
 	CKS(uploadCtl());
-	if (!stepGraph_) {
-		// one step and its counter update as one graph launch
+	// one step and its counter update as one graph launch; with deferred MF
+	// input, the graph that first copies pinned slot k into the ring
+	auto capture = [&](cudaGraphExec_t *out, int mfSlot) -> std::string {
 		cudaGraph_t g;
 		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
+		if (mfSlot >= 0) {
+			Network &n = *nets_[0];
+			cudaMemcpyAsync((void *)n.h_.mfBits, n.hPinnedBits_ + (size_t)mfSlot * n.h_.mfWords, 4ull * n.h_.mfWords,
+					cudaMemcpyHostToDevice, s0_);
+			cudaEventRecordWithFlags(n.mfStageEv_[mfSlot], s0_, cudaEventRecordExternal);
+		}
 		std::string e = enqueueStep(0, false);
 		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
 		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
 		if (!e.empty()) return e;
 		CK(ce, "graph capture");
-		CK(cudaGraphInstantiate(&stepGraph_, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
+		CK(cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
 		cudaGraphDestroy(g);
+		return "";
+	};
+	for (uint32_t k = 0; k < nsteps; k++) {
+		if (pendingMF_ >= 0) {
+			const int slot = pendingMF_;
+			if (!stepGraphMF_[slot]) CKS(capture(&stepGraphMF_[slot], slot));
+			CK(cudaGraphLaunch(stepGraphMF_[slot], s0_), "graph launch");
+			pendingMF_ = -1;
+		} else {
+			if (!stepGraph_) CKS(capture(&stepGraph_, -1));
+			CK(cudaGraphLaunch(stepGraph_, s0_), "graph launch");
+		}
 	}
-	for (uint32_t k = 0; k < nsteps; k++) CK(cudaGraphLaunch(stepGraph_, s0_), "graph launch");
 	for (Network *n : nets_) n->hostT_ += nsteps;
+	return "";
+}
+
+std::string Simulator::flushPendingMF()
+{
+	if (pendingMF_ < 0) return "";
+	Network &n = *nets_[0];
+	const int k = pendingMF_;
+	pendingMF_ = -1;
+	CK(cudaMemcpyAsync((void *)n.h_.mfBits, n.hPinnedBits_ + (size_t)k * n.h_.mfWords, 4ull * n.h_.mfWords,
+			cudaMemcpyHostToDevice, s0_), "MF upload");
+	CK(cudaEventRecord(n.mfStageEv_[k], s0_), "MF staging");
 	return "";
 }
 
@@ -1213,11 +1243,14 @@ void Simulator::dropGraphs()
 	if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
 	if (flushKernGraph_) { cudaGraphExecDestroy(flushKernGraph_); flushKernGraph_ = nullptr; }
 	if (stepGraph_) { cudaGraphExecDestroy(stepGraph_); stepGraph_ = nullptr; }
+	for (cudaGraphExec_t &e : stepGraphMF_)
+		if (e) { cudaGraphExecDestroy(e); e = nullptr; }
 }
 
 std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	pendingMF_ = -1;  // the protocol drives the MF input from now on
 	CKS(uploadCtl());
 	CK(cudaStreamSynchronize(s0_), "sync");
 	return nets_[i]->setProtocol(p, s0_);
@@ -1228,15 +1261,40 @@ std::string Simulator::stageMF(size_t i, const uint8_t *mf)
 	Network &n = *nets_[i];
 	if (n.hasProtocol()) return "a device protocol drives the MF input of this network";
 	const uint32_t W = n.h_.mfWords, M = n.h_.numMF;
-	const uint32_t k = n.mfStageNext_++ % Network::kMFStage;
-	if (n.mfStageUsed_[k]) CK(cudaEventSynchronize(n.mfStageEv_[k]), "MF staging");
+	const uint32_t k = n.mfStageNext_++ % kMFStage;
+	if (n.mfStageUsed_[k]) {
+		// usually long done: a query is cheaper than a synchronisation
+		const cudaError_t q = cudaEventQuery(n.mfStageEv_[k]);
+		if (q == cudaErrorNotReady) CK(cudaEventSynchronize(n.mfStageEv_[k]), "MF staging");
+		else CK(q, "MF staging");
+	}
 	uint32_t *bits = n.hPinnedBits_ + (size_t)k * W;
 	memset(bits, 0, 4ull * W);
 	bool raw = false;
-	for (uint32_t c = 0; c < M; c++) {
+	// eight input bytes at a time: the bytes' low bits gathered by one
+	// multiply; any byte above 1 marks raw (graded) input
+	uint64_t hi = 0;
+	uint32_t c = 0;
+	for (; c + 8 <= M; c += 8) {
+		uint64_t x;
+		memcpy(&x, mf + c, 8);
+		hi |= x & 0xFEFEFEFEFEFEFEFEull;
+		const uint64_t lo = (x | (x >> 1) | (x >> 2) | (x >> 3) | (x >> 4) | (x >> 5) | (x >> 6) | (x >> 7)) &
+			0x0101010101010101ull;
+		bits[c >> 5] |= (uint32_t)((lo * 0x0102040810204080ull) >> 56) << (c & 31);
+	}
+	for (; c < M; c++) {
 		if (mf[c]) bits[c >> 5] |= 1u << (c & 31);
 		if (mf[c] > 1) raw = true;
 	}
+	if (hi) raw = true;
+	if (nets_.size() == 1 && n.h_.mfRing == 1 && !raw && !n.h_.hasMFRaw) {
+		// the next single step's graph copies slot k (and records its event)
+		pendingMF_ = (int)k;
+		n.mfStageUsed_[k] = true;
+		return "";
+	}
+	pendingMF_ = -1;  // this input supersedes a deferred one
 	const uint64_t slot = n.hostT_ % n.h_.mfRing;
 	CK(cudaMemcpyAsync((void *)(n.h_.mfBits + slot * W), bits, 4ull * W, cudaMemcpyHostToDevice, s0_), "MF upload");
 	if (raw || n.h_.hasMFRaw) {
@@ -1282,6 +1340,7 @@ std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, 
 std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (chunk == 0) chunk = 1;
 	if (!graphExec_ || graphChunk_ != chunk || graphInstrumented_ != instrument) {
@@ -1339,6 +1398,7 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (flushBytes && flushBytes != flushBuf_.bytes) {
 		// the flush graphs write the old buffer
@@ -1384,6 +1444,7 @@ std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *ste
 std::string Simulator::runFlushedKernels(uint64_t nsteps, size_t flushBytes, float *passMs, float *tailMs)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (flushBytes && flushBytes != flushBuf_.bytes) {
 		if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);

@@ -33,6 +33,9 @@ struct DeviceBuf {
 
 class Network;
 
+// Pinned staging slots for host MF input per network (updateMFInput).
+constexpr uint32_t kMFStage = 8;
+
 // A GR-pass kernel choice: kind 0 plain, 1 per-tile TMA (W consumer warps of
 // RW rows, S stages, B CTAs/SM, slot bound M), 2 persistent TMA (W, S, B, M).
 struct PassGeometry {
@@ -102,7 +105,14 @@ private:
 	std::string uploadCtl();
 	std::string enqueueStep(uint32_t stepOffset, bool instrument);
 	void dropGraphs();
+	// Issue the copy of MF input that a single-step graph would have carried.
+	std::string flushPendingMF();
 	cudaGraphExec_t stepGraph_ = nullptr;  // one step and its counter update (launchSteps)
+	// One network, one-slot MF ring, spike-bit input: updateMFInput only
+	// packs the bits into pinned slot k, and the next step's graph
+	// (stepGraphMF_[k]) copies them in before the kernels.
+	int pendingMF_ = -1;
+	cudaGraphExec_t stepGraphMF_[kMFStage] = {};
 	uint32_t *hErr_ = nullptr;             // pinned copies of the networks' error words
 	uint8_t *hExport_ = nullptr;           // pinned export staging
 	size_t hExportBytes_ = 0;
@@ -200,7 +210,6 @@ private:
 	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;
 	// pinned staging of host MF input: kMFStage slots, each reused once the
 	// copy that last read it has run (mfStageEv_)
-	static constexpr uint32_t kMFStage = 8;
 	uint32_t *hPinnedBits_ = nullptr;
 	uint8_t *hPinnedRaw_ = nullptr;
 	cudaEvent_t mfStageEv_[kMFStage] = {};
