@@ -304,12 +304,13 @@ template <> struct PassShape<1> {
 
 template <int W, int RW, int S, int MINB, int MS, int SH>
 __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevNet *const *nets,
-		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
+		const uint32_t *blockOffset, int numNets, uint32_t stepOffset, const DevNet *net0)
 {
 	using Sh = PassShape<SH>;
 	constexpr uint32_t R = W * RW;
-	uint32_t local;
-	const DevNet *__restrict__ N = locateNet(nets, blockOffset, numNets, blockIdx.x, local);
+	// one network: its descriptor comes as a parameter (a round trip fewer)
+	uint32_t local = blockIdx.x;
+	const DevNet *__restrict__ N = net0 ? net0 : locateNet(nets, blockOffset, numNets, blockIdx.x, local);
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 
 	const uint32_t P = N->P, bs = N->bs, K = N->K, Z = Sh::z ? Sh::z : N->numZones;
@@ -348,16 +349,42 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	const uint32_t bcBase = (pc * P) >> N->bcShift, scBase = (pc * P) >> N->scShift;
 
 	if (warp == W) {
-		// ---- producer
-		if (lane == 0) {
-			const CUtensorMap *maps = N->passMaps;
+		// ---- producer: lane 0 issues the copies; the whole warp takes the
+		// running sums of the PF->PC reduction (sumInputsNew's per-thread
+		// tempSum += x[i] + x[i+bs], kernels.cu:326-362, lane = j) stage by
+		// stage in row order, as each stage is consumed
+		const CUtensorMap *maps = N->passMaps;
+		if (lane == 0)
 			for (int m = 0; m < PM_W0 + (int)Z; m++) tma::prefetchMap(&maps[m]);
-			const uint32_t tx = L.txBase + (plastStep ? L.txHist : 0u);
-			uint32_t issued = 0, slot = 0, phase = 0;
-			bool ok = true;
+		const uint32_t tx = L.txBase + (plastStep ? L.txHist : 0u);
+		uint32_t issued = 0, slot = 0, phase = 0;
+		bool ok = true;
+		float run[kMaxZones], even[kMaxZones];
+#pragma unroll
+		for (uint32_t z = 0; z < kMaxZones; z++) run[z] = even[z] = 0.0f;
+		auto sumStage = [&](uint32_t sst) {
+			for (uint32_t rr = 0; rr < R; rr++) {
+				const uint32_t r = sst * R + rr;
+#pragma unroll
+				for (uint32_t z = 0; z < kMaxZones; z++) {
+					if (z >= Z) break;
+					const float x = sX[((size_t)z * rows + r) * 32u + lane];
+					if (r & 1u) run[z] += even[z] + x;
+					else even[z] = x;
+				}
+			}
+		};
+		{
 			for (uint32_t st = 0; st < nStages; st++) {
-				// refill number st/S of this slot waits until its previous contents are consumed
-				if (st >= (uint32_t)S && !tma::waitBounded(&empty[slot], phase ^ 1u, kPassWaitLimitNs)) { ok = false; break; }
+				// refill number st/S of this slot waits until its previous
+				// contents are consumed (and summed)
+				if (st >= (uint32_t)S) {
+					const bool done = tma::waitBounded(&empty[slot], phase ^ 1u, kPassWaitLimitNs);
+					if (!__all_sync(0xffffffffu, done)) { ok = false; break; }
+					sumStage(st - S);
+				}
+				issued = st + 1;
+				if (lane != 0) { if (++slot == (uint32_t)S) { slot = 0; phase ^= 1u; } continue; }
 				uint8_t *b = stages + (size_t)slot * L.bytes;
 				uint64_t *bar = &full[slot];
 				tma::arriveExpectTx(bar, tx);
@@ -370,10 +397,23 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 				tma::load2d(b + L.pfDelay, &maps[PM_PFDELAY], x, y, bar);
 				for (uint32_t z = 0; z < Z; z++) tma::load2d(b + L.w + z * 128u * R, &maps[PM_W0 + z], x, y, bar);
 				if (plastStep) tma::load2d(b + L.hist, &maps[PM_HIST], x, y, bar);
-				issued = st + 1;
 				if (++slot == (uint32_t)S) { slot = 0; phase ^= 1u; }
 			}
-			if (!ok) {
+			__syncwarp();
+			// the last stages, once consumed
+			for (uint32_t st = issued > (uint32_t)S ? issued - S : 0; ok && st < issued; st++) {
+				const bool done = tma::waitBounded(&empty[st % S], (st / S) & 1u, kPassWaitLimitNs);
+				if (!__all_sync(0xffffffffu, done)) { ok = false; break; }
+				sumStage(st);
+			}
+			if (ok) {
+				const uint32_t buf = (uint32_t)(t % 3);
+#pragma unroll
+				for (uint32_t z = 0; z < kMaxZones; z++) {
+					if (z >= Z) break;
+					N->zones[z].pcPartial[((size_t)buf * N->numPC + pc) * bs + j0 + lane] = run[z];
+				}
+			} else if (lane == 0) {
 				atomicOr(N->errFlag, kErrPassWait);
 				// let the copies in flight land before the CTA's shared memory is released
 				for (uint32_t st = issued > (uint32_t)S ? issued - S : 0; st < issued; st++)
@@ -536,15 +576,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	}
 	__syncthreads();
 
-	// sumInputsNew's per-thread running sums: tempSum += x[i] + x[i+bs]
+	// the BC and SC counts of the tile (the producer wrote the PF->PC partials)
 	const uint32_t buf = (uint32_t)(t % 3);
-	for (uint32_t task = threadIdx.x; task < Z * 32u; task += blockDim.x) {
-		const uint32_t z = task / 32u, jj = task % 32u;
-		const float *xs = sX + (size_t)z * rows * 32u + jj;
-		float s = 0;
-		for (uint32_t kk = 0; kk < K; kk++) s += xs[(2 * kk) * 32u] + xs[(2 * kk + 1) * 32u];
-		N->zones[z].pcPartial[((size_t)buf * N->numPC + pc) * bs + j0 + jj] = s;
-	}
 	uint32_t *bcOut = N->bcCount + (size_t)buf * N->numBC;
 	uint32_t *scOut = N->scCount + (size_t)buf * N->numSC;
 	for (uint32_t i = threadIdx.x; i < N->bcLocal + N->scLocal; i += blockDim.x) {
@@ -562,7 +595,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	X(8, 1, 3, 2, 4) X(8, 1, 3, 3, 4) X(8, 1, 4, 2, 4) X(8, 1, 2, 3, 4) X(4, 1, 4, 4, 4) X(4, 2, 3, 3, 4) X(4, 2, 4, 2, 4) \
 	X(4, 2, 2, 4, 4) X(8, 1, 3, 2, 0) X(4, 1, 4, 1, 0) X(2, 1, 4, 1, 0) X(1, 1, 4, 1, 0)
 #define CBM_PASS_TMA_INST(W, RW, S, B, M) \
-	template __global__ void grPassTmaKernel<W, RW, S, B, M, 0>(const DevNet *const *, const uint32_t *, int, uint32_t);
+	template __global__ void grPassTmaKernel<W, RW, S, B, M, 0>(const DevNet *const *, const uint32_t *, int, uint32_t, \
+		const DevNet *);
 CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_INST)
 
 int passTmaConfigCount()
@@ -1653,16 +1687,17 @@ __global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet
 // (one bulk copy in and one out per step instead of a global round trip per
 // phase).
 __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, const uint32_t *stageBytes,
-		uint32_t stepOffset)
+		uint32_t stepOffset, const DevNet *net0, uint32_t stage0)
 {
 	// the GR pass of the same step may launch once these CTAs are resident
 	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 	const uint32_t net = blockIdx.x >> 1;
-	const DevNet *__restrict__ N = nets[net];
+	// one network: descriptor and staging size come as parameters
+	const DevNet *__restrict__ N = net0 ? net0 : nets[net];
 	extern __shared__ __align__(16) uint32_t tailSmem[];
 	__shared__ ZoneIn in;
 	if (blockIdx.x & 1) {
-		const uint32_t bytes = stageBytes[net];
+		const uint32_t bytes = net0 ? stage0 : stageBytes[net];
 		if (bytes) {
 			uint8_t *base = reinterpret_cast<uint8_t *>(tailSmem);
 			stageIn(N, base, bytes);

@@ -13,8 +13,9 @@ __global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOff
 // TMA GR pass with W consumer warps of RW rows each per stage, S stages
 // deep, at least B resident CTAs per SM, synapse-slot loops bounded by M
 // (0: any count), compiled for network shape `shape` (0: any network; see
-// passShapeOf); launched with 32 * (W + 1) threads and the grPassKernel
-// arguments.  Returns null for a geometry that is not compiled in.
+// passShapeOf); launched with 32 * (W + 1) threads, the grPassKernel
+// arguments and the descriptor of a single network (null for a batch).
+// Returns null for a geometry that is not compiled in.
 const void *passTmaKernelFor(int W, int RW, int S, int B, int M, int shape);
 // The most specific pass shape a network matches (0 when none).
 int passShapeOf(const DevNet &h);
@@ -26,8 +27,10 @@ void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M);
 // 32 * (W + 1) threads, the grPassKernel arguments with one network.
 const void *passPersistentKernelFor(int W, int S, int B, int M);
 // Small-cell update; stageBytes[n] is network n's staging block size (0:
-// its microzone CTA works on global memory).
-__global__ void tailKernel(const DevNet *const *nets, const uint32_t *stageBytes, uint32_t stepOffset);
+// its microzone CTA works on global memory).  With one network, net0 and
+// stage0 give its descriptor and staging size directly (else null, 0).
+__global__ void tailKernel(const DevNet *const *nets, const uint32_t *stageBytes, uint32_t stepOffset,
+		const DevNet *net0, uint32_t stage0);
 __global__ void protocolPrimeKernel(const DevNet *N);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);

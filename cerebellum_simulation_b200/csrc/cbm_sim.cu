@@ -1130,9 +1130,12 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	const uint32_t *offsArg = (const uint32_t *)dBlockOffset_.ptr;
 	int numNetsArg = (int)nets_.size();
 	uint32_t stepArg = k;
+	const DevNet *net0Arg = nets_.size() == 1 ? nets_[0]->devPtr() : nullptr;
+	const uint32_t stage0Arg = nets_.size() == 1 ? nets_[0]->stageBytes() : 0u;
 	auto launchPass = [&](cudaStream_t st, bool dependent) -> std::string {
 		if (passTmaFn_) {
-			void *args[] = {&netsArg, &offsArg, &numNetsArg, &stepArg};
+			// the per-tile pass takes the single network's descriptor too
+			void *args[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg};
 			cudaLaunchConfig_t cfg = {};
 			cfg.gridDim = dim3(passGrid_);
 			cfg.blockDim = dim3(32 * (passTmaW_ + 1));
@@ -1167,7 +1170,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 		CKS(launchPass(s0_, false));
 		CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k], s1_, cudaEventRecordExternal), "tail timing");
-		tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>(netsArg, stageArg, k);
+		tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>(netsArg, stageArg, k, net0Arg, stage0Arg);
 		CK(cudaGetLastError(), "launching the small-cell update");
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
 		CK(cudaEventRecord(join_, s1_), "join");
@@ -1178,7 +1181,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	// as soon as they are resident (programmatic dependent launch; the two
 	// kernels of a step share no buffer), so the pass cannot take the SMs the
 	// small-cell CTAs need.  The next step waits for both.
-	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s0_>>>(netsArg, stageArg, k);
+	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s0_>>>(netsArg, stageArg, k, net0Arg, stage0Arg);
 	CK(cudaGetLastError(), "launching the small-cell update");
 	CK(cudaEventRecord(join_, s0_), "join");
 	CKS(launchPass(s0_, true));
