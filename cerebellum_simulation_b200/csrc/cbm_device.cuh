@@ -213,7 +213,7 @@ struct DevNet {
 	const uint8_t *mfRaw;    // [mfRing][numMF] raw MF input bytes (NC inputs), or null
 	uint64_t *tBase;     // steps completed
 	HostCtl *ctl;
-	uint32_t *errFlag;   // device error word (kErr* bits)
+	uint32_t *errFlag;   // error word (kErr* bits), in mapped pinned host memory
 	const CUtensorMap *passMaps;  // [PM_COUNT] descriptors of the TMA GR pass, or null
 	DevProtocol *proto;           // device-driven trial protocol, or null
 	const StageSeg *zoneSegs;     // arrays the microzone CTA stages in shared memory

@@ -114,6 +114,15 @@ __device__ __forceinline__ float errDriveOf(const DevNet *N, uint64_t t, uint32_
 	return N->ctl->errDrive[z];
 }
 
+// Report an error to the host: the error word lives in mapped pinned host
+// memory, read after the host synchronises; a plain store (there is one
+// error kind, so no read-modify-write is needed).
+__device__ __forceinline__ void raiseError(const DevNet *N, uint32_t bit)
+{
+	*reinterpret_cast<volatile uint32_t *>(N->errFlag) = bit;
+	__threadfence_system();
+}
+
 __device__ __forceinline__ const DevNet *locateNet(const DevNet *const *nets, const uint32_t *blockOffset,
 		int numNets, uint32_t b, uint32_t &local)
 {
@@ -414,7 +423,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 					N->zones[z].pcPartial[((size_t)buf * N->numPC + pc) * bs + j0 + lane] = run[z];
 				}
 			} else if (lane == 0) {
-				atomicOr(N->errFlag, kErrPassWait);
+				raiseError(N, kErrPassWait);
 				// let the copies in flight land before the CTA's shared memory is released
 				for (uint32_t st = issued > (uint32_t)S ? issued - S : 0; st < issued; st++)
 					tma::waitBounded(&full[st % S], (st / S) & 1u, kPassWaitLimitNs);
@@ -477,7 +486,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 		for (uint32_t st = 0; st < nStages; st++) {
 			const bool ready = tma::waitBounded(&full[slot], phase, kPassWaitLimitNs);
 			if (!__all_sync(0xffffffffu, ready)) {
-				if (lane == 0) atomicOr(N->errFlag, kErrPassWait);
+				if (lane == 0) raiseError(N, kErrPassWait);
 				break;
 			}
 			const uint8_t *b = stages + (size_t)slot * L.bytes;
@@ -748,7 +757,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(con
 				if (++slot == (uint32_t)S) { slot = 0; phase ^= 1u; }
 			}
 			if (!ok) {
-				atomicOr(N->errFlag, kErrPassWait);
+				raiseError(N, kErrPassWait);
 				for (uint32_t k = issued > (uint32_t)S ? issued - S : 0; k < issued; k++)
 					tma::waitBounded(&full[k % S], (k / S) & 1u, kPassWaitLimitNs);
 			}
@@ -790,7 +799,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(con
 	for (uint32_t u = blockIdx.x; u < numUnits; u += gridDim.x) {
 		const bool ready = tma::waitBounded(&full[slot], phase, kPassWaitLimitNs);
 		if (!__all_sync(0xffffffffu, ready)) {
-			if (lane == 0) atomicOr(N->errFlag, kErrPassWait);
+			if (lane == 0) raiseError(N, kErrPassWait);
 			break;
 		}
 		const uint32_t tile = u / unitsPerTile, chunk = u % unitsPerTile;

@@ -47,6 +47,7 @@ Network::~Network()
 	for (void *p : allocs_) cudaFree(p);
 	if (dNet_.ptr) cudaFree(dNet_.ptr);
 	if (hPinnedBits_) cudaFreeHost(hPinnedBits_);
+	if (hErr_) cudaFreeHost(hErr_);
 	if (hPinnedRaw_) cudaFreeHost(hPinnedRaw_);
 	for (cudaEvent_t e : mfStageEv_) if (e) cudaEventDestroy(e);
 }
@@ -588,7 +589,12 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	h.hasMFRaw = 0;
 	h.tBase = alloc<uint64_t>(1);
 	h.ctl = alloc<HostCtl>(1);
-	h.errFlag = alloc<uint32_t>(1);
+	// the error word in mapped pinned host memory: the host reads it after a
+	// synchronisation without a copy
+	if (cudaHostAlloc((void **)&hErr_, sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess)
+		return "pinned allocation failed";
+	*hErr_ = 0;
+	CK(cudaHostGetDevicePointer((void **)&h.errFlag, hErr_, 0), "mapping the error word");
 	for (void *p : allocs_) if (!p) return "device allocation failed";
 	CKS(buildZoneStaging());
 	if (cudaMallocHost((void **)&hPinnedBits_, (size_t)kMFStage * h.mfWords * 4) != cudaSuccess ||
@@ -922,7 +928,6 @@ Simulator::~Simulator()
 {
 	dropGraphs();
 	if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
-	if (hErr_) cudaFreeHost(hErr_);
 	if (hExport_) cudaFreeHost(hExport_);
 	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
@@ -1320,7 +1325,6 @@ std::string Simulator::stageMF(size_t i, const uint8_t *mf)
 std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, size_t bytes)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
-	if (!hErr_) CK(cudaMallocHost((void **)&hErr_, 4 * nets_.size()), "pinned allocation");
 	if (bytes > hExportBytes_) {
 		if (hExport_) cudaFreeHost(hExport_);
 		hExport_ = nullptr;
@@ -1329,13 +1333,9 @@ std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, 
 		hExportBytes_ = bytes;
 	}
 	CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s0_));
-	for (size_t k = 0; k < nets_.size(); k++)
-		CK(cudaMemcpyAsync(hErr_ + k, nets_[k]->h_.errFlag, 4, cudaMemcpyDeviceToHost, s0_), "reading the device error word");
 	CK(cudaStreamSynchronize(s0_), "export");
-	for (size_t k = 0; k < nets_.size(); k++) {
-		if (hErr_[k] & kErrPassWait) return "GR pass: a pipeline wait timed out on the device";
-		if (hErr_[k]) return "device error word set";
-	}
+	markInputSlotsFree();
+	CKS(checkDeviceErrors());
 	memcpy(dst, hExport_, bytes);
 	return "";
 }
@@ -1509,19 +1509,27 @@ std::string Simulator::timerStop(float *ms)
 	return "";
 }
 
+void Simulator::markInputSlotsFree()
+{
+	// every copy enqueued so far has run: no staging slot needs a query
+	for (Network *n : nets_)
+		for (bool &u : n->mfStageUsed_) u = false;
+}
+
 std::string Simulator::sync()
 {
 	CK(cudaStreamSynchronize(s0_), "sync");
 	CK(cudaStreamSynchronize(s1_), "sync");
+	markInputSlotsFree();
 	CK(cudaGetLastError(), "sync");
 	return checkDeviceErrors();
 }
 
 std::string Simulator::checkDeviceErrors()
 {
+	// after a synchronisation with the kernels that may have written them
 	for (Network *n : nets_) {
-		uint32_t flag = 0;
-		CK(cudaMemcpy(&flag, n->h_.errFlag, sizeof(flag), cudaMemcpyDeviceToHost), "reading the device error word");
+		const uint32_t flag = *reinterpret_cast<volatile uint32_t *>(n->hErr_);
 		if (flag & kErrPassWait) return "GR pass: a pipeline wait timed out on the device";
 		if (flag) return "device error word set";
 	}

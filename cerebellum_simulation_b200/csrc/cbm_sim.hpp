@@ -105,6 +105,7 @@ private:
 	std::string uploadCtl();
 	std::string enqueueStep(uint32_t stepOffset, bool instrument);
 	void dropGraphs();
+	void markInputSlotsFree();  // after a full synchronisation
 	// Issue the copy of MF input that a single-step graph would have carried.
 	std::string flushPendingMF();
 	cudaGraphExec_t stepGraph_ = nullptr;  // one step and its counter update (launchSteps)
@@ -113,7 +114,6 @@ private:
 	// (stepGraphMF_[k]) copies them in before the kernels.
 	int pendingMF_ = -1;
 	cudaGraphExec_t stepGraphMF_[kMFStage] = {};
-	uint32_t *hErr_ = nullptr;             // pinned copies of the networks' error words
 	uint8_t *hExport_ = nullptr;           // pinned export staging
 	size_t hExportBytes_ = 0;
 	std::vector<Network *> nets_;
@@ -210,6 +210,7 @@ private:
 	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;
 	// pinned staging of host MF input: kMFStage slots, each reused once the
 	// copy that last read it has run (mfStageEv_)
+	uint32_t *hErr_ = nullptr;  // the error word (mapped pinned host memory; h_.errFlag maps it)
 	uint32_t *hPinnedBits_ = nullptr;
 	uint8_t *hPinnedRaw_ = nullptr;
 	cudaEvent_t mfStageEv_[kMFStage] = {};
