@@ -32,9 +32,14 @@ constexpr uint32_t kErrPassWait = 1u;  // a GR-pass pipeline wait timed out
 // copied in boxes of 32 cells x R rows (x all slots).
 enum PassMap : int {
 	PM_V = 0, PM_GKCA, PM_THRESH, PM_GESUM, PM_GISUM, PM_APBUF,  // 4-byte state, read and rewritten
-	PM_MFIDX, PM_GOIDX, PM_OUTCON, PM_PFDELAY, PM_HIST, PM_W0,
+	PM_MFIDX, PM_GOIDX, PM_OUTCON, PM_PFDELAY, PM_HIST, PM_OUTCON16, PM_W0,
 	PM_COUNT = PM_W0 + kMaxZones
 };
+
+// 16-bit GR->GO synapse: (GO << 5) | delay bit, for networks of at most
+// 2047 GO; kOut16None marks an empty slot.
+constexpr uint16_t kOut16None = 0xFFFFu;
+constexpr uint32_t kOut16MaxGO = 2047u;
 
 // A device array that a small-cell CTA copies into shared memory for the
 // step (and back when it changes): the CTA then runs on a shared-memory copy
@@ -57,7 +62,9 @@ struct PassLayout {
 
 CBM_LAYOUT_FN uint32_t align128(uint32_t x) { return (x + 127u) & ~127u; }
 
-CBM_LAYOUT_FN PassLayout passLayout(uint32_t R, uint32_t nMF, uint32_t nGO, uint32_t nOut, uint32_t Z)
+// outBytes: 4 for the 32-bit GR->GO slot table, 2 for the 16-bit one.
+CBM_LAYOUT_FN PassLayout passLayout(uint32_t R, uint32_t nMF, uint32_t nGO, uint32_t nOut, uint32_t Z,
+		uint32_t outBytes = 4)
 {
 	const uint32_t mfS = nMF ? nMF : 1, goS = nGO ? nGO : 1, outS = nOut ? nOut : 1;
 	const uint32_t row4 = 128u * R;  // one 4-byte array: R rows x 32 cells
@@ -65,12 +72,12 @@ CBM_LAYOUT_FN PassLayout passLayout(uint32_t R, uint32_t nMF, uint32_t nGO, uint
 	uint32_t o = 6 * row4;
 	L.mfIdx = o; o = align128(o + 64u * R * mfS);
 	L.goIdx = o; o = align128(o + 64u * R * goS);
-	L.outCon = o; o = align128(o + row4 * outS);
+	L.outCon = o; o = align128(o + 32u * outBytes * R * outS);
 	L.pfDelay = o; o = align128(o + 32u * R);
 	L.w = o; o = align128(o + row4 * Z);
 	L.hist = o; o = align128(o + 256u * R);
 	L.bytes = o;
-	L.txBase = 6 * row4 + 64u * R * mfS + 64u * R * goS + row4 * outS + 32u * R + row4 * Z;
+	L.txBase = 6 * row4 + 64u * R * mfS + 64u * R * goS + 32u * outBytes * R * outS + 32u * R + row4 * Z;
 	L.txHist = 256u * R;
 	return L;
 }
@@ -188,6 +195,7 @@ struct DevNet {
 	const uint16_t *mfIdx;    // [nMFSlots][numGR], sentinel numMF
 	const uint16_t *goIdx;    // [nGOSlots][numGR], sentinel numGO
 	const uint32_t *outCon;   // [nOutSlots][numGR]: (GO << 8) | delay bit, kNoDelay when empty
+	const uint16_t *outCon16; // the same as 16-bit entries (kOut16None when empty), or null (> 2047 GO)
 	const uint8_t *pfDelay;   // delay bit of the PF->BC/SC/PC output, kNoDelay when none
 
 	// ---- GO / MF / SC state (innetactivitystate.h)

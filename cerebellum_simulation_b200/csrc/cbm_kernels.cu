@@ -302,13 +302,13 @@ __device__ __forceinline__ int countSpikes(const uint8_t *spikes, const uint16_t
 // loops lose their predicates).  Shape 0 reads them at run time.
 template <int SH> struct PassShape {
 	static constexpr uint32_t mf = 0, go = 0, out = 0, z = 0;
-	static constexpr bool uniform = false;
+	static constexpr bool uniform = false, out16 = false;
 };
-// 4 MF and 3 GO dendrites, 4 GR->GO slots, one zone, BC and SC blocks of at
-// least 32 cells (the eyelid networks)
+// 4 MF and 3 GO dendrites, 4 GR->GO slots (streamed as the 16-bit table),
+// one zone, BC and SC blocks of at least 32 cells (the eyelid networks)
 template <> struct PassShape<1> {
 	static constexpr uint32_t mf = 4, go = 3, out = 4, z = 1;
-	static constexpr bool uniform = true;
+	static constexpr bool uniform = true, out16 = true;
 };
 
 template <int W, int RW, int S, int MINB, int MS, int SH>
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	const uint32_t rows = 2 * K, nStages = rows / R;
 	const uint32_t nMFSlots = Sh::mf ? Sh::mf : N->nMFSlots, nGOSlots = Sh::go ? Sh::go : N->nGOSlots,
 		nOutSlots = Sh::out ? Sh::out : N->nOutSlots;
-	const PassLayout L = passLayout(R, nMFSlots, nGOSlots, nOutSlots, Z);
+	const PassLayout L = passLayout(R, nMFSlots, nGOSlots, nOutSlots, Z, Sh::out16 ? 2u : 4u);
 
 	extern __shared__ uint8_t passSmemRaw[];
 	uint8_t *stages = passSmemRaw + ((128u - (tma::smemAddr(passSmemRaw) & 127u)) & 127u);
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 				for (int m = PM_V; m <= PM_APBUF; m++) tma::load2d(b + (uint32_t)m * 128u * R, &maps[m], x, y, bar);
 				tma::load3d(b + L.mfIdx, &maps[PM_MFIDX], x, y, 0, bar);
 				tma::load3d(b + L.goIdx, &maps[PM_GOIDX], x, y, 0, bar);
-				tma::load3d(b + L.outCon, &maps[PM_OUTCON], x, y, 0, bar);
+				tma::load3d(b + L.outCon, &maps[Sh::out16 ? PM_OUTCON16 : PM_OUTCON], x, y, 0, bar);
 				tma::load2d(b + L.pfDelay, &maps[PM_PFDELAY], x, y, bar);
 				for (uint32_t z = 0; z < Z; z++) tma::load2d(b + L.w + z * 128u * R, &maps[PM_W0 + z], x, y, bar);
 				if (plastStep) tma::load2d(b + L.hist, &maps[PM_HIST], x, y, bar);
@@ -506,7 +506,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 				const uint32_t ab = reinterpret_cast<const uint32_t *>(b)[5 * 32 * R + e];
 				const uint16_t *mfI = reinterpret_cast<const uint16_t *>(b + L.mfIdx) + e;
 				const uint16_t *goI = reinterpret_cast<const uint16_t *>(b + L.goIdx) + e;
-				const uint32_t *outC = reinterpret_cast<const uint32_t *>(b + L.outCon) + e;
+				// the 32-bit slot table at element e (the 16-bit one is indexed from its base)
+				const uint32_t *outC = reinterpret_cast<const uint32_t *>(b + L.outCon) + (Sh::out16 ? 0u : e);
 				const uint32_t d = (b + L.pfDelay)[e];
 				const uint64_t h = plastStep ? reinterpret_cast<const uint64_t *>(b + L.hist)[e] : 0ull;
 				const int cntMF = countSpikes<MS>(sMF, mfI, nMFSlots, 32 * R);
@@ -546,7 +547,14 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 				if (plastStep) historyGR[g] = (h << 1) | ((abN & 0x0000001Fu) > 0);
 				// GR->GO synapses whose delayed spike arrives now
 				if (abN) {
-					if constexpr (MS > 0) {
+					if constexpr (Sh::out16) {
+						const uint16_t *outC16 = reinterpret_cast<const uint16_t *>(outC) + e;
+#pragma unroll
+						for (uint32_t s = 0; s < Sh::out; s++) {
+							const uint32_t c = outC16[s * 32 * R];
+							if (c != kOut16None && ((abN >> (c & 31u)) & 1u)) atomicAdd(&goCount[c >> 5], 1u);
+						}
+					} else if constexpr (MS > 0) {
 #pragma unroll
 						for (uint32_t s = 0; s < (uint32_t)MS; s++) {
 							if (s >= nOutSlots) break;
@@ -642,7 +650,7 @@ int passShapeOf(const DevNet &h)
 {
 	using E = PassShape<1>;
 	if (h.numZones == E::z && h.nMFSlots == E::mf && h.nGOSlots == E::go && h.nOutSlots == E::out &&
-			(1u << h.bcShift) >= 32u && (1u << h.scShift) >= 32u)
+			(1u << h.bcShift) >= 32u && (1u << h.scShift) >= 32u && h.outCon16)
 		return 1;
 	return 0;
 }

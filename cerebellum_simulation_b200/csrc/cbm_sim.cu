@@ -77,9 +77,9 @@ size_t Network::passSmemBytes() const
 		sizeof(float) * (size_t)h_.numZones * 2 * h_.K * h_.J;
 }
 
-size_t Network::passTmaSmemBytes(uint32_t R, uint32_t S) const
+size_t Network::passTmaSmemBytes(uint32_t R, uint32_t S, uint32_t outBytes) const
 {
-	const PassLayout L = passLayout(R, h_.nMFSlots, h_.nGOSlots, h_.nOutSlots, h_.numZones);
+	const PassLayout L = passLayout(R, h_.nMFSlots, h_.nGOSlots, h_.nOutSlots, h_.numZones, outBytes);
 	return 128 + (size_t)S * L.bytes + 16ull * S + sizeof(uint32_t) * (((size_t)h_.bcLocal + h_.scLocal + 3) & ~(size_t)3) +
 		sizeof(float) * (size_t)h_.numZones * 2 * h_.K * 32 + 32ull * (h_.mfWords + h_.goWords);
 }
@@ -141,6 +141,8 @@ std::string Network::buildPassMaps(uint32_t R)
 	CKS(enc3(PM_MFIDX, h_.mfIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nMFSlots)));
 	CKS(enc3(PM_GOIDX, h_.goIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nGOSlots)));
 	CKS(enc3(PM_OUTCON, h_.outCon, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, std::max(1u, h_.nOutSlots)));
+	if (h_.outCon16)
+		CKS(enc3(PM_OUTCON16, h_.outCon16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nOutSlots)));
 	CKS(enc2(PM_PFDELAY, h_.pfDelay, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1));
 	CKS(enc2(PM_HIST, h_.historyGR, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8));
 	for (uint32_t z = 0; z < h_.numZones; z++) CKS(enc2(PM_W0 + z, h_.zones[z].w, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
@@ -284,7 +286,7 @@ double Network::bytesPerStepLayout() const
 	// GR state read and written (6 x 4 B each way), synapse slots (u16 MF and
 	// GO indices, u32 GR->GO targets), the PF delay byte, the PF->PC weight
 	// of every zone; history read + write and weight writes on plasticity steps
-	const double perGR = 48.0 + 2.0 * h_.nMFSlots + 2.0 * h_.nGOSlots + 4.0 * h_.nOutSlots + 1.0 + 4.0 * h_.numZones +
+	const double perGR = 48.0 + 2.0 * h_.nMFSlots + 2.0 * h_.nGOSlots + (double)outBytes_ * h_.nOutSlots + 1.0 + 4.0 * h_.numZones +
 		(16.0 + 4.0 * h_.numZones) / h_.tsPerHistBinGR;
 	return perGR * h_.numGR;
 }
@@ -414,6 +416,14 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	h.mfIdx = upload(mfIdx.data(), mfIdx.size());
 	h.goIdx = upload(goIdx.data(), goIdx.size());
 	h.outCon = upload(outCon.data(), outCon.size());
+	h.outCon16 = nullptr;
+	if (c.numGO <= kOut16MaxGO) {
+		// the 16-bit copy the shape-specialised GR pass streams
+		std::vector<uint16_t> out16(outCon.size(), kOut16None);
+		for (size_t i = 0; i < outCon.size(); i++)
+			if ((outCon[i] & 0xFFu) < 32u) out16[i] = (uint16_t)(((outCon[i] >> 8) << 5) | (outCon[i] & 0x1Fu));
+		h.outCon16 = upload(out16.data(), out16.size());
+	}
 	h.pfDelay = upload(pfDelay.data(), pfDelay.size());
 
 	auto upF = [&](const char *n, int z = -1) { NamedArray *x = A(n, z); return upload(x->as<float>(), x->count); };
@@ -1053,6 +1063,7 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 		minRows = std::min(minRows, n->passRows());
 		maxSlots = std::max({maxSlots, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutSlots});
 	}
+	for (Network *n : nets_) n->outBytes_ = 4;
 	if (g.kind == 0) {
 		passTmaFn_ = nullptr;
 		passPersistent_ = false;
@@ -1077,7 +1088,8 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 		if (!fn) return "per-tile GR-pass geometry not compiled in";
 		R = (uint32_t)(g.W * g.RW);
 		if (R > minRows) return "more rows per stage than a tile has";
-		for (Network *n : nets_) smem = std::max(smem, n->passTmaSmemBytes(R, (uint32_t)g.S));
+		for (Network *n : nets_) smem = std::max(smem, n->passTmaSmemBytes(R, (uint32_t)g.S, shape == 1 ? 2u : 4u));
+		for (Network *n : nets_) n->outBytes_ = shape == 1 ? 2u : 4u;
 		threads = 32u * (g.W + 1);
 	} else {
 		if (nets_.size() != 1) return "the persistent GR pass runs one network";

@@ -179,7 +179,7 @@ public:
 	uint32_t passRows() const { return 2 * h_.K; }
 	// Encode the TMA descriptors for boxes of R rows and upload them.
 	std::string buildPassMaps(uint32_t R);
-	size_t passTmaSmemBytes(uint32_t R, uint32_t S) const;
+	size_t passTmaSmemBytes(uint32_t R, uint32_t S, uint32_t outBytes = 4) const;
 	size_t zoneScratchBytes() const;
 	// shared memory a small-cell CTA may use (the staged arrays included)
 	static constexpr size_t kTailSmemBudget = 200 * 1024;
@@ -208,6 +208,7 @@ private:
 	std::vector<void *> allocs_;
 	std::map<const void *, size_t> allocBytes_;
 	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;
+	uint32_t outBytes_ = 4;  // bytes per GR->GO slot the GR pass in use streams
 	// pinned staging of host MF input: kMFStage slots, each reused once the
 	// copy that last read it has run (mfStageEv_)
 	uint32_t *hErr_ = nullptr;  // the error word (mapped pinned host memory; h_.errFlag maps it)
