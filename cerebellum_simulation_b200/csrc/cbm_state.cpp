@@ -580,7 +580,7 @@ std::string State::create(const std::string &conText, const std::string &actText
 			pcsc[(size_t)pc * cp.numpPCfromSCtoPC + i % cp.numpPCfromSCtoPC] = i;
 		}
 		// connectPCtoNC: the regular block, then the random extra synapses
-		// (the reference draws them with SFMT IRandomX; this build draws them
+		// (the reference draws them with SFMT IRandomX; this library draws them
 		// from its counter-based stream keyed by the zone's seed)
 		uint32_t *ncpc = find("pNCfromPCtoNC", z)->as<uint32_t>();
 		uint32_t *pcnc = find("pPCfromPCtoNC", z)->as<uint32_t>();

@@ -6,7 +6,7 @@ plain way simulates every candidate.  Here the batched simulator
 surrogate MLP (:mod:`.surrogate`, tensor-core kernels) learns the trial's
 50-bin NC rate trace from a 64-value description of the parameters and the
 MF input, ranks all candidates, and only the best ones are simulated in full;
-the simulator stays the judge of the surrogate's error.
+the simulator stays the arbiter of the surrogate's error.
 
 Parameters of a set (each drawn uniformly, scales log-uniformly):
   GO threshold scale 0.8-1.2, PF->PC LTD and LTP step scales 0.5-2,

@@ -158,6 +158,33 @@ def test_graph_run_equals_step_calls(tmp_path):
     assert open(fa, "rb").read() == open(fb, "rb").read()
 
 
+def test_flushed_runs_equal_graph_runs(tmp_path):
+    """The measurement paths (each step alone after an L2 flush, and the
+    same with the two kernels on separate streams) advance the network
+    exactly as graph-chunk replays do."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    net = networks.config1_network(seed=2)
+    p = str(tmp_path / "c1.state")
+    net.writeState(p)
+    mf = networks.uniform_mf_stream(1024, 240, seed=6)
+    a = cbm.CBMSimCore(cbm.CBMState(p), [5], device=0, resident_steps=240)
+    a.load_mf_stream(cbm.mf_bits(mf, a.mf_words()))
+    a.run(240, chunk=40)
+    fa = str(tmp_path / "a.state")
+    a.writeToState(fa)
+    b = cbm.CBMSimCore(cbm.CBMState(p), [5], device=0, resident_steps=240)
+    b.load_mf_stream(cbm.mf_bits(mf, b.mf_words()))
+    assert b.run_flushed(80, 1 << 20) > 0
+    pass_ms, tail_ms = b.run_flushed_kernels(80, 1 << 20)
+    assert pass_ms > 0 and tail_ms > 0
+    b.run(80, chunk=40)
+    assert b.steps_done() == 240
+    fb = str(tmp_path / "b.state")
+    b.writeToState(fb)
+    assert open(fa, "rb").read() == open(fb, "rb").read()
+
+
 def test_device_expf_matches_host_expf():
     """The small-cell updates' float exponential equals the host C library's
     expf (the reference's exp(float)) on every probed input."""
