@@ -937,6 +937,7 @@ std::string Network::resetGOGODepression(cudaStream_t s)
 Simulator::~Simulator()
 {
 	dropGraphs();
+	if (stepDoneEv_) cudaEventDestroy(stepDoneEv_);
 	if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
 	if (hExport_) cudaFreeHost(hExport_);
 	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
@@ -1222,6 +1223,8 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 			cudaEventRecordWithFlags(n.mfStageEv_[mfSlot], s0_, cudaEventRecordExternal);
 		}
 		std::string e = enqueueStep(0, false);
+		// both kernels done: exports wait for this, not for the counter update
+		cudaEventRecordWithFlags(stepDoneEv_, s0_, cudaEventRecordExternal);
 		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
 		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
 		if (!e.empty()) return e;
@@ -1230,6 +1233,7 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 		cudaGraphDestroy(g);
 		return "";
 	};
+	if (!stepDoneEv_) CK(cudaEventCreateWithFlags(&stepDoneEv_, cudaEventDisableTiming), "event");
 	for (uint32_t k = 0; k < nsteps; k++) {
 		if (pendingMF_ >= 0) {
 			const int slot = pendingMF_;
@@ -1242,6 +1246,8 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 		}
 	}
 	for (Network *n : nets_) n->hostT_ += nsteps;
+	lastWasStepGraph_ = nsteps > 0;
+	directCopySinceStep_ = false;
 	return "";
 }
 
@@ -1251,6 +1257,7 @@ std::string Simulator::flushPendingMF()
 	Network &n = *nets_[0];
 	const int k = pendingMF_;
 	pendingMF_ = -1;
+	directCopySinceStep_ = true;
 	CK(cudaMemcpyAsync((void *)n.h_.mfBits, n.hPinnedBits_ + (size_t)k * n.h_.mfWords, 4ull * n.h_.mfWords,
 			cudaMemcpyHostToDevice, s0_), "MF upload");
 	CK(cudaEventRecord(n.mfStageEv_[k], s0_), "MF staging");
@@ -1270,6 +1277,7 @@ void Simulator::dropGraphs()
 std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	lastWasStepGraph_ = false;
 	pendingMF_ = -1;  // the protocol drives the MF input from now on
 	CKS(uploadCtl());
 	CK(cudaStreamSynchronize(s0_), "sync");
@@ -1315,6 +1323,7 @@ std::string Simulator::stageMF(size_t i, const uint8_t *mf)
 		return "";
 	}
 	pendingMF_ = -1;  // this input supersedes a deferred one
+	directCopySinceStep_ = true;
 	const uint64_t slot = n.hostT_ % n.h_.mfRing;
 	CK(cudaMemcpyAsync((void *)(n.h_.mfBits + slot * W), bits, 4ull * W, cudaMemcpyHostToDevice, s0_), "MF upload");
 	if (raw || n.h_.hasMFRaw) {
@@ -1344,9 +1353,20 @@ std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, 
 		CK(cudaMallocHost((void **)&hExport_, bytes), "pinned allocation");
 		hExportBytes_ = bytes;
 	}
-	CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s0_));
-	CK(cudaStreamSynchronize(s0_), "export");
-	markInputSlotsFree();
+	if (lastWasStepGraph_) {
+		// after a single-step graph: copy on the second stream as soon as
+		// both kernels are done, beside the step-counter update
+		CK(cudaStreamWaitEvent(s1_, stepDoneEv_, 0), "export");
+		CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s1_));
+		CK(cudaStreamSynchronize(s1_), "export");
+		// every staging slot a launched graph read has been copied (unless
+		// an input copy was issued outside the graphs since)
+		if (!directCopySinceStep_) markInputSlotsFree();
+	} else {
+		CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s0_));
+		CK(cudaStreamSynchronize(s0_), "export");
+		markInputSlotsFree();
+	}
 	CKS(checkDeviceErrors());
 	memcpy(dst, hExport_, bytes);
 	return "";
@@ -1355,6 +1375,7 @@ std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, 
 std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	lastWasStepGraph_ = false;
 	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (chunk == 0) chunk = 1;
@@ -1413,6 +1434,7 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	lastWasStepGraph_ = false;
 	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (flushBytes && flushBytes != flushBuf_.bytes) {
@@ -1459,6 +1481,7 @@ std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *ste
 std::string Simulator::runFlushedKernels(uint64_t nsteps, size_t flushBytes, float *passMs, float *tailMs)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
+	lastWasStepGraph_ = false;
 	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (flushBytes && flushBytes != flushBuf_.bytes) {

@@ -114,6 +114,11 @@ private:
 	// (stepGraphMF_[k]) copies them in before the kernels.
 	int pendingMF_ = -1;
 	cudaGraphExec_t stepGraphMF_[kMFStage] = {};
+	// the last launch was a single-step graph: exports wait on stepDoneEv_
+	// (recorded in that graph once both kernels finish) on the second stream
+	cudaEvent_t stepDoneEv_ = nullptr;
+	bool lastWasStepGraph_ = false;
+	bool directCopySinceStep_ = false;  // an MF copy issued outside the step graphs since the last one
 	uint8_t *hExport_ = nullptr;           // pinned export staging
 	size_t hExportBytes_ = 0;
 	std::vector<Network *> nets_;
