@@ -40,6 +40,9 @@ enum PassMap : int {
 // 2047 GO; kOut16None marks an empty slot.
 constexpr uint16_t kOut16None = 0xFFFFu;
 constexpr uint32_t kOut16MaxGO = 2047u;
+// GR->GO slot planes the per-tile pass streams when some GR has more synapses
+// (the rest go to per-tile lists).
+constexpr uint32_t kOutInline = 4u;
 
 // A device array that a small-cell CTA copies into shared memory for the
 // step (and back when it changes): the CTA then runs on a shared-memory copy
@@ -158,6 +161,7 @@ struct DevNet {
 	uint32_t P, bs, K, J, tilesPerPC;     // PF->PC reduction geometry (kernels.cu:435-470)
 	uint32_t bcShift, scShift, bcLocal, scLocal;
 	uint32_t nMFSlots, nGOSlots, nOutSlots;
+	uint32_t nOutTma;                     // GR->GO slot planes the per-tile TMA pass streams (the rest: ovStart)
 	uint32_t mfWords, goWords;            // spike-bit vectors incl. the always-zero sentinel
 	uint32_t maxnumpMFfromMFtoGO, maxnumpGOCoupInGOGO;
 	uint32_t numpPCfromSCtoPC, numpNCfromPCtoNC, numpNCfromMFtoNC, numpIOfromNCtoIO, numpIOInIOIO;
@@ -196,6 +200,11 @@ struct DevNet {
 	const uint16_t *goIdx;    // [nGOSlots][numGR], sentinel numGO
 	const uint32_t *outCon;   // [nOutSlots][numGR]: (GO << 8) | delay bit, kNoDelay when empty
 	const uint16_t *outCon16; // the same as 16-bit entries (kOut16None when empty), or null (> 2047 GO)
+	// GR->GO synapses in slots >= nOutTma, per TMA-pass tile (null when none):
+	// tile b's are ovEntry[ovStart[b] .. ovStart[b+1]), x = tile-local cell
+	// (row * 32 + lane) | delay bit << 24, y = GO
+	const uint32_t *ovStart;
+	const uint2 *ovEntry;
 	const uint8_t *pfDelay;   // delay bit of the PF->BC/SC/PC output, kNoDelay when none
 
 	// ---- GO / MF / SC state (innetactivitystate.h)

@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	const uint32_t j0 = (local % N->tilesPerPC) * 32u;
 	const uint32_t rows = 2 * K, nStages = rows / R;
 	const uint32_t nMFSlots = Sh::mf ? Sh::mf : N->nMFSlots, nGOSlots = Sh::go ? Sh::go : N->nGOSlots,
-		nOutSlots = Sh::out ? Sh::out : N->nOutSlots;
+		nOutSlots = Sh::out ? Sh::out : N->nOutTma;
 	const PassLayout L = passLayout(R, nMFSlots, nGOSlots, nOutSlots, Z, Sh::out16 ? 2u : 4u);
 
 	extern __shared__ uint8_t passSmemRaw[];
@@ -592,6 +592,19 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 		}
 	}
 	__syncthreads();
+
+	// GR->GO synapses past the streamed slot planes: their cells' new spike
+	// buffers were written by this CTA before the barrier
+	if (!Sh::out && N->ovStart) {
+		const uint32_t e1 = N->ovStart[local + 1];
+		uint32_t *goCountOv = N->goCount + (size_t)(t & 1) * N->numGO;
+		for (uint32_t e = N->ovStart[local] + threadIdx.x; e < e1; e += blockDim.x) {
+			const uint2 en = N->ovEntry[e];
+			const uint32_t cl = en.x & 0xFFFFFFu, dl = en.x >> 24;
+			const uint32_t g = pc * P + (cl >> 5) * bs + j0 + (cl & 31u);
+			if ((N->apBufGR[g] >> dl) & 1u) atomicAdd(&goCountOv[en.y], 1u);
+		}
+	}
 
 	// the BC and SC counts of the tile (the producer wrote the PF->PC partials)
 	const uint32_t buf = (uint32_t)(t % 3);

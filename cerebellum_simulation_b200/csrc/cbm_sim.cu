@@ -79,7 +79,7 @@ size_t Network::passSmemBytes() const
 
 size_t Network::passTmaSmemBytes(uint32_t R, uint32_t S, uint32_t outBytes) const
 {
-	const PassLayout L = passLayout(R, h_.nMFSlots, h_.nGOSlots, h_.nOutSlots, h_.numZones, outBytes);
+	const PassLayout L = passLayout(R, h_.nMFSlots, h_.nGOSlots, h_.nOutTma, h_.numZones, outBytes);
 	return 128 + (size_t)S * L.bytes + 16ull * S + sizeof(uint32_t) * (((size_t)h_.bcLocal + h_.scLocal + 3) & ~(size_t)3) +
 		sizeof(float) * (size_t)h_.numZones * 2 * h_.K * 32 + 32ull * (h_.mfWords + h_.goWords);
 }
@@ -121,10 +121,11 @@ std::string Network::buildPassMaps(uint32_t R)
 			return "encoding a TMA descriptor failed";
 		return "";
 	};
-	auto enc3 = [&](int m, const void *ptr, CUtensorMapDataType dt, uint32_t es, uint32_t slots) -> std::string {
+	auto enc3 = [&](int m, const void *ptr, CUtensorMapDataType dt, uint32_t es, uint32_t slots,
+			uint32_t boxSlots) -> std::string {
 		const cuuint64_t dims[3] = {bs, N / bs, slots};
 		const cuuint64_t strides[2] = {(cuuint64_t)bs * es, (cuuint64_t)N * es};
-		const cuuint32_t box[3] = {32, R, slots};
+		const cuuint32_t box[3] = {32, R, boxSlots};
 		const cuuint32_t estr[3] = {1, 1, 1};
 		if (enc(&maps[m], dt, 3, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
 				CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
@@ -138,11 +139,13 @@ std::string Network::buildPassMaps(uint32_t R)
 	CKS(enc2(PM_GESUM, h_.gESum, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
 	CKS(enc2(PM_GISUM, h_.gISum, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
 	CKS(enc2(PM_APBUF, h_.apBufGR, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4));
-	CKS(enc3(PM_MFIDX, h_.mfIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nMFSlots)));
-	CKS(enc3(PM_GOIDX, h_.goIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nGOSlots)));
-	CKS(enc3(PM_OUTCON, h_.outCon, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, std::max(1u, h_.nOutSlots)));
+	const uint32_t mfS = std::max(1u, h_.nMFSlots), goS = std::max(1u, h_.nGOSlots), outS = std::max(1u, h_.nOutSlots);
+	const uint32_t outT = std::max(1u, h_.nOutTma);
+	CKS(enc3(PM_MFIDX, h_.mfIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, mfS, mfS));
+	CKS(enc3(PM_GOIDX, h_.goIdx, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, goS, goS));
+	CKS(enc3(PM_OUTCON, h_.outCon, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, outS, outT));
 	if (h_.outCon16)
-		CKS(enc3(PM_OUTCON16, h_.outCon16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, std::max(1u, h_.nOutSlots)));
+		CKS(enc3(PM_OUTCON16, h_.outCon16, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, outS, outT));
 	CKS(enc2(PM_PFDELAY, h_.pfDelay, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1));
 	CKS(enc2(PM_HIST, h_.historyGR, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8));
 	for (uint32_t z = 0; z < h_.numZones; z++) CKS(enc2(PM_W0 + z, h_.zones[z].w, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4));
@@ -286,7 +289,8 @@ double Network::bytesPerStepLayout() const
 	// GR state read and written (6 x 4 B each way), synapse slots (u16 MF and
 	// GO indices, u32 GR->GO targets), the PF delay byte, the PF->PC weight
 	// of every zone; history read + write and weight writes on plasticity steps
-	const double perGR = 48.0 + 2.0 * h_.nMFSlots + 2.0 * h_.nGOSlots + (double)outBytes_ * h_.nOutSlots + 1.0 + 4.0 * h_.numZones +
+	const double perGR = 48.0 + 2.0 * h_.nMFSlots + 2.0 * h_.nGOSlots + (double)outBytes_ * outPlanes_ +
+		12.0 * ovUsed_ / h_.numGR + 1.0 + 4.0 * h_.numZones +
 		(16.0 + 4.0 * h_.numZones) / h_.tsPerHistBinGR;
 	return perGR * h_.numGR;
 }
@@ -416,6 +420,36 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	h.mfIdx = upload(mfIdx.data(), mfIdx.size());
 	h.goIdx = upload(goIdx.data(), goIdx.size());
 	h.outCon = upload(outCon.data(), outCon.size());
+	// Networks with more than 4 GR->GO synapses on some GR (a fan-out padded
+	// to its maximum): the per-tile TMA pass streams the first 4 slot planes
+	// and takes the rest from per-tile lists after its rows
+	h.nOutTma = nOut;
+	h.ovStart = nullptr;
+	h.ovEntry = nullptr;
+	if (nOut > kOutInline && h.J == 32) {
+		const uint32_t tiles = c.numPC * h.tilesPerPC;
+		std::vector<std::vector<uint2>> per(tiles);
+		for (uint32_t g = 0; g < N; g++)
+			for (int k = (int)kOutInline; k < numOut[g]; k++) {
+				const uint32_t cv = outCon[(size_t)k * N + g];
+				if ((cv & 0xFFu) >= 32u) continue;  // a synapse without a delay bit never fires
+				const uint32_t off = g % P, r = off / h.bs, jf = off % h.bs;
+				const uint32_t tile = (g / P) * h.tilesPerPC + jf / 32;
+				per[tile].push_back(make_uint2((r * 32 + jf % 32) | ((cv & 0xFFu) << 24), cv >> 8));
+			}
+		std::vector<uint32_t> start(tiles + 1, 0);
+		std::vector<uint2> ent;
+		for (uint32_t b = 0; b < tiles; b++) {
+			start[b] = (uint32_t)ent.size();
+			ent.insert(ent.end(), per[b].begin(), per[b].end());
+		}
+		start[tiles] = (uint32_t)ent.size();
+		if (ent.empty()) ent.push_back(make_uint2(0, 0));  // never read: every range is empty
+		h.nOutTma = kOutInline;
+		h.ovStart = upload(start.data(), start.size());
+		h.ovEntry = upload(ent.data(), ent.size());
+		ovEntries_ = start[tiles];
+	}
 	h.outCon16 = nullptr;
 	if (c.numGO <= kOut16MaxGO) {
 		// the 16-bit copy the shape-specialised GR pass streams
@@ -1031,7 +1065,7 @@ std::vector<PassGeometry> Simulator::passCandidates() const
 	for (Network *n : nets_) {
 		tma = tma && n->passTmaCapable();
 		minRows = std::min(minRows, n->passRows());
-		maxSlots = std::max({maxSlots, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutSlots});
+		maxSlots = std::max({maxSlots, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutTma});
 	}
 	if (tma) {
 		PassGeometry d;
@@ -1059,12 +1093,14 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 	CK(cudaSetDevice(device_), "selecting the device");
 	uint32_t minRows = UINT32_MAX, maxSlots = 0;
 	bool capable = !nets_.empty();
+	uint32_t maxSlotsTile = 0;  // the per-tile pass streams nOutTma GR->GO planes
 	for (Network *n : nets_) {
 		capable = capable && n->passTmaCapable();
 		minRows = std::min(minRows, n->passRows());
 		maxSlots = std::max({maxSlots, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutSlots});
+		maxSlotsTile = std::max({maxSlotsTile, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutTma});
 	}
-	for (Network *n : nets_) n->outBytes_ = 4;
+	for (Network *n : nets_) { n->outBytes_ = 4; n->outPlanes_ = n->dev().nOutSlots; n->ovUsed_ = 0; }
 	if (g.kind == 0) {
 		passTmaFn_ = nullptr;
 		passPersistent_ = false;
@@ -1074,7 +1110,8 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 		return "";
 	}
 	if (!capable) return "the TMA GR pass needs tiles of 32-cell rows in every network";
-	if (g.M > 0 && maxSlots > (uint32_t)g.M) return "a network has more synapse slots than the geometry's slot bound";
+	if (g.M > 0 && (g.kind == 1 ? maxSlotsTile : maxSlots) > (uint32_t)g.M)
+		return "a network has more synapse slots than the geometry's slot bound";
 	const void *fn = nullptr;
 	uint32_t R = 0, threads = 0, grid = passBlocks_;
 	size_t smem = 0;
@@ -1090,10 +1127,15 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 		R = (uint32_t)(g.W * g.RW);
 		if (R > minRows) return "more rows per stage than a tile has";
 		for (Network *n : nets_) smem = std::max(smem, n->passTmaSmemBytes(R, (uint32_t)g.S, shape == 1 ? 2u : 4u));
-		for (Network *n : nets_) n->outBytes_ = shape == 1 ? 2u : 4u;
+		for (Network *n : nets_) {
+			n->outBytes_ = shape == 1 ? 2u : 4u;
+			n->outPlanes_ = n->dev().nOutTma;
+			n->ovUsed_ = n->ovEntries_;
+		}
 		threads = 32u * (g.W + 1);
 	} else {
 		if (nets_.size() != 1) return "the persistent GR pass runs one network";
+		if (nets_[0]->dev().ovStart) return "the persistent GR pass streams every GR->GO slot; this network has per-tile lists";
 		fn = passPersistentKernelFor(g.W, g.S, g.B, g.M);
 		if (!fn) return "persistent GR-pass geometry not compiled in";
 		R = (uint32_t)(2 * g.W);

@@ -214,6 +214,9 @@ private:
 	std::map<const void *, size_t> allocBytes_;
 	double avgMF_ = 0, avgGO_ = 0, avgOut_ = 0;
 	uint32_t outBytes_ = 4;  // bytes per GR->GO slot the GR pass in use streams
+	uint32_t outPlanes_ = 0; // GR->GO slot planes it streams
+	size_t ovEntries_ = 0;   // GR->GO synapses in the per-tile lists
+	size_t ovUsed_ = 0;      // those the GR pass in use reads (0 unless the per-tile pass)
 	// pinned staging of host MF input: kMFStage slots, each reused once the
 	// copy that last read it has run (mfStageEv_)
 	uint32_t *hErr_ = nullptr;  // the error word (mapped pinned host memory; h_.errFlag maps it)
