@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--trials", type=int, default=10)
     ap.add_argument("--candidates", type=int, default=4096)
     ap.add_argument("--simulate-top", type=int, default=256)
+    ap.add_argument("--no-truth", action="store_true",
+                    help="surrogate workload: skip simulating every candidate (the plain sweep's answer)")
     ap.add_argument("--instances", type=int, default=64)
     return ap.parse_args()
 
@@ -351,6 +353,11 @@ def main_surrogate(args):
         sim_top, gpu_top = sweep.simulate(base, p_c[top], s_c[top], T, device=device)
         wall_top = time.time() - t0
         sim_rnd, _ = sweep.simulate(base, p_c[rnd], s_c[rnd], T, device=device)
+        # the plain sweep's answer: every candidate simulated (batched), to
+        # judge what the surrogate's ranking loses
+        sim_all = gpu_all = None
+        if not args.no_truth:
+            sim_all, gpu_all = sweep.simulate(base, p_c, s_c, T, device=device)
         # the plain alternative: one candidate at a time through the single-network simulator
         one = cbm.CBMSimCore(cbm.CBMState(base), [11], device=device)
         proto = cbm.eyelid_protocol_defaults(st, mfSeed=1, numDataTrials=1, dataStartTrial=0, **sweep.TRIAL)
@@ -385,6 +392,23 @@ def main_surrogate(args):
                       "objective_random_mean": float(sweep.objective(sim_rnd[:, T - 1]).mean())},
         "batched_top_gpu_s": gpu_top, "batched_top_wall_s": wall_top,
     }
+    if sim_all is not None:
+        # the sweep delivers simulated traces of its picks (the same simulator,
+        # so they equal the plain sweep's); the surrogate only chooses them
+        tr_all = sim_all[:, T - 1]
+        obj_all = sweep.objective(tr_all)
+        true_top = set(np.argsort(-obj_all)[:K].tolist())
+        err_all = pred - tr_all
+        rmse_all = float(np.sqrt(np.mean(err_all ** 2)))
+        span = float(tr_all.max() - tr_all.min())
+        out["versus_every_candidate"] = {
+            "simulated_gpu_s": gpu_all,
+            "recall_of_true_top_k": len(true_top & set(top.tolist())) / K,
+            "best_objective_all": float(obj_all.max()), "best_objective_picked": float(obj_all[top].max()),
+            "best_objective_gap_over_trace_range": float(obj_all.max() - obj_all[top].max()) / max(span, 1e-9),
+            "surrogate_nc_trace_rmse_hz": rmse_all, "nc_trace_range_hz": span,
+            "surrogate_nc_trace_rmse_over_range": rmse_all / max(span, 1e-9),
+            "delivered_trace_error": 0.0}
     print(json.dumps(out))
 
 
