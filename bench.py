@@ -392,6 +392,15 @@ def main_surrogate(args):
                       "objective_random_mean": float(sweep.objective(sim_rnd[:, T - 1]).mean())},
         "batched_top_gpu_s": gpu_top, "batched_top_wall_s": wall_top,
     }
+    # tensor-core throughput of the surrogate: algorithmic FLOPs of the
+    # unpadded layers (a multiply-add is 2), training counted as 3 forward
+    # passes, over the wall-clock of the library calls (host copies included)
+    n_in, h1, h2, n_out = sweep.N_FEATURES, 256, 256, sweep.N_TRACE
+    fwd = 2.0 * (n_in * h1 + h1 * h2 + h2 * n_out)
+    out["mlp"] = {"forward_flop_per_sample": fwd,
+                  "train_tflops": 3.0 * fwd * len(y) * 100 / train_s / 1e12,
+                  "inference_tflops": fwd * len(p_c) / infer_s / 1e12,
+                  "bound": "latency (batches of 256 rows; 0.2 M parameters)"}
     if sim_all is not None:
         # the sweep delivers simulated traces of its picks (the same simulator,
         # so they equal the plain sweep's); the surrogate only chooses them
