@@ -198,10 +198,23 @@ def cpu_reference(state_path, mf, steps, threads, warmup=0):
                              capture_output=True, text=True, env=env, check=True).stdout
     line = [l for l in out.splitlines() if l.startswith("{")][-1]
     r = json.loads(line)
-    return {"value": r["steps_per_s"], "unit": "steps/s", "cores": threads, "kind": "reference",
-            "sample": f"{steps} steps of the same 1M-GR network and MF input (ms {warmup}-{warmup + steps} of "
-                      f"trial 1, after {warmup} untimed steps), reference host code + CPU kernel restatement, "
-                      f"OpenMP {threads} threads"}
+    res = {"value": r["steps_per_s"], "unit": "steps/s", "cores": threads, "kind": "reference",
+           "sample": f"{steps} steps of the same 1M-GR network and MF input (ms {warmup}-{warmup + steps} of "
+                     f"trial 1, after {warmup} untimed steps), reference host code + CPU kernel restatement, "
+                     f"OpenMP {threads} threads"}
+    # the reference as it builds by default: no OpenMP, one core (a shorter sample)
+    one = os.path.join(ROOT, "oracle", "_ref", "ref_run")
+    if threads > 1 and os.path.exists(one):
+        n1 = max(1, min(steps, 10))
+        with tempfile.TemporaryDirectory() as d:
+            mfp = os.path.join(d, "mf.u8")
+            np.ascontiguousarray(mf[:warmup + n1], dtype=np.uint8).tofile(mfp)
+            out = subprocess.run([one, state_path, mfp, str(warmup + n1), "-", "-", "7", "-t", "-w", str(warmup)],
+                                 capture_output=True, text=True, check=True).stdout
+        r1 = json.loads([l for l in out.splitlines() if l.startswith("{")][-1])
+        res["single_core"] = {"value": r1["steps_per_s"], "unit": "steps/s", "cores": 1,
+                              "sample": f"{n1} steps after the same {warmup} untimed steps, no OpenMP"}
+    return res
 
 
 WORKLOAD = ("1M-GR eyelid network: 1,048,576 GR (4 MF + 3 GO inputs, 4 GO targets each), 1024 GO, 1024 MF, "
