@@ -1,0 +1,66 @@
+"""Host-side inputs and the benchmark's reference arm, without a GPU.
+
+* The state-variable MF coding of the dense configuration: each variable's
+  fibres blend their relaxed and excited rates by a Gaussian of the distance
+  between the variable's value and the fibre's preferred value
+  (StateVariable::gaussMFAct, Matthew_Sim_CBM/includes/statevariable.hpp:108-129).
+* The regenerating Poisson fibres are a deterministic function of the seed.
+* `bench.py --impl reference` prints one JSON line that carries the fields
+  the benchmark contract asks for (or its `unavailable` line).
+"""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+from cerebellum_simulation_b200 import networks
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_state_variable_rates_follow_the_gaussian_tuning():
+    c = networks.StateVariableMF(1024, seed=4)
+    per = 1024 // 4
+    for t in (1, 250, 777):
+        r = c.rates(t)
+        x = c.values(t)
+        assert np.all(r >= c.relaxed - 1e-5) and np.all(r <= 40.0 + 1e-4)
+        for v in range(4):
+            share = slice(v * per, (v + 1) * per)
+            a = (r[share] - c.relaxed[share]) / (c.excited[share] - c.relaxed[share])
+            # the blend weight falls with the distance to the preferred value
+            d = np.abs(c.mean[share] - x[v])
+            order = np.argsort(d)
+            assert np.all(np.diff(a[order]) <= 1e-5)
+            want = np.exp(-(d * d) / (2 * c.variance * c.variance))
+            assert np.allclose(a, want, atol=1e-5)
+
+
+def test_config3_stream_is_deterministic():
+    a = networks.config3_mf_stream(1024, 300, seed=2)
+    b = networks.config3_mf_stream(1024, 300, seed=2)
+    c = networks.config3_mf_stream(1024, 300, seed=3)
+    assert a.dtype == np.uint8 and a.shape == (300, 1024)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    rate_hz = a.mean() * 1000.0
+    assert 2.0 < rate_hz < 40.0
+
+
+def test_reference_arm_prints_one_contract_line():
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "3",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    if "unavailable" in d:
+        return
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "config",
+              "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["value"] > 0 and d["warmup"] == 3
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
