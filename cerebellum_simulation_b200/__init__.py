@@ -106,6 +106,7 @@ def _load():
         "cbm_batch_num_gr": (U64, [P]),
         "cbm_sim_trial_record_bytes": (U64, [P, I]),
         "cbm_sim_trial_record": (I, [P, I, P, U64]),
+        "cbm_sim_record_gr": (I, [P]),
         "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_destroy": (None, [P]),
         "cbm_device_expf": (I, [I, P, P, U64]),
@@ -353,13 +354,23 @@ class CBMSimCore:
         _check(lib.cbm_sim_set_eyelid_protocol(self._h, ctypes.byref(p)))
         self._protocol = protocol
 
+    def record_gr(self):
+        """Record the running protocol's GR peri-stimulus histogram on the
+        device from the next step on (cbm_sim_record_gr)."""
+        _check(lib.cbm_sim_record_gr(self._h))
+
     def trial_record(self, kind):
         """Records of the running protocol: 'nc' / 'pc' spike counts
-        [trials, bins, cells] (u32) or 'eyelid' [trials, window steps] (f32)."""
-        k = {"nc": 0, "pc": 1, "eyelid": 2}[kind]
+        [trials, bins, cells] (u32), 'eyelid' [trials, window steps] (f32), or
+        'gr' [bins, numGR] (u16, the kept trials summed; after record_gr)."""
+        k = {"nc": 0, "pc": 1, "eyelid": 2, "gr": 3}[kind]
         n = lib.cbm_sim_trial_record_bytes(self._h, k)
         if not n:
-            raise CBMError(1, "no protocol is running")
+            raise CBMError(1, "no protocol is running" if kind != "gr" else "the GR histogram is not recorded")
+        if kind == "gr":
+            out = np.empty(n // 2, dtype=np.uint16)
+            _check(lib.cbm_sim_trial_record(self._h, k, out.ctypes.data, n))
+            return out.reshape(-1, self.state.con("numGR"))
         out = np.empty(n // 4, dtype=np.float32 if kind == "eyelid" else np.uint32)
         _check(lib.cbm_sim_trial_record(self._h, k, out.ctypes.data, n))
         p = self._protocol

@@ -350,6 +350,13 @@ int cbm_sim_trial_record(cbm_sim *sim, int kind, void *dst, uint64_t bytes)
 	return CBM_OK;
 }
 
+int cbm_sim_record_gr(cbm_sim *sim)
+{
+	NEED(sim);
+	TRY(sim->sim.recordGR());
+	return CBM_OK;
+}
+
 // ---------------------------------------------------------------- batches
 struct cbm_batch {
 	Simulator sim;

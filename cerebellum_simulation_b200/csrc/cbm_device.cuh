@@ -126,6 +126,7 @@ struct DevProtocol {
 	float *eyelid;         // [numDataTrials][recLen] integrator output per step
 	float *eyeG;           // [numNC] integrator conductances
 	float *eyeVm;          // [1]
+	uint16_t *grPSH;       // [nBins][numGR] GR spike counts of the kept trials, or null
 	float eyeGDecay, eyeGInc, eyeGShift, eyeGLeak, eyeMaxAmp;
 };
 

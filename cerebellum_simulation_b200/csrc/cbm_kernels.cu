@@ -1705,6 +1705,37 @@ __device__ void protocolRecord(const DevNet *__restrict__ N, uint64_t t)
 	}
 }
 
+// GR peri-stimulus histogram of step t (ECTrialsData::updatePSH("gr") of the
+// eyelid driver, ecmanagementdelay.cpp:259-262; PeriStimHistFloat::update,
+// peristimhistfloat.cpp): inside the recording window of a kept trial, the
+// GR's spike of step t (bit 0 of its spike buffer, written by the step's GR
+// pass) adds one to its count in the step's bin.  The kept trials add into
+// one histogram, as the reference's does.  Counts stay below 65536 (the host
+// checks binSteps x numDataTrials), so two u16 counts share a word safely.
+__global__ void grPSHKernel(const DevNet *N, uint32_t stepOffset)
+{
+	const DevProtocol *P = N->proto;
+	const uint64_t t = stepsDone(N) + 1 + stepOffset;
+	if (!P || !P->grPSH || t < P->startT + 1) return;
+	const uint64_t k = t - 1 - P->startT;
+	const int32_t time = (int32_t)(k % P->trialSteps);
+	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const int32_t ct = time - P->recFrom;
+	if (trial < P->dataStartTrial || trial >= P->dataStartTrial + P->numDataTrials || ct < 0 || ct >= P->recLen)
+		return;
+	const uint32_t i = 8u * (blockIdx.x * blockDim.x + threadIdx.x);
+	if (i >= N->numGR) return;
+	uint16_t *cnt = P->grPSH + (size_t)((uint32_t)ct / P->binSteps) * N->numGR + i;
+	const uint4 a = *reinterpret_cast<const uint4 *>(N->apBufGR + i);
+	const uint4 b = *reinterpret_cast<const uint4 *>(N->apBufGR + i + 4);
+	uint4 c = *reinterpret_cast<const uint4 *>(cnt);
+	c.x += (a.x & 1u) | ((a.y & 1u) << 16);
+	c.y += (a.z & 1u) | ((a.w & 1u) << 16);
+	c.z += (b.x & 1u) | ((b.y & 1u) << 16);
+	c.w += (b.z & 1u) | ((b.w & 1u) << 16);
+	*reinterpret_cast<uint4 *>(cnt) = c;
+}
+
 // Prepare the first step of a newly set protocol (the network's step tBase + 1).
 __global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet *N)
 {

@@ -32,6 +32,9 @@ const void *passPersistentKernelFor(int W, int S, int B, int M);
 __global__ void tailKernel(const DevNet *const *nets, const uint32_t *stageBytes, uint32_t stepOffset,
 		const DevNet *net0, uint32_t stage0);
 __global__ void protocolPrimeKernel(const DevNet *N);
+// GR peri-stimulus histogram of step t = stepsDone(N) + 1 + stepOffset, after
+// the GR pass of that step: 8 GR per thread.
+__global__ void grPSHKernel(const DevNet *N, uint32_t stepOffset);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);
 __global__ void expfProbeKernel(const float *in, float *out, uint32_t n);

@@ -767,8 +767,23 @@ size_t Network::recordBytes(int kind) const
 	case CBM_REC_NC_PSH: return 4 * nd * hProto_.nBins * h_.numNC;
 	case CBM_REC_PC_PSH: return 4 * nd * hProto_.nBins * h_.numPC;
 	case CBM_REC_EYELID: return 4 * nd * (size_t)hProto_.recLen;
+	case CBM_REC_GR_PSH: return hProto_.grPSH ? 2ull * hProto_.nBins * h_.numGR : 0;
 	default: return 0;
 	}
+}
+
+std::string Network::recordGR(cudaStream_t s)
+{
+	if (!h_.proto) return "the GR histogram records a running protocol: set one first";
+	if (hProto_.grPSH) return "";
+	if ((uint64_t)hProto_.binSteps * std::max<uint32_t>(1, hProto_.numDataTrials) > 65535)
+		return "GR histogram counts are 16-bit: binSteps x numDataTrials must be at most 65535";
+	uint16_t *c = alloc<uint16_t>((size_t)hProto_.nBins * h_.numGR);  // zeroed
+	if (!c) return "device allocation failed";
+	hProto_.grPSH = c;
+	CK(cudaMemcpyAsync(h_.proto, &hProto_, sizeof(DevProtocol), cudaMemcpyHostToDevice, s), "uploading the protocol");
+	CK(cudaStreamSynchronize(s), "uploading the protocol");
+	return "";
 }
 
 std::string Network::readRecord(int kind, void *dst, size_t bytes, cudaStream_t s)
@@ -778,7 +793,8 @@ std::string Network::readRecord(int kind, void *dst, size_t bytes, cudaStream_t 
 	if (!need) return "unknown record kind";
 	if (bytes != need) return "record size mismatch";
 	const void *src = kind == CBM_REC_NC_PSH ? (const void *)hProto_.ncPSH
-		: kind == CBM_REC_PC_PSH ? (const void *)hProto_.pcPSH : (const void *)hProto_.eyelid;
+		: kind == CBM_REC_PC_PSH ? (const void *)hProto_.pcPSH
+		: kind == CBM_REC_GR_PSH ? (const void *)hProto_.grPSH : (const void *)hProto_.eyelid;
 	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "reading a record");
 	CK(cudaStreamSynchronize(s), "reading a record");
 	return "";
@@ -1235,7 +1251,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
 		CK(cudaEventRecord(join_, s1_), "join");
 		CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
-		return "";
+		return recordStepGR(k);
 	}
 	// One stream: the small-cell CTAs launch first and let the GR pass start
 	// as soon as they are resident (programmatic dependent launch; the two
@@ -1246,6 +1262,16 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	CK(cudaEventRecord(join_, s0_), "join");
 	CKS(launchPass(s0_, true));
 	CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
+	return recordStepGR(k);
+}
+
+std::string Simulator::recordStepGR(uint32_t k)
+{
+	// after both kernels of the step: its GR spikes into the histogram
+	if (nets_.size() != 1 || !nets_[0]->recordsGR()) return "";
+	const uint32_t threads = (nets_[0]->dev().numGR + 7) / 8;
+	grPSHKernel<<<(threads + 255) / 256, 256, 0, s0_>>>(nets_[0]->devPtr(), k);
+	CK(cudaGetLastError(), "launching the GR histogram");
 	return "";
 }
 
@@ -1324,6 +1350,17 @@ std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
 	CKS(uploadCtl());
 	CK(cudaStreamSynchronize(s0_), "sync");
 	return nets_[i]->setProtocol(p, s0_);
+}
+
+std::string Simulator::recordGR()
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	if (nets_.size() != 1) return "the GR histogram is recorded for single-network simulators";
+	CK(cudaStreamSynchronize(s0_), "sync");
+	const bool was = nets_[0]->recordsGR();
+	CKS(nets_[0]->recordGR(s0_));
+	if (!was) dropGraphs();  // the step graphs gain the histogram kernel
+	return "";
 }
 
 std::string Simulator::stageMF(size_t i, const uint8_t *mf)

@@ -58,6 +58,8 @@ public:
 	std::string stageMF(size_t i, const uint8_t *mf);
 	// Start a device-driven trial protocol on network i from the next step.
 	std::string setProtocol(size_t i, const cbm_eyelid_protocol &p);
+	// Record network 0's GR peri-stimulus histogram (single-network simulators).
+	std::string recordGR();
 	// Run nsteps as CUDA-graph chunks of chunk steps (inputs resident in HBM).
 	// With instrument, external events around every GR pass of the chunk
 	// give lastPassMs(): the pass's mean duration over the last replay.
@@ -104,6 +106,7 @@ private:
 	friend class Network;
 	std::string uploadCtl();
 	std::string enqueueStep(uint32_t stepOffset, bool instrument);
+	std::string recordStepGR(uint32_t stepOffset);
 	void dropGraphs();
 	void markInputSlotsFree();  // after a full synchronisation
 	// Issue the copy of MF input that a single-step graph would have carried.
@@ -165,6 +168,9 @@ public:
 	std::string resetGOGODepression(cudaStream_t s);
 	// Device-driven trial protocol (cbm_eyelid_protocol) from the next step on.
 	std::string setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s);
+	// Allocate and start the protocol's GR peri-stimulus histogram.
+	std::string recordGR(cudaStream_t s);
+	bool recordsGR() const { return hProto_.grPSH != nullptr; }
 	bool hasProtocol() const { return h_.proto != nullptr; }
 	size_t recordBytes(int kind) const;
 	std::string readRecord(int kind, void *dst, size_t bytes, cudaStream_t s);

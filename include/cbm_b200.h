@@ -231,7 +231,8 @@ typedef struct cbm_eyelid_protocol {
 enum {
 	CBM_REC_NC_PSH = 0,  /* u32 [numDataTrials][bins][numNC] */
 	CBM_REC_PC_PSH = 1,  /* u32 [numDataTrials][bins][numPC] */
-	CBM_REC_EYELID = 2   /* f32 [numDataTrials][window steps] */
+	CBM_REC_EYELID = 2,  /* f32 [numDataTrials][window steps] */
+	CBM_REC_GR_PSH = 3   /* u16 [bins][numGR], summed over the kept trials (cbm_sim_record_gr) */
 };
 
 /* Start a device protocol on network 0 of the simulator (no counterpart in
@@ -241,6 +242,16 @@ int cbm_sim_set_eyelid_protocol(cbm_sim *sim, const cbm_eyelid_protocol *protoco
 uint64_t cbm_sim_trial_record_bytes(cbm_sim *sim, int kind);
 /* Copy a record of the running protocol to host memory. */
 int cbm_sim_trial_record(cbm_sim *sim, int kind, void *dst, uint64_t bytes);
+/* Record the running protocol's GR peri-stimulus histogram on the device from
+ * the next step on: in the recording window of every kept trial, each GR's
+ * spike adds to its count in the step's bin, all kept trials into one
+ * histogram.  Replaces the eyelid driver's per-step exportAPGR into
+ * ECTrialsData::updatePSH("gr") (Eyelid_Sim_CBM_Dev/src/ectrial/
+ * ecmanagementdelay.cpp:259-262, CBM_DATA_LIB_DEV/src/peristimhist/
+ * peristimhistfloat.cpp update), whose float counts these u16 counts equal.
+ * Needs a protocol, and binSteps x numDataTrials of at most 65535; the
+ * counts start at zero. */
+int cbm_sim_record_gr(cbm_sim *sim);
 
 /* ---- Batched instances (no counterpart in the reference, which runs one
  * network per CBMSimCore).  n independent networks of any sizes, seeds and

@@ -78,3 +78,42 @@ def test_protocol_graph_replay_bit_exact(tmp_path):
     assert compare_states(fin_o, fin_p) == []
     with pytest.raises(cbm.CBMError):
         sim.updateMFInput(np.zeros(st.con("numMF"), dtype=np.uint8))
+
+
+def test_gr_histogram_matches_oracle_spikes(tmp_path):
+    """The device GR peri-stimulus histogram (cbm_sim_record_gr) equals the
+    oracle's GR spikes counted over the recording windows of the kept trials,
+    both under graph replay and step by step."""
+    import cerebellum_simulation_b200 as cbm
+    st_path = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol(dataStartTrial=1, numDataTrials=2)
+    st = cbm.CBMState(st_path)
+    rates = cbmtest.protocol_rates(st.con("numMF"), seed=2)
+    steps = 3 * proto["trialSteps"]
+    o = Oracle(st_path, seeds=[7])
+    tr, _, _, _ = o.run_protocol(proto, rates, steps)
+    n_gr = st.con("numGR")
+    rec_from = proto["csOn"] - proto["preCS"]
+    rec_len = proto["csOff"] + proto["postCS"] - rec_from
+    bins = (rec_len + proto["binSteps"] - 1) // proto["binSteps"]
+    want = np.zeros((bins, n_gr), np.uint32)
+    nb = (n_gr + 7) // 8
+    for s in range(steps):
+        time, trial = s % proto["trialSteps"], s // proto["trialSteps"]
+        ct = time - rec_from
+        if proto["dataStartTrial"] <= trial < proto["dataStartTrial"] + proto["numDataTrials"] and 0 <= ct < rec_len:
+            want[ct // proto["binSteps"]] += np.unpackbits(np.asarray(tr[s][:nb], np.uint8), bitorder="little")[:n_gr]
+    assert want.sum() > 0
+    for replay in (True, False):
+        sim = cbm.CBMSimCore(cbm.CBMState(st_path), [7], device=0)
+        sim.set_eyelid_protocol(rates, **proto)
+        sim.record_gr()
+        if replay:
+            sim.run(steps, chunk=100)
+        else:
+            for _ in range(steps):
+                sim.calcActivity()
+        got = sim.trial_record("gr")
+        sim.close()
+        assert got.dtype == np.uint16 and got.shape == want.shape
+        assert np.array_equal(got.astype(np.uint32), want), f"replay={replay}"
