@@ -23,8 +23,12 @@
  *       restated below); the reference's EyelidIntegrator
  *       (CBM_TOOLS_LIB_DEV/src/eyelidintegrator.cpp) runs on zone 0's NC
  *       spikes; RECORDS receives NC and PC spike counts per bin and the
- *       integrator's output over the recording window of the kept trials
- *       (MFBYTES is then ignored).  PROTOCOL is "key value" text: trialSteps,
+ *       integrator's output over the recording window of the kept trials,
+ *       then the reference's GR peri-stimulus histogram (PeriStimHistFloat,
+ *       CBM_DATA_LIB_DEV/src/peristimhist/peristimhistfloat.cpp, updated with
+ *       exportAPGR as the eyelid driver does,
+ *       Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:262) as
+ *       f32 [bins][numGR] (MFBYTES is then ignored).  PROTOCOL is "key value" text: trialSteps,
  *       csOn, csOff, csPhasicOff, csStartTrial, plastOnDelay, plastOffDelay,
  *       plastLTD, plastLTP, usErrDrive, mfSeed, mfThreshDecayTau, rates (a file
  *       of 3 x numMF f32: background, CS tonic, CS phasic), dataStartTrial,
@@ -63,6 +67,7 @@
 #include <CBMCoreInclude/interface/cbmsimcore.h>
 #include <CBMToolsInclude/poissonregencells.h>
 #include <CBMToolsInclude/eyelidintegrator.h>
+#include <CBMDataInclude/peristimhist/peristimhistfloat.h>
 uint64_t cbm_refshim_step = 0;
 void cbm_refshim_set_step(uint64_t t) { cbm_refshim_step = t; }
 #endif
@@ -234,6 +239,7 @@ int main(int argc, char **argv)
 	PoissonRegenCells *mfs = NULL;
 	EyelidIntegrator *eyelid = NULL;
 	std::vector<ct_uint32_t> ncPSH, pcPSH;
+	PeriStimHistFloat *grPSH = NULL;
 	std::vector<float> eyeTrace;
 	bool grPCPlastSet = false, grPCPlastReset = true;
 	if (useProtocol)
@@ -254,6 +260,7 @@ int main(int argc, char **argv)
 		ncPSH.assign(nd * nBins * cp->numNC, 0);
 		pcPSH.assign(nd * nBins * cp->numPC, 0);
 		eyeTrace.assign(nd * (size_t)recLen, 0.0f);
+		grPSH = new PeriStimHistFloat(recLen, (int)binSteps, (int)cp->numGR);
 	}
 
 	auto t0 = std::chrono::steady_clock::now();
@@ -296,6 +303,7 @@ int main(int argc, char **argv)
 				for (unsigned int i = 0; i < cp->numNC; i++) ncPSH[(dt * nBins + bin) * cp->numNC + i] += apNC[i];
 				for (unsigned int i = 0; i < cp->numPC; i++) pcPSH[(dt * nBins + bin) * cp->numPC + i] += apPC[i];
 				eyeTrace[dt * recLen + ct] = vm;
+				grPSH->update(inet->exportAPGR());
 			}
 		}
 		while (!useProtocol && evi < events.size() && events[evi].t == t)
@@ -350,7 +358,13 @@ int main(int argc, char **argv)
 		put(f, ncPSH.data(), ncPSH.size());
 		put(f, pcPSH.data(), pcPSH.size());
 		put(f, eyeTrace.data(), eyeTrace.size());
+		const std::vector<std::vector<float> > cells = grPSH->getPopPSHs();  // [cell][bin]
+		std::vector<float> byBin((size_t)grPSH->getNumBins() * cp->numGR);
+		for (unsigned int i = 0; i < cp->numGR; i++)
+			for (unsigned int b = 0; b < grPSH->getNumBins(); b++) byBin[(size_t)b * cp->numGR + i] = cells[i][b];
+		put(f, byBin.data(), byBin.size());
 		fclose(f);
+		delete grPSH;
 		delete mfs;
 		delete eyelid;
 	}

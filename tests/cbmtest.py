@@ -176,6 +176,25 @@ def ref_run_protocol(state_path, proto, rates, nsteps, seeds):
         return np.fromfile(trp, dtype=np.uint8), np.fromfile(rec, dtype=np.uint8)
 
 
+def gr_psh_from_trace(trace, proto, n_gr):
+    """GR peri-stimulus histogram [bins][numGR] of a protocol run from its
+    per-step trace records (protocol started at step 0): in the recording
+    window of every kept trial, each GR spike adds one to its bin, all kept
+    trials into one histogram (the eyelid driver's updatePSH("gr"))."""
+    rec_from = proto["csOn"] - proto["preCS"]
+    rec_len = proto["csOff"] + proto["postCS"] - rec_from
+    bins = (rec_len + proto["binSteps"] - 1) // proto["binSteps"]
+    out = np.zeros((bins, n_gr), np.uint32)
+    nb = (n_gr + 7) // 8
+    first, last = proto["dataStartTrial"], proto["dataStartTrial"] + proto["numDataTrials"]
+    for s in range(trace.shape[0]):
+        time, trial = s % proto["trialSteps"], s // proto["trialSteps"]
+        ct = time - rec_from
+        if first <= trial < last and 0 <= ct < rec_len:
+            out[ct // proto["binSteps"]] += np.unpackbits(np.asarray(trace[s][:nb], np.uint8), bitorder="little")[:n_gr]
+    return out
+
+
 def events_file(events, path):
     with open(path, "w") as f:
         for t in sorted(events):

@@ -92,17 +92,8 @@ def test_gr_histogram_matches_oracle_spikes(tmp_path):
     steps = 3 * proto["trialSteps"]
     o = Oracle(st_path, seeds=[7])
     tr, _, _, _ = o.run_protocol(proto, rates, steps)
-    n_gr = st.con("numGR")
-    rec_from = proto["csOn"] - proto["preCS"]
-    rec_len = proto["csOff"] + proto["postCS"] - rec_from
-    bins = (rec_len + proto["binSteps"] - 1) // proto["binSteps"]
-    want = np.zeros((bins, n_gr), np.uint32)
-    nb = (n_gr + 7) // 8
-    for s in range(steps):
-        time, trial = s % proto["trialSteps"], s // proto["trialSteps"]
-        ct = time - rec_from
-        if proto["dataStartTrial"] <= trial < proto["dataStartTrial"] + proto["numDataTrials"] and 0 <= ct < rec_len:
-            want[ct // proto["binSteps"]] += np.unpackbits(np.asarray(tr[s][:nb], np.uint8), bitorder="little")[:n_gr]
+    # the rule test_oracle_pin.py pins to the reference's PeriStimHistFloat
+    want = cbmtest.gr_psh_from_trace(tr, proto, st.con("numGR"))
     assert want.sum() > 0
     for replay in (True, False):
         sim = cbm.CBMSimCore(cbm.CBMState(st_path), [7], device=0)

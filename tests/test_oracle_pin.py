@@ -104,8 +104,14 @@ def test_oracle_protocol_matches_reference_driver(tmp_path):
     assert tr_r.size == tr_o.size
     assert cbmtest.same_values(tr_r, tr_o.ravel()).all()
     rec_o = np.concatenate([nc.view(np.uint8), pc.view(np.uint8), eye.view(np.uint8)])
-    assert rec_r.size == rec_o.size
+    gr_r = rec_r[rec_o.size:].view(np.float32)  # the reference's GR histogram follows
+    rec_r = rec_r[: rec_o.size]
     assert cbmtest.same_values(rec_r.view(np.float32)[-eye.size:], eye).all()
     assert np.array_equal(rec_r[: nc.nbytes + pc.nbytes], rec_o[: nc.nbytes + pc.nbytes])
+    # the GR histogram rule the device follows, restated from the oracle's
+    # trace, equals the reference's PeriStimHistFloat
+    gr_o = cbmtest.gr_psh_from_trace(tr_o, proto, o.num["GR"])
+    assert gr_r.size == gr_o.size and gr_o.sum() > 0
+    assert np.array_equal(gr_r.reshape(gr_o.shape), gr_o.astype(np.float32))
     # the protocol did something: CS trials spike NCs and move the eyelid
     assert nc.sum() > 0 and eye.max() > 0
