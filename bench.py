@@ -367,7 +367,7 @@ def main_surrogate(args):
         wall_top = time.time() - t0
         sim_rnd, _ = sweep.simulate(base, p_c[rnd], s_c[rnd], T, device=device)
         # the plain sweep's answer: every candidate simulated (batched), to
-        # judge what the surrogate's ranking loses
+        # measure what the surrogate's ranking loses
         sim_all = gpu_all = None
         if not args.no_truth:
             sim_all, gpu_all = sweep.simulate(base, p_c, s_c, T, device=device)

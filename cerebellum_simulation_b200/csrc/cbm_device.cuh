@@ -115,7 +115,7 @@ struct DevProtocol {
 	float *mfThresh;       // regeneration state per MF
 	uint64_t mfKey;        // stream key of the MF draws
 	float sPerTS, mfThreshDecay;
-	int32_t *plastState;   // [2]: the driver's grPCPlastSet, grPCPlastReset
+	int32_t *plastState;   // [2]: the eyelid driver's grPCPlastSet, grPCPlastReset
 	float *curSteps;       // [2]: zone 0's LTD and LTP steps in force
 	float *ctlSlots;       // [2][3]: zone 0's LTD step, LTP step and error drive per step parity
 	// recording

@@ -1643,7 +1643,7 @@ __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 		if ((threadIdx.x & 31u) == 0 && i < 32u * words) bits[i >> 5] = word;
 	}
 	if (threadIdx.x == 0) {
-		int32_t *ps = P->plastState;  // the driver's grPCPlastSet, grPCPlastReset
+		int32_t *ps = P->plastState;  // the eyelid driver's grPCPlastSet, grPCPlastReset
 		float *cur = P->curSteps;     // zone 0's LTD and LTP steps in force
 		if (time >= P->csOn + P->plastOn && !ps[0] && csTrial && time < P->csOff + P->plastOff) {
 			ps[0] = 1; ps[1] = 0;

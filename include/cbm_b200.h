@@ -236,7 +236,7 @@ enum {
 };
 
 /* Start a device protocol on network 0 of the simulator (no counterpart in
- * the reference's core library: it replaces the driver's per-step calls). */
+ * the reference's core library: it replaces the eyelid driver's per-step calls). */
 int cbm_sim_set_eyelid_protocol(cbm_sim *sim, const cbm_eyelid_protocol *protocol);
 /* Size in bytes of a record of the running protocol (0 without one). */
 uint64_t cbm_sim_trial_record_bytes(cbm_sim *sim, int kind);
