@@ -77,7 +77,8 @@ int cbm_state_save(cbm_state *s, const char *path)
 	TRY(s->st.save(path));
 	// innetactivitystate.cpp:247-248 run on write as well
 	NamedArray *a = s->st.find("inputGOGABASynDepGO"), *b = s->st.find("goGABAOutSynScaleGOGO");
-	for (size_t i = 0; i < a->count; i++) { a->as<float>()[i] = 1.0f; b->as<float>()[i] = 0.0f; }
+	if (a) for (size_t i = 0; i < a->count; i++) a->as<float>()[i] = 1.0f;
+	if (b) for (size_t i = 0; i < b->count; i++) b->as<float>()[i] = 0.0f;
 	return CBM_OK;
 }
 

@@ -115,3 +115,27 @@ def test_oracle_protocol_matches_reference_driver(tmp_path):
     assert np.array_equal(gr_r.reshape(gr_o.shape), gr_o.astype(np.float32))
     # the protocol did something: CS trials spike NCs and move the eyelid
     assert nc.sum() > 0 and eye.max() > 0
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+def test_oracle_matches_reference_two_zones(tmp_path):
+    """Two microzones and GO->GO wiring from the package's generator: zone 1
+    takes its own plasticity steps and error drive (mzone.cpp:726-736,
+    cbmsimcore.cpp:322-325), and both zones' records and final state must
+    equal the reference's."""
+    from cerebellum_simulation_b200 import networks
+    net = networks.build_random_network(8, 6, 4, 4, 10, networks.act_params("16k"), seed=5, gr_per_go=128,
+                                       mf_per_go=3, vel=40, gogo=((1, 1, 0.0),), n_zones=2)
+    st = str(tmp_path / "z2.state")
+    net.writeState(st)
+    mf = cbmtest.counter_mf(1024, 600, 8, rate_hi=0.08)
+    ev = {2: [("plast", 1, -0.003, 0.002)], 300: [("errdrive", 1, 1.0), ("errdrive", 0, 0.5)],
+          450: [("plastreset", 1)]}
+    fin_ref = str(tmp_path / "ref_final.state")
+    ref = cbmtest.ref_run(st, mf, [3, 4], ev, final_path=fin_ref).reshape(600, -1)
+    o = Oracle(st, seeds=[3, 4])
+    tr = o.run(mf, ev)
+    assert cbmtest.first_difference(ref, tr, o.num) is None
+    fin = str(tmp_path / "oracle_final.state")
+    o.save(fin)
+    assert open(fin, "rb").read() == open(fin_ref, "rb").read()
