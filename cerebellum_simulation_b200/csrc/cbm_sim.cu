@@ -295,20 +295,93 @@ double Network::bytesPerStepLayout() const
 	return perGR * h_.numGR;
 }
 
+std::string checkNetwork(const State &st)
+{
+	const ConParams &c = st.cp;
+	const ActParams &a = st.ap;
+	auto A = [&](const char *n, int z = -1) -> const NamedArray * { return const_cast<State &>(st).find(n, z); };
+	if (st.numZones < 1 || st.numZones > (uint32_t)kMaxZones) return "zone count must be 1..4";
+	if (!c.numMF || !c.numGO || !c.numSC || !c.numBC || !c.numPC || !c.numNC || !c.numIO)
+		return "every cell count must be positive";
+	if (c.numMF >= 65535 || c.numGO >= 65535) return "numMF and numGO must be below 65535";
+	const uint32_t N = c.numGR, P = c.numpPCfromGRtoPC;
+	if (P < 4 || (P & (P - 1)) || N % 32) return "GR per PC must be a power of two >= 4 and numGR a multiple of 32";
+	if ((uint64_t)c.numPC * P != N) return "numGR must be numPC x GR per PC";
+	if (c.numpBCfromGRtoBCP2 > 31 || c.numpSCfromGRtoSCP2 > 31 ||
+			(1u << c.numpBCfromGRtoBCP2) != c.numpBCfromGRtoBC || (1u << c.numpSCfromGRtoSCP2) != c.numpSCfromGRtoSC)
+		return "PF->BC/SC block sizes are not powers of two";
+	if (a.tsPerHistBinGR == 0 || a.numTSinMFHist == 0 || a.tsPerPopHistBinPC == 0 || a.numPopHistBinsPC == 0)
+		return "time-bin parameters must be positive";
+
+	// GR synapse tables; the reference stores pGRfromMFtoGR with
+	// maxnumpGRfromGOtoGR columns
+	const int32_t *numMFin = A("numpGRfromMFtoGR")->as<int32_t>();
+	const uint32_t *pMF = A("pGRfromMFtoGR")->as<uint32_t>();
+	const int32_t *numGOin = A("numpGRfromGOtoGR")->as<int32_t>();
+	const uint32_t *pGO = A("pGRfromGOtoGR")->as<uint32_t>();
+	const int32_t *numOut = A("numpGRfromGRtoGO")->as<int32_t>();
+	const uint32_t *pOut = A("pGRfromGRtoGO")->as<uint32_t>();
+	const uint32_t *pOutMask = A("pGRDelayMaskfromGRtoGO")->as<uint32_t>();
+	const uint32_t *pfMask = A("pGRDelayMaskfromGRtoBSP")->as<uint32_t>();
+	const uint32_t strideGO = c.maxnumpGRfromGOtoGR, strideOut = c.maxnumpGRfromGRtoGO;
+	uint32_t bit;
+	for (uint32_t g = 0; g < N; g++) {
+		if (numMFin[g] < 0 || (uint32_t)numMFin[g] > std::min(c.maxnumpGRfromMFtoGR, strideGO))
+			return "MF->GR count out of range";
+		if (numGOin[g] < 0 || (uint32_t)numGOin[g] > strideGO) return "GO->GR count out of range";
+		if (numOut[g] < 0 || (uint32_t)numOut[g] > strideOut) return "GR->GO count out of range";
+		for (int k = 0; k < numMFin[g]; k++)
+			if (pMF[(size_t)g * strideGO + k] >= c.numMF) return "MF->GR index out of range";
+		for (int k = 0; k < numGOin[g]; k++)
+			if (pGO[(size_t)g * strideGO + k] >= c.numGO) return "GO->GR index out of range";
+		for (int k = 0; k < numOut[g]; k++) {
+			if (pOut[(size_t)g * strideOut + k] >= c.numGO) return "GR->GO index out of range";
+			if (!singleBitOrZero(pOutMask[(size_t)g * strideOut + k], bit)) return "GR->GO delay masks must have one bit";
+		}
+		if (!singleBitOrZero(pfMask[g], bit)) return "PF delay masks must have one bit";
+	}
+
+	// MF->GO out-lists, GO->GO GABA out-lists and GO coupling in-lists
+	auto lists = [&](const char *num, const char *idx, uint32_t rows, uint32_t stride, uint32_t lim) -> bool {
+		const int32_t *n = A(num)->as<int32_t>();
+		const uint32_t *p = A(idx)->as<uint32_t>();
+		for (uint32_t i = 0; i < rows; i++) {
+			if (n[i] < 0 || (uint32_t)n[i] > stride) return false;
+			for (int j = 0; j < n[i]; j++) if (p[(size_t)i * stride + j] >= lim) return false;
+		}
+		return true;
+	};
+	if (!lists("numpMFfromMFtoGO", "pMFfromMFtoGO", c.numMF, c.maxnumpMFfromMFtoGO, c.numGO))
+		return "MF->GO count or index out of range";
+	if (!lists("numpGOGABAOutGOGO", "pGOGABAOutGOGO", c.numGO, c.maxnumpGOGABAOutGOGO, c.numGO))
+		return "GO->GO count or index out of range";
+	if (!lists("numpGOCoupInGOGO", "pGOCoupInGOGO", c.numGO, c.maxnumpGOCoupInGOGO, c.numGO))
+		return "GO coupling count or index out of range";
+
+	// microzone wiring: every entry of each table is an index
+	for (uint32_t z = 0; z < st.numZones; z++) {
+		auto all = [&](const char *n, uint32_t lim) -> bool {
+			const NamedArray *x = A(n, (int)z);
+			const uint32_t *p = x->as<uint32_t>();
+			for (size_t k = 0; k < x->count; k++) if (p[k] >= lim) return false;
+			return true;
+		};
+		if (!all("pPCfromSCtoPC", c.numSC) || !all("pNCfromPCtoNC", c.numPC) || !all("pNCfromMFtoNC", c.numMF) ||
+				!all("pIOfromNCtoIO", c.numNC) || !all("pIOInIOIO", c.numIO) || !all("pBCfromBCtoPC", c.numPC) ||
+				!all("pPCfromPCtoBC", c.numBC))
+			return "microzone connectivity index out of range";
+	}
+	return "";
+}
+
 std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mfRing, uint32_t mfSeed)
 {
 	(void)mfSeed;
 	st_ = st;
 	const ConParams &c = st->cp;
 	const ActParams &a = st->ap;
-	if (st->numZones < 1 || st->numZones > (uint32_t)kMaxZones) return "zone count must be 1..4";
-	if (c.numMF >= 65535 || c.numGO >= 65535) return "numMF and numGO must be below 65535";
+	// checkNetwork(*st) has passed: every count and index below is in range
 	const uint32_t N = c.numGR, P = c.numpPCfromGRtoPC;
-	if (P < 4 || (P & (P - 1)) || N % 32) return "GR per PC must be a power of two >= 4 and numGR a multiple of 32";
-	if ((1u << c.numpBCfromGRtoBCP2) != c.numpBCfromGRtoBC || (1u << c.numpSCfromGRtoSCP2) != c.numpSCfromGRtoSC)
-		return "PF->BC/SC block sizes are not powers of two";
-	if (a.tsPerHistBinGR == 0 || a.numTSinMFHist == 0 || a.tsPerPopHistBinPC == 0 || a.numPopHistBinsPC == 0)
-		return "time-bin parameters must be positive";
 
 	DevNet &h = h_;
 	h.numGR = N; h.numMF = c.numMF; h.numGO = c.numGO; h.numSC = c.numSC; h.numBC = c.numBC;
@@ -369,8 +442,8 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	auto A = [&](const char *n, int z = -1) -> NamedArray * { return st->find(n, z); };
 
 	// ---- GR synapse tables: [gr][slot] (reference) -> [slot][gr] with
-	// sentinel padding; counts and indices are checked here once so the
-	// kernels need no bounds checks.
+	// sentinel padding; checkNetwork bounds every count and index once, so
+	// the kernels need no bounds checks.
 	const int32_t *numMFin = A("numpGRfromMFtoGR")->as<int32_t>();
 	const uint32_t *pMF = A("pGRfromMFtoGR")->as<uint32_t>();
 	const int32_t *numGOin = A("numpGRfromGOtoGR")->as<int32_t>();
@@ -383,9 +456,6 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	uint32_t nMF = 0, nGO = 0, nOut = 0;
 	uint64_t sumMF = 0, sumGO = 0, sumOut = 0;
 	for (uint32_t g = 0; g < N; g++) {
-		if (numMFin[g] < 0 || (uint32_t)numMFin[g] > c.maxnumpGRfromMFtoGR) return "MF->GR count out of range";
-		if (numGOin[g] < 0 || (uint32_t)numGOin[g] > c.maxnumpGRfromGOtoGR) return "GO->GR count out of range";
-		if (numOut[g] < 0 || (uint32_t)numOut[g] > c.maxnumpGRfromGRtoGO) return "GR->GO count out of range";
 		nMF = std::max<uint32_t>(nMF, numMFin[g]); nGO = std::max<uint32_t>(nGO, numGOin[g]);
 		nOut = std::max<uint32_t>(nOut, numOut[g]);
 		sumMF += numMFin[g]; sumGO += numGOin[g]; sumOut += numOut[g];
@@ -397,24 +467,14 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	std::vector<uint32_t> outCon((size_t)std::max(1u, nOut) * N, kNoDelay);
 	std::vector<uint8_t> pfDelay(N);
 	for (uint32_t g = 0; g < N; g++) {
-		for (int k = 0; k < numMFin[g]; k++) {
-			uint32_t v = pMF[(size_t)g * strideGO + k];
-			if (v >= c.numMF) return "MF->GR index out of range";
-			mfIdx[(size_t)k * N + g] = (uint16_t)v;
-		}
-		for (int k = 0; k < numGOin[g]; k++) {
-			uint32_t v = pGO[(size_t)g * strideGO + k];
-			if (v >= c.numGO) return "GO->GR index out of range";
-			goIdx[(size_t)k * N + g] = (uint16_t)v;
-		}
+		for (int k = 0; k < numMFin[g]; k++) mfIdx[(size_t)k * N + g] = (uint16_t)pMF[(size_t)g * strideGO + k];
+		for (int k = 0; k < numGOin[g]; k++) goIdx[(size_t)k * N + g] = (uint16_t)pGO[(size_t)g * strideGO + k];
+		uint32_t bit = 0;
 		for (int k = 0; k < numOut[g]; k++) {
-			uint32_t v = pOut[(size_t)g * strideOut + k], bit;
-			if (v >= c.numGO) return "GR->GO index out of range";
-			if (!singleBitOrZero(pOutMask[(size_t)g * strideOut + k], bit)) return "GR->GO delay masks must have one bit";
-			outCon[(size_t)k * N + g] = (v << 8) | bit;
+			singleBitOrZero(pOutMask[(size_t)g * strideOut + k], bit);
+			outCon[(size_t)k * N + g] = (pOut[(size_t)g * strideOut + k] << 8) | bit;
 		}
-		uint32_t bit;
-		if (!singleBitOrZero(pfMask[g], bit)) return "PF delay masks must have one bit";
+		singleBitOrZero(pfMask[g], bit);
 		pfDelay[g] = (uint8_t)bit;
 	}
 	h.mfIdx = upload(mfIdx.data(), mfIdx.size());
@@ -482,25 +542,13 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 
 	// MF->GO out-lists as stored; GO->GO in-lists per destination in the
 	// reference's (source, slot) iteration order (innet.cpp:937-950)
-	const int32_t *numMFGO = A("numpMFfromMFtoGO")->as<int32_t>();
-	const uint32_t *pMFGO = A("pMFfromMFtoGO")->as<uint32_t>();
-	for (uint32_t i = 0; i < c.numMF; i++) {
-		if (numMFGO[i] < 0 || (uint32_t)numMFGO[i] > c.maxnumpMFfromMFtoGO) return "MF->GO count out of range";
-		for (int j = 0; j < numMFGO[i]; j++) if (pMFGO[(size_t)i * c.maxnumpMFfromMFtoGO + j] >= c.numGO) return "MF->GO index out of range";
-	}
 	h.numpMFfromMFtoGO = upI("numpMFfromMFtoGO"); h.pMFfromMFtoGO = upU("pMFfromMFtoGO");
 	{
 		const int32_t *numOutGG = A("numpGOGABAOutGOGO")->as<int32_t>();
 		const uint32_t *pOutGG = A("pGOGABAOutGOGO")->as<uint32_t>();
 		std::vector<std::vector<uint32_t>> in(c.numGO);
-		for (uint32_t i = 0; i < c.numGO; i++) {
-			if (numOutGG[i] < 0 || (uint32_t)numOutGG[i] > c.maxnumpGOGABAOutGOGO) return "GO->GO count out of range";
-			for (int j = 0; j < numOutGG[i]; j++) {
-				uint32_t d = pOutGG[(size_t)i * c.maxnumpGOGABAOutGOGO + j];
-				if (d >= c.numGO) return "GO->GO index out of range";
-				in[d].push_back(i);
-			}
-		}
+		for (uint32_t i = 0; i < c.numGO; i++)
+			for (int j = 0; j < numOutGG[i]; j++) in[pOutGG[(size_t)i * c.maxnumpGOGABAOutGOGO + j]].push_back(i);
 		std::vector<uint32_t> start(c.numGO + 1, 0), src;
 		for (uint32_t d = 0; d < c.numGO; d++) { start[d + 1] = start[d] + (uint32_t)in[d].size(); src.insert(src.end(), in[d].begin(), in[d].end()); }
 		h.gogoStart = upload(start.data(), start.size());
@@ -513,10 +561,8 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 		std::vector<uint32_t> level(c.numGO, 0);
 		uint32_t maxLevel = 0;
 		for (uint32_t i = 0; i < c.numGO; i++) {
-			if (numC[i] < 0 || (uint32_t)numC[i] > c.maxnumpGOCoupInGOGO) return "GO coupling count out of range";
 			for (int j = 0; j < numC[i]; j++) {
 				uint32_t n = pC[(size_t)i * c.maxnumpGOCoupInGOGO + j];
-				if (n >= c.numGO) return "GO coupling index out of range";
 				any = true;
 				if (n < i) level[i] = std::max(level[i], level[n] + 1);
 			}
@@ -557,16 +603,6 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 			ioOfPC[pc] = std::min<uint32_t>(cur, c.numIO - 1);
 		}
 		Q.ioOfPC = upload(ioOfPC.data(), ioOfPC.size());
-		auto chk = [&](const char *n, uint32_t lim) -> bool {
-			NamedArray *x = A(n, z);
-			const uint32_t *p = x->as<uint32_t>();
-			for (size_t k = 0; k < x->count; k++) if (p[k] >= lim) return false;
-			return true;
-		};
-		if (!chk("pPCfromSCtoPC", c.numSC) || !chk("pNCfromPCtoNC", c.numPC) || !chk("pNCfromMFtoNC", c.numMF) ||
-				!chk("pIOfromNCtoIO", c.numNC) || !chk("pIOInIOIO", c.numIO) || !chk("pBCfromBCtoPC", c.numPC) ||
-				!chk("pPCfromPCtoBC", c.numBC))
-			return "microzone connectivity index out of range";
 		Q.pPCfromSCtoPC = upU("pPCfromSCtoPC", z); Q.pNCfromPCtoNC = upU("pNCfromPCtoNC", z);
 		Q.pNCfromMFtoNC = upU("pNCfromMFtoNC", z); Q.pIOfromNCtoIO = upU("pIOfromNCtoIO", z);
 		Q.pIOInIOIO = upU("pIOInIOIO", z);
@@ -1004,6 +1040,9 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 		int device, uint32_t mfRing, const std::vector<uint32_t> *mfSeeds)
 {
 	device_ = device;
+	// host-side validation first, so a malformed network is rejected
+	// before any device work
+	for (const State *st : states) CKS(checkNetwork(*st));
 	CK(cudaSetDevice(device), "selecting the device");
 	// The small-cell CTAs (one SM's register file each) go on the
 	// high-priority stream so that they are dispatched before the GR pass

@@ -33,6 +33,11 @@ struct DeviceBuf {
 
 class Network;
 
+// Host-side validation of a network before it goes to a device: the
+// structural limits of the kernels and every connectivity count and index.
+// Returns an empty string or the reason; Simulator::create calls it first.
+std::string checkNetwork(const State &st);
+
 // Pinned staging slots for host MF input per network (updateMFInput).
 constexpr uint32_t kMFStage = 8;
 

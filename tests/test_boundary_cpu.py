@@ -105,3 +105,55 @@ def test_cpp_facade_compiles_and_loads_a_reference_state(tmp_path):
     p = cbmtest.golden_state("ref16k", str(tmp_path))
     out = subprocess.run([exe, p], check=True, capture_output=True, text=True).stdout
     assert "zones 1" in out
+
+
+def _damage(s, name):
+    """One out-of-range entry in a reference network's wiring."""
+    if name == "pGRfromMFtoGR":
+        assert s.array("numpGRfromMFtoGR")[0] >= 1
+        s.array(name)[0] = s.con("numMF")
+    elif name == "numpGRfromGOtoGR":
+        s.array(name)[5] = s.con("maxnumpGRfromGOtoGR") + 1
+    elif name == "pGRfromGRtoGO":
+        g = int(np.argmax(s.array("numpGRfromGRtoGO") > 0))
+        s.array(name)[g * s.con("maxnumpGRfromGRtoGO")] = s.con("numGO")
+    elif name == "pGRDelayMaskfromGRtoGO":
+        g = int(np.argmax(s.array("numpGRfromGRtoGO") > 0))
+        s.array(name)[g * s.con("maxnumpGRfromGRtoGO")] = 3
+    elif name == "numpGOCoupInGOGO":
+        s.array(name)[7] = s.con("maxnumpGOCoupInGOGO") + 1
+    elif name == "pBCfromBCtoPC":
+        s.array(name, 0)[0] = s.con("numPC")
+
+
+@pytest.mark.parametrize("name,code,words", [
+    ("pGRfromMFtoGR", 5, "MF->GR index"),
+    ("numpGRfromGOtoGR", 5, "GO->GR count"),
+    ("pGRfromGRtoGO", 5, "GR->GO index"),
+    ("pGRDelayMaskfromGRtoGO", 6, "one bit"),
+    ("numpGOCoupInGOGO", 5, "GO coupling"),
+    ("pBCfromBCtoPC", 5, "microzone"),
+])
+def test_malformed_network_is_rejected_before_the_device(tmp_path, name, code, words):
+    """Every connectivity count and index is checked on the host when the
+    simulator is created, before any device work, so the kernels carry no
+    bounds checks and a bad network never reaches a GPU."""
+    import cerebellum_simulation_b200 as cbm
+    s = cbm.CBMState(cbmtest.golden_state("ref16k", str(tmp_path)))
+    _damage(s, name)
+    with pytest.raises(cbm.CBMError) as e:
+        cbm.CBMSimCore(s, [7])
+    assert e.value.code == code and words in str(e.value), str(e.value)
+
+
+def test_valid_network_needs_a_device(tmp_path):
+    """Without a GPU the simulator fails loudly (CBM_ERR_CUDA): there is no
+    CPU fallback behind the API."""
+    import cerebellum_simulation_b200 as cbm
+    s = cbm.CBMState(cbmtest.golden_state("ref16k", str(tmp_path)))
+    try:
+        sim = cbm.CBMSimCore(s, [7])
+    except cbm.CBMError as e:
+        assert e.code == 2, str(e)
+    else:
+        sim.close()
