@@ -1144,8 +1144,76 @@ void cbm_oracle_protocol_sizes(const cbm_oracle *o, const cbm_oracle_protocol *p
 	*eyelid = nd * (uint64_t)len;
 }
 
+/* cells of each trial-data record, in record order */
+static void trial_data_cells(const cbm_oracle *o, uint32_t psh[9], uint32_t raster[6])
+{
+	const uint32_t p9[9] = {o->numGO, o->numGO, o->numGO, o->numGO, o->numMF, o->numSC, o->numBC, o->numPC, o->numIO};
+	const uint32_t r6[6] = {o->numGO, o->numSC, o->numBC, o->numPC, o->numNC, o->numIO};
+	memcpy(psh, p9, sizeof(p9));
+	memcpy(raster, r6, sizeof(r6));
+}
+
+void cbm_oracle_trial_data_sizes(const cbm_oracle *o, const cbm_oracle_protocol *p, uint64_t *psh,
+		uint64_t *raster)
+{
+	int32_t from, len; uint32_t bins, pc[9], rc[6];
+	protocol_window(p, &from, &len, &bins);
+	trial_data_cells(o, pc, rc);
+	*psh = 0; *raster = 0;
+	for (int k = 0; k < 9; k++) *psh += (uint64_t)bins * pc[k];
+	for (int k = 0; k < 6; k++) *raster += (uint64_t)p->numDataTrials * (uint32_t)(len / 32) * rc[k];
+}
+
+/* One step of ECTrialsData recording at window step ct of kept trial dt
+ * (ecmanagementdelay.cpp:240-265): every histogram adds the step's value to
+ * its bin (PeriStimHistFloat::update, peristimhistfloat.cpp: u8 spikes as
+ * (ap > 0), u32 counts and floats as they are, in float); every 32nd window
+ * step after the first, each raster takes the cells' apBuf words into its
+ * next row (SpikeRasterBitArray::updateRaster, spikerasterbitarray.cpp:62-80),
+ * rows counted over all updates, recLen / 32 rows to a raster trial. */
+static void trial_data_step(const cbm_oracle *o, const cbm_oracle_protocol *p, const uint8_t *apMF, uint32_t dt,
+		int32_t ct, float *psh, uint32_t *raster)
+{
+	int32_t from, len; uint32_t bins, pc[9], rc[6];
+	protocol_window(p, &from, &len, &bins);
+	trial_data_cells(o, pc, rc);
+	const zone_t *z = &o->zones[0];
+	const uint32_t bin = (uint32_t)ct / p->binSteps;
+	if (psh)
+	{
+		float *h[9];
+		h[0] = psh;
+		for (int k = 1; k < 9; k++) h[k] = h[k - 1] + (size_t)bins * pc[k - 1];
+		for (int k = 0; k < 9; k++) h[k] += (size_t)bin * pc[k];
+		for (uint32_t i = 0; i < o->numGO; i++)
+		{
+			h[0][i] += (float)(o->apGO[i] > 0);
+			h[1][i] += o->sumGRInputGO[i];
+			h[2][i] += o->sumInputGOGABASynDepGO[i];
+			h[3][i] += o->goGABAOutSynScaleGOGO[i];
+		}
+		for (uint32_t i = 0; i < o->numMF; i++) h[4][i] += (float)(apMF[i] > 0);
+		for (uint32_t i = 0; i < o->numSC; i++) h[5][i] += (float)(o->apSC[i] > 0);
+		for (uint32_t i = 0; i < o->numBC; i++) h[6][i] += (float)(z->apBC[i] > 0);
+		for (uint32_t i = 0; i < o->numPC; i++) h[7][i] += (float)(z->apPC[i] > 0);
+		for (uint32_t i = 0; i < o->numIO; i++) h[8][i] += (float)(z->apIO[i] > 0);
+	}
+	const uint32_t rows = (uint32_t)len / 32;
+	if (!raster || !rows || ct % 32 != 0 || ct == 0) return;
+	const uint64_t u = (uint64_t)dt * (uint32_t)((len - 1) / 32) + (uint32_t)ct / 32 - 1;
+	const uint64_t rt = u / rows, row = u % rows;
+	if (rt >= p->numDataTrials) return;
+	const uint32_t *src[6] = {o->apBufGO, o->apBufSC, z->apBufBC, z->apBufPC, z->apBufNC, z->apBufIO};
+	uint32_t *r = raster;
+	for (int k = 0; k < 6; k++)
+	{
+		memcpy(r + ((size_t)rt * rows + row) * rc[k], src[k], rc[k] * sizeof(uint32_t));
+		r += (size_t)p->numDataTrials * rows * rc[k];
+	}
+}
+
 void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, uint64_t nsteps,
-		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid)
+		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid, float *psh, uint32_t *raster)
 {
 	const uint32_t numMF = o->numMF, numNC = o->numNC, numPC = o->numPC;
 	const float *freqBG = rates, *freqCST = rates + numMF, *freqCSP = rates + 2 * (size_t)numMF;
@@ -1154,6 +1222,10 @@ void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const 
 	uint64_t nNC, nPC, nEye;
 	cbm_oracle_protocol_sizes(o, p, &nNC, &nPC, &nEye);
 	memset(ncPSH, 0, nNC * 4); memset(pcPSH, 0, nPC * 4); memset(eyelid, 0, nEye * 4);
+	uint64_t nPSH, nRaster;
+	cbm_oracle_trial_data_sizes(o, p, &nPSH, &nRaster);
+	if (psh) memset(psh, 0, nPSH * 4);
+	if (raster) memset(raster, 0, nRaster * 4);
 	/* PoissonRegenCells(numMF, mfSeed, tau, 1) (ecmanagementdelay.cpp:96,
 	 * poissonregencells.cpp:10-35): its generator's seed is the first draw of
 	 * a generator seeded with mfSeed, scaled to [0, 2^31) */
@@ -1220,6 +1292,7 @@ void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const 
 			for (uint32_t i = 0; i < numNC; i++) ncPSH[(dt * nBins + bin) * numNC + i] += z0->apNC[i];
 			for (uint32_t i = 0; i < numPC; i++) pcPSH[(dt * nBins + bin) * numPC + i] += z0->apPC[i];
 			eyelid[dt * recLen + ct] = vm;
+			trial_data_step(o, p, apMF, (uint32_t)dt, ct, psh, raster);
 		}
 	}
 	free(thresh); free(apMF); free(gIn);

@@ -72,8 +72,17 @@ typedef struct {
 /* Record sizes in elements: *ncPSH, *pcPSH (u32) and *eyelid (f32). */
 void cbm_oracle_protocol_sizes(const cbm_oracle *o, const cbm_oracle_protocol *p, uint64_t *ncPSH,
 		uint64_t *pcPSH, uint64_t *eyelid);
+/* Sizes in elements of the trial-data records (the eyelid driver's
+ * ECTrialsData, ecmanagementdelay.cpp:107-156, 236-265): *psh f32 and
+ * *raster u32.  psh: the peri-stimulus histograms go, grInputGO, goInputGO,
+ * goOutSynScale, mf, sc, bc, pc, io, each f32 [bins][cells] summed over the
+ * kept trials; raster: the apBuf words of go, sc, bc, pc, nc, io, each u32
+ * [numDataTrials][recLen / 32][cells] (zone 0 for the microzone cells). */
+void cbm_oracle_trial_data_sizes(const cbm_oracle *o, const cbm_oracle_protocol *p, uint64_t *psh,
+		uint64_t *raster);
+/* psh and raster (either may be NULL) receive the trial-data records. */
 void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, uint64_t nsteps,
-		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid);
+		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid, float *psh, uint32_t *raster);
 
 /* Sizes, for callers sizing buffers. */
 uint32_t cbm_oracle_num(const cbm_oracle *o, const char *what);

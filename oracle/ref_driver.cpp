@@ -68,6 +68,7 @@
 #include <CBMToolsInclude/poissonregencells.h>
 #include <CBMToolsInclude/eyelidintegrator.h>
 #include <CBMDataInclude/peristimhist/peristimhistfloat.h>
+#include <CBMDataInclude/interfaces/ectrialsdata.h>
 uint64_t cbm_refshim_step = 0;
 void cbm_refshim_set_step(uint64_t t) { cbm_refshim_step = t; }
 #endif
@@ -240,6 +241,10 @@ int main(int argc, char **argv)
 	EyelidIntegrator *eyelid = NULL;
 	std::vector<ct_uint32_t> ncPSH, pcPSH;
 	PeriStimHistFloat *grPSH = NULL;
+	ECTrialsData *data = NULL;
+	// the driver's histograms and rasters, in the order RECORDS holds them
+	const char *pshNames[] = {"go", "grInputGO", "goInputGO", "goOutSynScale", "mf", "sc", "bc", "pc", "io", "gr"};
+	const char *rasterNames[] = {"go", "sc", "bc", "pc", "nc", "io"};
 	std::vector<float> eyeTrace;
 	bool grPCPlastSet = false, grPCPlastReset = true;
 	if (useProtocol)
@@ -261,6 +266,21 @@ int main(int argc, char **argv)
 		pcPSH.assign(nd * nBins * cp->numPC, 0);
 		eyeTrace.assign(nd * (size_t)recLen, 0.0f);
 		grPSH = new PeriStimHistFloat(recLen, (int)binSteps, (int)cp->numGR);
+		// ECTrialsData as the eyelid driver builds it (ecmanagementdelay.cpp:107-156),
+		// with this protocol's window and bin width
+		std::map<std::string, PSHParams> pshParams;
+		std::map<std::string, RasterParams> rasterParams;
+		std::map<std::string, RawUIntParams> uintParams;
+		const unsigned int pshCells[] = {cp->numGO, cp->numGO, cp->numGO, cp->numGO, cp->numMF, cp->numSC,
+			cp->numBC, cp->numPC, cp->numIO, cp->numGR / 10};
+		const unsigned int rasterCells[] = {cp->numGO, cp->numSC, cp->numBC, cp->numPC, cp->numNC, cp->numIO};
+		for (int k = 0; k < 10; k++) { PSHParams pp; pp.numTimeStepsPerBin = binSteps; pp.numCells = pshCells[k]; pshParams[pshNames[k]] = pp; }
+		for (int k = 0; k < 6; k++) { RasterParams rp; rp.numCells = rasterCells[k]; rasterParams[rasterNames[k]] = rp; }
+		EyelidOutParams eyelidParams;
+		eyelidParams.numTimeStepSmooth = 4;
+		data = new ECTrialsData((unsigned int)proto.num("preCS"), (unsigned int)(csOff - csOn),
+				(unsigned int)proto.num("postCS"), (unsigned int)st->getActParamsInternal()->msPerTimeStep,
+				numDataT, pshParams, rasterParams, uintParams, eyelidParams);
 	}
 
 	auto t0 = std::chrono::steady_clock::now();
@@ -304,6 +324,27 @@ int main(int argc, char **argv)
 				for (unsigned int i = 0; i < cp->numPC; i++) pcPSH[(dt * nBins + bin) * cp->numPC + i] += apPC[i];
 				eyeTrace[dt * recLen + ct] = vm;
 				grPSH->update(inet->exportAPGR());
+				// ecmanagementdelay.cpp:244-265
+				if (data->getTSPerRasterUpdate() > 0 && ct % data->getTSPerRasterUpdate() == 0 && ct > 0)
+				{
+					data->updateRaster("go", inet->exportAPBufGO());
+					data->updateRaster("sc", inet->exportAPBufSC());
+					data->updateRaster("bc", zones[0]->exportAPBufBC());
+					data->updateRaster("pc", zones[0]->exportAPBufPC());
+					data->updateRaster("nc", zones[0]->exportAPBufNC());
+					data->updateRaster("io", zones[0]->exportAPBufIO());
+				}
+				data->updatePSH("go", inet->exportAPGO());
+				data->updatePSH("grInputGO", inet->exportSumGRInputGO());
+				data->updatePSH("goInputGO", inet->exportSumGOInputGO());
+				data->updatePSH("goOutSynScale", inet->exportGOOutSynScaleGOGO());
+				data->updatePSH("mf", apMF);
+				data->updatePSH("gr", inet->exportAPGR());
+				data->updatePSH("sc", inet->exportAPSC());
+				data->updatePSH("bc", zones[0]->exportAPBC());
+				data->updatePSH("pc", zones[0]->exportAPPC());
+				data->updatePSH("io", zones[0]->exportAPIO());
+				data->updateEyelid(vm);
 			}
 		}
 		while (!useProtocol && evi < events.size() && events[evi].t == t)
@@ -363,7 +404,36 @@ int main(int argc, char **argv)
 		for (unsigned int i = 0; i < cp->numGR; i++)
 			for (unsigned int b = 0; b < grPSH->getNumBins(); b++) byBin[(size_t)b * cp->numGR + i] = cells[i][b];
 		put(f, byBin.data(), byBin.size());
+		// the driver's histograms [bin][cell], then its rasters [trial][row][cell]
+		// as 32-step words (bit 31 the earliest step, SpikeRasterBitArray's order
+		// of getPopSpikesAtTS; rows the raster did not reach are whatever its
+		// allocation held)
+		for (int k = 0; k < 10; k++)
+		{
+			PeriStimHistFloat *h = data->getPSH(pshNames[k]);
+			const std::vector<std::vector<float> > c = h->getPopPSHs();
+			std::vector<float> v((size_t)h->getNumBins() * h->getNumCells());
+			for (unsigned int i = 0; i < h->getNumCells(); i++)
+				for (unsigned int b = 0; b < h->getNumBins(); b++) v[(size_t)b * h->getNumCells() + i] = c[i][b];
+			put(f, v.data(), v.size());
+		}
+		const unsigned int rows = (unsigned int)recLen / 32;
+		for (int k = 0; k < 6; k++)
+		{
+			ISpikeRaster *r = data->getRaster(rasterNames[k]);
+			const unsigned int n = r->getNumCells();
+			std::vector<ct_uint32_t> w((size_t)numDataT * rows * n, 0);
+			for (unsigned int tr2 = 0; tr2 < numDataT; tr2++)
+				for (unsigned int ts = 0; ts < rows * 32; ts++)
+				{
+					const std::vector<bool> aps = r->getPopSpikesAtTS(ts, tr2);
+					for (unsigned int i = 0; i < n; i++)
+						if (aps[i]) w[((size_t)tr2 * rows + ts / 32) * n + i] |= 0x80000000u >> (ts % 32);
+				}
+			put(f, w.data(), w.size());
+		}
 		fclose(f);
+		delete data;
 		delete grPSH;
 		delete mfs;
 		delete eyelid;

@@ -52,7 +52,8 @@ class Oracle:
             lib.cbm_oracle_num.restype = ctypes.c_uint32
             lib.cbm_oracle_num.argtypes = [P, S]
             lib.cbm_oracle_protocol_sizes.argtypes = [P, P, P, P, P]
-            lib.cbm_oracle_run_protocol.argtypes = [P, P, P, ctypes.c_uint64, P, P, P, P]
+            lib.cbm_oracle_run_protocol.argtypes = [P, P, P, ctypes.c_uint64, P, P, P, P, P, P]
+            lib.cbm_oracle_trial_data_sizes.argtypes = [P, P, P, P]
             cls._lib = lib
         return cls._lib
 
@@ -100,9 +101,10 @@ class Oracle:
             lib.cbm_oracle_run(self.h, row.ctypes.data, 1, tr[s].ctypes.data)
         return tr
 
-    def run_protocol(self, proto, rates, nsteps, record=True):
+    def run_protocol(self, proto, rates, nsteps, record=True, trial_data=False):
         """The eyelid driver around nsteps steps (cbm_oracle_run_protocol):
-        (trace, ncPSH, pcPSH, eyelid)."""
+        (trace, ncPSH, pcPSH, eyelid), and with trial_data the eyelid driver's
+        ECTrialsData records as a dict (split_trial_data)."""
         lib = self.lib()
         p = ProtocolStruct.from_dict(proto)
         sizes = [ctypes.c_uint64() for _ in range(3)]
@@ -110,16 +112,57 @@ class Oracle:
         nc = np.zeros(sizes[0].value, dtype=np.uint32)
         pc = np.zeros(sizes[1].value, dtype=np.uint32)
         eye = np.zeros(sizes[2].value, dtype=np.float32)
+        psh = raster = None
+        if trial_data:
+            ts = [ctypes.c_uint64() for _ in range(2)]
+            lib.cbm_oracle_trial_data_sizes(self.h, ctypes.byref(p), *[ctypes.byref(x) for x in ts])
+            psh = np.zeros(ts[0].value, dtype=np.float32)
+            raster = np.zeros(ts[1].value, dtype=np.uint32)
         rates = np.ascontiguousarray(rates, dtype=np.float32)
         tr = np.zeros((nsteps, self.rb), dtype=np.uint8) if record else None
         lib.cbm_oracle_run_protocol(self.h, ctypes.byref(p), rates.ctypes.data, nsteps,
                                     tr.ctypes.data if record else None, nc.ctypes.data, pc.ctypes.data,
-                                    eye.ctypes.data)
+                                    eye.ctypes.data, _data(psh), _data(raster))
+        if trial_data:
+            return tr, nc, pc, eye, split_trial_data(psh, raster, self.num, proto)
         return tr, nc, pc, eye
 
     def save(self, path):
         if self.lib().cbm_oracle_save(self.h, os.fsencode(path)) != 0:
             raise RuntimeError("oracle save failed")
+
+
+def _data(a):
+    return None if a is None else a.ctypes.data
+
+
+# the trial-data records in their order (cbm_oracle_trial_data_sizes)
+TRIAL_PSH = [("go", "GO"), ("grInputGO", "GO"), ("goInputGO", "GO"), ("goOutSynScale", "GO"), ("mf", "MF"),
+             ("sc", "SC"), ("bc", "BC"), ("pc", "PC"), ("io", "IO")]
+TRIAL_RASTER = [("go", "GO"), ("sc", "SC"), ("bc", "BC"), ("pc", "PC"), ("nc", "NC"), ("io", "IO")]
+
+
+def split_trial_data(psh, raster, num, proto):
+    """{"psh": {name: f32 [bins][cells]}, "raster": {name: u32 [trials][rows][cells]}}
+    from the concatenated records."""
+    rec_from = proto["csOn"] - proto["preCS"]
+    rec_len = proto["csOff"] + proto["postCS"] - rec_from
+    bins = (rec_len + proto["binSteps"] - 1) // proto["binSteps"]
+    rows, nd = rec_len // 32, proto["numDataTrials"]
+    out = {"psh": {}, "raster": {}}
+    off = 0
+    for name, cell in TRIAL_PSH:
+        n = bins * num[cell]
+        out["psh"][name] = psh[off: off + n].reshape(bins, num[cell])
+        off += n
+    assert off == psh.size
+    off = 0
+    for name, cell in TRIAL_RASTER:
+        n = nd * rows * num[cell]
+        out["raster"][name] = raster[off: off + n].reshape(nd, rows, num[cell])
+        off += n
+    assert off == raster.size
+    return out
 
 
 PROTOCOL_FIELDS = [("trialSteps", "u"), ("csOn", "i"), ("csOff", "i"), ("csPhasicOff", "i"), ("csStartTrial", "u"),
@@ -174,6 +217,45 @@ def ref_run_protocol(state_path, proto, rates, nsteps, seeds):
         cmd = [REF_RUN, state_path, "-", str(nsteps), trp, "-"] + [str(s) for s in seeds] + ["-p", pp, "-r", rec]
         subprocess.run(cmd, check=True, capture_output=True)
         return np.fromfile(trp, dtype=np.uint8), np.fromfile(rec, dtype=np.uint8)
+
+
+def split_ref_records(rec, num, proto):
+    """The RECORDS file of ref_run -p as a dict: nc, pc (u32 per trial),
+    eye, gr (f32 [bins][numGR]), psh {name: f32 [bins][cells]} (the driver's
+    ECTrialsData histograms; "gr" covers numGR / 10 cells there), raster
+    {name: u32 [trials][rows][cells]}."""
+    rec_from = proto["csOn"] - proto["preCS"]
+    rec_len = proto["csOff"] + proto["postCS"] - rec_from
+    bins = (rec_len + proto["binSteps"] - 1) // proto["binSteps"]
+    nd, rows = proto["numDataTrials"], rec_len // 32
+    out, off = {"psh": {}, "raster": {}}, 0
+
+    def take(n, dtype):
+        nonlocal off
+        a = rec[off: off + 4 * n].view(dtype)
+        off += 4 * n
+        return a
+
+    out["nc"] = take(nd * bins * num["NC"], np.uint32)
+    out["pc"] = take(nd * bins * num["PC"], np.uint32)
+    out["eye"] = take(nd * rec_len, np.float32)
+    out["gr"] = take(bins * num["GR"], np.float32).reshape(bins, num["GR"])
+    for name, cell in TRIAL_PSH + [("gr", None)]:
+        n = num[cell] if cell else num["GR"] // 10
+        out["psh"][name] = take(bins * n, np.float32).reshape(bins, n)
+    for name, cell in TRIAL_RASTER:
+        out["raster"][name] = take(nd * rows * num[cell], np.uint32).reshape(nd, rows, num[cell])
+    assert off == rec.size
+    return out
+
+
+def raster_rows_filled(proto):
+    """Rows of the trial-data rasters that a run of whole trials fills, in
+    (trial, row) order: one per 32nd window step after the first, so
+    (recLen - 1) // 32 per trial against recLen // 32 rows a raster trial."""
+    rec_len = proto["csOff"] + proto["postCS"] - (proto["csOn"] - proto["preCS"])
+    nd, rows = proto["numDataTrials"], rec_len // 32
+    return min(nd * rows, nd * ((rec_len - 1) // 32))
 
 
 def gr_psh_from_trace(trace, proto, n_gr):

@@ -89,32 +89,50 @@ def test_reference_sharded_path_equals_single(tmp_path, gpus):
 
 
 @pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
-def test_oracle_protocol_matches_reference_driver(tmp_path):
+@pytest.mark.parametrize("window", [dict(), dict(preCS=56, postCS=60)])
+def test_oracle_protocol_matches_reference_driver(tmp_path, window):
     """The oracle's eyelid driver (MF generation, US, plasticity window,
-    eyelid integrator, records) against the reference's PoissonRegenCells and
-    EyelidIntegrator driven in the order of ECManagementDelay, over 3 short
-    trials of the reference's 16K network."""
+    eyelid integrator, records) against the reference's PoissonRegenCells,
+    EyelidIntegrator and ECTrialsData driven in the order of
+    ECManagementDelay, over 3 short trials of the reference's 16K network.
+    The second window is 256 steps long: 7 raster updates a trial against 8
+    rows a raster trial, so the reference's raster trials drift across the
+    protocol's trials, and the oracle must drift the same way."""
     st = cbmtest.golden_state("ref16k", str(tmp_path))
-    proto = cbmtest.short_protocol()
+    proto = cbmtest.short_protocol(**window)
     o = Oracle(st, seeds=[7])
     rates = cbmtest.protocol_rates(o.num["MF"], seed=1)
     steps = 3 * proto["trialSteps"]
-    tr_o, nc, pc, eye = o.run_protocol(proto, rates, steps)
+    tr_o, nc, pc, eye, td = o.run_protocol(proto, rates, steps, trial_data=True)
     tr_r, rec_r = cbmtest.ref_run_protocol(st, proto, rates, steps, [7])
     assert tr_r.size == tr_o.size
     assert cbmtest.same_values(tr_r, tr_o.ravel()).all()
-    rec_o = np.concatenate([nc.view(np.uint8), pc.view(np.uint8), eye.view(np.uint8)])
-    gr_r = rec_r[rec_o.size:].view(np.float32)  # the reference's GR histogram follows
-    rec_r = rec_r[: rec_o.size]
-    assert cbmtest.same_values(rec_r.view(np.float32)[-eye.size:], eye).all()
-    assert np.array_equal(rec_r[: nc.nbytes + pc.nbytes], rec_o[: nc.nbytes + pc.nbytes])
+    r = cbmtest.split_ref_records(rec_r, o.num, proto)
+    assert cbmtest.same_values(r["eye"], eye).all()
+    assert np.array_equal(r["nc"], nc) and np.array_equal(r["pc"], pc)
     # the GR histogram rule the device follows, restated from the oracle's
-    # trace, equals the reference's PeriStimHistFloat
+    # trace, equals the reference's PeriStimHistFloat; the driver's own "gr"
+    # histogram covers the first numGR / 10 cells
     gr_o = cbmtest.gr_psh_from_trace(tr_o, proto, o.num["GR"])
-    assert gr_r.size == gr_o.size and gr_o.sum() > 0
-    assert np.array_equal(gr_r.reshape(gr_o.shape), gr_o.astype(np.float32))
-    # the protocol did something: CS trials spike NCs and move the eyelid
+    assert gr_o.sum() > 0
+    assert np.array_equal(r["gr"], gr_o.astype(np.float32))
+    assert np.array_equal(r["psh"]["gr"], r["gr"][:, : o.num["GR"] // 10])
+    # every ECTrialsData histogram, bit for bit (float sums included)
+    for name, _ in cbmtest.TRIAL_PSH:
+        assert cbmtest.same_values(r["psh"][name].ravel(), td["psh"][name].ravel()).all(), name
+    # the rasters, over the rows the run fills (the reference leaves the
+    # others as allocated)
+    filled = cbmtest.raster_rows_filled(proto)
+    for name, _ in cbmtest.TRIAL_RASTER:
+        a, b = r["raster"][name], td["raster"][name]
+        a, b = a.reshape(-1, a.shape[-1])[:filled], b.reshape(-1, b.shape[-1])
+        assert np.array_equal(a, b[:filled]), name
+        assert not b[filled:].any()
+    # the protocol did something: CS trials spike NCs, move the eyelid and
+    # fill the histograms and rasters
     assert nc.sum() > 0 and eye.max() > 0
+    assert all(td["psh"][n].any() for n in ("go", "grInputGO", "goOutSynScale", "mf", "sc", "pc"))
+    assert td["raster"]["go"].any() and td["raster"]["pc"].any()
 
 
 @pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
