@@ -43,6 +43,15 @@ def _field_dtype(name):
     return _FIELD_DTYPE[name.split("_")[0]]
 
 
+# ECTrialsData record kinds (CBM_REC_PSH_*, CBM_REC_RASTER_*) and the cells
+# each covers, under the eyelid driver's names
+TRIAL_PSH = {"go": (4, "numGO"), "grInputGO": (5, "numGO"), "goInputGO": (6, "numGO"),
+             "goOutSynScale": (7, "numGO"), "mf": (8, "numMF"), "sc": (9, "numSC"), "bc": (10, "numBC"),
+             "pc": (11, "numPC"), "io": (12, "numIO")}
+TRIAL_RASTER = {"go": (13, "numGO"), "sc": (14, "numSC"), "bc": (15, "numBC"), "pc": (16, "numPC"),
+                "nc": (17, "numNC"), "io": (18, "numIO")}
+
+
 class CBMError(RuntimeError):
     """A failed call of the C ABI; .code holds the CBM_ERR_* status."""
 
@@ -107,6 +116,7 @@ def _load():
         "cbm_sim_trial_record_bytes": (U64, [P, I]),
         "cbm_sim_trial_record": (I, [P, I, P, U64]),
         "cbm_sim_record_gr": (I, [P]),
+        "cbm_sim_record_trial_data": (I, [P]),
         "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_destroy": (None, [P]),
         "cbm_device_expf": (I, [I, P, P, U64]),
@@ -358,6 +368,28 @@ class CBMSimCore:
         """Record the running protocol's GR peri-stimulus histogram on the
         device from the next step on (cbm_sim_record_gr)."""
         _check(lib.cbm_sim_record_gr(self._h))
+
+    def record_trial_data(self):
+        """Record the running protocol's ECTrialsData histograms and rasters
+        on the device from the next step on (cbm_sim_record_trial_data)."""
+        _check(lib.cbm_sim_record_trial_data(self._h))
+
+    def trial_data(self):
+        """The ECTrialsData records (after record_trial_data):
+        {"psh": {name: f32 [bins, cells]}, "raster": {name: u32 [trials,
+        window steps // 32, cells]}} under the eyelid driver's names."""
+        out = {"psh": {}, "raster": {}}
+        for kinds, key, dtype in ((TRIAL_PSH, "psh", np.float32), (TRIAL_RASTER, "raster", np.uint32)):
+            for name, (k, cell) in kinds.items():
+                n = lib.cbm_sim_trial_record_bytes(self._h, k)
+                if not n:
+                    raise CBMError(1, "the trial data is not recorded")
+                a = np.empty(n // 4, dtype=dtype)
+                _check(lib.cbm_sim_trial_record(self._h, k, a.ctypes.data, n))
+                cells = self.state.con(cell)
+                out[key][name] = a.reshape(-1, cells) if key == "psh" else \
+                    a.reshape(self._protocol["numDataTrials"], -1, cells)
+        return out
 
     def trial_record(self, kind):
         """Records of the running protocol: 'nc' / 'pc' spike counts

@@ -358,6 +358,13 @@ int cbm_sim_record_gr(cbm_sim *sim)
 	return CBM_OK;
 }
 
+int cbm_sim_record_trial_data(cbm_sim *sim)
+{
+	NEED(sim);
+	TRY(sim->sim.recordTrialData());
+	return CBM_OK;
+}
+
 // ---------------------------------------------------------------- batches
 struct cbm_batch {
 	Simulator sim;

@@ -127,6 +127,11 @@ struct DevProtocol {
 	float *eyeG;           // [numNC] integrator conductances
 	float *eyeVm;          // [1]
 	uint16_t *grPSH;       // [nBins][numGR] GR spike counts of the kept trials, or null
+	// the eyelid driver's trial data, or null: histograms go, grInputGO,
+	// goInputGO, goOutSynScale, mf, sc, bc, pc, io, each f32 [nBins][cells];
+	// rasters go, sc, bc, pc, nc, io, each u32 [numDataTrials][recLen / 32][cells]
+	float *tdPSH;
+	uint32_t *tdRaster;
 	float eyeGDecay, eyeGInc, eyeGShift, eyeGLeak, eyeMaxAmp;
 };
 

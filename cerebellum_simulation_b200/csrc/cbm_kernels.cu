@@ -1736,6 +1736,89 @@ __global__ void grPSHKernel(const DevNet *N, uint32_t stepOffset)
 	*reinterpret_cast<uint4 *>(cnt) = c;
 }
 
+// The eyelid driver's trial data after step t (ecmanagementdelay.cpp:240-265,
+// ECTrialsData): in the window of a kept trial, every histogram adds the
+// step's value of each cell to the step's bin (PeriStimHistFloat::update,
+// peristimhistfloat.cpp: spikes as 1 or 0, counts and floats as they are, in
+// float, one add per step as the reference's), and at every 32nd window step
+// after the first each raster takes the cells' apBuf words into its next row
+// (SpikeRasterBitArray::updateRaster, spikerasterbitarray.cpp:62-80).  Rows
+// are counted over all updates: (recLen - 1) / 32 updates a trial against
+// recLen / 32 rows a raster trial.  One thread per cell; cells are GO, MF,
+// SC, then zone 0's BC, PC, IO and NC.
+__global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset)
+{
+	const DevProtocol *P = N->proto;
+	const uint64_t t = stepsDone(N) + 1 + stepOffset;
+	if (!P || !P->tdPSH || t < P->startT + 1) return;
+	const uint64_t k = t - 1 - P->startT;
+	const int32_t time = (int32_t)(k % P->trialSteps);
+	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const int32_t ct = time - P->recFrom;
+	if (trial < P->dataStartTrial || trial >= P->dataStartTrial + P->numDataTrials || ct < 0 || ct >= P->recLen)
+		return;
+	const uint32_t nGO = N->numGO, nMF = N->numMF, nSC = N->numSC, nBC = N->numBC, nPC = N->numPC;
+	const uint32_t nIO = N->numIO, nNC = N->numNC;
+	const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= nGO + nMF + nSC + nBC + nPC + nIO + nNC) return;
+	const DevZone &Z = N->zones[0];
+	const size_t B = P->nBins, bin = (uint32_t)ct / P->binSteps;
+	// histogram bases: go, grInputGO, goInputGO, goOutSynScale, mf, sc, bc, pc, io
+	float *const hGO = P->tdPSH, *const hMF = hGO + 4 * B * nGO, *const hSC = hMF + B * nMF;
+	float *const hBC = hSC + B * nSC, *const hPC = hBC + B * nBC, *const hIO = hPC + B * nPC;
+	// raster row of this step: rt * rows + row within each raster, or none
+	const uint32_t rows = (uint32_t)P->recLen / 32;
+	uint64_t rrow = ~0ull;
+	if (rows && ct > 0 && ct % 32 == 0) {
+		const uint64_t u = (uint64_t)(trial - P->dataStartTrial) * (uint32_t)((P->recLen - 1) / 32) + (uint32_t)ct / 32 - 1;
+		if (u < (uint64_t)P->numDataTrials * rows) rrow = u;
+	}
+	const size_t R = (size_t)P->numDataTrials * rows;
+	uint32_t *const rGO = P->tdRaster, *const rSC = rGO + R * nGO, *const rBC = rSC + R * nSC;
+	uint32_t *const rPC = rBC + R * nBC, *const rNC = rPC + R * nPC, *const rIO = rNC + R * nNC;
+	uint32_t i = c;
+	if (i < nGO) {
+		float *h = hGO + bin * nGO + i;
+		h[0] += (float)(N->apGO[i] > 0);
+		h[B * nGO] += (float)N->sumGRInputGO[i];
+		h[2 * B * nGO] += N->sumInputGOGABASynDepGO[i];
+		h[3 * B * nGO] += N->goGABAOutSynScaleGOGO[i];
+		if (rrow != ~0ull) rGO[rrow * nGO + i] = N->apBufGO[i];
+		return;
+	}
+	i -= nGO;
+	if (i < nMF) {
+		hMF[bin * nMF + i] += (float)(N->apBufMF[i] & 1u);  // this step's MF spike
+		return;
+	}
+	i -= nMF;
+	if (i < nSC) {
+		hSC[bin * nSC + i] += (float)(N->apSC[i] > 0);
+		if (rrow != ~0ull) rSC[rrow * nSC + i] = N->apBufSC[i];
+		return;
+	}
+	i -= nSC;
+	if (i < nBC) {
+		hBC[bin * nBC + i] += (float)(Z.apBC[i] > 0);
+		if (rrow != ~0ull) rBC[rrow * nBC + i] = Z.apBufBC[i];
+		return;
+	}
+	i -= nBC;
+	if (i < nPC) {
+		hPC[bin * nPC + i] += (float)(Z.apPC[i] > 0);
+		if (rrow != ~0ull) rPC[rrow * nPC + i] = Z.apBufPC[i];
+		return;
+	}
+	i -= nPC;
+	if (i < nIO) {
+		hIO[bin * nIO + i] += (float)(Z.apIO[i] > 0);
+		if (rrow != ~0ull) rIO[rrow * nIO + i] = Z.apBufIO[i];
+		return;
+	}
+	i -= nIO;
+	if (rrow != ~0ull) rNC[rrow * nNC + i] = Z.apBufNC[i];
+}
+
 // Prepare the first step of a newly set protocol (the network's step tBase + 1).
 __global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet *N)
 {

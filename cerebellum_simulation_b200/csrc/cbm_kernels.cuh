@@ -35,6 +35,7 @@ __global__ void protocolPrimeKernel(const DevNet *N);
 // GR peri-stimulus histogram of step t = stepsDone(N) + 1 + stepOffset, after
 // the GR pass of that step: 8 GR per thread.
 __global__ void grPSHKernel(const DevNet *N, uint32_t stepOffset);
+__global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);
 __global__ void expfProbeKernel(const float *in, float *out, uint32_t n);

@@ -804,8 +804,52 @@ size_t Network::recordBytes(int kind) const
 	case CBM_REC_PC_PSH: return 4 * nd * hProto_.nBins * h_.numPC;
 	case CBM_REC_EYELID: return 4 * nd * (size_t)hProto_.recLen;
 	case CBM_REC_GR_PSH: return hProto_.grPSH ? 2ull * hProto_.nBins * h_.numGR : 0;
-	default: return 0;
+	default: break;
 	}
+	size_t off, n;
+	return trialDataRecord(kind, &off, &n) ? 4 * n : 0;
+}
+
+// Where a trial-data record sits in its buffer (elements), or false for
+// another kind or while the trial data is not recorded.
+bool Network::trialDataRecord(int kind, size_t *offset, size_t *count) const
+{
+	if (!hProto_.tdPSH) return false;
+	const size_t B = hProto_.nBins, R = (size_t)hProto_.numDataTrials * ((uint32_t)hProto_.recLen / 32);
+	const uint32_t psh[9] = {h_.numGO, h_.numGO, h_.numGO, h_.numGO, h_.numMF, h_.numSC, h_.numBC, h_.numPC, h_.numIO};
+	const uint32_t raster[6] = {h_.numGO, h_.numSC, h_.numBC, h_.numPC, h_.numNC, h_.numIO};
+	size_t off = 0;
+	if (kind >= CBM_REC_PSH_GO && kind <= CBM_REC_PSH_IO) {
+		for (int k = 0; k < kind - CBM_REC_PSH_GO; k++) off += B * psh[k];
+		*offset = off;
+		*count = B * psh[kind - CBM_REC_PSH_GO];
+		return true;
+	}
+	if (kind >= CBM_REC_RASTER_GO && kind <= CBM_REC_RASTER_IO) {
+		for (int k = 0; k < kind - CBM_REC_RASTER_GO; k++) off += R * raster[k];
+		*offset = off;
+		*count = R * raster[kind - CBM_REC_RASTER_GO];
+		return true;
+	}
+	return false;
+}
+
+std::string Network::recordTrialData(cudaStream_t s)
+{
+	if (!h_.proto) return "the trial data records a running protocol: set one first";
+	if (hProto_.tdPSH) return "";
+	if (hProto_.recLen < 32) return "the recording window must be at least 32 steps for the trial-data rasters";
+	const size_t B = hProto_.nBins, R = (size_t)hProto_.numDataTrials * ((uint32_t)hProto_.recLen / 32);
+	const size_t nPSH = B * (4ull * h_.numGO + h_.numMF + h_.numSC + h_.numBC + h_.numPC + h_.numIO);
+	const size_t nRaster = R * ((size_t)h_.numGO + h_.numSC + h_.numBC + h_.numPC + h_.numNC + h_.numIO);
+	float *psh = alloc<float>(nPSH);  // zeroed
+	uint32_t *raster = alloc<uint32_t>(std::max<size_t>(1, nRaster));
+	if (!psh || !raster) return "device allocation failed";
+	hProto_.tdPSH = psh;
+	hProto_.tdRaster = raster;
+	CK(cudaMemcpyAsync(h_.proto, &hProto_, sizeof(DevProtocol), cudaMemcpyHostToDevice, s), "uploading the protocol");
+	CK(cudaStreamSynchronize(s), "uploading the protocol");
+	return "";
 }
 
 std::string Network::recordGR(cudaStream_t s)
@@ -828,9 +872,14 @@ std::string Network::readRecord(int kind, void *dst, size_t bytes, cudaStream_t 
 	const size_t need = recordBytes(kind);
 	if (!need) return "unknown record kind";
 	if (bytes != need) return "record size mismatch";
+	size_t off = 0, n = 0;
 	const void *src = kind == CBM_REC_NC_PSH ? (const void *)hProto_.ncPSH
 		: kind == CBM_REC_PC_PSH ? (const void *)hProto_.pcPSH
-		: kind == CBM_REC_GR_PSH ? (const void *)hProto_.grPSH : (const void *)hProto_.eyelid;
+		: kind == CBM_REC_GR_PSH ? (const void *)hProto_.grPSH
+		: kind == CBM_REC_EYELID ? (const void *)hProto_.eyelid
+		: !trialDataRecord(kind, &off, &n) ? nullptr
+		: kind <= CBM_REC_PSH_IO ? (const void *)(hProto_.tdPSH + off) : (const void *)(hProto_.tdRaster + off);
+	if (!src) return "unknown record kind";
 	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "reading a record");
 	CK(cudaStreamSynchronize(s), "reading a record");
 	return "";
@@ -1290,7 +1339,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
 		CK(cudaEventRecord(join_, s1_), "join");
 		CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
-		return recordStepGR(k);
+		return recordStep(k);
 	}
 	// One stream: the small-cell CTAs launch first and let the GR pass start
 	// as soon as they are resident (programmatic dependent launch; the two
@@ -1301,16 +1350,25 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	CK(cudaEventRecord(join_, s0_), "join");
 	CKS(launchPass(s0_, true));
 	CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
-	return recordStepGR(k);
+	return recordStep(k);
 }
 
-std::string Simulator::recordStepGR(uint32_t k)
+std::string Simulator::recordStep(uint32_t k)
 {
-	// after both kernels of the step: its GR spikes into the histogram
-	if (nets_.size() != 1 || !nets_[0]->recordsGR()) return "";
-	const uint32_t threads = (nets_[0]->dev().numGR + 7) / 8;
-	grPSHKernel<<<(threads + 255) / 256, 256, 0, s0_>>>(nets_[0]->devPtr(), k);
-	CK(cudaGetLastError(), "launching the GR histogram");
+	// after both kernels of the step: its GR spikes into the histogram, and
+	// its small-cell state into the trial data
+	if (nets_.size() != 1) return "";
+	const DevNet &h = nets_[0]->dev();
+	if (nets_[0]->recordsGR()) {
+		const uint32_t threads = (h.numGR + 7) / 8;
+		grPSHKernel<<<(threads + 255) / 256, 256, 0, s0_>>>(nets_[0]->devPtr(), k);
+		CK(cudaGetLastError(), "launching the GR histogram");
+	}
+	if (nets_[0]->recordsTrialData()) {
+		const uint32_t cells = h.numGO + h.numMF + h.numSC + h.numBC + h.numPC + h.numIO + h.numNC;
+		trialDataKernel<<<(cells + 255) / 256, 256, 0, s0_>>>(nets_[0]->devPtr(), k);
+		CK(cudaGetLastError(), "launching the trial-data record");
+	}
 	return "";
 }
 
@@ -1399,6 +1457,17 @@ std::string Simulator::recordGR()
 	const bool was = nets_[0]->recordsGR();
 	CKS(nets_[0]->recordGR(s0_));
 	if (!was) dropGraphs();  // the step graphs gain the histogram kernel
+	return "";
+}
+
+std::string Simulator::recordTrialData()
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	if (nets_.size() != 1) return "the trial data is recorded for single-network simulators";
+	CK(cudaStreamSynchronize(s0_), "sync");
+	const bool was = nets_[0]->recordsTrialData();
+	CKS(nets_[0]->recordTrialData(s0_));
+	if (!was) dropGraphs();  // the step graphs gain the trial-data kernel
 	return "";
 }
 

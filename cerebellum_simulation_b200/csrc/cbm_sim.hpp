@@ -65,6 +65,7 @@ public:
 	std::string setProtocol(size_t i, const cbm_eyelid_protocol &p);
 	// Record network 0's GR peri-stimulus histogram (single-network simulators).
 	std::string recordGR();
+	std::string recordTrialData();
 	// Run nsteps as CUDA-graph chunks of chunk steps (inputs resident in HBM).
 	// With instrument, external events around every GR pass of the chunk
 	// give lastPassMs(): the pass's mean duration over the last replay.
@@ -111,7 +112,7 @@ private:
 	friend class Network;
 	std::string uploadCtl();
 	std::string enqueueStep(uint32_t stepOffset, bool instrument);
-	std::string recordStepGR(uint32_t stepOffset);
+	std::string recordStep(uint32_t stepOffset);
 	void dropGraphs();
 	void markInputSlotsFree();  // after a full synchronisation
 	// Issue the copy of MF input that a single-step graph would have carried.
@@ -176,6 +177,9 @@ public:
 	// Allocate and start the protocol's GR peri-stimulus histogram.
 	std::string recordGR(cudaStream_t s);
 	bool recordsGR() const { return hProto_.grPSH != nullptr; }
+	std::string recordTrialData(cudaStream_t s);
+	bool recordsTrialData() const { return hProto_.tdPSH != nullptr; }
+	bool trialDataRecord(int kind, size_t *offset, size_t *count) const;
 	bool hasProtocol() const { return h_.proto != nullptr; }
 	size_t recordBytes(int kind) const;
 	std::string readRecord(int kind, void *dst, size_t bytes, cudaStream_t s);

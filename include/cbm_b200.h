@@ -232,7 +232,30 @@ enum {
 	CBM_REC_NC_PSH = 0,  /* u32 [numDataTrials][bins][numNC] */
 	CBM_REC_PC_PSH = 1,  /* u32 [numDataTrials][bins][numPC] */
 	CBM_REC_EYELID = 2,  /* f32 [numDataTrials][window steps] */
-	CBM_REC_GR_PSH = 3   /* u16 [bins][numGR], summed over the kept trials (cbm_sim_record_gr) */
+	CBM_REC_GR_PSH = 3,  /* u16 [bins][numGR], summed over the kept trials (cbm_sim_record_gr) */
+	/* The eyelid driver's ECTrialsData records (cbm_sim_record_trial_data).
+	 * Histograms: f32 [bins][cells] summed over the kept trials, as
+	 * PeriStimHistFloat holds them. */
+	CBM_REC_PSH_GO = 4,             /* GO spikes */
+	CBM_REC_PSH_GR_INPUT_GO = 5,    /* GR->GO input counts (exportSumGRInputGO) */
+	CBM_REC_PSH_GO_INPUT_GO = 6,    /* GO->GO input (exportSumGOInputGO) */
+	CBM_REC_PSH_GO_OUT_SCALE = 7,   /* GO->GO output scale (exportGOOutSynScaleGOGO) */
+	CBM_REC_PSH_MF = 8,             /* MF spikes */
+	CBM_REC_PSH_SC = 9,
+	CBM_REC_PSH_BC = 10,            /* zone 0 */
+	CBM_REC_PSH_PC = 11,            /* zone 0 */
+	CBM_REC_PSH_IO = 12,            /* zone 0 */
+	/* Rasters: u32 [numDataTrials][window steps / 32][cells], the cells' apBuf
+	 * words at every 32nd window step after the first, as SpikeRasterBitArray
+	 * holds them: rows are counted over all updates, so when the window is a
+	 * multiple of 32 steps its rows drift across trials as the reference's
+	 * do; rows no update reached stay zero. */
+	CBM_REC_RASTER_GO = 13,
+	CBM_REC_RASTER_SC = 14,
+	CBM_REC_RASTER_BC = 15,         /* zone 0 */
+	CBM_REC_RASTER_PC = 16,         /* zone 0 */
+	CBM_REC_RASTER_NC = 17,         /* zone 0 */
+	CBM_REC_RASTER_IO = 18          /* zone 0 */
 };
 
 /* Start a device protocol on network 0 of the simulator (no counterpart in
@@ -252,6 +275,14 @@ int cbm_sim_trial_record(cbm_sim *sim, int kind, void *dst, uint64_t bytes);
  * Needs a protocol, and binSteps x numDataTrials of at most 65535; the
  * counts start at zero. */
 int cbm_sim_record_gr(cbm_sim *sim);
+/* Record the running protocol's ECTrialsData histograms and rasters
+ * (CBM_REC_PSH_* and CBM_REC_RASTER_*) on the device from the next step on,
+ * as the eyelid driver fills them after each step of the window of a kept
+ * trial (Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:240-265,
+ * CBM_DATA_LIB_DEV/src/interfaces/ectrialsdata.cpp): one small kernel after
+ * each step instead of the per-step exports and host loops.  Needs a
+ * protocol whose window is at least 32 steps; the records start at zero. */
+int cbm_sim_record_trial_data(cbm_sim *sim);
 
 /* ---- Batched instances (no counterpart in the reference, which runs one
  * network per CBMSimCore).  n independent networks of any sizes, seeds and

@@ -108,3 +108,39 @@ def test_gr_histogram_matches_oracle_spikes(tmp_path):
         sim.close()
         assert got.dtype == np.uint16 and got.shape == want.shape
         assert np.array_equal(got.astype(np.uint32), want), f"replay={replay}"
+
+
+@pytest.mark.parametrize("window,replay", [(dict(), True), (dict(preCS=56, postCS=60), False)])
+def test_trial_data_matches_oracle(tmp_path, window, replay):
+    """The device ECTrialsData records (cbm_sim_record_trial_data), recorded
+    together with the GR histogram, equal the oracle's (pinned to the
+    reference's ECTrialsData in test_oracle_pin.py) bit for bit: every
+    histogram, float sums included, and every raster, under graph replay and
+    step by step; the 256-step window makes the raster trials drift."""
+    import cerebellum_simulation_b200 as cbm
+    st_path = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol(**window)
+    st = cbm.CBMState(st_path)
+    rates = cbmtest.protocol_rates(st.con("numMF"), seed=1)
+    steps = 3 * proto["trialSteps"]
+    o = Oracle(st_path, seeds=[7])
+    tr, _, _, _, want = o.run_protocol(proto, rates, steps, trial_data=True)
+    sim = cbm.CBMSimCore(cbm.CBMState(st_path), [7], device=0)
+    sim.set_eyelid_protocol(rates, **proto)
+    sim.record_gr()
+    sim.record_trial_data()
+    if replay:
+        sim.run(steps, chunk=100)
+    else:
+        for _ in range(steps):
+            sim.calcActivity()
+    got = sim.trial_data()
+    gr = sim.trial_record("gr")
+    sim.close()
+    for name, a in want["psh"].items():
+        assert got["psh"][name].shape == a.shape, name
+        assert cbmtest.same_values(got["psh"][name].ravel(), a.ravel()).all(), name
+    for name, a in want["raster"].items():
+        assert np.array_equal(got["raster"][name], a), name
+    assert np.array_equal(gr.astype(np.uint32), cbmtest.gr_psh_from_trace(tr, proto, st.con("numGR")))
+    assert want["psh"]["go"].any() and want["raster"]["go"].any() and want["psh"]["mf"].any()
