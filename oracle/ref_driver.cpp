@@ -28,7 +28,13 @@
  *       CBM_DATA_LIB_DEV/src/peristimhist/peristimhistfloat.cpp, updated with
  *       exportAPGR as the eyelid driver does,
  *       Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:262) as
- *       f32 [bins][numGR] (MFBYTES is then ignored).  PROTOCOL is "key value" text: trialSteps,
+ *       f32 [bins][numGR], then the reference's ECTrialsData
+ *       (CBM_DATA_LIB_DEV/src/interfaces/ectrialsdata.cpp) built and filled
+ *       as the eyelid driver does (ecmanagementdelay.cpp:107-156, 240-265):
+ *       its histograms go, grInputGO, goInputGO, goOutSynScale, mf, sc, bc,
+ *       pc, io, gr (numGR / 10 cells) as f32 [bins][cells], and its rasters
+ *       go, sc, bc, pc, nc, io as u32 [numDataTrials][window / 32][cells]
+ *       (MFBYTES is then ignored).  PROTOCOL is "key value" text: trialSteps,
  *       csOn, csOff, csPhasicOff, csStartTrial, plastOnDelay, plastOffDelay,
  *       plastLTD, plastLTP, usErrDrive, mfSeed, mfThreshDecayTau, rates (a file
  *       of 3 x numMF f32: background, CS tonic, CS phasic), dataStartTrial,
