@@ -351,3 +351,64 @@ def uniform_mf_stream(num_mf, steps, seed=0, lo=1.0, hi=30.0):
     rates = rng.uniform(lo, hi, num_mf).astype(np.float32)
     gen = RegenPoissonMF(num_mf, seed)
     return gen.run(lambda t: rates, steps)
+
+
+class MFPopulation:
+    """MF rate tables of an eyelid protocol in the reference's ECMFPopulation
+    form (CBM_TOOLS_LIB_DEV/src/ecmfpopulation.cpp): background, CS-tonic and
+    CS-phasic Hz per fibre.  ``rates()`` is what set_eyelid_protocol takes.
+
+    Tables the reference's tools library generates can be read from its file
+    (``read``; writeToFile's layout: i32 numMF, then the three f32 tables), and
+    ``from_trial_data`` re-estimates the tables from a recorded MF histogram
+    as the reference's ECMFPopulation(ECTrialsData *) does."""
+
+    def __init__(self, bg, cs_tonic, cs_phasic):
+        self.bg = np.ascontiguousarray(bg, dtype=np.float32)
+        self.cs_tonic = np.ascontiguousarray(cs_tonic, dtype=np.float32)
+        self.cs_phasic = np.ascontiguousarray(cs_phasic, dtype=np.float32)
+
+    def rates(self):
+        """[3, numMF] Hz: background, CS tonic, CS phasic."""
+        return np.stack([self.bg, self.cs_tonic, self.cs_phasic])
+
+    @classmethod
+    def read(cls, path):
+        """ECMFPopulation(fstream &) (ecmfpopulation.cpp:192-211)."""
+        with open(path, "rb") as f:
+            n = int(np.frombuffer(f.read(4), np.int32)[0])
+            t = np.frombuffer(f.read(12 * n), np.float32)
+        if t.size != 3 * n:
+            raise ValueError(f"{path}: truncated MF population file")
+        return cls(t[:n], t[n: 2 * n], t[2 * n:])
+
+    def write(self, path):
+        """ECMFPopulation::writeToFile (ecmfpopulation.cpp:220-235)."""
+        with open(path, "wb") as f:
+            f.write(np.int32(self.bg.size).tobytes())
+            for a in (self.bg, self.cs_tonic, self.cs_phasic):
+                f.write(a.tobytes())
+
+    @classmethod
+    def from_trial_data(cls, mf_psh, num_trials, bin_steps, pre_cs, cs_ms):
+        """ECMFPopulation(ECTrialsData *) (ecmfpopulation.cpp:11-65) from the
+        MF histogram f32 [bins][numMF] of num_trials recorded trials, binned
+        by bin_steps, with pre_cs ms before the CS and a CS of cs_ms: the mean
+        rate over the background bins [2, preBins - 2), the CS-phasic bins
+        [preBins + 1, preBins + 3) and the CS-tonic bins
+        [preBins + csBins - 6, preBins + csBins - 1), in float as the
+        reference sums them (bin by bin, then one divide).  As in the
+        reference, the bin width counts as milliseconds."""
+        f32 = np.float32
+        # float scaling = numTrials * (msPerBin / 1000.0): a double product stored as float
+        scaling = f32(num_trials * (bin_steps / 1000.0))
+        pre_bins, cs_bins = pre_cs // bin_steps, cs_ms // bin_steps
+        psh = np.asarray(mf_psh, dtype=np.float32)
+
+        def mean(lo, hi, count):
+            s = np.zeros(psh.shape[1], np.float32)
+            for j in range(lo, hi):
+                s = (s + psh[j]).astype(np.float32)
+            return (s / (f32(count) * scaling)).astype(np.float32)
+        return cls(mean(2, pre_bins - 2, pre_bins - 4), mean(pre_bins + cs_bins - 6, pre_bins + cs_bins - 1, 5),
+                   mean(pre_bins + 1, pre_bins + 3, 2))

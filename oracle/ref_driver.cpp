@@ -34,7 +34,9 @@
  *       its histograms go, grInputGO, goInputGO, goOutSynScale, mf, sc, bc,
  *       pc, io, gr (numGR / 10 cells) as f32 [bins][cells], and its rasters
  *       go, sc, bc, pc, nc, io as u32 [numDataTrials][window / 32][cells]
- *       (MFBYTES is then ignored).  PROTOCOL is "key value" text: trialSteps,
+ *       (MFBYTES is then ignored).  -m MFPOP then writes the
+ *       reference's ECMFPopulation estimated from that ECTrialsData
+ *       (CBM_TOOLS_LIB_DEV/src/ecmfpopulation.cpp:11-65) with writeToFile.  PROTOCOL is "key value" text: trialSteps,
  *       csOn, csOff, csPhasicOff, csStartTrial, plastOnDelay, plastOffDelay,
  *       plastLTD, plastLTP, usErrDrive, mfSeed, mfThreshDecayTau, rates (a file
  *       of 3 x numMF f32: background, CS tonic, CS phasic), dataStartTrial,
@@ -75,6 +77,7 @@
 #include <CBMToolsInclude/eyelidintegrator.h>
 #include <CBMDataInclude/peristimhist/peristimhistfloat.h>
 #include <CBMDataInclude/interfaces/ectrialsdata.h>
+#include <CBMToolsInclude/ecmfpopulation.h>
 uint64_t cbm_refshim_step = 0;
 void cbm_refshim_set_step(uint64_t t) { cbm_refshim_step = t; }
 #endif
@@ -177,7 +180,7 @@ int main(int argc, char **argv)
 	const char *statePath = argv[1], *mfPath = argv[2], *tracePath = argv[4], *finalPath = argv[5];
 	unsigned long steps = strtoul(argv[3], NULL, 10);
 	std::vector<int> seeds;
-	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL;
+	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL, *mfPopPath = NULL;
 	int numGPUP2 = 0;
 	bool timeOnly = false;
 	unsigned long warm = 0;  // leading steps run before the clock starts
@@ -186,6 +189,7 @@ int main(int argc, char **argv)
 		if (!strcmp(argv[i], "-e") && i + 1 < argc) eventsPath = argv[++i];
 		else if (!strcmp(argv[i], "-p") && i + 1 < argc) protocolPath = argv[++i];
 		else if (!strcmp(argv[i], "-r") && i + 1 < argc) recordsPath = argv[++i];
+		else if (!strcmp(argv[i], "-m") && i + 1 < argc) mfPopPath = argv[++i];
 		else if (!strcmp(argv[i], "-g") && i + 1 < argc) numGPUP2 = atoi(argv[++i]);
 		else if (!strcmp(argv[i], "-t")) timeOnly = true;
 		else if (!strcmp(argv[i], "-w") && i + 1 < argc) warm = strtoul(argv[++i], NULL, 10);
@@ -439,6 +443,14 @@ int main(int argc, char **argv)
 			put(f, w.data(), w.size());
 		}
 		fclose(f);
+		if (mfPopPath)
+		{
+			// the MF rates the reference estimates from the run's MF histogram
+			// (ECMFPopulation(ECTrialsData *), ecmfpopulation.cpp:11-65), in its file format
+			ECMFPopulation pop(data);
+			std::fstream pf(mfPopPath, std::ios::out | std::ios::binary | std::ios::trunc);
+			pop.writeToFile(pf);
+		}
 		delete data;
 		delete grPSH;
 		delete mfs;

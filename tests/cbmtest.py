@@ -203,8 +203,10 @@ def protocol_rates(num_mf, seed=0):
     return np.stack([bg, tonic, phasic])
 
 
-def ref_run_protocol(state_path, proto, rates, nsteps, seeds):
-    """oracle/_ref/ref_run in protocol mode: (trace, ncPSH, pcPSH, eyelid)."""
+def ref_run_protocol(state_path, proto, rates, nsteps, seeds, mf_population=None):
+    """oracle/_ref/ref_run in protocol mode: (trace bytes, records bytes).
+    With mf_population (a path), the reference's ECMFPopulation estimated
+    from the run's ECTrialsData is written there."""
     with tempfile.TemporaryDirectory() as d:
         rp = os.path.join(d, "rates.f32")
         np.ascontiguousarray(rates, dtype=np.float32).tofile(rp)
@@ -215,6 +217,8 @@ def ref_run_protocol(state_path, proto, rates, nsteps, seeds):
             f.write(f"rates {rp}\n")
         trp, rec = os.path.join(d, "trace.bin"), os.path.join(d, "records.bin")
         cmd = [REF_RUN, state_path, "-", str(nsteps), trp, "-"] + [str(s) for s in seeds] + ["-p", pp, "-r", rec]
+        if mf_population:
+            cmd += ["-m", mf_population]
         subprocess.run(cmd, check=True, capture_output=True)
         return np.fromfile(trp, dtype=np.uint8), np.fromfile(rec, dtype=np.uint8)
 

@@ -157,3 +157,31 @@ def test_oracle_matches_reference_two_zones(tmp_path):
     fin = str(tmp_path / "oracle_final.state")
     o.save(fin)
     assert open(fin, "rb").read() == open(fin_ref, "rb").read()
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+def test_mf_population_estimate_matches_reference(tmp_path):
+    """networks.MFPopulation.from_trial_data over the oracle's MF histogram
+    equals the reference's ECMFPopulation(ECTrialsData *) over its own, bit
+    for bit, and MFPopulation reads and writes the reference's file byte for
+    byte."""
+    from cerebellum_simulation_b200 import networks
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol()
+    o = Oracle(st, seeds=[7])
+    rates = cbmtest.protocol_rates(o.num["MF"], seed=1)
+    steps = 3 * proto["trialSteps"]
+    _, _, _, _, td = o.run_protocol(proto, rates, steps, record=False, trial_data=True)
+    ref_path = str(tmp_path / "ref.mfpop")
+    cbmtest.ref_run_protocol(st, proto, rates, steps, [7], mf_population=ref_path)
+    ref = networks.MFPopulation.read(ref_path)
+    got = networks.MFPopulation.from_trial_data(td["psh"]["mf"], proto["numDataTrials"], proto["binSteps"],
+                                                proto["preCS"], proto["csOff"] - proto["csOn"])
+    for a, b in ((got.bg, ref.bg), (got.cs_tonic, ref.cs_tonic), (got.cs_phasic, ref.cs_phasic)):
+        assert cbmtest.same_values(a, b).all()
+    # the estimate follows the rates the fibres were driven with (60 ms of
+    # background per fibre, so only roughly)
+    assert np.corrcoef(got.bg, rates[0])[0, 1] > 0.3 and got.cs_phasic.mean() > got.bg.mean()
+    out = str(tmp_path / "rt.mfpop")
+    ref.write(out)
+    assert open(out, "rb").read() == open(ref_path, "rb").read()
