@@ -373,6 +373,40 @@ class MFPopulation:
         return np.stack([self.bg, self.cs_tonic, self.cs_phasic])
 
     @classmethod
+    def random(cls, num_mf, seed, frac_cs_tonic, frac_cs_phasic, frac_context,
+               bg_min, cs_bg_min, context_min, cs_tonic_min, cs_phasic_min,
+               bg_max, cs_bg_max, context_max, cs_tonic_max, cs_phasic_max):
+        """ECMFPopulation(numMF, randSeed, fracCSTMF, ...) (ecmfpopulation.cpp:
+        67-190), the parameters in its order: every fibre starts at a uniform
+        background rate; distinct CS-tonic, then CS-phasic, then context
+        fibres are picked (int(frac x numMF) of each, in float as the
+        reference counts them); context fibres get one context rate for all
+        three tables, CS fibres a CS-background rate plus a CS-tonic
+        (tonic fibres, used in both CS tables) or CS-phasic rate (phasic
+        fibres, phasic table only).  The draws come from the package's
+        generator, not the reference's SFMT stream, which the eyelid driver
+        seeds with the wall clock (mainw.cpp:208)."""
+        f32 = np.float32
+        rng = np.random.Generator(np.random.PCG64(seed + 404))
+
+        def u(lo, hi, n):
+            return (rng.random(n) * (f32(hi) - f32(lo)) + f32(lo)).astype(np.float32)
+        bg = u(bg_min, bg_max, num_mf)
+        tonic, phasic = bg.copy(), bg.copy()
+        n_t, n_p, n_c = (int(f32(f) * f32(num_mf)) for f in (frac_cs_tonic, frac_cs_phasic, frac_context))
+        if n_t + n_p + n_c > num_mf:
+            raise ValueError("the CS-tonic, CS-phasic and context fractions add up to more than every fibre")
+        order = rng.permutation(num_mf)
+        t_idx, p_idx, c_idx = order[:n_t], order[n_t: n_t + n_p], order[n_t + n_p: n_t + n_p + n_c]
+        bg[c_idx] = u(context_min, context_max, n_c)
+        tonic[c_idx] = phasic[c_idx] = bg[c_idx]
+        bg[t_idx] = u(cs_bg_min, cs_bg_max, n_t)
+        tonic[t_idx] = phasic[t_idx] = u(cs_tonic_min, cs_tonic_max, n_t)
+        bg[p_idx] = tonic[p_idx] = u(cs_bg_min, cs_bg_max, n_p)
+        phasic[p_idx] = u(cs_phasic_min, cs_phasic_max, n_p)
+        return cls(bg, tonic, phasic)
+
+    @classmethod
     def read(cls, path):
         """ECMFPopulation(fstream &) (ecmfpopulation.cpp:192-211)."""
         with open(path, "rb") as f:

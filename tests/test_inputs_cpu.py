@@ -64,3 +64,21 @@ def test_reference_arm_prints_one_contract_line():
     assert d["value"] > 0 and d["warmup"] == 3
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
+
+
+def test_random_mf_population_follows_the_reference_rules():
+    """MFPopulation.random: the category counts and rate ranges of the
+    reference's ECMFPopulation random constructor (ecmfpopulation.cpp:67-190)."""
+    p = networks.MFPopulation.random(1024, 3, 0.05, 0.03, 0.1, 1, 2, 30, 60, 110, 10, 5, 40, 80, 150)
+    bg, t, ph = p.bg, p.cs_tonic, p.cs_phasic
+    tonic = (t != bg) & (t == ph)
+    phasic = (ph != bg) & (t == bg)
+    context = (bg >= 30) & (t == bg) & (ph == bg)
+    assert tonic.sum() == int(np.float32(0.05) * np.float32(1024)) == 51
+    assert phasic.sum() == 30 and context.sum() == 102
+    assert np.all((t[tonic] >= 60) & (t[tonic] < 80)) and np.all((ph[phasic] >= 110) & (ph[phasic] < 150))
+    assert np.all((bg[tonic | phasic] >= 2) & (bg[tonic | phasic] < 5))
+    plain = ~(tonic | phasic | context)
+    assert np.all((bg[plain] >= 1) & (bg[plain] < 10))
+    q = networks.MFPopulation.random(1024, 3, 0.05, 0.03, 0.1, 1, 2, 30, 60, 110, 10, 5, 40, 80, 150)
+    assert np.array_equal(q.rates(), p.rates())
