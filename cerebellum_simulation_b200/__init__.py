@@ -52,6 +52,27 @@ TRIAL_RASTER = {"go": (13, "numGO"), "sc": (14, "numSC"), "bc": (15, "numBC"), "
                 "nc": (17, "numNC"), "io": (18, "numIO")}
 
 
+def eyelid_out(raw, num_ts_smooth=4):
+    """The eyelid driver's recorded eyelid trace (EyelidOut::updateData,
+    CBM_DATA_LIB_DEV/src/outdata/eyelidout.cpp) from the integrator's raw
+    output [trials, window steps]: the first num_ts_smooth - 1 values as
+    they are, then each value the float mean of the previous num_ts_smooth -
+    1 recorded (already smoothed) values and the new one, summed in order."""
+    raw = np.atleast_2d(np.asarray(raw, dtype=np.float32))
+    out = np.zeros_like(raw)
+    n = int(num_ts_smooth)
+    for ts in range(raw.shape[1]):
+        if ts < n - 1:
+            out[:, ts] = raw[:, ts]
+            continue
+        avg = np.zeros(raw.shape[0], np.float32)
+        for j in range(-(n - 1), 0):
+            avg = (avg + out[:, ts + j]).astype(np.float32)
+        avg = (avg + raw[:, ts]).astype(np.float32)
+        out[:, ts] = (avg / np.float32(n)).astype(np.float32)
+    return out
+
+
 class CBMError(RuntimeError):
     """A failed call of the C ABI; .code holds the CBM_ERR_* status."""
 
@@ -377,8 +398,10 @@ class CBMSimCore:
     def trial_data(self):
         """The ECTrialsData records (after record_trial_data):
         {"psh": {name: f32 [bins, cells]}, "raster": {name: u32 [trials,
-        window steps // 32, cells]}} under the eyelid driver's names."""
-        out = {"psh": {}, "raster": {}}
+        window steps // 32, cells]}, "eyelid": f32 [trials, window steps]}
+        under the eyelid driver's names; "eyelid" is the driver's smoothed
+        trace (eyelid_out of the raw integrator output)."""
+        out = {"psh": {}, "raster": {}, "eyelid": eyelid_out(self.trial_record("eyelid"))}
         for kinds, key, dtype in ((TRIAL_PSH, "psh", np.float32), (TRIAL_RASTER, "raster", np.uint32)):
             for name, (k, cell) in kinds.items():
                 n = lib.cbm_sim_trial_record_bytes(self._h, k)

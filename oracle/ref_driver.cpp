@@ -33,8 +33,9 @@
  *       as the eyelid driver does (ecmanagementdelay.cpp:107-156, 240-265):
  *       its histograms go, grInputGO, goInputGO, goOutSynScale, mf, sc, bc,
  *       pc, io, gr (numGR / 10 cells) as f32 [bins][cells], and its rasters
- *       go, sc, bc, pc, nc, io as u32 [numDataTrials][window / 32][cells]
- *       (MFBYTES is then ignored).  -m MFPOP then writes the
+ *       go, sc, bc, pc, nc, io as u32 [numDataTrials][window / 32][cells],
+ *       and its smoothed eyelid trace (EyelidOut) as f32
+ *       [numDataTrials][window] (MFBYTES is then ignored).  -m MFPOP then writes the
  *       reference's ECMFPopulation estimated from that ECTrialsData
  *       (CBM_TOOLS_LIB_DEV/src/ecmfpopulation.cpp:11-65) with writeToFile.  PROTOCOL is "key value" text: trialSteps,
  *       csOn, csOff, csPhasicOff, csStartTrial, plastOnDelay, plastOffDelay,
@@ -441,6 +442,12 @@ int main(int argc, char **argv)
 						if (aps[i]) w[((size_t)tr2 * rows + ts / 32) * n + i] |= 0x80000000u >> (ts % 32);
 				}
 			put(f, w.data(), w.size());
+		}
+		// the driver's smoothed eyelid trace (EyelidOut, eyelidout.cpp), [numDataTrials][window]
+		for (unsigned int tr2 = 0; tr2 < numDataT; tr2++)
+		{
+			const std::vector<float> e = data->getEyelidData()->getEyelidData(tr2);
+			put(f, e.data(), e.size());
 		}
 		fclose(f);
 		if (mfPopPath)

@@ -227,7 +227,8 @@ def split_ref_records(rec, num, proto):
     """The RECORDS file of ref_run -p as a dict: nc, pc (u32 per trial),
     eye, gr (f32 [bins][numGR]), psh {name: f32 [bins][cells]} (the driver's
     ECTrialsData histograms; "gr" covers numGR / 10 cells there), raster
-    {name: u32 [trials][rows][cells]}."""
+    {name: u32 [trials][rows][cells]}, eyelid_out (the driver's smoothed
+    eyelid trace, f32 [trials][window])."""
     rec_from = proto["csOn"] - proto["preCS"]
     rec_len = proto["csOff"] + proto["postCS"] - rec_from
     bins = (rec_len + proto["binSteps"] - 1) // proto["binSteps"]
@@ -249,6 +250,7 @@ def split_ref_records(rec, num, proto):
         out["psh"][name] = take(bins * n, np.float32).reshape(bins, n)
     for name, cell in TRIAL_RASTER:
         out["raster"][name] = take(nd * rows * num[cell], np.uint32).reshape(nd, rows, num[cell])
+    out["eyelid_out"] = take(nd * rec_len, np.float32).reshape(nd, rec_len)
     assert off == rec.size
     return out
 

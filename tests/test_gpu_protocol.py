@@ -124,7 +124,7 @@ def test_trial_data_matches_oracle(tmp_path, window, replay):
     rates = cbmtest.protocol_rates(st.con("numMF"), seed=1)
     steps = 3 * proto["trialSteps"]
     o = Oracle(st_path, seeds=[7])
-    tr, _, _, _, want = o.run_protocol(proto, rates, steps, trial_data=True)
+    tr, _, _, o_eye, want = o.run_protocol(proto, rates, steps, trial_data=True)
     sim = cbm.CBMSimCore(cbm.CBMState(st_path), [7], device=0)
     sim.set_eyelid_protocol(rates, **proto)
     sim.record_gr()
@@ -143,4 +143,6 @@ def test_trial_data_matches_oracle(tmp_path, window, replay):
     for name, a in want["raster"].items():
         assert np.array_equal(got["raster"][name], a), name
     assert np.array_equal(gr.astype(np.uint32), cbmtest.gr_psh_from_trace(tr, proto, st.con("numGR")))
+    smooth = cbm.eyelid_out(o_eye.reshape(proto["numDataTrials"], -1))
+    assert cbmtest.same_values(got["eyelid"].ravel(), smooth.ravel()).all()
     assert want["psh"]["go"].any() and want["raster"]["go"].any() and want["psh"]["mf"].any()

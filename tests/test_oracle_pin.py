@@ -110,6 +110,10 @@ def test_oracle_protocol_matches_reference_driver(tmp_path, window):
     r = cbmtest.split_ref_records(rec_r, o.num, proto)
     assert cbmtest.same_values(r["eye"], eye).all()
     assert np.array_equal(r["nc"], nc) and np.array_equal(r["pc"], pc)
+    # the driver's smoothed eyelid record (EyelidOut) from the raw trace
+    import cerebellum_simulation_b200 as cbm
+    smooth = cbm.eyelid_out(eye.reshape(proto["numDataTrials"], -1))
+    assert cbmtest.same_values(r["eyelid_out"].ravel(), smooth.ravel()).all()
     # the GR histogram rule the device follows, restated from the oracle's
     # trace, equals the reference's PeriStimHistFloat; the driver's own "gr"
     # histogram covers the first numGR / 10 cells
