@@ -189,3 +189,29 @@ def test_mf_population_estimate_matches_reference(tmp_path):
     out = str(tmp_path / "rt.mfpop")
     ref.write(out)
     assert open(out, "rb").read() == open(ref_path, "rb").read()
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+def test_oracle_matches_reference_1m(tmp_path):
+    """The 1M-GR network (32 PC x 32,768 PF): the reference's PF->PC
+    reduction takes its widest shape here (512 threads, 32 pair-adds each,
+    kernels.cu:445-469), which the 16K networks never reach.  300 steps of
+    eyelid-coded MF input with a CS, plasticity and an error drive; records
+    and final state must equal the reference's."""
+    from cerebellum_simulation_b200 import networks
+    net = networks.config2_network(seed=0)
+    st = str(tmp_path / "c2.state")
+    net.writeState(st)
+    steps = 300
+    mf = networks.eyelid_mf_stream(1024, steps, seed=0, cs_on=50, cs_off=250)
+    ev = {2: [("plast", 0, -0.01, 0.005)], 249: [("errdrive", 0, 1.0)]}
+    fin_ref = str(tmp_path / "ref_final.state")
+    ref = cbmtest.ref_run(st, mf, [7], ev, final_path=fin_ref).reshape(steps, -1)
+    o = Oracle(st, seeds=[7])
+    tr = o.run(mf, ev)
+    assert cbmtest.first_difference(ref, tr, o.num) is None
+    gr_spikes = np.unpackbits(tr[:, : o.num["GR"] // 8], axis=1).sum()
+    assert gr_spikes > 100000
+    fin = str(tmp_path / "oracle_final.state")
+    o.save(fin)
+    assert open(fin, "rb").read() == open(fin_ref, "rb").read()
