@@ -401,17 +401,19 @@ class CBMSimCore:
         window steps // 32, cells]}, "eyelid": f32 [trials, window steps]}
         under the eyelid driver's names; "eyelid" is the driver's smoothed
         trace (eyelid_out of the raw integrator output)."""
+        if not lib.cbm_sim_trial_record_bytes(self._h, TRIAL_PSH["go"][0]):
+            raise CBMError(1, "the trial data is not recorded")
+        p = self._protocol
+        rows = (p["csOff"] + p["postCS"] - (p["csOn"] - p["preCS"])) // 32
         out = {"psh": {}, "raster": {}, "eyelid": eyelid_out(self.trial_record("eyelid"))}
         for kinds, key, dtype in ((TRIAL_PSH, "psh", np.float32), (TRIAL_RASTER, "raster", np.uint32)):
             for name, (k, cell) in kinds.items():
-                n = lib.cbm_sim_trial_record_bytes(self._h, k)
-                if not n:
-                    raise CBMError(1, "the trial data is not recorded")
-                a = np.empty(n // 4, dtype=dtype)
-                _check(lib.cbm_sim_trial_record(self._h, k, a.ctypes.data, n))
                 cells = self.state.con(cell)
-                out[key][name] = a.reshape(-1, cells) if key == "psh" else \
-                    a.reshape(self._protocol["numDataTrials"], -1, cells)
+                n = lib.cbm_sim_trial_record_bytes(self._h, k)
+                a = np.empty(n // 4, dtype=dtype)
+                if n:  # rasters of a protocol that keeps no trial are empty
+                    _check(lib.cbm_sim_trial_record(self._h, k, a.ctypes.data, n))
+                out[key][name] = a.reshape(-1, cells) if key == "psh" else a.reshape(p["numDataTrials"], rows, cells)
         return out
 
     def trial_record(self, kind):
