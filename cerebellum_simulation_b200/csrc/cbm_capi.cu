@@ -170,6 +170,37 @@ int cbm_state_set_act_param(cbm_state *s, const char *key, float value)
 	return CBM_OK;
 }
 
+int cbm_state_param_names(const cbm_state *s, int which, char *buf, uint64_t size, uint64_t *needed)
+{
+	NEED(s); NEED(needed);
+	if (which != 0 && which != 1) return fail(CBM_ERR_ARG, "which must be 0 (connectivity) or 1 (activity)");
+	std::string list;
+	if (which == 0) for (const auto &kv : s->st.cp.raw) list += kv.first + "\n";
+	else for (const auto &kv : s->st.ap.raw) list += kv.first + "\n";
+	*needed = list.size() + 1;
+	if (!buf || size < list.size() + 1) return fail(CBM_ERR_ARG, "name buffer too small");
+	memcpy(buf, list.c_str(), list.size() + 1);
+	return CBM_OK;
+}
+
+int cbm_state_raw_param(const cbm_state *s, int which, const char *name, double *value)
+{
+	NEED(s); NEED(name); NEED(value);
+	if (which == 0) {
+		auto it = s->st.cp.raw.find(name);
+		if (it == s->st.cp.raw.end()) return fail(CBM_ERR_ARG, std::string("no connectivity parameter ") + name);
+		*value = it->second;
+		return CBM_OK;
+	}
+	if (which == 1) {
+		auto it = s->st.ap.raw.find(name);
+		if (it == s->st.ap.raw.end()) return fail(CBM_ERR_ARG, std::string("no activity parameter ") + name);
+		*value = it->second;
+		return CBM_OK;
+	}
+	return fail(CBM_ERR_ARG, "which must be 0 (connectivity) or 1 (activity)");
+}
+
 static int simCreate(cbm_state *s, const int *seeds, int device, uint32_t ring, cbm_sim **out)
 {
 	NEED(s); NEED(out);

@@ -120,6 +120,15 @@ int cbm_state_con_param(const cbm_state *s, const char *name, uint32_t *value);
 int cbm_state_act_param(const cbm_state *s, const char *name, double *value);
 /* ActivityParams::setParam (activityparams.cpp:423-434): raw key, re-derive. */
 int cbm_state_set_act_param(cbm_state *s, const char *rawKey, float value);
+/* The keys of the parameter file as read (which: 0 connectivity, 1 activity),
+ * in the order of the reference's paramMap (a std::map, so sorted), each
+ * followed by '\n', NUL-terminated.  *needed gets the bytes the list takes
+ * with its NUL; a buffer too small fails with CBM_ERR_ARG.  Backs
+ * getParamCopy (connectivityparams.cpp / activityparams.cpp:404-416). */
+int cbm_state_param_names(const cbm_state *s, int which, char *buf, uint64_t size, uint64_t *needed);
+/* A key of the parameter file as read, before derivation: ActivityParams::
+ * getParam (activityparams.cpp:418-421) and the connectivity paramMap. */
+int cbm_state_raw_param(const cbm_state *s, int which, const char *name, double *value);
 
 /* ----------------------------------------------------------- CBMSimCore */
 /* CBMSimCore(CBMState*, int *mzoneRSeed, gpuIndStart, numGPUP2)

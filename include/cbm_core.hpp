@@ -5,6 +5,8 @@
 //
 // Mirrors (paths within the reference project):
 //   CBMState        CBM_STATE_LIB_DEV/CBMStateInclude/interfaces/cbmstate.h:37-62
+//   IConnectivityParams, IActivityParams, IInNetConState, IMZoneActState
+//                   CBM_STATE_LIB_DEV/CBMStateInclude/interfaces/i*.h
 //   CBMSimCore      CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/cbmsimcore.h:35-49
 //   InNetInterface  CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/innetinterface.h:18-41
 //   MZoneInterface  CBM_CORE_LIB_MGPU_DEV/CBMCoreInclude/interface/mzoneinterface.h:18-34
@@ -17,9 +19,14 @@
 #ifndef CBM_CORE_HPP
 #define CBM_CORE_HPP
 
+#include <algorithm>
 #include <climits>
+#include <deque>
 #include <cstdint>
 #include <fstream>
+#include <map>
+#include <ostream>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -49,7 +56,176 @@ struct StreamPath {
 	std::string path;
 };
 
+// Keys of a state's parameter file (0 connectivity, 1 activity), in the
+// reference's paramMap order.
+inline std::vector<std::string> paramNames(const cbm_state *s, int which)
+{
+	uint64_t need = 0;
+	cbm_state_param_names(s, which, nullptr, 0, &need);
+	std::string buf(need, '\0');
+	check(cbm_state_param_names(s, which, &buf[0], need, &need));
+	std::vector<std::string> names;
+	std::istringstream in(buf.c_str());
+	for (std::string line; std::getline(in, line);) names.push_back(line);
+	return names;
+}
+
+inline double rawParam(const cbm_state *s, int which, const std::string &name)
+{
+	double v = 0;
+	check(cbm_state_raw_param(s, which, name.c_str(), &v));
+	return v;
+}
+
 }  // namespace cbm
+
+// IConnectivityParams (iconnectivityparams.h): cell counts and the
+// parameter file's values.  showParams prints the file's keys and values.
+class IConnectivityParams {
+public:
+	explicit IConnectivityParams(cbm_state *const *s) : s_(s) {}
+	virtual ~IConnectivityParams() {}
+	virtual void showParams(std::ostream &outSt)
+	{
+		for (const auto &kv : getParamCopy()) outSt << kv.first << " " << kv.second << std::endl;
+	}
+	virtual ct_uint32_t getGOX() { return con("goX"); }
+	virtual ct_uint32_t getGOY() { return con("goY"); }
+	virtual ct_uint32_t getGRX() { return con("grX"); }
+	virtual ct_uint32_t getGRY() { return con("grY"); }
+	virtual ct_uint32_t getGLX() { return con("glX"); }
+	virtual ct_uint32_t getGLY() { return con("glY"); }
+	virtual ct_uint32_t getNumMF() { return con("numMF"); }
+	virtual ct_uint32_t getNumGO() { return con("numGO"); }
+	virtual ct_uint32_t getNumGR() { return con("numGR"); }
+	virtual ct_uint32_t getNumGL() { return con("numGL"); }
+	virtual ct_uint32_t getNumSC() { return con("numSC"); }
+	virtual ct_uint32_t getNumBC() { return con("numBC"); }
+	virtual ct_uint32_t getNumPC() { return con("numPC"); }
+	virtual ct_uint32_t getNumNC() { return con("numNC"); }
+	virtual ct_uint32_t getNumIO() { return con("numIO"); }
+	virtual std::map<std::string, ct_uint32_t> getParamCopy()
+	{
+		std::map<std::string, ct_uint32_t> m;
+		for (const std::string &n : cbm::paramNames(*s_, 0)) m[n] = (ct_uint32_t)cbm::rawParam(*s_, 0, n);
+		return m;
+	}
+
+private:
+	ct_uint32_t con(const char *name)
+	{
+		uint32_t v = 0;
+		cbm::check(cbm_state_con_param(*s_, name, &v));
+		return v;
+	}
+	cbm_state *const *s_;
+};
+
+// IActivityParams (iactivityparams.h): getParam / setParam work on the
+// parameter file's keys, and setParam re-derives the values the step uses
+// (activityparams.cpp:418-434).
+class IActivityParams {
+public:
+	explicit IActivityParams(cbm_state *const *s) : s_(s) {}
+	virtual ~IActivityParams() {}
+	virtual unsigned int getMSPerTimeStep()
+	{
+		double v = 0;
+		cbm::check(cbm_state_act_param(*s_, "msPerTimeStep", &v));
+		return (unsigned int)v;
+	}
+	virtual void showParams(std::ostream &outSt)
+	{
+		for (const auto &kv : getParamCopy()) outSt << kv.first << " " << kv.second << std::endl;
+	}
+	virtual std::map<std::string, float> getParamCopy()
+	{
+		std::map<std::string, float> m;
+		for (const std::string &n : cbm::paramNames(*s_, 1)) m[n] = (float)cbm::rawParam(*s_, 1, n);
+		return m;
+	}
+	// an unknown key reads 0, as the reference's paramMap[key] does
+	virtual float getParam(std::string paramName)
+	{
+		double v = 0;
+		return cbm_state_raw_param(*s_, 1, paramName.c_str(), &v) == CBM_OK ? (float)v : 0.0f;
+	}
+	virtual bool setParam(std::string paramName, float value)
+	{
+		return cbm_state_set_act_param(*s_, paramName.c_str(), value) == CBM_OK;
+	}
+
+private:
+	cbm_state *const *s_;
+};
+
+class CBMState;
+
+// IInNetConState (iinnetconstate.h): per-cell connection lists of the input
+// network, read from (and, for the GO->GO pairs, edited in) the state arrays
+// before a simulator is built on them (innetconnectivitystate.cpp:245-470).
+class IInNetConState {
+public:
+	explicit IInNetConState(CBMState *st) : st_(st) {}
+	virtual ~IInNetConState() {}
+	virtual std::vector<ct_uint32_t> getpGOfromGOtoGLCon(int goN) { return con("numpGOfromGOtoGL", "pGOfromGOtoGL", goN); }
+	virtual std::vector<ct_uint32_t> getpGOfromGLtoGOCon(int goN) { return con("numpGOfromGLtoGO", "pGOfromGLtoGO", goN); }
+	virtual std::vector<ct_uint32_t> getpMFfromMFtoGLCon(int mfN) { return con("numpMFfromMFtoGL", "pMFfromMFtoGL", mfN); }
+	virtual std::vector<ct_uint32_t> getpGLfromGLtoGRCon(int glN) { return con("numpGLfromGLtoGR", "pGLfromGLtoGR", glN); }
+	virtual std::vector<ct_uint32_t> getpGRfromMFtoGR(int grN) { return con("numpGRfromMFtoGR", "pGRfromMFtoGR", grN); }
+	virtual std::vector<std::vector<ct_uint32_t> > getpGRPopfromMFtoGR() { return all("numpGRfromMFtoGR", "pGRfromMFtoGR"); }
+	virtual std::vector<ct_uint32_t> getpGRfromGOtoGR(int grN) { return con("numpGRfromGOtoGR", "pGRfromGOtoGR", grN); }
+	virtual std::vector<std::vector<ct_uint32_t> > getpGRPopfromGOtoGR() { return all("numpGRfromGOtoGR", "pGRfromGOtoGR"); }
+	virtual std::vector<ct_uint32_t> getpGOfromGRtoGOCon(int goN) { return con("numpGOfromGRtoGO", "pGOfromGRtoGO", goN); }
+	virtual std::vector<ct_uint32_t> getpGOfromGOtoGRCon(int goN) { return con("numpGOfromGOtoGR", "pGOfromGOtoGR", goN); }
+	virtual std::vector<ct_uint32_t> getpMFfromMFtoGRCon(int mfN) { return con("numpMFfromMFtoGR", "pMFfromMFtoGR", mfN); }
+	virtual std::vector<ct_uint32_t> getpMFfromMFtoGOCon(int mfN) { return con("numpMFfromMFtoGO", "pMFfromMFtoGO", mfN); }
+	virtual std::vector<ct_uint32_t> getpGOfromMFtoGOCon(int goN) { return con("numpGOfromMFtoGO", "pGOfromMFtoGO", goN); }
+	virtual std::vector<std::vector<ct_uint32_t> > getpGOPopfromMFtoGOCon() { return all("numpGOfromMFtoGO", "pGOfromMFtoGO"); }
+	virtual std::vector<ct_uint32_t> getpGOOutGOGOCon(int goN) { return con("numpGOGABAOutGOGO", "pGOGABAOutGOGO", goN); }
+	virtual std::vector<ct_uint32_t> getpGOInGOGOCon(int goN) { return con("numpGOGABAInGOGO", "pGOGABAInGOGO", goN); }
+	// cells whose GR->GO lists are below their maximum (innetconnectivitystate.cpp:371-396)
+	virtual std::vector<ct_uint32_t> getGOIncompIndfromGRtoGO() { return incomplete("numpGOfromGRtoGO", "maxnumpGOfromGRtoGO"); }
+	virtual std::vector<ct_uint32_t> getGRIncompIndfromGRtoGO() { return incomplete("numpGRfromGRtoGO", "maxnumpGRfromGRtoGO"); }
+	// remove / add one GO->GO GABA pair in both directions' lists
+	// (innetconnectivitystate.cpp:398-452)
+	virtual bool deleteGOGOConPair(int srcGON, int destGON);
+	virtual bool addGOGOConPair(int srcGON, int destGON);
+
+private:
+	struct Table { int32_t *num; ct_uint32_t *p; uint64_t rows, stride; };
+	Table table(const char *num, const char *list);
+	std::vector<ct_uint32_t> con(const char *num, const char *list, int n)
+	{
+		Table t = table(num, list);
+		if (n < 0 || (uint64_t)n >= t.rows) throw cbm::Error(CBM_ERR_ARG, "cell index out of range");
+		const ct_uint32_t *row = t.p + (uint64_t)n * t.stride;
+		return std::vector<ct_uint32_t>(row, row + t.num[n]);
+	}
+	std::vector<std::vector<ct_uint32_t> > all(const char *num, const char *list)
+	{
+		Table t = table(num, list);
+		std::vector<std::vector<ct_uint32_t> > v(t.rows);
+		for (uint64_t i = 0; i < t.rows; i++) v[i].assign(t.p + i * t.stride, t.p + i * t.stride + t.num[i]);
+		return v;
+	}
+	std::vector<ct_uint32_t> incomplete(const char *num, const char *maxName);
+	CBMState *st_;
+};
+
+// IMZoneActState (imzoneactstate.h): zone z's PF->PC weights, PC-major
+// (mzoneactivitystate.cpp:202-228).
+class IMZoneActState {
+public:
+	IMZoneActState(CBMState *st, unsigned int zone) : st_(st), zone_(zone) {}
+	virtual ~IMZoneActState() {}
+	virtual std::vector<float> getGRPCSynWeightLinear();
+	virtual void resetGRPCSynWeight();
+
+private:
+	CBMState *st_;
+	unsigned int zone_;
+};
 
 class CBMState {
 public:
@@ -84,9 +260,104 @@ public:
 	}
 	cbm_state *handle() { return s_; }
 
+	// the reference's accessors; the objects live as long as the state
+	IConnectivityParams *getConnectivityParams() { return &conParams_; }
+	IActivityParams *getActivityParams() { return &actParams_; }
+	IInNetConState *getInnetConState() { return &innetCon_; }
+	IMZoneActState *getMZoneActState(unsigned int zoneN)
+	{
+		if (zoneN >= getNumZones()) throw cbm::Error(CBM_ERR_ARG, "zone out of range");
+		while (zoneAct_.size() <= zoneN) zoneAct_.emplace_back(this, (unsigned int)zoneAct_.size());
+		return &zoneAct_[zoneN];
+	}
+	// CBMState::equivalent (cbmstate.cpp:105-121, innetconnectivitystate.cpp:
+	// 228-243): the same zone count, MF->GL glomeruli, GO->GR and GR<-GO counts
+	bool equivalent(CBMState &compState)
+	{
+		if (getNumZones() != compState.getNumZones()) return false;
+		for (const char *n : {"haspGLfromMFtoGL", "numpGOfromGOtoGR", "numpGRfromGOtoGR"}) {
+			uint64_t a = 0, b = 0;
+			const uint8_t *x = array<uint8_t>(n, -1, &a), *y = compState.array<uint8_t>(n, -1, &b);
+			const uint64_t bytes = std::string(n) == "haspGLfromMFtoGL" ? a : 4 * a;
+			if (a != b || !std::equal(x, x + bytes, y)) return false;
+		}
+		return true;
+	}
+
 private:
 	cbm_state *s_ = nullptr;
+	IConnectivityParams conParams_{&s_};
+	IActivityParams actParams_{&s_};
+	IInNetConState innetCon_{this};
+	std::deque<IMZoneActState> zoneAct_;  // stable addresses as zones are added
 };
+
+inline IInNetConState::Table IInNetConState::table(const char *num, const char *list)
+{
+	Table t;
+	uint64_t cnt = 0;
+	t.num = st_->array<int32_t>(num, -1, &t.rows);
+	t.p = st_->array<ct_uint32_t>(list, -1, &cnt);
+	t.stride = t.rows ? cnt / t.rows : 0;
+	return t;
+}
+
+inline std::vector<ct_uint32_t> IInNetConState::incomplete(const char *num, const char *maxName)
+{
+	uint64_t rows = 0;
+	const int32_t *k = st_->array<int32_t>(num, -1, &rows);
+	uint32_t limit = 0;
+	cbm::check(cbm_state_con_param(st_->handle(), maxName, &limit));
+	std::vector<ct_uint32_t> v;
+	for (uint64_t i = 0; i < rows; i++) if ((uint32_t)k[i] < limit) v.push_back((ct_uint32_t)i);
+	return v;
+}
+
+inline bool IInNetConState::deleteGOGOConPair(int srcGON, int destGON)
+{
+	Table out = table("numpGOGABAOutGOGO", "pGOGABAOutGOGO"), in = table("numpGOGABAInGOGO", "pGOGABAInGOGO");
+	ct_uint32_t *o = out.p + (uint64_t)srcGON * out.stride;
+	int at = -1;
+	for (int i = 0; i < out.num[srcGON]; i++) if (o[i] == (ct_uint32_t)destGON) { at = i; break; }
+	if (at < 0) return false;
+	for (int i = at; i < out.num[srcGON] - 1; i++) o[i] = o[i + 1];
+	out.num[srcGON]--;
+	// the reference removes the last matching entry of the in-list (with
+	// in- and out-lists that mirror each other, as every state has them)
+	ct_uint32_t *q = in.p + (uint64_t)destGON * in.stride;
+	int last = -1;
+	for (int i = 0; i < in.num[destGON]; i++) if (q[i] == (ct_uint32_t)srcGON) last = i;
+	if (last >= 0) {
+		for (int i = last; i < in.num[destGON] - 1; i++) q[i] = q[i + 1];
+		in.num[destGON]--;
+	}
+	return true;
+}
+
+inline bool IInNetConState::addGOGOConPair(int srcGON, int destGON)
+{
+	Table out = table("numpGOGABAOutGOGO", "pGOGABAOutGOGO"), in = table("numpGOGABAInGOGO", "pGOGABAInGOGO");
+	if ((uint64_t)out.num[srcGON] >= out.stride || (uint64_t)in.num[destGON] >= in.stride) return false;
+	out.p[(uint64_t)srcGON * out.stride + out.num[srcGON]++] = (ct_uint32_t)destGON;
+	in.p[(uint64_t)destGON * in.stride + in.num[destGON]++] = (ct_uint32_t)srcGON;
+	return true;
+}
+
+inline std::vector<float> IMZoneActState::getGRPCSynWeightLinear()
+{
+	uint64_t n = 0;
+	const float *w = st_->array<float>("pfSynWeightPC", (int)zone_, &n);
+	return std::vector<float>(w, w + n);
+}
+
+inline void IMZoneActState::resetGRPCSynWeight()
+{
+	double w0 = 0;
+	cbm::check(cbm_state_act_param(st_->handle(), "initSynWofGRtoPC", &w0));
+	uint64_t n = 0;
+	float *w = st_->array<float>("pfSynWeightPC", (int)zone_, &n);
+	for (uint64_t i = 0; i < n; i++) w[i] = (float)w0;
+}
 
 class InNetInterface {
 public:

@@ -1,6 +1,7 @@
 // A driver written against the reference's CBMState / CBMSimCore classes,
-// compiled against include/cbm_core.hpp.  With one argument it only loads a
-// state; with two it also steps the network on GPU 0 and reads NC spikes.
+// compiled against include/cbm_core.hpp.  With one argument it loads a state
+// and goes through the state library's accessors; with two it steps the
+// network on GPU 0 and reads NC spikes.
 #include <cbm_core.hpp>
 
 #include <cstdio>
@@ -11,6 +12,36 @@ int main(int argc, char **argv)
 	if (argc < 2) return 2;
 	CBMState st(argv[1]);
 	std::printf("zones %u\n", st.getNumZones());
+	// the state library's accessors, as the eyelid driver reaches them
+	// (ecmanagementdelay.cpp:106-150); they edit the state, so only without
+	// the stepping run
+	if (argc == 2) {
+	IConnectivityParams *cp = st.getConnectivityParams();
+	IActivityParams *ap = st.getActivityParams();
+	std::printf("cells %u %u %u %u %u %u %u %u ms %u\n", cp->getNumGR(), cp->getNumGO(), cp->getNumMF(),
+			cp->getNumSC(), cp->getNumBC(), cp->getNumPC(), cp->getNumNC(), cp->getNumIO(), ap->getMSPerTimeStep());
+	const float ltd = ap->getParam("grPCLTDDecIO");
+	const bool set = ap->setParam("grPCLTDDecIO", 2 * ltd), bad = ap->setParam("noSuchParam", 1);
+	std::printf("params %zu %zu ltd %g set %d %g bad %d\n", cp->getParamCopy().size(), ap->getParamCopy().size(),
+			ltd, (int)set, ap->getParam("grPCLTDDecIO"), (int)bad);
+	IInNetConState *con = st.getInnetConState();
+	std::printf("gr0 mf %zu go %zu go0 gr %zu incomplete %zu\n", con->getpGRfromMFtoGR(0).size(),
+			con->getpGRfromGOtoGR(0).size(), con->getpGOfromGRtoGOCon(0).size(),
+			con->getGRIncompIndfromGRtoGO().size());
+	// a GO->GO pair added to and removed from both lists of GO 0 and GO 1
+	const size_t out0 = con->getpGOOutGOGOCon(0).size(), in0 = con->getpGOInGOGOCon(1).size();
+	const bool add = con->addGOGOConPair(0, 1);
+	const size_t out1 = con->getpGOOutGOGOCon(0).size(), in1 = con->getpGOInGOGOCon(1).size();
+	const ct_uint32_t last = out1 ? con->getpGOOutGOGOCon(0).back() : 0;
+	const bool del = con->deleteGOGOConPair(0, 1), again = con->deleteGOGOConPair(0, 1);
+	std::printf("gogo %zu %zu add %d %zu %zu last %u del %d again %d %zu %zu\n", out0, in0, (int)add, out1, in1,
+			last, (int)del, (int)again, con->getpGOOutGOGOCon(0).size(), con->getpGOInGOGOCon(1).size());
+	st.array<float>("pfSynWeightPC", 0)[0] = 0.25f;
+	std::vector<float> w = st.getMZoneActState(0)->getGRPCSynWeightLinear();
+	st.getMZoneActState(0)->resetGRPCSynWeight();
+	std::printf("weights %zu %g reset %g equivalent %d\n", w.size(), w[0],
+			st.getMZoneActState(0)->getGRPCSynWeightLinear()[0], (int)st.equivalent(st));
+	}
 	if (argc > 2) {
 		int seeds[1] = {7};
 		CBMSimCore sim(&st, seeds, 0, -1);

@@ -105,6 +105,23 @@ def test_cpp_facade_compiles_and_loads_a_reference_state(tmp_path):
     p = cbmtest.golden_state("ref16k", str(tmp_path))
     out = subprocess.run([exe, p], check=True, capture_output=True, text=True).stdout
     assert "zones 1" in out
+    lines = {l.split()[0]: l.split()[1:] for l in out.splitlines()}
+    s = __import__("cerebellum_simulation_b200").CBMState(p)
+    assert lines["cells"] == [str(s.con(n)) for n in ("numGR", "numGO", "numMF", "numSC", "numBC", "numPC",
+                                                       "numNC", "numIO")] + ["ms", "1"]
+    n_con, n_act, _, ltd, _, set_ok, ltd2, _, bad = lines["params"]
+    assert int(n_con) > 20 and int(n_act) > 80 and set_ok == "1" and bad == "0"
+    assert float(ltd2) == pytest.approx(2 * float(ltd))
+    assert lines["gr0"][1] == str(int(s.array("numpGRfromMFtoGR")[0]))
+    assert lines["gr0"][3] == str(int(s.array("numpGRfromGOtoGR")[0]))
+    assert lines["gr0"][6] == str(int(s.array("numpGOfromGRtoGO")[0]))
+    # the reference network has no GO->GO pairs and room for one per GO: the
+    # pair goes to the end of both lists, and its removal empties them again
+    # (a second removal finds nothing)
+    assert lines["gogo"] == ["0", "0", "add", "1", "1", "1", "last", "1", "del", "1", "again", "0", "0", "0"]
+    w = lines["weights"]
+    assert int(w[0]) == 16384 and float(w[1]) == 0.25
+    assert float(w[3]) == pytest.approx(s.act("initSynWofGRtoPC")) and w[5] == "1"
 
 
 def _damage(s, name):
