@@ -137,6 +137,8 @@ def _load():
         "cbm_sim_trial_record_bytes": (U64, [P, I]),
         "cbm_sim_trial_record": (I, [P, I, P, U64]),
         "cbm_sim_record_gr": (I, [P]),
+        "cbm_state_param_names": (I, [P, I, ctypes.c_char_p, U64, ctypes.POINTER(U64)]),
+        "cbm_state_raw_param": (I, [P, I, ctypes.c_char_p, ctypes.POINTER(D)]),
         "cbm_sim_record_trial_data": (I, [P]),
         "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_destroy": (None, [P]),
@@ -217,6 +219,176 @@ class CBMState:
 
     def setActParam(self, key, value):
         _check(lib.cbm_state_set_act_param(self._h, key.encode(), value))
+
+    # the reference's accessor interfaces (cbmstate.cpp:105-146)
+    def getConnectivityParams(self):
+        return IConnectivityParams(self)
+
+    def getActivityParams(self):
+        return IActivityParams(self)
+
+    def getInnetConState(self):
+        return IInNetConState(self)
+
+    def getMZoneActState(self, zoneN):
+        if not 0 <= zoneN < self.getNumZones():
+            raise CBMError(1, "zone out of range")
+        return IMZoneActState(self, zoneN)
+
+    def equivalent(self, other):
+        """CBMState::equivalent (cbmstate.cpp:105-121,
+        innetconnectivitystate.cpp:228-243): zone count, MF->GL glomeruli and
+        the GO->GR / GR<-GO counts."""
+        return self.getNumZones() == other.getNumZones() and all(
+            np.array_equal(self.array(n), other.array(n))
+            for n in ("haspGLfromMFtoGL", "numpGOfromGOtoGR", "numpGRfromGOtoGR"))
+
+    def _param_names(self, which):
+        need = ctypes.c_uint64()
+        lib.cbm_state_param_names(self._h, which, None, 0, ctypes.byref(need))
+        buf = ctypes.create_string_buffer(need.value)
+        _check(lib.cbm_state_param_names(self._h, which, buf, need.value, ctypes.byref(need)))
+        return buf.value.decode().split()
+
+    def _raw_param(self, which, name):
+        v = ctypes.c_double()
+        rc = lib.cbm_state_raw_param(self._h, which, name.encode(), ctypes.byref(v))
+        return v.value if rc == CBM_OK else None
+
+
+class IConnectivityParams:
+    """IConnectivityParams (CBM_STATE_LIB_DEV/CBMStateInclude/interfaces/iconnectivityparams.h)."""
+
+    def __init__(self, state):
+        self._s = state
+
+    def getParamCopy(self):
+        return {n: int(self._s._raw_param(0, n)) for n in self._s._param_names(0)}
+
+    def showParams(self, out=None):
+        """The parameter file's keys and values in key order."""
+        import sys
+        for k, v in self.getParamCopy().items():
+            print(k, v, file=out or sys.stdout)
+
+
+for _name, _field in (("getGOX", "goX"), ("getGOY", "goY"), ("getGRX", "grX"), ("getGRY", "grY"),
+                      ("getGLX", "glX"), ("getGLY", "glY"), ("getNumMF", "numMF"), ("getNumGO", "numGO"),
+                      ("getNumGR", "numGR"), ("getNumGL", "numGL"), ("getNumSC", "numSC"), ("getNumBC", "numBC"),
+                      ("getNumPC", "numPC"), ("getNumNC", "numNC"), ("getNumIO", "numIO")):
+    setattr(IConnectivityParams, _name, (lambda f: lambda self: self._s.con(f))(_field))
+
+
+class IActivityParams:
+    """IActivityParams (iactivityparams.h): getParam / setParam work on the
+    parameter file's keys; setParam re-derives the step's values
+    (activityparams.cpp:418-434)."""
+
+    def __init__(self, state):
+        self._s = state
+
+    def getMSPerTimeStep(self):
+        return int(self._s.act("msPerTimeStep"))
+
+    def getParamCopy(self):
+        return {n: float(np.float32(self._s._raw_param(1, n))) for n in self._s._param_names(1)}
+
+    def getParam(self, paramName):
+        v = self._s._raw_param(1, paramName)
+        return 0.0 if v is None else float(np.float32(v))  # an unknown key reads 0, as paramMap[key] does
+
+    def setParam(self, paramName, value):
+        return lib.cbm_state_set_act_param(self._s._h, paramName.encode(), value) == CBM_OK
+
+    def showParams(self, out=None):
+        import sys
+        for k, v in self.getParamCopy().items():
+            print(k, v, file=out or sys.stdout)
+
+
+class IInNetConState:
+    """IInNetConState (iinnetconstate.h): per-cell connection lists of the
+    input network, read from and (GO->GO pairs) edited in the state arrays
+    (innetconnectivitystate.cpp:245-470)."""
+
+    _LISTS = {"getpGOfromGOtoGLCon": "GOfromGOtoGL", "getpGOfromGLtoGOCon": "GOfromGLtoGO",
+              "getpMFfromMFtoGLCon": "MFfromMFtoGL", "getpGLfromGLtoGRCon": "GLfromGLtoGR",
+              "getpGRfromMFtoGR": "GRfromMFtoGR", "getpGRfromGOtoGR": "GRfromGOtoGR",
+              "getpGOfromGRtoGOCon": "GOfromGRtoGO", "getpGOfromGOtoGRCon": "GOfromGOtoGR",
+              "getpMFfromMFtoGRCon": "MFfromMFtoGR", "getpMFfromMFtoGOCon": "MFfromMFtoGO",
+              "getpGOfromMFtoGOCon": "GOfromMFtoGO", "getpGOOutGOGOCon": "GOGABAOutGOGO",
+              "getpGOInGOGOCon": "GOGABAInGOGO"}
+
+    def __init__(self, state):
+        self._s = state
+
+    def _table(self, key):
+        num, p = self._s.array("nump" + key), self._s.array("p" + key)
+        return num, p.reshape(num.size, -1)
+
+    def _con(self, key, n):
+        num, p = self._table(key)
+        return [int(x) for x in p[n, : num[n]]]
+
+    def __getattr__(self, name):
+        if name in IInNetConState._LISTS:
+            return lambda n: self._con(IInNetConState._LISTS[name], n)
+        raise AttributeError(name)
+
+    def getpGRPopfromMFtoGR(self):
+        return [self._con("GRfromMFtoGR", i) for i in range(self._s.con("numGR"))]
+
+    def getpGRPopfromGOtoGR(self):
+        return [self._con("GRfromGOtoGR", i) for i in range(self._s.con("numGR"))]
+
+    def getpGOPopfromMFtoGOCon(self):
+        return [self._con("GOfromMFtoGO", i) for i in range(self._s.con("numGO"))]
+
+    def getGOIncompIndfromGRtoGO(self):
+        return list(np.nonzero(self._s.array("numpGOfromGRtoGO") < self._s.con("maxnumpGOfromGRtoGO"))[0])
+
+    def getGRIncompIndfromGRtoGO(self):
+        return list(np.nonzero(self._s.array("numpGRfromGRtoGO") < self._s.con("maxnumpGRfromGRtoGO"))[0])
+
+    def addGOGOConPair(self, srcGON, destGON):
+        on, op = self._table("GOGABAOutGOGO")
+        inn, ip = self._table("GOGABAInGOGO")
+        if on[srcGON] >= op.shape[1] or inn[destGON] >= ip.shape[1]:
+            return False
+        op[srcGON, on[srcGON]] = destGON
+        on[srcGON] += 1
+        ip[destGON, inn[destGON]] = srcGON
+        inn[destGON] += 1
+        return True
+
+    def deleteGOGOConPair(self, srcGON, destGON):
+        on, op = self._table("GOGABAOutGOGO")
+        inn, ip = self._table("GOGABAInGOGO")
+        hit = np.nonzero(op[srcGON, : on[srcGON]] == destGON)[0]
+        if hit.size == 0:
+            return False
+        k = on[srcGON]
+        op[srcGON, hit[0]: k - 1] = op[srcGON, hit[0] + 1: k].copy()
+        on[srcGON] -= 1
+        hit = np.nonzero(ip[destGON, : inn[destGON]] == srcGON)[0]  # the last match, as the reference
+        if hit.size:
+            k = inn[destGON]
+            ip[destGON, hit[-1]: k - 1] = ip[destGON, hit[-1] + 1: k].copy()
+            inn[destGON] -= 1
+        return True
+
+
+class IMZoneActState:
+    """IMZoneActState (imzoneactstate.h, mzoneactivitystate.cpp:202-228)."""
+
+    def __init__(self, state, zone):
+        self._s, self._z = state, zone
+
+    def getGRPCSynWeightLinear(self):
+        return self._s.array("pfSynWeightPC", self._z).copy()
+
+    def resetGRPCSynWeight(self):
+        self._s.array("pfSynWeightPC", self._z)[:] = np.float32(self._s.act("initSynWofGRtoPC"))
 
 
 class _Exporter:

@@ -174,3 +174,38 @@ def test_valid_network_needs_a_device(tmp_path):
         assert e.code == 2, str(e)
     else:
         sim.close()
+
+
+def test_python_state_accessors_match_the_facade(tmp_path):
+    """The Python mirror of the state library's accessors gives what the C++
+    facade's do on the same state file."""
+    import subprocess
+    import cerebellum_simulation_b200 as cbm
+    exe = cbmtest.build_facade_check(str(tmp_path))
+    p = cbmtest.golden_state("ref16k", str(tmp_path))
+    lines = {l.split()[0]: l.split()[1:]
+             for l in subprocess.run([exe, p], check=True, capture_output=True, text=True).stdout.splitlines()}
+    s = cbm.CBMState(p)
+    cp, ap, con = s.getConnectivityParams(), s.getActivityParams(), s.getInnetConState()
+    assert lines["cells"][:8] == [str(f()) for f in (cp.getNumGR, cp.getNumGO, cp.getNumMF, cp.getNumSC,
+                                                     cp.getNumBC, cp.getNumPC, cp.getNumNC, cp.getNumIO)]
+    assert int(lines["cells"][9]) == ap.getMSPerTimeStep()
+    assert int(lines["params"][0]) == len(cp.getParamCopy()) and int(lines["params"][1]) == len(ap.getParamCopy())
+    ltd = ap.getParam("grPCLTDDecIO")
+    assert float(lines["params"][3]) == pytest.approx(ltd)
+    assert ap.setParam("grPCLTDDecIO", 2 * ltd) and not ap.setParam("noSuchParam", 1.0)
+    assert ap.getParam("grPCLTDDecIO") == pytest.approx(2 * ltd) and ap.getParam("noSuchParam") == 0.0
+    assert lines["gr0"] == ["mf", str(len(con.getpGRfromMFtoGR(0))), "go", str(len(con.getpGRfromGOtoGR(0))),
+                            "go0", "gr", str(len(con.getpGOfromGRtoGOCon(0))), "incomplete",
+                            str(len(con.getGRIncompIndfromGRtoGO()))]
+    assert con.getpGRPopfromMFtoGR()[5] == con.getpGRfromMFtoGR(5)
+    assert con.addGOGOConPair(0, 1) and not con.addGOGOConPair(0, 2)
+    assert con.getpGOOutGOGOCon(0) == [1] and con.getpGOInGOGOCon(1) == [0]
+    assert con.deleteGOGOConPair(0, 1) and not con.deleteGOGOConPair(0, 1)
+    assert con.getpGOOutGOGOCon(0) == [] and con.getpGOInGOGOCon(1) == []
+    z = s.getMZoneActState(0)
+    s.array("pfSynWeightPC", 0)[0] = 0.25
+    assert z.getGRPCSynWeightLinear()[0] == np.float32(0.25)
+    z.resetGRPCSynWeight()
+    assert np.all(z.getGRPCSynWeightLinear() == np.float32(s.act("initSynWofGRtoPC")))
+    assert s.equivalent(cbm.CBMState(p))
