@@ -588,6 +588,14 @@ class CBMSimCore:
                 out[key][name] = a.reshape(-1, cells) if key == "psh" else a.reshape(p["numDataTrials"], rows, cells)
         return out
 
+    def write_trial_data(self, path):
+        """The eyelid driver's data file (ECTrialsData::writeData) of the
+        running protocol's records, after record_gr and record_trial_data and
+        a run over all kept trials (trialdata.write_ec_trials_data)."""
+        from .trialdata import write_ec_trials_data
+        write_ec_trials_data(path, self.trial_data(), self.trial_record("gr"), self.trial_record("eyelid"),
+                             self._protocol, self.state.con("numGR"), int(self.state.act("msPerTimeStep")))
+
     def trial_record(self, kind):
         """Records of the running protocol: 'nc' / 'pc' spike counts
         [trials, bins, cells] (u32), 'eyelid' [trials, window steps] (f32), or

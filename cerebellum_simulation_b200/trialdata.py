@@ -1,0 +1,69 @@
+"""The eyelid driver's data file from device records.
+
+``write_ec_trials_data`` lays out a run's trial records the way the
+reference's ECTrialsData::writeData writes its own
+(CBM_DATA_LIB_DEV/src/interfaces/ectrialsdata.cpp): a text header line, the
+eyelid record (EyelidOut::writeData, outdata/eyelidout.cpp), every
+peri-stimulus histogram (PeriStimHistFloat::writeData,
+peristimhist/peristimhistfloat.cpp) and every raster
+(ISpikeRaster / SpikeRasterBitArray::writeData, spikeraster/
+spikerasterbitarray.cpp) in the order of the reference's std::map (byte
+order of the names), then the count of raw-uint records (none).  The
+histogram and raster sets are those the eyelid driver builds
+(Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:107-156); its "gr"
+histogram covers the first numGR / 10 cells.
+
+The counters written with each record are those of a run whose kept trials
+were all recorded to their end, which is what the driver writes at the end
+of a session.
+"""
+import numpy as np
+
+
+def _line(*values):
+    return (" ".join(str(int(v)) for v in values) + "\n").encode()
+
+
+def write_ec_trials_data(path, trial_data, gr_psh, eyelid_raw, proto, num_gr, ms_per_step=1, num_ts_smooth=4):
+    """Write the driver's data file.
+
+    trial_data: {"psh": {name: f32 [bins, cells]}, "raster": {name: u32
+    [trials, rows, cells]}} (CBMSimCore.trial_data); gr_psh: [bins, numGR]
+    GR counts (CBMSimCore.trial_record("gr")); eyelid_raw: the integrator's
+    output [trials, window steps] (trial_record("eyelid")); proto: the
+    protocol's fields (preCS, postCS, csOn, csOff, binSteps,
+    numDataTrials)."""
+    from . import eyelid_out
+    pre, post = int(proto["preCS"]), int(proto["postCS"])
+    cs = int(proto["csOff"]) - int(proto["csOn"])
+    nd, bin_steps = int(proto["numDataTrials"]), int(proto["binSteps"])
+    ms_total = pre + cs + post
+    ts_total = ms_total // ms_per_step
+    n_bins = -(-ts_total // bin_steps)
+    psh = dict(trial_data["psh"])
+    psh["gr"] = np.asarray(gr_psh)[:, : num_gr // 10].astype(np.float32)
+    rows = ts_total // 32
+    with open(path, "wb") as f:
+        f.write(_line(pre, cs, post, ms_total, ms_per_step, ts_total, nd))
+        # EyelidOut: every kept trial recorded to its end
+        f.write(_line(nd, ms_per_step, num_ts_smooth, ms_total, ts_total, nd, 0))
+        f.write(np.ascontiguousarray(eyelid_out(eyelid_raw, num_ts_smooth), dtype=np.float32).tobytes())
+        f.write(_line(len(psh)))
+        for name in sorted(psh):
+            h = np.ascontiguousarray(psh[name], dtype=np.float32)
+            if h.shape[0] != n_bins:
+                raise ValueError(f"histogram {name}: {h.shape[0]} bins, the window has {n_bins}")
+            f.write(name.encode() + b"\n")
+            f.write(_line(h.shape[1], ts_total, bin_steps, n_bins, 0, nd))
+            f.write(h.tobytes())
+        rasters = trial_data["raster"]
+        updates = nd * ((ts_total - 1) // 32)
+        cur_trial, cur_buf = (updates // rows, updates % rows) if rows else (0, 0)
+        f.write(_line(len(rasters)))
+        for name in sorted(rasters):
+            r = np.ascontiguousarray(rasters[name], dtype=np.uint32)
+            f.write(name.encode() + b"\n")
+            f.write(name.encode() + b" " + _line(r.shape[2], nd, ms_total).rstrip(b"\n") + b" ")
+            f.write(_line(ms_per_step, cur_trial, 32 * cur_buf, cur_buf, ts_total, rows))
+            f.write(r.tobytes())
+        f.write(_line(0))

@@ -37,7 +37,8 @@
  *       and its smoothed eyelid trace (EyelidOut) as f32
  *       [numDataTrials][window] (MFBYTES is then ignored).  -m MFPOP then writes the
  *       reference's ECMFPopulation estimated from that ECTrialsData
- *       (CBM_TOOLS_LIB_DEV/src/ecmfpopulation.cpp:11-65) with writeToFile.  PROTOCOL is "key value" text: trialSteps,
+ *       (CBM_TOOLS_LIB_DEV/src/ecmfpopulation.cpp:11-65) with writeToFile, and
+ *       -d DATA the ECTrialsData itself with its writeData.  PROTOCOL is "key value" text: trialSteps,
  *       csOn, csOff, csPhasicOff, csStartTrial, plastOnDelay, plastOffDelay,
  *       plastLTD, plastLTP, usErrDrive, mfSeed, mfThreshDecayTau, rates (a file
  *       of 3 x numMF f32: background, CS tonic, CS phasic), dataStartTrial,
@@ -181,7 +182,7 @@ int main(int argc, char **argv)
 	const char *statePath = argv[1], *mfPath = argv[2], *tracePath = argv[4], *finalPath = argv[5];
 	unsigned long steps = strtoul(argv[3], NULL, 10);
 	std::vector<int> seeds;
-	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL, *mfPopPath = NULL;
+	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL, *mfPopPath = NULL, *dataPath = NULL;
 	int numGPUP2 = 0;
 	bool timeOnly = false;
 	unsigned long warm = 0;  // leading steps run before the clock starts
@@ -191,6 +192,7 @@ int main(int argc, char **argv)
 		else if (!strcmp(argv[i], "-p") && i + 1 < argc) protocolPath = argv[++i];
 		else if (!strcmp(argv[i], "-r") && i + 1 < argc) recordsPath = argv[++i];
 		else if (!strcmp(argv[i], "-m") && i + 1 < argc) mfPopPath = argv[++i];
+		else if (!strcmp(argv[i], "-d") && i + 1 < argc) dataPath = argv[++i];
 		else if (!strcmp(argv[i], "-g") && i + 1 < argc) numGPUP2 = atoi(argv[++i]);
 		else if (!strcmp(argv[i], "-t")) timeOnly = true;
 		else if (!strcmp(argv[i], "-w") && i + 1 < argc) warm = strtoul(argv[++i], NULL, 10);
@@ -450,6 +452,12 @@ int main(int argc, char **argv)
 			put(f, e.data(), e.size());
 		}
 		fclose(f);
+		if (dataPath)
+		{
+			// the driver's data file (ECTrialsData::writeData, ectrialsdata.cpp)
+			std::fstream df(dataPath, std::ios::out | std::ios::binary | std::ios::trunc);
+			data->writeData(df);
+		}
 		if (mfPopPath)
 		{
 			// the MF rates the reference estimates from the run's MF histogram

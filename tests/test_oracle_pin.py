@@ -215,3 +215,24 @@ def test_oracle_matches_reference_1m(tmp_path):
     fin = str(tmp_path / "oracle_final.state")
     o.save(fin)
     assert open(fin, "rb").read() == open(fin_ref, "rb").read()
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+def test_trial_data_file_matches_reference(tmp_path):
+    """trialdata.write_ec_trials_data over the oracle's records writes the
+    reference's ECTrialsData::writeData file byte for byte (a 280-step
+    window, so every raster row is written by the run)."""
+    from cerebellum_simulation_b200.trialdata import write_ec_trials_data
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol()
+    o = Oracle(st, seeds=[7])
+    rates = cbmtest.protocol_rates(o.num["MF"], seed=1)
+    steps = 3 * proto["trialSteps"]
+    tr, _, _, eye, td = o.run_protocol(proto, rates, steps, trial_data=True)
+    ref_path = str(tmp_path / "ref.data")
+    cbmtest.ref_run_protocol(st, proto, rates, steps, [7], data_file=ref_path)
+    ours = str(tmp_path / "ours.data")
+    write_ec_trials_data(ours, td, cbmtest.gr_psh_from_trace(tr, proto, o.num["GR"]),
+                         eye.reshape(proto["numDataTrials"], -1), proto, o.num["GR"])
+    a, b = open(ours, "rb").read(), open(ref_path, "rb").read()
+    assert len(a) == len(b) and a == b, next(i for i in range(min(len(a), len(b))) if a[i] != b[i])
