@@ -136,6 +136,7 @@ def test_trial_data_matches_oracle(tmp_path, window, replay):
             sim.calcActivity()
     got = sim.trial_data()
     gr = sim.trial_record("gr")
+    sim.write_trial_data(str(tmp_path / "device.data"))
     sim.close()
     for name, a in want["psh"].items():
         assert got["psh"][name].shape == a.shape, name
@@ -145,4 +146,10 @@ def test_trial_data_matches_oracle(tmp_path, window, replay):
     assert np.array_equal(gr.astype(np.uint32), cbmtest.gr_psh_from_trace(tr, proto, st.con("numGR")))
     smooth = cbm.eyelid_out(o_eye.reshape(proto["numDataTrials"], -1))
     assert cbmtest.same_values(got["eyelid"].ravel(), smooth.ravel()).all()
+    # the driver's data file from the device equals the one from the oracle's
+    # records (which test_oracle_pin.py holds to the reference's file)
+    from cerebellum_simulation_b200.trialdata import write_ec_trials_data
+    write_ec_trials_data(str(tmp_path / "oracle.data"), want, cbmtest.gr_psh_from_trace(tr, proto, st.con("numGR")),
+                         o_eye.reshape(proto["numDataTrials"], -1), proto, st.con("numGR"))
+    assert open(tmp_path / "device.data", "rb").read() == open(tmp_path / "oracle.data", "rb").read()
     assert want["psh"]["go"].any() and want["raster"]["go"].any() and want["psh"]["mf"].any()
