@@ -596,6 +596,24 @@ class CBMSimCore:
         write_ec_trials_data(path, self.trial_data(), self.trial_record("gr"), self.trial_record("eyelid"),
                              self._protocol, self.state.con("numGR"), int(self.state.act("msPerTimeStep")))
 
+    def write_session(self, path, mf_population=None):
+        """ECManagementDelay::writeDataToFile (Eyelid_Sim_CBM_Dev/src/ectrial/
+        ecmanagementdelay.cpp:275-290): the state, then the driver's data
+        file, in one file (the driver reads it back with CBMState(fstream&)
+        and ECTrialsData(fstream&)); with mf_population (networks.MFPopulation)
+        also its tables in path + "_MFPop"."""
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            st, td = os.path.join(d, "state"), os.path.join(d, "data")
+            self.writeToState(st)
+            self.write_trial_data(td)
+            with open(path, "wb") as out:
+                for part in (st, td):
+                    with open(part, "rb") as f:
+                        out.write(f.read())
+        if mf_population is not None:
+            mf_population.write(path + "_MFPop")
+
     def trial_record(self, kind):
         """Records of the running protocol: 'nc' / 'pc' spike counts
         [trials, bins, cells] (u32), 'eyelid' [trials, window steps] (f32), or

@@ -38,7 +38,9 @@
  *       [numDataTrials][window] (MFBYTES is then ignored).  -m MFPOP then writes the
  *       reference's ECMFPopulation estimated from that ECTrialsData
  *       (CBM_TOOLS_LIB_DEV/src/ecmfpopulation.cpp:11-65) with writeToFile, and
- *       -d DATA the ECTrialsData itself with its writeData.  PROTOCOL is "key value" text: trialSteps,
+ *       -d DATA the ECTrialsData itself with its writeData, and -s SESSION
+ *       the state followed by the ECTrialsData, as the driver's
+ *       writeDataToFile writes them.  PROTOCOL is "key value" text: trialSteps,
  *       csOn, csOff, csPhasicOff, csStartTrial, plastOnDelay, plastOffDelay,
  *       plastLTD, plastLTP, usErrDrive, mfSeed, mfThreshDecayTau, rates (a file
  *       of 3 x numMF f32: background, CS tonic, CS phasic), dataStartTrial,
@@ -182,7 +184,7 @@ int main(int argc, char **argv)
 	const char *statePath = argv[1], *mfPath = argv[2], *tracePath = argv[4], *finalPath = argv[5];
 	unsigned long steps = strtoul(argv[3], NULL, 10);
 	std::vector<int> seeds;
-	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL, *mfPopPath = NULL, *dataPath = NULL;
+	const char *eventsPath = NULL, *protocolPath = NULL, *recordsPath = NULL, *mfPopPath = NULL, *dataPath = NULL, *sessionPath = NULL;
 	int numGPUP2 = 0;
 	bool timeOnly = false;
 	unsigned long warm = 0;  // leading steps run before the clock starts
@@ -193,6 +195,7 @@ int main(int argc, char **argv)
 		else if (!strcmp(argv[i], "-r") && i + 1 < argc) recordsPath = argv[++i];
 		else if (!strcmp(argv[i], "-m") && i + 1 < argc) mfPopPath = argv[++i];
 		else if (!strcmp(argv[i], "-d") && i + 1 < argc) dataPath = argv[++i];
+		else if (!strcmp(argv[i], "-s") && i + 1 < argc) sessionPath = argv[++i];
 		else if (!strcmp(argv[i], "-g") && i + 1 < argc) numGPUP2 = atoi(argv[++i]);
 		else if (!strcmp(argv[i], "-t")) timeOnly = true;
 		else if (!strcmp(argv[i], "-w") && i + 1 < argc) warm = strtoul(argv[++i], NULL, 10);
@@ -457,6 +460,14 @@ int main(int argc, char **argv)
 			// the driver's data file (ECTrialsData::writeData, ectrialsdata.cpp)
 			std::fstream df(dataPath, std::ios::out | std::ios::binary | std::ios::trunc);
 			data->writeData(df);
+		}
+		if (sessionPath)
+		{
+			// ECManagementDelay::writeDataToFile (ecmanagementdelay.cpp:275-290):
+			// the state, then the trial data, in one file
+			std::fstream sf(sessionPath, std::ios::out | std::ios::binary | std::ios::trunc);
+			sim->writeToState(sf);
+			data->writeData(sf);
 		}
 		if (mfPopPath)
 		{

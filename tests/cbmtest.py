@@ -203,11 +203,13 @@ def protocol_rates(num_mf, seed=0):
     return np.stack([bg, tonic, phasic])
 
 
-def ref_run_protocol(state_path, proto, rates, nsteps, seeds, mf_population=None, data_file=None):
+def ref_run_protocol(state_path, proto, rates, nsteps, seeds, mf_population=None, data_file=None,
+                     session_file=None):
     """oracle/_ref/ref_run in protocol mode: (trace bytes, records bytes).
     With mf_population (a path), the reference's ECMFPopulation estimated
     from the run's ECTrialsData is written there; with data_file, the
-    ECTrialsData itself (writeData)."""
+    ECTrialsData itself (writeData); with session_file, the final state and
+    the ECTrialsData as the driver's writeDataToFile writes them."""
     with tempfile.TemporaryDirectory() as d:
         rp = os.path.join(d, "rates.f32")
         np.ascontiguousarray(rates, dtype=np.float32).tofile(rp)
@@ -222,6 +224,8 @@ def ref_run_protocol(state_path, proto, rates, nsteps, seeds, mf_population=None
             cmd += ["-m", mf_population]
         if data_file:
             cmd += ["-d", data_file]
+        if session_file:
+            cmd += ["-s", session_file]
         subprocess.run(cmd, check=True, capture_output=True)
         return np.fromfile(trp, dtype=np.uint8), np.fromfile(rec, dtype=np.uint8)
 

@@ -229,10 +229,14 @@ def test_trial_data_file_matches_reference(tmp_path):
     rates = cbmtest.protocol_rates(o.num["MF"], seed=1)
     steps = 3 * proto["trialSteps"]
     tr, _, _, eye, td = o.run_protocol(proto, rates, steps, trial_data=True)
-    ref_path = str(tmp_path / "ref.data")
-    cbmtest.ref_run_protocol(st, proto, rates, steps, [7], data_file=ref_path)
+    ref_path, ref_session = str(tmp_path / "ref.data"), str(tmp_path / "ref.session")
+    cbmtest.ref_run_protocol(st, proto, rates, steps, [7], data_file=ref_path, session_file=ref_session)
     ours = str(tmp_path / "ours.data")
     write_ec_trials_data(ours, td, cbmtest.gr_psh_from_trace(tr, proto, o.num["GR"]),
                          eye.reshape(proto["numDataTrials"], -1), proto, o.num["GR"])
     a, b = open(ours, "rb").read(), open(ref_path, "rb").read()
     assert len(a) == len(b) and a == b, next(i for i in range(min(len(a), len(b))) if a[i] != b[i])
+    # the driver's session file (writeDataToFile): final state, then the data
+    fin = str(tmp_path / "final.state")
+    o.save(fin)
+    assert open(ref_session, "rb").read() == open(fin, "rb").read() + a
