@@ -67,3 +67,82 @@ def write_ec_trials_data(path, trial_data, gr_psh, eyelid_raw, proto, num_gr, ms
             f.write(_line(ms_per_step, cur_trial, 32 * cur_buf, cur_buf, ts_total, rows))
             f.write(r.tobytes())
         f.write(_line(0))
+
+
+class _Reader:
+    """Whitespace-separated numbers and names, then raw bytes after one
+    separator character, as the reference's fstream readers take them
+    (operator>> then seekg(1, ios::cur))."""
+
+    def __init__(self, buf, pos=0):
+        self.buf, self.pos = buf, pos
+
+    def word(self):
+        b = self.buf
+        while b[self.pos: self.pos + 1].isspace():
+            self.pos += 1
+        start = self.pos
+        while self.pos < len(b) and not b[self.pos: self.pos + 1].isspace():
+            self.pos += 1
+        if start == self.pos:
+            raise ValueError("trial data file truncated")
+        return b[start: self.pos].decode()
+
+    def ints(self, n):
+        return [int(self.word()) for _ in range(n)]
+
+    def raw(self, dtype, count):
+        self.pos += 1  # the separator after the header line
+        nbytes = np.dtype(dtype).itemsize * count
+        if self.pos + nbytes > len(self.buf):
+            raise ValueError("trial data file truncated")
+        a = np.frombuffer(self.buf, dtype=dtype, count=count, offset=self.pos).copy()
+        self.pos += nbytes
+        return a
+
+
+def read_ec_trials_data(buf, pos=0):
+    """Parse a data file of ECTrialsData::writeData starting at byte pos
+    (ECTrialsData(fstream &), ectrialsdata.cpp): {"header": {...},
+    "eyelid": f32 [trials, steps], "psh": {name: f32 [bins, cells]},
+    "psh_trials": {name: trials recorded}, "raster": {name: u32 [trials,
+    rows, cells]}}."""
+    r = _Reader(buf, pos)
+    pre, cs, post, ms_total, ms_per_ts, ts_total, n_trials = r.ints(7)
+    out = {"header": dict(msPreCS=pre, msCS=cs, msPostCS=post, msTotal=ms_total, msPerTimeStep=ms_per_ts,
+                          tsTotal=ts_total, numTrials=n_trials), "psh": {}, "psh_trials": {}, "raster": {}}
+    e_trials, _, _, _, e_ts, _, _ = r.ints(7)
+    out["eyelid"] = r.raw(np.float32, e_trials * e_ts).reshape(e_trials, e_ts)
+    for _ in range(r.ints(1)[0]):
+        name = r.word()
+        cells, _, _, bins, _, trials = r.ints(6)
+        out["psh"][name] = r.raw(np.float32, bins * cells).reshape(bins, cells)
+        out["psh_trials"][name] = trials
+    for _ in range(r.ints(1)[0]):
+        name = r.word()
+        r.word()  # the raster's own copy of its name
+        cells, trials, _ = r.ints(3)
+        _, _, _, _, _, rows = r.ints(6)
+        out["raster"][name] = r.raw(np.uint32, trials * rows * cells).reshape(trials, rows, cells)
+    if r.ints(1)[0] != 0:
+        raise ValueError("raw-uint records are not read")
+    out["end"] = r.pos + (buf[r.pos: r.pos + 1] == b"\n")  # past the count's line end
+    return out
+
+
+def read_session(path):
+    """The driver's session file (writeDataToFile): (CBMState, trial data)
+    as ECManagementDelay's resume constructor reads it
+    (ecmanagementdelay.cpp:26-50)."""
+    import os
+    import tempfile
+    from . import CBMState
+    state = CBMState(path)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "state")
+        state.writeState(p)
+        state_bytes = os.path.getsize(p)
+    state = CBMState(path)  # writeState resets the GO->GO depression arrays, as the reference's does
+    with open(path, "rb") as f:
+        buf = f.read()
+    return state, read_ec_trials_data(buf, state_bytes)

@@ -240,3 +240,15 @@ def test_trial_data_file_matches_reference(tmp_path):
     fin = str(tmp_path / "final.state")
     o.save(fin)
     assert open(ref_session, "rb").read() == open(fin, "rb").read() + a
+    # and read back as the driver's resume constructor does
+    from cerebellum_simulation_b200 import networks
+    from cerebellum_simulation_b200.trialdata import read_session
+    state, data = read_session(ref_session)
+    assert state.getNumZones() == 1 and data["end"] == len(open(ref_session, "rb").read())
+    for name, h in td["psh"].items():
+        assert cbmtest.same_values(data["psh"][name].ravel(), h.ravel()).all(), name
+    for name, r in td["raster"].items():
+        assert np.array_equal(data["raster"][name], r), name
+    pop = networks.MFPopulation.from_trial_data(data["psh"]["mf"], data["psh_trials"]["mf"], proto["binSteps"],
+                                                data["header"]["msPreCS"], data["header"]["msCS"])
+    assert pop.bg.shape == (o.num["MF"],) and np.isfinite(pop.rates()).all()
