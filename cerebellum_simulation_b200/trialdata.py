@@ -105,19 +105,21 @@ def read_ec_trials_data(buf, pos=0):
     """Parse a data file of ECTrialsData::writeData starting at byte pos
     (ECTrialsData(fstream &), ectrialsdata.cpp): {"header": {...},
     "eyelid": f32 [trials, steps], "psh": {name: f32 [bins, cells]},
-    "psh_trials": {name: trials recorded}, "raster": {name: u32 [trials,
-    rows, cells]}}."""
+    "psh_trials": {name: trials recorded}, "psh_bin_steps": {name: steps a
+    bin}, "raster": {name: u32 [trials, rows, cells]}}."""
     r = _Reader(buf, pos)
     pre, cs, post, ms_total, ms_per_ts, ts_total, n_trials = r.ints(7)
     out = {"header": dict(msPreCS=pre, msCS=cs, msPostCS=post, msTotal=ms_total, msPerTimeStep=ms_per_ts,
-                          tsTotal=ts_total, numTrials=n_trials), "psh": {}, "psh_trials": {}, "raster": {}}
+                          tsTotal=ts_total, numTrials=n_trials), "psh": {}, "psh_trials": {},
+           "psh_bin_steps": {}, "raster": {}}
     e_trials, _, _, _, e_ts, _, _ = r.ints(7)
     out["eyelid"] = r.raw(np.float32, e_trials * e_ts).reshape(e_trials, e_ts)
     for _ in range(r.ints(1)[0]):
         name = r.word()
-        cells, _, _, bins, _, trials = r.ints(6)
+        cells, _, bin_steps, bins, _, trials = r.ints(6)
         out["psh"][name] = r.raw(np.float32, bins * cells).reshape(bins, cells)
         out["psh_trials"][name] = trials
+        out["psh_bin_steps"][name] = bin_steps
     for _ in range(r.ints(1)[0]):
         name = r.word()
         r.word()  # the raster's own copy of its name

@@ -153,3 +153,42 @@ def test_trial_data_matches_oracle(tmp_path, window, replay):
                          o_eye.reshape(proto["numDataTrials"], -1), proto, st.con("numGR"))
     assert open(tmp_path / "device.data", "rb").read() == open(tmp_path / "oracle.data", "rb").read()
     assert want["psh"]["go"].any() and want["raster"]["go"].any() and want["psh"]["mf"].any()
+
+
+def test_eyelid_session_matches_oracle(tmp_path):
+    """EyelidSession (the driver's trial loop and writeDataToFile) on the
+    device: its session file holds the oracle's final state and, byte for
+    byte, the data file of the oracle's records; its MF tables file holds
+    the tables it ran with."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    from cerebellum_simulation_b200.eyelid import EyelidSession
+    from cerebellum_simulation_b200.trialdata import read_session, write_ec_trials_data
+    st_path = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol()
+    n_trials = 3
+    rates = cbmtest.protocol_rates(cbm.CBMState(st_path).con("numMF"), seed=1)
+    pop = networks.MFPopulation(*rates)
+    fixed = ("trialSteps", "csOn", "csOff", "csPhasicOff", "csStartTrial", "dataStartTrial", "numDataTrials", "mfSeed")
+    s = EyelidSession(cbm.CBMState(st_path), pop, 7, n_trials, proto["trialSteps"], proto["csOn"], proto["csOff"],
+                      proto["csPhasicOff"], proto["csStartTrial"], proto["dataStartTrial"], proto["numDataTrials"],
+                      **{k: v for k, v in proto.items() if k not in fixed})
+    s.run(chunk=100)
+    out = str(tmp_path / "device.session")
+    s.write_data_to_file(out)
+    s.sim.close()
+    o = Oracle(st_path, seeds=[7])
+    tr, _, _, eye, td = o.run_protocol(s.protocol, rates, n_trials * proto["trialSteps"], trial_data=True)
+    fin = str(tmp_path / "oracle.state")
+    o.save(fin)
+    state, data = read_session(out)
+    dev_state = str(tmp_path / "device.state")
+    state.writeState(dev_state)
+    assert compare_states(fin, dev_state) == []
+    odata = str(tmp_path / "oracle.data")
+    n_gr = state.con("numGR")
+    write_ec_trials_data(odata, td, cbmtest.gr_psh_from_trace(tr, s.protocol, n_gr),
+                         eye.reshape(proto["numDataTrials"], -1), s.protocol, n_gr)
+    raw, want = open(out, "rb").read(), open(odata, "rb").read()
+    assert raw.endswith(want) and data["end"] == len(raw)
+    assert np.array_equal(networks.MFPopulation.read(out + "_MFPop").rates(), pop.rates())

@@ -252,3 +252,52 @@ def test_trial_data_file_matches_reference(tmp_path):
     pop = networks.MFPopulation.from_trial_data(data["psh"]["mf"], data["psh_trials"]["mf"], proto["binSteps"],
                                                 data["header"]["msPreCS"], data["header"]["msCS"])
     assert pop.bg.shape == (o.num["MF"],) and np.isfinite(pop.rates()).all()
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+def test_eyelid_session_follows_the_driver(tmp_path):
+    """EyelidSession (the driver's three constructors, run and
+    writeDataToFile) drives a simulator through the calls the device tests
+    check, with the protocol the driver uses; resuming from the reference's
+    own session file gives the state and the MF tables the reference
+    re-estimates from it."""
+    from cerebellum_simulation_b200 import networks
+    from cerebellum_simulation_b200.eyelid import EyelidSession
+    st_path = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol()
+    o = Oracle(st_path, seeds=[7])
+    rates = cbmtest.protocol_rates(o.num["MF"], seed=1)
+    steps = 3 * proto["trialSteps"]
+    ref_session, ref_pop = str(tmp_path / "ref.session"), str(tmp_path / "ref.mfpop")
+    cbmtest.ref_run_protocol(st_path, proto, rates, steps, [7], session_file=ref_session, mf_population=ref_pop)
+
+    calls = []
+
+    class FakeSim:
+        def __init__(self, state, seeds, device=0):
+            calls.append(("create", seeds, device))
+
+        def __getattr__(self, name):
+            return lambda *a, **k: calls.append((name, a, k))
+
+    args = (7, 4, 400, 120, 260, 150, 1, 0, 3)
+    s = EyelidSession.resume(ref_session, *args, sim_factory=FakeSim, preCS=60, postCS=80)
+    want = networks.MFPopulation.read(ref_pop)
+    assert np.array_equal(s.mf_population.rates(), want.rates())
+    assert s.state.getNumZones() == 1 and s.state.con("numGR") == o.num["GR"]
+    p = s.protocol
+    assert (p["trialSteps"], p["csOn"], p["csOff"], p["csPhasicOff"], p["csStartTrial"], p["mfSeed"]) == \
+        (400, 120, 260, 150, 1, 7)
+    # the driver's LTD step: -0.0005 x ((csOff - csOn + msLTDStartAPIO) / msLTDDurationIO), at least 0.5
+    ratio = max((140 + s.state.act("msLTDStartAPIO")) / s.state.act("msLTDDurationIO"), 0.5)
+    assert p["plastLTD"] == pytest.approx(-0.0005 * ratio) and p["plastLTP"] == 0.0005
+    s.run(chunk=50)
+    s.write_data_to_file(str(tmp_path / "out.session"))
+    names = [c[0] for c in calls]
+    assert names == ["create", "set_eyelid_protocol", "record_gr", "record_trial_data", "run", "write_session"]
+    assert calls[0][1] == [7] and calls[4][1] == (4 * 400,) and calls[4][2] == {"chunk": 50}
+    assert np.array_equal(calls[1][1][0], want.rates()) and calls[1][2] == p
+    assert calls[5][1] == (str(tmp_path / "out.session"), s.mf_population)
+    # the file constructor reads the same tables back
+    f = EyelidSession.from_files(st_path, ref_pop, *args, sim_factory=FakeSim)
+    assert np.array_equal(f.mf_population.rates(), want.rates())
