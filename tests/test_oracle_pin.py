@@ -191,30 +191,40 @@ def test_mf_population_estimate_matches_reference(tmp_path):
     assert open(out, "rb").read() == open(ref_path, "rb").read()
 
 
-@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
-def test_oracle_matches_reference_1m(tmp_path):
-    """The 1M-GR network (32 PC x 32,768 PF): the reference's PF->PC
-    reduction takes its widest shape here (512 threads, 32 pair-adds each,
-    kernels.cu:445-469), which the 16K networks never reach.  300 steps of
-    eyelid-coded MF input with a CS, plasticity and an error drive; records
-    and final state must equal the reference's."""
+@pytest.mark.parametrize("name", ["config2", "config3"])
+def test_oracle_matches_reference_golden_large(tmp_path, name):
+    """The 1M-GR network (32 PC x 32,768 PF: the reference's PF->PC reduction
+    in its widest shape, 512 threads and 32 pair-adds each, kernels.cu:
+    445-469, which the 16K networks never reach) over 300 active steps, and
+    the dense 4M-GR network (4096 GO, 128 PC) over 60: every trace record and
+    the final state against the reference's, recorded by
+    tests/golden/make_golden.py."""
     from cerebellum_simulation_b200 import networks
-    net = networks.config2_network(seed=0)
-    st = str(tmp_path / "c2.state")
+    gold = cbmtest.load_json(name + "_digests.json")
+    net = networks.config2_network(seed=0) if name == "config2" else networks.config3_network(seed=0)
+    st = str(tmp_path / "net.state")
     net.writeState(st)
-    steps = 300
-    mf = networks.eyelid_mf_stream(1024, steps, seed=0, cs_on=50, cs_off=250)
-    ev = {2: [("plast", 0, -0.01, 0.005)], 249: [("errdrive", 0, 1.0)]}
-    fin_ref = str(tmp_path / "ref_final.state")
-    ref = cbmtest.ref_run(st, mf, [7], ev, final_path=fin_ref).reshape(steps, -1)
+    with open(st, "rb") as f:
+        assert cbmtest.sha(np.frombuffer(f.read(), np.uint8)) == gold["initial_state"], \
+            "network generator is not deterministic"
+    steps = gold["steps"]
+    if name == "config2":
+        mf = networks.eyelid_mf_stream(1024, steps, seed=0, cs_on=50, cs_off=250)
+        ev = {2: [("plast", 0, -0.01, 0.005)], 249: [("errdrive", 0, 1.0)]}
+    else:
+        mf = networks.config3_mf_stream(1024, steps, seed=0)
+        ev = {1: [("plast", 0, -0.0005, 0.0005)], 40: [("errdrive", 0, 1.0)]}
     o = Oracle(st, seeds=[7])
     tr = o.run(mf, ev)
-    assert cbmtest.first_difference(ref, tr, o.num) is None
-    gr_spikes = np.unpackbits(tr[:, : o.num["GR"] // 8], axis=1).sum()
-    assert gr_spikes > 100000
-    fin = str(tmp_path / "oracle_final.state")
+    assert tr.shape[1] == gold["record_bytes"]
+    assert np.unpackbits(tr[:, : o.num["GR"] // 8], axis=1).sum() > 100000
+    got = [cbmtest.sha(r) for r in tr]
+    bad = [i for i, (a, b) in enumerate(zip(got, gold["records"])) if a != b]
+    assert not bad, f"first differing step {bad[0] + 1}"
+    fin = str(tmp_path / "final.state")
     o.save(fin)
-    assert open(fin, "rb").read() == open(fin_ref, "rb").read()
+    with open(fin, "rb") as f:
+        assert cbmtest.sha(np.frombuffer(f.read(), np.uint8)) == gold["final_state"]
 
 
 @pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
