@@ -14,6 +14,7 @@ import subprocess
 import sys
 
 import numpy as np
+import pytest
 
 from cerebellum_simulation_b200 import networks
 
@@ -82,3 +83,52 @@ def test_random_mf_population_follows_the_reference_rules():
     assert np.all((bg[plain] >= 1) & (bg[plain] < 10))
     q = networks.MFPopulation.random(1024, 3, 0.05, 0.03, 0.1, 1, 2, 30, 60, 110, 10, 5, 40, 80, 150)
     assert np.array_equal(q.rates(), p.rates())
+
+
+def test_mf_population_file_round_trip_and_truncation(tmp_path):
+    p = networks.MFPopulation.random(256, 1, 0.05, 0.05, 0.1, 1, 2, 30, 60, 110, 10, 5, 40, 80, 150)
+    path = str(tmp_path / "pop")
+    p.write(path)
+    q = networks.MFPopulation.read(path)
+    assert np.array_equal(p.rates(), q.rates())
+    data = open(path, "rb").read()
+    assert len(data) == 4 + 3 * 256 * 4
+    with open(path, "wb") as f:
+        f.write(data[:-4])
+    with pytest.raises(ValueError):
+        networks.MFPopulation.read(path)
+
+
+def test_eyelid_out_smoothing_rule():
+    """EyelidOut::updateData: the first three values as they are, then the
+    mean of the three previous recorded values and the new one."""
+    import cerebellum_simulation_b200 as cbm
+    raw = np.arange(1, 9, dtype=np.float32)[None, :]
+    out = cbm.eyelid_out(raw)
+    want = list(raw[0, :3])
+    for t in range(3, 8):
+        want.append(np.float32((np.float32(want[t - 3] + want[t - 2]) + want[t - 1] + raw[0, t]) / 4))
+    assert np.array_equal(out[0], np.array(want, np.float32))
+
+
+def test_trial_data_file_reader_rejects_truncation(tmp_path):
+    from cerebellum_simulation_b200.trialdata import read_ec_trials_data, write_ec_trials_data
+    proto = dict(preCS=40, postCS=40, csOn=100, csOff=180, binSteps=10, numDataTrials=2)
+    rec_len, cells = 160, {"go": 8, "grInputGO": 8, "goInputGO": 8, "goOutSynScale": 8, "mf": 16, "sc": 4,
+                           "bc": 4, "pc": 2, "io": 1}
+    rng = np.random.Generator(np.random.PCG64(0))
+    td = {"psh": {n: rng.random((16, c)).astype(np.float32) for n, c in cells.items()},
+          "raster": {n: rng.integers(0, 2 ** 32, (2, rec_len // 32, c), dtype=np.uint32)
+                     for n, c in (("go", 8), ("sc", 4), ("bc", 4), ("pc", 2), ("nc", 3), ("io", 1))}}
+    path = str(tmp_path / "data")
+    write_ec_trials_data(path, td, rng.integers(0, 9, (16, 40)), rng.random((2, rec_len)), proto, 40)
+    buf = open(path, "rb").read()
+    back = read_ec_trials_data(buf)
+    assert back["end"] == len(buf) and back["header"]["msTotal"] == rec_len
+    for n, h in td["psh"].items():
+        assert np.array_equal(back["psh"][n], h)
+    for n, r in td["raster"].items():
+        assert np.array_equal(back["raster"][n], r)
+    assert back["psh"]["gr"].shape == (16, 4)
+    with pytest.raises(ValueError):
+        read_ec_trials_data(buf[: len(buf) // 2])
