@@ -29,7 +29,7 @@ template <typename T> T *Network::alloc(size_t n)
 	// whole 16-byte units, so that arrays can be copied with 16-byte accesses
 	size_t bytes = (std::max<size_t>(n * sizeof(T), 16) + 15) & ~(size_t)15;
 	if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
-	cudaMemset(p, 0, bytes);
+	if (cudaMemset(p, 0, bytes) != cudaSuccess) { cudaFree(p); return nullptr; }
 	allocs_.push_back(p);
 	allocBytes_[p] = bytes;
 	return (T *)p;
@@ -651,7 +651,8 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 			for (uint32_t i = 0; i < c.numIO; i++)
 				sel[c.numIO + i] = tm[i] < h.tsLTDEndIO ? 1 : (tm[i] > h.tsLTPStartAPIO ? 2 : 0);
 		}
-		cudaMemcpy(Q.plastSel, sel.data(), sel.size(), cudaMemcpyHostToDevice);
+		if (!Q.plastSel) return "device allocation failed";
+		CK(cudaMemcpy(Q.plastSel, sel.data(), sel.size(), cudaMemcpyHostToDevice), "uploading the plasticity selector");
 		ctl.ltdStep[z] = a.synLTDStepSizeGRtoPC;
 		ctl.ltpStep[z] = a.synLTPStepSizeGRtoPC;
 		ctl.errDrive[z] = zs.errDrive;
