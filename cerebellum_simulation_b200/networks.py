@@ -17,6 +17,7 @@ MF spikes follow the reference's regenerating Poisson rule
 counter-based stream (cbm_rng.hpp), so any MF sequence can be regenerated
 from (seed, step, fibre).
 """
+import math
 import os
 
 import numpy as np
@@ -259,14 +260,20 @@ class StateVariableMF:
     """Cart-pole-style MF rate coding: each of n_vars state variables owns an
     equal, ordered share of the fibres (StateVariable::assignOrderedMFInds,
     Matthew_Sim_CBM/includes/statevariable.hpp:35-43, with the unassigned
-    list built from the last fibre down, environment.cpp:47-51), and fibre k
-    of a variable fires at a Gaussian blend of its relaxed and excited rates
-    around preferred value min + (k + 1/2) * range / n (gaussMFAct,
-    statevariable.hpp:108-129): with a = exp(-(x - mean)^2 / (2 var^2)), the
-    rate is a * excited + (1 - a) * relaxed, in float32.  Relaxed rates are
-    U(1, 10) Hz and excited rates 40 Hz (Environment::setupMossyFibers,
-    environment.cpp:19-39, whose excited range expression reduces to its
-    minimum).  var is sigma_frac of the variable's range.
+    list built from the last fibre down, environment.cpp:47-51), and the k-th
+    fibre of a variable fires at a blend of its relaxed and excited rates
+    weighted by a Gaussian of the distance between the variable's value and
+    the fibre's preferred value (gaussMFAct, statevariable.hpp:108-129).
+    rates() follows gaussMFAct's arithmetic: float values, the preferred
+    values accumulated fibre by fibre from min + interval / 2, the width
+    gaussWidth x interval, the Gaussian's exp and normalisation in double
+    (the C library's exp, as the reference's unqualified exp on a float
+    resolves to it), each rounded to float where the reference stores a
+    float.  Relaxed rates are U(1, 10) Hz and excited rates 40 Hz
+    (Environment::setupMossyFibers, environment.cpp:19-39, whose excited
+    range expression reduces to its minimum).  gauss_width defaults to
+    sigma_frac x the fibres a variable owns, a width of sigma_frac of the
+    variable's range.
 
     The environment that moves the variables (the cart-pole dynamics) lies
     outside the simulator; values() supplies a fixed synthetic trajectory:
@@ -276,41 +283,61 @@ class StateVariableMF:
 
     PERIODS = (1000.0, 1700.0, 2300.0, 3100.0)
 
-    def __init__(self, num_mf, seed=0, n_vars=4, sigma_frac=0.2, lo=-1.0, hi=1.0):
+    def __init__(self, num_mf, seed=0, n_vars=4, sigma_frac=0.2, lo=-1.0, hi=1.0, gauss_width=None):
+        f32 = np.float32
         rng = np.random.Generator(np.random.PCG64(seed + 303))
         self.num_mf = num_mf
         self.n_vars = n_vars
-        self.lo, self.hi = np.float32(lo), np.float32(hi)
+        self.lo, self.hi = f32(lo), f32(hi)
         self.relaxed = rng.uniform(1.0, 10.0, num_mf).astype(np.float32)
         self.excited = np.full(num_mf, 40.0, dtype=np.float32)
         self.phase = rng.uniform(0, 2 * np.pi, n_vars)
-        per = num_mf // n_vars
-        rng_f = np.float32(hi - lo)
-        interval = np.float32(rng_f / np.float32(per))
+        # StateVariable::initialize: numMF = totalMF * mfProportion, a float product truncated
+        per = int(f32(num_mf) * (f32(1) / f32(n_vars)))
+        self.per = per
+        self.gauss_width = f32(sigma_frac * per) if gauss_width is None else f32(gauss_width)
+        self.interval = f32(f32(self.hi - self.lo) / f32(per))
+        # preferred values: pos = min + interval / 2.0 (a double sum stored as float), then pos += interval
+        pos = f32(float(self.lo) + float(self.interval) / 2.0)
+        means = np.zeros(per, np.float32)
+        for k in range(per):
+            means[k] = pos
+            pos = f32(pos + self.interval)
         self.var_of = np.full(num_mf, -1, dtype=np.int64)
         self.mean = np.zeros(num_mf, dtype=np.float32)
         for v in range(n_vars):
-            idx = np.arange(v * per, (v + 1) * per)
-            self.var_of[idx] = v
-            self.mean[idx] = (self.lo + interval / np.float32(2) + interval * np.arange(per, dtype=np.float32)).astype(
-                np.float32)
-        self.variance = np.float32(np.float32(sigma_frac) * rng_f)
+            self.var_of[v * per: (v + 1) * per] = v
+            self.mean[v * per: (v + 1) * per] = means
+        self.variance = f32(self.gauss_width * self.interval)  # the reference's name for the width
+        var2 = f32(self.variance * self.variance)
+        self._den = f32(f32(2) * var2)
+        self._norm = math.sqrt(2 * math.pi * float(var2))
+        self._max_possible = f32(1.0 / self._norm)
 
     def values(self, t):
         """The n_vars state-variable values at step t (synthetic trajectory)."""
         ph = 2 * np.pi * t / np.array(self.PERIODS[: self.n_vars]) + self.phase
         return (self.lo + (self.hi - self.lo) * (0.5 + 0.45 * np.sin(ph))).astype(np.float32)
 
-    def rates(self, t):
-        """[num_mf] Hz at step t; fibres beyond the variables' shares stay relaxed."""
-        x = self.values(t)
+    def rates_for(self, x):
+        """[num_mf] Hz for state values x [n_vars] (gaussMFAct for every
+        variable); fibres beyond the variables' shares stay relaxed."""
+        f32 = np.float32
         out = self.relaxed.copy()
         m = self.var_of >= 0
-        xv = np.clip(x[self.var_of[m]], self.lo, self.hi).astype(np.float32)
+        x = np.asarray(x, dtype=np.float32)
+        xv = np.maximum(self.lo, np.minimum(self.hi, x))[self.var_of[m]]
         d = (xv - self.mean[m]).astype(np.float32)
-        a = np.exp(-(d * d) / (np.float32(2) * (self.variance * self.variance)), dtype=np.float32)
-        out[m] = (a * self.excited[m] + (np.float32(1) - a) * self.relaxed[m]).astype(np.float32)
+        arg = ((-(d * d)).astype(np.float32) / self._den).astype(np.float32)
+        value = (np.array([math.exp(a) for a in arg.astype(np.float64)]) / self._norm).astype(np.float32)
+        a = (value / self._max_possible).astype(np.float32)
+        out[m] = ((a * self.excited[m]).astype(np.float32) +
+                  ((f32(1) - a).astype(np.float32) * self.relaxed[m]).astype(np.float32)).astype(np.float32)
         return out
+
+    def rates(self, t):
+        """[num_mf] Hz at step t of the synthetic trajectory."""
+        return self.rates_for(self.values(t))
 
 
 def config3_mf_stream(num_mf, steps, seed=0):

@@ -16,6 +16,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "libcbm_oracle.so")
 REF_RUN = os.path.join(ORACLE_DIR, "_ref", "ref_run")
 REF_GEN = os.path.join(ORACLE_DIR, "_ref", "ref_gen")
+REF_STATEVAR = os.path.join(ORACLE_DIR, "_ref", "ref_statevar")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 

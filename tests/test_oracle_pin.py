@@ -311,3 +311,28 @@ def test_eyelid_session_follows_the_driver(tmp_path):
     # the file constructor reads the same tables back
     f = EyelidSession.from_files(st_path, ref_pop, *args, sim_factory=FakeSim)
     assert np.array_equal(f.mf_population.rates(), want.rates())
+
+
+@pytest.mark.skipif(not os.path.exists(cbmtest.REF_STATEVAR), reason="reference harness oracle/_ref not built")
+def test_state_variable_coding_matches_reference():
+    """networks.StateVariableMF's rates equal the reference's StateVariable
+    (Gaussian updates of 4 variables over ordered fibre shares, compiled from
+    Matthew_Sim_CBM/includes/statevariable.hpp) bit for bit, over a stretch
+    of the synthetic trajectory plus clamped and edge values."""
+    import subprocess
+    import tempfile
+    from cerebellum_simulation_b200 import networks
+    c = networks.StateVariableMF(1024, seed=4)
+    vals = np.stack([c.values(t) for t in range(0, 3000, 37)]).astype(np.float32)
+    vals[3] = np.float32([-5, 5, -1, 1])
+    with tempfile.TemporaryDirectory() as d:
+        for n, a in (("r", c.relaxed), ("e", c.excited), ("v", vals)):
+            np.ascontiguousarray(a, np.float32).tofile(os.path.join(d, n))
+        out = os.path.join(d, "o")
+        subprocess.run([cbmtest.REF_STATEVAR, "1024", "4", repr(float(c.lo)), repr(float(c.hi)),
+                        repr(float(c.gauss_width)), os.path.join(d, "r"), os.path.join(d, "e"), os.path.join(d, "v"),
+                        str(len(vals)), out], check=True, capture_output=True)
+        ref = np.fromfile(out, np.float32).reshape(len(vals), 1024)
+    ours = np.stack([c.rates_for(v) for v in vals])
+    assert np.array_equal(ref.view(np.uint32), ours.view(np.uint32))
+    assert ours.max() > 39 and ours.min() < 10
