@@ -2,6 +2,7 @@
 #include "cbm_sim.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstddef>
 #include <cstdio>
@@ -754,7 +755,8 @@ std::string Network::setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s)
 	// (poissonregencells.cpp:12-19): the first draw of the seed's stream.
 	const float msPerTS = 1.0f;
 	d.sPerTS = msPerTS / 1000;
-	d.mfThreshDecay = 1 - expf(-msPerTS / p.mfThreshDecayTau);
+	// 1 - exp(...) in double, stored as float (poissonregencells.cpp:20)
+	d.mfThreshDecay = (float)(1.0 - std::exp((double)(-msPerTS / p.mfThreshDecayTau)));
 	const double u0 = (double)rng::uniform24((uint32_t)p.mfSeed, rng::kStreamNCIO, 0);
 	const int derived = (int)(u0 * 2147483648.0);
 	d.mfKey = rng::streamKey((uint32_t)derived, rng::kStreamNCIO);

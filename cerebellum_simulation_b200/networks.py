@@ -56,9 +56,10 @@ def uniform24(seed, stream, counter):
 class RegenPoissonMF:
     """PoissonRegenCells (poissonregencells.cpp:10-66) over numMF fibres.
 
-    threshDecay = 1 - exp(-msPerTS/threshDecayTau) and the per-step rule
-    thresh += (1-thresh)*threshDecay; ap = U < (freq*sPerTS)*thresh;
-    thresh = (!ap)*thresh, all in float32.
+    threshDecay = 1 - exp(-msPerTS/threshDecayTau) (exp in double, as the
+    reference's call on a float resolves to the C library's double exp) and
+    the per-step rule thresh += (1-thresh)*threshDecay; ap = U < (freq*sPerTS)
+    *thresh; thresh = (!ap)*thresh, in float32.
     """
 
     def __init__(self, num_mf, seed, thresh_decay_tau=4.0, ms_per_step=1.0):
@@ -66,7 +67,8 @@ class RegenPoissonMF:
         self.seed = seed
         ms = np.float32(ms_per_step)
         self.s_per_ts = np.float32(ms / np.float32(1000))
-        self.thresh_decay = np.float32(np.float32(1) - np.exp(np.float32(-ms / np.float32(thresh_decay_tau)), dtype=np.float32))
+        # threshDecay = 1 - exp(-msPerTS / tau): a float quotient, the C library's double exp, stored as float
+        self.thresh_decay = np.float32(1.0 - math.exp(float(np.float32(-ms / np.float32(thresh_decay_tau)))))
         self.thresh = np.ones(num_mf, dtype=np.float32)
         self.t = 0
 

@@ -1230,7 +1230,9 @@ void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const 
 	 * poissonregencells.cpp:10-35): its generator's seed is the first draw of
 	 * a generator seeded with mfSeed, scaled to [0, 2^31) */
 	const float msPerTS = 1.0f, sPerTS = msPerTS / 1000;
-	const float threshDecay = 1 - expf(-msPerTS / p->mfThreshDecayTau);
+	/* 1 - exp(...) with the C library's double exp, stored as float, as
+	 * poissonregencells.cpp:20 computes it */
+	const float threshDecay = (float)(1 - exp((double)(-msPerTS / p->mfThreshDecayTau)));
 	const double u0 = (double)cbm_oracle_uniform24((uint32_t)p->mfSeed, CBM_STREAM_NCIO, 0);
 	const uint32_t mfGenSeed = (uint32_t)(int)(u0 * 2147483648.0);
 	float *thresh = malloc(numMF * sizeof(float));
