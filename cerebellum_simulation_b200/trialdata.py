@@ -148,3 +148,126 @@ def read_session(path):
     with open(path, "rb") as f:
         buf = f.read()
     return state, read_ec_trials_data(buf, state_bytes)
+
+
+class PeriStimHist:
+    """PeriStimHistFloat's getters (peristimhist/peristimhistfloat.cpp) over
+    one histogram [bins, cells]."""
+
+    def __init__(self, counts, steps_per_bin, trials):
+        self.counts = np.asarray(counts, dtype=np.float32)
+        self.steps_per_bin, self.trials = int(steps_per_bin), int(trials)
+
+    def getCellPSH(self, cellN):
+        return [float(v) for v in self.counts[:, cellN]]
+
+    def getPopPSHs(self):
+        return [self.getCellPSH(i) for i in range(self.getNumCells())]
+
+    def getNumCells(self):
+        return self.counts.shape[1]
+
+    def getNumBins(self):
+        return self.counts.shape[0]
+
+    def getBinWidthInMS(self):
+        return self.steps_per_bin
+
+    def getNumTrials(self):
+        return self.trials
+
+
+class SpikeRaster:
+    """SpikeRasterBitArray's getters (spikeraster/spikerasterbitarray.cpp:
+    82-170) over one raster [trials, rows, cells] of 32-step apBuf words:
+    bit 31 of a row is its earliest step."""
+
+    def __init__(self, words, ms_per_step=1, trials_done=None):
+        self.words = np.asarray(words, dtype=np.uint32)
+        self.ms_per_step = int(ms_per_step)
+        self.trials_done = self.words.shape[0] if trials_done is None else int(trials_done)
+
+    def getNumCells(self):
+        return self.words.shape[2]
+
+    def getNumTrials(self):
+        return self.trials_done
+
+    def getUpdateInterval(self):
+        return 32
+
+    def getCellSpikeTimes(self, cellN, trialN=None, offset=0):
+        """Spike times of a cell in one trial, or (trialN None, the
+        reference's two-argument form) in every recorded trial."""
+        if trialN is None:
+            return [self.getCellSpikeTimes(cellN, t, offset) for t in range(self.trials_done)]
+        times, t = [], offset
+        for w in self.words[trialN, :, cellN]:
+            for j in range(32):
+                if (int(w) << j) & 0x80000000:
+                    times.append(t)
+                t += self.ms_per_step
+        return times
+
+    def getPopSpikesAtTS(self, timeStep, trialN):
+        row, bit = divmod(int(timeStep), 32)
+        if row >= self.words.shape[1]:
+            return [False] * self.getNumCells()
+        return [bool(w & (0x80000000 >> bit)) for w in self.words[trialN, row]]
+
+
+class TrialsData:
+    """ECTrialsData's getters (interfaces/ectrialsdata.cpp) over a data
+    file (``from_file``) or a simulator's records (``from_sim``)."""
+
+    def __init__(self, parsed):
+        self._d = parsed
+        h = parsed["header"]
+        self._ms_per_step = h["msPerTimeStep"]
+
+    @classmethod
+    def from_file(cls, path, offset=0):
+        with open(path, "rb") as f:
+            return cls(read_ec_trials_data(f.read(), offset))
+
+    @classmethod
+    def from_sim(cls, sim):
+        import os
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "data")
+            sim.write_trial_data(p)
+            return cls.from_file(p)
+
+    def getPSH(self, cellT):
+        return PeriStimHist(self._d["psh"][cellT], self._d["psh_bin_steps"][cellT], self._d["psh_trials"][cellT])
+
+    def getRaster(self, cellT):
+        return SpikeRaster(self._d["raster"][cellT], self._ms_per_step)
+
+    def getEyelidData(self, trialN):
+        return [float(v) for v in self._d["eyelid"][trialN]]
+
+    def getTSPerRasterUpdate(self):
+        return 32 if self._d["raster"] else 0
+
+    def getMSPreTrial(self):
+        return self._d["header"]["msPreCS"]
+
+    def getMSTrial(self):
+        return self._d["header"]["msCS"]
+
+    def getMSPostTrial(self):
+        return self._d["header"]["msPostCS"]
+
+    def getMSPerTimeStep(self):
+        return self._ms_per_step
+
+    def getMSTotal(self):
+        return self._d["header"]["msTotal"]
+
+    def getTimeStepsTotal(self):
+        return self._d["header"]["tsTotal"]
+
+    def getMaxNumTrials(self):
+        return self._d["header"]["numTrials"]

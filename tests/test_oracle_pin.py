@@ -336,3 +336,52 @@ def test_state_variable_coding_matches_reference():
     ours = np.stack([c.rates_for(v) for v in vals])
     assert np.array_equal(ref.view(np.uint32), ours.view(np.uint32))
     assert ours.max() > 39 and ours.min() < 10
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+def test_trials_data_getters_read_the_reference_file(tmp_path):
+    """trialdata.TrialsData over the reference's own data file: the
+    histograms' trial counts and bin widths, and the rasters' spike times
+    (SpikeRasterBitArray::getCellSpikeTimes: bit 31 first, one step apart),
+    which must be the window steps at which the oracle's trace has the cells
+    spiking (time k is window step k + 1: the first update comes at window
+    step 32 and covers steps 1-32)."""
+    from cerebellum_simulation_b200.trialdata import TrialsData
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.short_protocol()
+    o = Oracle(st, seeds=[7])
+    rates = cbmtest.protocol_rates(o.num["MF"], seed=1)
+    steps = 3 * proto["trialSteps"]
+    tr, _, _, eye, _ = o.run_protocol(proto, rates, steps, trial_data=True)
+    ref_path = str(tmp_path / "ref.data")
+    cbmtest.ref_run_protocol(st, proto, rates, steps, [7], data_file=ref_path)
+    d = TrialsData.from_file(ref_path)
+    rec_from = proto["csOn"] - proto["preCS"]
+    rec_len = proto["csOff"] + proto["postCS"] - rec_from
+    assert d.getMSTotal() == rec_len and d.getMaxNumTrials() == proto["numDataTrials"]
+    assert d.getTSPerRasterUpdate() == 32
+    go = d.getPSH("go")
+    assert go.getNumTrials() == proto["numDataTrials"] and go.getBinWidthInMS() == proto["binSteps"]
+    assert go.getNumBins() == -(-rec_len // proto["binSteps"]) and go.getNumCells() == o.num["GO"]
+    # spike times from the trace, field by field
+    off, fields = 0, {}
+    for name, dt, cnt in cbmtest.record_layout(o.num):
+        nb = np.dtype(dt).itemsize * cnt
+        fields[name] = tr[:, off: off + nb].view(dt)
+        off += nb
+    rows = rec_len // 32
+    seen = 0
+    for name, key in (("pc", "apPC0"), ("go", "apGO"), ("nc", "apNC0")):
+        raster = d.getRaster(name)
+        for trial in range(proto["numDataTrials"]):
+            first = (proto["dataStartTrial"] + trial) * proto["trialSteps"] + rec_from  # trace row of window step 0
+            ap = fields[key][first + 1: first + 1 + 32 * rows]
+            for cell in range(raster.getNumCells()):
+                want = [int(k) for k in np.nonzero(ap[:, cell])[0]]
+                assert raster.getCellSpikeTimes(cell, trial) == want, (name, trial, cell)
+                seen += len(want)
+        k = 37
+        assert raster.getPopSpikesAtTS(k, 0) == [bool(v) for v in
+                                                  fields[key][proto["dataStartTrial"] * proto["trialSteps"] + rec_from + k + 1]]
+    assert seen > 100
+    assert d.getEyelidData(0)[:3] == [float(v) for v in eye[:3]]
