@@ -57,7 +57,54 @@ def parse():
     ap.add_argument("--no-truth", action="store_true",
                     help="surrogate workload: skip simulating every candidate (the plain sweep's answer)")
     ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--dry-run", action="store_true",
+                    help="exercise the rank plumbing (launch, gloo process group, max over ranks) without a GPU")
     return ap.parse_args()
+
+
+def standalone_networks():
+    """cerebellum_simulation_b200/networks.py loaded as a module of its own
+    (not through the package, whose import loads the CUDA library)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "cbm_networks_standalone", os.path.join(ROOT, "cerebellum_simulation_b200", "networks.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def launch_ranks(n):
+    """Re-run this command as n ranks, one process per GPU, under
+    torch.distributed.run on this node (127.0.0.1); rank 0 prints the line."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    rc = subprocess.run(cmd).returncode
+    if rc:
+        sys.exit(rc)
+
+
+def main_dry_run(args):
+    """The multi-rank plumbing alone, on the CPU: every rank joins a gloo
+    process group, contributes a timing, and rank 0 prints one line with the
+    maximum over ranks and the world size (no device work, no contract
+    metric)."""
+    from cerebellum_simulation_b200 import replicas
+    dist, rank, world, local = replicas.init("gloo", timeout_s=60)
+    t0 = time.perf_counter()
+    ms = (time.perf_counter() - t0) * 1000.0 + 1.0 + rank
+    ms_max, = replicas.max_over_ranks(dist, [ms])
+    pids = [os.getpid()]
+    if dist is not None:
+        pids = [None] * world
+        dist.all_gather_object(pids, os.getpid())
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "ranks": world, "pids": pids, "ms_max": ms_max,
+                          "throughput": replicas.throughput(world, args.steps, ms_max)}))
+    replicas.finish(dist)
 
 
 def protocol_events(t0, t1):
@@ -181,21 +228,50 @@ def profiled_traffic():
     return None
 
 
+CPU_STEPS, CPU_WARMUP = 200, 20   # the CPU baseline's bounded sample of the 1M workload
+
+
+def stream_plan(steps, warmup, chunk, cpu_steps=CPU_STEPS, cpu_warmup=CPU_WARMUP):
+    """Rows of the 1M workload's MF stream that each consumer in main() reads.
+
+    main: warm-up, the flushed timed steps, then the continuous ones;
+    roofline: the kernel-timing copy (flushed passes, then graph replay);
+    e2e: 20 untimed then the timed per-step C-ABI calls; cpu: the CPU
+    baseline's untimed then timed steps.  One stream of `rows` rows serves
+    them all, so every slice fits by construction."""
+    n_roof = min(steps, 1000)
+    n_roof -= n_roof % chunk
+    n_roof = n_roof or chunk
+    n_fl = min(steps, 300)
+    n_e2e = min(steps, 2000)
+    plan = {"main": warmup + 2 * steps, "roofline": n_fl + n_roof + 2 * chunk, "e2e": 20 + n_e2e,
+            "cpu": cpu_warmup + cpu_steps, "n_roof": n_roof, "n_fl": n_fl, "n_e2e": n_e2e}
+    plan["rows"] = max(plan["main"], plan["roofline"], plan["e2e"], plan["cpu"])
+    return plan
+
+
 def cpu_reference(state_path, mf, steps, threads, warmup=0):
     """The reference's own calcActivity (oracle/_ref, OpenMP build) on host cores:
-    warmup untimed steps, then steps timed ones (mf holds rows for both)."""
+    warmup untimed steps, then steps timed ones (mf holds rows for both).
+    Returns None when the harness is not built; raises ValueError when mf is
+    too short and RuntimeError when the harness fails."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_run_omp")
     if not os.path.exists(exe):
         exe = os.path.join(ROOT, "oracle", "_ref", "ref_run")
         threads = 1
     if not os.path.exists(exe):
         return None
+    if len(mf) < warmup + steps:
+        raise ValueError(f"the CPU sample needs {warmup + steps} MF rows, the stream has {len(mf)}")
     with tempfile.TemporaryDirectory() as d:
         mfp = os.path.join(d, "mf.u8")
         np.ascontiguousarray(mf[:warmup + steps], dtype=np.uint8).tofile(mfp)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        out = subprocess.run([exe, state_path, mfp, str(warmup + steps), "-", "-", "7", "-t", "-w", str(warmup)],
-                             capture_output=True, text=True, env=env, check=True).stdout
+        proc = subprocess.run([exe, state_path, mfp, str(warmup + steps), "-", "-", "7", "-t", "-w", str(warmup)],
+                              capture_output=True, text=True, env=env)
+        if proc.returncode != 0:
+            raise RuntimeError(f"{os.path.basename(exe)} exited {proc.returncode}: {proc.stderr.strip()[-300:]}")
+        out = proc.stdout
     line = [l for l in out.splitlines() if l.startswith("{")][-1]
     r = json.loads(line)
     res = {"value": r["steps_per_s"], "unit": "steps/s", "cores": threads, "kind": "reference",
@@ -209,9 +285,11 @@ def cpu_reference(state_path, mf, steps, threads, warmup=0):
         with tempfile.TemporaryDirectory() as d:
             mfp = os.path.join(d, "mf.u8")
             np.ascontiguousarray(mf[:warmup + n1], dtype=np.uint8).tofile(mfp)
-            out = subprocess.run([one, state_path, mfp, str(warmup + n1), "-", "-", "7", "-t", "-w", str(warmup)],
-                                 capture_output=True, text=True, check=True).stdout
-        r1 = json.loads([l for l in out.splitlines() if l.startswith("{")][-1])
+            proc = subprocess.run([one, state_path, mfp, str(warmup + n1), "-", "-", "7", "-t", "-w", str(warmup)],
+                                  capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"ref_run exited {proc.returncode}: {proc.stderr.strip()[-300:]}")
+        r1 = json.loads([l for l in proc.stdout.splitlines() if l.startswith("{")][-1])
         res["single_core"] = {"value": r1["steps_per_s"], "unit": "steps/s", "cores": 1,
                               "sample": f"{n1} steps after the same {warmup} untimed steps, no OpenMP"}
     return res
@@ -533,15 +611,25 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    total_steps = args.warmup + 2 * args.steps  # flushed timed steps, then the continuous ones
-
-    from cerebellum_simulation_b200 import networks
+    if args.impl == "b200" and args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
+    if args.dry_run:
+        return main_dry_run(args)
+    plan = stream_plan(args.steps, args.warmup, args.chunk)
+    total_steps = plan["main"]  # warm-up, the flushed timed steps, then the continuous ones
 
     if args.impl == "reference":
         if rank != 0:
             return
+        # the reference's own host code on the host cores, on the same
+        # network and input as the B200 arm: the network is built by the
+        # package's generator module loaded on its own, into an oracle-made
+        # state, so nothing of the product's library is loaded here
+        networks = standalone_networks()
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle_state import OracleState
         threads = os.cpu_count() or 1
-        st = networks.config2_network(seed=args.seed)
+        st = networks.config2_network(seed=args.seed, new_state=OracleState.new)
         n_ref, w_ref = min(args.steps, 200), min(args.warmup, 200)
         mf = networks.eyelid_mf_stream(1024, w_ref + n_ref + 3, seed=args.seed)
         with tempfile.TemporaryDirectory() as d:
@@ -561,7 +649,7 @@ def main():
         return
 
     import torch
-    from cerebellum_simulation_b200 import replicas
+    from cerebellum_simulation_b200 import networks, replicas
     if world > 1:
         torch.cuda.set_device(local)
     dist, rank, world, local = replicas.init("nccl")
@@ -570,7 +658,7 @@ def main():
 
     import cerebellum_simulation_b200 as cbm
     st = networks.config2_network(seed=replicas.replica_seed(args.seed, rank))
-    mf = networks.eyelid_mf_stream(1024, total_steps, seed=replicas.replica_seed(args.seed, rank))
+    mf = networks.eyelid_mf_stream(1024, plan["rows"], seed=replicas.replica_seed(args.seed, rank))
     sim = cbm.CBMSimCore(st, [replicas.replica_seed(7, rank)], device=device, resident_steps=total_steps)
     bits = cbm.mf_bits(mf, sim.mf_words())
     sim.load_mf_stream(bits)
@@ -604,11 +692,7 @@ def main():
     # roofline: GR-pass durations from events around each pass, the two step
     # kernels on separate streams: after an L2 flush (the timed region's
     # regime), and in back-to-back graph replay (L2-resident)
-    n_roof = min(args.steps, 1000)
-    n_roof -= n_roof % args.chunk
-    n_roof = n_roof or args.chunk
-    n_fl = min(args.steps, 300)
-    n_res = n_fl + n_roof + 2 * args.chunk
+    n_roof, n_fl, n_res = plan["n_roof"], plan["n_fl"], plan["roofline"]
     sim2 = cbm.CBMSimCore(st, [replicas.replica_seed(7, rank)], device=device, resident_steps=n_res)
     sim2.load_mf_stream(cbm.mf_bits(mf[:n_res], sim2.mf_words()))
     sim2.run(2 * args.chunk, args.chunk, time_pass=True)
@@ -624,7 +708,7 @@ def main():
     sim2.close()
 
     # end to end through the per-step C ABI
-    n_e2e = min(args.steps, 2000)
+    n_e2e = plan["n_e2e"]
     sim3 = cbm.CBMSimCore(st, [replicas.replica_seed(7, rank)], device=device)
     zone = sim3.getMZoneList()[0]
     for s in range(20):
@@ -635,7 +719,7 @@ def main():
         dist.barrier()
     sim3.timer_start()
     for s in range(20, 20 + n_e2e):
-        sim3.updateMFInput(mf[s % total_steps])
+        sim3.updateMFInput(mf[s])
         sim3.calcActivity()
         zone.exportAPNC()
     e2e_ms = sim3.timer_stop()
@@ -645,12 +729,15 @@ def main():
     d2h = st.con("numNC")
     sim3.close()
 
-    cpu = None
+    cpu, cpu_error = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as d:
             p = os.path.join(d, "c2.state")
             st.writeState(p)
-            cpu = cpu_reference(p, mf, 200, os.cpu_count() or 1, warmup=20)
+            try:
+                cpu = cpu_reference(p, mf, CPU_STEPS, os.cpu_count() or 1, warmup=CPU_WARMUP)
+            except (RuntimeError, ValueError) as e:
+                cpu_error = str(e)
 
     launches = 2 * args.steps + (args.steps // args.chunk + 8)
     if rank == 0:
@@ -687,6 +774,9 @@ def main():
         }
         if cpu:
             out["cpu_baseline"] = cpu
+        elif cpu_error:
+            out["cpu_baseline"] = None
+            out["cpu_baseline_error"] = cpu_error
         print(json.dumps(out))
     replicas.finish(dist)
 

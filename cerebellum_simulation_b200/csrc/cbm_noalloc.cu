@@ -2,9 +2,9 @@
 //
 // Some host programs cannot let a library allocate device memory when they
 // call it: frameworks that own every device allocation through their own
-// pool, code that calls in while a stream is being captured into a CUDA graph
-// in the global capture mode (where cudaMalloc is not permitted), and
-// real-time control loops that cannot absorb the latency of an allocation.
+// pool (a foreign cudaMalloc escapes their budget and fragments their
+// arena), and real-time control loops that cannot absorb the latency of an
+// allocation.
 // For them this file computes the per-PC parallel-fibre input sums (the
 // reference's updatePFPCOutGPU followed by sumInputsNew, in the same float
 // order) from buffers the caller already holds, with its only scratch in a
@@ -20,7 +20,15 @@
 //     the array; callers on several streams must order them.
 //   - The first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     before any stream capture.  The address is kept for later calls; it
+//     does not survive a reset of the device's context (cudaDeviceReset, or
+//     a framework resetting the primary context), after which the module
+//     may load elsewhere: each call checks that the kept address is still
+//     device memory of the current device and looks it up again if not, but
+//     after a reset the first call must again come before any capture.
+//   - A CUDA error already pending in the calling thread (from the
+//     caller's own earlier launches) is reported as such and left pending;
+//     nothing is launched then.
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -114,9 +122,22 @@ extern "C" int cbm_pfpc_sums_noalloc(const uint32_t *apBuf, const uint32_t *pfDe
 	cudaError_t e = cudaGetDevice(&dev);
 	if (e != cudaSuccess) return fail(CBM_ERR_CUDA, cudaGetErrorString(e));
 	if (dev < 0 || dev >= kMaxDevices) return fail(CBM_ERR_ARG, "device index out of range");
+	e = cudaPeekAtLastError();
+	if (e != cudaSuccess)
+		return fail(CBM_ERR_CUDA, std::string("a CUDA error is already pending in this thread: ") + cudaGetErrorString(e));
 	float *partials;
 	{
 		std::lock_guard<std::mutex> lock(g_setupMutex);
+		if (g_partialsAddr[dev]) {
+			// a kept address from before a context reset no longer resolves
+			// to this device's memory: look it up again
+			cudaPointerAttributes attr{};
+			if (cudaPointerGetAttributes(&attr, g_partialsAddr[dev]) != cudaSuccess ||
+					attr.type != cudaMemoryTypeDevice || attr.device != dev) {
+				cudaGetLastError();  // the failed query's own error, not the caller's
+				g_partialsAddr[dev] = nullptr;
+			}
+		}
 		if (!g_partialsAddr[dev]) {
 			void *p = nullptr;
 			e = cudaGetSymbolAddress(&p, g_pfpcPartials);
@@ -128,8 +149,10 @@ extern "C" int cbm_pfpc_sums_noalloc(const uint32_t *apBuf, const uint32_t *pfDe
 	cudaStream_t s = (cudaStream_t)stream;
 	const uint32_t n = numPC * bs;
 	partialsKernel<<<(n + 255) / 256, 256, 0, s>>>(apBuf, pfDelayMask, weights, P, bs, numPC, partials);
+	e = cudaGetLastError();
+	if (e != cudaSuccess) return fail(CBM_ERR_CUDA, std::string("partial sums launch: ") + cudaGetErrorString(e));
 	treeKernel<<<numPC, bs < 256 ? bs : 256, 0, s>>>(partials, bs, sums);
 	e = cudaGetLastError();
-	if (e != cudaSuccess) return fail(CBM_ERR_CUDA, cudaGetErrorString(e));
+	if (e != cudaSuccess) return fail(CBM_ERR_CUDA, std::string("tree launch: ") + cudaGetErrorString(e));
 	return CBM_OK;
 }

@@ -755,8 +755,10 @@ std::string Network::setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s)
 	// (poissonregencells.cpp:12-19): the first draw of the seed's stream.
 	const float msPerTS = 1.0f;
 	d.sPerTS = msPerTS / 1000;
-	// 1 - exp(...) in double, stored as float (poissonregencells.cpp:20)
-	d.mfThreshDecay = (float)(1.0 - std::exp((double)(-msPerTS / p.mfThreshDecayTau)));
+	// 1 - exp(...) of poissonregencells.cpp:20: the argument is a float, so
+	// C++ picks the float overload (the C library's expf) and the subtraction
+	// is in float too
+	d.mfThreshDecay = 1.0f - expf(-msPerTS / p.mfThreshDecayTau);
 	const double u0 = (double)rng::uniform24((uint32_t)p.mfSeed, rng::kStreamNCIO, 0);
 	const int derived = (int)(u0 * 2147483648.0);
 	d.mfKey = rng::streamKey((uint32_t)derived, rng::kStreamNCIO);

@@ -17,12 +17,12 @@ MF spikes follow the reference's regenerating Poisson rule
 counter-based stream (cbm_rng.hpp), so any MF sequence can be regenerated
 from (seed, step, fibre).
 """
+import ctypes
+import ctypes.util
 import math
 import os
 
 import numpy as np
-
-from . import CBMState
 
 PARAMS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "params")
 
@@ -35,6 +35,20 @@ def act_params(name):
     """Text of a bundled activity-parameter set ("16k" or "dense")."""
     with open(os.path.join(PARAMS_DIR, f"act_{name}.txt")) as f:
         return f.read()
+
+
+def _libm_expf(x):
+    """The C library's expf (numpy's float32 exp rounds differently)."""
+    global _EXPF
+    if _EXPF is None:
+        libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+        libm.expf.restype = ctypes.c_float
+        libm.expf.argtypes = [ctypes.c_float]
+        _EXPF = libm.expf
+    return np.float32(_EXPF(x))
+
+
+_EXPF = None
 
 
 def splitmix64(x):
@@ -56,8 +70,8 @@ def uniform24(seed, stream, counter):
 class RegenPoissonMF:
     """PoissonRegenCells (poissonregencells.cpp:10-66) over numMF fibres.
 
-    threshDecay = 1 - exp(-msPerTS/threshDecayTau) (exp in double, as the
-    reference's call on a float resolves to the C library's double exp) and
+    threshDecay = 1 - exp(-msPerTS/threshDecayTau) (in float: the reference's
+    exp of a float argument is C++'s float overload, the C library's expf) and
     the per-step rule thresh += (1-thresh)*threshDecay; ap = U < (freq*sPerTS)
     *thresh; thresh = (!ap)*thresh, in float32.
     """
@@ -67,8 +81,8 @@ class RegenPoissonMF:
         self.seed = seed
         ms = np.float32(ms_per_step)
         self.s_per_ts = np.float32(ms / np.float32(1000))
-        # threshDecay = 1 - exp(-msPerTS / tau): a float quotient, the C library's double exp, stored as float
-        self.thresh_decay = np.float32(1.0 - math.exp(float(np.float32(-ms / np.float32(thresh_decay_tau)))))
+        # threshDecay = 1 - exp(-msPerTS / tau): a float quotient, the C library's expf, a float subtraction
+        self.thresh_decay = np.float32(np.float32(1) - _libm_expf(float(np.float32(-ms / np.float32(thresh_decay_tau)))))
         self.thresh = np.ones(num_mf, dtype=np.float32)
         self.t = 0
 
@@ -153,11 +167,16 @@ def build_random_network(gr_xp2, gr_yp2, go_xp2, go_yp2, mf_p2, act_text, *, see
                          mf_per_gr=4, go_per_gr=3, gr_per_go=None, go_out_per_gr=None,
                          mf_per_go=16, vel=147, af_delay=1, pc_p2=5, sc_p2=9, nc_p2=3, io_p2=2,
                          pcnc=3, gogo=((0, -1, 1.0), (-1, -1, 1.0), (-1, 0, 1.0), (-1, 1, 1.0)),
-                         n_zones=1):
+                         n_zones=1, new_state=None):
     """A CBMState with random input-net wiring.
 
     GR->GO synapses are drawn either from the GO side (gr_per_go random GR per
-    GO) or from the GR side (go_out_per_gr random GO per GR)."""
+    GO) or from the GR side (go_out_per_gr random GO per GR).  new_state
+    (default CBMState.new) makes the empty state from the parameter texts;
+    any object with the same con() / array() interface works."""
+    if new_state is None:
+        from . import CBMState
+        new_state = CBMState.new
     rng = np.random.Generator(np.random.PCG64(seed))
     n_gr = 1 << (gr_xp2 + gr_yp2)
     gr_x = 1 << gr_xp2
@@ -180,7 +199,7 @@ def build_random_network(gr_xp2, gr_yp2, go_xp2, go_yp2, mf_p2, act_text, *, see
     con = con_params_text(gr_xp2, gr_yp2, go_xp2, go_yp2, mf_p2, max_gr_out=max_out,
                           max_mf_go_per_mf=max_mf_go, vel=vel, af_delay=af_delay, sc_p2=sc_p2,
                           pc_p2=pc_p2, nc_p2=nc_p2, io_p2=io_p2, pcnc=pcnc, gogo=gogo)
-    st = CBMState.new(con, act_text, n_zones, wiring_seeds=[seed * 7 + z + 1 for z in range(n_zones)])
+    st = new_state(con, act_text, n_zones, wiring_seeds=[seed * 7 + z + 1 for z in range(n_zones)])
     max_go_stride = st.con("maxnumpGRfromGOtoGR")
     max_out_stride = st.con("maxnumpGRfromGRtoGO")
     mf_go_stride = st.con("maxnumpMFfromMFtoGO")
@@ -238,24 +257,24 @@ def build_random_network(gr_xp2, gr_yp2, go_xp2, go_yp2, mf_p2, act_text, *, see
 
 
 # ------------------------------------------------------------ configurations
-def config1_network(seed=0):
+def config1_network(seed=0, new_state=None):
     """16,384 GR (4 MF + 3 GO dendrites), 256 GO x 128 random GR, 1024 MF,
     32 PC x 512 PF, 128 BC, 512 SC, 8 NC, 4 IO."""
     return build_random_network(8, 6, 4, 4, 10, act_params("16k"), seed=seed, gr_per_go=128,
-                                mf_per_go=3, vel=40, gogo=((1, 1, 0.0),))
+                                mf_per_go=3, vel=40, gogo=((1, 1, 0.0),), new_state=new_state)
 
 
-def config2_network(seed=0):
+def config2_network(seed=0, new_state=None):
     """1,048,576 GR (4 MF + 3 GO dendrites, 4 GO targets each), 1024 GO,
     1024 MF, 32 PC x 32,768 PF, 128 BC, 512 SC, 8 NC, 4 IO."""
     return build_random_network(11, 9, 6, 4, 10, act_params("dense"), seed=seed, go_out_per_gr=4,
-                                mf_per_go=16, vel=147)
+                                mf_per_go=16, vel=147, new_state=new_state)
 
 
-def config3_network(seed=0):
+def config3_network(seed=0, new_state=None):
     """4,194,304 GR, 4096 GO x 1024 random GR, 1024 MF, 128 PC x 32,768 PF."""
     return build_random_network(12, 10, 6, 6, 10, act_params("dense"), seed=seed, gr_per_go=1024,
-                                mf_per_go=16, vel=294, pc_p2=7)
+                                mf_per_go=16, vel=294, pc_p2=7, new_state=new_state)
 
 
 class StateVariableMF:

@@ -106,12 +106,13 @@ def read_ec_trials_data(buf, pos=0):
     (ECTrialsData(fstream &), ectrialsdata.cpp): {"header": {...},
     "eyelid": f32 [trials, steps], "psh": {name: f32 [bins, cells]},
     "psh_trials": {name: trials recorded}, "psh_bin_steps": {name: steps a
-    bin}, "raster": {name: u32 [trials, rows, cells]}}."""
+    bin}, "raster": {name: u32 [trials, rows, cells]}, "raster_trials":
+    {name: the raster's completed trials, its curTrialN}}."""
     r = _Reader(buf, pos)
     pre, cs, post, ms_total, ms_per_ts, ts_total, n_trials = r.ints(7)
     out = {"header": dict(msPreCS=pre, msCS=cs, msPostCS=post, msTotal=ms_total, msPerTimeStep=ms_per_ts,
                           tsTotal=ts_total, numTrials=n_trials), "psh": {}, "psh_trials": {},
-           "psh_bin_steps": {}, "raster": {}}
+           "psh_bin_steps": {}, "raster": {}, "raster_trials": {}}
     e_trials, _, _, _, e_ts, _, _ = r.ints(7)
     out["eyelid"] = r.raw(np.float32, e_trials * e_ts).reshape(e_trials, e_ts)
     for _ in range(r.ints(1)[0]):
@@ -124,8 +125,9 @@ def read_ec_trials_data(buf, pos=0):
         name = r.word()
         r.word()  # the raster's own copy of its name
         cells, trials, _ = r.ints(3)
-        _, _, _, _, _, rows = r.ints(6)
+        _, cur_trial, _, _, _, rows = r.ints(6)
         out["raster"][name] = r.raw(np.uint32, trials * rows * cells).reshape(trials, rows, cells)
+        out["raster_trials"][name] = cur_trial
     if r.ints(1)[0] != 0:
         raise ValueError("raw-uint records are not read")
     out["end"] = r.pos + (buf[r.pos: r.pos + 1] == b"\n")  # past the count's line end
@@ -243,7 +245,11 @@ class TrialsData:
         return PeriStimHist(self._d["psh"][cellT], self._d["psh_bin_steps"][cellT], self._d["psh_trials"][cellT])
 
     def getRaster(self, cellT):
-        return SpikeRaster(self._d["raster"][cellT], self._ms_per_step)
+        # getNumTrials and the all-trials spike times count the raster's
+        # completed trials (SpikeRasterBitArray's curTrialN), which fall
+        # behind the allocated trials when the window is a multiple of 32 steps
+        return SpikeRaster(self._d["raster"][cellT], self._ms_per_step,
+                           trials_done=self._d.get("raster_trials", {}).get(cellT))
 
     def getEyelidData(self, trialN):
         return [float(v) for v in self._d["eyelid"][trialN]]

@@ -357,9 +357,8 @@ void cbm_sim_destroy(cbm_sim *sim);
 /* PF->PC input sums without device allocation.  No counterpart in the
  * reference; it is for callers that cannot let a library allocate device
  * memory while they call it (a framework that owns every allocation through
- * its own pool, code running while a stream is captured into a CUDA graph in
- * the global capture mode, a real-time loop that cannot absorb allocation
- * latency).  From buffers on the current device it computes, for each of
+ * its own pool, a real-time loop that cannot absorb allocation latency).
+ * From buffers on the current device it computes, for each of
  * numPC rows of numGR/numPC parallel fibres, the sum of
  * weights[i] * ((apBuf[i] & pfDelayMask[i]) != 0) in the reference's
  * order (updatePFPCOutGPU then sumInputsNew) into sums[numPC], on `stream`
@@ -370,7 +369,11 @@ void cbm_sim_destroy(cbm_sim *sim);
  * the call fails with CBM_ERR_ARG.  All calls on a device share the array;
  * each call rewrites the part it reads, so no clearing is needed, but calls
  * that overlap on the GPU race.  The first call on a device looks up the
- * array's address; make it before any stream capture. */
+ * array's address; make it before any stream capture.  The address is kept;
+ * after a reset of the device's context it is looked up again, and the
+ * first call after the reset must again precede any capture.  A CUDA error
+ * already pending in the calling thread fails the call (CBM_ERR_CUDA) and is
+ * left pending. */
 #define CBM_NOALLOC_MAX_PARTIALS 65536
 int cbm_pfpc_sums_noalloc(const uint32_t *apBuf, const uint32_t *pfDelayMask, const float *weights,
 		uint32_t numGR, uint32_t numPC, float *sums, void *stream);

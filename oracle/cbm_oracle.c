@@ -339,11 +339,13 @@ static int next_tok(rd_t *r, char *out, size_t outlen)
 	return 0;
 }
 
-typedef struct { int reading; rd_t *r; FILE *w; int err; } io_t;
+/* reading: 1 = from r, 0 = to w, 2 = allocate only (a new state),
+ * 3 = find the array named want (found, foundBytes) */
+typedef struct { int reading; rd_t *r; FILE *w; int err; const char *want; void *found; size_t foundBytes; } io_t;
 
 static void *blk(io_t *io, void *p, size_t bytes)
 {
-	if (io->err) return p;
+	if (io->err || io->reading == 2) return p;
 	if (io->reading)
 	{
 		if (io->r->pos + bytes > io->r->len) { io->err = 1; return p; }
@@ -354,8 +356,17 @@ static void *blk(io_t *io, void *p, size_t bytes)
 	return p;
 }
 
+/* an array's block, or in find mode its address when its field name
+ * (the text after "->") is the one wanted */
+static void blk_named(io_t *io, const char *field, void *p, size_t bytes)
+{
+	if (io->reading != 3) { blk(io, p, bytes); return; }
+	const char *arrow = strstr(field, "->");
+	if (arrow && !io->found && !strcmp(arrow + 2, io->want)) { io->found = p; io->foundBytes = bytes; }
+}
+
 #define ALLOC(ptr, n) do { size_t cnt_ = (size_t)(n); if (!(ptr)) (ptr) = calloc(cnt_ ? cnt_ : 1, sizeof(*(ptr))); } while (0)
-#define RW(ptr, n) do { ALLOC(ptr, n); blk(io, (ptr), (size_t)(n) * sizeof(*(ptr))); } while (0)
+#define RW(ptr, n) do { ALLOC(ptr, n); blk_named(io, #ptr, (ptr), (size_t)(n) * sizeof(*(ptr))); } while (0)
 
 /* innetconnectivitystate.cpp:530-606 */
 static void rw_innet_con(cbm_oracle *o, io_t *io)
@@ -491,6 +502,8 @@ static void setup_runtime(cbm_oracle *o)
 	o->curTime = 0;
 }
 
+static int parse_header(cbm_oracle *o, rd_t *rp);
+
 cbm_oracle *cbm_oracle_load(const char *path, char *err, size_t errlen)
 {
 	FILE *f = fopen(path, "rb");
@@ -503,6 +516,32 @@ cbm_oracle *cbm_oracle_load(const char *path, char *err, size_t errlen)
 	fclose(f);
 	rd_t r = { buf, (size_t)len, 0 };
 	cbm_oracle *o = calloc(1, sizeof(cbm_oracle));
+	if (parse_header(o, &r)) goto bad;
+	o->zones = calloc(o->numZones ? o->numZones : 1, sizeof(zone_t));
+	io_t io = { 1, &r, NULL, 0 };
+	rw_innet_con(o, &io);
+	for (uint32_t z = 0; z < o->numZones; z++) rw_mzone_con(o, &o->zones[z], &io);
+	rw_innet_act(o, &io);
+	for (uint32_t z = 0; z < o->numZones; z++) rw_mzone_act(o, &o->zones[z], &io);
+	if (io.err) { snprintf(err, errlen, "state file truncated"); free(buf); cbm_oracle_free(o); return NULL; }
+	free(buf);
+	setup_runtime(o);
+	return o;
+bad:
+	snprintf(err, errlen, "malformed parameter header");
+	free(buf);
+	cbm_oracle_free(o);
+	return NULL;
+}
+
+/* The state file's text header (cbmstate.cpp:12-19): numZones, the
+ * connectivity parameters (ConnectivityParams(fstream&),
+ * connectivityparams.cpp:12-88), the activity parameters
+ * (ActivityParams(fstream&), activityparams.cpp:12-30), then one separator
+ * byte.  Derives both parameter sets.  Returns 0, or -1 when malformed. */
+static int parse_header(cbm_oracle *o, rd_t *rp)
+{
+	rd_t r = *rp;
 	char tok[128];
 	/* cbmstate.cpp:14: numZones, then ConnectivityParams(fstream&) */
 	if (next_tok(&r, tok, sizeof tok)) goto bad;
@@ -545,21 +584,10 @@ cbm_oracle *cbm_oracle_load(const char *path, char *err, size_t errlen)
 	r.pos += 1; /* cbmstate.cpp:19 */
 	derive_con(o);
 	derive_act(o);
-	o->zones = calloc(o->numZones ? o->numZones : 1, sizeof(zone_t));
-	io_t io = { 1, &r, NULL, 0 };
-	rw_innet_con(o, &io);
-	for (uint32_t z = 0; z < o->numZones; z++) rw_mzone_con(o, &o->zones[z], &io);
-	rw_innet_act(o, &io);
-	for (uint32_t z = 0; z < o->numZones; z++) rw_mzone_act(o, &o->zones[z], &io);
-	if (io.err) { snprintf(err, errlen, "state file truncated"); free(buf); cbm_oracle_free(o); return NULL; }
-	free(buf);
-	setup_runtime(o);
-	return o;
+	*rp = r;
+	return 0;
 bad:
-	snprintf(err, errlen, "malformed parameter header");
-	free(buf);
-	cbm_oracle_free(o);
-	return NULL;
+	return -1;
 }
 
 static void write_params(cbm_oracle *o, FILE *f)
@@ -601,6 +629,249 @@ int cbm_oracle_save(cbm_oracle *o, const char *path)
 	for (uint32_t z = 0; z < o->numZones; z++) rw_mzone_act(o, &o->zones[z], &io);
 	fclose(f);
 	return io.err ? -1 : 0;
+}
+
+/* ------------------------------------------------------------ new state */
+#define FILL(ptr, n, v) do { for (size_t i_ = 0; i_ < (size_t)(n); i_++) (ptr)[i_] = (v); } while (0)
+
+cbm_oracle *cbm_oracle_new(const char *conText, const char *actText, uint32_t nZones, const int *pcncSeeds,
+		char *err, size_t errlen)
+{
+	/* CBMState(actPF, conPF, nZones, ...) (CBM_STATE_LIB_DEV/src/interfaces/
+	 * cbmstate.cpp:60-64, 176-204) without the spatial input-net generator:
+	 * the parameters, every array allocated, the initial values of
+	 * InNetConnectivityState::initializeVals (innetconnectivitystate.cpp:
+	 * 650-713), InNetActivityState::initializeVals (innetactivitystate.cpp:
+	 * 277-337), MZoneActivityState::initializeVals (mzoneactivitystate.cpp:
+	 * 357-445) and the microzone wiring of MZoneConnectivityState
+	 * (mzoneconnectivitystate.cpp:12-40, 187-417).  The input-net tables are
+	 * left at their initial values for the caller to fill.  The random
+	 * PC->NC synapses (connectPCtoNC's IRandomX draws from SFMT seeded with
+	 * the zone's seed) are drawn from the counter-based stream keyed by
+	 * pcncSeeds[z], index = (int)(draw * numPC), retried while the PC is full
+	 * or already connected to that NC. */
+	size_t lc = strlen(conText), la = strlen(actText);
+	char *buf = malloc(lc + la + 32);
+	int n0 = snprintf(buf, 32, "%u\n", nZones);
+	memcpy(buf + n0, conText, lc);
+	buf[n0 + lc] = '\n';
+	memcpy(buf + n0 + lc + 1, actText, la);
+	size_t len = (size_t)n0 + lc + 1 + la;
+	buf[len] = '\n';
+	rd_t r = { buf, len + 1, 0 };
+	cbm_oracle *o = calloc(1, sizeof(cbm_oracle));
+	if (parse_header(o, &r))
+	{
+		snprintf(err, errlen, "malformed parameter text");
+		free(buf);
+		cbm_oracle_free(o);
+		return NULL;
+	}
+	free(buf);
+	o->zones = calloc(o->numZones ? o->numZones : 1, sizeof(zone_t));
+	io_t io = { 2, NULL, NULL, 0, NULL, NULL, 0 };
+	rw_innet_con(o, &io);
+	for (uint32_t z = 0; z < o->numZones; z++) rw_mzone_con(o, &o->zones[z], &io);
+	rw_innet_act(o, &io);
+	for (uint32_t z = 0; z < o->numZones; z++) rw_mzone_act(o, &o->zones[z], &io);
+
+	/* input-net connectivity: counts and has-flags 0, indices UINT_MAX,
+	 * the BSP delay masks 0 */
+	FILL(o->pGLfromMFtoGL, o->numGL, UINT32_MAX);
+	FILL(o->pGLfromGLtoGO, (size_t)o->numGL * o->maxnumpGLfromGLtoGO, UINT32_MAX);
+	FILL(o->pGLfromGOtoGL, (size_t)o->numGL * o->maxnumpGLfromGOtoGL, UINT32_MAX);
+	FILL(o->pGLfromGLtoGR, (size_t)o->numGL * o->maxnumpGLfromGLtoGR, UINT32_MAX);
+	FILL(o->pMFfromMFtoGL, (size_t)o->numMF * o->cp_numpMFfromMFtoGL, UINT32_MAX);
+	FILL(o->pMFfromMFtoGR, (size_t)o->numMF * o->maxnumpMFfromMFtoGR, UINT32_MAX);
+	FILL(o->pMFfromMFtoGO, (size_t)o->numMF * o->maxnumpMFfromMFtoGO, UINT32_MAX);
+	FILL(o->pGOfromGLtoGO, (size_t)o->numGO * o->maxnumpGOfromGLtoGO, UINT32_MAX);
+	FILL(o->pGOfromGOtoGL, (size_t)o->numGO * o->maxnumpGOfromGOtoGL, UINT32_MAX);
+	FILL(o->pGOfromMFtoGO, (size_t)o->numGO * o->maxnumpGOfromMFtoGO, UINT32_MAX);
+	FILL(o->pGOfromGOtoGR, (size_t)o->numGO * o->maxnumpGOfromGOtoGR, UINT32_MAX);
+	FILL(o->pGOfromGRtoGO, (size_t)o->numGO * o->maxnumpGOfromGRtoGO, UINT32_MAX);
+	FILL(o->pGOGABAInGOGO, (size_t)o->numGO * o->maxnumpGOGABAInGOGO, UINT32_MAX);
+	FILL(o->pGOGABAOutGOGO, (size_t)o->numGO * o->maxnumpGOGABAOutGOGO, UINT32_MAX);
+	FILL(o->pGOCoupInGOGO, (size_t)o->numGO * o->maxnumpGOCoupInGOGO, UINT32_MAX);
+	FILL(o->pGOCoupOutGOGO, (size_t)o->numGO * o->maxnumpGOCoupOutGOGO, UINT32_MAX);
+	/* the GR tables, over the whole allocation (pGRfromGLtoGR and
+	 * pGRfromMFtoGR are stored with maxnumpGRfromGOtoGR columns) */
+	FILL(o->pGRfromGLtoGR, (size_t)o->numGR * o->maxnumpGRfromGOtoGR, UINT32_MAX);
+	FILL(o->pGRfromGRtoGO, (size_t)o->numGR * o->maxnumpGRfromGRtoGO, UINT32_MAX);
+	FILL(o->pGRDelayMaskfromGRtoGO, (size_t)o->numGR * o->maxnumpGRfromGRtoGO, UINT32_MAX);
+	FILL(o->pGRfromGOtoGR, (size_t)o->numGR * o->maxnumpGRfromGOtoGR, UINT32_MAX);
+	FILL(o->pGRfromMFtoGR, (size_t)o->numGR * o->maxnumpGRfromGOtoGR, UINT32_MAX);
+
+	/* input-net activity (everything else starts at 0) */
+	FILL(o->vGO, o->numGO, o->eLeakGO);
+	FILL(o->threshCurGO, o->numGO, o->threshRestGO);
+	FILL(o->threshGR, o->numGR, o->threshRestGR);
+	FILL(o->vGR, o->numGR, o->eLeakGR);
+	FILL(o->threshSC, o->numSC, o->threshRestSC);
+	FILL(o->vSC, o->numSC, o->eLeakSC);
+
+	for (uint32_t zi = 0; zi < o->numZones; zi++)
+	{
+		zone_t *z = &o->zones[zi];
+		/* MZoneActivityState::initializeVals */
+		FILL(z->threshBC, o->numBC, o->threshRestBC);
+		FILL(z->vBC, o->numBC, o->eLeakBC);
+		FILL(z->vPC, o->numPC, o->eLeakPC);
+		FILL(z->threshPC, o->numPC, o->threshRestPC);
+		FILL(z->pfSynWeightPC, (size_t)o->numPC * o->numpPCfromGRtoPC, o->initSynWofGRtoPC);
+		FILL(z->threshIO, o->numIO, o->threshRestIO);
+		FILL(z->vIO, o->numIO, o->eLeakIO);
+		FILL(z->threshNC, o->numNC, o->threshRestNC);
+		FILL(z->vNC, o->numNC, o->eLeakNC);
+		FILL(z->gPCScaleNC, (size_t)o->numNC * o->numpNCfromPCtoNC, o->gIncAvgPCtoNC);
+		FILL(z->mfSynWeightNC, (size_t)o->numNC * o->numpNCfromMFtoNC, o->initSynWofMFtoNC);
+		/* MZoneConnectivityState::initalizeVars */
+		FILL(z->pBCfromBCtoPC, (size_t)o->numBC * o->numpBCfromBCtoPC, UINT32_MAX);
+		FILL(z->pBCfromPCtoBC, (size_t)o->numBC * o->numpBCfromPCtoBC, UINT32_MAX);
+		FILL(z->pSCfromSCtoPC, (size_t)o->numSC * o->numpSCfromSCtoPC, UINT32_MAX);
+		FILL(z->pPCfromBCtoPC, (size_t)o->numPC * o->numpPCfromBCtoPC, UINT32_MAX);
+		FILL(z->pPCfromPCtoBC, (size_t)o->numPC * o->numpPCfromPCtoBC, UINT32_MAX);
+		FILL(z->pPCfromSCtoPC, (size_t)o->numPC * o->numpPCfromSCtoPC, UINT32_MAX);
+		FILL(z->pPCfromPCtoNC, (size_t)o->numPC * o->numpPCfromPCtoNC, UINT32_MAX);
+		FILL(z->pPCfromIOtoPC, o->numPC, UINT32_MAX);
+		FILL(z->pNCfromPCtoNC, (size_t)o->numNC * o->numpNCfromPCtoNC, UINT32_MAX);
+		FILL(z->pNCfromNCtoIO, (size_t)o->numNC * o->numpNCfromNCtoIO, UINT32_MAX);
+		FILL(z->pNCfromMFtoNC, (size_t)o->numNC * o->numpNCfromMFtoNC, UINT32_MAX);
+		FILL(z->pIOfromIOtoPC, (size_t)o->numIO * o->numpIOfromIOtoPC, UINT32_MAX);
+		FILL(z->pIOfromNCtoIO, (size_t)o->numIO * o->numpIOfromNCtoIO, UINT32_MAX);
+		FILL(z->pIOInIOIO, (size_t)o->numIO * o->numpIOInIOIO, UINT32_MAX);
+		FILL(z->pIOOutIOIO, (size_t)o->numIO * o->numpIOOutIOIO, UINT32_MAX);
+		const int nPC = (int)o->numPC, nBC = (int)o->numBC, ratio = nBC / nPC;
+		/* connectBCtoPC: BC r of each PC's block projects to PCs at the
+		 * offsets of its row */
+		static const int offs[4][4] = { {1, -1, 2, -2}, {1, -1, 3, -3}, {3, -3, 6, -6}, {4, -4, 9, -9} };
+		for (int i = 0; i < nPC; i++)
+			for (int rr = 0; rr < 4; rr++)
+				for (int j = 0; j < 4; j++)
+					z->pBCfromBCtoPC[(size_t)(i * ratio + rr) * o->numpBCfromBCtoPC + j] =
+						(uint32_t)(((i + offs[rr][j]) % nPC + nPC) % nPC);
+		/* connectPCtoBC */
+		for (int i = 0; i < nPC; i++)
+			for (int j = 0; j < (int)o->numpPCfromPCtoBC; j++)
+			{
+				int bcInd = i * ratio - 6 + j;
+				z->pPCfromPCtoBC[(size_t)i * o->numpPCfromPCtoBC + j] = (uint32_t)((bcInd % nBC + nBC) % nBC);
+			}
+		/* connectSCtoPC */
+		for (uint32_t i = 0; i < o->numSC; i++)
+			for (uint32_t j = 0; j < o->numpSCfromSCtoPC; j++)
+			{
+				uint32_t pcInd = i / o->numpPCfromSCtoPC;
+				z->pSCfromSCtoPC[(size_t)i * o->numpSCfromSCtoPC + j] = pcInd;
+				z->pPCfromSCtoPC[(size_t)pcInd * o->numpPCfromSCtoPC + i % o->numpPCfromSCtoPC] = i;
+			}
+		/* connectPCtoNC */
+		int *pcNum = malloc(sizeof(int) * o->numPC);
+		for (uint32_t i = 0; i < o->numPC; i++) pcNum[i] = 1;
+		const uint32_t perNC = o->numPC / o->numNC;
+		for (uint32_t i = 0; i < o->numNC; i++)
+			for (uint32_t j = 0; j < perNC; j++)
+			{
+				uint32_t pcInd = i * perNC + j;
+				z->pNCfromPCtoNC[(size_t)i * o->numpNCfromPCtoNC + j] = pcInd;
+				z->pPCfromPCtoNC[(size_t)pcInd * o->numpPCfromPCtoNC + 0] = i;
+			}
+		const uint32_t seed = (uint32_t)(pcncSeeds ? pcncSeeds[zi] : (int)(7919 + zi));
+		uint64_t ctr = 0;
+		for (uint32_t i = 0; i + 1 < o->numNC; i++)
+			for (uint32_t j = o->numpNCfromPCtoNC / 3; j < o->numpNCfromPCtoNC; j++)
+			{
+				uint32_t pcInd = 0;
+				for (long tries = 0; tries < 1000000; tries++)
+				{
+					pcInd = (uint32_t)(cbm_oracle_uniform24(seed, CBM_STREAM_WIRING, ctr++) * o->numPC);
+					if ((uint32_t)pcNum[pcInd] >= o->numpPCfromPCtoNC) continue;
+					int connect = 1;
+					for (int k = 0; k < pcNum[pcInd]; k++)
+						if (z->pPCfromPCtoNC[(size_t)pcInd * o->numpPCfromPCtoNC + k] == i) { connect = 0; break; }
+					if (connect) break;
+				}
+				z->pNCfromPCtoNC[(size_t)i * o->numpNCfromPCtoNC + j] = pcInd;
+				z->pPCfromPCtoNC[(size_t)pcInd * o->numpPCfromPCtoNC + pcNum[pcInd]] = i;
+				pcNum[pcInd]++;
+			}
+		{
+			uint32_t numSyn = perNC;
+			for (uint32_t h = 1; h < o->numpPCfromPCtoNC; h++)
+				for (uint32_t i = 0; i < o->numPC; i++)
+					if ((uint32_t)pcNum[i] < o->numpPCfromPCtoNC)
+					{
+						z->pNCfromPCtoNC[(size_t)(o->numNC - 1) * o->numpNCfromPCtoNC + numSyn] = i;
+						z->pPCfromPCtoNC[(size_t)i * o->numpPCfromPCtoNC + pcNum[i]] = o->numNC - 1;
+						pcNum[i]++;
+						numSyn++;
+					}
+		}
+		free(pcNum);
+		/* connectNCtoIO */
+		for (uint32_t i = 0; i < o->numIO; i++)
+			for (uint32_t j = 0; j < o->numpIOfromNCtoIO; j++)
+			{
+				z->pIOfromNCtoIO[(size_t)i * o->numpIOfromNCtoIO + j] = j;
+				z->pNCfromNCtoIO[(size_t)j * o->numpNCfromNCtoIO + i] = i;
+			}
+		/* connectMFtoNC */
+		for (uint32_t i = 0; i < o->numMF; i++)
+			z->pNCfromMFtoNC[(size_t)(i / o->numpNCfromMFtoNC) * o->numpNCfromMFtoNC + i % o->numpNCfromMFtoNC] = i;
+		/* connectIOtoPC */
+		for (uint32_t i = 0; i < o->numIO; i++)
+			for (uint32_t j = 0; j < o->numpIOfromIOtoPC; j++)
+			{
+				uint32_t pcInd = i * o->numpIOfromIOtoPC + j;
+				z->pIOfromIOtoPC[(size_t)i * o->numpIOfromIOtoPC + j] = pcInd;
+				z->pPCfromIOtoPC[pcInd] = i;
+			}
+		/* connectIOtoIO */
+		for (uint32_t i = 0; i < o->numIO; i++)
+		{
+			uint32_t inInd = 0;
+			for (uint32_t j = 0; j < o->numpIOInIOIO; j++)
+			{
+				if (inInd == i) inInd++;
+				z->pIOInIOIO[(size_t)i * o->numpIOInIOIO + j] = inInd;
+				inInd++;
+			}
+		}
+	}
+	setup_runtime(o);
+	return o;
+}
+
+void *cbm_oracle_array(cbm_oracle *o, const char *name, int zone, uint64_t *bytes)
+{
+	io_t io = { 3, NULL, NULL, 0, name, NULL, 0 };
+	if (zone < 0)
+	{
+		rw_innet_con(o, &io);
+		if (!io.found) rw_innet_act(o, &io);
+	}
+	else if ((uint32_t)zone < o->numZones)
+	{
+		rw_mzone_con(o, &o->zones[zone], &io);
+		if (!io.found) rw_mzone_act(o, &o->zones[zone], &io);
+	}
+	if (bytes) *bytes = io.foundBytes;
+	return io.found;
+}
+
+int cbm_oracle_con(const cbm_oracle *o, const char *key, uint32_t *value)
+{
+	/* derived connectivity parameters (connectivityparams.cpp:90-183) by name */
+#define CON_KEY(f) if (!strcmp(key, #f)) { *value = o->f; return 0; }
+	CON_KEY(numGL) CON_KEY(numMF) CON_KEY(numGO) CON_KEY(numGR) CON_KEY(numSC) CON_KEY(numPC) CON_KEY(numBC)
+	CON_KEY(numNC) CON_KEY(numIO) CON_KEY(maxnumpGLfromGLtoGR) CON_KEY(maxnumpGLfromGLtoGO)
+	CON_KEY(maxnumpGLfromGOtoGL) CON_KEY(maxnumpMFfromMFtoGO) CON_KEY(maxnumpMFfromMFtoGR)
+	CON_KEY(maxnumpGOfromGRtoGO) CON_KEY(maxnumpGOfromGLtoGO) CON_KEY(maxnumpGOfromMFtoGO)
+	CON_KEY(maxnumpGOfromGOtoGL) CON_KEY(maxnumpGOfromGOtoGR) CON_KEY(maxnumpGRfromGRtoGO)
+	CON_KEY(maxnumpGRfromGLtoGR) CON_KEY(maxnumpGRfromGOtoGR) CON_KEY(maxnumpGRfromMFtoGR)
+	CON_KEY(maxnumpGOGABAInGOGO) CON_KEY(maxnumpGOGABAOutGOGO) CON_KEY(maxnumpGOCoupInGOGO)
+	CON_KEY(maxnumpGOCoupOutGOGO) CON_KEY(numpPCfromGRtoPC) CON_KEY(numpBCfromGRtoBC) CON_KEY(numpSCfromGRtoSC)
+#undef CON_KEY
+	return -1;
 }
 
 void cbm_oracle_free(cbm_oracle *o)
@@ -663,6 +934,7 @@ static void gr_activity(cbm_oracle *o)
 	/* kernels.cu:79-110 */
 	const float gLeak = o->gLeakGR, eLeak = o->eLeakGR, eGOIn = o->eGOGR;
 	const float threshBase = o->threshRestGR, threshMax = o->threshMaxGR, threshDecay = o->threshDecGR;
+	#pragma omp parallel for schedule(static)
 	for (uint32_t i = 0; i < o->numGR; i++)
 	{
 		float tempV = o->vGR[i];
@@ -685,6 +957,7 @@ static void gr_inputs(cbm_oracle *o, float *gSum, const uint32_t *ap, const int3
 		const uint32_t *con, uint32_t stride, float gDecay, float gInc)
 {
 	/* kernels.cu:169-199 (con is [gr][stride], as in the state) */
+	#pragma omp parallel for schedule(static)
 	for (uint32_t i = 0; i < o->numGR; i++)
 	{
 		int n = num[i];
@@ -991,6 +1264,7 @@ static void pfpc_plasticity(cbm_oracle *o, zone_t *z, uint64_t t)
 	{
 		if (i >= (curIOInd + 1) * numGRPerIO) curIOInd++;
 		float step = z->pfPCPlastStepIO[curIOInd];
+		#pragma omp parallel for schedule(static)
 		for (uint32_t k = i; k < i + o->numpPCfromGRtoPC; k++)
 		{
 			float *w = &z->pfSynWeightPC[k];
@@ -1019,6 +1293,7 @@ void cbm_oracle_step(cbm_oracle *o, const uint8_t *mf)
 	for (uint32_t zi = 0; zi < o->numZones; zi++)
 	{
 		zone_t *z = &o->zones[zi];
+		#pragma omp parallel for schedule(static)
 		for (uint32_t pc = 0; pc < o->numPC; pc++)
 			z->sumPFPCdev[pc] = sum_row_ordered(&z->rowsPFPC[(size_t)pc * o->numpPCfromGRtoPC], o->numpPCfromGRtoPC);
 	}
@@ -1043,6 +1318,7 @@ void cbm_oracle_step(cbm_oracle *o, const uint8_t *mf)
 	for (uint32_t zi = 0; zi < o->numZones; zi++)
 	{
 		zone_t *z = &o->zones[zi];
+		#pragma omp parallel for schedule(static)
 		for (uint32_t i = 0; i < o->numGR; i++)
 		{
 			unsigned int pf = (o->apBufGR[i] & o->pGRDelayMaskfromGRtoBSP[i]) > 0;
@@ -1053,21 +1329,28 @@ void cbm_oracle_step(cbm_oracle *o, const uint8_t *mf)
 	memset(o->pendBC, 0, o->numBC * 4);
 	memset(o->pendSC, 0, o->numSC * 4);
 	memset(o->pendGO, 0, o->numGO * 4);
-	for (uint32_t i = 0; i < o->numGR; i++)
 	{
-		unsigned int pf = (o->apBufGR[i] & o->pGRDelayMaskfromGRtoBSP[i]) > 0;
-		o->pendBC[i >> o->numpBCfromGRtoBCP2] += pf;
-		o->pendSC[i >> o->numpSCfromGRtoSCP2] += pf;
-		for (int k = 0; k < o->numpGRfromGRtoGO[i]; k++)
+		/* integer counts: any summation order gives the same values */
+		uint32_t *pendBC = o->pendBC, *pendSC = o->pendSC, *pendGO = o->pendGO;
+		const uint32_t nBC = o->numBC, nSC = o->numSC, nGO = o->numGO;
+		#pragma omp parallel for schedule(static) reduction(+: pendBC[:nBC], pendSC[:nSC], pendGO[:nGO])
+		for (uint32_t i = 0; i < o->numGR; i++)
 		{
-			size_t s = (size_t)i * o->maxnumpGRfromGRtoGO + k;
-			if ((o->apBufGR[i] & o->pGRDelayMaskfromGRtoGO[s]) > 0) o->pendGO[o->pGRfromGRtoGO[s]] += 1;
+			unsigned int pf = (o->apBufGR[i] & o->pGRDelayMaskfromGRtoBSP[i]) > 0;
+			pendBC[i >> o->numpBCfromGRtoBCP2] += pf;
+			pendSC[i >> o->numpSCfromGRtoSCP2] += pf;
+			for (int k = 0; k < o->numpGRfromGRtoGO[i]; k++)
+			{
+				size_t s = (size_t)i * o->maxnumpGRfromGRtoGO + k;
+				if ((o->apBufGR[i] & o->pGRDelayMaskfromGRtoGO[s]) > 0) pendGO[o->pGRfromGRtoGO[s]] += 1;
+			}
 		}
 	}
 	memcpy(o->inputSumPFBCH, o->sumBCdev, o->numBC * 4);
 	memcpy(o->inputSumPFSCH, o->sumSCdev, o->numSC * 4);
 	memcpy(o->grInputGOSumH, o->sumGOdev, o->numGO * 4);
 	if (t % o->tsPerHistBinGR == 0)
+		#pragma omp parallel for schedule(static)
 		for (uint32_t i = 0; i < o->numGR; i++)
 			o->historyGR[i] = (o->historyGR[i] << 1) | ((o->apBufGR[i] & 0x0000001F) > 0);
 
@@ -1230,9 +1513,9 @@ void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const 
 	 * poissonregencells.cpp:10-35): its generator's seed is the first draw of
 	 * a generator seeded with mfSeed, scaled to [0, 2^31) */
 	const float msPerTS = 1.0f, sPerTS = msPerTS / 1000;
-	/* 1 - exp(...) with the C library's double exp, stored as float, as
-	 * poissonregencells.cpp:20 computes it */
-	const float threshDecay = (float)(1 - exp((double)(-msPerTS / p->mfThreshDecayTau)));
+	/* 1 - exp(...) as poissonregencells.cpp:20 computes it: exp of a float
+	 * argument is the float overload in C++ (expf), the subtraction float */
+	const float threshDecay = 1.0f - expf(-msPerTS / p->mfThreshDecayTau);
 	const double u0 = (double)cbm_oracle_uniform24((uint32_t)p->mfSeed, CBM_STREAM_NCIO, 0);
 	const uint32_t mfGenSeed = (uint32_t)(int)(u0 * 2147483648.0);
 	float *thresh = malloc(numMF * sizeof(float));

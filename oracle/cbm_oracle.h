@@ -28,6 +28,19 @@ typedef struct cbm_oracle cbm_oracle;
 cbm_oracle *cbm_oracle_load(const char *path, char *err, size_t errlen);
 void cbm_oracle_free(cbm_oracle *o);
 
+/* CBMState(actPF, conPF, nZones, ...) from parameter text, with the
+ * microzone wiring and every initial value but the input-net tables, which
+ * stay at their initial values (counts 0, indices UINT_MAX) for the caller
+ * to fill through cbm_oracle_array.  pcncSeeds (nZones entries, or NULL)
+ * key each zone's random PC->NC synapses.  NULL on error (message in err). */
+cbm_oracle *cbm_oracle_new(const char *conText, const char *actText, uint32_t nZones, const int *pcncSeeds,
+		char *err, size_t errlen);
+/* Address and size of a state array by its reference name (zone < 0: the
+ * input net; else that microzone); NULL when there is none. */
+void *cbm_oracle_array(cbm_oracle *o, const char *name, int zone, uint64_t *bytes);
+/* A derived connectivity parameter by name; 0, or -1 for an unknown name. */
+int cbm_oracle_con(const cbm_oracle *o, const char *key, uint32_t *value);
+
 /* Mirror of the reference's CBMSimCore(state, mzoneRSeed, ...) seeds and of
  * its host setters (cbmsimcore.cpp:322, mzone.cpp:726-736, innet.cpp:669-677). */
 void cbm_oracle_set_seeds(cbm_oracle *o, const int *mzoneSeeds);

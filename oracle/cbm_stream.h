@@ -14,6 +14,7 @@
 
 #define CBM_STREAM_NCIO 0x4E43494Fu /* "NCIO": NC->IO release draws */
 #define CBM_STREAM_MF   0x4D46494Eu /* "MFIN": mossy-fibre Poisson draws */
+#define CBM_STREAM_WIRING 0x57495245u /* "WIRE": network construction draws */
 
 static inline uint64_t cbm_oracle_splitmix64(uint64_t x)
 {

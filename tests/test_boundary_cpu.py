@@ -209,3 +209,22 @@ def test_python_state_accessors_match_the_facade(tmp_path):
     z.resetGRPCSynWeight()
     assert np.all(z.getGRPCSynWeightLinear() == np.float32(s.act("initSynWofGRtoPC")))
     assert s.equivalent(cbm.CBMState(p))
+
+
+@pytest.mark.parametrize("config", ["config1_network", "config2_network"])
+def test_oracle_built_network_equals_the_products(tmp_path, config):
+    """The oracle's restatement of CBMState(actPF, conPF, nZones) (initial
+    values and microzone wiring, cbm_oracle_new) with the package's random
+    input-net wiring writes the same state file, byte for byte, as the
+    product's state library: the benchmark's CPU baseline builds its network
+    this way, without the product's library."""
+    import filecmp
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_state import OracleState
+    from cerebellum_simulation_b200 import networks
+    fn = getattr(networks, config)
+    a, b = tmp_path / "product.state", tmp_path / "oracle.state"
+    fn(seed=5).writeState(str(a))
+    fn(seed=5, new_state=OracleState.new).writeState(str(b))
+    assert filecmp.cmp(a, b, shallow=False)

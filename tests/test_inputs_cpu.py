@@ -49,10 +49,68 @@ def test_config3_stream_is_deterministic():
     assert 2.0 < rate_hz < 40.0
 
 
-def test_reference_arm_prints_one_contract_line():
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "3",
-                        "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+def _bench_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.mark.parametrize("steps,warmup,chunk", [(20, 5, 50), (5000, 200, 50), (1, 3, 50), (3000, 3, 7),
+                                                (123, 4, 10)])
+def test_bench_stream_covers_every_consumer(steps, warmup, chunk):
+    """The 1M workload's MF stream has a row for every step each part of
+    bench.py reads: the timed runs, the kernel-timing copy, the per-step
+    C-ABI run and the CPU baseline's sample (the driver's --steps 20
+    --warmup 5 included)."""
+    b = _bench_module()
+    plan = b.stream_plan(steps, warmup, chunk)
+    rows = plan["rows"]
+    assert plan["main"] == warmup + 2 * steps
+    assert plan["n_roof"] % chunk == 0 and plan["n_roof"] > 0
+    assert plan["roofline"] == plan["n_fl"] + plan["n_roof"] + 2 * chunk
+    assert plan["e2e"] == 20 + plan["n_e2e"]
+    assert plan["cpu"] == b.CPU_WARMUP + b.CPU_STEPS
+    for k in ("main", "roofline", "e2e", "cpu"):
+        assert plan[k] <= rows, k
+
+
+def test_cpu_baseline_rejects_a_short_stream(tmp_path):
+    """A stream shorter than the CPU sample is refused before the harness
+    runs (the failure the driver's first run met)."""
+    b = _bench_module()
+    import shutil
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_run")):
+        pytest.skip("reference harness oracle/_ref not built")
+    with pytest.raises(ValueError):
+        b.cpu_reference(str(tmp_path / "none.state"), np.zeros((45, 1024), np.uint8), b.CPU_STEPS, 1,
+                        warmup=b.CPU_WARMUP)
+    del shutil
+
+
+def test_bench_launches_ranks_itself_dry_run():
+    """`bench.py --gpus 2 --dry-run` starts two processes itself (under
+    torch.distributed.run, gloo), and rank 0 reports a world of 2."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--dry-run", "--steps", "5",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=300, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["ranks"] == 2 and len(set(d["pids"])) == 2
+
+
+def test_reference_arm_prints_one_contract_line():
+    """--impl reference prints one contract line, and its process never maps
+    the product's CUDA library (the network is built by the oracle)."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '3', '--warmup', '3']; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('MAPS_PRODUCT', 'libcbm_b200' in maps)")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "MAPS_PRODUCT False" in r.stdout
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
@@ -65,6 +123,32 @@ def test_reference_arm_prints_one_contract_line():
     assert d["value"] > 0 and d["warmup"] == 3
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
+
+
+@pytest.mark.parametrize("tau", [4.0, 10.0, 37.5, 100.0])
+def test_mf_threshold_decay_constant_is_the_references(tmp_path, tau):
+    """PoissonRegenCells' threshDecay = 1 - exp(-msPerTS / threshDecayTau)
+    (CBM_TOOLS_LIB_DEV/src/poissonregencells.cpp:20) with float operands: in
+    C++ that exp is the float overload, so the constant is 1.0f - expf(x).
+    The expression is compiled here as C++ with the reference's header
+    (<math.h>) and its result compared with the host generator's constant.
+    At 4 ms a double exp rounded to float gives the same value; at the
+    other time constants it does not."""
+    import shutil
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "decay.cpp"
+    src.write_text('#include <math.h>\n#include <stdio.h>\n#include <stdlib.h>\n'
+                   'int main(int c, char **v) { float msPerTS = 1, threshDecayTau = strtof(v[1], 0);\n'
+                   '  float threshDecay = 1 - exp(-msPerTS / threshDecayTau);\n'
+                   '  printf("%.9e\\n", (double)threshDecay); return 0; }\n')
+    exe = tmp_path / "decay"
+    subprocess.run([gxx, "-O2", "-ffp-contract=off", str(src), "-o", str(exe)], check=True)
+    ref = np.float32(float(subprocess.run([str(exe), repr(tau)], capture_output=True, text=True,
+                                          check=True).stdout))
+    got = networks.RegenPoissonMF(8, 1, thresh_decay_tau=tau).thresh_decay
+    assert got == ref
 
 
 def test_random_mf_population_follows_the_reference_rules():
@@ -109,6 +193,33 @@ def test_eyelid_out_smoothing_rule():
     for t in range(3, 8):
         want.append(np.float32((np.float32(want[t - 3] + want[t - 2]) + want[t - 1] + raw[0, t]) / 4))
     assert np.array_equal(out[0], np.array(want, np.float32))
+
+
+@pytest.mark.parametrize("pre,post", [(40, 40), (48, 48)])
+def test_raster_getters_count_completed_trials(tmp_path, pre, post):
+    """A raster read back from a data file reports the raster's completed
+    trials (curTrialN) as SpikeRasterBitArray::getNumTrials does.  With a
+    160-step window, 4 updates fill each 5-row raster trial short of its
+    last row: 2 trials x 4 updates = 8 rows, one completed trial.  With a
+    176-step window (a multiple of 32 plus 16) it is 2 x 5 = 10 updates of 5
+    rows: 2 trials."""
+    from cerebellum_simulation_b200.trialdata import TrialsData, write_ec_trials_data
+    proto = dict(preCS=pre, postCS=post, csOn=100, csOff=180, binSteps=16, numDataTrials=2)
+    rec_len = pre + 80 + post
+    bins = -(-rec_len // 16)
+    cells = {"go": 8, "grInputGO": 8, "goInputGO": 8, "goOutSynScale": 8, "mf": 16, "sc": 4, "bc": 4, "pc": 2,
+             "io": 1}
+    rng = np.random.Generator(np.random.PCG64(1))
+    td = {"psh": {n: rng.random((bins, c)).astype(np.float32) for n, c in cells.items()},
+          "raster": {n: rng.integers(0, 2 ** 32, (2, rec_len // 32, c), dtype=np.uint32)
+                     for n, c in (("go", 8), ("sc", 4), ("bc", 4), ("pc", 2), ("nc", 3), ("io", 1))}}
+    path = str(tmp_path / "data")
+    write_ec_trials_data(path, td, rng.integers(0, 9, (bins, 40)), rng.random((2, rec_len)), proto, 40)
+    updates, rows = 2 * ((rec_len - 1) // 32), rec_len // 32
+    assert updates // rows == ({160: 1, 176: 2}[rec_len])
+    r = TrialsData.from_file(path).getRaster("go")
+    assert r.getNumTrials() == updates // rows
+    assert len(r.getCellSpikeTimes(0)) == updates // rows
 
 
 def test_trial_data_file_reader_rejects_truncation(tmp_path):

@@ -1,8 +1,8 @@
 """The allocation-free PF->PC sum entry point (cbm_pfpc_sums_noalloc).
 
 It serves callers that cannot let the library allocate device memory during
-a call (their framework owns all device memory, or they call in while a
-stream is captured into a CUDA graph, or they run a real-time loop).  Here it
+a call (their framework owns all device memory through its own pool, or they
+run a real-time loop that cannot absorb an allocation).  Here it
 is checked through the C ABI against the simulator's own PF->PC input sums
 (cbm_sim_write_to_state's inputSumPFPC), bit for bit, on two calls in a row,
 and its size limit is checked.  This file runs last so that a failure here
