@@ -93,6 +93,9 @@ def _load():
         "cbm_state_load": (I, [S, ctypes.POINTER(P)]),
         "cbm_state_new": (I, [S, S, U, P, ctypes.POINTER(P)]),
         "cbm_state_save": (I, [P, S]),
+        "cbm_state_load_mem": (I, [P, U64, ctypes.POINTER(U64), ctypes.POINTER(P)]),
+        "cbm_state_save_mem": (I, [P, P, U64, ctypes.POINTER(U64)]),
+        "cbm_sim_save_mem": (I, [P, P, U64, ctypes.POINTER(U64)]),
         "cbm_state_free": (None, [P]),
         "cbm_state_num_zones": (I, [P, ctypes.POINTER(U)]),
         "cbm_state_array": (I, [P, S, I, ctypes.POINTER(P), ctypes.POINTER(U64), ctypes.POINTER(I)]),
@@ -163,13 +166,32 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else None
 
 
+def _serialised(save):
+    """Bytes of one of the C ABI's two-call serialisations (size, then data)."""
+    n = ctypes.c_uint64()
+    _check(save(None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value)
+    _check(save(buf, n.value, ctypes.byref(n)))
+    return buf.raw[: n.value]
+
+
 class CBMState:
     """The reference's CBMState (CBM_STATE_LIB_DEV/CBMStateInclude/interfaces/cbmstate.h:37-62)."""
 
     def __init__(self, path=None, _handle=None):
+        """CBMState(fstream&): path is a state file's name, or a binary file
+        object positioned at a state, which is left positioned just after it
+        (where the eyelid driver's session file continues with its trial
+        data)."""
         self._h = ctypes.c_void_p()
         if _handle is not None:
             self._h = _handle
+        elif hasattr(path, "read"):
+            start = path.tell()
+            data = path.read()
+            used = ctypes.c_uint64()
+            _check(lib.cbm_state_load_mem(data, len(data), ctypes.byref(used), ctypes.byref(self._h)))
+            path.seek(start + used.value)
         elif path is not None:
             _check(lib.cbm_state_load(os.fsencode(path), ctypes.byref(self._h)))
         else:
@@ -189,7 +211,12 @@ class CBMState:
             self._h = ctypes.c_void_p()
 
     def writeState(self, path):
-        _check(lib.cbm_state_save(self._h, os.fsencode(path)))
+        """writeState(fstream&): to a file name, or into a binary file object
+        at its position."""
+        if hasattr(path, "write"):
+            path.write(_serialised(lambda d, c, n: lib.cbm_state_save_mem(self._h, d, c, n)))
+        else:
+            _check(lib.cbm_state_save(self._h, os.fsencode(path)))
 
     def getNumZones(self):
         n = ctypes.c_uint()
@@ -205,6 +232,7 @@ class CBMState:
         if count.value == 0:
             return np.zeros(0, dtype=dtype)
         buf = (ctypes.c_char * (count.value * dtype.itemsize)).from_address(data.value)
+        buf._owner = self  # the view keeps the state (and its memory) alive
         return np.frombuffer(buf, dtype=dtype)
 
     def con(self, name):
@@ -501,8 +529,13 @@ class CBMSimCore:
         _check(lib.cbm_sim_update_err_drive(self._h, zoneN, errDriveRelative))
 
     def writeToState(self, path=None):
+        """writeToState(): the device state back into the CBMState;
+        writeToState(fstream&): then saved to a file name, or into a binary
+        file object at its position."""
         if path is None:
             _check(lib.cbm_sim_write_to_state(self._h))
+        elif hasattr(path, "write"):
+            path.write(_serialised(lambda d, c, n: lib.cbm_sim_save_mem(self._h, d, c, n)))
         else:
             _check(lib.cbm_sim_save(self._h, os.fsencode(path)))
 
@@ -604,13 +637,12 @@ class CBMSimCore:
         also its tables in path + "_MFPop"."""
         import tempfile
         with tempfile.TemporaryDirectory() as d:
-            st, td = os.path.join(d, "state"), os.path.join(d, "data")
-            self.writeToState(st)
+            td = os.path.join(d, "data")
             self.write_trial_data(td)
             with open(path, "wb") as out:
-                for part in (st, td):
-                    with open(part, "rb") as f:
-                        out.write(f.read())
+                self.writeToState(out)
+                with open(td, "rb") as f:
+                    out.write(f.read())
         if mf_population is not None:
             mf_population.write(path + "_MFPop")
 

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -75,6 +76,48 @@ int cbm_state_save(cbm_state *s, const char *path)
 {
 	NEED(s); NEED(path);
 	TRY(s->st.save(path));
+	// innetactivitystate.cpp:247-248 run on write as well
+	NamedArray *a = s->st.find("inputGOGABASynDepGO"), *b = s->st.find("goGABAOutSynScaleGOGO");
+	if (a) for (size_t i = 0; i < a->count; i++) a->as<float>()[i] = 1.0f;
+	if (b) for (size_t i = 0; i < b->count; i++) b->as<float>()[i] = 0.0f;
+	return CBM_OK;
+}
+
+int cbm_state_load_mem(const void *data, uint64_t len, uint64_t *consumed, cbm_state **out)
+{
+	NEED(data); NEED(out);
+	cbm_state *s = new (std::nothrow) cbm_state();
+	if (!s) return fail(CBM_ERR_ARG, "out of host memory");
+	size_t used = 0;
+	std::string e = s->st.loadBytes(std::string((const char *)data, (size_t)len), &used);
+	if (!e.empty()) { delete s; return fail(classify(e), e); }
+	if (consumed) *consumed = used;
+	*out = s;
+	return CBM_OK;
+}
+
+// Serialises st into dst (cap bytes) through a memory stream; *size gets the
+// bytes the state occupies.  dst == NULL only asks for the size.
+static int saveToMemory(const State &st, void *dst, uint64_t cap, uint64_t *size)
+{
+	const size_t n = st.fileBytes();
+	*size = n;
+	if (!dst) return CBM_OK;
+	if (cap < n) return fail(CBM_ERR_ARG, "buffer smaller than the state (" + std::to_string(n) + " bytes)");
+	std::ostringstream os(std::ios::binary);
+	std::string e = st.writeTo(os);
+	if (!e.empty()) return fail(CBM_ERR_IO, e);
+	const std::string &b = os.str();
+	if (b.size() != n) return fail(CBM_ERR_IO, "state serialisation size mismatch");
+	memcpy(dst, b.data(), n);
+	return CBM_OK;
+}
+
+int cbm_state_save_mem(cbm_state *s, void *dst, uint64_t cap, uint64_t *size)
+{
+	NEED(s); NEED(size);
+	int rc = saveToMemory(s->st, dst, cap, size);
+	if (rc != CBM_OK || !dst) return rc;
 	// innetactivitystate.cpp:247-248 run on write as well
 	NamedArray *a = s->st.find("inputGOGABASynDepGO"), *b = s->st.find("goGABAOutSynScaleGOGO");
 	if (a) for (size_t i = 0; i < a->count; i++) a->as<float>()[i] = 1.0f;
@@ -306,6 +349,18 @@ int cbm_sim_save(cbm_sim *sim, const char *path)
 	TRY(sim->sim.sync());
 	TRY(NET(sim).writeToState(sim->sim.stream()));
 	TRY(NET(sim).state()->save(path));
+	TRY(NET(sim).resetGOGODepression(sim->sim.stream()));
+	return CBM_OK;
+}
+
+int cbm_sim_save_mem(cbm_sim *sim, void *dst, uint64_t cap, uint64_t *size)
+{
+	NEED(sim); NEED(size);
+	if (!dst) return saveToMemory(*NET(sim).state(), nullptr, 0, size);
+	TRY(sim->sim.sync());
+	TRY(NET(sim).writeToState(sim->sim.stream()));
+	int rc = saveToMemory(*NET(sim).state(), dst, cap, size);
+	if (rc != CBM_OK) return rc;
 	TRY(NET(sim).resetGOGODepression(sim->sim.stream()));
 	return CBM_OK;
 }

@@ -439,6 +439,12 @@ std::string State::load(const std::string &path)
 	std::ifstream f(path, std::ios::binary);
 	if (!f) return "cannot open " + path;
 	std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+	size_t used = 0;
+	return loadBytes(data, &used);
+}
+
+std::string State::loadBytes(const std::string &data, size_t *consumed)
+{
 	size_t pos = 0;
 	cp = ConParams(); ap = ActParams();
 	std::string err = parseHeader(data, pos, true);
@@ -465,6 +471,7 @@ std::string State::load(const std::string &path)
 	if (!readSec(innetActSpecs(cp), innetAct)) return "state file truncated";
 	for (uint32_t z = 0; z < numZones; z++) if (!readSec(zoneActSpecs(cp, ap), zoneAct[z])) return "state file truncated";
 	fixLoaded();
+	*consumed = pos;
 	return "";
 }
 
@@ -502,6 +509,24 @@ std::string State::save(const std::string &path) const
 {
 	std::ofstream f(path, std::ios::binary | std::ios::trunc);
 	if (!f) return "cannot open " + path + " for writing";
+	return writeTo(f);
+}
+
+size_t State::fileBytes() const
+{
+	size_t n = formatHeader(*this).size();
+	auto secBytes = [&](const std::vector<Spec> &specs) {
+		for (const Spec &s : specs) n += s.count * dtypeSize(s.t);
+	};
+	secBytes(innetConSpecs(cp));
+	for (uint32_t z = 0; z < numZones; z++) secBytes(zoneConSpecs(cp));
+	secBytes(innetActSpecs(cp));
+	for (uint32_t z = 0; z < numZones; z++) secBytes(zoneActSpecs(cp, ap));
+	return n;
+}
+
+std::string State::writeTo(std::ostream &f) const
+{
 	std::string h = formatHeader(*this);
 	f.write(h.data(), (std::streamsize)h.size());
 	auto writeSec = [&](const std::vector<Spec> &specs, const std::vector<NamedArray> &arrs) {

@@ -10,6 +10,7 @@
 #pragma once
 #include <cstdint>
 #include <map>
+#include <ostream>
 #include <string>
 #include <vector>
 
@@ -110,8 +111,16 @@ public:
 
 	// CBMState(fstream&) (cbmstate.cpp:12-33).  Returns "" or an error.
 	std::string load(const std::string &path);
+	// The same from bytes in memory (a stream's content from its current
+	// position): *consumed receives the bytes the state occupies, so that
+	// whatever follows it (the eyelid driver's trial data) can be read next.
+	std::string loadBytes(const std::string &data, size_t *consumed);
 	// CBMState::writeState (cbmstate.cpp:86-103).
 	std::string save(const std::string &path) const;
+	// The same into a stream at its current position.
+	std::string writeTo(std::ostream &out) const;
+	// Bytes writeTo emits.
+	size_t fileBytes() const;
 	// A new network of the given parameter texts with every array at the
 	// reference's initial values (initializeVals of the four containers) and
 	// the microzone wiring of MZoneConnectivityState (mzoneconnectivitystate.cpp:

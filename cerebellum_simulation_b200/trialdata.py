@@ -138,16 +138,11 @@ def read_session(path):
     """The driver's session file (writeDataToFile): (CBMState, trial data)
     as ECManagementDelay's resume constructor reads it
     (ecmanagementdelay.cpp:26-50)."""
-    import os
-    import tempfile
     from . import CBMState
-    state = CBMState(path)
-    with tempfile.TemporaryDirectory() as d:
-        p = os.path.join(d, "state")
-        state.writeState(p)
-        state_bytes = os.path.getsize(p)
-    state = CBMState(path)  # writeState resets the GO->GO depression arrays, as the reference's does
     with open(path, "rb") as f:
+        state = CBMState(f)  # leaves f just after the state, like CBMState(fstream&)
+        state_bytes = f.tell()
+        f.seek(0)
         buf = f.read()
     return state, read_ec_trials_data(buf, state_bytes)
 

@@ -92,6 +92,15 @@ const char *cbm_last_error(void);
  * (histPCPopActSum) and zero. */
 int cbm_state_load(const char *path, cbm_state **out);
 
+/* CBMState(fstream&) on a stream positioned mid-file: reads one state from
+ * the len bytes at data (the stream's content from its position on) and sets
+ * *consumed (if not NULL) to the bytes the state took, so that a caller can
+ * position the stream after it, where the eyelid driver's session file keeps
+ * its trial data (ECManagementDelay(fstream&), Eyelid_Sim_CBM_Dev/src/
+ * ectrial/ecmanagementdelay.cpp:26-50).  Same interface as cbm_state_load
+ * otherwise (cbmstate.cpp:12-33). */
+int cbm_state_load_mem(const void *data, uint64_t len, uint64_t *consumed, cbm_state **out);
+
 /* A new network from the texts of a connectivity-parameter file and an
  * activity-parameter file (the two fstreams of CBMState(actPF, conPF,
  * nZones, ...), cbmstate.cpp:60-64 / 176-204).  Activity state takes the
@@ -106,6 +115,14 @@ int cbm_state_new(const char *conParamsText, const char *actParamsText, unsigned
  * reference.  Like the reference it resets the two GO->GO depression arrays
  * of the state it writes (innetactivitystate.cpp:247-248). */
 int cbm_state_save(cbm_state *s, const char *path);
+
+/* CBMState::writeState(fstream&) into memory, for a caller that writes the
+ * state into an open stream followed by other data (ECManagementDelay::
+ * writeDataToFile, ecmanagementdelay.cpp:275-290): *size receives the bytes
+ * the state occupies; with dst == NULL nothing else happens, otherwise the
+ * state is written to dst (cap bytes, at least *size, or CBM_ERR_ARG) and the
+ * GO->GO depression arrays are reset as cbm_state_save does. */
+int cbm_state_save_mem(cbm_state *s, void *dst, uint64_t cap, uint64_t *size);
 void cbm_state_free(cbm_state *s);
 int cbm_state_num_zones(const cbm_state *s, unsigned *out);
 
@@ -175,6 +192,12 @@ int cbm_sim_write_to_state(cbm_sim *sim);
  * save; like the reference, the save also resets the live GO->GO depression
  * arrays. */
 int cbm_sim_save(cbm_sim *sim, const char *path);
+
+/* CBMSimCore::writeToState(fstream&) (cbmsimcore.cpp:75-80) into memory:
+ * *size receives the bytes of the state; with dst == NULL nothing else
+ * happens, otherwise the device state is written back and serialised into
+ * dst (cap bytes, at least *size, or CBM_ERR_ARG), as cbm_sim_save does. */
+int cbm_sim_save_mem(cbm_sim *sim, void *dst, uint64_t cap, uint64_t *size);
 
 int cbm_sim_steps_done(cbm_sim *sim, uint64_t *steps);
 /* Words per MF bit row: bit k of word k/32 is MF k (numMF/32 + 1 words). */

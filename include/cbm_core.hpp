@@ -24,6 +24,7 @@
 #include <deque>
 #include <cstdint>
 #include <fstream>
+#include <iterator>
 #include <map>
 #include <ostream>
 #include <sstream>
@@ -49,12 +50,6 @@ inline void check(int rc)
 {
 	if (rc != CBM_OK) throw Error(rc, cbm_last_error());
 }
-
-// Path of an fstream the reference's API passes around: the facade reopens
-// the named file because the C ABI works on paths.
-struct StreamPath {
-	std::string path;
-};
 
 // Keys of a state's parameter file (0 connectivity, 1 activity), in the
 // reference's paramMap order.
@@ -227,9 +222,41 @@ private:
 	unsigned int zone_;
 };
 
+namespace cbm {
+// The rest of a stream from its get position (the C ABI parses memory).
+inline std::string restOf(std::istream &in, std::streampos &start)
+{
+	start = in.tellg();
+	std::string data((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+	return data;
+}
+// Writes one of the C ABI's two-call serialisations into a stream.
+template <typename F> void writeSerialised(std::ostream &out, F save)
+{
+	uint64_t n = 0;
+	check(save(nullptr, 0, &n));
+	std::vector<char> buf((size_t)n);
+	check(save(buf.data(), n, &n));
+	out.write(buf.data(), (std::streamsize)n);
+	if (!out) throw Error(CBM_ERR_IO, "stream write failed");
+}
+}  // namespace cbm
+
 class CBMState {
 public:
-	// CBMState(fstream&) reads a state file; this facade takes its path.
+	// CBMState(fstream&) (cbmstate.h:37): reads one state from the stream's
+	// position and leaves the stream just after it, where the eyelid driver's
+	// session file continues with its trial data.
+	explicit CBMState(std::fstream &infile)
+	{
+		std::streampos start;
+		std::string data = cbm::restOf(infile, start);
+		uint64_t used = 0;
+		cbm::check(cbm_state_load_mem(data.data(), data.size(), &used, &s_));
+		infile.clear();
+		infile.seekg(start + (std::streamoff)used);
+	}
+	// The same from a file name.
 	explicit CBMState(const std::string &statePath) { cbm::check(cbm_state_load(statePath.c_str(), &s_)); }
 	// CBMState(actPF, conPF, nZones, innetCRSeed, mzoneCRSeed, mzoneARSeed) from the
 	// parameter texts; the input-net wiring is left for the caller (see cbm_state_new).
@@ -242,6 +269,11 @@ public:
 	CBMState &operator=(const CBMState &) = delete;
 	virtual ~CBMState() { cbm_state_free(s_); }
 
+	// writeState(fstream&) (cbmstate.h:43): the state at the stream's position.
+	void writeState(std::fstream &outfile)
+	{
+		cbm::writeSerialised(outfile, [this](void *d, uint64_t c, uint64_t *n) { return cbm_state_save_mem(s_, d, c, n); });
+	}
 	void writeState(const std::string &path) { cbm::check(cbm_state_save(s_, path.c_str())); }
 	ct_uint32_t getNumZones()
 	{
@@ -441,6 +473,12 @@ public:
 	void updateMFInput(const ct_uint8_t *mfIn) { cbm::check(cbm_sim_update_mf(sim_, mfIn)); }
 	void updateErrDrive(unsigned int zoneN, float errDriveRelative) { cbm::check(cbm_sim_update_err_drive(sim_, zoneN, errDriveRelative)); }
 	void writeToState() { cbm::check(cbm_sim_write_to_state(sim_)); }
+	// writeToState(fstream&) (cbmsimcore.h:46): the device state written back,
+	// then the state at the stream's position.
+	void writeToState(std::fstream &outfile)
+	{
+		cbm::writeSerialised(outfile, [this](void *d, uint64_t c, uint64_t *n) { return cbm_sim_save_mem(sim_, d, c, n); });
+	}
 	void writeToState(const std::string &path) { cbm::check(cbm_sim_save(sim_, path.c_str())); }
 	InNetInterface *getInputNet() { return innet_; }
 	MZoneInterface **getMZoneList() { return zones_.data(); }

@@ -89,6 +89,7 @@ class OracleState:
             raise KeyError(name)
         dt = np.dtype(_dtype(name))
         buf = (ctypes.c_uint8 * n.value).from_address(p)
+        buf._owner = self  # the view keeps the state alive
         return np.frombuffer(buf, dtype=dt)
 
     def writeState(self, path):

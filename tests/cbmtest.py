@@ -428,6 +428,46 @@ def load_json(name):
         return json.load(f)
 
 
+def golden_large_case(name):
+    """(network, MF input [steps, numMF], events) of a large golden fixture
+    (tests/golden/make_golden.py records the reference's run of it).
+
+    config2: the 1M-GR network over 1000 steps of eyelid-coded MF input with
+    a CS from 50 to 250, large LTD/LTP steps from step 2 and an error drive at
+    249 and 749; GR history bit 39, which gates PF->PC plasticity
+    (kernels.cu:282-291), is first set about 200 steps in, so weights move in
+    the last 800 steps.  config3: the dense 4M-GR network over 400 steps of
+    state-variable-coded input, with plasticity from step 1 and an error drive
+    at 40 and 340."""
+    from cerebellum_simulation_b200 import networks
+    if name == "config2":
+        steps = 1000
+        return (networks.config2_network(seed=0),
+                networks.eyelid_mf_stream(1024, steps, seed=0, cs_on=50, cs_off=250),
+                {2: [("plast", 0, -0.01, 0.005)], 249: [("errdrive", 0, 1.0)], 749: [("errdrive", 0, 1.0)]})
+    if name == "config3":
+        steps = 400
+        return (networks.config3_network(seed=0), networks.config3_mf_stream(1024, steps, seed=0),
+                {1: [("plast", 0, -0.0005, 0.0005)], 40: [("errdrive", 0, 1.0)], 340: [("errdrive", 0, 1.0)]})
+    raise KeyError(name)
+
+
+def state_array_digests(path):
+    """SHA-256 of every array of a state file, by (zone, name): lets a run
+    whose few FP-tolerant arrays may differ in the last bits be compared
+    array by array with a recorded one."""
+    import cerebellum_simulation_b200 as cbm
+    from test_gpu_parity import INNET_ACT, INNET_CON, ZONE_ACT
+    st = cbm.CBMState(path)
+    out = {}
+    for n in INNET_CON + INNET_ACT:
+        out[f"-1/{n}"] = sha(st.array(n, -1))
+    for z in range(st.getNumZones()):
+        for n in ZONE_ACT:
+            out[f"{z}/{n}"] = sha(st.array(n, z))
+    return out
+
+
 # The GO glutamate/mGluR state uses the double-precision exp of the host C
 # library in the reference and CUDA's double exp on the device; the two can
 # differ in the last double bit, which reaches these float arrays as at most a

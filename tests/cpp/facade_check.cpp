@@ -1,16 +1,47 @@
 // A driver written against the reference's CBMState / CBMSimCore classes,
 // compiled against include/cbm_core.hpp.  With one argument it loads a state
 // and goes through the state library's accessors; with two it steps the
-// network on GPU 0 and reads NC spikes.
+// network on GPU 0 and reads NC spikes.  "--stream OUT" (after the state)
+// writes the state and then other data into one fstream and reads both
+// back, as the eyelid driver's session file does (ECManagementDelay::
+// writeDataToFile and its resume constructor, Eyelid_Sim_CBM_Dev/src/
+// ectrial/ecmanagementdelay.cpp:26-50, 275-290); after the stepping run's
+// two arguments it does the same with CBMSimCore::writeToState(fstream&).
 #include <cbm_core.hpp>
 
 #include <cstdio>
+#include <cstring>
+#include <string>
 #include <vector>
+
+// The state, then a trailer, in one stream; then both read back from one
+// stream: the state through CBMState(fstream&), the trailer after it.
+template <typename W> static void streamRoundTrip(const char *path, W writeState)
+{
+	{
+		std::fstream out(path, std::ios::out | std::ios::binary | std::ios::trunc);
+		writeState(out);
+		out << "trailer 4242\n";
+	}
+	std::fstream in(path, std::ios::in | std::ios::binary);
+	CBMState back(in);
+	std::string word;
+	int value = 0;
+	in >> word >> value;
+	std::printf("stream zones %u trailer %s %d\n", back.getNumZones(), word.c_str(), value);
+	std::string again = std::string(path) + ".again";
+	back.writeState(again);
+}
 
 int main(int argc, char **argv)
 {
 	if (argc < 2) return 2;
+	const char *streamOut = nullptr;
+	for (int i = 1; i + 1 < argc; i++)
+		if (!std::strcmp(argv[i], "--stream")) { streamOut = argv[i + 1]; argc = i; break; }
 	CBMState st(argv[1]);
+	if (streamOut && argc == 2)
+		streamRoundTrip(streamOut, [&](std::fstream &f) { st.writeState(f); });
 	std::printf("zones %u\n", st.getNumZones());
 	// the state library's accessors, as the eyelid driver reaches them
 	// (ecmanagementdelay.cpp:106-150); they edit the state, so only without
@@ -55,6 +86,7 @@ int main(int argc, char **argv)
 		const float *vpc = sim.getMZoneList()[0]->exportVmPC();
 		std::printf("steps 50 nc0 %d vpc0 %.6f\n", nc[0], vpc[0]);
 		sim.writeToState(argv[2]);
+		if (streamOut) streamRoundTrip(streamOut, [&](std::fstream &f) { sim.writeToState(f); });
 	}
 	return 0;
 }

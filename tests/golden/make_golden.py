@@ -12,11 +12,14 @@ Runs here, where the reference tree and its harness (oracle/_ref, built by
   config1_digests.json   the same for the synthetic 16K network of the package
                          (config 1), built with networks.config1_network(seed=0)
   config2_digests.json   the same for the 1M-GR network (networks.config2_network,
-                         300 steps of eyelid-coded MF input with a CS, plasticity
-                         and an error drive)
+                         1000 steps of eyelid-coded MF input with a CS,
+                         plasticity that moves PF->PC weights, and error
+                         drives), plus the SHA-256 of every array of the
+                         initial and final states
   config3_digests.json   the same for the dense 4M-GR network
-                         (networks.config3_network, 60 steps of state-variable
+                         (networks.config3_network, 400 steps of state-variable
                          coded MF input)
+  (the inputs of both: cbmtest.golden_large_case)
 
 usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -46,18 +49,6 @@ EVENTS16K = {
 STEPS16K = 1500
 MF_SEED16K = 11
 ZONE_SEEDS = [7]
-
-
-def _large_cases():
-    from cerebellum_simulation_b200 import networks
-    return [
-        ("config2", lambda: networks.config2_network(seed=0),
-         lambda n: networks.eyelid_mf_stream(1024, n, seed=0, cs_on=50, cs_off=250), 300,
-         {2: [("plast", 0, -0.01, 0.005)], 249: [("errdrive", 0, 1.0)]}),
-        ("config3", lambda: networks.config3_network(seed=0),
-         lambda n: networks.config3_mf_stream(1024, n, seed=0), 60,
-         {1: [("plast", 0, -0.0005, 0.0005)], 40: [("errdrive", 0, 1.0)]}),
-    ]
 
 
 def digests(trace, rb, final_state):
@@ -97,16 +88,20 @@ def main(ref_root):
         with open(os.path.join(HERE, "config1_digests.json"), "w") as f:
             json.dump(out, f)
 
-        for name, build, stream, steps, events in _large_cases():
-            net = build()
+        for name in ("config2", "config3"):
+            net, mf, events = cbmtest.golden_large_case(name)
+            steps = mf.shape[0]
             p = os.path.join(d, name + ".state")
             net.writeState(p)
-            mf = stream(steps)
+            del net
             fin = os.path.join(d, name + "_final.state")
             tr = cbmtest.ref_run(p, mf, ZONE_SEEDS, events, final_path=fin)
             out = digests(tr, tr.size // steps, fin)
+            del tr
             with open(p, "rb") as f:
                 out["initial_state"] = cbmtest.sha(np.frombuffer(f.read(), np.uint8))
+            out["initial_arrays"] = cbmtest.state_array_digests(p)
+            out["final_arrays"] = cbmtest.state_array_digests(fin)
             with open(os.path.join(HERE, name + "_digests.json"), "w") as f:
                 json.dump(out, f)
 

@@ -176,6 +176,55 @@ def test_valid_network_needs_a_device(tmp_path):
         sim.close()
 
 
+def test_cpp_facade_state_in_a_stream_with_trailing_data(tmp_path):
+    """CBMState::writeState(fstream&) then other data into one stream, and
+    CBMState(fstream&) reading the state back and leaving the stream where
+    the data starts, as the eyelid driver's session file is written and
+    resumed (ecmanagementdelay.cpp:26-50, 275-290).  The state read back from
+    the stream saves to the same bytes as the original file."""
+    import subprocess
+    exe = cbmtest.build_facade_check(str(tmp_path))
+    p = cbmtest.golden_state("ref16k", str(tmp_path))
+    out_path = str(tmp_path / "session")
+    out = subprocess.run([exe, p, "--stream", out_path], check=True, capture_output=True, text=True).stdout
+    assert "stream zones 1 trailer trailer 4242" in out
+    state_bytes = open(p, "rb").read()
+    session = open(out_path, "rb").read()
+    assert session[: len(state_bytes)] == state_bytes
+    assert session[len(state_bytes):] == b"trailer 4242\n"
+    assert open(out_path + ".again", "rb").read() == state_bytes
+
+
+def test_state_memory_calls_reject_a_small_buffer(tmp_path):
+    """cbm_state_save_mem reports the state's size for a NULL buffer and
+    refuses one that is too small; cbm_state_load_mem reports the bytes it
+    consumed when data follows the state."""
+    import ctypes
+    import cerebellum_simulation_b200 as cbm
+    lib = cbm.lib
+    p = cbmtest.golden_state("ref16k", str(tmp_path))
+    st = cbm.CBMState(p)
+    size = ctypes.c_uint64()
+    lib.cbm_state_save_mem.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                       ctypes.POINTER(ctypes.c_uint64)]
+    assert lib.cbm_state_save_mem(st._h, None, 0, ctypes.byref(size)) == 0
+    want = open(p, "rb").read()
+    assert size.value == len(want)
+    small = ctypes.create_string_buffer(16)
+    assert lib.cbm_state_save_mem(st._h, small, 16, ctypes.byref(size)) == 1  # CBM_ERR_ARG
+    buf = ctypes.create_string_buffer(size.value)
+    assert lib.cbm_state_save_mem(st._h, buf, size.value, ctypes.byref(size)) == 0
+    assert buf.raw == want
+    data = want + b"next"
+    h, used = ctypes.c_void_p(), ctypes.c_uint64()
+    lib.cbm_state_load_mem.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                       ctypes.POINTER(ctypes.c_void_p)]
+    assert lib.cbm_state_load_mem(data, len(data), ctypes.byref(used), ctypes.byref(h)) == 0
+    assert used.value == len(want)
+    lib.cbm_state_free(h)
+    assert lib.cbm_state_load_mem(data[: len(want) // 2], len(want) // 2, ctypes.byref(used), ctypes.byref(h)) != 0
+
+
 def test_python_state_accessors_match_the_facade(tmp_path):
     """The Python mirror of the state library's accessors gives what the C++
     facade's do on the same state file."""

@@ -137,6 +137,45 @@ def test_config3_4m_bit_exact_short(tmp_path):
     assert compare_states(fo, fp) == []
 
 
+@pytest.mark.parametrize("name", ["config2", "config3"])
+def test_large_networks_match_reference_golden(tmp_path, name):
+    """The device against the reference itself, with no oracle in between:
+    every step's spike raster and spike-relevant float state of the 1M-GR
+    network over 1000 steps (PF->PC weights moving both ways from about step
+    200) and of the dense 4M-GR network over 400, and every array of the
+    final state, equal the digests of the reference's own run
+    (tests/golden/make_golden.py; inputs cbmtest.golden_large_case).  The
+    four GO glutamate/mGluR arrays, which no spike reads, are compared with
+    the oracle in the tests above instead."""
+    import cerebellum_simulation_b200 as cbm
+    gold = cbmtest.load_json(name + "_digests.json")
+    net, mf, ev = cbmtest.golden_large_case(name)
+    p = str(tmp_path / "net.state")
+    net.writeState(p)
+    del net
+    sim = cbm.CBMSimCore(cbm.CBMState(p), [7], device=0)
+    zones, inet = sim.getMZoneList(), sim.getInputNet()
+    for s in range(mf.shape[0]):
+        for e in ev.get(s + 1, []):
+            if e[0] == "plast":
+                zones[e[1]].setGRPCPlastSteps(e[2], e[3])
+            elif e[0] == "errdrive":
+                sim.updateErrDrive(e[1], e[2])
+        sim.updateMFInput(mf[s])
+        sim.calcActivity()
+        rec = cbmtest.product_record(sim, None)
+        if cbmtest.sha(rec) != gold["records"][s]:
+            pytest.fail(f"step {s + 1}: the device's record differs from the reference's")
+    fin = str(tmp_path / "b200.state")
+    sim.writeToState(fin)
+    sim.close()
+    got = cbmtest.state_array_digests(fin)
+    bad = [k for k, v in gold["final_arrays"].items()
+           if k.split("/")[1] not in cbmtest.FP_TOLERANT_ARRAYS and got[k] != v]
+    assert not bad, f"final state arrays differ from the reference's: {bad}"
+    assert gold["final_arrays"]["0/pfSynWeightPC"] != gold["initial_arrays"]["0/pfSynWeightPC"]
+
+
 def test_graph_run_equals_step_calls(tmp_path):
     """Resident-input CUDA-graph runs give the step-by-step API's result."""
     import cerebellum_simulation_b200 as cbm

@@ -192,3 +192,47 @@ def test_eyelid_session_matches_oracle(tmp_path):
     raw, want = open(out, "rb").read(), open(odata, "rb").read()
     assert raw.endswith(want) and data["end"] == len(raw)
     assert np.array_equal(networks.MFPopulation.read(out + "_MFPop").rates(), pop.rates())
+
+
+def test_config2_1m_full_trial_bit_exact(tmp_path):
+    """A whole eyelid trial of the 1M-GR network (1,048,576 GR, 32 PC x 32,768
+    PF: the benchmark's network and the widest PF->PC reduction) run on the
+    device as graph replays: 5000 steps, CS at 2000-2500 ms, the US at step
+    2499, LTD/LTP steps in force from 2200 to 2700 ms.  History bit 39 is set
+    200 steps after a GR's first spiking bin, so plasticity moves PF->PC
+    weights in this trial.  The final state (every GR array, every PF->PC
+    weight), the NC/PC records, the eyelid trace and the ECTrialsData
+    histograms and rasters equal the oracle's bit for bit, and weights have
+    moved both down (LTD) and up (LTP)."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    st = networks.config2_network(seed=2)
+    st_path = str(tmp_path / "c2.state")
+    st.writeState(st_path)
+    bg, cs = networks.eyelid_mf_rates(st.con("numMF"), seed=2)
+    rates = np.stack([bg, cs, cs])
+    proto = cbm.eyelid_protocol_defaults(st, mfSeed=5, numDataTrials=1)
+    steps = proto["trialSteps"]
+    assert steps == 5000 and proto["csOn"] == 2000 and proto["csOff"] == 2500
+    o = Oracle(st_path, seeds=[7])
+    _, o_nc, o_pc, o_eye, want = o.run_protocol(proto, rates, steps, record=False, trial_data=True)
+    fin_o = str(tmp_path / "oracle.state")
+    o.save(fin_o)
+    sim = cbm.CBMSimCore(cbm.CBMState(st_path), [7], device=0)
+    sim.set_eyelid_protocol(rates, **proto)
+    sim.record_trial_data()
+    sim.run(steps, 50)
+    _compare_records(sim, o_nc, o_pc, o_eye)
+    got = sim.trial_data()
+    fin_p = str(tmp_path / "b200.state")
+    sim.writeToState(fin_p)
+    sim.close()
+    assert compare_states(fin_o, fin_p) == []
+    for name, a in want["psh"].items():
+        assert cbmtest.same_values(got["psh"][name].ravel(), a.ravel()).all(), name
+    for name, a in want["raster"].items():
+        assert np.array_equal(got["raster"][name], a), name
+    w0 = cbm.CBMState(st_path).array("pfSynWeightPC", 0)
+    w1 = cbm.CBMState(fin_p).array("pfSynWeightPC", 0)
+    assert (w1 < w0).sum() > 0 and (w1 > w0).sum() > 0, "no PF->PC weight moved both ways"
+    assert o_pc.sum() > 0

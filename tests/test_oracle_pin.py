@@ -199,36 +199,39 @@ def test_mf_population_estimate_matches_reference(tmp_path):
 def test_oracle_matches_reference_golden_large(tmp_path, name):
     """The 1M-GR network (32 PC x 32,768 PF: the reference's PF->PC reduction
     in its widest shape, 512 threads and 32 pair-adds each, kernels.cu:
-    445-469, which the 16K networks never reach) over 300 active steps, and
-    the dense 4M-GR network (4096 GO, 128 PC) over 60: every trace record and
-    the final state against the reference's, recorded by
-    tests/golden/make_golden.py."""
-    from cerebellum_simulation_b200 import networks
+    445-469, which the 16K networks never reach) over 1000 active steps in
+    which plasticity moves PF->PC weights both ways, and the dense 4M-GR
+    network (4096 GO, 128 PC) over 400: every trace record and the final
+    state against the reference's, recorded by tests/golden/make_golden.py
+    (inputs: cbmtest.golden_large_case)."""
     gold = cbmtest.load_json(name + "_digests.json")
-    net = networks.config2_network(seed=0) if name == "config2" else networks.config3_network(seed=0)
+    net, mf, ev = cbmtest.golden_large_case(name)
     st = str(tmp_path / "net.state")
     net.writeState(st)
+    del net
     with open(st, "rb") as f:
         assert cbmtest.sha(np.frombuffer(f.read(), np.uint8)) == gold["initial_state"], \
             "network generator is not deterministic"
     steps = gold["steps"]
-    if name == "config2":
-        mf = networks.eyelid_mf_stream(1024, steps, seed=0, cs_on=50, cs_off=250)
-        ev = {2: [("plast", 0, -0.01, 0.005)], 249: [("errdrive", 0, 1.0)]}
-    else:
-        mf = networks.config3_mf_stream(1024, steps, seed=0)
-        ev = {1: [("plast", 0, -0.0005, 0.0005)], 40: [("errdrive", 0, 1.0)]}
+    assert mf.shape[0] == steps
     o = Oracle(st, seeds=[7])
     tr = o.run(mf, ev)
     assert tr.shape[1] == gold["record_bytes"]
     assert np.unpackbits(tr[:, : o.num["GR"] // 8], axis=1).sum() > 100000
     got = [cbmtest.sha(r) for r in tr]
+    del tr
     bad = [i for i, (a, b) in enumerate(zip(got, gold["records"])) if a != b]
     assert not bad, f"first differing step {bad[0] + 1}"
     fin = str(tmp_path / "final.state")
     o.save(fin)
     with open(fin, "rb") as f:
         assert cbmtest.sha(np.frombuffer(f.read(), np.uint8)) == gold["final_state"]
+    # the run exercises plasticity: the reference's final weights differ
+    # from the initial ones, and the oracle's final state is the reference's
+    assert gold["final_arrays"]["0/pfSynWeightPC"] != gold["initial_arrays"]["0/pfSynWeightPC"]
+    import cerebellum_simulation_b200 as cbm
+    w0, w1 = cbm.CBMState(st).array("pfSynWeightPC", 0), cbm.CBMState(fin).array("pfSynWeightPC", 0)
+    assert (w1 < w0).any() and (w1 > w0).any()
 
 
 @pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
