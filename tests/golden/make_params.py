@@ -7,7 +7,10 @@ bundled sets are taken from the reference's parameter files
 and written in the key/value form ActivityParams(fstream&) reads
 (CBM_STATE_LIB_DEV/src/params/activityparams.cpp:12-42).
 
-usage: python make_params.py /path/to/reference/CBM_Params
+Test-side tooling: it reads the reference tree, so it lives beside the golden
+fixtures' generator and writes into cerebellum_simulation_b200/params/.
+
+usage: python tests/golden/make_params.py /path/to/reference/CBM_Params
 """
 import os
 import sys
@@ -31,7 +34,8 @@ def convert(src, dst):
 
 if __name__ == "__main__":
     ref = sys.argv[1]
-    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    dest = os.path.join(root, "cerebellum_simulation_b200", "params")
     for out, src in SETS.items():
-        convert(os.path.join(ref, src), os.path.join(here, out))
+        convert(os.path.join(ref, src), os.path.join(dest, out))
         print(out)

@@ -75,3 +75,38 @@ def test_batch_autotune_keeps_results(tmp_path):
     b.run(2 * protos[0]["trialSteps"] - 150, 50)
     _check_instances(b, [cbmtest.golden_state("ref16k", str(tmp_path))] + paths[1:], protos, rates,
                      2 * protos[0]["trialSteps"], tmp_path, "b")
+
+
+def test_batch_config4_sizes_match_instances_alone(tmp_path):
+    """Instances at the batched sweep's sizes, built as its workload builds
+    them (random wiring with 4 GO targets per GR, 1024 GO, 32 PC, GO
+    threshold and LTD step scaled per instance): 2,097,152 GR (32 PC x 65,536
+    PF), 1,048,576 GR (the shape-specialised pass's network shape) and
+    262,144 GR, advanced together in one batch over two 400-step trials
+    whose second trial moves PF->PC weights.  Each instance's records and
+    final state equal the oracle's for that instance alone."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    paths, protos = [], []
+    for i, (gx, gy, go_scale, ltd_scale) in enumerate([(11, 10, 0.9, 1.6), (11, 9, 1.1, 0.7), (10, 8, 1.0, 1.0)]):
+        st = networks.build_random_network(gx, gy, 6, 4, 10, networks.act_params("dense"), seed=70 + i,
+                                           go_out_per_gr=4, mf_per_go=16, vel=147)
+        st.setActParam("threshBaseGO", st.act("threshBaseGO") * go_scale)
+        p = str(tmp_path / f"inst{i}.state")
+        st.writeState(p)
+        del st
+        paths.append(p)
+        protos.append(cbmtest.short_protocol(mfSeed=51 + i, plastLTD=-0.004 * ltd_scale, numDataTrials=2))
+    states = [cbm.CBMState(p) for p in paths]
+    assert [s.con("numGR") for s in states] == [1 << 21, 1 << 20, 1 << 18]
+    rates = [cbmtest.protocol_rates(st.con("numMF"), seed=20 + i) for i, st in enumerate(states)]
+    b = cbm.CBMBatch(states, [[40 + i] for i in range(len(states))], device=0)
+    for i in range(len(states)):
+        b.set_eyelid_protocol(i, rates[i], **protos[i])
+    steps = 2 * protos[0]["trialSteps"]
+    b.run(steps, 50)
+    _check_instances(b, paths, protos, rates, steps, tmp_path, "c4")
+    for i, p in enumerate(paths):
+        w0 = cbm.CBMState(p).array("pfSynWeightPC", 0)
+        w1 = cbm.CBMState(str(tmp_path / f"b{i}_c4.state")).array("pfSynWeightPC", 0)
+        assert (w1 != w0).any(), f"instance {i}: no PF->PC weight moved"
