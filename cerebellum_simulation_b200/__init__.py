@@ -146,6 +146,9 @@ def _load():
         "cbm_sim_timer_stop": (I, [P, ctypes.POINTER(F)]),
         "cbm_sim_destroy": (None, [P]),
         "cbm_device_expf": (I, [I, P, P, U64]),
+        "cbm_device_exp": (I, [I, P, P, U64]),
+        "cbm_sim_set_statevar_input": (I, [P, P]),
+        "cbm_sim_statevar_rates": (I, [P, U64, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -590,6 +593,33 @@ class CBMSimCore:
         _check(lib.cbm_sim_set_eyelid_protocol(self._h, ctypes.byref(p)))
         self._protocol = protocol
 
+    def set_statevar_input(self, coding, values, mfSeed=0, mfThreshDecayTau=4.0):
+        """Drive the MF input from the next step on by the state-variable
+        coding on the device (cbm_sim_set_statevar_input): coding is a
+        networks.StateVariableMF (its fibre assignment, preferred values,
+        width and rates), values the environment's state, [steps, numVars],
+        used row by row and cyclically."""
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        if values.ndim != 2 or values.shape[1] != coding.n_vars:
+            raise ValueError("values must be [steps, numVars]")
+        mean = np.ascontiguousarray(coding.mean, dtype=np.float32)
+        relaxed = np.ascontiguousarray(coding.relaxed, dtype=np.float32)
+        excited = np.ascontiguousarray(coding.excited, dtype=np.float32)
+        c = StateVarInput(numVars=coding.n_vars, fibresPerVar=coding.per, lo=float(coding.lo), hi=float(coding.hi),
+                          den=float(coding._den), norm=float(coding._norm), maxPossible=float(coding._max_possible),
+                          mean=mean.ctypes.data, relaxed=relaxed.ctypes.data, excited=excited.ctypes.data,
+                          values=values.ctypes.data, numSteps=values.shape[0], mfSeed=mfSeed,
+                          mfThreshDecayTau=mfThreshDecayTau)
+        _check(lib.cbm_sim_set_statevar_input(self._h, ctypes.byref(c)))
+        self._protocol = None
+
+    def statevar_rates(self, row):
+        """The MF rates (Hz) the device computes for row `row` of the
+        running state-variable input's values."""
+        out = np.empty(self.state.con("numMF"), dtype=np.float32)
+        _check(lib.cbm_sim_statevar_rates(self._h, row, out.ctypes.data))
+        return out
+
     def record_gr(self):
         """Record the running protocol's GR peri-stimulus histogram on the
         device from the next step on (cbm_sim_record_gr)."""
@@ -687,7 +717,7 @@ class CBMSimCore:
         """(kernel name, consumer warps, rows per stage, stages) of the GR pass."""
         v = [ctypes.c_uint32() for _ in range(4)]
         _check(lib.cbm_sim_pass_geometry(self._h, *[ctypes.byref(x) for x in v]))
-        kind = ("grPassKernel", "grPassTmaKernel", "grPassPersistentKernel")[v[0].value]
+        kind = ("grPassKernel", "grPassTmaKernel", "grPassPersistentKernel", "grPassVecKernel")[v[0].value]
         return kind, v[1].value, v[2].value, v[3].value
 
 
@@ -766,6 +796,15 @@ _PROTOCOL_FIELDS = [("trialSteps", ctypes.c_uint32), ("csOn", ctypes.c_int32), (
                     ("eyeGShift", ctypes.c_float), ("eyeGLeakRaw", ctypes.c_float), ("eyeMaxAmp", ctypes.c_float)]
 
 
+class StateVarInput(ctypes.Structure):
+    """cbm_statevar_input (include/cbm_b200.h)."""
+    _fields_ = [("numVars", ctypes.c_uint32), ("fibresPerVar", ctypes.c_uint32), ("lo", ctypes.c_float),
+                ("hi", ctypes.c_float), ("den", ctypes.c_float), ("norm", ctypes.c_double),
+                ("maxPossible", ctypes.c_float), ("mean", ctypes.c_void_p), ("relaxed", ctypes.c_void_p),
+                ("excited", ctypes.c_void_p), ("values", ctypes.c_void_p), ("numSteps", ctypes.c_uint64),
+                ("mfSeed", ctypes.c_int32), ("mfThreshDecayTau", ctypes.c_float)]
+
+
 class EyelidProtocol(ctypes.Structure):
     """cbm_eyelid_protocol (include/cbm_b200.h)."""
     _fields_ = _PROTOCOL_FIELDS
@@ -810,4 +849,12 @@ def device_expf(x, device=0):
     x = np.ascontiguousarray(x, dtype=np.float32)
     out = np.empty_like(x)
     _check(lib.cbm_device_expf(device, _ptr(x), _ptr(out), x.size))
+    return out
+
+
+def device_exp(x, device=0):
+    """The device's double exp (cbm_device_exp) of float64 values."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    _check(lib.cbm_device_exp(device, _ptr(x), _ptr(out), x.size))
     return out

@@ -25,7 +25,8 @@ NVCC_FLAGS = [
     "-I", os.path.join(ROOT, "include"),
 ]
 
-SOURCES = ["cbm_state.cpp", "cbm_sim.cu", "cbm_kernels.cu", "cbm_capi.cu", "cbm_noalloc.cu", "cbm_mlp.cu"]
+SOURCES = ["cbm_state.cpp", "cbm_sim.cu", "cbm_kernels.cu", "cbm_pass_vec.cu", "cbm_capi.cu", "cbm_noalloc.cu",
+           "cbm_mlp.cu"]
 
 
 def nvcc():

@@ -425,6 +425,21 @@ int cbm_sim_set_eyelid_protocol(cbm_sim *sim, const cbm_eyelid_protocol *protoco
 	return CBM_OK;
 }
 
+int cbm_sim_set_statevar_input(cbm_sim *sim, const cbm_statevar_input *input)
+{
+	NEED(sim); NEED(input);
+	TRY(sim->sim.setStateVarInput(0, *input));
+	return CBM_OK;
+}
+
+int cbm_sim_statevar_rates(cbm_sim *sim, uint64_t step, float *out)
+{
+	NEED(sim); NEED(out);
+	TRY(sim->sim.sync());
+	TRY(NET(sim).stateVarRates(step, out, sim->sim.stream()));
+	return CBM_OK;
+}
+
 uint64_t cbm_sim_trial_record_bytes(cbm_sim *sim, int kind)
 {
 	return sim ? NET(sim).recordBytes(kind) : 0;
@@ -640,6 +655,21 @@ int cbm_device_expf(int device, const float *in, float *out, uint64_t n)
 	cudaMemcpy(d, in, n * sizeof(float), cudaMemcpyHostToDevice);
 	expfProbeKernel<<<(unsigned)((n + 255) / 256), 256>>>(d, d + n, (uint32_t)n);
 	cudaError_t e = cudaMemcpy(out, d + n, n * sizeof(float), cudaMemcpyDeviceToHost);
+	cudaFree(d);
+	if (e != cudaSuccess) return fail(CBM_ERR_CUDA, cudaGetErrorString(e));
+	return CBM_OK;
+}
+
+int cbm_device_exp(int device, const double *in, double *out, uint64_t n)
+{
+	NEED(in); NEED(out);
+	if (n > 0xFFFFFFFFull) return fail(CBM_ERR_ARG, "at most 2^32-1 values per call");
+	if (cudaSetDevice(device) != cudaSuccess) return fail(CBM_ERR_CUDA, "cannot select device");
+	double *d = nullptr;
+	if (cudaMalloc(&d, 2 * n * sizeof(double)) != cudaSuccess) return fail(CBM_ERR_CUDA, "device allocation failed");
+	cudaMemcpy(d, in, n * sizeof(double), cudaMemcpyHostToDevice);
+	expProbeKernel<<<(unsigned)((n + 255) / 256), 256>>>(d, d + n, (uint32_t)n);
+	cudaError_t e = cudaMemcpy(out, d + n, n * sizeof(double), cudaMemcpyDeviceToHost);
 	cudaFree(d);
 	if (e != cudaSuccess) return fail(CBM_ERR_CUDA, cudaGetErrorString(e));
 	return CBM_OK;

@@ -133,12 +133,20 @@ struct DevProtocol {
 	float *tdPSH;
 	uint32_t *tdRaster;
 	float eyeGDecay, eyeGInc, eyeGShift, eyeGLeak, eyeMaxAmp;
+	// state-variable MF coding (cbm_statevar_input), or svValues null: the
+	// rate tables above
+	const float *svMean, *svRelaxed, *svExcited, *svValues;
+	uint64_t svSteps;
+	uint32_t svVars, svPer;
+	float svLo, svHi, svDen, svMaxPossible;
+	double svNorm;
 };
 
 struct DevZone {
 	float *w;           // pfSynWeightPC, PC-major (mzone.cpp:97-103)
 	float *pcPartial;   // [3][numPC][bs] per-thread partial sums of the PF->PC reduction
-	float *pairSum;     // [2][numPC][K][bs] x[i] + x[i+bs] of the reduction per step parity (persistent GR pass)
+	float *pairSum;     // [2][numPC][K][bs] x[i] + x[i+bs] of the reduction per step parity (persistent and vector GR passes)
+	float *pcSum;       // [3][numPC] PF->PC input sums (the whole reduction), made by the vector GR pass
 	uint8_t *plastSel;  // [2][numIO]: 0 none, 1 LTD, 2 LTP for the next plasticity step
 	const uint32_t *ioOfPC;  // IO whose timer drives each PC block's plasticity (mzone.cpp:682-705)
 
@@ -175,6 +183,7 @@ struct DevNet {
 	uint32_t numCoupLevels;
 	uint32_t mfRing;                      // slots in the MF input ring
 	uint32_t hasMFRaw;
+	uint32_t pcSumMode;                   // 1: the small-cell update reads pcSum, else it reduces pcPartial
 
 	// ---- parameters (activityparams.h)
 	float gLeakGR, eLeakGR, eGOGR, threshRestGR, threshMaxGR, threshDecGR;
@@ -228,6 +237,8 @@ struct DevNet {
 	const uint32_t *coupLevelStart, *coupLevelGO;  // coupling sweep schedule
 
 	// ---- step pipeline
+	uint64_t *pairStep;  // [2] the step whose PF->PC pair sums each pairSum slot holds (vector GR pass)
+	uint32_t *passClaim; // [3] work counters of the vector GR pass, per step mod 3
 	uint32_t *goCount;   // [2][numGO] GR->GO input counts per step parity
 	uint32_t *bcCount;   // [3][numBC] PF->BC counts
 	uint32_t *scCount;   // [3][numSC] PF->SC counts
@@ -262,6 +273,16 @@ constexpr uint32_t kStageArenaOff = kStageNetBytes + 16;
 __device__ __forceinline__ uint64_t stepsDone(const DevNet *N)
 {
 	return *reinterpret_cast<const uint64_t *>(reinterpret_cast<const char *>(N) + kStageNetBytes);
+}
+
+// Zone z's PF->PC step for plasticity selector sel (1 LTD, 2 LTP) at step t:
+// the host setters' value, or for zone 0 under a device protocol the value
+// the protocol set for step t.
+__device__ __forceinline__ float plasticityStep(const DevNet *N, uint64_t t, uint32_t z, uint8_t sel)
+{
+	if (sel == 0) return 0.0f;
+	if (z == 0 && N->proto) return N->proto->ctlSlots[(t & 1) * 3 + (sel == 1 ? 0 : 1)];
+	return sel == 1 ? N->ctl->ltdStep[z] : N->ctl->ltpStep[z];
 }
 #endif
 

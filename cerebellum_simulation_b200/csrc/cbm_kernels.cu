@@ -92,19 +92,143 @@ __global__ void expfProbeKernel(const float *in, float *out, uint32_t n)
 	if (i < n) out[i] = cbmExpf(in[i], kExp2Tab);
 }
 
+// exp of a double, where the reference calls the C library's double exp
+// (the GO glutamate term, innet.cpp:850-858; the state-variable MF coding,
+// Matthew_Sim_CBM/includes/statevariable.hpp:108-129).  The same published
+// algorithm as glibc 2.28+ (ARM optimized-routines exp, N = 128) with the
+// fused multiply-adds of its x86-64 FMA build: x = (k + r) ln2/128 with
+// ln2/128 split in two parts, 2^(k/128) = H[k] (1 + T[k]) from the table,
+// exp(r) - 1 from a quintic in r, and for |x| > 512 the rescaled paths that
+// keep the scale finite.  kExpTab holds for each k the tail T[k] and
+// asuint64(H[k]) - (k << 45), where H[k] is 2^(k/128) rounded to the nearest
+// double and T[k] = (2^(k/128) - H[k]) / H[k] rounded likewise.
+__device__ uint64_t kExpTab[256] = {
+	0x0000000000000000ull, 0x3ff0000000000000ull, 0x3c9b3b4f1a88bf6eull, 0x3feff63da9fb3335ull,
+	0xbc7160139cd8dc5dull, 0x3fefec9a3e778061ull, 0xbc905e7a108766d1ull, 0x3fefe315e86e7f85ull,
+	0x3c8cd2523567f613ull, 0x3fefd9b0d3158574ull, 0xbc8bce8023f98efaull, 0x3fefd06b29ddf6deull,
+	0x3c60f74e61e6c861ull, 0x3fefc74518759bc8ull, 0x3c90a3e45b33d399ull, 0x3fefbe3ecac6f383ull,
+	0x3c979aa65d837b6dull, 0x3fefb5586cf9890full, 0x3c8eb51a92fdeffcull, 0x3fefac922b7247f7ull,
+	0x3c3ebe3d702f9cd1ull, 0x3fefa3ec32d3d1a2ull, 0xbc6a033489906e0bull, 0x3fef9b66affed31bull,
+	0xbc9556522a2fbd0eull, 0x3fef9301d0125b51ull, 0xbc5080ef8c4eea55ull, 0x3fef8abdc06c31ccull,
+	0xbc91c923b9d5f416ull, 0x3fef829aaea92de0ull, 0x3c80d3e3e95c55afull, 0x3fef7a98c8a58e51ull,
+	0xbc801b15eaa59348ull, 0x3fef72b83c7d517bull, 0xbc8f1ff055de323dull, 0x3fef6af9388c8deaull,
+	0x3c8b898c3f1353bfull, 0x3fef635beb6fcb75ull, 0xbc96d99c7611eb26ull, 0x3fef5be084045cd4ull,
+	0x3c9aecf73e3a2f60ull, 0x3fef54873168b9aaull, 0xbc8fe782cb86389dull, 0x3fef4d5022fcd91dull,
+	0x3c8a6f4144a6c38dull, 0x3fef463b88628cd6ull, 0x3c807a05b0e4047dull, 0x3fef3f49917ddc96ull,
+	0x3c968efde3a8a894ull, 0x3fef387a6e756238ull, 0x3c875e18f274487dull, 0x3fef31ce4fb2a63full,
+	0x3c80472b981fe7f2ull, 0x3fef2b4565e27cddull, 0xbc96b87b3f71085eull, 0x3fef24dfe1f56381ull,
+	0x3c82f7e16d09ab31ull, 0x3fef1e9df51fdee1ull, 0xbc3d219b1a6fbffaull, 0x3fef187fd0dad990ull,
+	0x3c8b3782720c0ab4ull, 0x3fef1285a6e4030bull, 0x3c6e149289cecb8full, 0x3fef0cafa93e2f56ull,
+	0x3c834d754db0abb6ull, 0x3fef06fe0a31b715ull, 0x3c864201e2ac744cull, 0x3fef0170fc4cd831ull,
+	0x3c8fdd395dd3f84aull, 0x3feefc08b26416ffull, 0xbc86a3803b8e5b04ull, 0x3feef6c55f929ff1ull,
+	0xbc924aedcc4b5068ull, 0x3feef1a7373aa9cbull, 0xbc9907f81b512d8eull, 0x3feeecae6d05d866ull,
+	0xbc71d1e83e9436d2ull, 0x3feee7db34e59ff7ull, 0xbc991919b3ce1b15ull, 0x3feee32dc313a8e5ull,
+	0x3c859f48a72a4c6dull, 0x3feedea64c123422ull, 0xbc9312607a28698aull, 0x3feeda4504ac801cull,
+	0xbc58a78f4817895bull, 0x3feed60a21f72e2aull, 0xbc7c2c9b67499a1bull, 0x3feed1f5d950a897ull,
+	0x3c4363ed60c2ac11ull, 0x3feece086061892dull, 0x3c9666093b0664efull, 0x3feeca41ed1d0057ull,
+	0x3c6ecce1daa10379ull, 0x3feec6a2b5c13cd0ull, 0x3c93ff8e3f0f1230ull, 0x3feec32af0d7d3deull,
+	0x3c7690cebb7aafb0ull, 0x3feebfdad5362a27ull, 0x3c931dbdeb54e077ull, 0x3feebcb299fddd0dull,
+	0xbc8f94340071a38eull, 0x3feeb9b2769d2ca7ull, 0xbc87deccdc93a349ull, 0x3feeb6daa2cf6642ull,
+	0xbc78dec6bd0f385full, 0x3feeb42b569d4f82ull, 0xbc861246ec7b5cf6ull, 0x3feeb1a4ca5d920full,
+	0x3c93350518fdd78eull, 0x3feeaf4736b527daull, 0x3c7b98b72f8a9b05ull, 0x3feead12d497c7fdull,
+	0x3c9063e1e21c5409ull, 0x3feeab07dd485429ull, 0x3c34c7855019c6eaull, 0x3feea9268a5946b7ull,
+	0x3c9432e62b64c035ull, 0x3feea76f15ad2148ull, 0xbc8ce44a6199769full, 0x3feea5e1b976dc09ull,
+	0xbc8c33c53bef4da8ull, 0x3feea47eb03a5585ull, 0xbc845378892be9aeull, 0x3feea34634ccc320ull,
+	0xbc93cedd78565858ull, 0x3feea23882552225ull, 0x3c5710aa807e1964ull, 0x3feea155d44ca973ull,
+	0xbc93b3efbf5e2228ull, 0x3feea09e667f3bcdull, 0xbc6a12ad8734b982ull, 0x3feea012750bdabfull,
+	0xbc6367efb86da9eeull, 0x3fee9fb23c651a2full, 0xbc80dc3d54e08851ull, 0x3fee9f7df9519484ull,
+	0xbc781f647e5a3ecfull, 0x3fee9f75e8ec5f74ull, 0xbc86ee4ac08b7db0ull, 0x3fee9f9a48a58174ull,
+	0xbc8619321e55e68aull, 0x3fee9feb564267c9ull, 0x3c909ccb5e09d4d3ull, 0x3feea0694fde5d3full,
+	0xbc7b32dcb94da51dull, 0x3feea11473eb0187ull, 0x3c94ecfd5467c06bull, 0x3feea1ed0130c132ull,
+	0x3c65ebe1abd66c55ull, 0x3feea2f336cf4e62ull, 0xbc88a1c52fb3cf42ull, 0x3feea427543e1a12ull,
+	0xbc9369b6f13b3734ull, 0x3feea589994cce13ull, 0xbc805e843a19ff1eull, 0x3feea71a4623c7adull,
+	0xbc94d450d872576eull, 0x3feea8d99b4492edull, 0x3c90ad675b0e8a00ull, 0x3feeaac7d98a6699ull,
+	0x3c8db72fc1f0eab4ull, 0x3feeace5422aa0dbull, 0xbc65b6609cc5e7ffull, 0x3feeaf3216b5448cull,
+	0x3c7bf68359f35f44ull, 0x3feeb1ae99157736ull, 0xbc93091fa71e3d83ull, 0x3feeb45b0b91ffc6ull,
+	0xbc5da9b88b6c1e29ull, 0x3feeb737b0cdc5e5ull, 0xbc6c23f97c90b959ull, 0x3feeba44cbc8520full,
+	0xbc92434322f4f9aaull, 0x3feebd829fde4e50ull, 0xbc85ca6cd7668e4bull, 0x3feec0f170ca07baull,
+	0x3c71affc2b91ce27ull, 0x3feec49182a3f090ull, 0x3c6dd235e10a73bbull, 0x3feec86319e32323ull,
+	0xbc87c50422622263ull, 0x3feecc667b5de565ull, 0x3c8b1c86e3e231d5ull, 0x3feed09bec4a2d33ull,
+	0xbc91bbd1d3bcbb15ull, 0x3feed503b23e255dull, 0x3c90cc319cee31d2ull, 0x3feed99e1330b358ull,
+	0x3c8469846e735ab3ull, 0x3feede6b5579fdbfull, 0xbc82dfcd978e9db4ull, 0x3feee36bbfd3f37aull,
+	0x3c8c1a7792cb3387ull, 0x3feee89f995ad3adull, 0xbc907b8f4ad1d9faull, 0x3feeee07298db666ull,
+	0xbc55c3d956dcaebaull, 0x3feef3a2b84f15fbull, 0xbc90a40e3da6f640ull, 0x3feef9728de5593aull,
+	0xbc68d6f438ad9334ull, 0x3feeff76f2fb5e47ull, 0xbc91eee26b588a35ull, 0x3fef05b030a1064aull,
+	0x3c74ffd70a5fddcdull, 0x3fef0c1e904bc1d2ull, 0xbc91bdfbfa9298acull, 0x3fef12c25bd71e09ull,
+	0x3c736eae30af0cb3ull, 0x3fef199bdd85529cull, 0x3c8ee3325c9ffd94ull, 0x3fef20ab5fffd07aull,
+	0x3c84e08fd10959acull, 0x3fef27f12e57d14bull, 0x3c63cdaf384e1a67ull, 0x3fef2f6d9406e7b5ull,
+	0x3c676b2c6c921968ull, 0x3fef3720dcef9069ull, 0xbc808a1883ccb5d2ull, 0x3fef3f0b555dc3faull,
+	0xbc8fad5d3ffffa6full, 0x3fef472d4a07897cull, 0xbc900dae3875a949ull, 0x3fef4f87080d89f2ull,
+	0x3c74a385a63d07a7ull, 0x3fef5818dcfba487ull, 0xbc82919e2040220full, 0x3fef60e316c98398ull,
+	0x3c8e5a50d5c192acull, 0x3fef69e603db3285ull, 0x3c843a59ac016b4bull, 0x3fef7321f301b460ull,
+	0xbc82d52107b43e1full, 0x3fef7c97337b9b5full, 0xbc892ab93b470dc9ull, 0x3fef864614f5a129ull,
+	0x3c74b604603a88d3ull, 0x3fef902ee78b3ff6ull, 0x3c83c5ec519d7271ull, 0x3fef9a51fbc74c83ull,
+	0xbc8ff7128fd391f0ull, 0x3fefa4afa2a490daull, 0xbc8dae98e223747dull, 0x3fefaf482d8e67f1ull,
+	0x3c8ec3bc41aa2008ull, 0x3fefba1bee615a27ull, 0x3c842b94c3a9eb32ull, 0x3fefc52b376bba97ull,
+	0x3c8a64a931d185eeull, 0x3fefd0765b6e4540ull, 0xbc8e37bae43be3edull, 0x3fefdbfdad9cbe14ull,
+	0x3c77893b4d91cd9dull, 0x3fefe7c1819e90d8ull, 0x3c5305c14160cc89ull, 0x3feff3c22b8f71f1ull,
+};
+
+__device__ __forceinline__ double expSpecial(double tmp, uint64_t sbits, uint64_t ki)
+{
+	if ((ki & 0x80000000ull) == 0) {
+		// k > 0: the scale's exponent may have overflowed; scale down by 2^1009
+		const double scale = __longlong_as_double((long long)(sbits - (1009ull << 52)));
+		return 0x1p1009 * fma(scale, tmp, scale);
+	}
+	// k < 0: the result may be subnormal; round once at the final precision
+	const double scale = __longlong_as_double((long long)(sbits + (1022ull << 52)));
+	double y = scale + scale * tmp;
+	if (y < 1.0) {
+		double lo = scale - y + scale * tmp;
+		const double hi = 1.0 + y;
+		lo = 1.0 - hi + y + lo;
+		y = (hi + lo) - 1.0;
+		if (y == 0.0) y = 0.0;
+	}
+	return 0x1p-1022 * y;
+}
+
+__device__ double cbmExp(double x, const uint64_t *__restrict__ tab)
+{
+	const uint64_t ux = (uint64_t)__double_as_longlong(x);
+	uint32_t abstop = (uint32_t)(ux >> 52) & 0x7ffu;
+	if (abstop - 0x3c9u >= 0x408u - 0x3c9u) {
+		if (abstop - 0x3c9u >= 0x80000000u) return 1.0 + x;         // |x| < 2^-54
+		if (abstop >= 0x409u) {                                      // |x| >= 1024
+			if (ux == 0xfff0000000000000ull) return 0.0;             // exp(-inf)
+			if (abstop >= 0x7ffu) return 1.0 + x;                    // inf or nan
+			return (ux >> 63) ? 0.0 : __longlong_as_double(0x7ff0000000000000ll);
+		}
+		abstop = 0;  // 512 <= |x| < 1024: the rescaled paths
+	}
+	const double invLn2N = 0x1.71547652b82fep0 * 128.0, negLn2hiN = -0x1.62e42fefa0000p-8,
+		negLn2loN = -0x1.cf79abc9e3b3ap-47, shift = 0x1.8p52;
+	const double c2 = 0x1.ffffffffffdbdp-2, c3 = 0x1.555555555543cp-3, c4 = 0x1.55555cf172b91p-5,
+		c5 = 0x1.1111167a4d017p-7;
+	double kd = fma(invLn2N, x, shift);
+	const uint64_t ki = (uint64_t)__double_as_longlong(kd);
+	kd = kd - shift;
+	const double r = fma(kd, negLn2loN, fma(kd, negLn2hiN, x));
+	const uint32_t idx = 2u * (uint32_t)(ki & 127u);
+	const double tail = __longlong_as_double((long long)tab[idx]);
+	const uint64_t sbits = tab[idx + 1] + (ki << 45);
+	const double r2 = r * r;
+	const double tmp = fma(r2 * r2, fma(r, c5, c4), fma(r2, fma(r, c3, c2), tail + r));
+	if (abstop == 0) return expSpecial(tmp, sbits, ki);
+	const double scale = __longlong_as_double((long long)sbits);
+	return fma(scale, tmp, scale);
+}
+
+__global__ void expProbeKernel(const double *in, double *out, uint32_t n)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = cbmExp(in[i], kExpTab);
+}
+
 __device__ __forceinline__ uint32_t spikeBit(const uint32_t *bits, uint32_t idx)
 {
 	return (bits[idx >> 5] >> (idx & 31u)) & 1u;
-}
-
-// Zone z's PF->PC step for plasticity selector sel (1 LTD, 2 LTP) at step t:
-// the host setters' value, or for zone 0 under a device protocol the value
-// the protocol set for step t.
-__device__ __forceinline__ float plasticityStep(const DevNet *N, uint64_t t, uint32_t z, uint8_t sel)
-{
-	if (sel == 0) return 0.0f;
-	if (z == 0 && N->proto) return N->proto->ctlSlots[(t & 1) * 3 + (sel == 1 ? 0 : 1)];
-	return sel == 1 ? N->ctl->ltdStep[z] : N->ctl->ltpStep[z];
 }
 
 // Zone z's error drive at step t (setters, or the protocol for zone 0).
@@ -1028,7 +1152,7 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 			const float gGO = inDep * N->gGABAIncGOtoGO + gGO0 * N->gGABADecGOtoGO;
 			N->gMFGO[i] = gMF; N->gGRGO[i] = gGR; N->gGOGO[i] = gGO;
 			float glu = glu0;
-			glu = glu * N->gluDecayGO + totalGRIn * N->gluScaleGO * exp(-1.5 * glu);
+			glu = glu * N->gluDecayGO + totalGRIn * N->gluScaleGO * cbmExp(-1.5 * glu, kExpTab);
 			float mg = mg0;
 			mg = mg * N->mGluRDecayGO + glu * N->mGluRScaleGO * cbmExpf(-mg, sExp2);
 			float mgi = mgi0;
@@ -1122,6 +1246,7 @@ struct ZoneIn {
 	const uint32_t *mf;                 // MF spike bits of step t
 	const uint32_t *bcSum, *scSum;      // PF->BC / PF->SC counts of pass(t-2)
 	const float *pcPart[kMaxZones];     // [numPC][bs] PF->PC partial sums of pass(t-2) per zone
+	const float *pcSum[kMaxZones];      // [numPC] PF->PC input sums of pass(t-2) per zone (pcSumMode), else null
 	const uint64_t *exp2;               // cbmExpf table
 };
 
@@ -1158,7 +1283,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	for (uint32_t task = warp; task < Z * numPC; task += nWarps) {
 		const uint32_t z = task / numPC, i = task % numPC;
 		const DevZone &Q = N->zones[z];
-		const float inputSum = pcRowTree(in.pcPart[z] + (size_t)i * N->bs, N->bs, lane);
+		const float inputSum = in.pcSum[z] ? in.pcSum[z][i] : pcRowTree(in.pcPart[z] + (size_t)i * N->bs, N->bs, lane);
 		float gSCPCSum = 0;
 		for (uint32_t j0 = 0; j0 < N->numpPCfromSCtoPC; j0 += 32) {
 			const uint32_t j = j0 + lane;
@@ -1576,9 +1701,16 @@ __device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &i
 		else { src = N->scCount + (size_t)R * N->numSC + (w - e2); dst = dyn + L.sc + 4 * (w - e2); }
 		cpAsync4(dst, src);
 	}
-	// the PF->PC partial sums of every zone: 16-byte pieces when the slot
-	// is 16-byte aligned (numPC * bs a multiple of 4), else words
+	// the PF->PC input sums of every zone when the GR pass made them, else
+	// the partial sums: 16-byte pieces when the slot is 16-byte aligned
+	// (numPC * bs a multiple of 4), else words
 	for (uint32_t z = 0; z < Z; z++) {
+		if (N->pcSumMode) {
+			const float *src = N->zones[z].pcSum + (size_t)R * numPC;
+			uint8_t *dst = dyn + L.pc + 4ull * z * numPC;
+			for (uint32_t w = tid; w < numPC; w += nThr) cpAsync4(dst + 4 * w, src + w);
+			continue;
+		}
 		const float *src = N->zones[z].pcPartial + (size_t)R * nPC;
 		uint8_t *dst = dyn + L.pc + 4ull * z * nPC;
 		if ((nPC & 3u) == 0)
@@ -1591,8 +1723,11 @@ __device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &i
 		in.mf = reinterpret_cast<const uint32_t *>(dyn + L.mf);
 		in.bcSum = reinterpret_cast<const uint32_t *>(dyn + L.bc);
 		in.scSum = reinterpret_cast<const uint32_t *>(dyn + L.sc);
-		for (uint32_t z = 0; z < kMaxZones; z++)
+		for (uint32_t z = 0; z < kMaxZones; z++) {
 			in.pcPart[z] = reinterpret_cast<const float *>(dyn + L.pc) + (size_t)(z < Z ? z : 0) * nPC;
+			in.pcSum[z] = N->pcSumMode ? reinterpret_cast<const float *>(dyn + L.pc) + (size_t)(z < Z ? z : 0) * numPC
+				: nullptr;
+		}
 		in.exp2 = reinterpret_cast<const uint64_t *>(dyn + L.exp2);
 	}
 }
@@ -1615,6 +1750,28 @@ __device__ void stageOut(const DevNet *N, const uint8_t *base, const DevNet *sNe
 // 175-194), and zone 0's error drive and PF->PC plasticity steps for step
 // t+1 (ECManagementDelay::calcSimActivity, ecmanagementdelay.cpp:201-235).
 // The draw of MF i for step t+1 is keyed by ((t+1) << 20) | i.
+// Rate of fibre i under the state-variable coding at row `row` of the
+// environment's values: gaussMFAct (statevariable.hpp:108-129) in its float
+// and double steps.
+__device__ __forceinline__ float stateVarRate(const DevProtocol *P, uint32_t i, uint64_t row)
+{
+	const uint32_t v = i / P->svPer;
+	if (v >= P->svVars) return P->svRelaxed[i];
+	float x = P->svValues[row * P->svVars + v];
+	x = fmaxf(P->svLo, fminf(P->svHi, x));
+	const float d = x - P->svMean[i];
+	const float arg = (-(d * d)) / P->svDen;
+	const float value = (float)(cbmExp((double)arg, kExpTab) / P->svNorm);
+	const float a = value / P->svMaxPossible;
+	return a * P->svExcited[i] + (1.0f - a) * P->svRelaxed[i];
+}
+
+__global__ void stateVarRatesKernel(const DevNet *N, uint64_t row, float *out)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < N->numMF) out[i] = stateVarRate(N->proto, i, row % N->proto->svSteps);
+}
+
 __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 {
 	DevProtocol *P = N->proto;
@@ -1632,7 +1789,7 @@ __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 		uint32_t ap = 0;
 		if (i < numMF) {
 			float th = P->mfThresh[i];
-			const float f = freq[i];
+			const float f = P->svValues ? stateVarRate(P, i, k % P->svSteps) : freq[i];
 			th = th + (1 - th) * P->mfThreshDecay;
 			const double u = (double)rng::uniform24Keyed(P->mfKey, ctr | i);
 			ap = u < ((f * P->sPerTS) * th);
@@ -1873,8 +2030,11 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 				in.mf = sMF;
 				in.bcSum = N->bcCount + (size_t)R * N->numBC;
 				in.scSum = N->scCount + (size_t)R * N->numSC;
-				for (uint32_t z = 0; z < kMaxZones; z++)
-					in.pcPart[z] = N->zones[z < N->numZones ? z : 0].pcPartial + (size_t)R * N->numPC * N->bs;
+				for (uint32_t z = 0; z < kMaxZones; z++) {
+					const DevZone &Q = N->zones[z < N->numZones ? z : 0];
+					in.pcPart[z] = Q.pcPartial + (size_t)R * N->numPC * N->bs;
+					in.pcSum[z] = N->pcSumMode ? Q.pcSum + (size_t)R * N->numPC : nullptr;
+				}
 				in.exp2 = sExp2;
 			}
 			__syncthreads();

@@ -26,6 +26,22 @@ void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M);
 // unit), S stages, B resident CTAs per SM, slot bound M; grid of any size,
 // 32 * (W + 1) threads, the grPassKernel arguments with one network.
 const void *passPersistentKernelFor(int W, int S, int B, int M);
+// Vector GR pass (cbm_pass_vec.cu): single network of the compiled shape,
+// kVecWarps warps per CTA, persistent grid, arguments (descriptor,
+// stepOffset), passVecSmemBytes of dynamic shared memory.  Units of
+// kVecClaim x 128 cells are claimed from DevNet::passClaim.
+constexpr int kVecWarps = 8;
+constexpr int kVecMinBlocks = 3;
+constexpr uint32_t kVecClaim = 2;
+bool passVecCapable(const DevNet &h);
+size_t passVecSmemBytes(const DevNet &h);
+const void *passVecKernel();
+// pairReduceKernel(N, t): step t's PF->PC running sums from its pair sums
+// (numPC * bs threads), for a switch away from the vector pass.
+const void *pairReduceKernelFn();
+// pcTreeKernel(N, t): step t's PF->PC input sums (pcSum) from its partial
+// sums, one block of 256 threads per PC, for a switch to the vector pass.
+const void *pcTreeKernelFn();
 // Small-cell update; stageBytes[n] is network n's staging block size (0:
 // its microzone CTA works on global memory).  With one network, net0 and
 // stage0 give its descriptor and staging size directly (else null, 0).
@@ -39,5 +55,8 @@ __global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);
 __global__ void expfProbeKernel(const float *in, float *out, uint32_t n);
+__global__ void expProbeKernel(const double *in, double *out, uint32_t n);
+// The state-variable input's MF rates for row `row` of its values.
+__global__ void stateVarRatesKernel(const DevNet *N, uint64_t row, float *out);
 
 }  // namespace cbm

@@ -154,8 +154,38 @@ std::string Network::buildPassMaps(uint32_t R)
 	if (!d) return "device allocation failed";
 	CK(cudaMemcpy(d, maps.data(), PM_COUNT * sizeof(CUtensorMap), cudaMemcpyHostToDevice), "uploading TMA descriptors");
 	h_.passMaps = d;
+	return uploadDesc();
+}
+
+std::string Network::uploadDesc()
+{
 	CK(cudaMemcpy(dNet_.ptr, &h_, sizeof(DevNet), cudaMemcpyHostToDevice), "uploading the network descriptor");
 	return "";
+}
+
+std::string Network::setPcSumMode(bool on, cudaStream_t s)
+{
+	if ((h_.pcSumMode != 0) == on) return "";
+	const uint64_t T = hostT_;
+	const DevNet *np = devPtr();
+	if (on) {
+		// the small-cell update of the next two steps reads the sums of steps
+		// T-1 and T, which the pass before made as partial sums
+		for (uint64_t st = T > 0 ? T - 1 : 0; T > 0 && st <= T; st++) {
+			uint64_t a = st;
+			void *args[] = {&np, &a};
+			CK(cudaLaunchKernel(pcTreeKernelFn(), dim3(h_.numPC), dim3(256), args, 0, s), "PF->PC input sums");
+		}
+	} else if (T > 0) {
+		// the vector pass left step T's reduction as pair sums
+		uint64_t a = T;
+		void *args[] = {&np, &a};
+		const uint32_t seqs = h_.numPC * h_.bs;
+		CK(cudaLaunchKernel(pairReduceKernelFn(), dim3((seqs + 255) / 256), dim3(256), args, 0, s), "PF->PC pair sums");
+	}
+	CK(cudaStreamSynchronize(s), "PF->PC sums");
+	h_.pcSumMode = on ? 1u : 0u;
+	return uploadDesc();
 }
 
 // Arrays the microzone CTA stages in shared memory for each step: its
@@ -595,6 +625,7 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 		Q.w = upF("pfSynWeightPC", z);
 		Q.pcPartial = alloc<float>((size_t)3 * c.numPC * h.bs);
 		Q.pairSum = alloc<float>((size_t)2 * c.numPC * h.K * h.bs);
+		Q.pcSum = alloc<float>((size_t)3 * c.numPC);
 		Q.plastSel = alloc<uint8_t>((size_t)2 * c.numIO);
 		std::vector<uint32_t> ioOfPC(c.numPC);
 		uint32_t cur = 0;
@@ -662,6 +693,8 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	ctlDirty = true;
 
 	// ---- pipeline and control
+	h.pairStep = alloc<uint64_t>(2);
+	h.passClaim = alloc<uint32_t>(4);
 	h.goCount = alloc<uint32_t>((size_t)2 * c.numGO);
 	h.bcCount = alloc<uint32_t>((size_t)3 * c.numBC);
 	h.scCount = alloc<uint32_t>((size_t)3 * c.numSC);
@@ -713,7 +746,53 @@ void Network::setErrDrive(uint32_t z, float rel) { ctl.errDrive[z] = rel * st_->
 void Network::setGIncGRtoGO(float v) { ctl.gIncGRtoGO = v; ctlDirty = true; }
 void Network::resetGIncGRtoGO() { ctl.gIncGRtoGO = st_->ap.gIncGRtoGO; ctlDirty = true; }
 
-std::string Network::setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s)
+std::string Network::setStateVarInput(const cbm_statevar_input &in, cudaStream_t s)
+{
+	const ConParams &c = st_->cp;
+	if (!in.mean || !in.relaxed || !in.excited || !in.values) return "state-variable input: a table is missing";
+	if (in.numVars == 0 || in.fibresPerVar == 0 || in.numSteps == 0) return "state-variable input: empty coding";
+	if (!(in.den > 0) || !(in.norm > 0) || !(in.lo <= in.hi)) return "state-variable input: bad width or range";
+	// an eyelid protocol with no CS trial, no US and no kept trial: the MF
+	// generator alone, fed by the coding
+	cbm_eyelid_protocol p{};
+	p.trialSteps = 1u << 30;
+	p.csOn = p.csOff = p.csPhasicOff = 0;
+	p.csStartTrial = 0xFFFFFFFFu;
+	p.mfSeed = in.mfSeed;
+	p.mfThreshDecayTau = in.mfThreshDecayTau;
+	p.mfFreqBG = p.mfFreqCSTonic = p.mfFreqCSPhasic = in.relaxed;
+	p.numDataTrials = 0;
+	p.postCS = 1;
+	p.binSteps = 1;
+	p.eyeGDecayTau = 10.5f; p.eyeGInc = 0.012f; p.eyeGShift = -0.13f; p.eyeGLeakRaw = 0.13f; p.eyeMaxAmp = 100.0f;
+	DevProtocol sv{};
+	sv.svMean = upload(in.mean, c.numMF);
+	sv.svRelaxed = upload(in.relaxed, c.numMF);
+	sv.svExcited = upload(in.excited, c.numMF);
+	sv.svValues = upload(in.values, (size_t)in.numSteps * in.numVars);
+	if (!sv.svMean || !sv.svRelaxed || !sv.svExcited || !sv.svValues) return "device allocation failed";
+	sv.svSteps = in.numSteps;
+	sv.svVars = in.numVars; sv.svPer = in.fibresPerVar;
+	sv.svLo = in.lo; sv.svHi = in.hi; sv.svDen = in.den; sv.svMaxPossible = in.maxPossible;
+	sv.svNorm = in.norm;
+	return setProtocol(p, s, &sv);
+}
+
+std::string Network::stateVarRates(uint64_t row, float *out, cudaStream_t s)
+{
+	if (!h_.proto || !hProto_.svValues) return "no state-variable input is running";
+	float *d = nullptr;
+	CK(cudaMalloc(&d, 4ull * h_.numMF), "rates buffer");
+	stateVarRatesKernel<<<(h_.numMF + 255) / 256, 256, 0, s>>>(devPtr(), row, d);
+	cudaError_t e = cudaGetLastError();
+	if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 4ull * h_.numMF, cudaMemcpyDeviceToHost, s);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+	cudaFree(d);
+	CK(e, "state-variable rates");
+	return "";
+}
+
+std::string Network::setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s, const DevProtocol *sv)
 {
 	const ConParams &c = st_->cp;
 	const ActParams &a = st_->ap;
@@ -786,6 +865,12 @@ std::string Network::setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s)
 	d.eyeGShift = p.eyeGShift;
 	d.eyeGLeak = p.eyeGLeakRaw / (6 - eyeMS);
 	d.eyeMaxAmp = p.eyeMaxAmp;
+	if (sv) {
+		d.svMean = sv->svMean; d.svRelaxed = sv->svRelaxed; d.svExcited = sv->svExcited; d.svValues = sv->svValues;
+		d.svSteps = sv->svSteps; d.svVars = sv->svVars; d.svPer = sv->svPer;
+		d.svLo = sv->svLo; d.svHi = sv->svHi; d.svDen = sv->svDen; d.svMaxPossible = sv->svMaxPossible;
+		d.svNorm = sv->svNorm;
+	}
 	for (void *q : {(void *)d.freqBG, (void *)d.freqCSTonic, (void *)d.freqCSPhasic, (void *)d.mfThresh,
 			(void *)d.plastState, (void *)d.curSteps, (void *)d.ctlSlots, (void *)d.ncPSH, (void *)d.pcPSH, (void *)d.eyelid, (void *)d.eyeG, (void *)d.eyeVm})
 		if (!q) return "device allocation failed";
@@ -1169,6 +1254,14 @@ std::vector<PassGeometry> Simulator::passCandidates() const
 	// the default first: 4 consumer warps of 1 row, 4 stages, 4 CTAs/SM,
 	// slot loops for at most 4 slots (8,1,3,2 with open slot loops past 4)
 	std::vector<PassGeometry> out;
+	// the vector pass first where it applies (single network of the compiled
+	// shape); CBM_PASS_VEC=0 leaves it out
+	const char *vecEnv = getenv("CBM_PASS_VEC");
+	if (nets_.size() == 1 && passVecCapable(nets_[0]->dev()) && !(vecEnv && !strcmp(vecEnv, "0"))) {
+		PassGeometry v;
+		v.kind = 3;
+		out.push_back(v);
+	}
 	bool tma = !nets_.empty();
 	uint32_t minRows = UINT32_MAX, maxSlots = 0;
 	for (Network *n : nets_) {
@@ -1210,6 +1303,36 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 		maxSlotsTile = std::max({maxSlotsTile, n->dev().nMFSlots, n->dev().nGOSlots, n->dev().nOutTma});
 	}
 	for (Network *n : nets_) { n->outBytes_ = 4; n->outPlanes_ = n->dev().nOutSlots; n->ovUsed_ = 0; }
+	// leaving the vector pass: the last step's PF->PC reduction is still pair
+	// sums, and the small-cell update goes back to partial sums
+	if (passVec_ && g.kind != 3 && nets_.size() == 1) CKS(nets_[0]->setPcSumMode(false, s0_));
+	if (g.kind == 3) {
+		if (nets_.size() != 1 || !passVecCapable(nets_[0]->dev()))
+			return "the vector GR pass runs one network of its compiled shape";
+		Network &n = *nets_[0];
+		const size_t smem = passVecSmemBytes(n.dev());
+		const void *fn = passVecKernel();
+		CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "pass smem");
+		int perSM = 0, numSMs = 0;
+		CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, 32 * kVecWarps, smem), "pass occupancy");
+		CK(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device_), "SM count");
+		const uint32_t claims = (n.dev().numGR / 128u + kVecClaim - 1) / kVecClaim;
+		passGrid_ = std::max<uint32_t>(1, std::min<uint32_t>((claims + kVecWarps - 1) / kVecWarps,
+				(uint32_t)std::max(1, perSM) * (uint32_t)numSMs));
+		// claim counters from zero (another pass kind may have run meanwhile)
+		CK(cudaMemset(n.dev().passClaim, 0, 4 * sizeof(uint32_t)), "pass claim counters");
+		CKS(n.setPcSumMode(true, s0_));
+		passTmaFn_ = fn;
+		passVec_ = true;
+		passPersistent_ = false;
+		passTmaW_ = kVecWarps - 1;  // launchPass's block is 32 * (W + 1) threads
+		passTmaR_ = passTmaS_ = 0;
+		passTmaSmem_ = smem;
+		passGeom_ = g;
+		dropGraphs();
+		return "";
+	}
+	passVec_ = false;
 	if (g.kind == 0) {
 		passTmaFn_ = nullptr;
 		passPersistent_ = false;
@@ -1303,8 +1426,11 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	const uint32_t stage0Arg = nets_.size() == 1 ? nets_[0]->stageBytes() : 0u;
 	auto launchPass = [&](cudaStream_t st, bool dependent) -> std::string {
 		if (passTmaFn_) {
-			// the per-tile pass takes the single network's descriptor too
-			void *args[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg};
+			// the per-tile pass takes the single network's descriptor too; the
+			// vector pass takes it alone
+			void *argsTma[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg};
+			void *argsVec[] = {&net0Arg, &stepArg};
+			void **args = passVec_ ? argsVec : argsTma;
 			cudaLaunchConfig_t cfg = {};
 			cfg.gridDim = dim3(passGrid_);
 			cfg.blockDim = dim3(32 * (passTmaW_ + 1));
@@ -1452,6 +1578,16 @@ std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
 	CKS(uploadCtl());
 	CK(cudaStreamSynchronize(s0_), "sync");
 	return nets_[i]->setProtocol(p, s0_);
+}
+
+std::string Simulator::setStateVarInput(size_t i, const cbm_statevar_input &in)
+{
+	CK(cudaSetDevice(device_), "selecting the device");
+	lastWasStepGraph_ = false;
+	pendingMF_ = -1;  // the coding drives the MF input from now on
+	CKS(uploadCtl());
+	CK(cudaStreamSynchronize(s0_), "sync");
+	return nets_[i]->setStateVarInput(in, s0_);
 }
 
 std::string Simulator::recordGR()

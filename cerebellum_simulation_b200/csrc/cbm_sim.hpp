@@ -42,7 +42,8 @@ std::string checkNetwork(const State &st);
 constexpr uint32_t kMFStage = 8;
 
 // A GR-pass kernel choice: kind 0 plain, 1 per-tile TMA (W consumer warps of
-// RW rows, S stages, B CTAs/SM, slot bound M), 2 persistent TMA (W, S, B, M).
+// RW rows, S stages, B CTAs/SM, slot bound M), 2 persistent TMA (W, S, B, M),
+// 3 vector (cbm_pass_vec.cu; no parameters).
 struct PassGeometry {
 	int kind = 0, W = 0, RW = 1, S = 0, B = 0, M = 0;
 };
@@ -63,6 +64,8 @@ public:
 	std::string stageMF(size_t i, const uint8_t *mf);
 	// Start a device-driven trial protocol on network i from the next step.
 	std::string setProtocol(size_t i, const cbm_eyelid_protocol &p);
+	// Start the state-variable MF input (cbm_statevar_input) on network i.
+	std::string setStateVarInput(size_t i, const cbm_statevar_input &in);
 	// Record network 0's GR peri-stimulus histogram (single-network simulators).
 	std::string recordGR();
 	std::string recordTrialData();
@@ -100,7 +103,7 @@ public:
 	std::string checkDeviceErrors();
 	void passGeometry(unsigned *kind, unsigned *warps, unsigned *rows, unsigned *stages) const
 	{
-		*kind = passTmaFn_ ? (passPersistent_ ? 2u : 1u) : 0u;
+		*kind = passVec_ ? 3u : passTmaFn_ ? (passPersistent_ ? 2u : 1u) : 0u;
 		*warps = passTmaW_;
 		*rows = passTmaR_;
 		*stages = passTmaS_;
@@ -141,6 +144,7 @@ private:
 	const void *passTmaFn_ = nullptr;
 	uint32_t passTmaW_ = 0, passTmaR_ = 0, passTmaS_ = 0, passGrid_ = 0;
 	bool passPersistent_ = false;
+	bool passVec_ = false;  // the vector pass (kind 3) runs
 	PassGeometry passGeom_;
 	size_t passTmaSmem_ = 0;
 	cudaGraphExec_t graphExec_ = nullptr;
@@ -173,7 +177,10 @@ public:
 	// live state (innetactivitystate.cpp:247-248); mirrored on the device.
 	std::string resetGOGODepression(cudaStream_t s);
 	// Device-driven trial protocol (cbm_eyelid_protocol) from the next step on.
-	std::string setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s);
+	// sv: the state-variable coding's fields of the protocol descriptor, or null
+	std::string setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s, const DevProtocol *sv = nullptr);
+	std::string setStateVarInput(const cbm_statevar_input &in, cudaStream_t s);
+	std::string stateVarRates(uint64_t row, float *out, cudaStream_t s);
 	// Allocate and start the protocol's GR peri-stimulus histogram.
 	std::string recordGR(cudaStream_t s);
 	bool recordsGR() const { return hProto_.grPSH != nullptr; }
@@ -195,6 +202,11 @@ public:
 	// bytes of the staging block the microzone CTA copies, 0 when not staged
 	uint32_t stageBytes() const { return h_.numZoneSegs ? h_.zoneStageBytes : 0; }
 	// TMA GR pass: possible when every row of the reduction tile is 32 cells
+	// Re-upload the host copy of the descriptor (h_) to the device.
+	std::string uploadDesc();
+	// Switch the small-cell update between pass-made PF->PC input sums (the
+	// vector pass) and partial sums, converting the last steps' buffers.
+	std::string setPcSumMode(bool on, cudaStream_t s);
 	bool passTmaCapable() const { return h_.J == 32; }
 	uint32_t passRows() const { return 2 * h_.K; }
 	// Encode the TMA descriptors for boxes of R rows and upload them.

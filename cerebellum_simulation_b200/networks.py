@@ -360,6 +360,12 @@ class StateVariableMF:
         """[num_mf] Hz at step t of the synthetic trajectory."""
         return self.rates_for(self.values(t))
 
+    def trajectory(self, steps):
+        """The synthetic trajectory's values for steps 1..steps, [steps,
+        n_vars]: the rows a device state-variable input takes step by step
+        (CBMSimCore.set_statevar_input)."""
+        return np.stack([self.values(t) for t in range(1, steps + 1)]).astype(np.float32)
+
 
 def config3_mf_stream(num_mf, steps, seed=0):
     """MF spikes of the dense 4M configuration: regenerating Poisson fibres

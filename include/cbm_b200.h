@@ -293,6 +293,42 @@ enum {
 /* Start a device protocol on network 0 of the simulator (no counterpart in
  * the reference's core library: it replaces the eyelid driver's per-step calls). */
 int cbm_sim_set_eyelid_protocol(cbm_sim *sim, const cbm_eyelid_protocol *protocol);
+/* State-variable MF input on the device: the mossy fibres of network 0 code
+ * the state of an environment (the cart-pole driver's MF input,
+ * Matthew_Sim_CBM/includes/statevariable.hpp:108-129 with the fibre
+ * assignment of :35-43 and the rates of environment.cpp:19-39) and fire as
+ * the reference's regenerating Poisson cells (poissonregencells.cpp:49-66),
+ * all generated on the device from the next step on.  Fibre i codes
+ * variable v = i / fibresPerVar (fibres past numVars * fibresPerVar stay at
+ * their relaxed rate) at
+ *   x = clamp(value of v, lo, hi), d = x - mean[i] (float),
+ *   a = (float)(exp((double)(-(d*d) / den)) / norm) / maxPossible,
+ *   rate = a * excited[i] + (1 - a) * relaxed[i]    (float),
+ * gaussMFAct's arithmetic, with the C library's double exp.  The values of
+ * the environment's state come from `values`, one row of numVars floats per
+ * step, used cyclically; the fibres' draws are keyed as the eyelid
+ * protocol's (mfSeed).  No CS, US, plasticity window or trial records: the
+ * setters keep their values.  No counterpart in the reference's core
+ * library (it replaces the driver's per-step MF update). */
+typedef struct cbm_statevar_input {
+	uint32_t numVars, fibresPerVar;
+	float lo, hi;                 /* range of every variable */
+	float den;                    /* 2 width^2, width = gaussWidth x the fibres' spacing */
+	double norm;                  /* sqrt(2 pi width^2) */
+	float maxPossible;            /* (float)(1 / norm) */
+	const float *mean;            /* numMF preferred values, host memory */
+	const float *relaxed, *excited;  /* numMF Hz each, host memory */
+	const float *values;          /* [numSteps][numVars], host memory */
+	uint64_t numSteps;
+	int32_t mfSeed;
+	float mfThreshDecayTau;       /* ms (4) */
+} cbm_statevar_input;
+int cbm_sim_set_statevar_input(cbm_sim *sim, const cbm_statevar_input *input);
+/* The MF rates (Hz, numMF floats into out) the running state-variable
+ * input gives for row `step` of its values, computed on the device by the
+ * same function the generator uses.  No counterpart in the reference. */
+int cbm_sim_statevar_rates(cbm_sim *sim, uint64_t step, float *out);
+
 /* Size in bytes of a record of the running protocol (0 without one). */
 uint64_t cbm_sim_trial_record_bytes(cbm_sim *sim, int kind);
 /* Copy a record of the running protocol to host memory. */
@@ -405,6 +441,12 @@ int cbm_pfpc_sums_noalloc(const uint32_t *apBuf, const uint32_t *pfDelayMask, co
  * (the published expf algorithm glibc ships), for checking it against the
  * host's expf: out[i] = exp(in[i]) for n values in host memory. */
 int cbm_device_expf(int device, const float *in, float *out, uint64_t n);
+
+/* Device evaluation of the double exponential the GO glutamate update and
+ * the state-variable MF coding use (the published exp algorithm glibc
+ * ships), for checking it against the host's exp: out[i] = exp(in[i]) for
+ * n values in host memory. */
+int cbm_device_exp(int device, const double *in, double *out, uint64_t n);
 
 #ifdef __cplusplus
 }

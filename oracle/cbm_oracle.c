@@ -1495,8 +1495,25 @@ static void trial_data_step(const cbm_oracle *o, const cbm_oracle_protocol *p, c
 	}
 }
 
+static void run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, const float *stepRates,
+		uint64_t rateRows, uint64_t nsteps, uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid,
+		float *psh, uint32_t *raster);
+
 void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, uint64_t nsteps,
 		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid, float *psh, uint32_t *raster)
+{
+	run_protocol(o, p, rates, NULL, 0, nsteps, trace, ncPSH, pcPSH, eyelid, psh, raster);
+}
+
+void cbm_oracle_run_protocol_step_rates(cbm_oracle *o, const cbm_oracle_protocol *p, const float *stepRates,
+		uint64_t rateRows, uint64_t nsteps, uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid)
+{
+	run_protocol(o, p, stepRates, stepRates, rateRows, nsteps, trace, ncPSH, pcPSH, eyelid, NULL, NULL);
+}
+
+static void run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, const float *stepRates,
+		uint64_t rateRows, uint64_t nsteps, uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid,
+		float *psh, uint32_t *raster)
 {
 	const uint32_t numMF = o->numMF, numNC = o->numNC, numPC = o->numPC;
 	const float *freqBG = rates, *freqCST = rates + numMF, *freqCSP = rates + 2 * (size_t)numMF;
@@ -1538,6 +1555,7 @@ void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const 
 		/* calcMFActivity (ecmanagementdelay.cpp:175-194) */
 		const float *freq = freqBG;
 		if (csTrial && time >= p->csOn && time < p->csOff) freq = time < p->csPhasicOff ? freqCSP : freqCST;
+		if (stepRates) freq = stepRates + (s % rateRows) * numMF;
 		for (uint32_t i = 0; i < numMF; i++)
 		{
 			thresh[i] = thresh[i] + (1 - thresh[i]) * threshDecay;
@@ -1587,6 +1605,12 @@ void cbm_oracle_expf_array(const float *in, float *out, uint64_t n)
 {
 	/* the host C library's expf, which the reference's exp(float) calls use */
 	for (uint64_t i = 0; i < n; i++) out[i] = expf(in[i]);
+}
+
+void cbm_oracle_exp_array(const double *in, double *out, uint64_t n)
+{
+	/* the host C library's exp, which the reference's exp(double) calls use */
+	for (uint64_t i = 0; i < n; i++) out[i] = exp(in[i]);
 }
 
 uint32_t cbm_oracle_num(const cbm_oracle *o, const char *w)

@@ -63,6 +63,8 @@ int cbm_oracle_save(cbm_oracle *o, const char *path);
 
 /* out[i] = the host C library's expf(in[i]) (the reference's exp(float)). */
 void cbm_oracle_expf_array(const float *in, float *out, uint64_t n);
+/* out[i] = the host C library's exp(in[i]) (the reference's exp(double)). */
+void cbm_oracle_exp_array(const double *in, double *out, uint64_t n);
 
 /* The eyelid-conditioning driver (ECManagementDelay::calcMFActivity and
  * calcSimActivity, Eyelid_Sim_CBM_Dev/src/ectrial/ecmanagementdelay.cpp:
@@ -96,6 +98,14 @@ void cbm_oracle_trial_data_sizes(const cbm_oracle *o, const cbm_oracle_protocol 
 /* psh and raster (either may be NULL) receive the trial-data records. */
 void cbm_oracle_run_protocol(cbm_oracle *o, const cbm_oracle_protocol *p, const float *rates, uint64_t nsteps,
 		uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid, float *psh, uint32_t *raster);
+
+/* The same driver with the MF rates of step s (0-based within the run)
+ * taken from row s % rateRows of stepRates ([rateRows][numMF] Hz) instead
+ * of the protocol's three tables: the state-variable MF input, whose rates
+ * the caller computes from the environment's values (gaussMFAct,
+ * Matthew_Sim_CBM/includes/statevariable.hpp:108-129). */
+void cbm_oracle_run_protocol_step_rates(cbm_oracle *o, const cbm_oracle_protocol *p, const float *stepRates,
+		uint64_t rateRows, uint64_t nsteps, uint8_t *trace, uint32_t *ncPSH, uint32_t *pcPSH, float *eyelid);
 
 /* Sizes, for callers sizing buffers. */
 uint32_t cbm_oracle_num(const cbm_oracle *o, const char *what);

@@ -55,6 +55,7 @@ class Oracle:
             lib.cbm_oracle_protocol_sizes.argtypes = [P, P, P, P, P]
             lib.cbm_oracle_run_protocol.argtypes = [P, P, P, ctypes.c_uint64, P, P, P, P, P, P]
             lib.cbm_oracle_trial_data_sizes.argtypes = [P, P, P, P]
+            lib.cbm_oracle_run_protocol_step_rates.argtypes = [P, P, P, ctypes.c_uint64, ctypes.c_uint64, P, P, P, P]
             cls._lib = lib
         return cls._lib
 
@@ -128,6 +129,20 @@ class Oracle:
             return tr, nc, pc, eye, split_trial_data(psh, raster, self.num, proto)
         return tr, nc, pc, eye
 
+    def run_protocol_step_rates(self, proto, step_rates, nsteps):
+        """The eyelid driver with the MF rates of step s from row s % rows of
+        step_rates [rows, numMF] (cbm_oracle_run_protocol_step_rates)."""
+        lib = self.lib()
+        p = ProtocolStruct.from_dict(proto)
+        sizes = [ctypes.c_uint64() for _ in range(3)]
+        lib.cbm_oracle_protocol_sizes(self.h, ctypes.byref(p), *[ctypes.byref(x) for x in sizes])
+        nc = np.zeros(sizes[0].value, dtype=np.uint32)
+        pc = np.zeros(sizes[1].value, dtype=np.uint32)
+        eye = np.zeros(sizes[2].value, dtype=np.float32)
+        rates = np.ascontiguousarray(step_rates, dtype=np.float32)
+        lib.cbm_oracle_run_protocol_step_rates(self.h, ctypes.byref(p), rates.ctypes.data, rates.shape[0], nsteps,
+                                               None, nc.ctypes.data, pc.ctypes.data, eye.ctypes.data)
+
     def save(self, path):
         if self.lib().cbm_oracle_save(self.h, os.fsencode(path)) != 0:
             raise RuntimeError("oracle save failed")
@@ -191,6 +206,16 @@ def short_protocol(**kw):
              eyeGInc=0.012, eyeGShift=-0.13, eyeGLeakRaw=0.13, eyeMaxAmp=100.0)
     p.update(kw)
     return p
+
+
+def statevar_protocol(mf_seed, tau=4.0):
+    """The eyelid-driver fields a device state-variable input runs with
+    (cbm_sim_set_statevar_input): no CS trial, no US, no plasticity window,
+    no kept trial; the MF generator's seed and time constant."""
+    return dict(trialSteps=1 << 30, csOn=0, csOff=0, csPhasicOff=0, csStartTrial=0xFFFFFFFF, plastOnDelay=0,
+                plastOffDelay=0, plastLTD=0.0, plastLTP=0.0, usErrDrive=0.0, mfSeed=mf_seed, mfThreshDecayTau=tau,
+                dataStartTrial=0, numDataTrials=0, preCS=0, postCS=1, binSteps=1, eyeGDecayTau=10.5, eyeGInc=0.012,
+                eyeGShift=-0.13, eyeGLeakRaw=0.13, eyeMaxAmp=100.0)
 
 
 def protocol_rates(num_mf, seed=0):

@@ -277,3 +277,26 @@ def test_oracle_built_network_equals_the_products(tmp_path, config):
     fn(seed=5).writeState(str(a))
     fn(seed=5, new_state=OracleState.new).writeState(str(b))
     assert filecmp.cmp(a, b, shallow=False)
+
+
+def test_device_exp_table_is_the_mathematical_one():
+    """kExpTab of the device's double exp holds, for k < 128, the tail
+    (2^(k/128) - H) / H and asuint64(H) - (k << 45), with H = 2^(k/128)
+    rounded to the nearest double: regenerated here at 80-digit precision
+    and compared entry by entry with the table in the kernel source."""
+    import struct
+    from decimal import Decimal, getcontext
+    src = open(os.path.join(ROOT, "cerebellum_simulation_b200", "csrc", "cbm_kernels.cu")).read()
+    body = src[src.index("kExpTab[256] = {"):]
+    body = body[body.index("{") + 1: body.index("};")]
+    got = [int(v, 16) for v in re.findall(r"0x([0-9a-f]+)ull", body)]
+    assert len(got) == 256
+    getcontext().prec = 80
+    ln2 = Decimal(2).ln()
+    for k in range(128):
+        v = (ln2 * k / 128).exp()
+        h = float(v)
+        tail = float((v - Decimal(h)) / Decimal(h))
+        hb = struct.unpack("<Q", struct.pack("<d", h))[0]
+        tb = struct.unpack("<Q", struct.pack("<d", tail))[0]
+        assert got[2 * k] == tb and got[2 * k + 1] == (hb - (k << 45)) % 2 ** 64, k

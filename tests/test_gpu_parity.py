@@ -224,6 +224,31 @@ def test_flushed_runs_equal_graph_runs(tmp_path):
     assert open(fa, "rb").read() == open(fb, "rb").read()
 
 
+def test_device_exp_matches_host_exp():
+    """The double exponential of the GO glutamate update and the
+    state-variable MF coding equals the host C library's exp (the
+    reference's exp(double)) on every probed input: the whole finite range,
+    the range the Gaussian coding and the glutamate term use, arguments
+    whose results are subnormal, and the special values."""
+    import ctypes
+    import cerebellum_simulation_b200 as cbm
+    rng = np.random.default_rng(1)
+    x = np.concatenate([
+        rng.uniform(-745, 710, 3_000_000), rng.uniform(-40, 0, 3_000_000), rng.uniform(-1, 1, 1_000_000),
+        rng.uniform(-760, -700, 500_000), rng.uniform(-1e-12, 1e-12, 100_000),
+        (rng.integers(0, 2**63, 1_000_000, dtype=np.uint64) | (rng.integers(0, 2, 1_000_000, dtype=np.uint64) << 63)
+         ).view(np.float64),
+        np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 709.78, 709.79, -745.13, -745.14, -708.4, 512.0, -512.0,
+                  1024.0, -1024.0, 2.0 ** -60, -2.0 ** -60])])
+    dev = cbm.device_exp(x)
+    lib = Oracle.lib()
+    lib.cbm_oracle_exp_array.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
+    host = np.empty_like(x)
+    lib.cbm_oracle_exp_array(x.ctypes.data, host.ctypes.data, x.size)
+    same = (dev.view(np.uint64) == host.view(np.uint64)) | (np.isnan(dev) & np.isnan(host))
+    assert same.all(), f"{int((~same).sum())} mismatches, first at x={x[~same][0]!r}"
+
+
 def test_device_expf_matches_host_expf():
     """The small-cell updates' float exponential equals the host C library's
     expf (the reference's exp(float)) on every probed input."""

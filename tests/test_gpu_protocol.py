@@ -236,3 +236,57 @@ def test_config2_1m_full_trial_bit_exact(tmp_path):
     w1 = cbm.CBMState(fin_p).array("pfSynWeightPC", 0)
     assert (w1 < w0).sum() > 0 and (w1 > w0).sum() > 0, "no PF->PC weight moved both ways"
     assert o_pc.sum() > 0
+
+
+def test_statevar_rates_match_host_coding(tmp_path):
+    """The device's state-variable MF coding (cbm_sim_set_statevar_input)
+    gives, row by row, the rates of networks.StateVariableMF (pinned to the
+    reference's StateVariable::gaussMFAct in test_oracle_pin.py) bit for bit:
+    the benchmark's coding (width 0.2 of the range) and a narrow one whose
+    Gaussian underflows far from a fibre's preferred value, with values that
+    leave the range (clamped)."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    st = networks.config1_network(seed=2)
+    p = str(tmp_path / "c1.state")
+    st.writeState(p)
+    sim = cbm.CBMSimCore(cbm.CBMState(p), [7], device=0)
+    for coding in (networks.StateVariableMF(1024, seed=3), networks.StateVariableMF(1024, seed=4, gauss_width=0.05)):
+        vals = coding.trajectory(1500)
+        vals[::97] *= 1.3  # some rows outside [lo, hi]
+        sim.set_statevar_input(coding, vals, mfSeed=9)
+        for r in range(0, vals.shape[0], 7):
+            got = sim.statevar_rates(r)
+            want = coding.rates_for(vals[r])
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"row {r}"
+    sim.close()
+
+
+def test_statevar_input_matches_oracle(tmp_path):
+    """A network driven by the device's state-variable MF input (the dense
+    configuration's coding) under graph replay ends in the oracle's state,
+    bit for bit, when the oracle's generator takes the host coding's rates
+    step by step; the input rows are reused cyclically."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    st = networks.build_random_network(9, 8, 5, 5, 10, networks.act_params("dense"), seed=8,
+                                       go_out_per_gr=4, mf_per_go=16, vel=147)
+    p = str(tmp_path / "net.state")
+    st.writeState(p)
+    coding = networks.StateVariableMF(1024, seed=5)
+    vals = coding.trajectory(250)
+    steps = 600
+    rates = np.stack([coding.rates_for(v) for v in vals])
+    o = Oracle(p, seeds=[7])
+    o.run_protocol_step_rates(cbmtest.statevar_protocol(13), rates, steps)
+    fin_o = str(tmp_path / "oracle.state")
+    o.save(fin_o)
+    sim = cbm.CBMSimCore(cbm.CBMState(p), [7], device=0)
+    sim.set_statevar_input(coding, vals, mfSeed=13)
+    sim.run(steps, 50)
+    fin_p = str(tmp_path / "b200.state")
+    sim.writeToState(fin_p)
+    sim.close()
+    assert compare_states(fin_o, fin_p) == []
+    a = cbm.CBMState(fin_p).array("apBufMF")
+    assert a.any(), "no MF spiked"

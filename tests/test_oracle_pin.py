@@ -392,3 +392,21 @@ def test_trials_data_getters_read_the_reference_file(tmp_path):
                                                   fields[key][proto["dataStartTrial"] * proto["trialSteps"] + rec_from + k + 1]]
     assert seen > 100
     assert d.getEyelidData(0)[:3] == [float(v) for v in eye[:3]]
+
+
+def test_oracle_step_rates_equal_protocol_tables(tmp_path):
+    """The oracle's driver with per-step rate rows (the state-variable input's
+    form) equals its driver with the protocol's tables when every row holds
+    the background table and no trial has a CS."""
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    proto = cbmtest.statevar_protocol(17)
+    a = Oracle(st, seeds=[7])
+    rates = cbmtest.protocol_rates(a.num["MF"], seed=3)
+    a.run_protocol(proto, rates, 400, record=False)
+    pa = str(tmp_path / "a.state")
+    a.save(pa)
+    b = Oracle(st, seeds=[7])
+    b.run_protocol_step_rates(proto, np.stack([rates[0]] * 7), 400)
+    pb = str(tmp_path / "b.state")
+    b.save(pb)
+    assert open(pa, "rb").read() == open(pb, "rb").read()
