@@ -148,6 +148,7 @@ def _load():
         "cbm_device_expf": (I, [I, P, P, U64]),
         "cbm_device_exp": (I, [I, P, P, U64]),
         "cbm_sim_set_statevar_input": (I, [P, P]),
+        "cbm_batch_record_trial_data": (I, [P, U]),
         "cbm_sim_statevar_rates": (I, [P, U64, P]),
     }
     for name, (res, args) in sig.items():
@@ -774,6 +775,29 @@ class CBMBatch:
         if kind == "eyelid":
             return out.reshape(trials, -1)
         return out.reshape(trials, -1, self.states[i].con("numNC" if kind == "nc" else "numPC"))
+
+    def record_trial_data(self, i):
+        """Record instance i's ECTrialsData from the next step on
+        (cbm_batch_record_trial_data)."""
+        _check(lib.cbm_batch_record_trial_data(self._h, i))
+
+    def trial_data(self, i):
+        """Instance i's ECTrialsData records, in the form of
+        CBMSimCore.trial_data (after record_trial_data)."""
+        p = self._protocols[i]
+        if not lib.cbm_batch_trial_record_bytes(self._h, i, TRIAL_PSH["go"][0]):
+            raise CBMError(1, "the trial data of that instance is not recorded")
+        rows = (p["csOff"] + p["postCS"] - (p["csOn"] - p["preCS"])) // 32
+        out = {"psh": {}, "raster": {}, "eyelid": eyelid_out(self.trial_record(i, "eyelid"))}
+        for kinds, key, dtype in ((TRIAL_PSH, "psh", np.float32), (TRIAL_RASTER, "raster", np.uint32)):
+            for name, (k, cell) in kinds.items():
+                cells = self.states[i].con(cell)
+                n = lib.cbm_batch_trial_record_bytes(self._h, i, k)
+                a = np.empty(n // 4, dtype=dtype)
+                if n:
+                    _check(lib.cbm_batch_trial_record(self._h, i, k, a.ctypes.data, n))
+                out[key][name] = a.reshape(-1, cells) if key == "psh" else a.reshape(p["numDataTrials"], rows, cells)
+        return out
 
     def writeToState(self, i, path=None):
         _check(lib.cbm_batch_write_to_state(self._h, i))

@@ -589,6 +589,13 @@ int cbm_batch_trial_record(cbm_batch *b, unsigned i, int kind, void *dst, uint64
 	return CBM_OK;
 }
 
+int cbm_batch_record_trial_data(cbm_batch *b, unsigned i)
+{
+	BATCH_OK(b, i);
+	TRY(b->sim.recordTrialData(i));
+	return CBM_OK;
+}
+
 int cbm_batch_write_to_state(cbm_batch *b, unsigned i)
 {
 	BATCH_OK(b, i);

@@ -1449,10 +1449,20 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			const uint32_t n = min(32u, N->numpNCfromPCtoNC - j0);
 			for (uint32_t q = 0; q < n; q++) gPCNCSum = gPCNCSum + __shfl_sync(0xffffffffu, g, q);
 		}
+		// lanes 0 and 1: the NMDA and AMPA sums over the NC's MF synapses in
+		// the reference's order; eight loads in flight ahead of the adds
 		float partial = 0;
 		if (lane < 2) {
 			const float *src = sN + lane * nMFNC;
-			for (uint32_t j = 0; j < nMFNC; j++) partial = partial + src[j];
+			uint32_t j = 0;
+			for (; j + 8 <= nMFNC; j += 8) {
+				float q[8];
+#pragma unroll
+				for (uint32_t u = 0; u < 8; u++) q[u] = src[j + u];
+#pragma unroll
+				for (uint32_t u = 0; u < 8; u++) partial = partial + q[u];
+			}
+			for (; j < nMFNC; j++) partial = partial + src[j];
 		}
 		const float ampaSum = __shfl_sync(0xffffffffu, partial, 1);
 		if (lane == 0) {
@@ -1903,7 +1913,9 @@ __global__ void grPSHKernel(const DevNet *N, uint32_t stepOffset)
 // are counted over all updates: (recLen - 1) / 32 updates a trial against
 // recLen / 32 rows a raster trial.  One thread per cell; cells are GO, MF,
 // SC, then zone 0's BC, PC, IO and NC.
-__global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset)
+// Cell c (GO, MF, SC, BC, PC, IO, NC in that order) of network N's
+// ECTrialsData records at step stepsDone + 1 + stepOffset.
+__device__ void trialDataCell(const DevNet *N, uint32_t stepOffset, uint32_t c)
 {
 	const DevProtocol *P = N->proto;
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
@@ -1916,7 +1928,6 @@ __global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset)
 		return;
 	const uint32_t nGO = N->numGO, nMF = N->numMF, nSC = N->numSC, nBC = N->numBC, nPC = N->numPC;
 	const uint32_t nIO = N->numIO, nNC = N->numNC;
-	const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= nGO + nMF + nSC + nBC + nPC + nIO + nNC) return;
 	const DevZone &Z = N->zones[0];
 	const size_t B = P->nBins, bin = (uint32_t)ct / P->binSteps;
@@ -1974,6 +1985,23 @@ __global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset)
 	}
 	i -= nIO;
 	if (rrow != ~0ull) rNC[rrow * nNC + i] = Z.apBufNC[i];
+}
+
+__global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset)
+{
+	trialDataCell(N, stepOffset, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The batched form: thread c of the grid is cell c - cellOffset[n] of the
+// network n with cellOffset[n] <= c < cellOffset[n + 1].
+__global__ void trialDataBatchKernel(const DevNet *const *nets, const uint32_t *cellOffset, int numNets,
+		uint32_t stepOffset)
+{
+	const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= cellOffset[numNets]) return;
+	uint32_t local = 0;
+	const DevNet *N = locateNet(nets, cellOffset, numNets, c, local);
+	trialDataCell(N, stepOffset, local);
 }
 
 // Prepare the first step of a newly set protocol (the network's step tBase + 1).

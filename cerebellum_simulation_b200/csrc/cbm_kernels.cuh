@@ -52,6 +52,10 @@ __global__ void protocolPrimeKernel(const DevNet *N);
 // the GR pass of that step: 8 GR per thread.
 __global__ void grPSHKernel(const DevNet *N, uint32_t stepOffset);
 __global__ void trialDataKernel(const DevNet *N, uint32_t stepOffset);
+// All networks of a batch: cellOffset[n] is the first grid thread of network
+// n's small cells (cellOffset[numNets] the total).
+__global__ void trialDataBatchKernel(const DevNet *const *nets, const uint32_t *cellOffset, int numNets,
+		uint32_t stepOffset);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);
 __global__ void expfProbeKernel(const float *in, float *out, uint32_t n);

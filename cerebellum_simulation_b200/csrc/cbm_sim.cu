@@ -1167,7 +1167,7 @@ Simulator::~Simulator()
 	if (hExport_) cudaFreeHost(hExport_);
 	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
-	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_}) if (b->ptr) cudaFree(b->ptr);
+	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_, &dCellOffset_}) if (b->ptr) cudaFree(b->ptr);
 	if (s0_) cudaStreamDestroy(s0_);
 	if (s1_) cudaStreamDestroy(s1_);
 	for (cudaEvent_t e : {fork_, join_, ev0_, ev1_, tev0_, tev1_}) if (e) cudaEventDestroy(e);
@@ -1488,7 +1488,13 @@ std::string Simulator::recordStep(uint32_t k)
 {
 	// after both kernels of the step: its GR spikes into the histogram, and
 	// its small-cell state into the trial data
-	if (nets_.size() != 1) return "";
+	if (nets_.size() != 1) {
+		if (!dCellOffset_.ptr) return "";  // no instance records its trial data
+		trialDataBatchKernel<<<(cellTotal_ + 255) / 256, 256, 0, s0_>>>((const DevNet *const *)dNetPtrs_.ptr,
+				(const uint32_t *)dCellOffset_.ptr, (int)nets_.size(), k);
+		CK(cudaGetLastError(), "launching the trial-data record");
+		return "";
+	}
 	const DevNet &h = nets_[0]->dev();
 	if (nets_[0]->recordsGR()) {
 		const uint32_t threads = (h.numGR + 7) / 8;
@@ -1601,13 +1607,25 @@ std::string Simulator::recordGR()
 	return "";
 }
 
-std::string Simulator::recordTrialData()
+std::string Simulator::recordTrialData(size_t i)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
-	if (nets_.size() != 1) return "the trial data is recorded for single-network simulators";
+	if (i >= nets_.size()) return "instance out of range";
 	CK(cudaStreamSynchronize(s0_), "sync");
-	const bool was = nets_[0]->recordsTrialData();
-	CKS(nets_[0]->recordTrialData(s0_));
+	const bool was = nets_[i]->recordsTrialData();
+	CKS(nets_[i]->recordTrialData(s0_));
+	if (nets_.size() > 1 && !dCellOffset_.ptr) {
+		// the batched record kernel's map from grid threads to instances
+		std::vector<uint32_t> off(1, 0);
+		for (Network *n : nets_) {
+			const DevNet &h = n->dev();
+			off.push_back(off.back() + h.numGO + h.numMF + h.numSC + h.numBC + h.numPC + h.numIO + h.numNC);
+		}
+		CK(cudaMalloc(&dCellOffset_.ptr, off.size() * sizeof(uint32_t)), "cell offsets");
+		dCellOffset_.bytes = off.size() * sizeof(uint32_t);
+		CK(cudaMemcpy(dCellOffset_.ptr, off.data(), dCellOffset_.bytes, cudaMemcpyHostToDevice), "cell offsets");
+		cellTotal_ = off.back();
+	}
 	if (!was) dropGraphs();  // the step graphs gain the trial-data kernel
 	return "";
 }

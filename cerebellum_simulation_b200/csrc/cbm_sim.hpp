@@ -68,7 +68,7 @@ public:
 	std::string setStateVarInput(size_t i, const cbm_statevar_input &in);
 	// Record network 0's GR peri-stimulus histogram (single-network simulators).
 	std::string recordGR();
-	std::string recordTrialData();
+	std::string recordTrialData(size_t i = 0);
 	// Run nsteps as CUDA-graph chunks of chunk steps (inputs resident in HBM).
 	// With instrument, external events around every GR pass of the chunk
 	// give lastPassMs(): the pass's mean duration over the last replay.
@@ -138,6 +138,8 @@ private:
 	cudaStream_t s0_ = nullptr, s1_ = nullptr;
 	cudaEvent_t fork_ = nullptr, join_ = nullptr, ev0_ = nullptr, ev1_ = nullptr, tev0_ = nullptr, tev1_ = nullptr;
 	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_, dStageBytes_;
+	DeviceBuf dCellOffset_;   // trialDataBatchKernel's instance map (batches recording trial data)
+	uint32_t cellTotal_ = 0;
 	uint32_t passBlocks_ = 0;
 	size_t passSmem_ = 0, tailSmem_ = 0;
 	// TMA GR pass geometry (passTmaFn_ null: the plain pass kernel runs)

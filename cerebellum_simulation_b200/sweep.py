@@ -87,6 +87,20 @@ def nc_trace(nc_psh, num_nc):
     return (c / (num_nc * 0.030)).astype(np.float32)
 
 
+def pc_trace(pc_psh, num_pc):
+    """[trials, bins, numPC] counts per 10-step bin -> [trials, 50] mean PC
+    rate (Hz), binned as nc_trace."""
+    return nc_trace(pc_psh, num_pc)
+
+
+def trace_rmse_over_range(pred, truth):
+    """Root-mean-square error of predicted traces over the range of the true
+    traces (max - min over all of them): the sweep's error measure."""
+    pred, truth = np.asarray(pred, np.float64), np.asarray(truth, np.float64)
+    span = float(truth.max() - truth.min())
+    return float(np.sqrt(np.mean((pred - truth) ** 2))) / max(span, 1e-9)
+
+
 def objective(traces):
     """Conditioned response of a trace (or [.., 50] traces): mean NC rate over
     the late CS (steps 800-1000) minus the pre-CS mean (steps 0-500)."""
@@ -97,7 +111,14 @@ def objective(traces):
 def simulate(base_state, params, mf_seeds, trials, device=0, batch=256, chunk=250):
     """Trials of every parameter set through the batched simulator:
     [n, trials, 50] NC rate traces and the seconds of device time."""
-    out, gpu_ms = [], 0.0
+    traces, secs = simulate_traces(base_state, params, mf_seeds, trials, device, batch, chunk)
+    return traces["nc"], secs
+
+
+def simulate_traces(base_state, params, mf_seeds, trials, device=0, batch=256, chunk=250):
+    """As simulate, with both responses: ({"nc": [n, trials, 50] NC rate
+    traces, "pc": [n, trials, 50] mean PC rate traces}, device seconds)."""
+    out, out_pc, gpu_ms = [], [], 0.0
     for b0 in range(0, params.shape[0], batch):
         idx = range(b0, min(params.shape[0], b0 + batch))
         states = []
@@ -118,8 +139,9 @@ def simulate(base_state, params, mf_seeds, trials, device=0, batch=256, chunk=25
         gpu_ms += b.run(steps, chunk)
         for k, i in enumerate(idx):
             out.append(nc_trace(b.trial_record(k, "nc"), states[k].con("numNC")))
+            out_pc.append(pc_trace(b.trial_record(k, "pc"), states[k].con("numPC")))
         b.close()
-    return np.stack(out), gpu_ms / 1000.0
+    return {"nc": np.stack(out), "pc": np.stack(out_pc)}, gpu_ms / 1000.0
 
 
 def fit_surrogate(net, x, traces, epochs=150, lr=1e-3, seed=0):

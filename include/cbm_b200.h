@@ -374,6 +374,11 @@ int cbm_batch_run(cbm_batch *b, uint64_t nsteps, uint32_t graphChunk, float *gpu
 int cbm_batch_autotune(cbm_batch *b, uint32_t nsteps, char *choice, size_t choiceLen, float *ms);
 uint64_t cbm_batch_trial_record_bytes(cbm_batch *b, unsigned instance, int kind);
 int cbm_batch_trial_record(cbm_batch *b, unsigned instance, int kind, void *dst, uint64_t bytes);
+/* Record instance i's ECTrialsData (as cbm_sim_record_trial_data, from the
+ * next step on; its protocol must be set).  One kernel after each step
+ * records every instance that does; read with cbm_batch_trial_record
+ * (CBM_REC_PSH_* / CBM_REC_RASTER_*). */
+int cbm_batch_record_trial_data(cbm_batch *b, unsigned instance);
 /* Write instance i's device state into its cbm_state (writeToState). */
 int cbm_batch_write_to_state(cbm_batch *b, unsigned instance);
 /* Total GR of the instances (GR updates per batch step). */

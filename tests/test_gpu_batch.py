@@ -110,3 +110,33 @@ def test_batch_config4_sizes_match_instances_alone(tmp_path):
         w0 = cbm.CBMState(p).array("pfSynWeightPC", 0)
         w1 = cbm.CBMState(str(tmp_path / f"b{i}_c4.state")).array("pfSynWeightPC", 0)
         assert (w1 != w0).any(), f"instance {i}: no PF->PC weight moved"
+
+
+def test_batch_trial_data_matches_instances_alone(tmp_path):
+    """ECTrialsData recorded for batch instances (cbm_batch_record_trial_data:
+    one kernel over every recording instance after each step) equals the
+    oracle's records of each instance alone, histograms (float sums
+    included) and rasters; an instance that does not record stays without
+    records."""
+    import cerebellum_simulation_b200 as cbm
+    paths, protos = _instances(tmp_path)
+    states = [cbm.CBMState(p) for p in paths]
+    rates = [cbmtest.protocol_rates(st.con("numMF"), seed=10 + i) for i, st in enumerate(states)]
+    b = cbm.CBMBatch(states, [[40 + i] for i in range(len(states))], device=0)
+    for i in range(len(states)):
+        b.set_eyelid_protocol(i, rates[i], **protos[i])
+    for i in (0, 2):
+        b.record_trial_data(i)
+    steps = 2 * protos[0]["trialSteps"]
+    b.run(steps, 40)
+    for i in (0, 2):
+        o = Oracle(paths[i], seeds=[40 + i])
+        _, _, _, _, want = o.run_protocol(protos[i], rates[i], steps, record=False, trial_data=True)
+        got = b.trial_data(i)
+        for name, a in want["psh"].items():
+            assert cbmtest.same_values(got["psh"][name].ravel(), a.ravel()).all(), (i, name)
+        for name, a in want["raster"].items():
+            assert np.array_equal(got["raster"][name], a), (i, name)
+        assert want["psh"]["go"].any() and want["raster"]["go"].any()
+    with pytest.raises(cbm.CBMError):
+        b.trial_data(1)
