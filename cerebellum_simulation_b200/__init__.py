@@ -93,6 +93,7 @@ def _load():
         "cbm_state_load": (I, [S, ctypes.POINTER(P)]),
         "cbm_state_new": (I, [S, S, U, P, ctypes.POINTER(P)]),
         "cbm_state_save": (I, [P, S]),
+        "cbm_state_generate": (I, [S, S, U, P, ctypes.POINTER(P)]),
         "cbm_state_load_mem": (I, [P, U64, ctypes.POINTER(U64), ctypes.POINTER(P)]),
         "cbm_state_save_mem": (I, [P, P, U64, ctypes.POINTER(U64)]),
         "cbm_sim_save_mem": (I, [P, P, U64, ctypes.POINTER(U64)]),
@@ -200,6 +201,21 @@ class CBMState:
             _check(lib.cbm_state_load(os.fsencode(path), ctypes.byref(self._h)))
         else:
             raise ValueError("CBMState needs a state file path (or use CBMState.new)")
+
+    @classmethod
+    def generate(cls, con_text, act_text, n_zones=1, innet_seed=None, zone_con_seeds=None, zone_act_seeds=None):
+        """CBMState(actPF, conPF, nZones, innetCRSeed, mzoneCRSeed,
+        mzoneARSeed): the network with the reference's own generator and
+        random sequence (cbm_state_generate); without seeds they are drawn
+        from the wall clock, as CBMState(actPF, conPF, nZones) does."""
+        h = ctypes.c_void_p()
+        seeds = None
+        if innet_seed is not None:
+            zc = list(zone_con_seeds) if zone_con_seeds is not None else [innet_seed + 1 + z for z in range(n_zones)]
+            za = list(zone_act_seeds) if zone_act_seeds is not None else [0] * n_zones
+            seeds = np.asarray([innet_seed] + zc[:n_zones] + za[:n_zones], dtype=np.int32)
+        _check(lib.cbm_state_generate(con_text.encode(), act_text.encode(), n_zones, _ptr(seeds), ctypes.byref(h)))
+        return cls(_handle=h)
 
     @classmethod
     def new(cls, con_text, act_text, n_zones=1, wiring_seeds=None):

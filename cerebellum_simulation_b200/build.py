@@ -25,7 +25,7 @@ NVCC_FLAGS = [
     "-I", os.path.join(ROOT, "include"),
 ]
 
-SOURCES = ["cbm_state.cpp", "cbm_sim.cu", "cbm_kernels.cu", "cbm_pass_vec.cu", "cbm_capi.cu", "cbm_noalloc.cu",
+SOURCES = ["cbm_state.cpp", "cbm_netgen.cpp", "cbm_sim.cu", "cbm_kernels.cu", "cbm_pass_vec.cu", "cbm_capi.cu", "cbm_noalloc.cu",
            "cbm_mlp.cu"]
 
 

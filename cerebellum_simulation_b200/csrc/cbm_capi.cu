@@ -72,6 +72,21 @@ int cbm_state_new(const char *conText, const char *actText, unsigned nZones, con
 	return CBM_OK;
 }
 
+int cbm_state_generate(const char *conText, const char *actText, unsigned nZones, const int *seeds, cbm_state **out)
+{
+	NEED(conText); NEED(actText); NEED(out);
+	if (nZones < 1 || nZones > (unsigned)kMaxZones) return fail(CBM_ERR_ARG, "zone count must be 1..4");
+	std::vector<int> sd = seeds ? std::vector<int>(seeds, seeds + 1 + 2 * nZones) : clockSeeds(nZones);
+	std::vector<int> conSeeds;
+	for (unsigned z = 0; z < nZones; z++) conSeeds.push_back(sd[1 + z]);
+	cbm_state *s = new (std::nothrow) cbm_state();
+	if (!s) return fail(CBM_ERR_ARG, "out of host memory");
+	std::string e = s->st.generate(conText, actText, nZones, sd[0], conSeeds);
+	if (!e.empty()) { delete s; return fail(classify(e), e); }
+	*out = s;
+	return CBM_OK;
+}
+
 int cbm_state_save(cbm_state *s, const char *path)
 {
 	NEED(s); NEED(path);

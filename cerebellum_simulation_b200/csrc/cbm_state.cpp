@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <sstream>
 
 #include "cbm_rng.hpp"
@@ -544,6 +545,50 @@ std::string State::writeTo(std::ostream &f) const
 }
 
 // ------------------------------------------------------------- new state
+// connectPCtoNC (mzoneconnectivitystate.cpp:268-345): each NC takes a
+// regular block of PCs, every NC but the last adds random PCs (drawPC)
+// that are not full and not yet connected to it, and the last NC takes the
+// PCs with free output slots.
+void wirePCtoNC(State &s, uint32_t z, const std::function<uint32_t()> &drawPC)
+{
+	const ConParams &cp = s.cp;
+	uint32_t *ncpc = s.find("pNCfromPCtoNC", (int)z)->as<uint32_t>();
+	uint32_t *pcnc = s.find("pPCfromPCtoNC", (int)z)->as<uint32_t>();
+	std::fill(ncpc, ncpc + (size_t)cp.numNC * cp.numpNCfromPCtoNC, 0xFFFFFFFFu);
+	std::fill(pcnc, pcnc + (size_t)cp.numPC * cp.numpPCfromPCtoNC, 0xFFFFFFFFu);
+	std::vector<int> pcNum(cp.numPC, 1);
+	const uint32_t perNC = cp.numPC / cp.numNC;
+	for (uint32_t i = 0; i < cp.numNC; i++)
+		for (uint32_t j = 0; j < perNC; j++) {
+			uint32_t pc = i * perNC + j;
+			ncpc[(size_t)i * cp.numpNCfromPCtoNC + j] = pc;
+			pcnc[(size_t)pc * cp.numpPCfromPCtoNC + 0] = i;
+		}
+	for (uint32_t i = 0; i + 1 < cp.numNC; i++)
+		for (uint32_t j = cp.numpNCfromPCtoNC / 3; j < cp.numpNCfromPCtoNC; j++) {
+			uint32_t pc = 0;
+			for (int tries = 0; tries < 1000000; tries++) {
+				pc = drawPC();
+				if ((uint32_t)pcNum[pc] >= cp.numpPCfromPCtoNC) continue;
+				bool ok = true;
+				for (int k = 0; k < pcNum[pc]; k++) if (pcnc[(size_t)pc * cp.numpPCfromPCtoNC + k] == i) { ok = false; break; }
+				if (ok) break;
+			}
+			ncpc[(size_t)i * cp.numpNCfromPCtoNC + j] = pc;
+			pcnc[(size_t)pc * cp.numpPCfromPCtoNC + pcNum[pc]] = i;
+			pcNum[pc]++;
+		}
+	uint32_t numSyn = perNC;
+	for (uint32_t h = 1; h < cp.numpPCfromPCtoNC; h++)
+		for (uint32_t i = 0; i < cp.numPC; i++)
+			if ((uint32_t)pcNum[i] < cp.numpPCfromPCtoNC && numSyn < cp.numpNCfromPCtoNC) {
+				ncpc[(size_t)(cp.numNC - 1) * cp.numpNCfromPCtoNC + numSyn] = i;
+				pcnc[(size_t)i * cp.numpPCfromPCtoNC + pcNum[i]] = cp.numNC - 1;
+				pcNum[i]++;
+				numSyn++;
+			}
+}
+
 std::string State::create(const std::string &conText, const std::string &actText, uint32_t nZones,
 		const std::vector<int> &pcncSeeds)
 {
@@ -604,45 +649,15 @@ std::string State::create(const std::string &conText, const std::string &actText
 			scpc[i] = pc;
 			pcsc[(size_t)pc * cp.numpPCfromSCtoPC + i % cp.numpPCfromSCtoPC] = i;
 		}
-		// connectPCtoNC: the regular block, then the random extra synapses
-		// (the reference draws them with SFMT IRandomX; this library draws them
-		// from its counter-based stream keyed by the zone's seed)
-		uint32_t *ncpc = find("pNCfromPCtoNC", z)->as<uint32_t>();
-		uint32_t *pcnc = find("pPCfromPCtoNC", z)->as<uint32_t>();
-		std::vector<int> pcNum(cp.numPC, 1);
-		uint32_t perNC = cp.numPC / cp.numNC;
-		for (uint32_t i = 0; i < cp.numNC; i++)
-			for (uint32_t j = 0; j < perNC; j++) {
-				uint32_t pc = i * perNC + j;
-				ncpc[(size_t)i * cp.numpNCfromPCtoNC + j] = pc;
-				pcnc[(size_t)pc * cp.numpPCfromPCtoNC + 0] = i;
-			}
-		uint64_t ctr = 0;
-		int seed = z < pcncSeeds.size() ? pcncSeeds[z] : (int)(7919 + z);
-		for (uint32_t i = 0; i + 1 < cp.numNC; i++)
-			for (uint32_t j = cp.numpNCfromPCtoNC / 3; j < cp.numpNCfromPCtoNC; j++) {
-				uint32_t pc = 0;
-				for (int tries = 0; tries < 1000000; tries++) {
-					pc = (uint32_t)(rng::uniform24((uint32_t)seed, rng::kStreamWiring, ctr++) * cp.numPC);
-					if ((uint32_t)pcNum[pc] >= cp.numpPCfromPCtoNC) continue;
-					bool ok = true;
-					for (int k = 0; k < pcNum[pc]; k++) if (pcnc[(size_t)pc * cp.numpPCfromPCtoNC + k] == i) { ok = false; break; }
-					if (ok) break;
-				}
-				ncpc[(size_t)i * cp.numpNCfromPCtoNC + j] = pc;
-				pcnc[(size_t)pc * cp.numpPCfromPCtoNC + pcNum[pc]] = i;
-				pcNum[pc]++;
-			}
+		// connectPCtoNC: the reference draws the random extra synapses with
+		// SFMT IRandomX from the zone's seed; this library's own networks draw
+		// them from its counter-based stream keyed by the zone's seed
+		// (State::generate uses the reference's generator)
 		{
-			uint32_t numSyn = perNC;
-			for (uint32_t h = 1; h < cp.numpPCfromPCtoNC; h++)
-				for (uint32_t i = 0; i < cp.numPC; i++)
-					if ((uint32_t)pcNum[i] < cp.numpPCfromPCtoNC && numSyn < cp.numpNCfromPCtoNC) {
-						ncpc[(size_t)(cp.numNC - 1) * cp.numpNCfromPCtoNC + numSyn] = i;
-						pcnc[(size_t)i * cp.numpPCfromPCtoNC + pcNum[i]] = cp.numNC - 1;
-						pcNum[i]++;
-						numSyn++;
-					}
+			uint64_t ctr = 0;
+			const uint32_t seed = (uint32_t)(z < pcncSeeds.size() ? pcncSeeds[z] : (int)(7919 + z));
+			const uint32_t nPC = cp.numPC;
+			wirePCtoNC(*this, z, [&]() { return (uint32_t)(rng::uniform24(seed, rng::kStreamWiring, ctr++) * nPC); });
 		}
 		// connectNCtoIO, connectMFtoNC, connectIOtoPC, connectIOtoIO
 		uint32_t *ionc = find("pIOfromNCtoIO", z)->as<uint32_t>();

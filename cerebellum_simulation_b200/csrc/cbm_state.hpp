@@ -128,6 +128,13 @@ public:
 	// "unconnected" values (counts 0, indices UINT_MAX) for the caller to fill.
 	std::string create(const std::string &conText, const std::string &actText, uint32_t nZones,
 			const std::vector<int> &pcncSeeds);
+	// CBMState(actPF, conPF, nZones, innetCRSeed, mzoneCRSeed, mzoneARSeed)
+	// (cbmstate.cpp:60-64, 176-204): create() plus the reference's own
+	// generator for the input net and the PC->NC wiring, drawing from its
+	// random generator seeded as the reference seeds it (cbm_netgen.cpp).
+	// The microzone activity seeds are not used by the reference.
+	std::string generate(const std::string &conText, const std::string &actText, uint32_t nZones, int innetSeed,
+			const std::vector<int> &mzoneConSeeds);
 
 	NamedArray *find(const std::string &name, int zone = -1);
 	const NamedArray *find(const std::string &name, int zone = -1) const;
@@ -137,6 +144,10 @@ private:
 	void allocate();
 	void fixLoaded();
 };
+
+// The seeds CBMState(actPF, conPF, nZones) draws from the wall clock:
+// innet, then connectivity and activity per zone.
+std::vector<int> clockSeeds(uint32_t nZones);
 
 // Byte-exact text of the parameter header as CBMState::writeState emits it.
 std::string formatHeader(const State &s);

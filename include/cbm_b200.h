@@ -111,6 +111,21 @@ int cbm_state_load_mem(const void *data, uint64_t len, uint64_t *consumed, cbm_s
 int cbm_state_new(const char *conParamsText, const char *actParamsText, unsigned nZones,
 		const int *wiringSeeds, cbm_state **out);
 
+/* CBMState(actPF, conPF, nZones, innetCRSeed, mzoneCRSeed, mzoneARSeed)
+ * (cbmstate.cpp:60-64, 176-204) from the parameter texts: the network with
+ * the reference's own generator, i.e. the spatial glomerulus-mediated
+ * input-net wiring and GR delays (innetconnectivitystate.cpp:12-44,
+ * 716-1123), the microzone wiring with its random PC->NC synapses
+ * (mzoneconnectivitystate.cpp:12-40, 187-417) and the initial activity, all
+ * drawn from the reference's random generator (SFMT, as CRandomSFMT0) seeded
+ * as the reference seeds it.  seeds: 1 + 2 nZones values (innetCRSeed, then
+ * mzoneCRSeed[nZones], then mzoneARSeed[nZones], which the reference does
+ * not use), or NULL to draw them from the wall clock as CBMState(actPF,
+ * conPF, nZones) does (cbmstate.cpp:35-57).  The state file equals the
+ * reference's for the same parameters and seeds. */
+int cbm_state_generate(const char *conParamsText, const char *actParamsText, unsigned nZones, const int *seeds,
+		cbm_state **out);
+
 /* CBMState::writeState (cbmstate.cpp:86-103), byte-compatible with the
  * reference.  Like the reference it resets the two GO->GO depression arrays
  * of the state it writes (innetactivitystate.cpp:247-248). */

@@ -258,6 +258,22 @@ public:
 	}
 	// The same from a file name.
 	explicit CBMState(const std::string &statePath) { cbm::check(cbm_state_load(statePath.c_str(), &s_)); }
+	// CBMState(actPF, conPF, nZones) and CBMState(actPF, conPF, nZones,
+	// innetCRSeed, mzoneCRSeed, mzoneARSeed) (cbmstate.h:38-40): a new
+	// network from the parameter files with the reference's own generator and
+	// random sequence; without seeds they come from the wall clock.
+	CBMState(std::fstream &actPFile, std::fstream &conPFile, unsigned int nZones)
+	{
+		generate(actPFile, conPFile, nZones, nullptr);
+	}
+	CBMState(std::fstream &actPFile, std::fstream &conPFile, unsigned int nZones, int innetCRSeed, int *mzoneCRSeed,
+			int *mzoneARSeed)
+	{
+		std::vector<int> seeds(1, innetCRSeed);
+		for (unsigned int z = 0; z < nZones; z++) seeds.push_back(mzoneCRSeed[z]);
+		for (unsigned int z = 0; z < nZones; z++) seeds.push_back(mzoneARSeed[z]);
+		generate(actPFile, conPFile, nZones, seeds.data());
+	}
 	// CBMState(actPF, conPF, nZones, innetCRSeed, mzoneCRSeed, mzoneARSeed) from the
 	// parameter texts; the input-net wiring is left for the caller (see cbm_state_new).
 	CBMState(const std::string &actParamsText, const std::string &conParamsText, unsigned int nZones,
@@ -291,6 +307,16 @@ public:
 		return static_cast<T *>(p);
 	}
 	cbm_state *handle() { return s_; }
+
+private:
+	void generate(std::fstream &actPFile, std::fstream &conPFile, unsigned int nZones, const int *seeds)
+	{
+		std::streampos a0, c0;
+		const std::string act = cbm::restOf(actPFile, a0), con = cbm::restOf(conPFile, c0);
+		cbm::check(cbm_state_generate(con.c_str(), act.c_str(), nZones, seeds, &s_));
+	}
+
+public:
 
 	// the reference's accessors; the objects live as long as the state
 	IConnectivityParams *getConnectivityParams() { return &conParams_; }

@@ -36,6 +36,16 @@ template <typename W> static void streamRoundTrip(const char *path, W writeState
 int main(int argc, char **argv)
 {
 	if (argc < 2) return 2;
+	// "--generate ACT CON OUT": CBMState(actPF, conPF, 1, 11, {22}, {33}) and
+	// writeState, as the reference's driver builds a new network
+	if (!std::strcmp(argv[1], "--generate") && argc == 5) {
+		std::fstream act(argv[2], std::ios::in), con(argv[3], std::ios::in);
+		int cs[1] = {22}, as[1] = {33};
+		CBMState st(act, con, 1, 11, cs, as);
+		st.writeState(std::string(argv[4]));
+		std::printf("generated zones %u\n", st.getNumZones());
+		return 0;
+	}
 	const char *streamOut = nullptr;
 	for (int i = 1; i + 1 < argc; i++)
 		if (!std::strcmp(argv[i], "--stream")) { streamOut = argv[i + 1]; argc = i; break; }

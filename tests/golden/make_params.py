@@ -16,6 +16,23 @@ import os
 import sys
 
 SETS = {"act_16k.txt": "actParams_16K_Gr.txt", "act_dense.txt": "actParams_dense_4MGR_dev.txt"}
+# connectivity sets, copied line by line up to their end marker (the GO-GO
+# matrix block has rows of three values)
+CON_SETS = {"con_16k.txt": "conParams_16K_Gr.txt"}
+
+
+def convert_con(src, dst):
+    out = []
+    with open(src) as f:
+        for line in f:
+            line = " ".join(line.split())
+            if not line:
+                continue
+            out.append(line)
+            if line.startswith("connectivityParamEnd"):
+                break
+    with open(dst, "w") as f:
+        f.write("\n".join(out) + "\n")
 
 
 def convert(src, dst):
@@ -38,4 +55,7 @@ if __name__ == "__main__":
     dest = os.path.join(root, "cerebellum_simulation_b200", "params")
     for out, src in SETS.items():
         convert(os.path.join(ref, src), os.path.join(dest, out))
+        print(out)
+    for out, src in CON_SETS.items():
+        convert_con(os.path.join(ref, src), os.path.join(dest, out))
         print(out)

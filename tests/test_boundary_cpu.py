@@ -300,3 +300,48 @@ def test_device_exp_table_is_the_mathematical_one():
         hb = struct.unpack("<Q", struct.pack("<d", h))[0]
         tb = struct.unpack("<Q", struct.pack("<d", tail))[0]
         assert got[2 * k] == tb and got[2 * k + 1] == (hb - (k << 45)) % 2 ** 64, k
+
+
+
+def test_reference_generator_reproduces_the_reference_network(tmp_path):
+    """CBMState(actPF, conPF, nZones, innetCRSeed, mzoneCRSeed, mzoneARSeed)
+    with the reference's generator (cbm_state_generate, the C++ facade's
+    constructor with the reference's signature): the 16K parameter files
+    and seeds 11 / 22 / 33 give the reference's own state file
+    (tests/golden/ref16k.state.xz, written by the reference's CBMState with
+    the same arguments), byte for byte."""
+    import lzma
+    import subprocess
+    import cerebellum_simulation_b200 as cbm
+    params = os.path.join(ROOT, "cerebellum_simulation_b200", "params")
+    act, con = os.path.join(params, "act_16k.txt"), os.path.join(params, "con_16k.txt")
+    want = lzma.open(os.path.join(ROOT, "tests", "golden", "ref16k.state.xz")).read()
+    st = cbm.CBMState.generate(open(con).read(), open(act).read(), 1, 11, [22], [33])
+    out = tmp_path / "py.state"
+    st.writeState(str(out))
+    assert out.read_bytes() == want
+    exe = cbmtest.build_facade_check(str(tmp_path))
+    out2 = tmp_path / "cpp.state"
+    r = subprocess.run([exe, "--generate", act, con, str(out2)], check=True, capture_output=True, text=True)
+    assert "generated zones 1" in r.stdout
+    assert out2.read_bytes() == want
+
+
+@pytest.mark.skipif(not cbmtest.ref_available(), reason="reference harness oracle/_ref not built")
+@pytest.mark.parametrize("zones,seeds", [(2, (5, 7, 9)), (1, (123456, 99, 1))])
+def test_reference_generator_matches_the_reference_live(tmp_path, zones, seeds):
+    """The same against the reference's generator run live (oracle/_ref/
+    ref_gen) with other seeds and two microzones, whose PC->NC wiring draws
+    from each zone's seed."""
+    import subprocess
+    import cerebellum_simulation_b200 as cbm
+    params = os.path.join(ROOT, "cerebellum_simulation_b200", "params")
+    act, con = os.path.join(params, "act_16k.txt"), os.path.join(params, "con_16k.txt")
+    ref = tmp_path / "ref.state"
+    subprocess.run([cbmtest.REF_GEN, act, con, str(zones), str(seeds[0]), str(seeds[1]), str(seeds[2]), str(ref)],
+                   check=True, capture_output=True)
+    st = cbm.CBMState.generate(open(con).read(), open(act).read(), zones, seeds[0],
+                               [seeds[1] + z for z in range(zones)], [seeds[2] + z for z in range(zones)])
+    out = tmp_path / "b200.state"
+    st.writeState(str(out))
+    assert out.read_bytes() == ref.read_bytes()
