@@ -134,6 +134,8 @@ def _load():
         "cbm_batch_set_eyelid_protocol": (I, [P, U32, P]),
         "cbm_batch_run": (I, [P, U64, U32, ctypes.POINTER(F)]),
         "cbm_batch_autotune": (I, [P, U32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(F)]),
+        "cbm_batch_pass_geometry": (I, [P, ctypes.POINTER(U32), ctypes.POINTER(U32), ctypes.POINTER(U32),
+                                        ctypes.POINTER(U32)]),
         "cbm_batch_trial_record_bytes": (U64, [P, U32, I]),
         "cbm_batch_trial_record": (I, [P, U32, I, P, U64]),
         "cbm_batch_write_to_state": (I, [P, U32]),
@@ -734,8 +736,14 @@ class CBMSimCore:
         """(kernel name, consumer warps, rows per stage, stages) of the GR pass."""
         v = [ctypes.c_uint32() for _ in range(4)]
         _check(lib.cbm_sim_pass_geometry(self._h, *[ctypes.byref(x) for x in v]))
-        kind = ("grPassKernel", "grPassTmaKernel", "grPassPersistentKernel", "grPassVecKernel")[v[0].value]
-        return kind, v[1].value, v[2].value, v[3].value
+        return _pass_kind_name(v[0].value, single=True), v[1].value, v[2].value, v[3].value
+
+
+def _pass_kind_name(kind, single):
+    """Kernel name of a GR-pass kind (cbm_sim_pass_geometry's *kind)."""
+    if kind == 3 and not single:
+        return "grPassVecBatchKernel"
+    return ("grPassKernel", "grPassTmaKernel", "grPassPersistentKernel", "grPassVecKernel")[kind]
 
 
 class CBMBatch:
@@ -771,6 +779,12 @@ class CBMBatch:
         ms = ctypes.c_float()
         _check(lib.cbm_batch_run(self._h, nsteps, chunk, ctypes.byref(ms)))
         return ms.value
+
+    def pass_geometry(self):
+        """(kernel name, consumer warps, rows per stage, stages) of the batch's GR pass."""
+        v = [ctypes.c_uint32() for _ in range(4)]
+        _check(lib.cbm_batch_pass_geometry(self._h, *[ctypes.byref(x) for x in v]))
+        return _pass_kind_name(v[0].value, single=len(self.states) == 1), v[1].value, v[2].value, v[3].value
 
     def autotune(self, nsteps=100):
         """Time every GR-pass geometry on a scratch copy; keep the fastest.

@@ -590,6 +590,14 @@ int cbm_batch_autotune(cbm_batch *b, uint32_t nsteps, char *choice, size_t choic
 	return CBM_OK;
 }
 
+int cbm_batch_pass_geometry(cbm_batch *b, unsigned *kind, unsigned *consumerWarps, unsigned *rowsPerStage,
+		unsigned *stages)
+{
+	NEED(b); NEED(kind); NEED(consumerWarps); NEED(rowsPerStage); NEED(stages);
+	b->sim.passGeometry(kind, consumerWarps, rowsPerStage, stages);
+	return CBM_OK;
+}
+
 uint64_t cbm_batch_trial_record_bytes(cbm_batch *b, unsigned i, int kind)
 {
 	if (!b || i >= b->states.size()) return 0;

@@ -33,6 +33,11 @@ const void *passPersistentKernelFor(int W, int S, int B, int M);
 constexpr int kVecWarps = 8;
 constexpr int kVecMinBlocks = 3;
 constexpr uint32_t kVecClaim = 2;
+constexpr uint32_t kVecBatchClaim = 8;
+constexpr int kVecBatchMinBlocks = 2;
+// The batched form (several networks of the shape; arguments nets,
+// unitOffset, pcOffset, numNets, stepOffset, claim counters [3]).
+const void *passVecBatchKernel();
 bool passVecCapable(const DevNet &h);
 size_t passVecSmemBytes(const DevNet &h);
 const void *passVecKernel();

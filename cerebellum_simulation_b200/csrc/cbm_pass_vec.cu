@@ -72,6 +72,19 @@ __device__ float blockRowTree(float *sTree, uint32_t bs)
 	return v;
 }
 
+// The network n with offset[n] <= g < offset[n + 1] (offset sorted), and g's
+// index within it.
+__device__ __forceinline__ int findNet(const uint32_t *offset, int numNets, uint32_t g, uint32_t &local)
+{
+	int lo = 0, hi = numNets - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (offset[mid] <= g) lo = mid; else hi = mid - 1;
+	}
+	local = g - offset[lo];
+	return lo;
+}
+
 __device__ __forceinline__ float4 ldState(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void stState(float *p, float a, float b, float c, float d)
 {
@@ -80,11 +93,183 @@ __device__ __forceinline__ void stState(float *p, float a, float b, float c, flo
 
 }  // namespace
 
+// The per-network values a unit needs.
+struct VecNet {
+	float gLeak, eLeak, eGOIn, threshBase, threshMax, threshDecay, gDecMF, gIncMF, gDecGO, gIncGO;
+	uint32_t numGR, P, bs, K, bcShift, scShift, jGroups;
+	uint32_t *goCount;
+	float *vGR, *gKCaGR, *threshGR, *gESum, *gISum, *wGR, *pairOut;
+	uint32_t *apBufGR;
+	uint64_t *historyGR;
+	const uint16_t *mfIdx, *goIdx, *out16;
+	const uint8_t *pfDelay;
+};
+
+__device__ __forceinline__ VecNet vecNet(const DevNet *N, uint64_t t)
+{
+	VecNet c;
+	c.gLeak = N->gLeakGR; c.eLeak = N->eLeakGR; c.eGOIn = N->eGOGR;
+	c.threshBase = N->threshRestGR; c.threshMax = N->threshMaxGR; c.threshDecay = N->threshDecGR;
+	c.gDecMF = N->gDecMFtoGR; c.gIncMF = N->gIncMFtoGR; c.gDecGO = N->gDecGOtoGR; c.gIncGO = N->gIncGOtoGR;
+	c.numGR = N->numGR; c.P = N->P; c.bs = N->bs; c.K = N->K;
+	c.bcShift = N->bcShift; c.scShift = N->scShift; c.jGroups = N->bs / 64u;
+	c.goCount = N->goCount + (size_t)(t & 1) * N->numGO;
+	c.vGR = N->vGR; c.gKCaGR = N->gKCaGR; c.threshGR = N->threshGR; c.gESum = N->gESum; c.gISum = N->gISum;
+	c.wGR = N->zones[0].w;
+	c.pairOut = N->zones[0].pairSum + (size_t)(t & 1) * N->numPC * N->K * N->bs;
+	c.apBufGR = N->apBufGR; c.historyGR = N->historyGR;
+	c.mfIdx = N->mfIdx; c.goIdx = N->goIdx; c.out16 = N->outCon16; c.pfDelay = N->pfDelay;
+	return c;
+}
+
+// Spike lookups from shared-memory byte tables (a single network).
+struct SpikeBytes {
+	const uint8_t *mfT, *goT;
+	__device__ __forceinline__ int mf(uint32_t i) const { return mfT[i]; }
+	__device__ __forceinline__ int go(uint32_t i) const { return goT[i]; }
+};
+// Spike lookups from the spike bit words in global memory (a batch: every
+// network has its own, read through the L1 cache).
+struct SpikeBits {
+	const uint32_t *mfW, *goW;
+	__device__ __forceinline__ int mf(uint32_t i) const { return (__ldg(mfW + (i >> 5)) >> (i & 31u)) & 1u; }
+	__device__ __forceinline__ int go(uint32_t i) const { return (__ldg(goW + (i >> 5)) >> (i & 31u)) & 1u; }
+};
+
+// One unit u (128 cells) of a network at step t: every cell's update, its
+// pair sums, its PF->BC/SC counts (into bcCnt / scCnt, indexed by the
+// network's BC and SC numbers) and its GR->GO deliveries.
+template <class Spikes, class StepOf>
+__device__ __forceinline__ void vecUnit(const VecNet &n, bool plastStep, uint32_t u, uint32_t lane, const Spikes &sp,
+		const StepOf &stepOf, uint32_t *bcCnt, uint32_t *scCnt)
+{
+	const float gLeak = n.gLeak, eLeak = n.eLeak, eGOIn = n.eGOIn;
+	const float threshBase = n.threshBase, threshMax = n.threshMax, threshDecay = n.threshDecay;
+	const float gDecMF = n.gDecMF, gIncMF = n.gIncMF, gDecGO = n.gDecGO, gIncGO = n.gIncGO;
+	const uint32_t numGR = n.numGR, P = n.P, bs = n.bs, K = n.K, jGroups = n.jGroups;
+	const uint32_t bcShift = n.bcShift, scShift = n.scShift;
+	uint32_t *const goCount = n.goCount;
+	float *const vGR = n.vGR, *const gKCaGR = n.gKCaGR, *const threshGR = n.threshGR;
+	float *const gESum = n.gESum, *const gISum = n.gISum, *const wGR = n.wGR, *const pairOut = n.pairOut;
+	uint32_t *const apBufGR = n.apBufGR;
+	uint64_t *const historyGR = n.historyGR;
+	const uint16_t *const mfIdx = n.mfIdx, *const goIdx = n.goIdx, *const out16 = n.out16;
+	const uint8_t *const pfDelay = n.pfDelay;
+	const uint32_t h = lane >> 4, l = lane & 15u;
+	const uint32_t jg = u % jGroups, pk = u / jGroups, k = pk % K, pc = pk / K;
+	const uint32_t rowStart = pc * P + (2u * k + h) * bs + jg * 64u;
+	const uint32_t g = rowStart + 4u * l;  // this lane's first cell
+
+	const float4 v4 = ldState(vGR + g), gk4 = ldState(gKCaGR + g), th4 = ldState(threshGR + g);
+	const float4 gE4 = ldState(gESum + g), gI4 = ldState(gISum + g);
+	const uint4 ab4 = *reinterpret_cast<const uint4 *>(apBufGR + g);
+	uint2 mfw[kMF], gow[kGO];
+#pragma unroll
+	for (uint32_t s = 0; s < kMF; s++) mfw[s] = __ldg(reinterpret_cast<const uint2 *>(mfIdx + (size_t)s * numGR + g));
+#pragma unroll
+	for (uint32_t s = 0; s < kGO; s++) gow[s] = __ldg(reinterpret_cast<const uint2 *>(goIdx + (size_t)s * numGR + g));
+	const uint32_t dly = __ldg(reinterpret_cast<const uint32_t *>(pfDelay + g));
+	const float4 w4 = ldState(wGR + g);
+	ulonglong2 hA = make_ulonglong2(0, 0), hB = make_ulonglong2(0, 0);
+	if (plastStep) {
+		hA = *reinterpret_cast<const ulonglong2 *>(historyGR + g);
+		hB = *reinterpret_cast<const ulonglong2 *>(historyGR + g + 2);
+	}
+	const float vIn[4] = {v4.x, v4.y, v4.z, v4.w}, gkIn[4] = {gk4.x, gk4.y, gk4.z, gk4.w};
+	const float thIn[4] = {th4.x, th4.y, th4.z, th4.w}, gEIn[4] = {gE4.x, gE4.y, gE4.z, gE4.w};
+	const float gIIn[4] = {gI4.x, gI4.y, gI4.z, gI4.w}, wIn[4] = {w4.x, w4.y, w4.z, w4.w};
+	const uint32_t abIn[4] = {ab4.x, ab4.y, ab4.z, ab4.w};
+	const uint64_t hIn[4] = {hA.x, hA.y, hB.x, hB.y};
+	const float stepW = plastStep ? stepOf(pc) : 0.0f;
+
+	float vO[4], gkO[4], thO[4], gEO[4], gIO[4], wO[4], x[4];
+	uint32_t abO[4], pfCount = 0, anySpike = 0;
+	uint64_t hO[4];
+#pragma unroll
+	for (uint32_t c = 0; c < 4; c++) {
+		int cntMF = 0, cntGO = 0;
+#pragma unroll
+		for (uint32_t s = 0; s < kMF; s++) cntMF += sp.mf(half16(mfw[s], c));
+#pragma unroll
+		for (uint32_t s = 0; s < kGO; s++) cntGO += sp.go(half16(gow[s], c));
+		const float v = vIn[c], gk = gkIn[c], th = thIn[c], gE = gEIn[c], gI = gIIn[c];
+		// calcActivityGRGPU (kernels.cu:79-110)
+		const float tempV = v + (gLeak + gk * gk * gk * gk) * (eLeak - v) - (gE) * v + (gI) * (eGOIn - v);
+		const float tempThresh = th + (threshBase - th) * threshDecay;
+		const unsigned int tempAP = tempV > tempThresh;
+		thO[c] = tempAP * threshMax + (!tempAP) * tempThresh;
+		const float gkd = gk * 0.9999f;
+		gkO[c] = tempAP * (gkd + 0.003f) + (!tempAP) * gkd;
+		const uint32_t abN = (abIn[c] << 1) | tempAP;
+		abO[c] = abN;
+		anySpike |= abN;
+		vO[c] = tempV;
+		// updateGRInOPGPU for MF (this step's spikes) and GO (last step's)
+		gEO[c] = gE * gDecMF + gIncMF * (cntMF);
+		gIO[c] = gI * gDecGO + gIncGO * (cntGO);
+		// plasticity (phase 1) before this step's PF->PC output (phase 2)
+		const uint32_t d = (dly >> (8u * c)) & 0xFFu;
+		const uint32_t pf = d < 32u ? (abN >> d) & 1u : 0u;
+		pfCount += pf;
+		float w = wIn[c];
+		if (plastStep) {
+			w = w + ((hIn[c] & 0x0000008000000000ull) > 0) * stepW;
+			w = (w > 0) * w;
+			w = (w > 1) + (w <= 1) * w;
+			hO[c] = (hIn[c] << 1) | ((abN & 0x0000001Fu) > 0);
+		}
+		wO[c] = w;
+		x[c] = w * pf;
+	}
+	stState(vGR + g, vO[0], vO[1], vO[2], vO[3]);
+	stState(gKCaGR + g, gkO[0], gkO[1], gkO[2], gkO[3]);
+	stState(threshGR + g, thO[0], thO[1], thO[2], thO[3]);
+	stState(gESum + g, gEO[0], gEO[1], gEO[2], gEO[3]);
+	stState(gISum + g, gIO[0], gIO[1], gIO[2], gIO[3]);
+	*reinterpret_cast<uint4 *>(apBufGR + g) = make_uint4(abO[0], abO[1], abO[2], abO[3]);
+	if (plastStep) {
+		stState(wGR + g, wO[0], wO[1], wO[2], wO[3]);
+		*reinterpret_cast<ulonglong2 *>(historyGR + g) = make_ulonglong2(hO[0], hO[1]);
+		*reinterpret_cast<ulonglong2 *>(historyGR + g + 2) = make_ulonglong2(hO[2], hO[3]);
+	}
+	// pair sums x[i] + x[i+bs]: row 2k's lane takes row 2k+1's values
+	float q[4];
+#pragma unroll
+	for (uint32_t c = 0; c < 4; c++) q[c] = x[c] + __shfl_xor_sync(0xffffffffu, x[c], 16);
+	if (h == 0) stState(pairOut + ((size_t)pc * K + k) * bs + jg * 64u + 4u * l, q[0], q[1], q[2], q[3]);
+	// PF->BC and PF->SC counts of the 64 cells of each half (one BC and
+	// one SC block each)
+	pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 8);
+	pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 4);
+	pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 2);
+	pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 1);
+	if (l == 0 && pfCount) {
+		atomicAdd(&bcCnt[rowStart >> bcShift], pfCount);
+		atomicAdd(&scCnt[rowStart >> scShift], pfCount);
+	}
+	// GR->GO synapses whose delayed spike arrives now; the slot table
+	// is read only by lanes with a spike in their buffers
+	if (anySpike) {
+		uint2 ow[kOut];
+#pragma unroll
+		for (uint32_t s = 0; s < kOut; s++) ow[s] = __ldg(reinterpret_cast<const uint2 *>(out16 + (size_t)s * numGR + g));
+#pragma unroll
+		for (uint32_t c = 0; c < 4; c++) {
+			if (!abO[c]) continue;
+#pragma unroll
+			for (uint32_t s = 0; s < kOut; s++) {
+				const uint32_t o = half16(ow[s], c);
+				if (o != kOut16None && ((abO[c] >> (o & 31u)) & 1u)) atomicAdd(&goCount[o >> 5], 1u);
+			}
+		}
+	}
+}
+
 __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel(const DevNet *__restrict__ N,
 		uint32_t stepOffset)
 {
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
-	const uint32_t numGR = N->numGR, P = N->P, bs = N->bs, K = N->K, numPC = N->numPC;
+	const uint32_t numGR = N->numGR, bs = N->bs, K = N->K, numPC = N->numPC;
 	const uint32_t numBC = N->numBC, numSC = N->numSC;
 	const uint32_t lane = threadIdx.x & 31u;
 
@@ -165,23 +350,11 @@ __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel
 	__syncthreads();
 
 	// ---- units
-	const float gLeak = N->gLeakGR, eLeak = N->eLeakGR, eGOIn = N->eGOGR;
-	const float threshBase = N->threshRestGR, threshMax = N->threshMaxGR, threshDecay = N->threshDecGR;
-	const float gDecMF = N->gDecMFtoGR, gIncMF = N->gIncMFtoGR, gDecGO = N->gDecGOtoGR, gIncGO = N->gIncGOtoGR;
-	uint32_t *const goCount = N->goCount + (size_t)(t & 1) * N->numGO;
-	float *const vGR = N->vGR, *const gKCaGR = N->gKCaGR, *const threshGR = N->threshGR;
-	float *const gESum = N->gESum, *const gISum = N->gISum;
-	uint32_t *const apBufGR = N->apBufGR;
-	uint64_t *const historyGR = N->historyGR;
-	float *const wGR = N->zones[0].w;
-	float *const pairOut = N->zones[0].pairSum + (size_t)(t & 1) * numPC * K * bs;
-	const uint16_t *const mfIdx = N->mfIdx, *const goIdx = N->goIdx, *const out16 = N->outCon16;
-	const uint8_t *const pfDelay = N->pfDelay;
-	const uint32_t bcShift = N->bcShift, scShift = N->scShift;
-	const uint32_t jGroups = bs / 64u, U = numGR / 128u;
-	const uint32_t h = lane >> 4, l = lane & 15u;
+	const VecNet net = vecNet(N, t);
+	const SpikeBytes sp{sMF, sGO};
+	const auto stepOf = [&](uint32_t pc) { return sStep[pc]; };
+	const uint32_t U = numGR / 128u;
 	uint32_t *const claim = N->passClaim + t % 3;
-
 	uint32_t base = 0;
 	if (lane == 0) base = atomicAdd(claim, kVecClaim);
 	base = __shfl_sync(0xffffffffu, base, 0);
@@ -190,115 +363,7 @@ __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel
 		uint32_t next = 0;
 		if (lane == 0) next = atomicAdd(claim, kVecClaim);
 		const uint32_t end = min(U, base + kVecClaim);
-		for (uint32_t u = base; u < end; u++) {
-			const uint32_t jg = u % jGroups, pk = u / jGroups, k = pk % K, pc = pk / K;
-			const uint32_t rowStart = pc * P + (2u * k + h) * bs + jg * 64u;
-			const uint32_t g = rowStart + 4u * l;  // this lane's first cell
-
-			const float4 v4 = ldState(vGR + g), gk4 = ldState(gKCaGR + g), th4 = ldState(threshGR + g);
-			const float4 gE4 = ldState(gESum + g), gI4 = ldState(gISum + g);
-			const uint4 ab4 = *reinterpret_cast<const uint4 *>(apBufGR + g);
-			uint2 mfw[kMF], gow[kGO];
-#pragma unroll
-			for (uint32_t s = 0; s < kMF; s++) mfw[s] = __ldg(reinterpret_cast<const uint2 *>(mfIdx + (size_t)s * numGR + g));
-#pragma unroll
-			for (uint32_t s = 0; s < kGO; s++) gow[s] = __ldg(reinterpret_cast<const uint2 *>(goIdx + (size_t)s * numGR + g));
-			const uint32_t dly = __ldg(reinterpret_cast<const uint32_t *>(pfDelay + g));
-			const float4 w4 = ldState(wGR + g);
-			ulonglong2 hA = make_ulonglong2(0, 0), hB = make_ulonglong2(0, 0);
-			if (plastStep) {
-				hA = *reinterpret_cast<const ulonglong2 *>(historyGR + g);
-				hB = *reinterpret_cast<const ulonglong2 *>(historyGR + g + 2);
-			}
-			const float vIn[4] = {v4.x, v4.y, v4.z, v4.w}, gkIn[4] = {gk4.x, gk4.y, gk4.z, gk4.w};
-			const float thIn[4] = {th4.x, th4.y, th4.z, th4.w}, gEIn[4] = {gE4.x, gE4.y, gE4.z, gE4.w};
-			const float gIIn[4] = {gI4.x, gI4.y, gI4.z, gI4.w}, wIn[4] = {w4.x, w4.y, w4.z, w4.w};
-			const uint32_t abIn[4] = {ab4.x, ab4.y, ab4.z, ab4.w};
-			const uint64_t hIn[4] = {hA.x, hA.y, hB.x, hB.y};
-			const float stepW = sStep[pc];
-
-			float vO[4], gkO[4], thO[4], gEO[4], gIO[4], wO[4], x[4];
-			uint32_t abO[4], pfCount = 0, anySpike = 0;
-			uint64_t hO[4];
-#pragma unroll
-			for (uint32_t c = 0; c < 4; c++) {
-				int cntMF = 0, cntGO = 0;
-#pragma unroll
-				for (uint32_t s = 0; s < kMF; s++) cntMF += sMF[half16(mfw[s], c)];
-#pragma unroll
-				for (uint32_t s = 0; s < kGO; s++) cntGO += sGO[half16(gow[s], c)];
-				const float v = vIn[c], gk = gkIn[c], th = thIn[c], gE = gEIn[c], gI = gIIn[c];
-				// calcActivityGRGPU (kernels.cu:79-110)
-				const float tempV = v + (gLeak + gk * gk * gk * gk) * (eLeak - v) - (gE) * v + (gI) * (eGOIn - v);
-				const float tempThresh = th + (threshBase - th) * threshDecay;
-				const unsigned int tempAP = tempV > tempThresh;
-				thO[c] = tempAP * threshMax + (!tempAP) * tempThresh;
-				const float gkd = gk * 0.9999f;
-				gkO[c] = tempAP * (gkd + 0.003f) + (!tempAP) * gkd;
-				const uint32_t abN = (abIn[c] << 1) | tempAP;
-				abO[c] = abN;
-				anySpike |= abN;
-				vO[c] = tempV;
-				// updateGRInOPGPU for MF (this step's spikes) and GO (last step's)
-				gEO[c] = gE * gDecMF + gIncMF * (cntMF);
-				gIO[c] = gI * gDecGO + gIncGO * (cntGO);
-				// plasticity (phase 1) before this step's PF->PC output (phase 2)
-				const uint32_t d = (dly >> (8u * c)) & 0xFFu;
-				const uint32_t pf = d < 32u ? (abN >> d) & 1u : 0u;
-				pfCount += pf;
-				float w = wIn[c];
-				if (plastStep) {
-					w = w + ((hIn[c] & 0x0000008000000000ull) > 0) * stepW;
-					w = (w > 0) * w;
-					w = (w > 1) + (w <= 1) * w;
-					hO[c] = (hIn[c] << 1) | ((abN & 0x0000001Fu) > 0);
-				}
-				wO[c] = w;
-				x[c] = w * pf;
-			}
-			stState(vGR + g, vO[0], vO[1], vO[2], vO[3]);
-			stState(gKCaGR + g, gkO[0], gkO[1], gkO[2], gkO[3]);
-			stState(threshGR + g, thO[0], thO[1], thO[2], thO[3]);
-			stState(gESum + g, gEO[0], gEO[1], gEO[2], gEO[3]);
-			stState(gISum + g, gIO[0], gIO[1], gIO[2], gIO[3]);
-			*reinterpret_cast<uint4 *>(apBufGR + g) = make_uint4(abO[0], abO[1], abO[2], abO[3]);
-			if (plastStep) {
-				stState(wGR + g, wO[0], wO[1], wO[2], wO[3]);
-				*reinterpret_cast<ulonglong2 *>(historyGR + g) = make_ulonglong2(hO[0], hO[1]);
-				*reinterpret_cast<ulonglong2 *>(historyGR + g + 2) = make_ulonglong2(hO[2], hO[3]);
-			}
-			// pair sums x[i] + x[i+bs]: row 2k's lane takes row 2k+1's values
-			float q[4];
-#pragma unroll
-			for (uint32_t c = 0; c < 4; c++) q[c] = x[c] + __shfl_xor_sync(0xffffffffu, x[c], 16);
-			if (h == 0) stState(pairOut + ((size_t)pc * K + k) * bs + jg * 64u + 4u * l, q[0], q[1], q[2], q[3]);
-			// PF->BC and PF->SC counts of the 64 cells of each half (one BC and
-			// one SC block each)
-			pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 8);
-			pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 4);
-			pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 2);
-			pfCount += __shfl_xor_sync(0xffffffffu, pfCount, 1);
-			if (l == 0 && pfCount) {
-				atomicAdd(&sBC[rowStart >> bcShift], pfCount);
-				atomicAdd(&sSC[rowStart >> scShift], pfCount);
-			}
-			// GR->GO synapses whose delayed spike arrives now; the slot table
-			// is read only by lanes with a spike in their buffers
-			if (anySpike) {
-				uint2 ow[kOut];
-#pragma unroll
-				for (uint32_t s = 0; s < kOut; s++) ow[s] = __ldg(reinterpret_cast<const uint2 *>(out16 + (size_t)s * numGR + g));
-#pragma unroll
-				for (uint32_t c = 0; c < 4; c++) {
-					if (!abO[c]) continue;
-#pragma unroll
-					for (uint32_t s = 0; s < kOut; s++) {
-						const uint32_t o = half16(ow[s], c);
-						if (o != kOut16None && ((abO[c] >> (o & 31u)) & 1u)) atomicAdd(&goCount[o >> 5], 1u);
-					}
-				}
-			}
-		}
+		for (uint32_t u = base; u < end; u++) vecUnit(net, plastStep, u, lane, sp, stepOf, sBC, sSC);
 		base = __shfl_sync(0xffffffffu, next, 0);
 	}
 	__syncthreads();
@@ -312,6 +377,109 @@ __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel
 		if (!c) continue;
 		if (i < numBC) atomicAdd(&bcOut[i], c);
 		else atomicAdd(&scOut[i - numBC], c);
+	}
+}
+
+// Step t-1's PF->PC reduction of one PC of network N (one CTA): the running
+// sums over k in ascending k, kept as the partial sums, and the halving tree
+// over j, kept as the PC's input sum.
+__device__ void reducePC(const DevNet *N, uint64_t t, uint32_t pc, float *sTree)
+{
+	const uint32_t numPC = N->numPC, bs = N->bs, K = N->K;
+	const DevZone &Z0 = N->zones[0];
+	const float *pairs = Z0.pairSum + (size_t)((t - 1) & 1) * numPC * K * bs + (size_t)pc * K * bs;
+	float *part = Z0.pcPartial + (size_t)((t - 1) % 3) * numPC * bs + (size_t)pc * bs;
+	for (uint32_t j = threadIdx.x; j < bs; j += blockDim.x) {
+		float a = 0.0f;
+		for (uint32_t k0 = 0; k0 < K; k0 += 8) {
+			float q[8];
+#pragma unroll
+			for (uint32_t u = 0; u < 8; u++) q[u] = k0 + u < K ? pairs[(size_t)(k0 + u) * bs + j] : 0.0f;
+#pragma unroll
+			for (uint32_t u = 0; u < 8; u++)
+				if (k0 + u < K) a += q[u];
+		}
+		part[j] = a;
+		sTree[j] = a;
+	}
+	const float sum = blockRowTree(sTree, bs);
+	if (threadIdx.x == 0) Z0.pcSum[(size_t)((t - 1) % 3) * numPC + pc] = sum;
+	__syncthreads();
+}
+
+// The vector pass over a batch of networks of the compiled shape: one
+// persistent launch whose warps claim kVecBatchClaim units at a time from a
+// counter over the units of every network (unitOffset[n] is network n's
+// first unit, unitOffset[numNets] the total; pcOffset likewise over their
+// PCs).  Spikes are looked up in each network's spike bit words, PF->BC/SC
+// counts go to global memory, and each network's previous-step PF->PC
+// reduction is spread over the CTAs, one PC each.
+__global__ void __launch_bounds__(32 * kVecWarps, kVecBatchMinBlocks) grPassVecBatchKernel(const DevNet *const *nets,
+		const uint32_t *unitOffset, const uint32_t *pcOffset, int numNets, uint32_t stepOffset, uint32_t *claimBase)
+{
+	__shared__ float sTree[512];
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t t0 = stepsDone(nets[0]) + 1 + stepOffset;
+	if (blockIdx.x == 0) {
+		if (threadIdx.x == 0) claimBase[(t0 + 1) % 3] = 0;  // the next step's counter
+		for (int n = threadIdx.x; n < numNets; n += blockDim.x) {
+			const DevNet *N = nets[n];
+			const uint64_t t = stepsDone(N) + 1 + stepOffset;
+			N->pairStep[t & 1] = t;
+		}
+	}
+	// previous-step PF->PC reductions, one (network, PC) per CTA in turn
+	for (uint32_t q = blockIdx.x; q < pcOffset[numNets]; q += gridDim.x) {
+		uint32_t pc = 0;
+		const DevNet *N = nets[findNet(pcOffset, numNets, q, pc)];
+		const uint64_t t = stepsDone(N) + 1 + stepOffset;
+		if (N->pairStep[(t - 1) & 1] == t - 1) reducePC(N, t, pc, sTree);
+	}
+
+	const uint32_t U = unitOffset[numNets];
+	uint32_t *const claim = claimBase + t0 % 3;
+	uint32_t base = 0;
+	if (lane == 0) base = atomicAdd(claim, kVecBatchClaim);
+	base = __shfl_sync(0xffffffffu, base, 0);
+	// the current network's values per warp in shared memory (read by the
+	// unit as it needs them, not held in registers across units)
+	__shared__ VecNet sNets[kVecWarps];
+	VecNet &net = sNets[threadIdx.x >> 5];
+	int cur = -1;
+	const DevNet *N = nullptr;
+	uint64_t t = 0;
+	bool plastStep = false;
+	SpikeBits sp{nullptr, nullptr};
+	uint32_t *bcCnt = nullptr, *scCnt = nullptr;
+	while (base < U) {
+		uint32_t next = 0;
+		if (lane == 0) next = atomicAdd(claim, kVecBatchClaim);
+		const uint32_t end = min(U, base + kVecBatchClaim);
+		for (uint32_t g = base; g < end; g++) {
+			uint32_t u = 0;
+			const int lo = findNet(unitOffset, numNets, g, u);
+			if (lo != cur) {
+				cur = lo;
+				N = nets[lo];
+				t = stepsDone(N) + 1 + stepOffset;
+				__syncwarp();
+				if (lane == 0) net = vecNet(N, t);
+				__syncwarp();
+				plastStep = (t % N->tsPerHistBinGR) == 0;
+				sp = SpikeBits{N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords,
+						N->goBits + (size_t)((t - 1) & 1) * N->goWords};
+				bcCnt = N->bcCount + (size_t)(t % 3) * N->numBC;
+				scCnt = N->scCount + (size_t)(t % 3) * N->numSC;
+			}
+			const DevNet *Nc = N;
+			const uint64_t tc = t;
+			const auto stepOf = [&](uint32_t pc) {
+				const DevZone &Z0 = Nc->zones[0];
+				return plasticityStep(Nc, tc, 0, Z0.plastSel[(tc & 1) * Nc->numIO + Z0.ioOfPC[pc]]);
+			};
+			vecUnit(net, plastStep, u, lane, sp, stepOf, bcCnt, scCnt);
+		}
+		base = __shfl_sync(0xffffffffu, next, 0);
 	}
 }
 
@@ -338,6 +506,8 @@ __global__ void pcTreeKernel(const DevNet *__restrict__ N, uint64_t t)
 	const float sum = blockRowTree(sTree, bs);
 	if (threadIdx.x == 0) N->zones[0].pcSum[(size_t)(t % 3) * numPC + pc] = sum;
 }
+
+const void *passVecBatchKernel() { return (const void *)&grPassVecBatchKernel; }
 
 bool passVecCapable(const DevNet &h)
 {

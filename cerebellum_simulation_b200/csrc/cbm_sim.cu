@@ -1167,7 +1167,9 @@ Simulator::~Simulator()
 	if (hExport_) cudaFreeHost(hExport_);
 	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
-	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_, &dCellOffset_}) if (b->ptr) cudaFree(b->ptr);
+	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_, &dCellOffset_, &dVecUnitOffset_,
+			&dVecPcOffset_, &dVecClaim_})
+		if (b->ptr) cudaFree(b->ptr);
 	if (s0_) cudaStreamDestroy(s0_);
 	if (s1_) cudaStreamDestroy(s1_);
 	for (cudaEvent_t e : {fork_, join_, ev0_, ev1_, tev0_, tev1_}) if (e) cudaEventDestroy(e);
@@ -1254,14 +1256,16 @@ std::vector<PassGeometry> Simulator::passCandidates() const
 	// the default first: 4 consumer warps of 1 row, 4 stages, 4 CTAs/SM,
 	// slot loops for at most 4 slots (8,1,3,2 with open slot loops past 4)
 	std::vector<PassGeometry> out;
-	// the vector pass first where it applies (single network of the compiled
-	// shape); CBM_PASS_VEC=0 leaves it out
+	// the vector pass where it applies (networks of the compiled shape):
+	// first for one network, after the per-tile default for a batch;
+	// CBM_PASS_VEC=0 leaves it out, CBM_PASS_VEC=1 puts it first for a batch
 	const char *vecEnv = getenv("CBM_PASS_VEC");
-	if (nets_.size() == 1 && passVecCapable(nets_[0]->dev()) && !(vecEnv && !strcmp(vecEnv, "0"))) {
-		PassGeometry v;
-		v.kind = 3;
-		out.push_back(v);
-	}
+	bool vec = !nets_.empty() && !(vecEnv && !strcmp(vecEnv, "0"));
+	for (Network *n : nets_) vec = vec && passVecCapable(n->dev());
+	PassGeometry v;
+	v.kind = 3;
+	const bool vecFirst = vec && (nets_.size() == 1 || (vecEnv && !strcmp(vecEnv, "1")));
+	if (vecFirst) out.push_back(v);
 	bool tma = !nets_.empty();
 	uint32_t minRows = UINT32_MAX, maxSlots = 0;
 	for (Network *n : nets_) {
@@ -1275,6 +1279,7 @@ std::vector<PassGeometry> Simulator::passCandidates() const
 		if (maxSlots <= 4) { d.W = 4; d.RW = 1; d.S = 4; d.B = 4; d.M = 4; }
 		else { d.W = 8; d.RW = 1; d.S = 3; d.B = 2; d.M = 0; }
 		if ((uint32_t)(d.W * d.RW) <= minRows) out.push_back(d);
+		if (vec && !vecFirst) out.push_back(v);
 		for (int i = 0; i < passTmaConfigCount(); i++) {
 			PassGeometry c;
 			c.kind = 1;
@@ -1284,6 +1289,7 @@ std::vector<PassGeometry> Simulator::passCandidates() const
 			out.push_back(c);
 		}
 	}
+	if (vec && !vecFirst && !tma) out.push_back(v);
 	PassGeometry plain;
 	plain.kind = 0;
 	out.push_back(plain);
@@ -1305,10 +1311,51 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 	for (Network *n : nets_) { n->outBytes_ = 4; n->outPlanes_ = n->dev().nOutSlots; n->ovUsed_ = 0; }
 	// leaving the vector pass: the last step's PF->PC reduction is still pair
 	// sums, and the small-cell update goes back to partial sums
-	if (passVec_ && g.kind != 3 && nets_.size() == 1) CKS(nets_[0]->setPcSumMode(false, s0_));
+	if (passVec_ && g.kind != 3)
+		for (Network *n : nets_) CKS(n->setPcSumMode(false, s0_));
+	if (g.kind == 3 && nets_.size() > 1) {
+		for (Network *n : nets_)
+			if (!passVecCapable(n->dev())) return "the vector GR pass runs networks of its compiled shape";
+		const void *fn = passVecBatchKernel();
+		if (!dVecUnitOffset_.ptr) {
+			std::vector<uint32_t> units(1, 0), pcs(1, 0);
+			for (Network *n : nets_) {
+				units.push_back(units.back() + n->dev().numGR / 128u);
+				pcs.push_back(pcs.back() + n->dev().numPC);
+			}
+			auto up = [&](DeviceBuf &b, const std::vector<uint32_t> &v) -> std::string {
+				CK(cudaMalloc(&b.ptr, v.size() * sizeof(uint32_t)), "allocating vector-pass tables");
+				b.bytes = v.size() * sizeof(uint32_t);
+				CK(cudaMemcpy(b.ptr, v.data(), b.bytes, cudaMemcpyHostToDevice), "uploading vector-pass tables");
+				return "";
+			};
+			CKS(up(dVecUnitOffset_, units));
+			CKS(up(dVecPcOffset_, pcs));
+			CKS(up(dVecClaim_, std::vector<uint32_t>(4, 0)));
+		}
+		int perSM = 0, numSMs = 0;
+		CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, 32 * kVecWarps, 0), "pass occupancy");
+		CK(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device_), "SM count");
+		uint32_t units = 0;
+		for (Network *n : nets_) units += n->dev().numGR / 128u;
+		const uint32_t claims = (units + kVecBatchClaim - 1) / kVecBatchClaim;
+		passGrid_ = std::max<uint32_t>(1, std::min<uint32_t>((claims + kVecWarps - 1) / kVecWarps,
+				(uint32_t)std::max(1, perSM) * (uint32_t)numSMs));
+		CK(cudaMemset(dVecClaim_.ptr, 0, dVecClaim_.bytes), "pass claim counters");
+		for (Network *n : nets_) CKS(n->setPcSumMode(true, s0_));
+		passTmaFn_ = fn;
+		passVec_ = true;
+		passPersistent_ = false;
+		passTmaW_ = kVecWarps - 1;
+		passTmaR_ = passTmaS_ = 0;
+		passTmaSmem_ = 0;
+		passGeom_ = g;
+		dropGraphs();
+		return "";
+	}
 	if (g.kind == 3) {
 		if (nets_.size() != 1 || !passVecCapable(nets_[0]->dev()))
-			return "the vector GR pass runs one network of its compiled shape";
+			return "the vector GR pass runs networks of its compiled shape";
 		Network &n = *nets_[0];
 		const size_t smem = passVecSmemBytes(n.dev());
 		const void *fn = passVecKernel();
@@ -1430,7 +1477,11 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 			// vector pass takes it alone
 			void *argsTma[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg};
 			void *argsVec[] = {&net0Arg, &stepArg};
-			void **args = passVec_ ? argsVec : argsTma;
+			const uint32_t *unitOffArg = (const uint32_t *)dVecUnitOffset_.ptr;
+			const uint32_t *pcOffArg = (const uint32_t *)dVecPcOffset_.ptr;
+			uint32_t *claimArg = (uint32_t *)dVecClaim_.ptr;
+			void *argsVecBatch[] = {&netsArg, &unitOffArg, &pcOffArg, &numNetsArg, &stepArg, &claimArg};
+			void **args = !passVec_ ? argsTma : nets_.size() == 1 ? argsVec : argsVecBatch;
 			cudaLaunchConfig_t cfg = {};
 			cfg.gridDim = dim3(passGrid_);
 			cfg.blockDim = dim3(32 * (passTmaW_ + 1));

@@ -139,6 +139,9 @@ private:
 	cudaEvent_t fork_ = nullptr, join_ = nullptr, ev0_ = nullptr, ev1_ = nullptr, tev0_ = nullptr, tev1_ = nullptr;
 	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_, dStageBytes_;
 	DeviceBuf dCellOffset_;   // trialDataBatchKernel's instance map (batches recording trial data)
+	// the batched vector pass: first 128-cell unit and first PC of each
+	// network (numNets + 1 prefix sums each), and its three claim counters
+	DeviceBuf dVecUnitOffset_, dVecPcOffset_, dVecClaim_;
 	uint32_t cellTotal_ = 0;
 	uint32_t passBlocks_ = 0;
 	size_t passSmem_ = 0, tailSmem_ = 0;

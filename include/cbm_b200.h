@@ -387,6 +387,10 @@ int cbm_batch_run(cbm_batch *b, uint64_t nsteps, uint32_t graphChunk, float *gpu
  * advance) over nsteps steps each, and keep the fastest.  *choice receives
  * "kind,W,RW,S,B,M" and *ms its time; either may be NULL. */
 int cbm_batch_autotune(cbm_batch *b, uint32_t nsteps, char *choice, size_t choiceLen, float *ms);
+/* cbm_sim_pass_geometry for a batch's one GR-pass launch.  No counterpart in
+ * the reference. */
+int cbm_batch_pass_geometry(cbm_batch *b, unsigned *kind, unsigned *consumerWarps, unsigned *rowsPerStage,
+		unsigned *stages);
 uint64_t cbm_batch_trial_record_bytes(cbm_batch *b, unsigned instance, int kind);
 int cbm_batch_trial_record(cbm_batch *b, unsigned instance, int kind, void *dst, uint64_t bytes);
 /* Record instance i's ECTrialsData (as cbm_sim_record_trial_data, from the
@@ -425,7 +429,8 @@ double cbm_sim_algorithmic_bytes_per_step(cbm_sim *sim);
 double cbm_sim_layout_bytes_per_step(cbm_sim *sim);
 
 /* Which GR-pass kernel runs: *kind 0 = plain (one warp-row per load), 1 =
- * TMA-pipelined per tile, 2 = TMA-pipelined persistent; *consumerWarps,
+ * TMA-pipelined per tile, 2 = TMA-pipelined persistent, 3 = vector pass
+ * (four cells per lane, claimed 128-cell units); *consumerWarps,
  * *rowsPerStage, *stages describe the TMA pipeline (0 for the plain kernel).
  * No counterpart in the reference. */
 int cbm_sim_pass_geometry(cbm_sim *sim, unsigned *kind, unsigned *consumerWarps, unsigned *rowsPerStage,

@@ -2,6 +2,8 @@
 parameters advanced together, each under its own device protocol, give for
 every instance the records and final state the oracle gives for that
 instance alone; the autotuner's switch of GR-pass kernel keeps that."""
+import os
+
 import numpy as np
 import pytest
 
@@ -71,7 +73,7 @@ def test_batch_autotune_keeps_results(tmp_path):
     b.run(150, 50)
     choice, ms = b.autotune(50)
     kind = int(choice.split(",")[0])
-    assert kind in (0, 1) and ms > 0
+    assert kind in (0, 1, 3) and ms > 0
     b.run(2 * protos[0]["trialSteps"] - 150, 50)
     _check_instances(b, [cbmtest.golden_state("ref16k", str(tmp_path))] + paths[1:], protos, rates,
                      2 * protos[0]["trialSteps"], tmp_path, "b")
@@ -140,3 +142,65 @@ def test_batch_trial_data_matches_instances_alone(tmp_path):
         assert want["psh"]["go"].any() and want["raster"]["go"].any()
     with pytest.raises(cbm.CBMError):
         b.trial_data(1)
+
+
+def _vec_batch(paths, protos, rates, steps, vec_env, tmp_path, tag):
+    """Run a batch with CBM_PASS_VEC set as given at its construction; the
+    pass kernel in use, every instance's records and final state bytes."""
+    import cerebellum_simulation_b200 as cbm
+    old = os.environ.get("CBM_PASS_VEC")
+    os.environ["CBM_PASS_VEC"] = vec_env
+    try:
+        b = cbm.CBMBatch([cbm.CBMState(p) for p in paths], [[60 + i] for i in range(len(paths))], device=0)
+    finally:
+        if old is None:
+            del os.environ["CBM_PASS_VEC"]
+        else:
+            os.environ["CBM_PASS_VEC"] = old
+    for i in range(len(paths)):
+        b.set_eyelid_protocol(i, rates[i], **protos[i])
+    b.run(steps, 50)
+    out = []
+    for i in range(len(paths)):
+        fin = str(tmp_path / f"{tag}{i}.state")
+        b.writeToState(i, fin)
+        with open(fin, "rb") as f:
+            out.append((b.trial_record(i, "nc").copy(), b.trial_record(i, "pc").copy(),
+                        b.trial_record(i, "eyelid").copy(), f.read()))
+    kind = b.pass_geometry()[0]
+    b.close()
+    return kind, out
+
+
+def test_batch_vector_pass_matches_per_tile_pass(tmp_path):
+    """The batched vector pass (one persistent launch whose warps claim
+    128-cell units across every instance; each instance's previous-step
+    PF->PC reduction spread over the CTAs) gives every instance the records
+    and final state, bit for bit, that the batch's per-tile pass gives (the
+    per-tile pass is pinned to the oracle above): 131,072, 262,144 and
+    524,288 GR of the eyelid shape with different GO thresholds and LTD
+    steps, two 400-step trials moving PF->PC weights."""
+    from cerebellum_simulation_b200 import networks
+    import cerebellum_simulation_b200 as cbm
+    paths, protos = [], []
+    for i, (gx, gy, go_scale, ltd_scale) in enumerate([(9, 8, 1.0, 1.0), (10, 8, 0.9, 1.5), (10, 9, 1.1, 0.6)]):
+        st = networks.build_random_network(gx, gy, 5, 5, 10, networks.act_params("dense"), seed=80 + i,
+                                           go_out_per_gr=4, mf_per_go=16, vel=147)
+        st.setActParam("threshBaseGO", st.act("threshBaseGO") * go_scale)
+        p = str(tmp_path / f"v{i}.state")
+        st.writeState(p)
+        del st
+        paths.append(p)
+        protos.append(cbmtest.short_protocol(mfSeed=71 + i, plastLTD=-0.004 * ltd_scale, numDataTrials=2))
+    rates = [cbmtest.protocol_rates(cbm.CBMState(p).con("numMF"), seed=30 + i) for i, p in enumerate(paths)]
+    steps = 2 * protos[0]["trialSteps"]
+    kind_vec, got = _vec_batch(paths, protos, rates, steps, "1", tmp_path, "vec")
+    kind_tile, want = _vec_batch(paths, protos, rates, steps, "0", tmp_path, "tile")
+    assert kind_vec == "grPassVecBatchKernel" and kind_tile == "grPassTmaKernel"
+    for i in range(len(paths)):
+        for k, name in enumerate(("nc", "pc", "eyelid")):
+            assert np.array_equal(got[i][k], want[i][k]), (i, name)
+        assert got[i][3] == want[i][3], f"instance {i}: final state differs"
+        w0 = cbm.CBMState(paths[i]).array("pfSynWeightPC", 0)
+        w1 = cbm.CBMState(str(tmp_path / f"vec{i}.state")).array("pfSynWeightPC", 0)
+        assert (w1 != w0).any(), f"instance {i}: no PF->PC weight moved"
