@@ -675,7 +675,7 @@ def main():
     st = networks.config2_network(seed=replicas.replica_seed(args.seed, rank))
     mf = networks.eyelid_mf_stream(1024, plan["rows"], seed=replicas.replica_seed(args.seed, rank))
     sim = cbm.CBMSimCore(st, [replicas.replica_seed(7, rank)], device=device, resident_steps=total_steps)
-    bits = cbm.mf_bits(mf, sim.mf_words())
+    bits = cbm.mf_bits(mf[:total_steps], sim.mf_words())  # the ring holds the main run's rows only
     sim.load_mf_stream(bits)
 
     # warm-up, then flush L2 before the timed region
