@@ -239,6 +239,7 @@ struct DevNet {
 	// ---- step pipeline
 	uint64_t *pairStep;  // [2] the step whose PF->PC pair sums each pairSum slot holds (vector GR pass)
 	uint32_t *passClaim; // [3] work counters of the vector GR pass, per step mod 3
+	uint32_t *pcDone;    // [numPC] reduction chunks of the previous step done per PC (vector GR pass)
 	uint32_t *goCount;   // [2][numGO] GR->GO input counts per step parity
 	uint32_t *bcCount;   // [3][numBC] PF->BC counts
 	uint32_t *scCount;   // [3][numSC] PF->SC counts

@@ -1810,21 +1810,33 @@ __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 		if ((threadIdx.x & 31u) == 0 && i < 32u * words) bits[i >> 5] = word;
 	}
 	if (threadIdx.x == 0) {
-		int32_t *ps = P->plastState;  // the eyelid driver's grPCPlastSet, grPCPlastReset
-		float *cur = P->curSteps;     // zone 0's LTD and LTP steps in force
-		if (time >= P->csOn + P->plastOn && !ps[0] && csTrial && time < P->csOff + P->plastOff) {
-			ps[0] = 1; ps[1] = 0;
-			cur[0] = P->plastLTD; cur[1] = P->plastLTP;
+		// every value loaded first, then the stores: one round trip
+		int32_t *const ps = P->plastState;  // the eyelid driver's grPCPlastSet, grPCPlastReset
+		float *const cur = P->curSteps;     // zone 0's LTD and LTP steps in force
+		float *const slot = P->ctlSlots + ((t + 1) & 1) * 3;  // step t reads the other parity's slot
+		const int32_t csOn = P->csOn, csOff = P->csOff, plastOn = P->plastOn, plastOff = P->plastOff;
+		const float plastLTD = P->plastLTD, plastLTP = P->plastLTP, defaultLTD = P->defaultLTD,
+			defaultLTP = P->defaultLTP, usErrDrive = P->usErrDrive;
+		int32_t set = ps[0], reset = ps[1];
+		float ltd = cur[0], ltp = cur[1];
+		bool changed = false;
+		if (time >= csOn + plastOn && !set && csTrial && time < csOff + plastOff) {
+			set = 1; reset = 0;
+			ltd = plastLTD; ltp = plastLTP;
+			changed = true;
 		}
-		if (!ps[1] && time >= P->csOff + P->plastOff && csTrial) {
-			ps[0] = 0; ps[1] = 1;
-			cur[0] = P->defaultLTD; cur[1] = P->defaultLTP;
+		if (!reset && time >= csOff + plastOff && csTrial) {
+			set = 0; reset = 1;
+			ltd = defaultLTD; ltp = defaultLTP;
+			changed = true;
 		}
-		// step t reads the other parity's slot while this one is written
-		float *slot = P->ctlSlots + ((t + 1) & 1) * 3;
-		slot[0] = cur[0];
-		slot[1] = cur[1];
-		slot[2] = (time == P->csOff - 1 && csTrial) ? P->usErrDrive : 0.0f;
+		if (changed) {
+			ps[0] = set; ps[1] = reset;
+			cur[0] = ltd; cur[1] = ltp;
+		}
+		slot[0] = ltd;
+		slot[1] = ltp;
+		slot[2] = (time == csOff - 1 && csTrial) ? usErrDrive : 0.0f;
 	}
 }
 
@@ -1836,38 +1848,58 @@ __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 // (ECTrialsData's PSH and eyelid trace, ecmanagementdelay.cpp:239-273).
 __device__ void protocolRecord(const DevNet *__restrict__ N, uint64_t t)
 {
-	DevProtocol *P = N->proto;
-	if (t < P->startT + 1) return;
-	const uint64_t k = t - 1 - P->startT;
-	const int32_t time = (int32_t)(k % P->trialSteps);
-	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const DevProtocol *P = N->proto;
+	// every field is read before anything is written, so that the loads go
+	// out together rather than one round trip after each store
+	const uint64_t startT = P->startT;
+	const uint32_t trialSteps = P->trialSteps, dataStart = P->dataStartTrial, numData = P->numDataTrials;
+	const uint32_t recLen = P->recLen, binSteps = P->binSteps, nBins = P->nBins;
+	const int32_t recFrom = P->recFrom;
+	if (t < startT + 1) return;
+	const uint64_t k = t - 1 - startT;
+	const int32_t time = (int32_t)(k % trialSteps);
+	const uint32_t trial = (uint32_t)(k / trialSteps);
 	const DevZone &Q = N->zones[0];
-	const int32_t ct = time - P->recFrom;
-	const bool rec = trial >= P->dataStartTrial && trial < P->dataStartTrial + P->numDataTrials && ct >= 0 &&
-		ct < P->recLen;
-	const uint32_t dt = trial - P->dataStartTrial;
-	if (threadIdx.x == 0) {
+	const int32_t ct = time - recFrom;
+	const bool rec = trial >= dataStart && trial < dataStart + numData && ct >= 0 && ct < (int32_t)recLen;
+	const uint32_t dt = trial - dataStart;
+	const uint32_t numNC = N->numNC, numPC = N->numPC;
+	if (threadIdx.x < 32) {
+		// the integrator: lane i's conductance, then lane 0 sums them in
+		// order i = 0, 1, ... as the reference's loop does
+		const uint32_t lane = threadIdx.x;
+		const float decay = P->eyeGDecay, inc = P->eyeGInc, shift = P->eyeGShift, leak = P->eyeGLeak,
+			maxAmp = P->eyeMaxAmp;
+		float *const eyeG = P->eyeG, *const eyeVm = P->eyeVm, *const eyelid = P->eyelid;
+		const float vm0 = lane == 0 ? *eyeVm : 0.0f;
 		float gSum = 0;
-		for (uint32_t i = 0; i < N->numNC; i++) {
-			float g = P->eyeG[i];
-			g = g * P->eyeGDecay;
-			g = g + Q.apNC[i] * P->eyeGInc;
-			P->eyeG[i] = g;
-			gSum += g;
+		for (uint32_t i0 = 0; i0 < numNC; i0 += 32) {
+			const uint32_t i = i0 + lane;
+			float g = 0;
+			if (i < numNC) {
+				g = eyeG[i];
+				g = g * decay;
+				g = g + Q.apNC[i] * inc;
+				eyeG[i] = g;
+			}
+			const uint32_t n = min(32u, numNC - i0);
+			for (uint32_t q = 0; q < n; q++) gSum += __shfl_sync(0xffffffffu, g, q);
 		}
-		gSum = gSum + P->eyeGShift;
-		gSum = (gSum > 0) * gSum;
-		float vm = *P->eyeVm;
-		vm = vm + (P->eyeGLeak * (0 - vm)) + (gSum * (P->eyeMaxAmp - vm));
-		*P->eyeVm = vm;
-		if (rec) P->eyelid[(size_t)dt * P->recLen + ct] = vm;
+		if (lane == 0) {
+			gSum = gSum + shift;
+			gSum = (gSum > 0) * gSum;
+			float vm = vm0;
+			vm = vm + (leak * (0 - vm)) + (gSum * (maxAmp - vm));
+			*eyeVm = vm;
+			if (rec) eyelid[(size_t)dt * recLen + ct] = vm;
+		}
 	}
 	if (rec) {
-		const uint32_t bin = (uint32_t)ct / P->binSteps;
-		const uint32_t numNC = N->numNC, numPC = N->numPC;
+		const uint32_t bin = (uint32_t)ct / binSteps;
+		uint32_t *const ncPSH = P->ncPSH, *const pcPSH = P->pcPSH;
 		for (uint32_t i = threadIdx.x; i < numNC + numPC; i += blockDim.x) {
-			if (i < numNC) P->ncPSH[((size_t)dt * P->nBins + bin) * numNC + i] += Q.apNC[i];
-			else P->pcPSH[((size_t)dt * P->nBins + bin) * numPC + (i - numNC)] += Q.apPC[i - numNC];
+			if (i < numNC) ncPSH[((size_t)dt * nBins + bin) * numNC + i] += Q.apNC[i];
+			else pcPSH[((size_t)dt * nBins + bin) * numPC + (i - numNC)] += Q.apPC[i - numNC];
 		}
 	}
 }

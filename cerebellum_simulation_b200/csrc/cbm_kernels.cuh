@@ -27,9 +27,10 @@ void passTmaConfig(int i, int *W, int *RW, int *S, int *B, int *M);
 // 32 * (W + 1) threads, the grPassKernel arguments with one network.
 const void *passPersistentKernelFor(int W, int S, int B, int M);
 // Vector GR pass (cbm_pass_vec.cu): single network of the compiled shape,
-// kVecWarps warps per CTA, persistent grid, arguments (descriptor,
-// stepOffset), passVecSmemBytes of dynamic shared memory.  Units of
-// kVecClaim x 128 cells are claimed from DevNet::passClaim.
+// kVecWarps warps per CTA, arguments (descriptor, stepOffset, units per
+// claim), passVecSmemBytes of dynamic shared memory.  The first
+// passVecReduceCTAs CTAs take the previous step's PF->PC reduction; the
+// others are persistent and claim units of 128 cells from DevNet::passClaim.
 constexpr int kVecWarps = 8;
 constexpr int kVecMinBlocks = 3;
 constexpr uint32_t kVecClaim = 2;
@@ -40,6 +41,7 @@ constexpr int kVecBatchMinBlocks = 2;
 const void *passVecBatchKernel();
 bool passVecCapable(const DevNet &h);
 size_t passVecSmemBytes(const DevNet &h);
+uint32_t passVecReduceCTAs(const DevNet &h);
 const void *passVecKernel();
 // pairReduceKernel(N, t): step t's PF->PC running sums from its pair sums
 // (numPC * bs threads), for a switch away from the vector pass.

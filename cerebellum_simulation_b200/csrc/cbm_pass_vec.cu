@@ -169,6 +169,10 @@ __device__ __forceinline__ void vecUnit(const VecNet &n, bool plastStep, uint32_
 #pragma unroll
 	for (uint32_t s = 0; s < kGO; s++) gow[s] = __ldg(reinterpret_cast<const uint2 *>(goIdx + (size_t)s * numGR + g));
 	const uint32_t dly = __ldg(reinterpret_cast<const uint32_t *>(pfDelay + g));
+	// the GR->GO slot words on their way to L2 with the rest (most warps
+	// have a lane with a spike in its 32-step buffer and read them below)
+#pragma unroll
+	for (uint32_t s = 0; s < kOut; s++) asm volatile("prefetch.global.L2 [%0];" ::"l"(out16 + (size_t)s * numGR + g));
 	const float4 w4 = ldState(wGR + g);
 	ulonglong2 hA = make_ulonglong2(0, 0), hB = make_ulonglong2(0, 0);
 	if (plastStep) {
@@ -247,8 +251,8 @@ __device__ __forceinline__ void vecUnit(const VecNet &n, bool plastStep, uint32_
 		atomicAdd(&bcCnt[rowStart >> bcShift], pfCount);
 		atomicAdd(&scCnt[rowStart >> scShift], pfCount);
 	}
-	// GR->GO synapses whose delayed spike arrives now; the slot table
-	// is read only by lanes with a spike in their buffers
+	// GR->GO synapses whose delayed spike arrives now (lanes with a spike in
+	// their buffers)
 	if (anySpike) {
 		uint2 ow[kOut];
 #pragma unroll
@@ -265,22 +269,91 @@ __device__ __forceinline__ void vecUnit(const VecNet &n, bool plastStep, uint32_
 	}
 }
 
+// Step t-1's PF->PC reduction, one (PC, 64-j chunk) task per warp: lanes
+// take two consecutive j each, the running sums over k, in ascending k, of
+// the stored pair sums (the reference's tempSum += x[i] + x[i+bs],
+// kernels.cu:326-362), kept as the partial sums; the warp that completes a
+// PC's last chunk (a counter per PC) then takes the halving tree over the
+// PC's bs partial sums in registers (lane l holds partials l + 32 m, so every
+// level of stride 32 or more pairs values of one lane) and stores the PC's
+// input sum.
+__device__ void reduceChunk(const DevNet *__restrict__ N, uint64_t t, uint32_t task, uint32_t lane)
+{
+	const uint32_t numPC = N->numPC, bs = N->bs, K = N->K;
+	const uint32_t chunks = bs / 64u, pc = task / chunks, j = (task % chunks) * 64u + 2u * lane;
+	const DevZone &Z0 = N->zones[0];
+	const float *src = Z0.pairSum + (size_t)((t - 1) & 1) * numPC * K * bs + (size_t)pc * K * bs + j;
+	float *part = Z0.pcPartial + (size_t)((t - 1) % 3) * numPC * bs + (size_t)pc * bs;
+	float a0 = 0.0f, a1 = 0.0f;
+	for (uint32_t k0 = 0; k0 < K; k0 += 16) {
+		float2 q[16];
+#pragma unroll
+		for (uint32_t u = 0; u < 16; u++)
+			q[u] = k0 + u < K ? __ldcg(reinterpret_cast<const float2 *>(src + (size_t)(k0 + u) * bs))
+				: make_float2(0.0f, 0.0f);
+#pragma unroll
+		for (uint32_t u = 0; u < 16; u++)
+			if (k0 + u < K) { a0 += q[u].x; a1 += q[u].y; }
+	}
+	*reinterpret_cast<float2 *>(part + j) = make_float2(a0, a1);
+	__threadfence();
+	uint32_t prev = 0;
+	if (lane == 0) prev = atomicAdd(&N->pcDone[pc], 1u);
+	prev = __shfl_sync(0xffffffffu, prev, 0);
+	if (prev != chunks - 1) return;
+	__threadfence();
+	const uint32_t m = bs / 32u;  // partials per lane: 2, 4, 8 or 16
+	float v[16];
+#pragma unroll
+	for (uint32_t i = 0; i < 16; i++) v[i] = i < m ? __ldcg(part + 32u * i + lane) : 0.0f;
+#pragma unroll
+	for (uint32_t hm = 8; hm >= 1; hm /= 2) {
+		if (2u * hm <= m) {
+#pragma unroll
+			for (uint32_t i = 0; i < hm; i++) v[i] = v[i] + v[i + hm];
+		}
+	}
+	float x = v[0];
+	x = x + __shfl_down_sync(0xffffffffu, x, 16);
+	x = x + __shfl_down_sync(0xffffffffu, x, 8);
+	x = x + __shfl_down_sync(0xffffffffu, x, 4);
+	x = x + __shfl_down_sync(0xffffffffu, x, 2);
+	x = x + __shfl_down_sync(0xffffffffu, x, 1);
+	if (lane == 0) {
+		Z0.pcSum[(size_t)((t - 1) % 3) * numPC + pc] = x;
+		N->pcDone[pc] = 0;  // for the next step's pass
+	}
+}
+
+// CTAs of the vector pass that take step t-1's reduction (the first ones of
+// the grid, one task per warp); the others take units.
+__host__ __device__ __forceinline__ uint32_t vecReduceCTAs(uint32_t numPC, uint32_t bs)
+{
+	return (numPC * (bs / 64u) + kVecWarps - 1) / kVecWarps;
+}
+
 __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel(const DevNet *__restrict__ N,
-		uint32_t stepOffset)
+		uint32_t stepOffset, uint32_t claimSize)
 {
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
-	const uint32_t numGR = N->numGR, bs = N->bs, K = N->K, numPC = N->numPC;
-	const uint32_t numBC = N->numBC, numSC = N->numSC;
+	const uint32_t numGR = N->numGR, numPC = N->numPC, bs = N->bs;
 	const uint32_t lane = threadIdx.x & 31u;
+
+	// the reduction CTAs: one task per warp, then done (their slots go to
+	// the unit CTAs that did not fit at launch)
+	const uint32_t redCTAs = vecReduceCTAs(numPC, bs);
+	if (blockIdx.x < redCTAs) {
+		const uint32_t task = blockIdx.x * kVecWarps + (threadIdx.x >> 5);
+		if (task < numPC * (bs / 64u) && N->pairStep[(t - 1) & 1] == t - 1) reduceChunk(N, t, task, lane);
+		return;
+	}
+	const uint32_t cta = blockIdx.x - redCTAs;
 
 	extern __shared__ __align__(16) uint8_t vecSmem[];
 	const uint32_t mfWords = N->mfWords, goWords = N->goWords;
 	uint8_t *sMF = vecSmem;                       // this step's MF spikes, a byte per fibre
 	uint8_t *sGO = sMF + 32u * mfWords;           // last step's GO spikes, a byte per cell
 	float *sStep = reinterpret_cast<float *>(sGO + ((32u * goWords + 15u) & ~15u));  // PF->PC step per PC
-	uint32_t *sBC = reinterpret_cast<uint32_t *>(sStep + numPC);                      // PF->BC counts
-	uint32_t *sSC = sBC + numBC;                                                      // PF->SC counts
-	float *sTree = reinterpret_cast<float *>(sSC + numSC);                            // one PC's bs partial sums
 
 	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
 
@@ -305,46 +378,9 @@ __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel
 			if (plastStep) s = plasticityStep(N, t, 0, Z0.plastSel[(t & 1) * N->numIO + Z0.ioOfPC[pc]]);
 			sStep[pc] = s;
 		}
-		for (uint32_t i = threadIdx.x; i < numBC + numSC; i += blockDim.x) sBC[i] = 0;
-		if (blockIdx.x == 0 && threadIdx.x == 0) {
+		if (cta == 0 && threadIdx.x == 0) {
 			N->passClaim[(t + 1) % 3] = 0;  // the next step's counter (last used two steps ago)
 			N->pairStep[t & 1] = t;         // read by the next step's pass, after this one ends
-		}
-	}
-	// Step t-1's PF->PC reduction, one PC per CTA (CTAs 0 .. numPC-1): the
-	// running sum over k of every j in ascending k (tempSum += x[i] +
-	// x[i+bs]), kept as the partial sums, then the halving tree over j, kept
-	// as the PC's input sum for the small-cell update.
-	if (N->pairStep[(t - 1) & 1] == t - 1) {
-		const DevZone &Z0 = N->zones[0];
-		const float *pairs = Z0.pairSum + (size_t)((t - 1) & 1) * numPC * K * bs;
-		float *part = Z0.pcPartial + (size_t)((t - 1) % 3) * numPC * bs;
-		for (uint32_t pc = blockIdx.x; pc < numPC; pc += gridDim.x) {
-			for (uint32_t j0 = 0; j0 < bs; j0 += 2u * blockDim.x) {
-				const uint32_t ja = j0 + threadIdx.x, jb = ja + blockDim.x;
-				const float *sa = pairs + (size_t)pc * K * bs + ja, *sb = pairs + (size_t)pc * K * bs + jb;
-				float a = 0.0f, b = 0.0f;
-				for (uint32_t k0 = 0; k0 < K; k0 += 8) {
-					float qa[8], qb[8];
-#pragma unroll
-					for (uint32_t u = 0; u < 8; u++) {
-						const bool in = k0 + u < K;
-						qa[u] = in && ja < bs ? sa[(size_t)(k0 + u) * bs] : 0.0f;
-						qb[u] = in && jb < bs ? sb[(size_t)(k0 + u) * bs] : 0.0f;
-					}
-#pragma unroll
-					for (uint32_t u = 0; u < 8; u++) {
-						if (k0 + u < K) { a += qa[u]; b += qb[u]; }
-					}
-				}
-				if (ja < bs) { part[(size_t)pc * bs + ja] = a; sTree[ja] = a; }
-				if (jb < bs) { part[(size_t)pc * bs + jb] = b; sTree[jb] = b; }
-			}
-			const float sum = blockRowTree(sTree, bs);
-			if (threadIdx.x == 0) {
-				Z0.pcSum[(size_t)((t - 1) % 3) * numPC + pc] = sum;
-			}
-			__syncthreads();
 		}
 	}
 	__syncthreads();
@@ -353,30 +389,20 @@ __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel
 	const VecNet net = vecNet(N, t);
 	const SpikeBytes sp{sMF, sGO};
 	const auto stepOf = [&](uint32_t pc) { return sStep[pc]; };
+	uint32_t *const bcOut = N->bcCount + (size_t)(t % 3) * N->numBC;
+	uint32_t *const scOut = N->scCount + (size_t)(t % 3) * N->numSC;
 	const uint32_t U = numGR / 128u;
 	uint32_t *const claim = N->passClaim + t % 3;
 	uint32_t base = 0;
-	if (lane == 0) base = atomicAdd(claim, kVecClaim);
+	if (lane == 0) base = atomicAdd(claim, claimSize);
 	base = __shfl_sync(0xffffffffu, base, 0);
 	while (base < U) {
 		// the next claim's round trip overlaps this one's units
 		uint32_t next = 0;
-		if (lane == 0) next = atomicAdd(claim, kVecClaim);
-		const uint32_t end = min(U, base + kVecClaim);
-		for (uint32_t u = base; u < end; u++) vecUnit(net, plastStep, u, lane, sp, stepOf, sBC, sSC);
+		if (lane == 0) next = atomicAdd(claim, claimSize);
+		const uint32_t end = min(U, base + claimSize);
+		for (uint32_t u = base; u < end; u++) vecUnit(net, plastStep, u, lane, sp, stepOf, bcOut, scOut);
 		base = __shfl_sync(0xffffffffu, next, 0);
-	}
-	__syncthreads();
-
-	// ---- the CTA's BC and SC counts
-	const uint32_t buf = (uint32_t)(t % 3);
-	uint32_t *bcOut = N->bcCount + (size_t)buf * numBC;
-	uint32_t *scOut = N->scCount + (size_t)buf * numSC;
-	for (uint32_t i = threadIdx.x; i < numBC + numSC; i += blockDim.x) {
-		const uint32_t c = sBC[i];
-		if (!c) continue;
-		if (i < numBC) atomicAdd(&bcOut[i], c);
-		else atomicAdd(&scOut[i - numBC], c);
 	}
 }
 
@@ -518,9 +544,10 @@ bool passVecCapable(const DevNet &h)
 
 size_t passVecSmemBytes(const DevNet &h)
 {
-	return 32u * h.mfWords + ((32u * h.goWords + 15u) & ~15u) + 4ull * h.numPC + 4ull * (h.numBC + h.numSC) +
-		4ull * h.bs;
+	return 32u * h.mfWords + ((32u * h.goWords + 15u) & ~15u) + 4ull * h.numPC;
 }
+
+uint32_t passVecReduceCTAs(const DevNet &h) { return vecReduceCTAs(h.numPC, h.bs); }
 
 const void *passVecKernel() { return (const void *)&grPassVecKernel; }
 const void *pairReduceKernelFn() { return (const void *)&pairReduceKernel; }

@@ -695,6 +695,7 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	// ---- pipeline and control
 	h.pairStep = alloc<uint64_t>(2);
 	h.passClaim = alloc<uint32_t>(4);
+	h.pcDone = alloc<uint32_t>(c.numPC);
 	h.goCount = alloc<uint32_t>((size_t)2 * c.numGO);
 	h.bcCount = alloc<uint32_t>((size_t)3 * c.numBC);
 	h.scCount = alloc<uint32_t>((size_t)3 * c.numSC);
@@ -704,6 +705,9 @@ std::string Network::build(State *st, const std::vector<int> &seeds, uint32_t mf
 	h.hasMFRaw = 0;
 	h.tBase = alloc<uint64_t>(1);
 	h.ctl = alloc<HostCtl>(1);
+	if (!h.pairStep || !h.passClaim || !h.pcDone || !h.goCount || !h.bcCount || !h.scCount || !h.goBits ||
+			!h.mfBits || !h.mfRaw || !h.tBase || !h.ctl)
+		return "device allocation failed";
 	// the error word in mapped pinned host memory: the host reads it after a
 	// synchronisation without a copy
 	if (cudaHostAlloc((void **)&hErr_, sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess)
@@ -1363,9 +1367,19 @@ std::string Simulator::usePassGeometry(const PassGeometry &g)
 		int perSM = 0, numSMs = 0;
 		CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, 32 * kVecWarps, smem), "pass occupancy");
 		CK(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device_), "SM count");
-		const uint32_t claims = (n.dev().numGR / 128u + kVecClaim - 1) / kVecClaim;
+		// units claimed at a time (CBM_VEC_CLAIM, tuning; default kVecClaim)
+		vecClaim_ = kVecClaim;
+		if (const char *env = getenv("CBM_VEC_CLAIM")) {
+			const int c = atoi(env);
+			if (c < 1 || c > 64) return "CBM_VEC_CLAIM must be 1..64";
+			vecClaim_ = (uint32_t)c;
+		}
+		// every CTA resident from the start: the small-cell kernel's two
+		// CTAs hold an SM each while the pass runs
+		const uint32_t claims = (n.dev().numGR / 128u + vecClaim_ - 1) / vecClaim_;
+		const uint32_t sms = (uint32_t)std::max(1, numSMs - 2);
 		passGrid_ = std::max<uint32_t>(1, std::min<uint32_t>((claims + kVecWarps - 1) / kVecWarps,
-				(uint32_t)std::max(1, perSM) * (uint32_t)numSMs));
+				(uint32_t)std::max(1, perSM) * sms)) + passVecReduceCTAs(n.dev());
 		// claim counters from zero (another pass kind may have run meanwhile)
 		CK(cudaMemset(n.dev().passClaim, 0, 4 * sizeof(uint32_t)), "pass claim counters");
 		CKS(n.setPcSumMode(true, s0_));
@@ -1471,12 +1485,13 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	uint32_t stepArg = k;
 	const DevNet *net0Arg = nets_.size() == 1 ? nets_[0]->devPtr() : nullptr;
 	const uint32_t stage0Arg = nets_.size() == 1 ? nets_[0]->stageBytes() : 0u;
+	uint32_t vecClaimArg = vecClaim_;
 	auto launchPass = [&](cudaStream_t st, bool dependent) -> std::string {
 		if (passTmaFn_) {
 			// the per-tile pass takes the single network's descriptor too; the
 			// vector pass takes it alone
 			void *argsTma[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg};
-			void *argsVec[] = {&net0Arg, &stepArg};
+			void *argsVec[] = {&net0Arg, &stepArg, &vecClaimArg};
 			const uint32_t *unitOffArg = (const uint32_t *)dVecUnitOffset_.ptr;
 			const uint32_t *pcOffArg = (const uint32_t *)dVecPcOffset_.ptr;
 			uint32_t *claimArg = (uint32_t *)dVecClaim_.ptr;

@@ -150,6 +150,7 @@ private:
 	uint32_t passTmaW_ = 0, passTmaR_ = 0, passTmaS_ = 0, passGrid_ = 0;
 	bool passPersistent_ = false;
 	bool passVec_ = false;  // the vector pass (kind 3) runs
+	uint32_t vecClaim_ = 2;  // its units claimed at a time (single network)
 	PassGeometry passGeom_;
 	size_t passTmaSmem_ = 0;
 	cudaGraphExec_t graphExec_ = nullptr;
