@@ -573,7 +573,8 @@ def main_dense4m(args):
         sim3.calcActivity()
         zone.exportAPNC()
     e2e_ms = sim3.timer_stop()
-    h2d, d2h = sim3.mf_words() * 4, st.con("numNC")
+    # the NC spikes and the 8-byte step stamp the small-cell kernel writes to mapped host memory
+    h2d, d2h = sim3.mf_words() * 4, st.con("numNC") + 8
     sim3.close()
 
     cpu = None
@@ -741,7 +742,7 @@ def main():
     e2e_ms, = replicas.max_over_ranks(dist, [e2e_ms], device=f"cuda:{device}")
     e2e = replicas.throughput(world, n_e2e, e2e_ms)
     h2d = sim3.mf_words() * 4
-    d2h = st.con("numNC")
+    d2h = st.con("numNC") + 8  # NC spikes and the step stamp, written to mapped host memory
     sim3.close()
 
     cpu, cpu_error = None, None

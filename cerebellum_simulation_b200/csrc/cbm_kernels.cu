@@ -2042,13 +2042,29 @@ __global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet
 	protocolPrepare(N, stepsDone(N));
 }
 
+// Step t's NC spikes into mapped host memory for a host that waits on them
+// (single steps through the reference API, cbm_sim_export's AP_NC): every
+// zone's bytes from offset 8, a system-scope fence, then the step number as
+// the 8-byte stamp at offset 0.  One thread, at the end of the microzone
+// CTA, where nothing waits on it.
+__device__ void publishNC(const DevNet *N, uint64_t t, uint8_t *box)
+{
+	const uint32_t numNC = N->numNC;
+	for (uint32_t z = 0; z < N->numZones; z++) {
+		const uint8_t *ap = N->zones[z].apNC;
+		for (uint32_t i = 0; i < numNC; i++) box[8 + z * numNC + i] = ap[i];
+	}
+	__threadfence_system();
+	*reinterpret_cast<volatile uint64_t *>(box) = t;
+}
+
 // Small-cell update of step t: block 2n is network n's Golgi role, block
 // 2n+1 its microzone role.  The two roles share no state.  The microzone
 // role runs on shared-memory copies of its arrays and inputs when they fit
 // (one bulk copy in and one out per step instead of a global round trip per
 // phase).
 __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, const uint32_t *stageBytes,
-		uint32_t stepOffset, const DevNet *net0, uint32_t stage0)
+		uint32_t stepOffset, const DevNet *net0, uint32_t stage0, uint8_t *ncMailbox)
 {
 	// the GR pass of the same step may launch once these CTAs are resident
 	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
@@ -2076,6 +2092,7 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 				__syncthreads();
 			}
 			stageOut(N, base, sNet);
+			if (ncMailbox && threadIdx.x == 0) publishNC(sNet, t, ncMailbox);
 		} else {
 			// global-memory mode: the table and the MF bits in shared
 			// memory, then the role's scratch
@@ -2102,6 +2119,10 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 			if (N->proto) {
 				__syncthreads();
 				protocolRecord(N, t);
+			}
+			if (ncMailbox) {
+				__syncthreads();
+				if (threadIdx.x == 0) publishNC(N, t, ncMailbox);
 			}
 		}
 	} else {

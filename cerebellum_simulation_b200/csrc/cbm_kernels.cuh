@@ -52,8 +52,10 @@ const void *pcTreeKernelFn();
 // Small-cell update; stageBytes[n] is network n's staging block size (0:
 // its microzone CTA works on global memory).  With one network, net0 and
 // stage0 give its descriptor and staging size directly (else null, 0).
+// ncMailbox (one network, or null): mapped host memory that receives the
+// step's NC spikes and then the step number (publishNC).
 __global__ void tailKernel(const DevNet *const *nets, const uint32_t *stageBytes, uint32_t stepOffset,
-		const DevNet *net0, uint32_t stage0);
+		const DevNet *net0, uint32_t stage0, uint8_t *ncMailbox);
 __global__ void protocolPrimeKernel(const DevNet *N);
 // GR peri-stimulus histogram of step t = stepsDone(N) + 1 + stepOffset, after
 // the GR pass of that step: 8 GR per thread.

@@ -150,6 +150,10 @@ private:
 	uint32_t passTmaW_ = 0, passTmaR_ = 0, passTmaS_ = 0, passGrid_ = 0;
 	bool passPersistent_ = false;
 	bool passVec_ = false;  // the vector pass (kind 3) runs
+	// the small-cell kernel argument of the step being enqueued: the NC
+	// mailbox while single-step graphs are captured (one network), else null
+	uint8_t *mailboxArg_ = nullptr;
+	bool lastStepPublishes_ = false;  // the last launch was a single-step graph that writes the mailbox
 	uint32_t vecClaim_ = 2;  // its units claimed at a time (single network)
 	PassGeometry passGeom_;
 	size_t passTmaSmem_ = 0;
@@ -253,6 +257,9 @@ private:
 	// pinned staging of host MF input: kMFStage slots, each reused once the
 	// copy that last read it has run (mfStageEv_)
 	uint32_t *hErr_ = nullptr;  // the error word (mapped pinned host memory; h_.errFlag maps it)
+	// NC mailbox (mapped pinned host memory): step stamp, then every zone's
+	// NC spikes, written by the small-cell kernel of single-step launches
+	uint8_t *hMailbox_ = nullptr, *dMailbox_ = nullptr;
 	uint32_t *hPinnedBits_ = nullptr;
 	uint8_t *hPinnedRaw_ = nullptr;
 	cudaEvent_t mfStageEv_[kMFStage] = {};

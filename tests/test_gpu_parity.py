@@ -82,6 +82,58 @@ def test_reference_network_16k_bit_exact(tmp_path):
     assert compare_states(fo, fp) == []
 
 
+def nc_offsets(num):
+    """Byte offsets of each zone's NC spikes in a trace record (cbmtest.product_record's layout)."""
+    off = num["GR"] // 8 + 9 * num["GO"] + 5 * num["SC"]
+    per_zone = 5 * (num["BC"] + num["PC"] + num["IO"] + num["NC"])
+    return [off + z * per_zone + 5 * (num["BC"] + num["PC"] + num["IO"]) for z in range(num["zones"])]
+
+
+def test_nc_export_right_after_each_step(tmp_path):
+    """exportAPNC called straight after each calcActivity, as a driver loop
+    does (the NC spikes come through mapped host memory while the step's GR
+    pass may still run), returns the oracle's NC spikes of that step, every
+    step of 1500 on the reference's 16K network and of 600 in both zones of
+    a two-zone network."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    st = cbmtest.golden_state("ref16k", str(tmp_path))
+    two = networks.build_random_network(8, 6, 4, 4, 10, networks.act_params("16k"), seed=5, gr_per_go=128,
+                                       mf_per_go=3, vel=40, gogo=((1, 1, 0.0),), n_zones=2)
+    p2 = str(tmp_path / "two.state")
+    two.writeState(p2)
+    for path, steps, rate in ((st, 1500, None), (p2, 600, 0.08)):
+        mf = cbmtest.counter_mf(1024, steps, 11) if rate is None else cbmtest.counter_mf(1024, steps, 8, rate_hi=rate)
+        o = Oracle(path, seeds=[7, 8])
+        tr = o.run(mf, EVENTS)
+        offs = nc_offsets(o.num)
+        sim = cbm.CBMSimCore(cbm.CBMState(path), [7, 8], device=0)
+        zones = sim.getMZoneList()
+        n_nc = o.num["NC"]
+        spikes = 0
+        for s in range(steps):
+            for ev in EVENTS.get(s + 1, []):
+                if ev[0] == "errdrive" and ev[1] < len(zones):
+                    sim.updateErrDrive(ev[1], ev[2])
+                elif ev[0] == "plast" and ev[1] < len(zones):
+                    zones[ev[1]].setGRPCPlastSteps(ev[2], ev[3])
+                elif ev[0] == "plastreset":
+                    zones[ev[1]].resetGRPCPlastSteps()
+                elif ev[0] == "grgoinc":
+                    sim.getInputNet().setGIncGRtoGO(ev[1])
+                elif ev[0] == "grgoincreset":
+                    sim.getInputNet().resetGIncGRtoGO()
+            sim.updateMFInput(mf[s])
+            sim.calcActivity()
+            for z, zone in enumerate(zones):
+                got = zone.exportAPNC()
+                want = tr[s, offs[z]:offs[z] + n_nc]
+                assert np.array_equal(got, want), f"step {s + 1} zone {z}"
+                spikes += int(want.sum())
+        assert spikes > 0
+        sim.close()
+
+
 def test_config1_bit_exact(tmp_path):
     """Config 1: 16,384 GR with random wiring, 2000 steps of regenerating
     Poisson MF input at 1-30 Hz, PF->PC plasticity forced on."""
@@ -137,8 +189,8 @@ def test_config3_4m_bit_exact_short(tmp_path):
     assert compare_states(fo, fp) == []
 
 
-@pytest.mark.parametrize("name", ["config2", "config3"])
-def test_large_networks_match_reference_golden(tmp_path, name):
+@pytest.mark.parametrize("name,vec", [("config2", "0"), ("config2", "1"), ("config3", "0")])
+def test_large_networks_match_reference_golden(tmp_path, name, vec, monkeypatch):
     """The device against the reference itself, with no oracle in between:
     every step's spike raster and spike-relevant float state of the 1M-GR
     network over 1000 steps (PF->PC weights moving both ways from about step
@@ -146,14 +198,18 @@ def test_large_networks_match_reference_golden(tmp_path, name):
     final state, equal the digests of the reference's own run
     (tests/golden/make_golden.py; inputs cbmtest.golden_large_case).  The
     four GO glutamate/mGluR arrays, which no spike reads, are compared with
-    the oracle in the tests above instead."""
+    the oracle in the tests above instead.  The 1M network runs with the
+    default GR pass and with the vector pass."""
     import cerebellum_simulation_b200 as cbm
+    monkeypatch.setenv("CBM_PASS_VEC", vec)
     gold = cbmtest.load_json(name + "_digests.json")
     net, mf, ev = cbmtest.golden_large_case(name)
     p = str(tmp_path / "net.state")
     net.writeState(p)
     del net
     sim = cbm.CBMSimCore(cbm.CBMState(p), [7], device=0)
+    if vec == "1":
+        assert sim.pass_geometry()[0] == "grPassVecKernel"
     zones, inet = sim.getMZoneList(), sim.getInputNet()
     for s in range(mf.shape[0]):
         for e in ev.get(s + 1, []):

@@ -61,38 +61,47 @@ def test_tma_pass_geometries_match_plain_pass(tmp_path):
     for g in PERSISTENT_GEOMETRIES:
         got = run_with({"CBM_PASS_PERSIST": g}, path, mf, str(tmp_path / f"persist_{g}.state"))
         assert got == want, f"persistent geometry {g} differs from the plain pass"
-    # the vector pass, this network's default (four cells per lane, claimed
-    # work, PF->PC running sums from the previous step's pair sums)
-    got = run_with({}, path, mf, str(tmp_path / "vec.state"))
-    assert got == want, "the vector pass differs from the plain pass"
+    # the vector pass (four cells per lane, claimed work, PF->PC running
+    # sums from the previous step's pair sums), and the default
+    for claim in ("1", "2", "4"):
+        got = run_with({"CBM_PASS_VEC": "1", "CBM_VEC_CLAIM": claim}, path, mf, str(tmp_path / f"vec{claim}.state"))
+        assert got == want, f"the vector pass ({claim} units per claim) differs from the plain pass"
+    got = run_with({}, path, mf, str(tmp_path / "default.state"))
+    assert got == want, "the default pass differs from the plain pass"
 
 
-def test_vector_pass_is_the_default_where_it_applies(tmp_path):
-    """Single networks of the eyelid shape run the vector pass unless
-    CBM_PASS_VEC=0; a 16K network whose SC blocks hold 32 cells runs the
-    per-tile pass."""
+def test_pass_kind_selection(tmp_path):
+    """Single networks of the eyelid shape run the per-tile pass by default
+    and the vector pass with CBM_PASS_VEC=1; a 16K network whose SC blocks
+    hold 32 cells never runs the vector pass."""
     import cerebellum_simulation_b200 as cbm
     from cerebellum_simulation_b200 import networks
     st = networks.build_random_network(9, 8, 5, 5, 10, networks.act_params("dense"), seed=5,
                                        go_out_per_gr=4, mf_per_go=16, vel=147)
     path = str(tmp_path / "net.state")
     st.writeState(path)
-    sim = cbm.CBMSimCore(cbm.CBMState(path), [3], device=0)
-    assert sim.pass_geometry()[0] == "grPassVecKernel"
-    sim.close()
-    os.environ["CBM_PASS_VEC"] = "0"
-    try:
-        sim = cbm.CBMSimCore(cbm.CBMState(path), [3], device=0)
-    finally:
-        del os.environ["CBM_PASS_VEC"]
-    assert sim.pass_geometry()[0] == "grPassTmaKernel"
-    sim.close()
+
+    def kind_with(env, p):
+        old = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            sim = cbm.CBMSimCore(cbm.CBMState(p), [3], device=0)
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    del os.environ[k]
+                else:
+                    os.environ[k] = v
+        kind = sim.pass_geometry()[0]
+        sim.close()
+        return kind
+
+    assert kind_with({}, path) == "grPassTmaKernel"
+    assert kind_with({"CBM_PASS_VEC": "1"}, path) == "grPassVecKernel"
     small = networks.config1_network(seed=1)
     p16 = str(tmp_path / "c1.state")
     small.writeState(p16)
-    sim = cbm.CBMSimCore(cbm.CBMState(p16), [3], device=0)
-    assert sim.pass_geometry()[0] != "grPassVecKernel"
-    sim.close()
+    assert kind_with({"CBM_PASS_VEC": "1"}, p16) != "grPassVecKernel"
 
 
 def test_zone_global_memory_mode_matches_staged(tmp_path):
