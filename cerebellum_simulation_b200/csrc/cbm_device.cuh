@@ -251,6 +251,7 @@ struct DevNet {
 	uint32_t *errFlag;   // error word (kErr* bits), in mapped pinned host memory
 	const CUtensorMap *passMaps;  // [PM_COUNT] descriptors of the TMA GR pass, or null
 	DevProtocol *proto;           // device-driven trial protocol, or null
+	float *protoSlots;            // its ctlSlots (read without going through proto), or null
 	const StageSeg *zoneSegs;     // arrays the microzone CTA stages in shared memory
 	uint32_t numZoneSegs;         // 0: the microzone CTA works on global memory
 	uint32_t zoneArenaBytes;      // staged arrays: read-only ones, then from zoneWbOff on the written ones
@@ -282,7 +283,7 @@ __device__ __forceinline__ uint64_t stepsDone(const DevNet *N)
 __device__ __forceinline__ float plasticityStep(const DevNet *N, uint64_t t, uint32_t z, uint8_t sel)
 {
 	if (sel == 0) return 0.0f;
-	if (z == 0 && N->proto) return N->proto->ctlSlots[(t & 1) * 3 + (sel == 1 ? 0 : 1)];
+	if (z == 0 && N->protoSlots) return N->protoSlots[(t & 1) * 3 + (sel == 1 ? 0 : 1)];
 	return sel == 1 ? N->ctl->ltdStep[z] : N->ctl->ltpStep[z];
 }
 #endif
@@ -294,10 +295,11 @@ CBM_LAYOUT_FN uint32_t stageBlockBytes(uint32_t arenaBytes, uint32_t numSegs)
 
 // Inputs of a microzone step that other kernels write, copied into shared
 // memory after the staging block: the cbmExpf table, the MF spike bits of
-// step t, the PF->BC and PF->SC counts and the PF->PC partial sums of
-// pass(t-2) for every zone (byte offsets, 16-byte aligned).
+// step t, the PF->BC and PF->SC counts, every zone's error drive of step t
+// and the PF->PC partial sums of pass(t-2) for every zone (byte offsets,
+// 16-byte aligned).
 struct ZoneInputLayout {
-	uint32_t exp2, mf, bc, sc, pc, bytes;
+	uint32_t exp2, mf, bc, sc, err, pc, bytes;
 };
 CBM_LAYOUT_FN ZoneInputLayout zoneInputLayout(uint32_t mfWords, uint32_t numBC, uint32_t numSC, uint32_t Z,
 		uint32_t numPC, uint32_t bs)
@@ -308,6 +310,7 @@ CBM_LAYOUT_FN ZoneInputLayout zoneInputLayout(uint32_t mfWords, uint32_t numBC, 
 	L.mf = o; o += (4 * mfWords + 15) & ~15u;
 	L.bc = o; o += (4 * numBC + 15) & ~15u;
 	L.sc = o; o += (4 * numSC + 15) & ~15u;
+	L.err = o; o += (4 * Z + 15) & ~15u;  // every zone's error drive of step t
 	L.pc = o; o += (4 * Z * numPC * bs + 15) & ~15u;
 	L.bytes = o;
 	return L;

@@ -234,7 +234,7 @@ __device__ __forceinline__ uint32_t spikeBit(const uint32_t *bits, uint32_t idx)
 // Zone z's error drive at step t (setters, or the protocol for zone 0).
 __device__ __forceinline__ float errDriveOf(const DevNet *N, uint64_t t, uint32_t z)
 {
-	if (z == 0 && N->proto) return N->proto->ctlSlots[(t & 1) * 3 + 2];
+	if (z == 0 && N->protoSlots) return N->protoSlots[(t & 1) * 3 + 2];
 	return N->ctl->errDrive[z];
 }
 
@@ -1248,7 +1248,10 @@ struct ZoneIn {
 	const float *pcPart[kMaxZones];     // [numPC][bs] PF->PC partial sums of pass(t-2) per zone
 	const float *pcSum[kMaxZones];      // [numPC] PF->PC input sums of pass(t-2) per zone (pcSumMode), else null
 	const uint64_t *exp2;               // cbmExpf table
+	const float *err;                   // [numZones] error drives of step t, or null (read errDriveOf)
 };
+
+__device__ void protocolRecordWarp(const DevNet *__restrict__ N, uint64_t t, uint32_t lane);
 
 __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm, const ZoneIn &in)
 {
@@ -1375,7 +1378,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
 	// this step's error drive of the IO a thread updates at the end, loaded
 	// now so that the load overlaps the synapse and NC updates
-	const float errOwn = tid < Z * numIO ? errDriveOf(N, t, tid / numIO) : 0.0f;
+	const float errOwn = tid < Z * numIO ? (in.err ? in.err[tid / numIO] : errDriveOf(N, t, tid / numIO)) : 0.0f;
 	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
 	// calcNCActivities (mzone.cpp:341-407) one warp per NC
 	// NC->IO conductances (one thread per synapse) and MF->NC synaptic
@@ -1486,7 +1489,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 		const uint32_t z = task / numIO, i = task % numIO;
 		const DevZone &Q = N->zones[z];
 		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], th0 = Q.threshIO[i];
-		const float errDrive = task == tid ? errOwn : errDriveOf(N, t, z);
+		const float errDrive = task == tid ? errOwn : (in.err ? in.err[z] : errDriveOf(N, t, z));
 		const uint32_t apBuf = Q.apBufIO[i];
 		float gNCSum = 0;
 		for (uint32_t j = 0; j < nIONC; j++) gNCSum = gNCSum + ioScratch[(size_t)task * nIONC + j];
@@ -1506,11 +1509,17 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// bookkeeping (mzone.cpp:536-580): independent gathers, run as one flat
 	// task space so that their loads are in flight together
 	const bool popStep = (t % N->tsPerPopHistBinPC) == 0;
+	// the device protocol's record of step t (its NC and PC spikes are final
+	// now) on the last warp, beside the outputs: neither reads what the
+	// other writes
+	const bool recWarp = N->proto != nullptr && warp == nWarps - 1;
+	const uint32_t oThr = N->proto != nullptr ? nThr - 32u : nThr;
+	if (recWarp) protocolRecordWarp(N, t, lane);
 	{
 		const uint32_t nMFIn = Z * numNC * nMFNC, nBCPC = Z * numPC, nSCPC = Z * numPC * N->numpPCfromSCtoPC,
 			nPCBC = Z * numBC, nPCNC = Z * numNC * N->numpNCfromPCtoNC, nIO = Z * numIO, nNC = Z * numNC;
 		const uint32_t total = nMFIn + nBCPC + nSCPC + nPCBC + nPCNC + nIO + nNC + Z;
-		for (uint32_t task = tid; task < total; task += nThr) {
+		for (uint32_t task = recWarp ? total : tid; task < total; task += oThr) {
 			uint32_t r = task;
 			if (r < nMFIn) {
 				const uint32_t z = r / (numNC * nMFNC), k = r % (numNC * nMFNC);
@@ -1711,6 +1720,12 @@ __device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &i
 		else { src = N->scCount + (size_t)R * N->numSC + (w - e2); dst = dyn + L.sc + 4 * (w - e2); }
 		cpAsync4(dst, src);
 	}
+	// the error drives: the protocol's slot for zone 0 under a device
+	// protocol, else the setters' values (errDriveOf)
+	if (tid < Z) {
+		const float *src = tid == 0 && N->protoSlots ? N->protoSlots + (t & 1) * 3 + 2 : N->ctl->errDrive + tid;
+		cpAsync4(dyn + L.err + 4 * tid, src);
+	}
 	// the PF->PC input sums of every zone when the GR pass made them, else
 	// the partial sums: 16-byte pieces when the slot is 16-byte aligned
 	// (numPC * bs a multiple of 4), else words
@@ -1739,6 +1754,7 @@ __device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &i
 				: nullptr;
 		}
 		in.exp2 = reinterpret_cast<const uint64_t *>(dyn + L.exp2);
+		in.err = reinterpret_cast<const float *>(dyn + L.err);
 	}
 }
 
@@ -1840,13 +1856,14 @@ __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 	}
 }
 
-// Record step t of a device protocol (in the microzone CTA of step t, after
-// its own work; N may be its shared-memory copy): the eyelid integrator on
+// Record step t of a device protocol (one warp of the microzone CTA of step
+// t, once the step's NC and PC spikes are final; N may be its shared-memory
+// copy): the eyelid integrator on
 // zone 0's NC spikes every step (EyelidIntegrator::calcStep,
 // eyelidintegrator.cpp:50-68) and, inside the recording window of a kept
 // trial, NC and PC spike counts per bin and the integrator's output
 // (ECTrialsData's PSH and eyelid trace, ecmanagementdelay.cpp:239-273).
-__device__ void protocolRecord(const DevNet *__restrict__ N, uint64_t t)
+__device__ void protocolRecordWarp(const DevNet *__restrict__ N, uint64_t t, uint32_t lane)
 {
 	const DevProtocol *P = N->proto;
 	// every field is read before anything is written, so that the loads go
@@ -1864,10 +1881,9 @@ __device__ void protocolRecord(const DevNet *__restrict__ N, uint64_t t)
 	const bool rec = trial >= dataStart && trial < dataStart + numData && ct >= 0 && ct < (int32_t)recLen;
 	const uint32_t dt = trial - dataStart;
 	const uint32_t numNC = N->numNC, numPC = N->numPC;
-	if (threadIdx.x < 32) {
+	{
 		// the integrator: lane i's conductance, then lane 0 sums them in
 		// order i = 0, 1, ... as the reference's loop does
-		const uint32_t lane = threadIdx.x;
 		const float decay = P->eyeGDecay, inc = P->eyeGInc, shift = P->eyeGShift, leak = P->eyeGLeak,
 			maxAmp = P->eyeMaxAmp;
 		float *const eyeG = P->eyeG, *const eyeVm = P->eyeVm, *const eyelid = P->eyelid;
@@ -1897,7 +1913,7 @@ __device__ void protocolRecord(const DevNet *__restrict__ N, uint64_t t)
 	if (rec) {
 		const uint32_t bin = (uint32_t)ct / binSteps;
 		uint32_t *const ncPSH = P->ncPSH, *const pcPSH = P->pcPSH;
-		for (uint32_t i = threadIdx.x; i < numNC + numPC; i += blockDim.x) {
+		for (uint32_t i = lane; i < numNC + numPC; i += 32) {
 			if (i < numNC) ncPSH[((size_t)dt * nBins + bin) * numNC + i] += Q.apNC[i];
 			else pcPSH[((size_t)dt * nBins + bin) * numPC + (i - numNC)] += Q.apPC[i - numNC];
 		}
@@ -2087,10 +2103,6 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 					sNet->numPC, sNet->bs);
 			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(dyn + L.bytes), in);
 			__syncthreads();
-			if (sNet->proto) {
-				protocolRecord(sNet, t);
-				__syncthreads();
-			}
 			stageOut(N, base, sNet);
 			if (ncMailbox && threadIdx.x == 0) publishNC(sNet, t, ncMailbox);
 		} else {
@@ -2113,13 +2125,10 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 					in.pcSum[z] = N->pcSumMode ? Q.pcSum + (size_t)R * N->numPC : nullptr;
 				}
 				in.exp2 = sExp2;
+				in.err = nullptr;
 			}
 			__syncthreads();
 			zoneRole(N, t, sMF + ((N->mfWords + 3) & ~3u), in);
-			if (N->proto) {
-				__syncthreads();
-				protocolRecord(N, t);
-			}
 			if (ncMailbox) {
 				__syncthreads();
 				if (threadIdx.x == 0) publishNC(N, t, ncMailbox);

@@ -890,6 +890,7 @@ std::string Network::setProtocol(const cbm_eyelid_protocol &p, cudaStream_t s, c
 	if (!dp) return "device allocation failed";
 	hProto_ = d;
 	h_.proto = dp;
+	h_.protoSlots = d.ctlSlots;
 	CK(cudaMemcpyAsync(dNet_.ptr, &h_, sizeof(DevNet), cudaMemcpyHostToDevice, s), "uploading the network descriptor");
 	protocolPrimeKernel<<<1, kTailThreads, 0, s>>>(devPtr());
 	CK(cudaGetLastError(), "starting the protocol");
