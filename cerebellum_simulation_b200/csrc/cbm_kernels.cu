@@ -1096,12 +1096,21 @@ __device__ float pcRowTree(const float *part, uint32_t bs, uint32_t lane)
 	return x;
 }
 
-// Sequential left-to-right float sum of one value per lane (lanes 0..n-1),
-// the order of the reference's `sum = sum + x[j]` loops; every lane gets it.
-__device__ __forceinline__ float orderedLaneSum(float v, uint32_t n)
+// Sequential left-to-right float sum of x[0..n) (the order of the
+// reference's `sum = sum + x[j]` loops, from 0), eight loads in flight ahead
+// of the adds.
+__device__ __forceinline__ float orderedSum(const float *x, uint32_t n)
 {
 	float s = 0;
-	for (uint32_t j = 0; j < n; j++) s = s + __shfl_sync(0xffffffffu, v, j);
+	uint32_t j = 0;
+	for (; j + 8 <= n; j += 8) {
+		float q[8];
+#pragma unroll
+		for (uint32_t u = 0; u < 8; u++) q[u] = x[j + u];
+#pragma unroll
+		for (uint32_t u = 0; u < 8; u++) s = s + q[u];
+	}
+	for (; j < n; j++) s = s + x[j];
 	return s;
 }
 
@@ -1287,22 +1296,19 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 		const uint32_t z = task / numPC, i = task % numPC;
 		const DevZone &Q = N->zones[z];
 		const float inputSum = in.pcSum[z] ? in.pcSum[z][i] : pcRowTree(in.pcPart[z] + (size_t)i * N->bs, N->bs, lane);
-		float gSCPCSum = 0;
-		for (uint32_t j0 = 0; j0 < N->numpPCfromSCtoPC; j0 += 32) {
-			const uint32_t j = j0 + lane;
-			float g = 0;
-			if (j < N->numpPCfromSCtoPC) {
-				const size_t k = (size_t)i * N->numpPCfromSCtoPC + j;
-				const float g0 = Q.gSCPC[k];
-				const uint8_t inp = Q.inputSCPC[k];
-				g = g0;
-				g = g + N->gIncSCtoPC * (1 - g) * inp;
-				g = g * N->gDecSCtoPC;
-				Q.gSCPC[k] = g;
-			}
-			const uint32_t n = min(32u, N->numpPCfromSCtoPC - j0);
-			for (uint32_t q = 0; q < n; q++) gSCPCSum += __shfl_sync(0xffffffffu, g, q);
+		const uint32_t nSC = N->numpPCfromSCtoPC;
+		for (uint32_t j = lane; j < nSC; j += 32) {
+			const size_t k = (size_t)i * nSC + j;
+			const float g0 = Q.gSCPC[k];
+			const uint8_t inp = Q.inputSCPC[k];
+			float g = g0;
+			g = g + N->gIncSCtoPC * (1 - g) * inp;
+			g = g * N->gDecSCtoPC;
+			Q.gSCPC[k] = g;
 		}
+		__syncwarp();
+		// lane 0: their sum in the reference's order, from the stored values
+		const float gSCPCSum = lane == 0 ? orderedSum(Q.gSCPC + (size_t)i * nSC, nSC) : 0.0f;
 		if (lane == 0) {
 			const float gPF0 = Q.gPFPC[i], gBC0 = Q.gBCPC[i], vPC0 = Q.vPC[i], th0 = Q.threshPC[i];
 			const uint32_t inBC = Q.inputBCPC[i], apBuf = Q.apBufPC[i];
@@ -1380,93 +1386,66 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// now so that the load overlaps the synapse and NC updates
 	const float errOwn = tid < Z * numIO ? (in.err ? in.err[tid / numIO] : errDriveOf(N, t, tid / numIO)) : 0.0f;
 	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
-	// calcNCActivities (mzone.cpp:341-407) one warp per NC
-	// NC->IO conductances (one thread per synapse) and MF->NC synaptic
-	// conductances (one thread per synapse), in rounds with the loads first
-	{
-		const uint32_t nIOSyn = Z * numIO * nIONC, nNCSyn = Z * numNC * nMFNC;
-		const uint32_t rounds2 = max((nIOSyn + nThr - 1) / nThr, (nNCSyn + nThr - 1) / nThr);
-		for (uint32_t rd = 0; rd < rounds2; rd++) {
-			const uint32_t c = rd * nThr + tid;
-			const bool hasIO = c < nIOSyn, hasNC = c < nNCSyn;
-			const uint32_t iz = hasIO ? c / (numIO * nIONC) : 0, ik = hasIO ? c % (numIO * nIONC) : 0;
-			float ig0 = 0;
-			uint8_t iIn = 0;
-			if (hasIO) { ig0 = N->zones[iz].gNCIO[ik]; iIn = N->zones[iz].inputNCIO[ik]; }
-			const uint32_t nz = hasNC ? c / (numNC * nMFNC) : 0, nk = hasNC ? c % (numNC * nMFNC) : 0;
-			float nIn = 0, nWt = 0, gmN0 = 0, gN0 = 0, gmA0 = 0, gA0 = 0;
-			if (hasNC) {
-				const DevZone &Q = N->zones[nz];
-				nIn = Q.inputMFNC[nk]; nWt = Q.mfSynWeightNC[nk];
-				gmN0 = Q.gmaxNMDAofMFtoNC[nk]; gN0 = Q.gMFNMDANC[nk];
-				gmA0 = Q.gmaxAMPAofMFtoNC[nk]; gA0 = Q.gMFAMPANC[nk];
-			}
-			if (hasIO) {
-				const DevZone &Q = N->zones[iz];
-				float g = ig0;
-				g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO, exp2) + N->gDecT0ofNCtoIO), exp2);
-				g = g + iIn * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO, exp2);
-				Q.gNCIO[ik] = g;
-				Q.inputNCIO[ik] = 0;
-				ioScratch[c] = g;
-			}
-			if (hasNC) {
-				const DevZone &Q = N->zones[nz];
-				const uint32_t i = nk / nMFNC, j = nk % nMFNC;
-				float gmN = gmN0;
-				gmN = gmN * N->gmaxNMDADecMFtoNC + nIn * nWt * (1 - gmN);
-				Q.gmaxNMDAofMFtoNC[nk] = gmN;
-				float gN = gN0;
-				gN = gN + N->gNMDAIncMFtoNC * (gmN - gN);
-				Q.gMFNMDANC[nk] = gN;
-				float gmA = gmA0;
-				gmA = gmA * N->gmaxAMPADecMFtoNC + nIn * nWt * (1 - gmA);
-				Q.gmaxAMPAofMFtoNC[nk] = gmA;
-				float gA = gA0;
-				gA = gA + N->gAMPAIncMFtoNC * (gmA - gA);
-				Q.gMFAMPANC[nk] = gA;
-				float *sN = ncScratch + ((size_t)nz * numNC + i) * 2 * nMFNC;
-				sN[j] = gN;
-				sN[nMFNC + j] = gA;
-			}
-		}
+	// calcNCActivities (mzone.cpp:341-407) one warp per NC.
+	// NC->IO conductances: one thread per synapse, numbered from the group's
+	// last thread down, so that they run on warps that take no NC (or the
+	// last NCs).
+	const uint32_t nIOSyn = Z * numIO * nIONC;
+	for (uint32_t c = nThr - 1 - tid; c < nIOSyn; c += nThr) {
+		const uint32_t iz = c / (numIO * nIONC), ik = c % (numIO * nIONC);
+		const DevZone &Q = N->zones[iz];
+		const float ig0 = Q.gNCIO[ik];
+		const uint8_t iIn = Q.inputNCIO[ik];
+		float g = ig0;
+		g = g * cbmExpf(-N->msPerTimeStep / (-N->gDecTSofNCtoIO * cbmExpf(-g / N->gDecTTofNCtoIO, exp2) + N->gDecT0ofNCtoIO), exp2);
+		g = g + iIn * N->gIncNCtoIO * cbmExpf(-g / N->gIncTauNCtoIO, exp2);
+		Q.gNCIO[ik] = g;
+		Q.inputNCIO[ik] = 0;
+		ioScratch[c] = g;
 	}
-	barSync(2, gThr);
+	// one warp per NC: its MF->NC synaptic conductances (lanes over the
+	// synapses) into the warp's scratch, then the sums and the update, with
+	// no barrier but the warp's own
 	for (uint32_t task = warp; task < Z * numNC; task += nWarps) {
 		const uint32_t z = task / numNC, i = task % numNC;
 		const DevZone &Q = N->zones[z];
-		const float *sN = ncScratch + (size_t)task * 2 * nMFNC;
+		float *const sNw = ncScratch + (size_t)task * 2 * nMFNC;
+		for (uint32_t j = lane; j < nMFNC; j += 32) {
+			const size_t nk = (size_t)i * nMFNC + j;
+			const float nIn = Q.inputMFNC[nk], nWt = Q.mfSynWeightNC[nk];
+			const float gmN0 = Q.gmaxNMDAofMFtoNC[nk], gN0 = Q.gMFNMDANC[nk];
+			const float gmA0 = Q.gmaxAMPAofMFtoNC[nk], gA0 = Q.gMFAMPANC[nk];
+			float gmN = gmN0;
+			gmN = gmN * N->gmaxNMDADecMFtoNC + nIn * nWt * (1 - gmN);
+			Q.gmaxNMDAofMFtoNC[nk] = gmN;
+			float gN = gN0;
+			gN = gN + N->gNMDAIncMFtoNC * (gmN - gN);
+			Q.gMFNMDANC[nk] = gN;
+			float gmA = gmA0;
+			gmA = gmA * N->gmaxAMPADecMFtoNC + nIn * nWt * (1 - gmA);
+			Q.gmaxAMPAofMFtoNC[nk] = gmA;
+			float gA = gA0;
+			gA = gA + N->gAMPAIncMFtoNC * (gmA - gA);
+			Q.gMFAMPANC[nk] = gA;
+			sNw[j] = gN;
+			sNw[nMFNC + j] = gA;
+		}
+		__syncwarp();
+		const float *sN = sNw;
 		const float vNC0 = Q.vNC[i], thNC0 = Q.threshNC[i];
 		const uint32_t apBufNC = Q.apBufNC[i];
-		float gPCNCSum = 0;
-		for (uint32_t j0 = 0; j0 < N->numpNCfromPCtoNC; j0 += 32) {
-			const uint32_t j = j0 + lane;
-			float g = 0;
-			if (j < N->numpNCfromPCtoNC) {
-				const size_t k = (size_t)i * N->numpNCfromPCtoNC + j;
-				const float g0 = Q.gPCNC[k], scale = Q.gPCScaleNC[k];
-				const uint8_t in = Q.inputPCNC[k];
-				g = g0 * N->gDecPCtoNC + in * scale * (1 - g0);
-				Q.gPCNC[k] = g;
-			}
-			const uint32_t n = min(32u, N->numpNCfromPCtoNC - j0);
-			for (uint32_t q = 0; q < n; q++) gPCNCSum = gPCNCSum + __shfl_sync(0xffffffffu, g, q);
+		const uint32_t nPCNC = N->numpNCfromPCtoNC;
+		for (uint32_t j = lane; j < nPCNC; j += 32) {
+			const size_t k = (size_t)i * nPCNC + j;
+			const float g0 = Q.gPCNC[k], scale = Q.gPCScaleNC[k];
+			const uint8_t in = Q.inputPCNC[k];
+			Q.gPCNC[k] = g0 * N->gDecPCtoNC + in * scale * (1 - g0);
 		}
+		__syncwarp();
+		float gPCNCSum = lane == 0 ? orderedSum(Q.gPCNC + (size_t)i * nPCNC, nPCNC) : 0.0f;
 		// lanes 0 and 1: the NMDA and AMPA sums over the NC's MF synapses in
 		// the reference's order; eight loads in flight ahead of the adds
-		float partial = 0;
-		if (lane < 2) {
-			const float *src = sN + lane * nMFNC;
-			uint32_t j = 0;
-			for (; j + 8 <= nMFNC; j += 8) {
-				float q[8];
-#pragma unroll
-				for (uint32_t u = 0; u < 8; u++) q[u] = src[j + u];
-#pragma unroll
-				for (uint32_t u = 0; u < 8; u++) partial = partial + q[u];
-			}
-			for (; j < nMFNC; j++) partial = partial + src[j];
-		}
+		const float partial = lane < 2 ? orderedSum(sN + lane * nMFNC, nMFNC) : 0.0f;
 		const float ampaSum = __shfl_sync(0xffffffffu, partial, 1);
 		if (lane == 0) {
 			float gMFNMDASum = partial, gMFAMPASum = ampaSum;
