@@ -1293,7 +1293,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// calcPCActivities (mzone.cpp:187-226), one warp per PC; the SC
 	// conductances update elementwise, their sum runs in the reference's order
 	for (uint32_t task = warp; task < Z * numPC; task += nWarps) {
-		const uint32_t z = task / numPC, i = task % numPC;
+		const uint32_t z = Z == 1 ? 0u : task / numPC, i = Z == 1 ? task : task % numPC;
 		const DevZone &Q = N->zones[z];
 		const float inputSum = in.pcSum[z] ? in.pcSum[z][i] : pcRowTree(in.pcPart[z] + (size_t)i * N->bs, N->bs, lane);
 		const uint32_t nSC = N->numpPCfromSCtoPC;
@@ -1332,7 +1332,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	}
 	// calcBCActivities (mzone.cpp:228-256)
 	for (uint32_t c = tid; c < Z * numBC; c += nThr) {
-		const uint32_t bz = c / numBC, bi = c % numBC;
+		const uint32_t bz = Z == 1 ? 0u : c / numBC, bi = Z == 1 ? c : c % numBC;
 		const DevZone &Q = N->zones[bz];
 		const uint32_t bInPF = in.bcSum[bi], bInPC = Q.inputPCBC[bi], bApBuf = Q.apBufBC[bi];
 		const float bth0 = Q.threshBC[bi];
@@ -1384,7 +1384,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
 	// this step's error drive of the IO a thread updates at the end, loaded
 	// now so that the load overlaps the synapse and NC updates
-	const float errOwn = tid < Z * numIO ? (in.err ? in.err[tid / numIO] : errDriveOf(N, t, tid / numIO)) : 0.0f;
+	const float errOwn = tid < Z * numIO ? (in.err ? in.err[Z == 1 ? 0u : tid / numIO] : errDriveOf(N, t, Z == 1 ? 0u : tid / numIO)) : 0.0f;
 	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
 	// calcNCActivities (mzone.cpp:341-407) one warp per NC.
 	// NC->IO conductances: one thread per synapse, numbered from the group's
@@ -1392,7 +1392,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// last NCs).
 	const uint32_t nIOSyn = Z * numIO * nIONC;
 	for (uint32_t c = nThr - 1 - tid; c < nIOSyn; c += nThr) {
-		const uint32_t iz = c / (numIO * nIONC), ik = c % (numIO * nIONC);
+		const uint32_t iz = Z == 1 ? 0u : c / (numIO * nIONC), ik = Z == 1 ? c : c % (numIO * nIONC);
 		const DevZone &Q = N->zones[iz];
 		const float ig0 = Q.gNCIO[ik];
 		const uint8_t iIn = Q.inputNCIO[ik];
@@ -1407,7 +1407,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// synapses) into the warp's scratch, then the sums and the update, with
 	// no barrier but the warp's own
 	for (uint32_t task = warp; task < Z * numNC; task += nWarps) {
-		const uint32_t z = task / numNC, i = task % numNC;
+		const uint32_t z = Z == 1 ? 0u : task / numNC, i = Z == 1 ? task : task % numNC;
 		const DevZone &Q = N->zones[z];
 		float *const sNw = ncScratch + (size_t)task * 2 * nMFNC;
 		for (uint32_t j = lane; j < nMFNC; j += 32) {
@@ -1465,7 +1465,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	}
 	barSync(2, gThr);
 	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
-		const uint32_t z = task / numIO, i = task % numIO;
+		const uint32_t z = Z == 1 ? 0u : task / numIO, i = Z == 1 ? task : task % numIO;
 		const DevZone &Q = N->zones[z];
 		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], th0 = Q.threshIO[i];
 		const float errDrive = task == tid ? errOwn : (in.err ? in.err[z] : errDriveOf(N, t, z));
@@ -1501,14 +1501,14 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 		for (uint32_t task = recWarp ? total : tid; task < total; task += oThr) {
 			uint32_t r = task;
 			if (r < nMFIn) {
-				const uint32_t z = r / (numNC * nMFNC), k = r % (numNC * nMFNC);
+				const uint32_t z = Z == 1 ? 0u : r / (numNC * nMFNC), k = Z == 1 ? r : r % (numNC * nMFNC);
 				const uint32_t src = N->zones[z].pNCfromMFtoNC[k];
 				N->zones[z].inputMFNC[k] = mfRaw ? mfRaw[src] : (uint8_t)spikeBit(sMF, src);
 				continue;
 			}
 			r -= nMFIn;
 			if (r < nBCPC) {
-				const uint32_t z = r / numPC, i = r % numPC;
+				const uint32_t z = Z == 1 ? 0u : r / numPC, i = Z == 1 ? r : r % numPC;
 				const DevZone &Q = N->zones[z];
 				uint32_t c = 0;
 				const uint32_t e0 = Q.bcpcStart[i], e1 = Q.bcpcStart[i + 1];
@@ -1520,13 +1520,13 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			r -= nBCPC;
 			if (r < nSCPC) {
 				const uint32_t per = numPC * N->numpPCfromSCtoPC;
-				const uint32_t z = r / per, k = r % per;
+				const uint32_t z = Z == 1 ? 0u : r / per, k = Z == 1 ? r : r % per;
 				N->zones[z].inputSCPC[k] = sApSC[N->zones[z].pPCfromSCtoPC[k]];
 				continue;
 			}
 			r -= nSCPC;
 			if (r < nPCBC) {
-				const uint32_t z = r / numBC, i = r % numBC;
+				const uint32_t z = Z == 1 ? 0u : r / numBC, i = Z == 1 ? r : r % numBC;
 				const DevZone &Q = N->zones[z];
 				uint32_t c = 0;
 				const uint32_t e0 = Q.pcbcStart[i], e1 = Q.pcbcStart[i + 1];
@@ -1538,13 +1538,13 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			r -= nPCBC;
 			if (r < nPCNC) {
 				const uint32_t per = numNC * N->numpNCfromPCtoNC;
-				const uint32_t z = r / per, k = r % per;
+				const uint32_t z = Z == 1 ? 0u : r / per, k = Z == 1 ? r : r % per;
 				N->zones[z].inputPCNC[k] = N->zones[z].apPC[N->zones[z].pNCfromPCtoNC[k]];
 				continue;
 			}
 			r -= nPCNC;
 			if (r < nIO) {
-				const uint32_t z = r / numIO, i = r % numIO;
+				const uint32_t z = Z == 1 ? 0u : r / numIO, i = Z == 1 ? r : r % numIO;
 				const DevZone &Q = N->zones[z];
 				const uint8_t ap = Q.apIO[i];
 				const int32_t timer = Q.pfPCPlastTimerIO[i];
@@ -1558,7 +1558,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			}
 			r -= nIO;
 			if (r < nNC) {
-				const uint32_t z = r / numNC, i = r % numNC;
+				const uint32_t z = Z == 1 ? 0u : r / numNC, i = Z == 1 ? r : r % numNC;
 				const DevZone &Q = N->zones[z];
 				const uint8_t apNC = Q.apNC[i];
 				float p = Q.synIOPReleaseNC[i];
@@ -1603,7 +1603,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			uint32_t r = task;
 			if (r < nDraw) {
 				const uint32_t per = numIO * nIONC;
-				const uint32_t z = r / per, k = r % per;
+				const uint32_t z = Z == 1 ? 0u : r / per, k = Z == 1 ? r : r % per;
 				const uint32_t i = k / nIONC, j = k % nIONC;
 				const DevZone &Q = N->zones[z];
 				const double u = (double)rng::uniform24Keyed(Q.ncioKey, rng::ncioCounter(t, i, j, nIONC));
@@ -1612,7 +1612,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			}
 			r -= nDraw;
 			if (r < nW) {
-				const uint32_t z = r / (numNC * nMFNC), k = r % (numNC * nMFNC);
+				const uint32_t z = Z == 1 ? 0u : r / (numNC * nMFNC), k = Z == 1 ? r : r % (numNC * nMFNC);
 				const DevZone &Q = N->zones[z];
 				const int doLTD = sFlags[2 * z], doLTP = sFlags[2 * z + 1];
 				const float wOld = Q.mfSynWeightNC[k];
@@ -1627,7 +1627,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			}
 			r -= nW;
 			{
-				const uint32_t z = r / numIO, i = r % numIO;
+				const uint32_t z = Z == 1 ? 0u : r / numIO, i = Z == 1 ? r : r % numIO;
 				const DevZone &Q = N->zones[z];
 				uint8_t sel = 0;
 				if (nextPlast) {
