@@ -269,6 +269,23 @@ struct DevNet {
 constexpr uint32_t kStageNetBytes = (uint32_t)((sizeof(DevNet) + 15) & ~(size_t)15);
 constexpr uint32_t kStageArenaOff = kStageNetBytes + 16;
 #if defined(__CUDACC__)
+// t mod d and t / d for a step count t: 32-bit arithmetic while both fit in
+// 32 bits (a 64-bit division is a long out-of-line routine that measured
+// microseconds on the small-cell update's critical path), the 64-bit form
+// beyond.
+__device__ __forceinline__ uint32_t stepMod(uint64_t t, uint32_t d)
+{
+	return (t >> 32) == 0 ? (uint32_t)t % d : (uint32_t)(t % d);
+}
+__device__ __forceinline__ uint64_t stepMod(uint64_t t, uint64_t d)
+{
+	return ((t | d) >> 32) == 0 ? (uint64_t)((uint32_t)t % (uint32_t)d) : t % d;
+}
+__device__ __forceinline__ uint64_t stepDiv(uint64_t t, uint32_t d)
+{
+	return (t >> 32) == 0 ? (uint64_t)((uint32_t)t / d) : t / d;
+}
+
 // Steps the network has completed: every descriptor allocation holds the
 // step counter at kStageNetBytes (DevNet::tBase points there), so kernels
 // read it together with the descriptor instead of after it.

@@ -283,14 +283,14 @@ __global__ void __launch_bounds__(kPassThreads) grPassKernel(const DevNet *const
 	uint32_t *sSC = sBC + N->bcLocal;
 	float *sX = reinterpret_cast<float *>(sSC + N->scLocal);
 
-	const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	const uint32_t *mfSrc = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 	const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
 	for (uint32_t i = threadIdx.x; i < N->mfWords; i += blockDim.x) sMF[i] = mfSrc[i];
 	for (uint32_t i = threadIdx.x; i < N->goWords; i += blockDim.x) sGO[i] = goSrc[i];
 	for (uint32_t i = threadIdx.x; i < N->bcLocal + N->scLocal; i += blockDim.x) sBC[i] = 0;
 	__syncthreads();
 
-	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
+	const bool plastStep = stepMod(t, N->tsPerHistBinGR) == 0;
 	float stepW[kMaxZones];
 	for (uint32_t z = 0; z < Z; z++) {
 		stepW[z] = 0.0f;
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	}
 	__syncthreads();
 
-	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
+	const bool plastStep = stepMod(t, N->tsPerHistBinGR) == 0;
 	const uint32_t rowBase = pc * rows;  // first row of the tile in the [numGR/bs][bs] view
 	const uint32_t bcBase = (pc * P) >> N->bcShift, scBase = (pc * P) >> N->scShift;
 
@@ -556,7 +556,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	} else {
 		// ---- consumers: warp w updates rows w, w+W, ..., w+(RW-1)W of every
 		// stage.  They stage the spike tables while the first copies fly.
-		const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+		const uint32_t *mfSrc = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 		const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
 		// one spike word per thread and round (the loads of a round in flight
 		// together), spread to a byte per cell: (nibble * 0x204081) & 0x01010101
@@ -860,8 +860,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(con
 		}
 		tma::fenceBarrierInit();
 	}
-	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
-	const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	const bool plastStep = stepMod(t, N->tsPerHistBinGR) == 0;
+	const uint32_t *mfSrc = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 	const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * N->goWords;
 	for (uint32_t i = threadIdx.x; i < 32u * N->mfWords; i += blockDim.x) sMF[i] = (uint8_t)spikeBit(mfSrc, i);
 	for (uint32_t i = threadIdx.x; i < 32u * N->goWords; i += blockDim.x) sGO[i] = (uint8_t)spikeBit(goSrc, i);
@@ -1122,7 +1122,7 @@ __device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm
 	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u;
 	const uint32_t numGO = N->numGO;
 	const uint32_t G = (uint32_t)((t - 1) & 1);
-	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	const uint32_t *mfW = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 	uint64_t *sExp2 = reinterpret_cast<uint64_t *>(sm);
 	uint32_t *sMF = sm + 64;
 	uint32_t *sMFGO = sMF + N->mfWords;  // MF->GO input counts of this step
@@ -1261,15 +1261,19 @@ struct ZoneIn {
 };
 
 __device__ void protocolRecordWarp(const DevNet *__restrict__ N, uint64_t t, uint32_t lane);
+__device__ void publishNC(const DevNet *N, uint64_t t, uint8_t *box);
 
-__device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm, const ZoneIn &in)
+// ncMailbox: mapped host memory that receives the step's NC spikes as soon
+// as they are final (publishNC), or null.
+__device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm, const ZoneIn &in,
+		uint8_t *ncMailbox)
 {
 	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u, warp = tid >> 5, nWarps = nThr >> 5;
 	const uint32_t Z = N->numZones;
 	const uint32_t numMF = N->numMF, numPC = N->numPC, numBC = N->numBC, numSC = N->numSC, numNC = N->numNC,
 		numIO = N->numIO;
 	const uint32_t R = (uint32_t)((t + 1) % 3);
-	const uint8_t *mfRaw = N->hasMFRaw ? N->mfRaw + (size_t)((t - 1) % N->mfRing) * numMF : nullptr;
+	const uint8_t *mfRaw = N->hasMFRaw ? N->mfRaw + (size_t)stepMod(t - 1, N->mfRing) * numMF : nullptr;
 	HostCtl *ctl = N->ctl;
 	const uint32_t nMFNC = N->numpNCfromMFtoNC, nIONC = N->numpIOfromNCtoIO;
 	const uint32_t *sMF = in.mf;
@@ -1464,6 +1468,10 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 		}
 	}
 	barSync(2, gThr);
+	// every NC spike of the step is final: a host waiting on them gets them
+	// now, from the group's last warp, which has no IO update (its system
+	// fence overlaps the IO updates)
+	if (ncMailbox && tid == nThr - 32u) publishNC(N, t, ncMailbox);
 	for (uint32_t task = tid; task < Z * numIO; task += nThr) {
 		const uint32_t z = Z == 1 ? 0u : task / numIO, i = Z == 1 ? task : task % numIO;
 		const DevZone &Q = N->zones[z];
@@ -1487,7 +1495,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// ---- microzone outputs (mzone.cpp:409-524) and the MF->NC population
 	// bookkeeping (mzone.cpp:536-580): independent gathers, run as one flat
 	// task space so that their loads are in flight together
-	const bool popStep = (t % N->tsPerPopHistBinPC) == 0;
+	const bool popStep = stepMod(t, N->tsPerPopHistBinPC) == 0;
 	// the device protocol's record of step t (its NC and PC spikes are final
 	// now) on the last warp, beside the outputs: neither reads what the
 	// other writes
@@ -1598,7 +1606,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// (mzone.cpp:586-600), plasticity selector of the next step
 	{
 		const uint32_t nDraw = Z * numIO * nIONC, nW = popStep ? Z * numNC * nMFNC : 0, nSel = Z * numIO;
-		const bool nextPlast = ((t + 1) % N->tsPerHistBinGR) == 0;
+		const bool nextPlast = stepMod(t + 1, N->tsPerHistBinGR) == 0;
 		for (uint32_t task = tid; task < nDraw + nW + nSel; task += nThr) {
 			uint32_t r = task;
 			if (r < nDraw) {
@@ -1639,7 +1647,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 		}
 	}
 	__syncthreads();
-	if ((t % N->numTSinMFHist) == 0)
+	if (stepMod(t, N->numTSinMFHist) == 0)
 		for (uint32_t i = tid; i < numMF; i += nThr) N->histMF[i] = 0;
 	// the error drive is consumed once (mzone.cpp:334)
 	if (tid < Z) ctl->errDrive[tid] = 0;
@@ -1687,7 +1695,7 @@ __device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &i
 	const uint32_t Z = N->numZones, numPC = N->numPC, bs = N->bs, R = (uint32_t)((t + 1) % 3);
 	const ZoneInputLayout L = zoneInputLayout(N->mfWords, N->numBC, N->numSC, Z, numPC, N->bs);
 	const uint32_t nPC = numPC * bs;
-	const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+	const uint32_t *mfW = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 	// small pieces as 4-byte words: table, MF bits, BC counts, SC counts
 	const uint32_t e0 = 64, e1 = e0 + N->mfWords, e2 = e1 + N->numBC, e3 = e2 + N->numSC;
 	for (uint32_t w = tid; w < e3; w += nThr) {
@@ -1774,19 +1782,19 @@ __device__ __forceinline__ float stateVarRate(const DevProtocol *P, uint32_t i, 
 __global__ void stateVarRatesKernel(const DevNet *N, uint64_t row, float *out)
 {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < N->numMF) out[i] = stateVarRate(N->proto, i, row % N->proto->svSteps);
+	if (i < N->numMF) out[i] = stateVarRate(N->proto, i, stepMod(row, N->proto->svSteps));
 }
 
 __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 {
 	DevProtocol *P = N->proto;
 	const uint64_t k = t - P->startT;  // index of step t+1 within the protocol
-	const int32_t time = (int32_t)(k % P->trialSteps);
-	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const int32_t time = (int32_t)stepMod(k, P->trialSteps);
+	const uint32_t trial = (uint32_t)stepDiv(k, P->trialSteps);
 	const bool csTrial = trial >= P->csStartTrial;
 	const float *freq = P->freqBG;
 	if (csTrial && time >= P->csOn && time < P->csOff) freq = time < P->csPOff ? P->freqCSPhasic : P->freqCSTonic;
-	uint32_t *bits = const_cast<uint32_t *>(N->mfBits) + (size_t)(t % N->mfRing) * N->mfWords;
+	uint32_t *bits = const_cast<uint32_t *>(N->mfBits) + (size_t)stepMod(t, N->mfRing) * N->mfWords;
 	const uint64_t ctr = (t + 1) << 20;
 	const uint32_t numMF = N->numMF, words = N->mfWords;
 	for (uint32_t base = 0; base < 32u * words; base += blockDim.x) {
@@ -1794,7 +1802,7 @@ __device__ void protocolPrepare(const DevNet *__restrict__ N, uint64_t t)
 		uint32_t ap = 0;
 		if (i < numMF) {
 			float th = P->mfThresh[i];
-			const float f = P->svValues ? stateVarRate(P, i, k % P->svSteps) : freq[i];
+			const float f = P->svValues ? stateVarRate(P, i, stepMod(k, P->svSteps)) : freq[i];
 			th = th + (1 - th) * P->mfThreshDecay;
 			const double u = (double)rng::uniform24Keyed(P->mfKey, ctr | i);
 			ap = u < ((f * P->sPerTS) * th);
@@ -1853,8 +1861,8 @@ __device__ void protocolRecordWarp(const DevNet *__restrict__ N, uint64_t t, uin
 	const int32_t recFrom = P->recFrom;
 	if (t < startT + 1) return;
 	const uint64_t k = t - 1 - startT;
-	const int32_t time = (int32_t)(k % trialSteps);
-	const uint32_t trial = (uint32_t)(k / trialSteps);
+	const int32_t time = (int32_t)stepMod(k, trialSteps);
+	const uint32_t trial = (uint32_t)stepDiv(k, trialSteps);
 	const DevZone &Q = N->zones[0];
 	const int32_t ct = time - recFrom;
 	const bool rec = trial >= dataStart && trial < dataStart + numData && ct >= 0 && ct < (int32_t)recLen;
@@ -1912,8 +1920,8 @@ __global__ void grPSHKernel(const DevNet *N, uint32_t stepOffset)
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 	if (!P || !P->grPSH || t < P->startT + 1) return;
 	const uint64_t k = t - 1 - P->startT;
-	const int32_t time = (int32_t)(k % P->trialSteps);
-	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const int32_t time = (int32_t)stepMod(k, P->trialSteps);
+	const uint32_t trial = (uint32_t)stepDiv(k, P->trialSteps);
 	const int32_t ct = time - P->recFrom;
 	if (trial < P->dataStartTrial || trial >= P->dataStartTrial + P->numDataTrials || ct < 0 || ct >= P->recLen)
 		return;
@@ -1948,8 +1956,8 @@ __device__ void trialDataCell(const DevNet *N, uint32_t stepOffset, uint32_t c)
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 	if (!P || !P->tdPSH || t < P->startT + 1) return;
 	const uint64_t k = t - 1 - P->startT;
-	const int32_t time = (int32_t)(k % P->trialSteps);
-	const uint32_t trial = (uint32_t)(k / P->trialSteps);
+	const int32_t time = (int32_t)stepMod(k, P->trialSteps);
+	const uint32_t trial = (uint32_t)stepDiv(k, P->trialSteps);
 	const int32_t ct = time - P->recFrom;
 	if (trial < P->dataStartTrial || trial >= P->dataStartTrial + P->numDataTrials || ct < 0 || ct >= P->recLen)
 		return;
@@ -2040,8 +2048,8 @@ __global__ void __launch_bounds__(kTailThreads) protocolPrimeKernel(const DevNet
 // Step t's NC spikes into mapped host memory for a host that waits on them
 // (single steps through the reference API, cbm_sim_export's AP_NC): every
 // zone's bytes from offset 8, a system-scope fence, then the step number as
-// the 8-byte stamp at offset 0.  One thread, at the end of the microzone
-// CTA, where nothing waits on it.
+// the 8-byte stamp at offset 0.  One thread of the microzone CTA, once the
+// NC updates of the step are done.
 __device__ void publishNC(const DevNet *N, uint64_t t, uint8_t *box)
 {
 	const uint32_t numNC = N->numNC;
@@ -2080,17 +2088,16 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 			__syncthreads();
 			const ZoneInputLayout L = zoneInputLayout(sNet->mfWords, sNet->numBC, sNet->numSC, sNet->numZones,
 					sNet->numPC, sNet->bs);
-			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(dyn + L.bytes), in);
+			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(dyn + L.bytes), in, ncMailbox);
 			__syncthreads();
 			stageOut(N, base, sNet);
-			if (ncMailbox && threadIdx.x == 0) publishNC(sNet, t, ncMailbox);
 		} else {
 			// global-memory mode: the table and the MF bits in shared
 			// memory, then the role's scratch
 			const uint64_t t = stepsDone(N) + 1 + stepOffset;
 			uint64_t *sExp2 = reinterpret_cast<uint64_t *>(tailSmem);
 			uint32_t *sMF = tailSmem + 64;
-			const uint32_t *mfW = N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords;
+			const uint32_t *mfW = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 			for (uint32_t i = threadIdx.x; i < N->mfWords; i += blockDim.x) sMF[i] = mfW[i];
 			if (threadIdx.x < 32) sExp2[threadIdx.x] = kExp2Tab[threadIdx.x];
 			const uint32_t R = (uint32_t)((t + 1) % 3);
@@ -2107,11 +2114,7 @@ __global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *
 				in.err = nullptr;
 			}
 			__syncthreads();
-			zoneRole(N, t, sMF + ((N->mfWords + 3) & ~3u), in);
-			if (ncMailbox) {
-				__syncthreads();
-				if (threadIdx.x == 0) publishNC(N, t, ncMailbox);
-			}
+			zoneRole(N, t, sMF + ((N->mfWords + 3) & ~3u), in, ncMailbox);
 		}
 	} else {
 		const uint64_t t = stepsDone(N) + 1 + stepOffset;

@@ -355,11 +355,11 @@ __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel
 	uint8_t *sGO = sMF + 32u * mfWords;           // last step's GO spikes, a byte per cell
 	float *sStep = reinterpret_cast<float *>(sGO + ((32u * goWords + 15u) & ~15u));  // PF->PC step per PC
 
-	const bool plastStep = (t % N->tsPerHistBinGR) == 0;
+	const bool plastStep = stepMod(t, N->tsPerHistBinGR) == 0;
 
 	// ---- prologue: spike tables, plasticity steps, counters
 	{
-		const uint32_t *mfSrc = N->mfBits + (size_t)((t - 1) % N->mfRing) * mfWords;
+		const uint32_t *mfSrc = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * mfWords;
 		const uint32_t *goSrc = N->goBits + (size_t)((t - 1) & 1) * goWords;
 		const uint32_t nWords = mfWords + goWords;
 		for (uint32_t w = threadIdx.x; w < nWords; w += blockDim.x) {
@@ -491,8 +491,8 @@ __global__ void __launch_bounds__(32 * kVecWarps, kVecBatchMinBlocks) grPassVecB
 				__syncwarp();
 				if (lane == 0) net = vecNet(N, t);
 				__syncwarp();
-				plastStep = (t % N->tsPerHistBinGR) == 0;
-				sp = SpikeBits{N->mfBits + (size_t)((t - 1) % N->mfRing) * N->mfWords,
+				plastStep = stepMod(t, N->tsPerHistBinGR) == 0;
+				sp = SpikeBits{N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords,
 						N->goBits + (size_t)((t - 1) & 1) * N->goWords};
 				bcCnt = N->bcCount + (size_t)(t % 3) * N->numBC;
 				scCnt = N->scCount + (size_t)(t % 3) * N->numSC;
