@@ -1283,15 +1283,17 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	float *ioScratch = ncScratch + (size_t)Z * numNC * 2 * nMFNC;
 	int *sFlags = reinterpret_cast<int *>(ioScratch + (size_t)Z * numIO * nIONC);
 
-	// The PC/BC/SC/MF updates (warps [0, half)) and the NC/IO updates (warps
-	// [half, all)) of a step do not read each other's results; the two warp
-	// groups run them side by side and meet before the outputs.
-	const uint32_t half = nWarps / 2, gThr = half * 32u;
-	const bool groupA = warp < half;
-	const uint32_t gTid = groupA ? tid : tid - gThr, gWarp = groupA ? warp : warp - half;
+	// The PC/BC/SC/MF updates (warps [0, aW)) and the NC/IO updates (warps
+	// [aW, all)) of a step do not read each other's results; the two warp
+	// groups run them side by side and meet before the outputs.  The first
+	// group (a warp per PC, then the element-parallel BC/SC/MF updates) gets
+	// two thirds of the warps, the second (a warp per NC) the rest.
+	const uint32_t aW = nWarps - nWarps / 3, aThr = aW * 32u, bW = nWarps - aW, bThr = bW * 32u;
+	const bool groupA = warp < aW;
+	const uint32_t gTid = groupA ? tid : tid - aThr, gWarp = groupA ? warp : warp - aW;
 	if (groupA) {
 	// (tid, nThr, warp, nWarps) of the PC/BC/SC/MF warp group
-	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
+	const uint32_t tid = gTid, nThr = aThr, warp = gWarp, nWarps = aW;
 	// ---- phase 1 (cbmsimcore.cpp:192-200): PC and BC per zone, SC, and the
 	// MF bookkeeping; the updates are independent.
 	// calcPCActivities (mzone.cpp:187-226), one warp per PC; the SC
@@ -1378,14 +1380,14 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 		N->histMF[c] = N->histMF[c] || (m > 0);
 		N->apBufMF[c] = (N->apBufMF[c] << 1) | (m * 0x00000001u);
 	}
-	barSync(1, gThr);
+	barSync(1, aThr);
 	for (uint32_t i = tid; i < numBC; i += nThr) N->bcCount[(size_t)R * numBC + i] = 0;
 	for (uint32_t i = tid; i < numSC; i += nThr) N->scCount[(size_t)R * numSC + i] = 0;
 	}
 
 	if (!groupA) {
 	// (tid, nThr, warp, nWarps) of the NC/IO warp group
-	const uint32_t tid = gTid, nThr = gThr, warp = gWarp, nWarps = half;
+	const uint32_t tid = gTid, nThr = bThr, warp = gWarp, nWarps = bW;
 	// this step's error drive of the IO a thread updates at the end, loaded
 	// now so that the load overlaps the synapse and NC updates
 	const float errOwn = tid < Z * numIO ? (in.err ? in.err[Z == 1 ? 0u : tid / numIO] : errDriveOf(N, t, Z == 1 ? 0u : tid / numIO)) : 0.0f;
@@ -1467,7 +1469,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 			Q.threshNC[i] = ap * N->threshMaxNC + (!ap) * th;
 		}
 	}
-	barSync(2, gThr);
+	barSync(2, bThr);
 	// every NC spike of the step is final: a host waiting on them gets them
 	// now, from the group's last warp, which has no IO update (its system
 	// fence overlaps the IO updates)
@@ -2066,7 +2068,7 @@ __device__ void publishNC(const DevNet *N, uint64_t t, uint8_t *box)
 // role runs on shared-memory copies of its arrays and inputs when they fit
 // (one bulk copy in and one out per step instead of a global round trip per
 // phase).
-__global__ void __launch_bounds__(kTailThreads) tailKernel(const DevNet *const *nets, const uint32_t *stageBytes,
+__global__ void __launch_bounds__(kTailThreads, 1) tailKernel(const DevNet *const *nets, const uint32_t *stageBytes,
 		uint32_t stepOffset, const DevNet *net0, uint32_t stage0, uint8_t *ncMailbox)
 {
 	// the GR pass of the same step may launch once these CTAs are resident

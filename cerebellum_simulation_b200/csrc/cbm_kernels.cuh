@@ -6,7 +6,10 @@
 namespace cbm {
 
 constexpr int kPassThreads = 256;
-constexpr int kTailThreads = 1024;
+// 24 warps: at 80 registers a thread the small-cell update keeps every value
+// in registers (at 1024 threads, 64 registers, it spilled, and the spill
+// reloads went to L2 between its phases)
+constexpr int kTailThreads = 768;
 
 __global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOffset, int numNets,
 		uint32_t stepOffset);
