@@ -44,6 +44,17 @@ constexpr uint32_t kOut16MaxGO = 2047u;
 // (the rest go to per-tile lists).
 constexpr uint32_t kOutInline = 4u;
 
+// A step's MF spike words passed by value to the step's kernels (one
+// network launched a step at a time: the host packs the caller's input and
+// the launch carries it, with no copy ahead of the kernels).  n = 0: the
+// kernels read the network's MF ring.  Networks of up to 32 x kMFParamWords
+// - 1 fibres.
+constexpr uint32_t kMFParamWords = 64;
+struct MFParam {
+	uint32_t n;
+	uint32_t w[kMFParamWords];
+};
+
 // A device array that a small-cell CTA copies into shared memory for the
 // step (and back when it changes): the CTA then runs on a shared-memory copy
 // of the network descriptor whose pointer at fieldOff points into the copy.

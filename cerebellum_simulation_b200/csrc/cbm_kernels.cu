@@ -267,6 +267,7 @@ __device__ __forceinline__ const DevNet *locateNet(const DevNet *const *nets, co
 __global__ void __launch_bounds__(kPassThreads) grPassKernel(const DevNet *const *nets,
 		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
 {
+	PassStepGuard stepGuard;
 	uint32_t local;
 	const DevNet *__restrict__ N = locateNet(nets, blockOffset, numNets, blockIdx.x, local);
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
@@ -437,8 +438,10 @@ template <> struct PassShape<1> {
 
 template <int W, int RW, int S, int MINB, int MS, int SH>
 __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevNet *const *nets,
-		const uint32_t *blockOffset, int numNets, uint32_t stepOffset, const DevNet *net0)
+		const uint32_t *blockOffset, int numNets, uint32_t stepOffset, const DevNet *net0,
+		const __grid_constant__ MFParam mfp)
 {
+	PassStepGuard stepGuard;
 	using Sh = PassShape<SH>;
 	constexpr uint32_t R = W * RW;
 	// one network: its descriptor comes as a parameter (a round trip fewer)
@@ -567,7 +570,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 #pragma unroll
 			for (int u = 0; u < 2; u++) {
 				const uint32_t w = w0 + u * 32u * W + threadIdx.x;
-				v[u] = w < nWords ? __ldg(w < mfWords ? mfSrc + w : goSrc + (w - mfWords)) : 0u;
+				// MF words from the launch when it carries them (mfp.n > 0)
+				v[u] = w >= nWords ? 0u : w >= mfWords ? __ldg(goSrc + (w - mfWords)) : mfp.n ? mfp.w[w] : __ldg(mfSrc + w);
 			}
 #pragma unroll
 			for (int u = 0; u < 2; u++) {
@@ -750,7 +754,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	X(4, 2, 2, 4, 4) X(8, 1, 3, 2, 0) X(4, 1, 4, 1, 0) X(2, 1, 4, 1, 0) X(1, 1, 4, 1, 0)
 #define CBM_PASS_TMA_INST(W, RW, S, B, M) \
 	template __global__ void grPassTmaKernel<W, RW, S, B, M, 0>(const DevNet *const *, const uint32_t *, int, uint32_t, \
-		const DevNet *);
+		const DevNet *, const __grid_constant__ MFParam);
 CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_INST)
 
 int passTmaConfigCount()
@@ -833,6 +837,7 @@ template <int W, int S, int MINB, int MS>
 __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(const DevNet *const *nets,
 		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
 {
+	PassStepGuard stepGuard;
 	(void)blockOffset; (void)numNets;
 	constexpr uint32_t R = 2 * W;
 	const DevNet *__restrict__ N = nets[0];
@@ -1117,12 +1122,12 @@ __device__ __forceinline__ float orderedSum(const float *x, uint32_t n)
 // Golgi role (one CTA per network): calcGOActivities, updateMFtoGOOut and
 // updateGOtoGOOut (innet.cpp:816-980).  Reads GR->GO counts of pass(t-1),
 // writes GO spikes of step t for pass(t+1).
-__device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm)
+// mfW: the step's MF spike words (its ring slot, or the launch's copy).
+__device__ void golgiRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm, const uint32_t *mfW)
 {
 	const uint32_t tid = threadIdx.x, nThr = blockDim.x, lane = tid & 31u;
 	const uint32_t numGO = N->numGO;
 	const uint32_t G = (uint32_t)((t - 1) & 1);
-	const uint32_t *mfW = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 	uint64_t *sExp2 = reinterpret_cast<uint64_t *>(sm);
 	uint32_t *sMF = sm + 64;
 	uint32_t *sMFGO = sMF + N->mfWords;  // MF->GO input counts of this step
@@ -1263,6 +1268,10 @@ struct ZoneIn {
 __device__ void protocolRecordWarp(const DevNet *__restrict__ N, uint64_t t, uint32_t lane);
 __device__ void publishNC(const DevNet *N, uint64_t t, uint8_t *box);
 
+// Warps of the microzone CTA's PC/BC/SC/MF group (the first ones); the rest
+// form the NC/IO group.
+__device__ __forceinline__ uint32_t zoneGroupAWarps(uint32_t nWarps) { return nWarps - nWarps / 3; }
+
 // ncMailbox: mapped host memory that receives the step's NC spikes as soon
 // as they are final (publishNC), or null.
 __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm, const ZoneIn &in,
@@ -1276,8 +1285,12 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	const uint8_t *mfRaw = N->hasMFRaw ? N->mfRaw + (size_t)stepMod(t - 1, N->mfRing) * numMF : nullptr;
 	HostCtl *ctl = N->ctl;
 	const uint32_t nMFNC = N->numpNCfromMFtoNC, nIONC = N->numpIOfromNCtoIO;
-	const uint32_t *sMF = in.mf;
-	const uint64_t *exp2 = in.exp2;
+	// the step inputs (`in`) are ready for the PC/BC/SC/MF group when it
+	// starts and for every thread after the two groups meet; the NC/IO group
+	// needs none of them (its table is the global copy, its error drives
+	// come from global memory), so that it may start before they arrive
+	const uint32_t *sMF = nullptr;
+	const uint64_t *exp2 = kExp2Tab;
 	uint8_t *sApSC = reinterpret_cast<uint8_t *>(sm);
 	float *ncScratch = reinterpret_cast<float *>(sApSC + ((numSC + 15) & ~15u));
 	float *ioScratch = ncScratch + (size_t)Z * numNC * 2 * nMFNC;
@@ -1288,9 +1301,13 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	// groups run them side by side and meet before the outputs.  The first
 	// group (a warp per PC, then the element-parallel BC/SC/MF updates) gets
 	// two thirds of the warps, the second (a warp per NC) the rest.
-	const uint32_t aW = nWarps - nWarps / 3, aThr = aW * 32u, bW = nWarps - aW, bThr = bW * 32u;
+	const uint32_t aW = zoneGroupAWarps(nWarps), aThr = aW * 32u, bW = nWarps - aW, bThr = bW * 32u;
 	const bool groupA = warp < aW;
 	const uint32_t gTid = groupA ? tid : tid - aThr, gWarp = groupA ? warp : warp - aW;
+	if (groupA) {
+		sMF = in.mf;
+		exp2 = in.exp2;
+	}
 	if (groupA) {
 	// (tid, nThr, warp, nWarps) of the PC/BC/SC/MF warp group
 	const uint32_t tid = gTid, nThr = aThr, warp = gWarp, nWarps = aW;
@@ -1390,7 +1407,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	const uint32_t tid = gTid, nThr = bThr, warp = gWarp, nWarps = bW;
 	// this step's error drive of the IO a thread updates at the end, loaded
 	// now so that the load overlaps the synapse and NC updates
-	const float errOwn = tid < Z * numIO ? (in.err ? in.err[Z == 1 ? 0u : tid / numIO] : errDriveOf(N, t, Z == 1 ? 0u : tid / numIO)) : 0.0f;
+	const float errOwn = tid < Z * numIO ? errDriveOf(N, t, Z == 1 ? 0u : tid / numIO) : 0.0f;
 	// ---- phase 2: calcIOActivities (mzone.cpp:258-339) element-parallel,
 	// calcNCActivities (mzone.cpp:341-407) one warp per NC.
 	// NC->IO conductances: one thread per synapse, numbered from the group's
@@ -1478,7 +1495,7 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 		const uint32_t z = Z == 1 ? 0u : task / numIO, i = Z == 1 ? task : task % numIO;
 		const DevZone &Q = N->zones[z];
 		const float v0 = Q.vIO[i], vCouple = Q.vCoupleIO[i], th0 = Q.threshIO[i];
-		const float errDrive = task == tid ? errOwn : (in.err ? in.err[z] : errDriveOf(N, t, z));
+		const float errDrive = task == tid ? errOwn : errDriveOf(N, t, z);
 		const uint32_t apBuf = Q.apBufIO[i];
 		float gNCSum = 0;
 		for (uint32_t j = 0; j < nIONC; j++) gNCSum = gNCSum + ioScratch[(size_t)task * nIONC + j];
@@ -1493,6 +1510,8 @@ __device__ void zoneRole(const DevNet *__restrict__ N, uint64_t t, uint32_t *sm,
 	}
 	}
 	__syncthreads();
+	sMF = in.mf;
+	exp2 = in.exp2;
 
 	// ---- microzone outputs (mzone.cpp:409-524) and the MF->NC population
 	// bookkeeping (mzone.cpp:536-580): independent gathers, run as one flat
@@ -1691,9 +1710,11 @@ __device__ void stageIn(const DevNet *N, uint8_t *base, uint32_t bytes)
 // (ZoneInputLayout) after the staging block and point `in` at them; the
 // caller synchronises the CTA before use.  N is the staged descriptor, whose
 // pointers to these inputs are global.
-__device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &in)
+// mfParam: the launch's copy of the step's MF spike words, or null (the
+// network's MF ring).
+__device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &in, const uint32_t *mfParam,
+		uint32_t tid, uint32_t nThr)
 {
-	const uint32_t tid = threadIdx.x, nThr = blockDim.x;
 	const uint32_t Z = N->numZones, numPC = N->numPC, bs = N->bs, R = (uint32_t)((t + 1) % 3);
 	const ZoneInputLayout L = zoneInputLayout(N->mfWords, N->numBC, N->numSC, Z, numPC, N->bs);
 	const uint32_t nPC = numPC * bs;
@@ -1704,7 +1725,15 @@ __device__ void stageInputs(const DevNet *N, uint64_t t, uint8_t *dyn, ZoneIn &i
 		const void *src;
 		uint8_t *dst;
 		if (w < e0) { src = reinterpret_cast<const uint32_t *>(kExp2Tab) + w; dst = dyn + L.exp2 + 4 * w; }
-		else if (w < e1) { src = mfW + (w - e0); dst = dyn + L.mf + 4 * (w - e0); }
+		else if (w < e1) {
+			dst = dyn + L.mf + 4 * (w - e0);
+			if (mfParam) {
+				// the launch's copy: not global memory, so a plain store
+				*reinterpret_cast<uint32_t *>(dst) = mfParam[w - e0];
+				continue;
+			}
+			src = mfW + (w - e0);
+		}
 		else if (w < e2) { src = N->bcCount + (size_t)R * N->numBC + (w - e1); dst = dyn + L.bc + 4 * (w - e1); }
 		else { src = N->scCount + (size_t)R * N->numSC + (w - e2); dst = dyn + L.sc + 4 * (w - e2); }
 		cpAsync4(dst, src);
@@ -2069,10 +2098,12 @@ __device__ void publishNC(const DevNet *N, uint64_t t, uint8_t *box)
 // (one bulk copy in and one out per step instead of a global round trip per
 // phase).
 __global__ void __launch_bounds__(kTailThreads, 1) tailKernel(const DevNet *const *nets, const uint32_t *stageBytes,
-		uint32_t stepOffset, const DevNet *net0, uint32_t stage0, uint8_t *ncMailbox)
+		uint32_t stepOffset, const DevNet *net0, uint32_t stage0, uint8_t *ncMailbox, const __grid_constant__ MFParam mfp)
 {
-	// the GR pass of the same step may launch once these CTAs are resident
-	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+	// the previous step first (its GR pass, and through that pass's exit
+	// wait its small-cell kernel); then this step's GR pass may launch
+	pdlWait();
+	pdlLaunchDependents();
 	const uint32_t net = blockIdx.x >> 1;
 	// one network: descriptor and staging size come as parameters
 	const DevNet *__restrict__ N = net0 ? net0 : nets[net];
@@ -2086,8 +2117,13 @@ __global__ void __launch_bounds__(kTailThreads, 1) tailKernel(const DevNet *cons
 			const DevNet *sNet = reinterpret_cast<const DevNet *>(base);
 			const uint64_t t = *reinterpret_cast<const uint64_t *>(base + kStageNetBytes) + 1 + stepOffset;
 			uint8_t *dyn = base + bytes;
-			stageInputs(sNet, t, dyn, in);
-			__syncthreads();
+			// the PC/BC/SC/MF warp group copies the step inputs and waits for
+			// them; the NC/IO group, which needs none, starts its updates
+			const uint32_t aThr = 32u * zoneGroupAWarps(blockDim.x / 32u);
+			if (threadIdx.x < aThr) {
+				stageInputs(sNet, t, dyn, in, mfp.n ? mfp.w : nullptr, threadIdx.x, aThr);
+				barSync(1, aThr);
+			}
 			const ZoneInputLayout L = zoneInputLayout(sNet->mfWords, sNet->numBC, sNet->numSC, sNet->numZones,
 					sNet->numPC, sNet->bs);
 			zoneRole(sNet, t, reinterpret_cast<uint32_t *>(dyn + L.bytes), in, ncMailbox);
@@ -2099,7 +2135,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) tailKernel(const DevNet *cons
 			const uint64_t t = stepsDone(N) + 1 + stepOffset;
 			uint64_t *sExp2 = reinterpret_cast<uint64_t *>(tailSmem);
 			uint32_t *sMF = tailSmem + 64;
-			const uint32_t *mfW = N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
+			const uint32_t *mfW = mfp.n ? mfp.w : N->mfBits + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
 			for (uint32_t i = threadIdx.x; i < N->mfWords; i += blockDim.x) sMF[i] = mfW[i];
 			if (threadIdx.x < 32) sExp2[threadIdx.x] = kExp2Tab[threadIdx.x];
 			const uint32_t R = (uint32_t)((t + 1) % 3);
@@ -2120,7 +2156,13 @@ __global__ void __launch_bounds__(kTailThreads, 1) tailKernel(const DevNet *cons
 		}
 	} else {
 		const uint64_t t = stepsDone(N) + 1 + stepOffset;
-		golgiRole(N, t, tailSmem);
+		uint32_t *ring = const_cast<uint32_t *>(N->mfBits) + (size_t)stepMod(t - 1, N->mfRing) * N->mfWords;
+		if (mfp.n) {
+			// the launch's MF words into the ring, for the kernels after the
+			// step (this step's kernels read the launch's copy)
+			for (uint32_t i = threadIdx.x; i < mfp.n; i += blockDim.x) ring[i] = mfp.w[i];
+		}
+		golgiRole(N, t, tailSmem, mfp.n ? mfp.w : ring);
 		if (N->proto) {
 			__syncthreads();
 			protocolPrepare(N, t);
@@ -2140,6 +2182,21 @@ __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_
 {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n) out[i] = (uint8_t)(apBuf[i] & 1u);
+}
+
+// Second half of the measurement helpers' L2 flush: read back the buffer the
+// flush has just written, so that the lines the next step finds in L2 are
+// clean copies of it (the step is not charged for writing back the flush).
+// The sink is written only if the buffer held a value the flush never
+// writes, which keeps the loads live.
+__global__ void flushReadKernel(const uint4 *buf, size_t n, uint32_t *sink)
+{
+	uint32_t acc = 0;
+	for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+		const uint4 v = __ldcg(buf + i);
+		acc |= (v.x ^ 0x5a5a5a5au) | (v.y ^ 0x5a5a5a5au) | (v.z ^ 0x5a5a5a5au) | (v.w ^ 0x5a5a5a5au);
+	}
+	if (acc) atomicOr(sink, acc);
 }
 
 }  // namespace cbm

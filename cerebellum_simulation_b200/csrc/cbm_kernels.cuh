@@ -11,6 +11,26 @@ constexpr int kPassThreads = 256;
 // reloads went to L2 between its phases)
 constexpr int kTailThreads = 768;
 
+// Programmatic dependent launch between the two kernels of consecutive
+// steps.  Steps launched one at a time run as small-cell(t) -> pass(t) ->
+// small-cell(t+1) -> ..., each launched as the programmatic dependent of the
+// kernel before it, so that the next kernel is resident before its
+// predecessor ends.  Two rules keep that equal to full stream order:
+//  - the small-cell kernel waits for its predecessor (the previous step's
+//    GR pass) before it reads anything, and only then lets its own
+//    dependent (this step's GR pass) launch;
+//  - every thread of a GR pass waits at its exit for its predecessor (this
+//    step's small-cell kernel), so that a finished GR pass means a finished
+//    step.
+// A pass lets the next small-cell kernel launch from its start.  Launched
+// without the attribute (CUDA graphs), each wait returns at once.
+__device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdlLaunchDependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+struct PassStepGuard {
+	__device__ PassStepGuard() { pdlLaunchDependents(); }
+	__device__ ~PassStepGuard() { pdlWait(); }
+};
+
 __global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOffset, int numNets,
 		uint32_t stepOffset);
 // TMA GR pass with W consumer warps of RW rows each per stage, S stages
@@ -56,9 +76,11 @@ const void *pcTreeKernelFn();
 // its microzone CTA works on global memory).  With one network, net0 and
 // stage0 give its descriptor and staging size directly (else null, 0).
 // ncMailbox (one network, or null): mapped host memory that receives the
-// step's NC spikes and then the step number (publishNC).
+// step's NC spikes and then the step number (publishNC).  mfp.n > 0 (one
+// network): the step's MF spike words, which the Golgi CTA also writes into
+// the MF ring for the kernels after the step.
 __global__ void tailKernel(const DevNet *const *nets, const uint32_t *stageBytes, uint32_t stepOffset,
-		const DevNet *net0, uint32_t stage0, uint8_t *ncMailbox);
+		const DevNet *net0, uint32_t stage0, uint8_t *ncMailbox, const __grid_constant__ MFParam mfp);
 __global__ void protocolPrimeKernel(const DevNet *N);
 // GR peri-stimulus histogram of step t = stepsDone(N) + 1 + stepOffset, after
 // the GR pass of that step: 8 GR per thread.
@@ -70,6 +92,7 @@ __global__ void trialDataBatchKernel(const DevNet *const *nets, const uint32_t *
 		uint32_t stepOffset);
 __global__ void advanceStepKernel(uint64_t *const *tBases, int numNets, uint32_t steps);
 __global__ void extractSpikesKernel(const uint32_t *apBuf, uint8_t *out, uint32_t n);
+__global__ void flushReadKernel(const uint4 *buf, size_t n, uint32_t *sink);
 __global__ void expfProbeKernel(const float *in, float *out, uint32_t n);
 __global__ void expProbeKernel(const double *in, double *out, uint32_t n);
 // The state-variable input's MF rates for row `row` of its values.

@@ -1175,10 +1175,9 @@ std::string Network::resetGOGODepression(cudaStream_t s)
 Simulator::~Simulator()
 {
 	dropGraphs();
-	if (stepDoneEv_) cudaEventDestroy(stepDoneEv_);
 	if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
 	if (hExport_) cudaFreeHost(hExport_);
-	for (cudaEvent_t e : {stepEv0_, stepEv1_}) if (e) cudaEventDestroy(e);
+	for (cudaEvent_t e : stepEv_) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
 	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_, &dCellOffset_, &dVecUnitOffset_,
 			&dVecPcOffset_, &dVecClaim_})
@@ -1488,7 +1487,7 @@ std::string Simulator::uploadCtl()
 	return "";
 }
 
-std::string Simulator::enqueueStep(uint32_t k, bool instrument)
+std::string Simulator::enqueueStep(uint32_t k, bool instrument, bool chained)
 {
 	const DevNet *const *netsArg = (const DevNet *const *)dNetPtrs_.ptr;
 	const uint32_t *stageArg = (const uint32_t *)dStageBytes_.ptr;
@@ -1502,7 +1501,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 		if (passTmaFn_) {
 			// the per-tile pass takes the single network's descriptor too; the
 			// vector pass takes it alone
-			void *argsTma[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg};
+			void *argsTma[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg, &stepMF_};
 			void *argsVec[] = {&net0Arg, &stepArg, &vecClaimArg};
 			const uint32_t *unitOffArg = (const uint32_t *)dVecUnitOffset_.ptr;
 			const uint32_t *pcOffArg = (const uint32_t *)dVecPcOffset_.ptr;
@@ -1544,11 +1543,32 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 		CK(cudaEventRecordWithFlags(passEv_[2 * k + 1], s0_, cudaEventRecordExternal), "pass timing");
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k], s1_, cudaEventRecordExternal), "tail timing");
 		tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s1_>>>(netsArg, stageArg, k, net0Arg, stage0Arg,
-				mailboxArg_);
+				mailboxArg_, stepMF_);
 		CK(cudaGetLastError(), "launching the small-cell update");
 		CK(cudaEventRecordWithFlags(tailEv_[2 * k + 1], s1_, cudaEventRecordExternal), "tail timing");
 		CK(cudaEventRecord(join_, s1_), "join");
 		CK(cudaStreamWaitEvent(s0_, join_, 0), "join");
+		return recordStep(k);
+	}
+	if (chained) {
+		// steps launched one at a time: the small-cell kernel is the
+		// programmatic dependent of the previous step's GR pass and waits for
+		// it on the device (pdlWait, cbm_kernels.cuh), so that it is resident
+		// when that pass ends; the GR pass follows as before, and its exit
+		// wait makes a finished pass a finished step, so no join is needed
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = dim3(2 * (unsigned)nets_.size());
+		cfg.blockDim = dim3(kTailThreads);
+		cfg.dynamicSmemBytes = tailSmem_;
+		cfg.stream = s0_;
+		cudaLaunchAttribute attr;
+		attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+		attr.val.programmaticStreamSerializationAllowed = 1;
+		cfg.attrs = &attr;
+		cfg.numAttrs = 1;
+		CK(cudaLaunchKernelEx(&cfg, tailKernel, netsArg, stageArg, k, net0Arg, stage0Arg, mailboxArg_, stepMF_),
+				"launching the small-cell update");
+		CKS(launchPass(s0_, true));
 		return recordStep(k);
 	}
 	// One stream: the small-cell CTAs launch first and let the GR pass start
@@ -1556,7 +1576,7 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument)
 	// kernels of a step share no buffer), so the pass cannot take the SMs the
 	// small-cell CTAs need.  The next step waits for both.
 	tailKernel<<<2 * (unsigned)nets_.size(), kTailThreads, tailSmem_, s0_>>>(netsArg, stageArg, k, net0Arg, stage0Arg,
-			mailboxArg_);
+			mailboxArg_, stepMF_);
 	CK(cudaGetLastError(), "launching the small-cell update");
 	CK(cudaEventRecord(join_, s0_), "join");
 	CKS(launchPass(s0_, true));
@@ -1593,47 +1613,61 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
 	CKS(uploadCtl());
-	// one step and its counter update as one graph launch; with deferred MF
-	// input, the graph that first copies pinned slot k into the ring
-	auto capture = [&](cudaGraphExec_t *out, int mfSlot) -> std::string {
-		cudaGraph_t g;
-		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
-		if (mfSlot >= 0) {
+	// Every step is launched on the stream directly, its two kernels each
+	// the programmatic dependent of the kernel before (enqueueStep, chained),
+	// so that each is resident before its predecessor ends.  A single-step
+	// graph launch queued behind a running one started about seven
+	// microseconds after it ended on B200, a plain kernel launch about five.
+	// The device step counter is not advanced per step: step k since the
+	// last settleSteps() runs with step offset k.  Deferred MF input travels
+	// in the launches (mfByParam) or is copied in from its pinned slot first.
+	for (uint32_t k = 0; k < nsteps; k++) {
+		if (directPending_ >= (1u << 30)) CKS(settleSteps());
+		if (pendingMF_ >= 0) {
 			Network &n = *nets_[0];
-			cudaMemcpyAsync((void *)n.h_.mfBits, n.hPinnedBits_ + (size_t)mfSlot * n.h_.mfWords, 4ull * n.h_.mfWords,
-					cudaMemcpyHostToDevice, s0_);
-			cudaEventRecordWithFlags(n.mfStageEv_[mfSlot], s0_, cudaEventRecordExternal);
+			const int slot = pendingMF_;
+			const uint32_t *bits = n.hPinnedBits_ + (size_t)slot * n.h_.mfWords;
+			if (mfByParam()) {
+				// the launches carry the words: the slot is free once they are issued
+				stepMF_.n = n.h_.mfWords;
+				memcpy(stepMF_.w, bits, 4ull * n.h_.mfWords);
+				n.mfStageUsed_[slot] = false;
+			} else {
+				CK(cudaMemcpyAsync((void *)n.h_.mfBits, bits, 4ull * n.h_.mfWords, cudaMemcpyHostToDevice, s0_),
+						"MF upload");
+				CK(cudaEventRecord(n.mfStageEv_[slot], s0_), "MF staging");
+			}
+			pendingMF_ = -1;
 		}
 		// one network: its small-cell kernel publishes the step's NC spikes
 		mailboxArg_ = nets_.size() == 1 ? nets_[0]->dMailbox_ : nullptr;
-		std::string e = enqueueStep(0, false);
+		std::string e = enqueueStep(directPending_, false, true);
 		mailboxArg_ = nullptr;
-		// both kernels done: exports wait for this, not for the counter update
-		cudaEventRecordWithFlags(stepDoneEv_, s0_, cudaEventRecordExternal);
-		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
-		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
+		stepMF_.n = 0;
 		if (!e.empty()) return e;
-		CK(ce, "graph capture");
-		CK(cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
-		cudaGraphDestroy(g);
-		return "";
-	};
-	if (!stepDoneEv_) CK(cudaEventCreateWithFlags(&stepDoneEv_, cudaEventDisableTiming), "event");
-	for (uint32_t k = 0; k < nsteps; k++) {
-		if (pendingMF_ >= 0) {
-			const int slot = pendingMF_;
-			if (!stepGraphMF_[slot]) CKS(capture(&stepGraphMF_[slot], slot));
-			CK(cudaGraphLaunch(stepGraphMF_[slot], s0_), "graph launch");
-			pendingMF_ = -1;
-		} else {
-			if (!stepGraph_) CKS(capture(&stepGraph_, -1));
-			CK(cudaGraphLaunch(stepGraph_, s0_), "graph launch");
-		}
+		directPending_++;
+		for (Network *n : nets_) n->hostT_ += 1;
 	}
-	for (Network *n : nets_) n->hostT_ += nsteps;
-	lastWasStepGraph_ = nsteps > 0;
 	lastStepPublishes_ = nsteps > 0 && nets_.size() == 1;
 	directCopySinceStep_ = false;
+	return "";
+}
+
+bool Simulator::mfByParam() const
+{
+	// the per-tile GR pass and the small-cell kernel take the words from
+	// their launch; the other pass kinds read the MF ring
+	return nets_.size() == 1 && nets_[0]->dev().mfWords <= kMFParamWords && passTmaFn_ && !passVec_ &&
+		!passPersistent_;
+}
+
+std::string Simulator::settleSteps()
+{
+	if (!directPending_) return "";
+	CK(cudaSetDevice(device_), "selecting the device");
+	advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), directPending_);
+	CK(cudaGetLastError(), "advancing the step counter");
+	directPending_ = 0;
 	return "";
 }
 
@@ -1653,19 +1687,15 @@ std::string Simulator::flushPendingMF()
 void Simulator::dropGraphs()
 {
 	if (graphExec_) { cudaGraphExecDestroy(graphExec_); graphExec_ = nullptr; }
-	if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
 	if (flushKernGraph_) { cudaGraphExecDestroy(flushKernGraph_); flushKernGraph_ = nullptr; }
-	if (stepGraph_) { cudaGraphExecDestroy(stepGraph_); stepGraph_ = nullptr; }
-	for (cudaGraphExec_t &e : stepGraphMF_)
-		if (e) { cudaGraphExecDestroy(e); e = nullptr; }
 }
 
 std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
-	lastWasStepGraph_ = false;
 	lastStepPublishes_ = false;
 	pendingMF_ = -1;  // the protocol drives the MF input from now on
+	CKS(settleSteps());
 	CKS(uploadCtl());
 	CK(cudaStreamSynchronize(s0_), "sync");
 	return nets_[i]->setProtocol(p, s0_);
@@ -1674,9 +1704,9 @@ std::string Simulator::setProtocol(size_t i, const cbm_eyelid_protocol &p)
 std::string Simulator::setStateVarInput(size_t i, const cbm_statevar_input &in)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
-	lastWasStepGraph_ = false;
 	lastStepPublishes_ = false;
 	pendingMF_ = -1;  // the coding drives the MF input from now on
+	CKS(settleSteps());
 	CKS(uploadCtl());
 	CK(cudaStreamSynchronize(s0_), "sync");
 	return nets_[i]->setStateVarInput(in, s0_);
@@ -1786,7 +1816,7 @@ std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, 
 		hExportBytes_ = bytes;
 	}
 	if (lastStepPublishes_ && f == F_AP_NC) {
-		// after a single-step graph of one network: the small-cell kernel
+		// after a single step of one network: the small-cell kernel
 		// writes the NC spikes and then the step number into mapped host
 		// memory; wait for the stamp (bounded), without a copy or a stream
 		// synchronisation, while the step's GR pass may still run
@@ -1812,20 +1842,10 @@ std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, 
 		}
 		// no stamp: the synchronising path below reports what happened
 	}
-	if (lastWasStepGraph_) {
-		// after a single-step graph: copy on the second stream as soon as
-		// both kernels are done, beside the step-counter update
-		CK(cudaStreamWaitEvent(s1_, stepDoneEv_, 0), "export");
-		CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s1_));
-		CK(cudaStreamSynchronize(s1_), "export");
-		// every staging slot a launched graph read has been copied (unless
-		// an input copy was issued outside the graphs since)
-		if (!directCopySinceStep_) markInputSlotsFree();
-	} else {
-		CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s0_));
-		CK(cudaStreamSynchronize(s0_), "export");
-		markInputSlotsFree();
-	}
+	// on the step stream, after every kernel launched so far
+	CKS(nets_[i]->exportField(f, zone, hExport_, bytes, s0_));
+	CK(cudaStreamSynchronize(s0_), "export");
+	markInputSlotsFree();
 	CKS(checkDeviceErrors());
 	memcpy(dst, hExport_, bytes);
 	return "";
@@ -1834,8 +1854,8 @@ std::string Simulator::exportField(size_t i, Field f, uint32_t zone, void *dst, 
 std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
-	lastWasStepGraph_ = false;
 	lastStepPublishes_ = false;
+	CKS(settleSteps());
 	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (chunk == 0) chunk = 1;
@@ -1891,48 +1911,65 @@ std::string Simulator::runGraph(uint64_t nsteps, uint32_t chunk, bool instrument
 	return "";
 }
 
+// The L2 flush before a timed step: 2 x L2 bytes written, then read back,
+// so that every line the step finds in L2 is a clean line of the flush
+// buffer and none of the step's inputs (CBM_FLUSH_READ=0: written only, the
+// step then also pays for writing the flush's dirty lines back).
+void Simulator::enqueueFlush()
+{
+	if (!flushBuf_.ptr) return;
+	cudaMemsetAsync(flushBuf_.ptr, 0x5a, flushBuf_.bytes, s0_);
+	const char *env = getenv("CBM_FLUSH_READ");
+	if (env && !strcmp(env, "0")) return;
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
+	flushReadKernel<<<4 * sms, 512, 0, s0_>>>((const uint4 *)flushBuf_.ptr, flushBuf_.bytes / 16,
+			(uint32_t *)flushBuf_.ptr);
+}
+
 std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
-	lastWasStepGraph_ = false;
 	lastStepPublishes_ = false;
+	CKS(settleSteps());
 	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (flushBytes && flushBytes != flushBuf_.bytes) {
-		// the flush graphs write the old buffer
-		if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
+		// the kernel-timing flush graph writes the old buffer
 		if (flushKernGraph_) { cudaGraphExecDestroy(flushKernGraph_); flushKernGraph_ = nullptr; }
 		if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
 		flushBuf_.ptr = nullptr;
 		CK(cudaMalloc(&flushBuf_.ptr, flushBytes), "allocating the L2 flush buffer");
 		flushBuf_.bytes = flushBytes;
 	}
-	if (!flushGraph_) {
-		// one step bracketed by events, after a write of the flush buffer
-		if (!stepEv0_) CK(cudaEventCreate(&stepEv0_), "event");
-		if (!stepEv1_) CK(cudaEventCreate(&stepEv1_), "event");
-		cudaGraph_t g;
-		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
-		if (flushBuf_.ptr) cudaMemsetAsync(flushBuf_.ptr, 0x5a, flushBuf_.bytes, s0_);
-		cudaEventRecordWithFlags(stepEv0_, s0_, cudaEventRecordExternal);
-		std::string e = enqueueStep(0, false);
-		cudaEventRecordWithFlags(stepEv1_, s0_, cudaEventRecordExternal);
-		// the step counter's bookkeeping kernel is not part of the timed step
-		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
-		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
-		if (!e.empty()) return e;
-		CK(ce, "graph capture");
-		CK(cudaGraphInstantiate(&flushGraph_, g, cudaGraphInstantiateFlagUseNodePriority), "graph instantiate");
-		cudaGraphDestroy(g);
+	// each step launched as launchSteps launches it, after the flush and
+	// between a pair of events on the step stream; batches of kBatch steps
+	// between synchronisations, the step counter advanced once per batch
+	constexpr uint32_t kBatch = 256;
+	while (stepEv_.size() < 2 * kBatch) {
+		cudaEvent_t e;
+		CK(cudaEventCreate(&e), "event");
+		stepEv_.push_back(e);
 	}
 	double total = 0;
-	for (uint64_t k = 0; k < nsteps; k++) {
-		CK(cudaGraphLaunch(flushGraph_, s0_), "graph launch");
-		CK(cudaStreamSynchronize(s0_), "step");
-		float ms = 0;
-		CK(cudaEventElapsedTime(&ms, stepEv0_, stepEv1_), "step timing");
-		total += ms;
-		for (Network *n : nets_) n->hostT_ += 1;
+	for (uint64_t done = 0; done < nsteps;) {
+		const uint32_t b = (uint32_t)std::min<uint64_t>(kBatch, nsteps - done);
+		for (uint32_t k = 0; k < b; k++) {
+			enqueueFlush();
+			CK(cudaEventRecord(stepEv_[2 * k], s0_), "step timing");
+			CKS(enqueueStep(k, false));
+			CK(cudaEventRecord(stepEv_[2 * k + 1], s0_), "step timing");
+		}
+		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), b);
+		CK(cudaGetLastError(), "advancing the step counter");
+		CK(cudaStreamSynchronize(s0_), "steps");
+		for (uint32_t k = 0; k < b; k++) {
+			float ms = 0;
+			CK(cudaEventElapsedTime(&ms, stepEv_[2 * k], stepEv_[2 * k + 1]), "step timing");
+			total += ms;
+		}
+		for (Network *n : nets_) n->hostT_ += b;
+		done += b;
 	}
 	CKS(checkDeviceErrors());
 	*stepMs = (float)total;
@@ -1942,14 +1979,13 @@ std::string Simulator::runFlushed(uint64_t nsteps, size_t flushBytes, float *ste
 std::string Simulator::runFlushedKernels(uint64_t nsteps, size_t flushBytes, float *passMs, float *tailMs)
 {
 	CK(cudaSetDevice(device_), "selecting the device");
-	lastWasStepGraph_ = false;
 	lastStepPublishes_ = false;
+	CKS(settleSteps());
 	CKS(flushPendingMF());
 	CKS(uploadCtl());
 	if (flushBytes && flushBytes != flushBuf_.bytes) {
 		if (flushBuf_.ptr) cudaFree(flushBuf_.ptr);
 		flushBuf_.ptr = nullptr;
-		if (flushGraph_) { cudaGraphExecDestroy(flushGraph_); flushGraph_ = nullptr; }
 		if (flushKernGraph_) { cudaGraphExecDestroy(flushKernGraph_); flushKernGraph_ = nullptr; }
 		CK(cudaMalloc(&flushBuf_.ptr, flushBytes), "allocating the L2 flush buffer");
 		flushBuf_.bytes = flushBytes;
@@ -1966,7 +2002,7 @@ std::string Simulator::runFlushedKernels(uint64_t nsteps, size_t flushBytes, flo
 		// a write of the flush buffer
 		cudaGraph_t g;
 		CK(cudaStreamBeginCapture(s0_, cudaStreamCaptureModeThreadLocal), "graph capture");
-		if (flushBuf_.ptr) cudaMemsetAsync(flushBuf_.ptr, 0x5a, flushBuf_.bytes, s0_);
+		enqueueFlush();
 		std::string e = enqueueStep(0, true);
 		advanceStepKernel<<<1, 64, 0, s0_>>>((uint64_t *const *)dTBasePtrs_.ptr, (int)nets_.size(), 1);
 		cudaError_t ce = cudaStreamEndCapture(s0_, &g);
@@ -2015,6 +2051,7 @@ void Simulator::markInputSlotsFree()
 
 std::string Simulator::sync()
 {
+	CKS(settleSteps());
 	CK(cudaStreamSynchronize(s0_), "sync");
 	CK(cudaStreamSynchronize(s1_), "sync");
 	markInputSlotsFree();

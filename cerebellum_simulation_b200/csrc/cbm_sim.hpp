@@ -60,6 +60,10 @@ public:
 
 	// One step of every network with MF input already in each network's ring.
 	std::string launchSteps(uint32_t nsteps);
+	// Add the steps launched one at a time since the last call to the device
+	// step counter (one kernel on the step stream); every other operation
+	// that launches work reading the counter calls it first.
+	std::string settleSteps();
 	// Host MF input for the next step of network i (updateMFInput).
 	std::string stageMF(size_t i, const uint8_t *mf);
 	// Start a device-driven trial protocol on network i from the next step.
@@ -74,9 +78,11 @@ public:
 	// give lastPassMs(): the pass's mean duration over the last replay.
 	std::string runGraph(uint64_t nsteps, uint32_t chunk, bool instrument = false);
 	// Measurement helper: nsteps single-step graph launches, each after a
-	// write of a flushBytes device buffer (an L2 flush when larger than L2),
-	// with events on the launch stream around every step only; *stepMs is
-	// the summed step time.
+	// write and read-back of a flushBytes device buffer (an L2 flush when
+	// larger than L2, leaving only clean lines of the buffer in L2), with
+	// events on the launch stream around every step only; *stepMs is the
+	// summed step time.
+	void enqueueFlush();
 	std::string runFlushed(uint64_t nsteps, size_t flushBytes, float *stepMs);
 	// The same steps in the two-stream form with events around each kernel:
 	// mean GR-pass and small-cell kernel durations of a step after a flush.
@@ -114,23 +120,26 @@ public:
 private:
 	friend class Network;
 	std::string uploadCtl();
-	std::string enqueueStep(uint32_t stepOffset, bool instrument);
+	// chained: launched one at a time, the small-cell kernel as the
+	// programmatic dependent of the previous step (see launchSteps)
+	std::string enqueueStep(uint32_t stepOffset, bool instrument, bool chained = false);
 	std::string recordStep(uint32_t stepOffset);
 	void dropGraphs();
 	void markInputSlotsFree();  // after a full synchronisation
 	// Issue the copy of MF input that a single-step graph would have carried.
 	std::string flushPendingMF();
-	cudaGraphExec_t stepGraph_ = nullptr;  // one step and its counter update (launchSteps)
 	// One network, one-slot MF ring, spike-bit input: updateMFInput only
-	// packs the bits into pinned slot k, and the next step's graph
-	// (stepGraphMF_[k]) copies them in before the kernels.
+	// packs the bits into pinned slot k, and the next step launched by
+	// launchSteps copies them in before its kernels.
 	int pendingMF_ = -1;
-	cudaGraphExec_t stepGraphMF_[kMFStage] = {};
-	// the last launch was a single-step graph: exports wait on stepDoneEv_
-	// (recorded in that graph once both kernels finish) on the second stream
-	cudaEvent_t stepDoneEv_ = nullptr;
-	bool lastWasStepGraph_ = false;
-	bool directCopySinceStep_ = false;  // an MF copy issued outside the step graphs since the last one
+	bool directCopySinceStep_ = false;  // an MF copy issued outside launchSteps since its last step
+	// Steps launched one at a time (launchSteps) since the device step
+	// counter was last advanced: step k of them ran with step offset k.
+	uint32_t directPending_ = 0;
+	// The MF words the next enqueued step's kernels take from their launch
+	// (n = 0: they read the MF ring); see mfByParam().
+	MFParam stepMF_{};
+	bool mfByParam() const;
 	uint8_t *hExport_ = nullptr;           // pinned export staging
 	size_t hExportBytes_ = 0;
 	std::vector<Network *> nets_;
@@ -151,9 +160,9 @@ private:
 	bool passPersistent_ = false;
 	bool passVec_ = false;  // the vector pass (kind 3) runs
 	// the small-cell kernel argument of the step being enqueued: the NC
-	// mailbox while single-step graphs are captured (one network), else null
+	// mailbox for steps launched one at a time (one network), else null
 	uint8_t *mailboxArg_ = nullptr;
-	bool lastStepPublishes_ = false;  // the last launch was a single-step graph that writes the mailbox
+	bool lastStepPublishes_ = false;  // the last launch was a single step that writes the mailbox
 	uint32_t vecClaim_ = 2;  // its units claimed at a time (single network)
 	PassGeometry passGeom_;
 	size_t passTmaSmem_ = 0;
@@ -161,9 +170,9 @@ private:
 	uint32_t graphChunk_ = 0;
 	bool graphInstrumented_ = false;
 	std::vector<cudaEvent_t> passEv_, tailEv_;
-	cudaGraphExec_t flushGraph_ = nullptr, flushKernGraph_ = nullptr;
+	cudaGraphExec_t flushKernGraph_ = nullptr;
 	DeviceBuf flushBuf_;
-	cudaEvent_t stepEv0_ = nullptr, stepEv1_ = nullptr;
+	std::vector<cudaEvent_t> stepEv_;  // runFlushed: a pair around each step of a batch
 	float lastGraphMs_ = 0, lastPassMs_ = 0, lastTailMs_ = 0;
 };
 
