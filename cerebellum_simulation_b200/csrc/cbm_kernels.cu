@@ -267,7 +267,6 @@ __device__ __forceinline__ const DevNet *locateNet(const DevNet *const *nets, co
 __global__ void __launch_bounds__(kPassThreads) grPassKernel(const DevNet *const *nets,
 		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
 {
-	PassStepGuard stepGuard;
 	uint32_t local;
 	const DevNet *__restrict__ N = locateNet(nets, blockOffset, numNets, blockIdx.x, local);
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
@@ -439,9 +438,10 @@ template <> struct PassShape<1> {
 template <int W, int RW, int S, int MINB, int MS, int SH>
 __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevNet *const *nets,
 		const uint32_t *blockOffset, int numNets, uint32_t stepOffset, const DevNet *net0,
-		const __grid_constant__ MFParam mfp)
+		const __grid_constant__ MFParam mfp, uint32_t *exitCount)
 {
-	PassStepGuard stepGuard;
+	// the next step's small-cell kernel may launch (it waits for this pass)
+	pdlLaunchDependents();
 	using Sh = PassShape<SH>;
 	constexpr uint32_t R = W * RW;
 	// one network: its descriptor comes as a parameter (a round trip fewer)
@@ -744,6 +744,8 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 		if (i < N->bcLocal) atomicAdd(&bcOut[bcBase + i], c);
 		else atomicAdd(&scOut[scBase + i - N->bcLocal], c);
 	}
+	__syncthreads();
+	passExitWait(exitCount);
 }
 
 // Geometries the host can pick: (consumer warps, rows per warp, stages,
@@ -754,7 +756,7 @@ __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassTmaKernel(const DevN
 	X(4, 2, 2, 4, 4) X(8, 1, 3, 2, 0) X(4, 1, 4, 1, 0) X(2, 1, 4, 1, 0) X(1, 1, 4, 1, 0)
 #define CBM_PASS_TMA_INST(W, RW, S, B, M) \
 	template __global__ void grPassTmaKernel<W, RW, S, B, M, 0>(const DevNet *const *, const uint32_t *, int, uint32_t, \
-		const DevNet *, const __grid_constant__ MFParam);
+		const DevNet *, const __grid_constant__ MFParam, uint32_t *);
 CBM_PASS_TMA_CONFIGS(CBM_PASS_TMA_INST)
 
 int passTmaConfigCount()
@@ -837,7 +839,6 @@ template <int W, int S, int MINB, int MS>
 __global__ void __launch_bounds__(32 * (W + 1), MINB) grPassPersistentKernel(const DevNet *const *nets,
 		const uint32_t *blockOffset, int numNets, uint32_t stepOffset)
 {
-	PassStepGuard stepGuard;
 	(void)blockOffset; (void)numNets;
 	constexpr uint32_t R = 2 * W;
 	const DevNet *__restrict__ N = nets[0];

@@ -19,17 +19,24 @@ constexpr int kTailThreads = 768;
 //  - the small-cell kernel waits for its predecessor (the previous step's
 //    GR pass) before it reads anything, and only then lets its own
 //    dependent (this step's GR pass) launch;
-//  - every thread of a GR pass waits at its exit for its predecessor (this
-//    step's small-cell kernel), so that a finished GR pass means a finished
-//    step.
+//  - the last CTA of such a GR pass to finish waits for its predecessor
+//    (this step's small-cell kernel) before it exits, so that a finished
+//    GR pass means a finished step (passExitWait).
 // A pass lets the next small-cell kernel launch from its start.  Launched
 // without the attribute (CUDA graphs), each wait returns at once.
 __device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdlLaunchDependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-struct PassStepGuard {
-	__device__ PassStepGuard() { pdlLaunchDependents(); }
-	__device__ ~PassStepGuard() { pdlWait(); }
-};
+// At the end of a GR-pass CTA, after a barrier of the whole CTA: with a
+// counter (chained single steps), the launch's last CTA to get here resets
+// it and waits for the step's small-cell kernel; the others exit, so that
+// the slots of early CTAs go to later waves.
+__device__ __forceinline__ void passExitWait(uint32_t *exitCount)
+{
+	if (exitCount && threadIdx.x == 0 && atomicAdd(exitCount, 1u) == gridDim.x - 1u) {
+		*exitCount = 0;
+		pdlWait();
+	}
+}
 
 __global__ void grPassKernel(const DevNet *const *nets, const uint32_t *blockOffset, int numNets,
 		uint32_t stepOffset);

@@ -335,7 +335,6 @@ __host__ __device__ __forceinline__ uint32_t vecReduceCTAs(uint32_t numPC, uint3
 __global__ void __launch_bounds__(32 * kVecWarps, kVecMinBlocks) grPassVecKernel(const DevNet *__restrict__ N,
 		uint32_t stepOffset, uint32_t claimSize)
 {
-	PassStepGuard stepGuard;
 	const uint64_t t = stepsDone(N) + 1 + stepOffset;
 	const uint32_t numGR = N->numGR, numPC = N->numPC, bs = N->bs;
 	const uint32_t lane = threadIdx.x & 31u;
@@ -444,7 +443,6 @@ __device__ void reducePC(const DevNet *N, uint64_t t, uint32_t pc, float *sTree)
 __global__ void __launch_bounds__(32 * kVecWarps, kVecBatchMinBlocks) grPassVecBatchKernel(const DevNet *const *nets,
 		const uint32_t *unitOffset, const uint32_t *pcOffset, int numNets, uint32_t stepOffset, uint32_t *claimBase)
 {
-	PassStepGuard stepGuard;
 	__shared__ float sTree[512];
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint64_t t0 = stepsDone(nets[0]) + 1 + stepOffset;

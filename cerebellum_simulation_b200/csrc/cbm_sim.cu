@@ -1180,7 +1180,7 @@ Simulator::~Simulator()
 	for (cudaEvent_t e : stepEv_) if (e) cudaEventDestroy(e);
 	for (Network *n : nets_) delete n;
 	for (DeviceBuf *b : {&dNetPtrs_, &dBlockOffset_, &dTBasePtrs_, &dStageBytes_, &dCellOffset_, &dVecUnitOffset_,
-			&dVecPcOffset_, &dVecClaim_})
+			&dVecPcOffset_, &dVecClaim_, &dExitCount_})
 		if (b->ptr) cudaFree(b->ptr);
 	if (s0_) cudaStreamDestroy(s0_);
 	if (s1_) cudaStreamDestroy(s1_);
@@ -1236,6 +1236,8 @@ std::string Simulator::create(const std::vector<State *> &states, const std::vec
 	CKS(up(dBlockOffset_, offs.data(), offs.size() * sizeof(uint32_t)));
 	CKS(up(dTBasePtrs_, tb.data(), tb.size() * sizeof(uint64_t *)));
 	CKS(up(dStageBytes_, stage.data(), stage.size() * sizeof(uint32_t)));
+	const uint32_t zero = 0;
+	CKS(up(dExitCount_, &zero, sizeof(zero)));
 	if (passSmem_ > 48 * 1024)
 		CK(cudaFuncSetAttribute(grPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem_), "pass smem");
 	if (tailSmem_ > 48 * 1024)
@@ -1501,7 +1503,10 @@ std::string Simulator::enqueueStep(uint32_t k, bool instrument, bool chained)
 		if (passTmaFn_) {
 			// the per-tile pass takes the single network's descriptor too; the
 			// vector pass takes it alone
-			void *argsTma[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg, &stepMF_};
+			// chained single steps: the pass's last CTA waits for the step's
+			// small-cell kernel (passExitWait) on this simulator's counter
+			uint32_t *exitArg = chained ? (uint32_t *)dExitCount_.ptr : nullptr;
+			void *argsTma[] = {&netsArg, &offsArg, &numNetsArg, &stepArg, &net0Arg, &stepMF_, &exitArg};
 			void *argsVec[] = {&net0Arg, &stepArg, &vecClaimArg};
 			const uint32_t *unitOffArg = (const uint32_t *)dVecUnitOffset_.ptr;
 			const uint32_t *pcOffArg = (const uint32_t *)dVecPcOffset_.ptr;
@@ -1641,7 +1646,9 @@ std::string Simulator::launchSteps(uint32_t nsteps)
 		}
 		// one network: its small-cell kernel publishes the step's NC spikes
 		mailboxArg_ = nets_.size() == 1 ? nets_[0]->dMailbox_ : nullptr;
-		std::string e = enqueueStep(directPending_, false, true);
+		// the chain needs the per-tile pass's exit wait; other pass kinds
+		// are launched in plain stream order
+		std::string e = enqueueStep(directPending_, false, passTmaFn_ && !passVec_ && !passPersistent_);
 		mailboxArg_ = nullptr;
 		stepMF_.n = 0;
 		if (!e.empty()) return e;

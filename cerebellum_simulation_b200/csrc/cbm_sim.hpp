@@ -147,6 +147,7 @@ private:
 	cudaStream_t s0_ = nullptr, s1_ = nullptr;
 	cudaEvent_t fork_ = nullptr, join_ = nullptr, ev0_ = nullptr, ev1_ = nullptr, tev0_ = nullptr, tev1_ = nullptr;
 	DeviceBuf dNetPtrs_, dBlockOffset_, dTBasePtrs_, dStageBytes_;
+	DeviceBuf dExitCount_;    // the per-tile pass's CTAs that finished a chained single step (passExitWait)
 	DeviceBuf dCellOffset_;   // trialDataBatchKernel's instance map (batches recording trial data)
 	// the batched vector pass: first 128-cell unit and first PC of each
 	// network (numNets + 1 prefix sums each), and its three claim counters
