@@ -189,6 +189,48 @@ def test_config3_4m_bit_exact_short(tmp_path):
     assert compare_states(fo, fp) == []
 
 
+@pytest.mark.parametrize("name", ["config2", "config3"])
+def test_chained_single_steps_equal_graph_runs(tmp_path, name):
+    """Single steps queued without a synchronisation between them run as a
+    chain of programmatic dependent launches (each small-cell kernel waits
+    on the device for the previous step's GR pass, whose last CTA waits for
+    its own step's small-cell kernel).  Such steps, on the 1M-GR network
+    (the pass in one wave) and on the dense 4M-GR network (the pass in four
+    waves), advance the network exactly as graph-chunk replays do."""
+    import cerebellum_simulation_b200 as cbm
+    from cerebellum_simulation_b200 import networks
+    if name == "config2":
+        net, n = networks.config2_network(seed=3), 240
+        mf = networks.eyelid_mf_stream(1024, n, seed=3, cs_on=40, cs_off=200)
+    else:
+        net, n = networks.config3_network(seed=3), 60
+        mf = networks.config3_mf_stream(1024, n, seed=3)
+    p = str(tmp_path / "net.state")
+    net.writeState(p)
+    events = {2: [("plast", 0, -0.0005, 0.0005)], n // 2: [("errdrive", 0, 1.0)]}
+    a = cbm.CBMSimCore(cbm.CBMState(p), [5], device=0)
+    cbmtest.product_run(a, mf, events, record=False)
+    fa = str(tmp_path / "a.state")
+    a.writeToState(fa)
+    b = cbm.CBMSimCore(cbm.CBMState(p), [5], device=0, resident_steps=n)
+    b.load_mf_stream(cbm.mf_bits(mf, b.mf_words()))
+    zone = b.getMZoneList()[0]
+    t = 0
+    for te in sorted(events):
+        b.run(te - 1 - t, chunk=16)
+        t = te - 1
+        for ev in events[te]:
+            if ev[0] == "plast":
+                zone.setGRPCPlastSteps(ev[2], ev[3])
+            else:
+                b.updateErrDrive(ev[1], ev[2])
+    b.run(n - t, chunk=16)
+    assert b.steps_done() == n
+    fb = str(tmp_path / "b.state")
+    b.writeToState(fb)
+    assert compare_states(fa, fb) == []
+
+
 @pytest.mark.parametrize("name,vec", [("config2", "0"), ("config2", "1"), ("config3", "0")])
 def test_large_networks_match_reference_golden(tmp_path, name, vec, monkeypatch):
     """The device against the reference itself, with no oracle in between:
