@@ -179,7 +179,10 @@ int cbm_sim_create_resident(cbm_state *s, const int *mzoneSeeds, int device, uin
  * Takes effect for the next cbm_sim_calc_activity. */
 int cbm_sim_update_mf(cbm_sim *sim, const uint8_t *mf);
 
-/* CBMSimCore::calcActivity (cbmsimcore.cpp:139-310): one 1 ms step. */
+/* CBMSimCore::calcActivity (cbmsimcore.cpp:139-310): one 1 ms step.  Returns
+ * once the step is queued on the device; calls without an export in between
+ * queue steps back to back.  An AP_NC export after a step of one network
+ * returns as soon as that step's NC spikes are final. */
 int cbm_sim_calc_activity(cbm_sim *sim);
 
 /* CBMSimCore::updateErrDrive (cbmsimcore.cpp:322-325). */
